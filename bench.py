@@ -1,0 +1,329 @@
+"""Benchmark of the splat path: one frame = project + SH + key + sort of the
+4M-splat SH-degree-3 float32 workload (1920x1080, fov 50, 32-bit keys).
+
+python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+One process per GPU (torchrun for N > 1): each rank runs its own replica of
+the workload (the path shards by object and view; no collective is needed),
+timed on the device with CUDA events between barriers; the time is the max
+over ranks and `value` counts the splats of every rank. Rank 0 prints one JSON
+line. --impl reference times the reference's CPU path (the float64 port of
+SortKeys.compute / SortKeys.sort and of the projection) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Msplats/s (project+SH+key+sort)"
+N_SPLATS = 4_000_000
+SH_DEGREE = 3
+BITS = 32
+# Algorithmic bytes per splat (project+SH+key+sort): inputs 236, outputs 40,
+# key + index 8, sort 16 per 8-bit pass + 4
+FRAME_BYTES = 236 + 40 + 8 + 16 * (BITS // 8) + 4
+# The projection kernel alone: inputs 236, outputs 40, the key 4
+PROJECT_BYTES = 236 + 40 + 4
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--n", type=int, default=N_SPLATS)
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per projection launch from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "project_kernel_4m_sh3.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+class Clocks:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(device)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in out.strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(n, device):
+    import numpy as np
+    import torch
+
+    from radix_b200 import synthetic as syn
+    d = syn.mixture_table(n, seed=0, sh_degree=SH_DEGREE)
+    cols = ("centers", "log_scales", "quats", "opacities", "colors")
+    host = {k: torch.from_numpy(np.ascontiguousarray(d[k])).pin_memory() for k in cols}
+    dev = {k: v.to(device) for k, v in host.items()}
+    return d, host, dev
+
+
+def table_of(cols):
+    import radix_b200 as rb
+    return rb.Table.raw(cols["centers"], cols["log_scales"], cols["quats"], cols["opacities"], cols["colors"], SH_DEGREE)
+
+
+def cpu_baseline(n_sample):
+    """The oracle (float64 port of the reference's CPU path) on a bounded sample:
+    projection + SH + keys on all host threads, SortKeys.sort single-threaded."""
+    import numpy as np
+
+    import radix_b200 as rb
+    from oracle import oracle as orc
+    from radix_b200 import synthetic as syn
+    d = syn.mixture_table(n_sample, seed=0, sh_degree=SH_DEGREE)
+    obj = [rb.SplatObject(rb.Table.from_dict(d))]
+    cam = syn.scale_camera()
+    times, sort_times = [], []
+    for i in range(4):
+        t0 = time.perf_counter()
+        ref = orc.project(obj, cam, None, BITS, cull_keys=True, threads=0)
+        t1 = time.perf_counter()
+        orc.sort(ref["keys"], n_sample, BITS)
+        t2 = time.perf_counter()
+        if i:
+            times.append(t2 - t0)
+            sort_times.append(t2 - t1)
+    t = statistics.median(times)
+    # the reference's own CPU path (SortKeys.compute + SortKeys.sort, one worker)
+    dist = ref["distance"]
+    ks = []
+    for i in range(4):
+        t0 = time.perf_counter()
+        keys = orc.sort_keys(dist, BITS)
+        orc.sort(keys, n_sample, BITS)
+        if i:
+            ks.append(time.perf_counter() - t0)
+    threads = os.cpu_count() or 1
+    return {"value": n_sample / t / 1e6, "unit": "Msplats/s", "cores": threads, "kind": "port",
+            "sample": f"{n_sample} splats of the same workload; float64 projection+SH+keys on {threads} threads "
+                      f"(OpenMP), SortKeys.sort restated in C on 1 thread; median of 3 after 1 warm-up",
+            "keys_sort_only_msplats_s_1thread": n_sample / statistics.median(ks) / 1e6}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import radix_b200 as rb
+    from oracle import oracle as orc
+    from radix_b200 import synthetic as syn
+    n = min(args.n, 1_000_000)
+    d = syn.mixture_table(n, seed=0, sh_degree=SH_DEGREE)
+    obj = [rb.SplatObject(rb.Table.from_dict(d))]
+    cam = syn.scale_camera()
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        ref = orc.project(obj, cam, None, BITS, cull_keys=True, threads=0)
+        orc.sort(ref["keys"], n, BITS)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    t = sum(times) / len(times)
+    value = n / t / 1e6
+    threads = os.cpu_count() or 1
+    line = {
+        "metric": METRIC, "value": value, "unit": "Msplats/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded mulberry32)",
+        "config": {"workload": f"project+SH+key+sort, {n} splats (a bounded sample of the 4M SH-3 workload), "
+                               "1920x1080 fov 50, 32-bit keys", "n": n, "sh_degree": SH_DEGREE, "bits": BITS},
+        "cpu_baseline": {"value": value, "unit": "Msplats/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} splats per step; float64 projection on {threads} threads, sort on 1"},
+        "e2e": {"value": value, "unit": "Msplats/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    import radix_b200 as rb
+    from radix_b200 import synthetic as syn
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+
+    n = args.n
+    d, host_cols, dev_cols = make_workload(n, device)
+    cam = syn.scale_camera()
+    ctx = rb.Context(local)
+    table = table_of(dev_cols)
+    obj = [rb.SplatObject(table)]
+    names = ("mean2d", "conic", "depth", "opacity", "rgb", "keys")
+    out = rb._alloc_outputs(names, n, 1, device)
+    ordering = torch.empty(n, dtype=torch.int32, device=device)
+    visible = torch.zeros(1, dtype=torch.int32, device=device)
+    ctx.reserve(n)
+
+    def step():
+        rb.frame(obj, cam, None, BITS, names, ctx=ctx, out=out, ordering=ordering, visible=visible)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.set_profiling(True)
+    ctx.phase_times()
+    launches0 = ctx.launches()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.steps):
+        step()
+    stop.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clock_info = clocks.stop()
+    ms_total = start.elapsed_time(stop)
+    launches = ctx.launches() - launches0
+    phases = ctx.phase_times()
+    ctx.set_profiling(False)
+    if world > 1:
+        t = torch.tensor([ms_total], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = world * n * args.steps / (ms_total / 1e3) / 1e6
+
+    # end to end through the public API: pinned host tables in, the order and
+    # the visible count out, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        host_table = table_of(host_cols)
+        host_order = torch.empty(n, dtype=torch.int32).pin_memory()
+        hobj = [rb.SplatObject(host_table)]
+        bi = sum(v.numel() * v.element_size() for v in host_cols.values())
+        bo = n * 4 + 4
+        e2e_steps = max(3, min(args.steps, 10))
+        rb.frame(hobj, cam, None, BITS, names, ctx=ctx, out=out, ordering=host_order)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(e2e_steps):
+            rb.frame(hobj, cam, None, BITS, names, ctx=ctx, out=out, ordering=host_order)
+        e1.record()
+        torch.cuda.synchronize()
+        e_ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([e_ms], device=device, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e2e = {"value": world * n * e2e_steps / (e_ms / 1e3) / 1e6, "unit": "Msplats/s",
+               "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo, "ms_per_step": e_ms / e2e_steps}
+
+    peak, peak_kind = peak_hbm()
+    proj_ms, proj_runs = phases["project"]
+    sort_ms, sort_runs = phases["sort"]
+    proj_avg = proj_ms / max(proj_runs, 1)
+    achieved = PROJECT_BYTES * n / (proj_avg / 1e3) / 1e9
+    traffic = ncu_traffic()
+    line = {
+        "metric": METRIC, "value": value, "unit": "Msplats/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded mulberry32 + Box-Muller)",
+        "config": {"workload": "project+SH+key+sort, 4M splats, SH degree 3 fp32, Gaussian-mixture centres, "
+                               "1920x1080 fov 50, 32-bit keys, stable order",
+                   "n": n, "sh_degree": SH_DEGREE, "bits": BITS, "parallelism": f"replicas{world}",
+                   "l2": "inputs 944 MB > 126 MB L2 (no flush)",
+                   "frame_bytes_per_splat": FRAME_BYTES,
+                   "hbm_frac_frame": FRAME_BYTES * n / (ms_step / 1e3) / 1e9 / peak,
+                   "project_ms": proj_avg, "sort_ms": sort_ms / max(sort_runs, 1)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "k_project (raw, SH 3, 1 eye)",
+                     "bytes_per_splat": PROJECT_BYTES, "peak_kind": peak_kind},
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clock_info,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(500_000)
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,297 @@
+/*
+ * radix_b200.h - C ABI of the B200 (sm_100a) splat pipeline: back-to-front
+ * sort keys, a stable onesweep radix sort of keys and indices, EWA projection
+ * of 3D covariances to 2D conics, and spherical-harmonic colour (bands 1-4
+ * over the base colour).
+ *
+ * Every entry point replaces one interface of @sparkjsdev/radix (paths below
+ * are inside that project). All pointers are plain C pointers. A pointer may
+ * address device memory (cudaMalloc / torch) or host memory; host buffers are
+ * staged through the context's device buffers, and a call that touches host
+ * memory returns only after its results are in place. A call on device memory
+ * only returns after enqueueing its kernels on the context's stream.
+ *
+ * Matrices are 4x4, float64, column-major (element (row r, column c) at
+ * [c * 4 + r]): the order of three.js Matrix4.elements.
+ *
+ * Errors: every call returns an RDX_* status; rdx_last_error() gives the
+ * message of the last failure on that context (the reference's Error texts
+ * where it has one).
+ */
+#ifndef RADIX_B200_H
+#define RADIX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RDX_VERSION 1
+
+#define RDX_OK 0
+#define RDX_ERR_ARG 1          /* invalid argument (bad bits, null pointer, ...) */
+#define RDX_ERR_CAPACITY 2     /* an output too small, or a size above a limit */
+#define RDX_ERR_CUDA 3         /* a CUDA runtime error */
+#define RDX_ERR_TIMEOUT 4      /* a bounded device wait gave up (lookback) */
+#define RDX_ERR_UNSUPPORTED 5  /* a layout / degree / option this build lacks */
+#define RDX_ERR_NOMEM 6        /* device or pinned host allocation failed */
+
+/* Splat table layouts */
+#define RDX_LAYOUT_RAW 0  /* float32 columns (3DGS parameters) */
+#define RDX_LAYOUT_EXT 1  /* Radix extSplats (2 x uint32x4) + extSh texels */
+
+/* Element types of a raw table's colour block */
+#define RDX_DTYPE_F32 0
+#define RDX_DTYPE_F16 1
+
+/* Projection passes (SplatProjector.ts ProjectPass) */
+#define RDX_PASS_FULL 0 /* words / float outputs and keys */
+#define RDX_PASS_KEYS 1 /* keys only (the CPU-sort pass, SplatProjection.writeKeys) */
+
+typedef struct rdx_ctx rdx_ctx;
+
+/*
+ * One splat table.
+ *
+ * RDX_LAYOUT_RAW: columns of `count` rows
+ *   centers      float32 [count][3]
+ *   log_scales   float32 [count][3]   (scale = exp(log_scale))
+ *   quats        float32 [count][4]   (x, y, z, w; normalised on use)
+ *   opacities    float32 [count]      (1 = opaque; above 1 = LoD stretch)
+ *   colors       [count][1 + K][3] of color_dtype: the base rgb (band 0),
+ *                then K = 3 / 8 / 15 / 24 SH coefficients of bands
+ *                1..sh_degree, coefficient-major RGB (src/core/sh.ts:7-11).
+ *   Rows of colors must start 4-byte aligned; other columns as their type.
+ *
+ * RDX_LAYOUT_EXT: Radix's ArrayData columns, drop-in
+ *   ext_a, ext_b uint32 [count][4]    (src/core/splats.ts:10-24)
+ *   ext_sh[t]    uint32 [count][4]    texel channel t (extShA, extShB, ...),
+ *                one ext rgb word per SH coefficient (src/core/sh.ts:114-135);
+ *                ceil(K / 4) channels for degree sh_degree.
+ */
+typedef struct rdx_table {
+  int32_t layout;      /* RDX_LAYOUT_RAW or RDX_LAYOUT_EXT */
+  int32_t sh_degree;   /* 0..4: SH bands stored above the base colour */
+  int32_t color_dtype; /* raw only: RDX_DTYPE_F32 or RDX_DTYPE_F16 */
+  int32_t reserved;
+  uint64_t count;
+  const float* centers;
+  const float* log_scales;
+  const float* quats;
+  const float* opacities;
+  const void* colors;
+  const uint32_t* ext_a;
+  const uint32_t* ext_b;
+  const uint32_t* ext_sh[6];
+} rdx_table;
+
+/*
+ * Projection parameters: SplatViewParams + SplatObjectParams
+ * (src/render/splatParams.ts:8-43), defaults from rdx_params_default
+ * (splatParams.ts:68-72).
+ */
+typedef struct rdx_params {
+  float max_std_dev;      /* sqrt(8) */
+  float min_alpha;        /* 0.5 / 255 */
+  float falloff;          /* 1 (read by the draw only) */
+  int32_t lod_inflate;    /* 1 */
+  float blur_amount;      /* 0.3 px^2 */
+  float pre_blur_amount;  /* 0 */
+  float clip_xy;          /* 1.4 */
+  float min_pixel_radius; /* 0 */
+  float max_pixel_radius; /* 512 */
+  float min_contribution; /* 0 */
+  float focal_distance;   /* 0 */
+  float aperture_tan;     /* 0 */
+  float sort_guard;       /* 0 */
+  int32_t max_sh_degree;  /* 4 */
+} rdx_params;
+
+/* One eye: world -> eye (camera.matrixWorldInverse) and its projection */
+typedef struct rdx_eye {
+  double view[16];
+  double projection[16];
+  int32_t ortho;
+  int32_t reserved;
+} rdx_eye;
+
+/*
+ * The camera of one render (SplatCamera.setViews, src/render/splatCamera.ts:
+ * 119-138): world -> head, 1 or 2 eyes sharing one render size, and the NDC
+ * depth of the near plane (0: WebGPU clip convention, -1: WebGL).
+ */
+typedef struct rdx_camera {
+  double head[16];
+  int32_t eyes;
+  int32_t reserved;
+  rdx_eye eye[2];
+  double width;
+  double height;
+  double ndc_z_min;
+} rdx_camera;
+
+/*
+ * One splat object of a collection (SplatCollection.ts:54-65): `count` splats
+ * of `table` drawn with `world` (object -> world). Projected splat i of the
+ * collection is splat i - offset of the object holding it; offsets are the
+ * running sum of counts in object order. `params` overrides the call's params
+ * for this object (NULL: the call's).
+ */
+typedef struct rdx_object {
+  const rdx_table* table;
+  uint64_t count;
+  double world[16];
+  const rdx_params* params;
+} rdx_object;
+
+/*
+ * Projection outputs; any pointer may be NULL (not written). E = eyes,
+ * n = splats of the collection. A culled eye writes zeros (opacity 0), as the
+ * reference marks a culled eye by a zero opacity byte.
+ *   mean2d   float32 [E][n][2]  pixels, (ndc + 1) / 2 * size (y up, as NDC)
+ *   conic    float32 [E][n][3]  inverse of the blurred 2D covariance
+ *                               (a, b, d) in px^2: (d, -b, a) / det
+ *   depth    float32 [E][n]     -z in the eye
+ *   opacity  float32 [E][n]     opacity after the blur compensation
+ *   rgb      float32 [E][n][3]  base colour + SH from the head, clamped at 0
+ *   radii    float32 [E][n][3]  bound half extents (px) and angle [0, pi)
+ *   words    uint32  [n][4E]    the ewa words per eye (projections.tsl.ts:
+ *                               135-140): ndc 2x16; depth20 | angle12 << 20;
+ *                               ext rgb; opacity8 | 2 x 12-bit log2 scales
+ *   keys     uint32  [n]        sort keys (SplatProjection.ts:141-153)
+ */
+typedef struct rdx_outputs {
+  float* mean2d;
+  float* conic;
+  float* depth;
+  float* opacity;
+  float* rgb;
+  float* radii;
+  uint32_t* words;
+  uint32_t* keys;
+} rdx_outputs;
+
+/* ---- context ---- */
+
+/* A context on CUDA device `device`: its stream, scratch and error state. */
+int rdx_ctx_create(int device, rdx_ctx** out);
+int rdx_ctx_destroy(rdx_ctx* ctx);
+/* Run on `stream` (a cudaStream_t; NULL: the context's own stream). */
+int rdx_ctx_set_stream(rdx_ctx* ctx, void* stream);
+/* Wait for the context's stream; reports a device-side timeout flag. */
+int rdx_ctx_synchronize(rdx_ctx* ctx);
+/* Grow scratch for sorts of up to max_keys keys, so later calls allocate nothing. */
+int rdx_ctx_reserve(rdx_ctx* ctx, uint64_t max_keys);
+/* Text of the context's last error ("" when none). */
+const char* rdx_last_error(const rdx_ctx* ctx);
+int rdx_version(void);
+
+/*
+ * Phase timing, after the reference's GpuProfiler phases (src/gpu/GpuProfiler.ts:
+ * 1-57, SplatRenderer.ts:141-142, 426-437): with profiling on, calls record CUDA
+ * events around each phase on the context's stream. rdx_ctx_phase_times waits
+ * for the stream and returns, per phase, the summed milliseconds and the number
+ * of timed runs since the last read, then clears them.
+ */
+#define RDX_PHASE_PROJECT 0 /* the fused projection kernel(s) */
+#define RDX_PHASE_SORT 1    /* histogram + onesweep passes (+ compaction) */
+#define RDX_PHASE_COPY_IN 2 /* host -> device staging */
+#define RDX_PHASE_COPY_OUT 3
+#define RDX_PHASES 4
+int rdx_ctx_set_profiling(rdx_ctx* ctx, int on);
+int rdx_ctx_phase_times(rdx_ctx* ctx, double* ms, uint64_t* runs);
+/* Kernels this context has launched since it was created. */
+int rdx_ctx_launches(rdx_ctx* ctx, uint64_t* launches);
+
+/* Fill `p` with the reference's defaults (splatParams.ts:68-72). */
+void rdx_params_default(rdx_params* p);
+
+/* ---- sort keys ---- */
+
+/*
+ * SortKeys.compute (src/core/sort.ts:46-58) for n float64 distances: the
+ * distance rounded to float32, non-finite -> the invalid key 2^bits - 1,
+ * else min(mask ^ q, validMax).
+ */
+int rdx_sort_keys_compute(rdx_ctx* ctx, const double* distances, uint64_t n, int bits, uint32_t* keys);
+/* GpuSortKeys.compute (src/gpu/sortKey.tsl.ts:17-26): float32 distances, max(d, 0). */
+int rdx_sort_keys_compute_f32(rdx_ctx* ctx, const float* distances, uint64_t n, int bits, uint32_t* keys);
+
+/* ---- sorting ---- */
+
+/*
+ * SortKeys.sort (src/core/sort.ts:64-82): the stable ascending order of the
+ * first `count` keys as indices into `ordering` (ordering_len >= count, else
+ * RDX_ERR_CAPACITY with the reference's message; entries past count are left
+ * as they are). Keys use their low `bits` bits. *visible = count minus the
+ * keys whose top digit of the reference's layout is all ones (16 bits: the
+ * key; 24: its top 13 bits; 32: its top 16 bits). visible may be NULL.
+ */
+int rdx_sort(rdx_ctx* ctx, const uint32_t* keys, uint64_t count, int bits,
+             uint32_t* ordering, uint64_t ordering_len, uint32_t* visible);
+
+/*
+ * WgpuRadixSort.sort (src/wgpu/WgpuRadixSort.ts:118-128): sort the first
+ * `count` keys and values in place, ascending and stable; keys below 2^bits.
+ * The result is always in the caller's buffers (no buffer swap).
+ */
+int rdx_sort_pairs(rdx_ctx* ctx, uint32_t* keys, uint32_t* values, uint64_t count, int bits);
+
+/*
+ * WgpuRadixSort.sortIndirect (WgpuRadixSort.ts:132-141): sort the first
+ * min(*count_dev, capacity) pairs, with the count read on the device (device
+ * pointers only; nothing is read back).
+ */
+int rdx_sort_pairs_indirect(rdx_ctx* ctx, uint32_t* keys, uint32_t* values,
+                            const uint32_t* count_dev, uint64_t capacity, int bits);
+
+/*
+ * WgpuCompact.compact (src/wgpu/WgpuCompact.ts:22-132): the keys of the first
+ * n that are not `invalid`, with their indices as values, to the front of
+ * keys_out / values_out in input order; their number to *count_out.
+ */
+int rdx_compact(rdx_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t invalid,
+                uint32_t* keys_out, uint32_t* values_out, uint32_t* count_out);
+
+/*
+ * WgpuSplatSorter.sort (src/wgpu/WgpuSplatSorter.ts:64-71): compact away the
+ * invalid keys (2^bits - 1) of `count` projected keys, sort the rest back to
+ * front: values[i] is the i-th splat drawn, *count_out the visible count, and
+ * draw_args (5 x uint32, may be NULL) the drawIndexedIndirect arguments
+ * [6 * 1024, ceil(visible / 1024), 0, 0, 0] (WgpuSplatSorter.ts:46-57).
+ */
+int rdx_splat_sort(rdx_ctx* ctx, const uint32_t* keys, uint64_t count, int bits,
+                   uint32_t* values, uint32_t* count_out, uint32_t* draw_args);
+
+/* ---- projection ---- */
+
+/*
+ * projectCollection (src/render/SplatProjector.ts:106-139) with the ewa
+ * method: every object's splats through its SH (from the head, in object
+ * space), its transform to head space, and each eye's EWA projection, fused
+ * in one launch. pass RDX_PASS_KEYS writes keys only. cull_keys: keys of
+ * splats culled in every eye are invalid (the GPU sort's order); else only
+ * invisible splats and those outside params.sort_guard get it.
+ */
+int rdx_project(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
+                const rdx_params* params, int sort_bits, int pass, int cull_keys,
+                const rdx_outputs* out);
+
+/*
+ * One frame: rdx_project (full pass, cull_keys on) then the stable sort of its
+ * keys, as SplatRenderer.update runs it (SplatRenderer.ts:412-456):
+ * ordering[i] (i < n) is the i-th splat back to front, culled splats last in
+ * index order; *visible the number drawn. out->keys may be NULL (the keys then
+ * live in scratch).
+ */
+int rdx_frame(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
+              const rdx_params* params, int sort_bits, const rdx_outputs* out,
+              uint32_t* ordering, uint32_t* visible);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RADIX_B200_H */

@@ -1,0 +1,846 @@
+/*
+ * oracle.c - CPU FP64 restatement of the @sparkjsdev/radix per-frame splat path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This file is the checker the CUDA kernels are
+ * compared against (tests/, the smoke check and the CPU baseline of bench.py);
+ * the product never links it. Paths in citations are inside the radix project.
+ *
+ * Precision: every value is float64, as the reference's CPU functions (JS
+ * numbers) are. Where the reference's CPU path rounds to float32 (the
+ * distance of a sort key goes through a Float32Array), this does too.
+ * Compile with -ffp-contract=off: the sort-key distance and the
+ * centre culls must round exactly as the device's non-contracted float64
+ * arithmetic does.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+static const double PI = 3.14159265358979323846;
+static const double E_CONST = 2.71828182845904523536;
+
+/* ---- sort keys: src/core/sort.ts:29-58 ---- */
+
+#define KEY16_LO (95u << 23)
+#define KEY16_HI ((159u << 23) - 1u)
+#define FLOAT_BITS_INFINITY 0x7f800000u
+
+uint32_t orc_invalid_key(int bits) { /* sort.ts:37-39 */
+  return bits == 32 ? 0xffffffffu : ((1u << bits) - 1u);
+}
+
+uint32_t orc_valid_max(int bits) { /* sort.ts:41-43 */
+  return (0xffu << (bits - 8)) - 1u;
+}
+
+static uint32_t key_of_bits(uint32_t f, int bits) {
+  const uint32_t mask = orc_invalid_key(bits);
+  if (!(f < FLOAT_BITS_INFINITY)) {
+    return mask;
+  }
+  uint32_t q;
+  if (bits == 32) {
+    q = f;
+  } else if (bits == 24) {
+    q = f >> 7;
+  } else {
+    uint32_t c = f < KEY16_LO ? KEY16_LO : (f > KEY16_HI ? KEY16_HI : f);
+    q = (c - KEY16_LO) >> 13;
+  }
+  uint32_t k = mask ^ q;
+  uint32_t vmax = orc_valid_max(bits);
+  return k < vmax ? k : vmax;
+}
+
+/* SortKeys.compute, sort.ts:46-58: the distance through a Float32Array */
+uint32_t orc_sort_key(double distance, int bits) {
+  float f32 = (float)distance;
+  uint32_t f;
+  memcpy(&f, &f32, 4);
+  return key_of_bits(f, bits);
+}
+
+/* GpuSortKeys.compute, sortKey.tsl.ts:17-26: float32 distance, max(d, 0) */
+uint32_t orc_sort_key_f32(float distance, int bits) {
+  float d = distance;
+  if (!(d > 0.0f) && !isnan(d)) {
+    d = 0.0f;
+  }
+  uint32_t f;
+  memcpy(&f, &d, 4);
+  return key_of_bits(f, bits);
+}
+
+void orc_sort_keys(const double* distances, uint64_t n, int bits, uint32_t* keys) {
+  for (uint64_t i = 0; i < n; i++) {
+    keys[i] = orc_sort_key(distances[i], bits);
+  }
+}
+
+/* ---- SortKeys.sort: sort.ts:64-163, the same digit layouts ---- */
+
+static uint32_t hist_lo[65536];
+static uint32_t hist_hi[65536];
+
+static void prefix_sum(uint32_t* h, uint32_t last) { /* sort.ts:85-92 */
+  uint32_t sum = 0;
+  for (uint32_t d = 0; d <= last; d++) {
+    uint32_t n = h[d];
+    h[d] = sum;
+    sum += n;
+  }
+}
+
+int orc_sort(const uint32_t* keys, uint64_t count, int bits, uint32_t* ordering,
+             uint64_t ordering_len, uint32_t* visible_out) {
+  if (ordering_len < count) {
+    return -1; /* sort.ts:70-72 */
+  }
+  uint32_t visible = 0;
+  if (bits == 16) { /* sort1x16, sort.ts:97-110 */
+    memset(hist_lo, 0, sizeof(hist_lo));
+    for (uint64_t i = 0; i < count; i++) hist_lo[keys[i] & 0xffffu] += 1;
+    visible = (uint32_t)count - hist_lo[0xffff];
+    prefix_sum(hist_lo, 0xffff);
+    for (uint64_t i = 0; i < count; i++) ordering[hist_lo[keys[i] & 0xffffu]++] = (uint32_t)i;
+  } else {
+    /* sort11x13 (sort.ts:113-137) and sort2x16 (139-163); 24-bit keys use their low 24 bits */
+    const int lo_bits = bits == 24 ? 11 : 16;
+    const uint32_t lo_mask = (1u << lo_bits) - 1u;
+    const uint32_t hi_last = bits == 24 ? 0x1fffu : 0xffffu;
+    const uint32_t key_mask = bits == 24 ? 0xffffffu : 0xffffffffu;
+    uint32_t* scratch_index = (uint32_t*)malloc(count ? count * 4 : 4);
+    uint16_t* scratch_digit = (uint16_t*)malloc(count ? count * 2 : 2);
+    memset(hist_lo, 0, (size_t)(lo_mask + 1) * 4);
+    memset(hist_hi, 0, (size_t)(hi_last + 1) * 4);
+    for (uint64_t i = 0; i < count; i++) {
+      uint32_t k = keys[i] & key_mask;
+      hist_lo[k & lo_mask] += 1;
+      hist_hi[k >> lo_bits] += 1;
+    }
+    visible = (uint32_t)count - hist_hi[hi_last];
+    prefix_sum(hist_lo, lo_mask);
+    prefix_sum(hist_hi, hi_last);
+    for (uint64_t i = 0; i < count; i++) {
+      uint32_t k = keys[i] & key_mask;
+      uint32_t pos = hist_lo[k & lo_mask]++;
+      scratch_index[pos] = (uint32_t)i;
+      scratch_digit[pos] = (uint16_t)(k >> lo_bits);
+    }
+    for (uint64_t j = 0; j < count; j++) {
+      ordering[hist_hi[scratch_digit[j]]++] = scratch_index[j];
+    }
+    free(scratch_index);
+    free(scratch_digit);
+  }
+  if (visible_out) *visible_out = visible;
+  return 0;
+}
+
+/* ---- codecs: src/core/encoding.ts ---- */
+
+double orc_decode_half(uint32_t h) { /* encoding.ts:191-202 */
+  double sign = (h & 0x8000u) ? -1.0 : 1.0;
+  int exponent = (int)((h >> 10) & 0x1fu);
+  double mantissa = (double)(h & 0x3ffu);
+  if (exponent == 0) return sign * mantissa * ldexp(1.0, -24);
+  if (exponent == 0x1f) return mantissa != 0.0 ? NAN : sign * INFINITY;
+  return sign * (1.0 + mantissa / 1024.0) * ldexp(1.0, exponent - 15);
+}
+
+/* encoding.ts:156-159 with Float16Array: float64 to half, ties to even */
+uint32_t orc_encode_half(double f) {
+  uint32_t sign = signbit(f) ? 0x8000u : 0u;
+  double a = fabs(f);
+  if (isnan(f)) return sign | 0x7e00u;
+  if (a >= 65520.0) return sign | 0x7c00u; /* rounds to infinity */
+  if (a < ldexp(1.0, -14)) { /* subnormal: multiples of 2^-24 */
+    double m = a * ldexp(1.0, 24);
+    double r = nearbyint(m); /* ties to even (default rounding mode) */
+    return sign | (uint32_t)r;
+  }
+  int e;
+  double frac = frexp(a, &e); /* a = frac * 2^e, frac in [0.5, 1) */
+  double m = (frac * 2.0 - 1.0) * 1024.0;
+  double r = nearbyint(m);
+  int exponent = e - 1 + 15;
+  if (r >= 1024.0) {
+    r = 0.0;
+    exponent += 1;
+  }
+  if (exponent >= 31) return sign | 0x7c00u;
+  return sign | ((uint32_t)exponent << 10) | (uint32_t)r;
+}
+
+void orc_decode_ext_rgb(uint32_t w, double rgb[3]) { /* encoding.ts:233-239 */
+  double unit = ldexp(1.0, (int)((w >> 27) & 0x1fu) - 15) / 255.0;
+  rgb[0] = (double)(w & 0xffu) * unit * ((w & 0x1000000u) ? -1.0 : 1.0);
+  rgb[1] = (double)((w >> 8) & 0xffu) * unit * ((w & 0x2000000u) ? -1.0 : 1.0);
+  rgb[2] = (double)((w >> 16) & 0xffu) * unit * ((w & 0x4000000u) ? -1.0 : 1.0);
+}
+
+static double js_round(double x) { return floor(x + 0.5); } /* Math.round */
+
+uint32_t orc_encode_ext_rgb(const double rgb[3]) { /* encoding.ts:219-231 */
+  double max_abs = fmax(fabs(rgb[0]), fmax(fabs(rgb[1]), fabs(rgb[2])));
+  int base = (max_abs > 0 ? (int)ceil(log2(max_abs)) : 0) + 15;
+  base = base < 0 ? 0 : (base > 31 ? 31 : base);
+  double scale = 255.0 * ldexp(1.0, 15 - base);
+  uint32_t m[3];
+  for (int c = 0; c < 3; c++) {
+    double v = js_round(fabs(rgb[c]) * scale);
+    m[c] = (uint32_t)(v > 255.0 ? 255.0 : v);
+  }
+  uint32_t signs = (rgb[0] < 0 ? 1u : 0u) | (rgb[1] < 0 ? 2u : 0u) | (rgb[2] < 0 ? 4u : 0u);
+  return m[0] | (m[1] << 8) | (m[2] << 16) | ((((uint32_t)base << 3) | signs) << 24);
+}
+
+void orc_decode_oct(uint32_t code, int bits, double out[3]) { /* encoding.ts:49-67 */
+  if (code == 0) {
+    out[0] = out[1] = out[2] = 0.0;
+    return;
+  }
+  double max = (double)((1u << bits) - 1u);
+  uint32_t mask = (1u << bits) - 1u;
+  double x = (double)(code & mask) / max * 2.0 - 1.0;
+  double y = (double)((code >> bits) & mask) / max * 2.0 - 1.0;
+  double z = 1.0 - fabs(x) - fabs(y);
+  double t = fmax(-z, 0.0);
+  x += x >= 0 ? -t : t;
+  y += y >= 0 ? -t : t;
+  double len = sqrt(x * x + y * y + z * z);
+  out[0] = x / len;
+  out[1] = y / len;
+  out[2] = z / len;
+}
+
+uint32_t orc_encode_oct(const double v[3], int bits) { /* encoding.ts:33-47 */
+  double l1 = fabs(v[0]) + fabs(v[1]) + fabs(v[2]);
+  if (!(l1 > 0)) return 0;
+  uint32_t max = (1u << bits) - 1u;
+  uint32_t all_ones = max | (max << bits);
+  double px = v[0] / l1, py = v[1] / l1;
+  if (v[2] < 0) {
+    double ax = fabs(px);
+    px = (1.0 - fabs(py)) * (px >= 0 ? 1.0 : -1.0);
+    py = (1.0 - ax) * (py >= 0 ? 1.0 : -1.0);
+  }
+  uint32_t code = (uint32_t)js_round((px * 0.5 + 0.5) * max) | ((uint32_t)js_round((py * 0.5 + 0.5) * max) << bits);
+  return code == 0 ? all_ones : code;
+}
+
+void orc_decode_quat_oct32(uint32_t code, double q[4]) { /* encoding.ts:101-110, axis 10+10, angle 12 */
+  double axis[3];
+  orc_decode_oct(code & 0xfffffu, 10, axis);
+  double angle = (double)((code >> 20) & 4095u) / 4095.0 * PI;
+  double s = sin(angle / 2.0);
+  q[0] = axis[0] * s;
+  q[1] = axis[1] * s;
+  q[2] = axis[2] * s;
+  q[3] = cos(angle / 2.0);
+}
+
+uint32_t orc_encode_quat_oct32(const double q[4]) { /* encoding.ts:86-99 */
+  double len = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  if (!(len > 0)) return 0;
+  double s = (q[3] < 0 ? -1.0 : 1.0) / len;
+  double axis[3] = {q[0] * s, q[1] * s, q[2] * s};
+  double angle = 2.0 * acos(fmin(1.0, q[3] * s));
+  uint32_t angle_code = (uint32_t)js_round(angle / PI * 4095.0);
+  return orc_encode_oct(axis, 10) | (angle_code << 20);
+}
+
+/* ---- spherical harmonics: src/core/sh.ts:362-407 ---- */
+
+static const int SH_COEFFS[5] = {0, 3, 8, 15, 24}; /* sh.ts:59 */
+
+void orc_sh_basis(const double d[3], double out[24]) {
+  const double x = d[0], y = d[1], z = d[2];
+  const double xx = x * x, yy = y * y, zz = z * z;
+  out[0] = -0.4886025 * y;
+  out[1] = 0.4886025 * z;
+  out[2] = -0.4886025 * x;
+  out[3] = 1.0925484 * x * y;
+  out[4] = -1.0925484 * y * z;
+  out[5] = 0.3153916 * (2 * zz - xx - yy);
+  out[6] = -1.0925484 * x * z;
+  out[7] = 0.5462742 * (xx - yy);
+  out[8] = -0.5900436 * y * (3 * xx - yy);
+  out[9] = 2.8906114 * x * y * z;
+  out[10] = -0.4570458 * y * (4 * zz - xx - yy);
+  out[11] = 0.3731763 * z * (2 * zz - 3 * xx - 3 * yy);
+  out[12] = -0.4570458 * x * (4 * zz - xx - yy);
+  out[13] = 1.4453057 * z * (xx - yy);
+  out[14] = -0.5900436 * x * (xx - 3 * yy);
+  out[15] = 2.5033429 * x * y * (xx - yy);
+  out[16] = -1.7701308 * y * z * (3 * xx - yy);
+  out[17] = 0.9461747 * x * y * (7 * zz - 1);
+  out[18] = -0.6690465 * y * z * (7 * zz - 3);
+  out[19] = 0.1057855 * (zz * (35 * zz - 30) + 3);
+  out[20] = -0.6690465 * x * z * (7 * zz - 3);
+  out[21] = 0.4730873 * (xx - yy) * (7 * zz - 1);
+  out[22] = -1.7701308 * x * z * (xx - 3 * yy);
+  out[23] = 0.6258357 * (xx * (xx - 3 * yy) - yy * (3 * xx - yy));
+}
+
+void orc_sh_evaluate(const double* c, const double dir[3], int degree, double out[3]) {
+  double basis[24];
+  orc_sh_basis(dir, basis);
+  int deg = degree < 0 ? 0 : (degree > 4 ? 4 : degree);
+  out[0] = out[1] = out[2] = 0.0;
+  for (int k = 0; k < SH_COEFFS[deg]; k++) {
+    out[0] += c[k * 3] * basis[k];
+    out[1] += c[k * 3 + 1] * basis[k];
+    out[2] += c[k * 3 + 2] * basis[k];
+  }
+}
+
+/* ---- table rows ---- */
+
+static double load_color(const rdx_table* t, uint64_t i, int j) {
+  const int coeffs = 1 + SH_COEFFS[t->sh_degree];
+  uint64_t at = i * (uint64_t)coeffs * 3 + (uint64_t)j;
+  if (t->color_dtype == RDX_DTYPE_F16) {
+    return orc_decode_half(((const uint16_t*)t->colors)[at]);
+  }
+  return (double)((const float*)t->colors)[at];
+}
+
+void orc_load_splat(const rdx_table* t, uint64_t i, orc_splat* s) {
+  s->sh_degree = t->sh_degree;
+  const int k = SH_COEFFS[t->sh_degree];
+  if (t->layout == RDX_LAYOUT_EXT) { /* splats.ts:188-197 */
+    const uint32_t* a = t->ext_a + i * 4;
+    const uint32_t* b = t->ext_b + i * 4;
+    for (int c = 0; c < 3; c++) {
+      float f;
+      memcpy(&f, &a[c], 4);
+      s->center[c] = f;
+    }
+    s->opacity = (double)(a[3] >> 24) / 128.0; /* encoding.ts:213-215 */
+    orc_decode_ext_rgb(b[0], s->rgb);
+    s->scales[0] = exp(orc_decode_half(b[1] & 0xffffu));
+    s->scales[1] = exp(orc_decode_half(b[1] >> 16));
+    s->scales[2] = exp(orc_decode_half(b[2] & 0xffffu));
+    orc_decode_quat_oct32(b[3], s->quat);
+    for (int c = 0; c < k; c++) { /* sh.ts:114-135: one ext rgb word per coefficient */
+      uint32_t w = t->ext_sh[c >> 2][i * 4 + (uint64_t)(c & 3)];
+      orc_decode_ext_rgb(w, &s->sh[c * 3]);
+    }
+  } else {
+    for (int c = 0; c < 3; c++) {
+      s->center[c] = t->centers[i * 3 + c];
+      s->scales[c] = exp((double)t->log_scales[i * 3 + c]);
+      s->rgb[c] = load_color(t, i, c);
+    }
+    for (int c = 0; c < 4; c++) s->quat[c] = t->quats[i * 4 + c];
+    s->opacity = t->opacities[i];
+    for (int c = 0; c < k * 3; c++) s->sh[c] = load_color(t, i, 3 + c);
+  }
+}
+
+/* ---- 4x4 matrices, column-major ---- */
+
+/* three.js multiplyMatrices: out = a * b, each sum left to right */
+void orc_mat4_mul(const double a[16], const double b[16], double out[16]) {
+  double r[16];
+  for (int row = 0; row < 4; row++) {
+    for (int col = 0; col < 4; col++) {
+      double s = a[0 * 4 + row] * b[col * 4 + 0];
+      s = s + a[1 * 4 + row] * b[col * 4 + 1];
+      s = s + a[2 * 4 + row] * b[col * 4 + 2];
+      s = s + a[3 * 4 + row] * b[col * 4 + 3];
+      r[col * 4 + row] = s;
+    }
+  }
+  memcpy(out, r, sizeof(r));
+}
+
+/* Inverse by the Laplace expansion in complementary 2x2 minors; 0 if singular */
+int orc_mat4_invert(const double m[16], double out[16]) {
+#define A(r, c) m[(c) * 4 + (r)]
+  double s0 = A(0, 0) * A(1, 1) - A(1, 0) * A(0, 1);
+  double s1 = A(0, 0) * A(1, 2) - A(1, 0) * A(0, 2);
+  double s2 = A(0, 0) * A(1, 3) - A(1, 0) * A(0, 3);
+  double s3 = A(0, 1) * A(1, 2) - A(1, 1) * A(0, 2);
+  double s4 = A(0, 1) * A(1, 3) - A(1, 1) * A(0, 3);
+  double s5 = A(0, 2) * A(1, 3) - A(1, 2) * A(0, 3);
+  double c5 = A(2, 2) * A(3, 3) - A(3, 2) * A(2, 3);
+  double c4 = A(2, 1) * A(3, 3) - A(3, 1) * A(2, 3);
+  double c3 = A(2, 1) * A(3, 2) - A(3, 1) * A(2, 2);
+  double c2 = A(2, 0) * A(3, 3) - A(3, 0) * A(2, 3);
+  double c1 = A(2, 0) * A(3, 2) - A(3, 0) * A(2, 2);
+  double c0 = A(2, 0) * A(3, 1) - A(3, 0) * A(2, 1);
+  double det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+  if (det == 0.0) {
+    memset(out, 0, 16 * sizeof(double));
+    return 0;
+  }
+  double inv = 1.0 / det;
+  double r[16];
+#define R(rr, cc) r[(cc) * 4 + (rr)]
+  R(0, 0) = (A(1, 1) * c5 - A(1, 2) * c4 + A(1, 3) * c3) * inv;
+  R(0, 1) = (-A(0, 1) * c5 + A(0, 2) * c4 - A(0, 3) * c3) * inv;
+  R(0, 2) = (A(3, 1) * s5 - A(3, 2) * s4 + A(3, 3) * s3) * inv;
+  R(0, 3) = (-A(2, 1) * s5 + A(2, 2) * s4 - A(2, 3) * s3) * inv;
+  R(1, 0) = (-A(1, 0) * c5 + A(1, 2) * c2 - A(1, 3) * c1) * inv;
+  R(1, 1) = (A(0, 0) * c5 - A(0, 2) * c2 + A(0, 3) * c1) * inv;
+  R(1, 2) = (-A(3, 0) * s5 + A(3, 2) * s2 - A(3, 3) * s1) * inv;
+  R(1, 3) = (A(2, 0) * s5 - A(2, 2) * s2 + A(2, 3) * s1) * inv;
+  R(2, 0) = (A(1, 0) * c4 - A(1, 1) * c2 + A(1, 3) * c0) * inv;
+  R(2, 1) = (-A(0, 0) * c4 + A(0, 1) * c2 - A(0, 3) * c0) * inv;
+  R(2, 2) = (A(3, 0) * s4 - A(3, 1) * s2 + A(3, 3) * s0) * inv;
+  R(2, 3) = (-A(2, 0) * s4 + A(2, 1) * s2 - A(2, 3) * s0) * inv;
+  R(3, 0) = (-A(1, 0) * c3 + A(1, 1) * c1 - A(1, 2) * c0) * inv;
+  R(3, 1) = (A(0, 0) * c3 - A(0, 1) * c1 + A(0, 2) * c0) * inv;
+  R(3, 2) = (-A(3, 0) * s3 + A(3, 1) * s1 - A(3, 2) * s0) * inv;
+  R(3, 3) = (A(2, 0) * s3 - A(2, 1) * s1 + A(2, 2) * s0) * inv;
+#undef R
+#undef A
+  memcpy(out, r, sizeof(r));
+  return 1;
+}
+
+/* point transform without the w divide (the GPU's matrix.mul(vec4(c, 1)).xyz) */
+static void xform_point(const double m[16], const double p[3], double out[3]) {
+  double r[3];
+  for (int row = 0; row < 3; row++) {
+    double s = m[0 * 4 + row] * p[0];
+    s = s + m[1 * 4 + row] * p[1];
+    s = s + m[2 * 4 + row] * p[2];
+    s = s + m[3 * 4 + row];
+    r[row] = s;
+  }
+  out[0] = r[0];
+  out[1] = r[1];
+  out[2] = r[2];
+}
+
+static void clip_of(const double p[16], const double c[3], double clip[4]) {
+  for (int row = 0; row < 4; row++) {
+    double s = p[0 * 4 + row] * c[0];
+    s = s + p[1 * 4 + row] * c[1];
+    s = s + p[2 * 4 + row] * c[2];
+    s = s + p[3 * 4 + row];
+    clip[row] = s;
+  }
+}
+
+/* 3x3 (row-major m[r][c]) helpers */
+static void m3_mul(const double a[9], const double b[9], double out[9]) {
+  double r[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) r[i * 3 + j] = a[i * 3 + 0] * b[0 * 3 + j] + a[i * 3 + 1] * b[1 * 3 + j] + a[i * 3 + 2] * b[2 * 3 + j];
+  memcpy(out, r, sizeof(r));
+}
+
+static void m3_transpose(const double a[9], double out[9]) {
+  double r[9];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) r[i * 3 + j] = a[j * 3 + i];
+  memcpy(out, r, sizeof(r));
+}
+
+/* mat3FromMat4 as row-major 3x3 */
+static void m3_from_m4(const double m[16], double out[9]) {
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) out[r * 3 + c] = m[c * 4 + r];
+}
+
+void orc_params_default(rdx_params* p) { /* splatParams.ts:68-72 */
+  p->max_std_dev = (float)sqrt(8.0);
+  p->min_alpha = (float)(0.5 / 255.0);
+  p->falloff = 1.0f;
+  p->lod_inflate = 1;
+  p->blur_amount = 0.3f;
+  p->pre_blur_amount = 0.0f;
+  p->clip_xy = 1.4f;
+  p->min_pixel_radius = 0.0f;
+  p->max_pixel_radius = 512.0f;
+  p->min_contribution = 0.0f;
+  p->focal_distance = 0.0f;
+  p->aperture_tan = 0.0f;
+  p->sort_guard = 0.0f;
+  p->max_sh_degree = 4;
+}
+
+/* ---- word codecs: src/render/projection.tsl.ts:277-311 ---- */
+
+static double clampd(double x, double lo, double hi) { return fmin(fmax(x, lo), hi); }
+
+static uint32_t encode_fixed16(double v) {
+  return (uint32_t)clampd(floor((v + 2.0) / 4.0 * 65535.0 + 0.5), 0.0, 65535.0);
+}
+
+uint32_t orc_encode_depth20(double view_z) {
+  float f32 = (float)(-view_z);
+  uint32_t f;
+  memcpy(&f, &f32, 4);
+  const uint32_t lo = 113u << 23, hi = (145u << 23) - 1u;
+  /* WGSL clamp on uint: f as unsigned (a negative depth has the sign bit set and clamps high) */
+  f = f < lo ? lo : (f > hi ? hi : f);
+  uint32_t code = (f - lo + 128u) >> 8;
+  return code < 0xfffffu ? code : 0xfffffu;
+}
+
+uint32_t orc_encode_angle12(double angle) {
+  return (uint32_t)floor(angle / PI * 4096.0 + 0.5) & 0xfffu;
+}
+
+static uint32_t encode_log_scale12(double scale) {
+  const double top = 4094.0;
+  double normalized = (clampd(log2(fmax(scale, 1e-20)), -4.0, 12.0) + 4.0) / 16.0 * top;
+  return (uint32_t)clampd(floor(normalized + 0.5), 0.0, top) + 1u;
+}
+
+static uint32_t encode_opacity8(double opacity) {
+  uint32_t v = (uint32_t)floor(clampd(opacity * 128.0, 0.0, 255.0) + 0.5);
+  return v > 1u ? v : 1u;
+}
+
+/* ---- the projection ---- */
+
+typedef struct eye_setup {
+  double from_head[16];
+  int identity;
+  double proj[16];
+  double from_head3[9];
+  double focal[2];
+  int ortho;
+} eye_setup;
+
+typedef struct object_setup {
+  double a[16];        /* object -> head */
+  double a3[9];
+  double origin[3];    /* the head in object space (the view origin of the SH) */
+  rdx_params params;
+  uint64_t offset;
+} object_setup;
+
+static int mat_equal(const double a[16], const double b[16]) {
+  for (int i = 0; i < 16; i++)
+    if (a[i] != b[i]) return 0;
+  return 1;
+}
+
+/* One splat: outputs at index `gi` of the collection (n splats, E eyes) */
+static void project_one(const orc_splat* s, const object_setup* o, const eye_setup* eyes, int n_eyes,
+                        const rdx_camera* cam, int sort_bits, int cull_keys, uint64_t gi, uint64_t n,
+                        const orc_outputs* out) {
+  const rdx_params* p = &o->params;
+  /* SH in object space from the view origin: splatGenerator.ts:152-158, sh.tsl.ts:255-266 */
+  /* A table with SH gets rgb + SH clamped at 0 even when the cap draws no band
+     (GpuShReader.apply); a table without SH has no reader and no clamp. A splat
+     at the view origin has no direction and gets no SH. */
+  double rgb[3] = {s->rgb[0], s->rgb[1], s->rgb[2]};
+  int degree = s->sh_degree < p->max_sh_degree ? s->sh_degree : p->max_sh_degree;
+  if (s->sh_degree >= 1) {
+    double sh[3] = {0.0, 0.0, 0.0};
+    if (degree >= 1) {
+      double dv[3] = {s->center[0] - o->origin[0], s->center[1] - o->origin[1], s->center[2] - o->origin[2]};
+      double len = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+      double dir[3] = {0, 0, 0};
+      if (len > 0) {
+        dir[0] = dv[0] / len;
+        dir[1] = dv[1] / len;
+        dir[2] = dv[2] / len;
+      }
+      orc_sh_evaluate(s->sh, dir, degree, sh);
+    }
+    for (int c = 0; c < 3; c++) rgb[c] = fmax(rgb[c] + sh[c], 0.0);
+  }
+  /* toCov: splats.tsl.ts:176-187, math.ts:12-45 */
+  double qx = s->quat[0], qy = s->quat[1], qz = s->quat[2], qw = s->quat[3];
+  double ql = sqrt(qx * qx + qy * qy + qz * qz + qw * qw);
+  if (!(ql > 0)) {
+    qx = qy = qz = 0.0;
+    qw = 1.0;
+  } else {
+    qx /= ql;
+    qy /= ql;
+    qz /= ql;
+    qw /= ql;
+  }
+  const double sx = s->scales[0], sy = s->scales[1], sz = s->scales[2];
+  /* M = R(q) diag(s) as row-major m[r][c]: column c is axis c scaled (math.tsl.ts:26-44) */
+  double M[9] = {
+      sx * (1 - 2 * (qy * qy + qz * qz)), sy * 2 * (qx * qy - qw * qz), sz * 2 * (qx * qz + qw * qy),
+      sx * 2 * (qx * qy + qw * qz), sy * (1 - 2 * (qx * qx + qz * qz)), sz * 2 * (qy * qz - qw * qx),
+      sx * 2 * (qx * qz - qw * qy), sy * 2 * (qy * qz + qw * qx), sz * (1 - 2 * (qx * qx + qy * qy)),
+  };
+  double Mt[9], cov[9];
+  m3_transpose(M, Mt);
+  m3_mul(M, Mt, cov);
+  /* transformCov: splatTransform.tsl.ts:120-140 */
+  double ch[3];
+  xform_point(o->a, s->center, ch);
+  double a3t[9], tmp[9], covh[9];
+  m3_transpose(o->a3, a3t);
+  m3_mul(o->a3, cov, tmp);
+  m3_mul(tmp, a3t, covh);
+  /* prepareSplat: projection.tsl.ts:42-64 */
+  double opacity = s->opacity;
+  double inflate = 1.0;
+  if (opacity > 1.0) {
+    opacity = fmin(opacity * 4.0 - 3.0, 5.0);
+    if (p->lod_inflate) {
+      inflate = pow(exp((opacity * opacity - 1.0) / E_CONST), 1.0 / 3.0);
+      opacity = 1.0;
+    }
+  }
+  for (int k = 0; k < 9; k++) covh[k] *= inflate * inflate;
+  const double std_dev = opacity > 1.0 ? (double)p->max_std_dev + (opacity - 1.0) * 0.7 : (double)p->max_std_dev;
+  /* cullInvisible: projection.tsl.ts:66-69 */
+  const int degenerate = covh[0] == 0.0 && covh[4] == 0.0 && covh[8] == 0.0;
+  const int invisible = opacity <= 0.0 || opacity < (double)p->min_alpha || degenerate;
+  /* the head view (SplatProjection.ts:131-137): distance and sort guard */
+  const double distance = sqrt(ch[0] * ch[0] + ch[1] * ch[1] + ch[2] * ch[2]);
+  int guarded = 1;
+  if (p->sort_guard > 0.0f) { /* inSortGuard, projection.tsl.ts:145-155 (cov form) */
+    double clip[4];
+    clip_of(eyes[0].proj, ch, clip);
+    double extent = sqrt(fmax(fmax(covh[0], covh[4]), covh[8]));
+    double radius = extent * p->max_std_dev;
+    double w = fmax(clip[3], 1e-6);
+    double rx = eyes[0].proj[0] * radius / w, ry = eyes[0].proj[5] * radius / w;
+    int inside = fabs(clip[0] / w) - rx <= (double)p->sort_guard + 1.0 && fabs(clip[1] / w) - ry <= (double)p->sort_guard + 1.0;
+    int near_ = -ch[2] <= radius;
+    guarded = ch[2] < radius && (inside || near_);
+  }
+  int any_visible = 0;
+  for (int v = 0; v < n_eyes; v++) {
+    const eye_setup* e = &eyes[v];
+    /* splatInView: projection.tsl.ts:112-129 */
+    double ce[3];
+    if (e->identity) {
+      ce[0] = ch[0];
+      ce[1] = ch[1];
+      ce[2] = ch[2];
+    } else {
+      xform_point(e->from_head, ch, ce);
+    }
+    double clip[4];
+    clip_of(e->proj, ce, clip);
+    double blur = p->blur_amount;
+    if (p->focal_distance > 0.0f && p->aperture_tan > 0.0f && ce[2] < 0.0) {
+      double depth = -ce[2];
+      double coc_view = fabs(depth - (double)p->focal_distance) * (double)p->aperture_tan;
+      double focal_pixels = cam->height * 0.5 * e->proj[5];
+      double coc = e->ortho ? coc_view * focal_pixels : coc_view * focal_pixels / depth;
+      blur = fmin(fmax(coc * coc, blur), (double)p->max_pixel_radius * p->max_pixel_radius);
+    }
+    double ndc[2] = {0.0, 0.0};
+    if (clip[3] > 0.0) {
+      ndc[0] = clip[0] / clip[3];
+      ndc[1] = clip[1] / clip[3];
+    }
+    /* culls: projection.tsl.ts:132-140 */
+    const double limit = fmin((double)p->clip_xy, 2.0) * clip[3];
+    int ok = !(invisible || ce[2] >= 0.0 || clip[2] < cam->ndc_z_min * clip[3] || clip[2] >= clip[3] ||
+               fabs(clip[0]) > limit || fabs(clip[1]) > limit);
+    double a = 0, b = 0, d = 0, det = 0, opacity_c = 0, scale1 = 0, scale2 = 0, angle = 0;
+    if (ok) {
+      /* ewa.project: projections.tsl.ts:95-148 */
+      double cov3[9];
+      if (e->identity) {
+        memcpy(cov3, covh, sizeof(cov3));
+      } else {
+        double ft[9], t2[9];
+        m3_transpose(e->from_head3, ft);
+        m3_mul(e->from_head3, covh, t2);
+        m3_mul(t2, ft, cov3);
+      }
+      /* J as 3x3 (row-major), cov2D = J^T cov J with J's columns (J1x,0,J2x), (0,J1y,J2y), 0 */
+      double J[9] = {0};
+      if (e->ortho) {
+        J[0] = e->focal[0];
+        J[4] = e->focal[1];
+      } else {
+        double inv_z = 1.0 / ce[2];
+        double j1x = e->focal[0] * inv_z, j1y = e->focal[1] * inv_z;
+        double j2x = -(j1x * ce[0]) * inv_z, j2y = -(j1y * ce[1]) * inv_z;
+        J[0 * 3 + 0] = j1x;
+        J[1 * 3 + 1] = j1y;
+        J[2 * 3 + 0] = j2x;
+        J[2 * 3 + 1] = j2y;
+      }
+      double Jt[9], t3[9], cov2[9];
+      m3_transpose(J, Jt);
+      m3_mul(Jt, cov3, t3);
+      m3_mul(t3, J, cov2);
+      a = cov2[0] + p->pre_blur_amount;
+      d = cov2[4] + p->pre_blur_amount;
+      b = cov2[1];
+      double det_orig = a * d - b * b;
+      a += blur;
+      d += blur;
+      det = a * d - b * b;
+      opacity_c = opacity * sqrt(fmax(0.0, det_orig / det));
+      double contribution = opacity_c * 2.0 * PI * sqrt(fmax(0.0, det));
+      /* boundFromCov: projection.tsl.ts:223-240 */
+      double half = (a - d) * 0.5;
+      double eigen1 = (a + d) * 0.5 + sqrt(half * half + b * b);
+      double eigen2 = eigen1 > 0.0 ? fmax(det / eigen1, 0.0) : 0.0;
+      scale1 = fmin((double)p->max_pixel_radius, std_dev * sqrt(fmax(eigen1, 0.0)));
+      scale2 = fmin((double)p->max_pixel_radius, std_dev * sqrt(eigen2));
+      int bound_ok = scale1 >= (double)p->min_pixel_radius || scale2 >= (double)p->min_pixel_radius;
+      if (bound_ok) { /* eigenvector2: projection.tsl.ts:215-219 */
+        double vx, vy;
+        if (fabs(a - eigen1) >= fabs(d - eigen1)) {
+          vx = b;
+          vy = eigen1 - a;
+        } else {
+          vx = eigen1 - d;
+          vy = b;
+        }
+        double len = sqrt(vx * vx + vy * vy);
+        if (len > 0) {
+          vx /= len;
+          vy /= len;
+        } else {
+          vx = 1.0;
+          vy = 0.0;
+        }
+        angle = atan2(vy, vx);
+        if (angle < 0.0) angle += PI;
+      }
+      ok = opacity_c >= (double)p->min_alpha && contribution >= (double)p->min_contribution && bound_ok;
+    }
+    const uint64_t ei = (uint64_t)v * n + gi;
+    if (out->visible) out->visible[ei] = (uint8_t)ok;
+    if (ok) {
+      if (out->mean2d) {
+        out->mean2d[ei * 2 + 0] = (ndc[0] + 1.0) * 0.5 * cam->width;
+        out->mean2d[ei * 2 + 1] = (ndc[1] + 1.0) * 0.5 * cam->height;
+      }
+      if (out->conic) {
+        out->conic[ei * 3 + 0] = d / det;
+        out->conic[ei * 3 + 1] = -b / det;
+        out->conic[ei * 3 + 2] = a / det;
+      }
+      if (out->depth) out->depth[ei] = -ce[2];
+      if (out->opacity) out->opacity[ei] = opacity_c;
+      if (out->rgb)
+        for (int c = 0; c < 3; c++) out->rgb[ei * 3 + c] = rgb[c];
+      if (out->radii) {
+        out->radii[ei * 3 + 0] = scale1;
+        out->radii[ei * 3 + 1] = scale2;
+        out->radii[ei * 3 + 2] = angle;
+      }
+      if (out->words) { /* projections.tsl.ts:135-140 */
+        uint32_t* w = out->words + gi * (uint64_t)(4 * n_eyes) + (uint64_t)v * 4;
+        double stored = opacity_c > 1.0 ? (opacity_c + 3.0) * 0.25 : opacity_c;
+        w[0] = encode_fixed16(ndc[0]) | (encode_fixed16(ndc[1]) << 16);
+        w[1] = orc_encode_depth20(ce[2]) | (orc_encode_angle12(angle) << 20);
+        w[2] = orc_encode_ext_rgb(rgb);
+        w[3] = encode_opacity8(stored) | (encode_log_scale12(scale1) << 8) | (encode_log_scale12(scale2) << 20);
+      }
+      any_visible = 1;
+    } else {
+      if (out->mean2d) out->mean2d[ei * 2] = out->mean2d[ei * 2 + 1] = 0.0;
+      if (out->conic) out->conic[ei * 3] = out->conic[ei * 3 + 1] = out->conic[ei * 3 + 2] = 0.0;
+      if (out->depth) out->depth[ei] = 0.0;
+      if (out->opacity) out->opacity[ei] = 0.0;
+      if (out->rgb) out->rgb[ei * 3] = out->rgb[ei * 3 + 1] = out->rgb[ei * 3 + 2] = 0.0;
+      if (out->radii) out->radii[ei * 3] = out->radii[ei * 3 + 1] = out->radii[ei * 3 + 2] = 0.0;
+      if (out->words) {
+        uint32_t* w = out->words + gi * (uint64_t)(4 * n_eyes) + (uint64_t)v * 4;
+        w[0] = w[1] = w[2] = w[3] = 0u;
+      }
+    }
+  }
+  /* SplatProjection.write: SplatProjection.ts:150-151 */
+  const int keyed = cull_keys ? any_visible : (!invisible && guarded);
+  if (out->keys) out->keys[gi] = keyed ? orc_sort_key(distance, sort_bits) : orc_invalid_key(sort_bits);
+  if (out->distance) out->distance[gi] = distance;
+}
+
+int orc_project(const rdx_object* objects, int n_objects, const rdx_camera* cam, const rdx_params* params,
+                int sort_bits, int cull_keys, int threads, const orc_outputs* out) {
+  if (cam->eyes < 1 || cam->eyes > 2) return -1;
+  eye_setup eyes[2];
+  double head_world[16];
+  orc_mat4_invert(cam->head, head_world);
+  for (int v = 0; v < cam->eyes; v++) { /* splatCamera.ts:119-138 */
+    eye_setup* e = &eyes[v];
+    e->identity = mat_equal(cam->eye[v].view, cam->head);
+    if (e->identity) {
+      memset(e->from_head, 0, sizeof(e->from_head));
+      e->from_head[0] = e->from_head[5] = e->from_head[10] = e->from_head[15] = 1.0;
+    } else {
+      orc_mat4_mul(cam->eye[v].view, head_world, e->from_head);
+    }
+    m3_from_m4(e->from_head, e->from_head3);
+    memcpy(e->proj, cam->eye[v].projection, sizeof(e->proj));
+    e->focal[0] = cam->width * 0.5 * e->proj[0];
+    e->focal[1] = cam->height * 0.5 * e->proj[5];
+    e->ortho = cam->eye[v].ortho;
+  }
+  object_setup* objs = (object_setup*)calloc((size_t)(n_objects > 0 ? n_objects : 1), sizeof(object_setup));
+  uint64_t n = 0;
+  for (int i = 0; i < n_objects; i++) { /* splatTransform.tsl.ts:78-107, splatGenerator.ts:105-112 */
+    object_setup* o = &objs[i];
+    orc_mat4_mul(cam->head, objects[i].world, o->a);
+    m3_from_m4(o->a, o->a3);
+    double inv[16];
+    orc_mat4_invert(o->a, inv);
+    o->origin[0] = inv[12];
+    o->origin[1] = inv[13];
+    o->origin[2] = inv[14];
+    o->params = objects[i].params ? *objects[i].params : *params;
+    o->offset = n;
+    n += objects[i].count;
+  }
+#ifdef _OPENMP
+  int nt = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(static, 4096) num_threads(nt)
+#endif
+  for (int64_t gi = 0; gi < (int64_t)n; gi++) {
+    int oi = 0;
+    while (oi + 1 < n_objects && (uint64_t)gi >= objs[oi + 1].offset) oi++;
+    orc_splat s;
+    orc_load_splat(objects[oi].table, (uint64_t)gi - objs[oi].offset, &s);
+    project_one(&s, &objs[oi], eyes, cam->eyes, cam, sort_bits, cull_keys, (uint64_t)gi, n, out);
+  }
+  free(objs);
+  return 0;
+}
+
+/* ---- ext fixtures: src/core/splats.ts store path (encodeExt) for a raw table ---- */
+
+/* Encoding.encodeLodOpacity, encoding.ts:209-211 */
+static uint32_t encode_lod_opacity(double opacity) {
+  double v = js_round(opacity * 128.0);
+  return (uint32_t)(v < 0 ? 0 : (v > 255 ? 255 : v));
+}
+
+int orc_encode_ext_table(const rdx_table* raw, uint32_t* ext_a, uint32_t* ext_b, uint32_t* const* ext_sh) {
+  if (raw->layout != RDX_LAYOUT_RAW) return -1;
+  const int k = SH_COEFFS[raw->sh_degree];
+  for (uint64_t i = 0; i < raw->count; i++) {
+    orc_splat s;
+    orc_load_splat(raw, i, &s);
+    uint32_t* a = ext_a + i * 4;
+    uint32_t* b = ext_b + i * 4;
+    for (int c = 0; c < 3; c++) {
+      float f = raw->centers[i * 3 + c];
+      memcpy(&a[c], &f, 4);
+    }
+    a[3] = encode_lod_opacity(s.opacity) << 24; /* no normal: Oct24 code 0 */
+    b[0] = orc_encode_ext_rgb(s.rgb);
+    b[1] = orc_encode_half(raw->log_scales[i * 3 + 0]) | (orc_encode_half(raw->log_scales[i * 3 + 1]) << 16);
+    b[2] = orc_encode_half(raw->log_scales[i * 3 + 2]); /* roughness, metallic 0 */
+    b[3] = orc_encode_quat_oct32(s.quat);
+    for (int c = 0; c < k; c++) {
+      ext_sh[c >> 2][i * 4 + (uint64_t)(c & 3)] = orc_encode_ext_rgb(&s.sh[c * 3]);
+    }
+    /* the padding word of a last texel is 0 */
+    for (int c = k; c < ((k + 3) / 4) * 4; c++) ext_sh[c >> 2][i * 4 + (uint64_t)(c & 3)] = 0u;
+  }
+  return 0;
+}

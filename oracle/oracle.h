@@ -1,0 +1,100 @@
+/*
+ * oracle.h - CPU FP64 restatement of the @sparkjsdev/radix per-frame splat
+ * path (sort keys, stable sort, ext decoding, SH, ewa projection).
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker that the CUDA path is compared
+ * against, and the timed CPU baseline. Nothing in the product links it.
+ * Each function cites the reference file:line it restates (paths inside the
+ * radix project).
+ */
+#ifndef RADIX_ORACLE_H
+#define RADIX_ORACLE_H
+
+#include <stdint.h>
+#include "../include/radix_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* src/core/sort.ts:37-58 */
+uint32_t orc_invalid_key(int bits);
+uint32_t orc_valid_max(int bits);
+uint32_t orc_sort_key(double distance, int bits);
+/* src/gpu/sortKey.tsl.ts:17-26 */
+uint32_t orc_sort_key_f32(float distance, int bits);
+void orc_sort_keys(const double* distances, uint64_t n, int bits, uint32_t* keys);
+
+/* src/core/sort.ts:64-163: returns 0, or -1 when ordering_len < count */
+int orc_sort(const uint32_t* keys, uint64_t count, int bits, uint32_t* ordering,
+             uint64_t ordering_len, uint32_t* visible);
+
+/* src/core/encoding.ts:156-239, 21-112 */
+double orc_decode_half(uint32_t h);
+uint32_t orc_encode_half(double f);
+void orc_decode_ext_rgb(uint32_t word, double rgb[3]);
+uint32_t orc_encode_ext_rgb(const double rgb[3]);
+void orc_decode_oct(uint32_t code, int bits, double out[3]);
+uint32_t orc_encode_oct(const double v[3], int bits);
+void orc_decode_quat_oct32(uint32_t code, double q[4]);
+uint32_t orc_encode_quat_oct32(const double q[4]);
+
+/* src/core/sh.ts:362-407 */
+void orc_sh_basis(const double dir[3], double out[24]);
+void orc_sh_evaluate(const double* coeffs, const double dir[3], int degree, double out[3]);
+
+/* The splat of a table row in object space (src/core/splats.ts:188-197 for ext) */
+typedef struct orc_splat {
+  double center[3];
+  double scales[3];
+  double quat[4];
+  double opacity;
+  double rgb[3];
+  double sh[24 * 3];
+  int sh_degree;
+} orc_splat;
+void orc_load_splat(const rdx_table* table, uint64_t index, orc_splat* out);
+
+/* Projection outputs in float64; any pointer may be NULL. Layouts as rdx_outputs. */
+typedef struct orc_outputs {
+  double* mean2d;
+  double* conic;
+  double* depth;
+  double* opacity;
+  double* rgb;
+  double* radii;
+  uint32_t* words;
+  uint32_t* keys;
+  double* distance;   /* [n] head-space distance */
+  uint8_t* visible;   /* [E][n] 1 when the eye draws the splat */
+} orc_outputs;
+
+/*
+ * projectCollection + SplatProjection.write + ewa.project
+ * (SplatProjector.ts:106-194, SplatProjection.ts:131-153, projections.tsl.ts:95-148)
+ * in float64. threads <= 0: all cores (OpenMP).
+ */
+int orc_project(const rdx_object* objects, int n_objects, const rdx_camera* camera,
+                const rdx_params* params, int sort_bits, int cull_keys, int threads,
+                const orc_outputs* out);
+
+/* Word codecs of the ewa projection (src/render/projection.tsl.ts:283-294) */
+uint32_t orc_encode_depth20(double view_z);
+uint32_t orc_encode_angle12(double angle);
+
+/* A raw table encoded as Radix's ext layout (src/core/splats.ts:150-181 store
+   path, src/core/sh.ts:114-135 ext SH), for fixtures of the ext reader */
+int orc_encode_ext_table(const rdx_table* raw, uint32_t* ext_a, uint32_t* ext_b, uint32_t* const* ext_sh);
+
+/* The reference's defaults (src/render/splatParams.ts:68-72) */
+void orc_params_default(rdx_params* p);
+
+/* 4x4 column-major helpers (three.js Matrix4 semantics) */
+void orc_mat4_mul(const double a[16], const double b[16], double out[16]);
+int orc_mat4_invert(const double m[16], double out[16]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

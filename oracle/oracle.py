@@ -1,0 +1,194 @@
+"""ctypes wrapper of liboracle.so, the CPU float64 oracle.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, the smoke check and the CPU
+baseline leg of bench.py, never by the radix_b200 package.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from radix_b200 import _abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+class orc_outputs(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name in
+                ("mean2d", "conic", "depth", "opacity", "rgb", "radii", "words", "keys", "distance", "visible")]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        u32, f64, vp, i = ctypes.c_uint32, ctypes.c_double, ctypes.c_void_p, ctypes.c_int
+        sigs = {
+            "orc_invalid_key": (u32, [i]),
+            "orc_valid_max": (u32, [i]),
+            "orc_sort_key": (u32, [f64, i]),
+            "orc_sort_key_f32": (u32, [ctypes.c_float, i]),
+            "orc_sort_keys": (None, [vp, ctypes.c_uint64, i, vp]),
+            "orc_sort": (i, [vp, ctypes.c_uint64, i, vp, ctypes.c_uint64, vp]),
+            "orc_decode_half": (f64, [u32]),
+            "orc_encode_half": (u32, [f64]),
+            "orc_decode_ext_rgb": (None, [u32, vp]),
+            "orc_encode_ext_rgb": (u32, [vp]),
+            "orc_decode_oct": (None, [u32, i, vp]),
+            "orc_encode_oct": (u32, [vp, i]),
+            "orc_decode_quat_oct32": (None, [u32, vp]),
+            "orc_encode_quat_oct32": (u32, [vp]),
+            "orc_sh_basis": (None, [vp, vp]),
+            "orc_sh_evaluate": (None, [vp, vp, i, vp]),
+            "orc_project": (i, [ctypes.POINTER(_abi.rdx_object), i, ctypes.POINTER(_abi.rdx_camera),
+                                ctypes.POINTER(_abi.rdx_params), i, i, i, ctypes.POINTER(orc_outputs)]),
+            "orc_encode_ext_table": (i, [ctypes.POINTER(_abi.rdx_table), vp, vp, vp]),
+            "orc_params_default": (None, [ctypes.POINTER(_abi.rdx_params)]),
+            "orc_encode_depth20": (u32, [f64]),
+            "orc_encode_angle12": (u32, [f64]),
+            "orc_mat4_mul": (None, [vp, vp, vp]),
+            "orc_mat4_invert": (i, [vp, vp]),
+        }
+        for name, (res, args) in sigs.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data
+
+
+def sort_key(distance, bits):
+    return lib().orc_sort_key(float(distance), bits)
+
+
+def sort_key_f32(distance, bits):
+    return lib().orc_sort_key_f32(float(np.float32(distance)), bits)
+
+
+def sort_keys(distances, bits):
+    d = np.ascontiguousarray(distances, dtype=np.float64)
+    out = np.empty(d.size, dtype=np.uint32)
+    lib().orc_sort_keys(_p(d), d.size, bits, _p(out))
+    return out
+
+
+def sort(keys, count=None, bits=32, ordering_len=None):
+    """SortKeys.sort: (ordering, visible); ValueError when ordering_len < count."""
+    k = np.ascontiguousarray(keys, dtype=np.uint32)
+    count = k.size if count is None else count
+    ordering_len = max(1, -(-count // 4096)) * 4096 if ordering_len is None else ordering_len
+    ordering = np.zeros(max(ordering_len, 1), dtype=np.uint32)
+    visible = ctypes.c_uint32(0)
+    if lib().orc_sort(_p(k), count, bits, _p(ordering), ordering_len, ctypes.addressof(visible)) != 0:
+        raise ValueError(f"SortKeys.sort: ordering holds {ordering_len} of {count} indices")
+    return ordering[:ordering_len], visible.value
+
+
+def decode_half(h):
+    return lib().orc_decode_half(int(h))
+
+
+def encode_half(f):
+    return lib().orc_encode_half(float(f))
+
+
+def decode_ext_rgb(w):
+    out = np.zeros(3)
+    lib().orc_decode_ext_rgb(int(w), _p(out))
+    return out
+
+
+def encode_ext_rgb(rgb):
+    a = np.ascontiguousarray(rgb, dtype=np.float64)
+    return lib().orc_encode_ext_rgb(_p(a))
+
+
+def decode_quat_oct32(code):
+    out = np.zeros(4)
+    lib().orc_decode_quat_oct32(int(code), _p(out))
+    return out
+
+
+def encode_quat_oct32(q):
+    a = np.ascontiguousarray(q, dtype=np.float64)
+    return lib().orc_encode_quat_oct32(_p(a))
+
+
+def sh_basis(d):
+    a = np.ascontiguousarray(d, dtype=np.float64)
+    out = np.zeros(24)
+    lib().orc_sh_basis(_p(a), _p(out))
+    return out
+
+
+def sh_evaluate(coeffs, d, degree):
+    c = np.zeros(72)
+    flat = np.asarray(coeffs, dtype=np.float64).reshape(-1)
+    c[:flat.size] = flat
+    a = np.ascontiguousarray(d, dtype=np.float64)
+    out = np.zeros(3)
+    lib().orc_sh_evaluate(_p(c), _p(a), int(degree), _p(out))
+    return out
+
+
+def params_default():
+    p = _abi.rdx_params()
+    lib().orc_params_default(ctypes.byref(p))
+    return p
+
+
+def project(objects, camera, params=None, sort_bits=24, cull_keys=False, threads=0):
+    """The float64 projection of radix_b200.SplatObject's (numpy tables) for a
+    radix_b200.Camera: a dict of float64 / uint32 arrays."""
+    import radix_b200 as rb
+    params = params or rb.SplatParams()
+    n = sum(o.count for o in objects)
+    E = len(camera.eyes)
+    out = {
+        "mean2d": np.zeros((E, n, 2)), "conic": np.zeros((E, n, 3)), "depth": np.zeros((E, n)),
+        "opacity": np.zeros((E, n)), "rgb": np.zeros((E, n, 3)), "radii": np.zeros((E, n, 3)),
+        "words": np.zeros((n, 4 * E), dtype=np.uint32), "keys": np.zeros(n, dtype=np.uint32),
+        "distance": np.zeros(n), "visible": np.zeros((E, n), dtype=np.uint8),
+    }
+    o = orc_outputs(**{k: _p(v) for k, v in out.items()})
+    objs, keep = rb._c_objects(objects)
+    cam = camera.to_c(_abi)
+    prm = params.to_c()
+    st = lib().orc_project(objs, len(objects), ctypes.byref(cam), ctypes.byref(prm), sort_bits,
+                           1 if cull_keys else 0, threads, ctypes.byref(o))
+    del keep
+    if st != 0:
+        raise ValueError("orc_project failed")
+    return out
+
+
+def encode_ext(raw):
+    """(ext_a, ext_b, [ext_sh channels]) of a numpy raw table dict (float32 colours)."""
+    import radix_b200 as rb
+    t = rb.Table.from_dict(raw)
+    n = t.count
+    deg = raw["sh_degree"]
+    texels = ((deg + 1) ** 2 - 1 + 3) // 4
+    a = np.zeros((n, 4), dtype=np.uint32)
+    b = np.zeros((n, 4), dtype=np.uint32)
+    sh = [np.zeros((n, 4), dtype=np.uint32) for _ in range(texels)]
+    ptrs = (ctypes.c_void_p * 6)(*([_p(c) for c in sh] + [None] * (6 - texels)))
+    if lib().orc_encode_ext_table(ctypes.byref(t.c), _p(a), _p(b), ptrs) != 0:
+        raise ValueError("orc_encode_ext_table failed")
+    return a, b, sh

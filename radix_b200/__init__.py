@@ -1,0 +1,449 @@
+"""radix_b200: the per-frame splat path of @sparkjsdev/radix on B200 (sm_100a).
+
+Host-side mirror of the reference's interfaces for this path, over the C ABI
+(include/radix_b200.h, radix_b200/lib/libradix_b200.so):
+
+  SortKeys        src/core/sort.ts            compute / sort / invalid / validMax
+  RadixSort       src/wgpu/WgpuRadixSort.ts   sort / sort_indirect (key-value, in place)
+  Compact         src/wgpu/WgpuCompact.ts     order-preserving compaction
+  SplatSorter     src/wgpu/WgpuSplatSorter.ts compact + sort + draw arguments
+  project_collection  src/render/SplatProjector.ts:106-139 (ewa, fused with SH and keys)
+  frame           project + sort, as SplatRenderer.update runs them
+
+Arrays are torch tensors (CUDA or CPU) or numpy arrays. Every computation
+runs in the CUDA library; there is no CPU fallback, and a missing build
+raises.
+"""
+import ctypes
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+from . import _abi
+from ._abi import RadixError
+from .camera import IDENTITY, Camera, look_at, perspective
+
+__all__ = [
+    "Context", "SortKeys", "RadixSort", "Compact", "SplatSorter", "SplatParams", "Table", "SplatObject",
+    "Camera", "look_at", "perspective", "project_collection", "frame", "RadixError", "align_capacity",
+]
+
+ROW_ELEMENTS = 4096  # TextureLayout.ROW_ELEMENTS (src/core/layout.ts:28-30)
+
+
+def align_capacity(count):
+    """TextureLayout.alignCapacity (src/core/layout.ts:70-72): whole 4096-element rows, at least one."""
+    return max(1, -(-int(count) // ROW_ELEMENTS)) * ROW_ELEMENTS
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if _is_torch(x):
+        if not x.is_contiguous():
+            raise ValueError("radix_b200: tensors must be contiguous")
+        return x.data_ptr()
+    if isinstance(x, np.ndarray):
+        if not x.flags.c_contiguous:
+            raise ValueError("radix_b200: arrays must be C-contiguous")
+        return x.ctypes.data
+    raise TypeError(f"radix_b200: expected a torch tensor or numpy array, got {type(x)}")
+
+
+def _on_cuda(x):
+    return _is_torch(x) and x.is_cuda
+
+
+def _empty_like_place(ref, shape, dtype_np):
+    """An output array where `ref` lives: CUDA tensor for a CUDA input, else numpy."""
+    if _on_cuda(ref):
+        torch = _torch()
+        tdt = {np.uint32: torch.int32, np.float32: torch.float32}[dtype_np]
+        return torch.empty(shape, dtype=tdt, device=ref.device)
+    return np.empty(shape, dtype=dtype_np)
+
+
+class Context:
+    """A device context (rdx_ctx): stream, scratch and error state. Calls run
+    on torch's current stream of the context's device."""
+
+    def __init__(self, device=0):
+        self.device = device
+        h = ctypes.c_void_p()
+        st = _abi.lib().rdx_ctx_create(device, ctypes.byref(h))
+        if st != _abi.RDX_OK:
+            raise RadixError(st, f"radix_b200: no CUDA device {device} (rdx_ctx_create status {st})")
+        self.handle = h
+
+    def _bind_stream(self):
+        try:
+            torch = _torch()
+            if torch.cuda.is_available():
+                _abi.lib().rdx_ctx_set_stream(self.handle, ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
+        except ImportError:
+            pass
+
+    def call(self, name, *args):
+        self._bind_stream()
+        _abi.check(getattr(_abi.lib(), name)(self.handle, *args), self.handle)
+
+    def synchronize(self):
+        _abi.check(_abi.lib().rdx_ctx_synchronize(self.handle), self.handle)
+
+    def set_profiling(self, on=True):
+        """Record CUDA events around each phase (project, sort, copies) of later calls."""
+        _abi.check(_abi.lib().rdx_ctx_set_profiling(self.handle, 1 if on else 0), self.handle)
+
+    def phase_times(self):
+        """{phase: (summed ms, runs)} since the last read (waits for the stream)."""
+        ms = (ctypes.c_double * _abi.RDX_PHASES)()
+        runs = (ctypes.c_uint64 * _abi.RDX_PHASES)()
+        _abi.check(_abi.lib().rdx_ctx_phase_times(self.handle, ms, runs), self.handle)
+        names = ("project", "sort", "copy_in", "copy_out")
+        return {names[i]: (ms[i], runs[i]) for i in range(_abi.RDX_PHASES)}
+
+    def launches(self):
+        """Kernels this context has launched."""
+        n = ctypes.c_uint64(0)
+        _abi.check(_abi.lib().rdx_ctx_launches(self.handle, ctypes.byref(n)), self.handle)
+        return n.value
+
+    def reserve(self, max_keys):
+        _abi.check(_abi.lib().rdx_ctx_reserve(self.handle, int(max_keys)), self.handle)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _abi.lib().rdx_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_contexts = {}
+
+
+def default_context(device=0):
+    if device not in _contexts:
+        _contexts[device] = Context(device)
+    return _contexts[device]
+
+
+def _ctx(ctx, *arrays):
+    if ctx is not None:
+        return ctx
+    for a in arrays:
+        if _on_cuda(a):
+            return default_context(a.device.index or 0)
+    return default_context(0)
+
+
+class SortKeys:
+    """src/core/sort.ts:27-83. invalid / valid_max are integer constants of a
+    width; compute and sort run on the GPU."""
+
+    KEY16_LO = 95 << 23
+    KEY16_HI = (159 << 23) - 1
+
+    @staticmethod
+    def invalid(bits):
+        return 2 ** bits - 1
+
+    @staticmethod
+    def valid_max(bits):
+        return 0xFF * 2 ** (bits - 8) - 1
+
+    @staticmethod
+    def compute(distances, bits, ctx=None):
+        """Keys of float64 distances (SortKeys.compute), or of float32 ones
+        (GpuSortKeys.compute: max(d, 0)); uint32 where the distances live."""
+        dt = str(distances.dtype)
+        n = int(np.prod(distances.shape))
+        keys = _empty_like_place(distances, (n,), np.uint32)
+        c = _ctx(ctx, distances)
+        if "float64" in dt:
+            c.call("rdx_sort_keys_compute", _ptr(distances), n, bits, _ptr(keys))
+        elif "float32" in dt:
+            c.call("rdx_sort_keys_compute_f32", _ptr(distances), n, bits, _ptr(keys))
+        else:
+            raise TypeError("SortKeys.compute: float64 or float32 distances")
+        return keys
+
+    @staticmethod
+    def sort(keys, count=None, bits=32, ordering=None, ctx=None):
+        """Stable ascending order of the first `count` keys into `ordering`
+        (default: a new array of align_capacity(count)); returns (ordering, visible)."""
+        count = int(np.prod(keys.shape)) if count is None else int(count)
+        if ordering is None:
+            ordering = _empty_like_place(keys, (align_capacity(count),), np.uint32)
+            if isinstance(ordering, np.ndarray):
+                ordering[:] = 0
+            else:
+                ordering.zero_()
+        visible = ctypes.c_uint32(0)
+        _ctx(ctx, keys).call("rdx_sort", _ptr(keys), count, bits, _ptr(ordering), int(np.prod(ordering.shape)),
+                             ctypes.byref(visible))
+        return ordering, visible.value
+
+
+class RadixSort:
+    """WgpuRadixSort (src/wgpu/WgpuRadixSort.ts:56-141): sorts the caller's
+    keys and values in place, ascending and stable."""
+
+    def __init__(self, keys, values, ctx=None):
+        self.keys = keys
+        self.values = values
+        self.ctx = _ctx(ctx, keys)
+
+    def sort(self, count, bits=32):
+        if bits not in (16, 24, 32):
+            raise ValueError(f"WgpuRadixSort: bits must be 16, 24 or 32 (got {bits})")
+        if count <= 0:
+            return
+        self.ctx.call("rdx_sort_pairs", _ptr(self.keys), _ptr(self.values), int(count), bits)
+
+    def sort_indirect(self, count_buffer, bits=32):
+        """Sort the first min(count_buffer[0], capacity) pairs, the count read on the GPU."""
+        cap = int(np.prod(self.keys.shape))
+        self.ctx.call("rdx_sort_pairs_indirect", _ptr(self.keys), _ptr(self.values), _ptr(count_buffer), cap, bits)
+
+
+class Compact:
+    """WgpuCompact (src/wgpu/WgpuCompact.ts:22-132): the keys that are not
+    `invalid`, with their indices, in input order, and their count."""
+
+    def __init__(self, ctx=None, invalid=0xFFFFFFFF):
+        self.ctx = ctx
+        self.invalid = invalid
+
+    def compact(self, keys, n=None):
+        n = int(np.prod(keys.shape)) if n is None else int(n)
+        c = _ctx(self.ctx, keys)
+        out_k = _empty_like_place(keys, (max(n, 1),), np.uint32)
+        out_v = _empty_like_place(keys, (max(n, 1),), np.uint32)
+        count = _empty_like_place(keys, (1,), np.uint32)
+        c.call("rdx_compact", _ptr(keys), n, ctypes.c_uint32(self.invalid), _ptr(out_k), _ptr(out_v), _ptr(count))
+        return out_k, out_v, count
+
+
+class SplatSorter:
+    """WgpuSplatSorter (src/wgpu/WgpuSplatSorter.ts:19-84): compaction of the
+    invalid keys, a back-to-front sort, and drawIndexedIndirect arguments."""
+
+    QUADS_PER_INSTANCE = 1024
+
+    def __init__(self, ctx=None):
+        self.ctx = ctx
+        self.values = None
+        self.count = None
+        self.indirect = None
+
+    def sort(self, keys, count, bits):
+        c = _ctx(self.ctx, keys)
+        self.values = _empty_like_place(keys, (max(int(count), 1),), np.uint32)
+        self.count = _empty_like_place(keys, (1,), np.uint32)
+        self.indirect = _empty_like_place(keys, (5,), np.uint32)
+        c.call("rdx_splat_sort", _ptr(keys), int(count), bits, _ptr(self.values), _ptr(self.count), _ptr(self.indirect))
+        return self.values, self.count, self.indirect
+
+    def read_count(self):
+        return int(np.asarray(self.count.cpu() if _is_torch(self.count) else self.count)[0])
+
+
+@dataclass
+class SplatParams:
+    """SplatViewParams + SplatObjectParams with the reference's defaults
+    (src/render/splatParams.ts:68-72)."""
+
+    max_std_dev: float = float(np.sqrt(8.0))
+    min_alpha: float = 0.5 / 255
+    falloff: float = 1.0
+    lod_inflate: bool = True
+    blur_amount: float = 0.3
+    pre_blur_amount: float = 0.0
+    clip_xy: float = 1.4
+    min_pixel_radius: float = 0.0
+    max_pixel_radius: float = 512.0
+    min_contribution: float = 0.0
+    focal_distance: float = 0.0
+    aperture_tan: float = 0.0
+    sort_guard: float = 0.0
+    max_sh_degree: int = 4
+
+    def to_c(self):
+        p = _abi.rdx_params()
+        for f in fields(self):
+            v = getattr(self, f.name)
+            setattr(p, f.name, int(v) if f.name in ("lod_inflate", "max_sh_degree") else float(v))
+        return p
+
+
+class Table:
+    """A splat table (rdx_table): raw float32 columns or Radix's ext layout."""
+
+    def __init__(self, c_table, keep):
+        self.c = c_table
+        self._keep = keep
+
+    @property
+    def count(self):
+        return int(self.c.count)
+
+    @classmethod
+    def raw(cls, centers, log_scales, quats, opacities, colors, sh_degree=None):
+        n = int(centers.shape[0])
+        k = int(colors.shape[1]) - 1 if len(colors.shape) == 3 else int(colors.shape[1]) // 3 - 1
+        deg = {0: 0, 3: 1, 8: 2, 15: 3, 24: 4}[k] if sh_degree is None else sh_degree
+        t = _abi.rdx_table()
+        t.layout = _abi.RDX_LAYOUT_RAW
+        t.sh_degree = deg
+        t.color_dtype = _abi.RDX_DTYPE_F16 if "float16" in str(colors.dtype) else _abi.RDX_DTYPE_F32
+        t.count = n
+        t.centers, t.log_scales, t.quats = _ptr(centers), _ptr(log_scales), _ptr(quats)
+        t.opacities, t.colors = _ptr(opacities), _ptr(colors)
+        return cls(t, [centers, log_scales, quats, opacities, colors])
+
+    @classmethod
+    def ext(cls, ext_a, ext_b, ext_sh=(), sh_degree=0):
+        """extA / extB uint32x4 columns (src/core/splats.ts:10-24) and the extSh
+        texel channels (src/core/sh.ts:114-135), each [count][4] uint32."""
+        t = _abi.rdx_table()
+        t.layout = _abi.RDX_LAYOUT_EXT
+        t.sh_degree = sh_degree
+        t.count = int(ext_a.shape[0])
+        t.ext_a, t.ext_b = _ptr(ext_a), _ptr(ext_b)
+        for i, ch in enumerate(ext_sh):
+            t.ext_sh[i] = _ptr(ch)
+        return cls(t, [ext_a, ext_b, *ext_sh])
+
+    @classmethod
+    def from_dict(cls, d, to=None):
+        """A raw table of a synthetic dict, its columns moved with `to(array)`."""
+        f = to or (lambda a: a)
+        return cls.raw(f(d["centers"]), f(d["log_scales"]), f(d["quats"]), f(d["opacities"]), f(d["colors"]),
+                       d["sh_degree"])
+
+
+class SplatObject:
+    """One object of a collection: `count` splats of `table` drawn with
+    `world` (column-major object -> world), optional per-object params."""
+
+    def __init__(self, table, count=None, world=None, params=None):
+        self.table = table
+        self.count = table.count if count is None else int(count)
+        self.world = IDENTITY if world is None else np.asarray(world, dtype=np.float64).reshape(16)
+        self.params = params
+
+
+def _c_objects(objects):
+    arr = (_abi.rdx_object * max(1, len(objects)))()
+    keep = []
+    for i, o in enumerate(objects):
+        arr[i].table = ctypes.pointer(o.table.c)
+        arr[i].count = o.count
+        arr[i].world[:] = list(o.world)
+        if o.params is not None:
+            p = o.params.to_c()
+            keep.append(p)
+            arr[i].params = ctypes.pointer(p)
+        keep.append(o.table)
+    return arr, keep
+
+
+OUTPUT_SHAPES = {  # per eye: trailing shape, dtype
+    "mean2d": ((2,), np.float32),
+    "conic": ((3,), np.float32),
+    "depth": ((), np.float32),
+    "opacity": ((), np.float32),
+    "rgb": ((3,), np.float32),
+    "radii": ((3,), np.float32),
+}
+
+
+def _alloc_outputs(names, n, eyes, device):
+    torch = _torch()
+    out = {}
+    for name in names:
+        if name == "words":
+            shape, dt = (n, 4 * eyes), torch.int32
+        elif name == "keys":
+            shape, dt = (n,), torch.int32
+        else:
+            tail, _ = OUTPUT_SHAPES[name]
+            shape, dt = (eyes, n, *tail), torch.float32
+        if device is None:
+            out[name] = np.empty(shape, dtype=np.uint32 if dt is torch.int32 else np.float32)
+        else:
+            out[name] = torch.empty(shape, dtype=dt, device=device)
+    return out
+
+
+def _c_outputs(out):
+    o = _abi.rdx_outputs()
+    for name, arr in out.items():
+        setattr(o, name, _ptr(arr))
+    return o
+
+
+DEFAULT_OUTPUTS = ("mean2d", "conic", "depth", "opacity", "rgb", "keys")
+
+
+def project_collection(objects, camera, params=None, sort_bits=24, pass_="full", cull_keys=False,
+                       outputs=DEFAULT_OUTPUTS, device="cuda", ctx=None):
+    """projectCollection with the ewa method: outputs (per eye [E][n][...],
+    words [n][4E], keys [n]) as CUDA tensors (device=None: numpy)."""
+    params = params or SplatParams()
+    n = sum(o.count for o in objects)
+    eyes = len(camera.eyes)
+    names = ("keys",) if pass_ == "keys" else tuple(outputs)
+    out = _alloc_outputs(names, n, eyes, device)
+    objs, keep = _c_objects(objects)
+    cam = camera.to_c(_abi)
+    prm = params.to_c()
+    c = ctx or default_context(0)
+    c.call("rdx_project", objs, len(objects), ctypes.byref(cam), ctypes.byref(prm), sort_bits,
+           _abi.RDX_PASS_KEYS if pass_ == "keys" else _abi.RDX_PASS_FULL, 1 if cull_keys else 0,
+           ctypes.byref(_c_outputs(out)))
+    del keep
+    return out
+
+
+def frame(objects, camera, params=None, sort_bits=24, outputs=DEFAULT_OUTPUTS, device="cuda", ctx=None,
+          out=None, ordering=None, visible=None):
+    """One frame: the projection (keys of splats culled in every eye invalid)
+    and the stable back-to-front order. Returns the outputs plus 'ordering'
+    ([n]: drawn splats first, culled ones after in index order) and 'visible'
+    (an int; or, when `visible` is a 1-element device tensor, that tensor, and
+    the call returns without waiting for the GPU)."""
+    params = params or SplatParams()
+    n = sum(o.count for o in objects)
+    eyes = len(camera.eyes)
+    if out is None:
+        out = _alloc_outputs(tuple(outputs), n, eyes, device)
+    if ordering is None:
+        ordering = _alloc_outputs(("keys",), n, 1, device)["keys"]
+    vis_host = ctypes.c_uint32(0) if visible is None else None
+    objs, keep = _c_objects(objects)
+    cam = camera.to_c(_abi)
+    prm = params.to_c()
+    c = ctx or default_context(0)
+    c.call("rdx_frame", objs, len(objects), ctypes.byref(cam), ctypes.byref(prm), sort_bits,
+           ctypes.byref(_c_outputs(out)), _ptr(ordering),
+           ctypes.byref(vis_host) if vis_host is not None else ctypes.c_void_p(_ptr(visible)))
+    del keep
+    res = dict(out)
+    res["ordering"] = ordering
+    res["visible"] = vis_host.value if vis_host is not None else visible
+    return res

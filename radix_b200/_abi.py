@@ -1,0 +1,181 @@
+"""ctypes binding of include/radix_b200.h.
+
+The structures mirror the C header field for field. The library is the
+in-tree build radix_b200/lib/libradix_b200.so; loading fails loudly when it is
+missing (there is no CPU fallback for any entry point).
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libradix_b200.so")
+
+RDX_OK = 0
+RDX_ERR_ARG = 1
+RDX_ERR_CAPACITY = 2
+RDX_ERR_CUDA = 3
+RDX_ERR_TIMEOUT = 4
+RDX_ERR_UNSUPPORTED = 5
+RDX_ERR_NOMEM = 6
+
+RDX_LAYOUT_RAW = 0
+RDX_LAYOUT_EXT = 1
+RDX_DTYPE_F32 = 0
+RDX_DTYPE_F16 = 1
+RDX_PASS_FULL = 0
+RDX_PASS_KEYS = 1
+RDX_PHASE_PROJECT = 0
+RDX_PHASE_SORT = 1
+RDX_PHASE_COPY_IN = 2
+RDX_PHASE_COPY_OUT = 3
+RDX_PHASES = 4
+
+c_u32p = ctypes.POINTER(ctypes.c_uint32)
+c_f32p = ctypes.POINTER(ctypes.c_float)
+c_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+class rdx_table(ctypes.Structure):
+    _fields_ = [
+        ("layout", ctypes.c_int32),
+        ("sh_degree", ctypes.c_int32),
+        ("color_dtype", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("count", ctypes.c_uint64),
+        ("centers", ctypes.c_void_p),
+        ("log_scales", ctypes.c_void_p),
+        ("quats", ctypes.c_void_p),
+        ("opacities", ctypes.c_void_p),
+        ("colors", ctypes.c_void_p),
+        ("ext_a", ctypes.c_void_p),
+        ("ext_b", ctypes.c_void_p),
+        ("ext_sh", ctypes.c_void_p * 6),
+    ]
+
+
+class rdx_params(ctypes.Structure):
+    _fields_ = [
+        ("max_std_dev", ctypes.c_float),
+        ("min_alpha", ctypes.c_float),
+        ("falloff", ctypes.c_float),
+        ("lod_inflate", ctypes.c_int32),
+        ("blur_amount", ctypes.c_float),
+        ("pre_blur_amount", ctypes.c_float),
+        ("clip_xy", ctypes.c_float),
+        ("min_pixel_radius", ctypes.c_float),
+        ("max_pixel_radius", ctypes.c_float),
+        ("min_contribution", ctypes.c_float),
+        ("focal_distance", ctypes.c_float),
+        ("aperture_tan", ctypes.c_float),
+        ("sort_guard", ctypes.c_float),
+        ("max_sh_degree", ctypes.c_int32),
+    ]
+
+
+class rdx_eye(ctypes.Structure):
+    _fields_ = [
+        ("view", ctypes.c_double * 16),
+        ("projection", ctypes.c_double * 16),
+        ("ortho", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+class rdx_camera(ctypes.Structure):
+    _fields_ = [
+        ("head", ctypes.c_double * 16),
+        ("eyes", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("eye", rdx_eye * 2),
+        ("width", ctypes.c_double),
+        ("height", ctypes.c_double),
+        ("ndc_z_min", ctypes.c_double),
+    ]
+
+
+class rdx_object(ctypes.Structure):
+    _fields_ = [
+        ("table", ctypes.POINTER(rdx_table)),
+        ("count", ctypes.c_uint64),
+        ("world", ctypes.c_double * 16),
+        ("params", ctypes.POINTER(rdx_params)),
+    ]
+
+
+class rdx_outputs(ctypes.Structure):
+    _fields_ = [
+        ("mean2d", ctypes.c_void_p),
+        ("conic", ctypes.c_void_p),
+        ("depth", ctypes.c_void_p),
+        ("opacity", ctypes.c_void_p),
+        ("rgb", ctypes.c_void_p),
+        ("radii", ctypes.c_void_p),
+        ("words", ctypes.c_void_p),
+        ("keys", ctypes.c_void_p),
+    ]
+
+
+# name -> (restype, argtypes); every symbol the header declares
+SIGNATURES = {
+    "rdx_version": (ctypes.c_int, []),
+    "rdx_params_default": (None, [ctypes.POINTER(rdx_params)]),
+    "rdx_ctx_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    "rdx_ctx_destroy": (ctypes.c_int, [ctypes.c_void_p]),
+    "rdx_ctx_set_stream": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "rdx_ctx_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "rdx_ctx_reserve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    "rdx_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "rdx_ctx_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "rdx_ctx_phase_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "rdx_ctx_launches": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "rdx_sort_keys_compute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),
+    "rdx_sort_keys_compute_f32": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),
+    "rdx_sort": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
+                                ctypes.c_uint64, ctypes.c_void_p]),
+    "rdx_sort_pairs": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int]),
+    "rdx_sort_pairs_indirect": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                               ctypes.c_uint64, ctypes.c_int]),
+    "rdx_compact": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_void_p,
+                                   ctypes.c_void_p, ctypes.c_void_p]),
+    "rdx_splat_sort": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p]),
+    "rdx_project": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_object), ctypes.c_int, ctypes.POINTER(rdx_camera),
+                                   ctypes.POINTER(rdx_params), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.POINTER(rdx_outputs)]),
+    "rdx_frame": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_object), ctypes.c_int, ctypes.POINTER(rdx_camera),
+                                 ctypes.POINTER(rdx_params), ctypes.c_int, ctypes.POINTER(rdx_outputs), ctypes.c_void_p,
+                                 ctypes.c_void_p]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded C library (raises when the build is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"radix_b200: the CUDA library {LIB_PATH} is not built; run __graft_entry__.build() "
+                "(there is no CPU fallback)")
+        handle = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+class RadixError(RuntimeError):
+    """A failed C-ABI call: .code is the RDX_* status."""
+
+    def __init__(self, code, message):
+        super().__init__(message)
+        self.code = code
+
+
+def check(status, ctx_handle=None):
+    if status != RDX_OK:
+        msg = lib().rdx_last_error(ctx_handle).decode() if ctx_handle else ""
+        raise RadixError(status, msg or f"radix_b200 status {status}")

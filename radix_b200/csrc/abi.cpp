@@ -1,0 +1,1105 @@
+// The C ABI (include/radix_b200.h): contexts, argument checks with the
+// reference's error texts, staging of host buffers, the per-object and
+// per-eye set-up of a camera in float64 (SplatCamera.setViews and
+// setTransforms), and dispatch of the kernels on the context's stream.
+//
+// Host float64 maths here must round exactly as the oracle's: keep every sum
+// in the same order and build with -ffp-contract=off.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/radix_b200.h"
+#include "rdx_internal.h"
+
+struct rdx_ctx {
+  int device = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  uint32_t* error_flag = nullptr;       // device word set by a bounded wait that gave up
+  uint32_t* error_host = nullptr;       // pinned copy of it
+  char* arena = nullptr;                // per-call device scratch
+  size_t arena_bytes = 0;
+  uint64_t launches = 0;                // kernels launched
+  bool profiling = false;
+  std::vector<cudaEvent_t> event_pool;  // free events
+  struct Pending {
+    int phase;
+    cudaEvent_t start, stop;
+  };
+  std::vector<Pending> pending;         // recorded, not yet read
+  double phase_ms[RDX_PHASES] = {0};
+  uint64_t phase_runs[RDX_PHASES] = {0};
+  // Pinned ring for small uploads (descriptors, segments): a copy from it is
+  // asynchronous; before the ring wraps, the last copy issued from it is awaited
+  char* ring = nullptr;
+  size_t ring_off = 0;
+  cudaEvent_t ring_event = nullptr;
+  bool ring_used = false;
+};
+
+static const size_t kRingBytes = 4u << 20;
+
+namespace {
+
+int fail(rdx_ctx* ctx, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (ctx) ctx->last_error = buf;
+  return code;
+}
+
+int cuda_fail(rdx_ctx* ctx, cudaError_t err, const char* what) {
+  return fail(ctx, RDX_ERR_CUDA, "%s: %s", what, cudaGetErrorString(err));
+}
+
+#define RDX_CUDA(call, what)                       \
+  do {                                             \
+    cudaError_t e_ = (call);                       \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+  } while (0)
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+bool aligned(const void* p, size_t a) { return ((uintptr_t)p % a) == 0; }
+
+// Bump allocation over the context's arena: a dry run sizes it, the real run carves it
+struct Arena {
+  char* base;
+  size_t used = 0;
+  explicit Arena(char* b) : base(b) {}
+  template <class T>
+  T* take(size_t count) {
+    used = (used + 255) & ~(size_t)255;
+    T* p = base ? reinterpret_cast<T*>(base + used) : nullptr;
+    used += count * sizeof(T);
+    return p;
+  }
+};
+
+int ensure_arena(rdx_ctx* ctx, size_t bytes) {
+  if (bytes <= ctx->arena_bytes) return RDX_OK;
+  RDX_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+  if (ctx->arena) cudaFree(ctx->arena);
+  ctx->arena = nullptr;
+  ctx->arena_bytes = 0;
+  size_t want = bytes + bytes / 4 + (1 << 20);
+  if (cudaMalloc(&ctx->arena, want) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, RDX_ERR_NOMEM, "could not allocate %zu bytes of device scratch", want);
+  }
+  ctx->arena_bytes = want;
+  return RDX_OK;
+}
+
+// Wait for the stream and report a device-side timeout
+int finish(rdx_ctx* ctx) {
+  RDX_CUDA(cudaMemcpyAsync(ctx->error_host, ctx->error_flag, 4, cudaMemcpyDeviceToHost, ctx->stream), "error flag");
+  RDX_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+  if (*ctx->error_host) {
+    *ctx->error_host = 0;
+    cudaMemsetAsync(ctx->error_flag, 0, 4, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    return fail(ctx, RDX_ERR_TIMEOUT, "a device wait gave up (lookback of a tile never published)");
+  }
+  return RDX_OK;
+}
+
+// A phase between begin and end is timed with events on the stream when profiling
+struct Phase {
+  rdx_ctx* ctx;
+  int phase;
+  cudaEvent_t start = nullptr;
+  Phase(rdx_ctx* c, int p) : ctx(c), phase(p) {
+    if (!ctx->profiling) return;
+    start = take_event(ctx);
+    if (start) cudaEventRecord(start, ctx->stream);
+  }
+  void end() {
+    if (!start) return;
+    cudaEvent_t stop = take_event(ctx);
+    if (!stop) return;
+    cudaEventRecord(stop, ctx->stream);
+    ctx->pending.push_back({phase, start, stop});
+    start = nullptr;
+  }
+  ~Phase() { end(); }
+  static cudaEvent_t take_event(rdx_ctx* ctx) {
+    if (!ctx->event_pool.empty()) {
+      cudaEvent_t e = ctx->event_pool.back();
+      ctx->event_pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return e;
+  }
+};
+
+// Copy `bytes` of host memory to the device asynchronously through the ring
+int upload(rdx_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return RDX_OK;
+  const size_t need = (bytes + 255) & ~(size_t)255;
+  if (need > kRingBytes) {  // too big for the ring: a pageable copy (synchronous staging)
+    RDX_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload");
+    return RDX_OK;
+  }
+  if (ctx->ring_off + need > kRingBytes) {
+    if (ctx->ring_used) RDX_CUDA(cudaEventSynchronize(ctx->ring_event), "ring wait");
+    ctx->ring_off = 0;
+  }
+  char* slot = ctx->ring + ctx->ring_off;
+  memcpy(slot, src, bytes);
+  RDX_CUDA(cudaMemcpyAsync(dst, slot, bytes, cudaMemcpyHostToDevice, ctx->stream), "upload");
+  RDX_CUDA(cudaEventRecord(ctx->ring_event, ctx->stream), "ring event");
+  ctx->ring_used = true;
+  ctx->ring_off += need;
+  return RDX_OK;
+}
+
+bool valid_bits(int bits) { return bits == 16 || bits == 24 || bits == 32; }
+
+uint32_t tiles_of(uint64_t n) { return (uint32_t)((n + rdx::kSortTile - 1) / rdx::kSortTile); }
+
+// Sort scratch for `segments` segments of `total` keys, max_tiles tiles, `passes` passes
+rdx::SortScratch take_sort_scratch(Arena& a, int segments, int passes, uint32_t max_tiles, uint64_t total) {
+  rdx::SortScratch s;
+  // hist, ref_hidden and counters contiguous (one memset)
+  uint32_t* small = a.take<uint32_t>(rdx::sort_small_state_words(segments, passes));
+  s.hist = small;
+  s.ref_hidden = small ? small + (size_t)segments * passes * rdx::kRadix : nullptr;
+  s.counters = small ? s.ref_hidden + segments : nullptr;
+  s.lookback = a.take<uint32_t>((size_t)passes * max_tiles * rdx::kRadix);
+  s.keys_a = a.take<uint32_t>(total);
+  s.vals_a = a.take<uint32_t>(total);
+  s.keys_b = a.take<uint32_t>(passes > 2 ? total : 0);
+  s.vals_b = a.take<uint32_t>(passes > 2 ? total : 0);
+  return s;
+}
+
+// ---- float64 matrices, column-major (the same sums, in the same order, as the oracle) ----
+
+void mat4_mul(const double a[16], const double b[16], double out[16]) {
+  double r[16];
+  for (int row = 0; row < 4; row++) {
+    for (int col = 0; col < 4; col++) {
+      double s = a[0 * 4 + row] * b[col * 4 + 0];
+      s = s + a[1 * 4 + row] * b[col * 4 + 1];
+      s = s + a[2 * 4 + row] * b[col * 4 + 2];
+      s = s + a[3 * 4 + row] * b[col * 4 + 3];
+      r[col * 4 + row] = s;
+    }
+  }
+  memcpy(out, r, sizeof(r));
+}
+
+int mat4_invert(const double m[16], double out[16]) {
+#define A(r, c) m[(c) * 4 + (r)]
+  double s0 = A(0, 0) * A(1, 1) - A(1, 0) * A(0, 1);
+  double s1 = A(0, 0) * A(1, 2) - A(1, 0) * A(0, 2);
+  double s2 = A(0, 0) * A(1, 3) - A(1, 0) * A(0, 3);
+  double s3 = A(0, 1) * A(1, 2) - A(1, 1) * A(0, 2);
+  double s4 = A(0, 1) * A(1, 3) - A(1, 1) * A(0, 3);
+  double s5 = A(0, 2) * A(1, 3) - A(1, 2) * A(0, 3);
+  double c5 = A(2, 2) * A(3, 3) - A(3, 2) * A(2, 3);
+  double c4 = A(2, 1) * A(3, 3) - A(3, 1) * A(2, 3);
+  double c3 = A(2, 1) * A(3, 2) - A(3, 1) * A(2, 2);
+  double c2 = A(2, 0) * A(3, 3) - A(3, 0) * A(2, 3);
+  double c1 = A(2, 0) * A(3, 2) - A(3, 0) * A(2, 2);
+  double c0 = A(2, 0) * A(3, 1) - A(3, 0) * A(2, 1);
+  double det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+  if (det == 0.0) {
+    memset(out, 0, 16 * sizeof(double));
+    return 0;
+  }
+  double inv = 1.0 / det;
+  double r[16];
+#define R(rr, cc) r[(cc) * 4 + (rr)]
+  R(0, 0) = (A(1, 1) * c5 - A(1, 2) * c4 + A(1, 3) * c3) * inv;
+  R(0, 1) = (-A(0, 1) * c5 + A(0, 2) * c4 - A(0, 3) * c3) * inv;
+  R(0, 2) = (A(3, 1) * s5 - A(3, 2) * s4 + A(3, 3) * s3) * inv;
+  R(0, 3) = (-A(2, 1) * s5 + A(2, 2) * s4 - A(2, 3) * s3) * inv;
+  R(1, 0) = (-A(1, 0) * c5 + A(1, 2) * c2 - A(1, 3) * c1) * inv;
+  R(1, 1) = (A(0, 0) * c5 - A(0, 2) * c2 + A(0, 3) * c1) * inv;
+  R(1, 2) = (-A(3, 0) * s5 + A(3, 2) * s2 - A(3, 3) * s1) * inv;
+  R(1, 3) = (A(2, 0) * s5 - A(2, 2) * s2 + A(2, 3) * s1) * inv;
+  R(2, 0) = (A(1, 0) * c4 - A(1, 1) * c2 + A(1, 3) * c0) * inv;
+  R(2, 1) = (-A(0, 0) * c4 + A(0, 1) * c2 - A(0, 3) * c0) * inv;
+  R(2, 2) = (A(3, 0) * s4 - A(3, 1) * s2 + A(3, 3) * s0) * inv;
+  R(2, 3) = (-A(2, 0) * s4 + A(2, 1) * s2 - A(2, 3) * s0) * inv;
+  R(3, 0) = (-A(1, 0) * c3 + A(1, 1) * c1 - A(1, 2) * c0) * inv;
+  R(3, 1) = (A(0, 0) * c3 - A(0, 1) * c1 + A(0, 2) * c0) * inv;
+  R(3, 2) = (-A(3, 0) * s3 + A(3, 1) * s1 - A(3, 2) * s0) * inv;
+  R(3, 3) = (A(2, 0) * s3 - A(2, 1) * s1 + A(2, 2) * s0) * inv;
+#undef R
+#undef A
+  memcpy(out, r, sizeof(r));
+  return 1;
+}
+
+const int kShCoeffs[5] = {0, 3, 8, 15, 24};
+
+// Kernels of one sort_segments call: the histogram and one onesweep per pass
+uint64_t sort_launches(int bits, uint32_t max_tiles) { return max_tiles ? 1 + (uint64_t)(bits / 8) : 0; }
+
+// ---- tables: checks and staging ----
+
+struct TableBytes {
+  size_t centers, scales, quats, opacities, colors, ext, sh_texels;
+};
+
+TableBytes table_bytes(const rdx_table& t, uint64_t n) {
+  TableBytes b{};
+  const int k = kShCoeffs[t.sh_degree];
+  if (t.layout == RDX_LAYOUT_RAW) {
+    b.centers = n * 12;
+    b.scales = n * 12;
+    b.quats = n * 16;
+    b.opacities = n * 4;
+    b.colors = n * (size_t)(1 + k) * 3 * (t.color_dtype == RDX_DTYPE_F16 ? 2 : 4);
+  } else {
+    b.ext = n * 16;
+    b.sh_texels = (size_t)((k + 3) / 4);
+  }
+  return b;
+}
+
+size_t color_vec_bytes(const rdx_table& t) {
+  const int k = kShCoeffs[t.sh_degree];
+  const size_t row = (size_t)(1 + k) * 3 * (t.color_dtype == RDX_DTYPE_F16 ? 2 : 4);
+  return row % 16 == 0 ? 16 : (row % 8 == 0 ? 8 : (row % 4 == 0 ? 4 : 2));
+}
+
+int check_table(rdx_ctx* ctx, const rdx_table* t, int index) {
+  if (!t) return fail(ctx, RDX_ERR_ARG, "object %d has no table", index);
+  if (t->layout != RDX_LAYOUT_RAW && t->layout != RDX_LAYOUT_EXT)
+    return fail(ctx, RDX_ERR_UNSUPPORTED, "table layout %d (raw 0 or ext 1)", t->layout);
+  if (t->sh_degree < 0 || t->sh_degree > 4) return fail(ctx, RDX_ERR_ARG, "sh_degree %d (0 to 4)", t->sh_degree);
+  if (t->layout == RDX_LAYOUT_RAW) {
+    if (t->color_dtype != RDX_DTYPE_F32 && t->color_dtype != RDX_DTYPE_F16)
+      return fail(ctx, RDX_ERR_ARG, "color_dtype %d", t->color_dtype);
+    if (!t->centers || !t->log_scales || !t->quats || !t->opacities || !t->colors)
+      return fail(ctx, RDX_ERR_ARG, "raw table of object %d: a column is NULL", index);
+  } else {
+    if (!t->ext_a || !t->ext_b) return fail(ctx, RDX_ERR_ARG, "ext table of object %d: extA or extB is NULL", index);
+    for (int c = 0; c < (kShCoeffs[t->sh_degree] + 3) / 4; c++)
+      if (!t->ext_sh[c]) return fail(ctx, RDX_ERR_ARG, "ext table of object %d: SH texel channel %d is NULL", index, c);
+  }
+  return RDX_OK;
+}
+
+// A table whose columns are on the device: the caller's pointers, or staged copies of host columns
+struct Staged {
+  rdx::DevTable dev;
+};
+
+template <class T>
+const T* stage_column(rdx_ctx* ctx, Arena& a, const T* src, size_t bytes, size_t align, int* status) {
+  if (is_device_ptr(src)) {
+    if (!aligned(src, align)) *status = fail(ctx, RDX_ERR_ARG, "a device column is not %zu-byte aligned", align);
+    a.take<char>(0);
+    return src;
+  }
+  char* dst = a.take<char>(bytes);
+  if (dst && bytes) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) *status = cuda_fail(ctx, e, "copy of a host column");
+  }
+  return reinterpret_cast<const T*>(dst);
+}
+
+rdx::DevTable stage_table(rdx_ctx* ctx, Arena& a, const rdx_table& t, int* status) {
+  rdx::DevTable d{};
+  d.layout = t.layout;
+  d.sh_degree = t.sh_degree;
+  d.color_dtype = t.color_dtype;
+  const uint64_t n = t.count;
+  const TableBytes b = table_bytes(t, n);
+  if (t.layout == RDX_LAYOUT_RAW) {
+    d.centers = stage_column(ctx, a, t.centers, b.centers, 4, status);
+    d.log_scales = stage_column(ctx, a, t.log_scales, b.scales, 4, status);
+    d.quats = stage_column(ctx, a, t.quats, b.quats, 16, status);
+    d.opacities = stage_column(ctx, a, t.opacities, b.opacities, 4, status);
+    d.colors = stage_column(ctx, a, reinterpret_cast<const char*>(t.colors), b.colors, color_vec_bytes(t), status);
+  } else {
+    d.ext_a = stage_column(ctx, a, t.ext_a, b.ext, 16, status);
+    d.ext_b = stage_column(ctx, a, t.ext_b, b.ext, 16, status);
+    for (size_t c = 0; c < b.sh_texels; c++) d.ext_sh[c] = stage_column(ctx, a, t.ext_sh[c], b.ext, 16, status);
+  }
+  return d;
+}
+
+rdx::DevParams dev_params(const rdx_params& p) {
+  rdx::DevParams d{};
+  d.max_std_dev = p.max_std_dev;
+  d.min_alpha = p.min_alpha;
+  d.blur_amount = p.blur_amount;
+  d.pre_blur_amount = p.pre_blur_amount;
+  d.clip_xy = p.clip_xy;
+  d.min_pixel_radius = p.min_pixel_radius;
+  d.max_pixel_radius = p.max_pixel_radius;
+  d.min_contribution = p.min_contribution;
+  d.focal_distance = p.focal_distance;
+  d.aperture_tan = p.aperture_tan;
+  d.sort_guard = p.sort_guard;
+  d.lod_inflate = p.lod_inflate;
+  d.max_sh_degree = p.max_sh_degree;
+  return d;
+}
+
+// Outputs on the device: the caller's pointers, or staging for host ones
+struct OutPlan {
+  rdx::ProjOutputs dev{};
+  struct Back {
+    void* host;
+    const void* dev;
+    size_t bytes;
+  };
+  std::vector<Back> back;
+};
+
+template <class T>
+T* stage_out(rdx_ctx* ctx, Arena& a, T* user, size_t bytes, size_t align, OutPlan& plan, int* status) {
+  if (!user) return nullptr;
+  if (is_device_ptr(user)) {
+    if (!aligned(user, align)) *status = fail(ctx, RDX_ERR_ARG, "a device output is not %zu-byte aligned", align);
+    return user;
+  }
+  T* d = reinterpret_cast<T*>(a.take<char>(bytes));
+  if (d) plan.back.push_back({user, d, bytes});
+  return d;
+}
+
+int copy_back(rdx_ctx* ctx, const OutPlan& plan) {
+  for (const auto& b : plan.back) {
+    if (b.bytes) RDX_CUDA(cudaMemcpyAsync(b.host, b.dev, b.bytes, cudaMemcpyDeviceToHost, ctx->stream), "copy of an output");
+  }
+  return RDX_OK;
+}
+
+struct Camera {
+  rdx::DevEye eye[2];
+  double fh3[2][9];  // from_head 3x3, row-major
+};
+
+int check_camera(rdx_ctx* ctx, const rdx_camera* cam) {
+  if (!cam) return fail(ctx, RDX_ERR_ARG, "camera is NULL");
+  if (cam->eyes < 1 || cam->eyes > 2) return fail(ctx, RDX_ERR_ARG, "SplatCamera: 1 or 2 eyes, not %d", cam->eyes);
+  if (!(cam->width > 0) || !(cam->height > 0)) return fail(ctx, RDX_ERR_ARG, "render size %gx%g", cam->width, cam->height);
+  return RDX_OK;
+}
+
+// SplatCamera.setViews (src/render/splatCamera.ts:119-138) in float64
+Camera setup_camera(const rdx_camera& cam) {
+  Camera c{};
+  double head_world[16];
+  mat4_invert(cam.head, head_world);
+  for (int v = 0; v < cam.eyes; v++) {
+    rdx::DevEye& e = c.eye[v];
+    double fh[16];
+    // Matrix4.equals: element values (splatCamera.ts:128)
+    const bool identity = std::equal(cam.eye[v].view, cam.eye[v].view + 16, cam.head);
+    e.identity = identity ? 1 : 0;
+    if (identity) {
+      memset(fh, 0, sizeof(fh));
+      fh[0] = fh[5] = fh[10] = fh[15] = 1.0;
+    } else {
+      mat4_mul(cam.eye[v].view, head_world, fh);
+    }
+    for (int r = 0; r < 3; r++) {
+      for (int col = 0; col < 4; col++) e.from_head[r * 4 + col] = fh[col * 4 + r];
+      for (int col = 0; col < 3; col++) c.fh3[v][r * 3 + col] = fh[col * 4 + r];
+    }
+    memcpy(e.proj, cam.eye[v].projection, sizeof(e.proj));
+    e.focal[0] = (float)(cam.width * 0.5 * e.proj[0]);
+    e.focal[1] = (float)(cam.height * 0.5 * e.proj[5]);
+    e.proj11 = (float)e.proj[5];
+    e.ortho = cam.eye[v].ortho ? 1 : 0;
+  }
+  return c;
+}
+
+// One descriptor: setTransforms (src/render/splatTransform.tsl.ts:78-107) and
+// the generator context's view origin (src/gpu/splatGenerator.ts:105-112)
+rdx::ProjDesc make_desc(const rdx_camera& cam, const Camera& c, const rdx_object& obj, const rdx::DevTable& table,
+                        const rdx_params& params, uint64_t out_offset, uint64_t out_n, int bits, int pass,
+                        int cull_keys) {
+  rdx::ProjDesc d{};
+  d.table = table;
+  d.params = dev_params(obj.params ? *obj.params : params);
+  double a[16];
+  mat4_mul(cam.head, obj.world, a);
+  double a3[9];
+  bool zero = true;
+  for (int r = 0; r < 3; r++) {
+    for (int col = 0; col < 4; col++) d.a[r * 4 + col] = a[col * 4 + r];
+    for (int col = 0; col < 3; col++) {
+      a3[r * 3 + col] = a[col * 4 + r];
+      zero = zero && a3[r * 3 + col] == 0.0;
+    }
+  }
+  double inv[16];
+  mat4_invert(a, inv);
+  d.origin[0] = inv[12];
+  d.origin[1] = inv[13];
+  d.origin[2] = inv[14];
+  d.degenerate = zero ? 1 : 0;
+  d.count = obj.count;
+  d.out_offset = out_offset;
+  d.out_n = out_n;
+  for (int v = 0; v < cam.eyes; v++) {
+    d.eye[v] = c.eye[v];
+    for (int r = 0; r < 3; r++) {
+      for (int col = 0; col < 3; col++) {
+        double s = c.fh3[v][r * 3 + 0] * a3[0 * 3 + col] + c.fh3[v][r * 3 + 1] * a3[1 * 3 + col] +
+                   c.fh3[v][r * 3 + 2] * a3[2 * 3 + col];
+        d.eye[v].w[r * 3 + col] = (float)s;
+      }
+    }
+  }
+  d.width = cam.width;
+  d.height = cam.height;
+  d.ndc_z_min = cam.ndc_z_min;
+  d.eyes = cam.eyes;
+  d.sort_bits = bits;
+  d.cull_keys = cull_keys;
+  d.keys_only = pass == RDX_PASS_KEYS ? 1 : 0;
+  return d;
+}
+
+struct ProjectCall {
+  std::vector<rdx::ProjDesc> descs;
+  std::vector<int> groups;  // start of each group of one kernel kind in descs (+ end)
+  std::vector<uint32_t> group_tiles;
+  uint64_t n = 0;
+};
+
+int plan_project(rdx_ctx* ctx, Arena& a, const rdx_object* objects, int n_objects, const rdx_camera* cam,
+                 const rdx_params* params, int bits, int pass, int cull_keys, ProjectCall& call) {
+  int status = RDX_OK;
+  const Camera c = setup_camera(*cam);
+  std::map<const rdx_table*, rdx::DevTable> staged;
+  uint64_t n = 0;
+  for (int i = 0; i < n_objects; i++) n += objects[i].count;
+  call.n = n;
+  // group by kernel kind, keeping the collection's output offsets
+  std::map<int, std::vector<rdx::ProjDesc>> by_kind;
+  uint64_t offset = 0;
+  for (int i = 0; i < n_objects; i++) {
+    const rdx_object& o = objects[i];
+    const rdx_table& t = *o.table;
+    if (!staged.count(o.table)) staged[o.table] = stage_table(ctx, a, t, &status);
+    const int kind = t.layout * 100 + t.sh_degree * 10 + (t.layout == RDX_LAYOUT_RAW ? t.color_dtype : 0);
+    if (o.count > 0) {
+      by_kind[kind].push_back(make_desc(*cam, c, o, staged[o.table], *params, offset, n, bits, pass, cull_keys));
+    }
+    offset += o.count;
+  }
+  for (auto& kv : by_kind) {
+    call.groups.push_back((int)call.descs.size());
+    uint32_t tiles = 0;
+    for (auto& d : kv.second) {
+      d.first_tile = tiles;
+      tiles += (uint32_t)((d.count + rdx::kProjThreads - 1) / rdx::kProjThreads);
+      call.descs.push_back(d);
+    }
+    call.group_tiles.push_back(tiles);
+  }
+  call.groups.push_back((int)call.descs.size());
+  return status;
+}
+
+int check_objects(rdx_ctx* ctx, const rdx_object* objects, int n_objects) {
+  if (n_objects < 0 || (n_objects > 0 && !objects)) return fail(ctx, RDX_ERR_ARG, "objects is NULL");
+  uint64_t n = 0;
+  for (int i = 0; i < n_objects; i++) {
+    int s = check_table(ctx, objects[i].table, i);
+    if (s != RDX_OK) return s;
+    if (objects[i].count > objects[i].table->count)
+      return fail(ctx, RDX_ERR_CAPACITY, "object %d draws %llu of its table's %llu splats", i,
+                  (unsigned long long)objects[i].count, (unsigned long long)objects[i].table->count);
+    n += objects[i].count;
+  }
+  if (n > rdx::kMaxSegmentKeys) return fail(ctx, RDX_ERR_CAPACITY, "%llu splats (at most %u)", (unsigned long long)n, rdx::kMaxSegmentKeys);
+  return RDX_OK;
+}
+
+// Enqueue a projection whose plan, descriptor slot and output pointers are ready
+int run_project(rdx_ctx* ctx, rdx::ProjDesc* dev_descs, const ProjectCall& call, const rdx::ProjOutputs& out) {
+  if (!call.descs.empty()) {
+    int st = upload(ctx, dev_descs, call.descs.data(), call.descs.size() * sizeof(rdx::ProjDesc));
+    if (st != RDX_OK) return st;
+  }
+  for (size_t g = 0; g + 1 < call.groups.size(); g++) {
+    const int start = call.groups[g];
+    const int count = call.groups[g + 1] - start;
+    RDX_CUDA(rdx::launch_project(dev_descs + start, call.descs.data() + start, count, call.group_tiles[g], out,
+                                 ctx->stream),
+             "projection launch");
+    if (call.group_tiles[g]) ctx->launches += 1;
+  }
+  return RDX_OK;
+}
+
+bool any_host(std::initializer_list<const void*> ptrs) {
+  for (const void* p : ptrs)
+    if (p && !is_device_ptr(p)) return true;
+  return false;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rdx_version(void) { return RDX_VERSION; }
+
+void rdx_params_default(rdx_params* p) {
+  if (!p) return;
+  p->max_std_dev = (float)sqrt(8.0);
+  p->min_alpha = (float)(0.5 / 255.0);
+  p->falloff = 1.0f;
+  p->lod_inflate = 1;
+  p->blur_amount = 0.3f;
+  p->pre_blur_amount = 0.0f;
+  p->clip_xy = 1.4f;
+  p->min_pixel_radius = 0.0f;
+  p->max_pixel_radius = 512.0f;
+  p->min_contribution = 0.0f;
+  p->focal_distance = 0.0f;
+  p->aperture_tan = 0.0f;
+  p->sort_guard = 0.0f;
+  p->max_sh_degree = 4;
+}
+
+int rdx_ctx_create(int device, rdx_ctx** out) {
+  if (!out) return RDX_ERR_ARG;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+    cudaGetLastError();
+    return RDX_ERR_CUDA;
+  }
+  rdx_ctx* ctx = new rdx_ctx();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&ctx->error_flag, 4) != cudaSuccess || cudaMallocHost(&ctx->error_host, 4) != cudaSuccess ||
+      cudaMemset(ctx->error_flag, 0, 4) != cudaSuccess || cudaMallocHost(&ctx->ring, kRingBytes) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ring_event, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    rdx_ctx_destroy(ctx);
+    return RDX_ERR_CUDA;
+  }
+  *ctx->error_host = 0;
+  ctx->stream = ctx->own_stream;
+  *out = ctx;
+  return RDX_OK;
+}
+
+int rdx_ctx_destroy(rdx_ctx* ctx) {
+  if (!ctx) return RDX_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->arena) cudaFree(ctx->arena);
+  if (ctx->error_flag) cudaFree(ctx->error_flag);
+  if (ctx->error_host) cudaFreeHost(ctx->error_host);
+  for (auto& p : ctx->pending) {
+    cudaEventDestroy(p.start);
+    cudaEventDestroy(p.stop);
+  }
+  for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+  if (ctx->ring_event) cudaEventDestroy(ctx->ring_event);
+  if (ctx->ring) cudaFreeHost(ctx->ring);
+  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return RDX_OK;
+}
+
+int rdx_ctx_set_stream(rdx_ctx* ctx, void* stream) {
+  if (!ctx) return RDX_ERR_ARG;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+  return RDX_OK;
+}
+
+int rdx_ctx_synchronize(rdx_ctx* ctx) {
+  if (!ctx) return RDX_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  return finish(ctx);
+}
+
+int rdx_ctx_reserve(rdx_ctx* ctx, uint64_t max_keys) {
+  if (!ctx) return RDX_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  Arena a(nullptr);
+  take_sort_scratch(a, 1, 4, tiles_of(max_keys), max_keys);
+  a.take<uint32_t>(max_keys * 3);  // keys / compacted pairs of a frame or splat sort
+  a.take<uint64_t>(4);
+  return ensure_arena(ctx, a.used);
+}
+
+int rdx_ctx_set_profiling(rdx_ctx* ctx, int on) {
+  if (!ctx) return RDX_ERR_ARG;
+  ctx->profiling = on != 0;
+  return RDX_OK;
+}
+
+int rdx_ctx_phase_times(rdx_ctx* ctx, double* ms, uint64_t* runs) {
+  if (!ctx) return RDX_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  RDX_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+  for (const auto& p : ctx->pending) {
+    float t = 0.0f;
+    if (cudaEventElapsedTime(&t, p.start, p.stop) == cudaSuccess) {
+      ctx->phase_ms[p.phase] += t;
+      ctx->phase_runs[p.phase] += 1;
+    } else {
+      cudaGetLastError();
+    }
+    ctx->event_pool.push_back(p.start);
+    ctx->event_pool.push_back(p.stop);
+  }
+  ctx->pending.clear();
+  for (int i = 0; i < RDX_PHASES; i++) {
+    if (ms) ms[i] = ctx->phase_ms[i];
+    if (runs) runs[i] = ctx->phase_runs[i];
+    ctx->phase_ms[i] = 0.0;
+    ctx->phase_runs[i] = 0;
+  }
+  return RDX_OK;
+}
+
+int rdx_ctx_launches(rdx_ctx* ctx, uint64_t* launches) {
+  if (!ctx || !launches) return RDX_ERR_ARG;
+  *launches = ctx->launches;
+  return RDX_OK;
+}
+
+const char* rdx_last_error(const rdx_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "no context"; }
+
+int rdx_sort_keys_compute(rdx_ctx* ctx, const double* distances, uint64_t n, int bits, uint32_t* keys) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (!valid_bits(bits)) return fail(ctx, RDX_ERR_ARG, "SortKeys: bits must be 16, 24 or 32 (got %d)", bits);
+  if (n == 0) return RDX_OK;
+  if (!distances || !keys) return fail(ctx, RDX_ERR_ARG, "distances or keys is NULL");
+  cudaSetDevice(ctx->device);
+  const bool host_in = !is_device_ptr(distances), host_out = !is_device_ptr(keys);
+  auto layout = [&](Arena& a, const double** d, uint32_t** k) {
+    *d = host_in ? a.take<double>(n) : distances;
+    *k = host_out ? a.take<uint32_t>(n) : keys;
+  };
+  Arena dry(nullptr);
+  const double* d;
+  uint32_t* k;
+  layout(dry, &d, &k);
+  int s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  layout(a, &d, &k);
+  if (host_in) RDX_CUDA(cudaMemcpyAsync((void*)d, distances, n * 8, cudaMemcpyHostToDevice, ctx->stream), "copy in");
+  RDX_CUDA(rdx::launch_keys_f64(d, n, bits, k, ctx->stream), "keys launch");
+  ctx->launches += 1;
+  if (host_out) RDX_CUDA(cudaMemcpyAsync(keys, k, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  return host_in || host_out ? finish(ctx) : RDX_OK;
+}
+
+int rdx_sort_keys_compute_f32(rdx_ctx* ctx, const float* distances, uint64_t n, int bits, uint32_t* keys) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (!valid_bits(bits)) return fail(ctx, RDX_ERR_ARG, "SortKeys: bits must be 16, 24 or 32 (got %d)", bits);
+  if (n == 0) return RDX_OK;
+  if (!distances || !keys) return fail(ctx, RDX_ERR_ARG, "distances or keys is NULL");
+  cudaSetDevice(ctx->device);
+  const bool host_in = !is_device_ptr(distances), host_out = !is_device_ptr(keys);
+  auto layout = [&](Arena& a, const float** d, uint32_t** k) {
+    *d = host_in ? a.take<float>(n) : distances;
+    *k = host_out ? a.take<uint32_t>(n) : keys;
+  };
+  Arena dry(nullptr);
+  const float* d;
+  uint32_t* k;
+  layout(dry, &d, &k);
+  int s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  layout(a, &d, &k);
+  if (host_in) RDX_CUDA(cudaMemcpyAsync((void*)d, distances, n * 4, cudaMemcpyHostToDevice, ctx->stream), "copy in");
+  RDX_CUDA(rdx::launch_keys_f32(d, n, bits, k, ctx->stream), "keys launch");
+  ctx->launches += 1;
+  if (host_out) RDX_CUDA(cudaMemcpyAsync(keys, k, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  return host_in || host_out ? finish(ctx) : RDX_OK;
+}
+
+// The single-segment descriptors of a sort of n keys, written on the device
+static int single_segment(rdx_ctx* ctx, uint64_t* seg_off, uint32_t* seg_tiles, uint64_t n) {
+  const uint64_t off[2] = {0, n};
+  const uint32_t tiles[2] = {0, tiles_of(n)};
+  int st = upload(ctx, seg_off, off, sizeof(off));
+  return st != RDX_OK ? st : upload(ctx, seg_tiles, tiles, sizeof(tiles));
+}
+
+int rdx_sort(rdx_ctx* ctx, const uint32_t* keys, uint64_t count, int bits, uint32_t* ordering, uint64_t ordering_len,
+             uint32_t* visible) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (!valid_bits(bits)) return fail(ctx, RDX_ERR_ARG, "SortKeys.sort: bits must be 16, 24 or 32 (got %d)", bits);
+  if (ordering_len < count)
+    return fail(ctx, RDX_ERR_CAPACITY, "SortKeys.sort: ordering holds %llu of %llu indices",
+                (unsigned long long)ordering_len, (unsigned long long)count);
+  if (count > rdx::kMaxSegmentKeys)
+    return fail(ctx, RDX_ERR_CAPACITY, "SortKeys.sort: %llu keys (at most %u)", (unsigned long long)count, rdx::kMaxSegmentKeys);
+  cudaSetDevice(ctx->device);
+  if (count == 0) {
+    if (visible) {
+      if (is_device_ptr(visible)) {
+        RDX_CUDA(cudaMemsetAsync(visible, 0, 4, ctx->stream), "visible");
+      } else {
+        *visible = 0;
+      }
+    }
+    return RDX_OK;
+  }
+  if (!keys || !ordering) return fail(ctx, RDX_ERR_ARG, "keys or ordering is NULL");
+  const bool host_keys = !is_device_ptr(keys), host_order = !is_device_ptr(ordering);
+  const bool host_visible = visible && !is_device_ptr(visible);
+  const int passes = bits / 8;
+  const uint32_t tiles = tiles_of(count);
+  auto layout = [&](Arena& a, const uint32_t** k, uint32_t** o, uint32_t** vis, uint64_t** so, uint32_t** st,
+                    rdx::SortScratch* sc) {
+    *k = host_keys ? a.take<uint32_t>(count) : keys;
+    *o = host_order ? a.take<uint32_t>(count) : ordering;
+    *vis = a.take<uint32_t>(1);
+    *so = a.take<uint64_t>(2);
+    *st = a.take<uint32_t>(2);
+    *sc = take_sort_scratch(a, 1, passes, tiles, count);
+  };
+  const uint32_t* k;
+  uint32_t *o, *vis, *st;
+  uint64_t* so;
+  rdx::SortScratch sc;
+  Arena dry(nullptr);
+  layout(dry, &k, &o, &vis, &so, &st, &sc);
+  int s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  layout(a, &k, &o, &vis, &so, &st, &sc);
+  if (host_keys) RDX_CUDA(cudaMemcpyAsync((void*)k, keys, count * 4, cudaMemcpyHostToDevice, ctx->stream), "copy in");
+  s = single_segment(ctx, so, st, count);
+  if (s != RDX_OK) return s;
+  rdx::SortSegments segs{so, st, 1, tiles};
+  Phase sorting(ctx, RDX_PHASE_SORT);
+  RDX_CUDA(rdx::sort_segments(k, nullptr, nullptr, o, segs, bits, sc, ctx->error_flag, ctx->stream), "sort launch");
+  ctx->launches += sort_launches(bits, tiles);
+  sorting.end();
+  if (visible) {
+    RDX_CUDA(rdx::launch_visible(so, sc.ref_hidden, 1, vis, ctx->stream), "visible");
+    ctx->launches += 1;
+    RDX_CUDA(cudaMemcpyAsync(visible, vis, 4, host_visible ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream),
+             "visible copy");
+  }
+  if (host_order) RDX_CUDA(cudaMemcpyAsync(ordering, o, count * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  return host_keys || host_order || host_visible ? finish(ctx) : RDX_OK;
+}
+
+int rdx_sort_pairs(rdx_ctx* ctx, uint32_t* keys, uint32_t* values, uint64_t count, int bits) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (!valid_bits(bits)) return fail(ctx, RDX_ERR_ARG, "WgpuRadixSort: bits must be 16, 24 or 32 (got %d)", bits);
+  if (count == 0) return RDX_OK;  // WgpuRadixSort.ts:119-121
+  if (count > rdx::kMaxSegmentKeys)
+    return fail(ctx, RDX_ERR_CAPACITY, "WgpuRadixSort: %llu keys (at most %u)", (unsigned long long)count, rdx::kMaxSegmentKeys);
+  if (!keys || !values) return fail(ctx, RDX_ERR_ARG, "keys or values is NULL");
+  cudaSetDevice(ctx->device);
+  const bool host_k = !is_device_ptr(keys), host_v = !is_device_ptr(values);
+  const int passes = bits / 8;
+  const uint32_t tiles = tiles_of(count);
+  auto layout = [&](Arena& a, uint32_t** k, uint32_t** v, uint64_t** so, uint32_t** st, rdx::SortScratch* sc) {
+    *k = host_k ? a.take<uint32_t>(count) : keys;
+    *v = host_v ? a.take<uint32_t>(count) : values;
+    *so = a.take<uint64_t>(2);
+    *st = a.take<uint32_t>(2);
+    *sc = take_sort_scratch(a, 1, passes, tiles, count);
+  };
+  uint32_t *k, *v, *st;
+  uint64_t* so;
+  rdx::SortScratch sc;
+  Arena dry(nullptr);
+  layout(dry, &k, &v, &so, &st, &sc);
+  int s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  layout(a, &k, &v, &so, &st, &sc);
+  if (host_k) RDX_CUDA(cudaMemcpyAsync(k, keys, count * 4, cudaMemcpyHostToDevice, ctx->stream), "copy in");
+  if (host_v) RDX_CUDA(cudaMemcpyAsync(v, values, count * 4, cudaMemcpyHostToDevice, ctx->stream), "copy in");
+  s = single_segment(ctx, so, st, count);
+  if (s != RDX_OK) return s;
+  rdx::SortSegments segs{so, st, 1, tiles};
+  {
+    Phase sorting(ctx, RDX_PHASE_SORT);
+    RDX_CUDA(rdx::sort_segments(k, v, k, v, segs, bits, sc, ctx->error_flag, ctx->stream), "sort launch");
+    ctx->launches += sort_launches(bits, tiles);
+  }
+  if (host_k) RDX_CUDA(cudaMemcpyAsync(keys, k, count * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  if (host_v) RDX_CUDA(cudaMemcpyAsync(values, v, count * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  return host_k || host_v ? finish(ctx) : RDX_OK;
+}
+
+int rdx_sort_pairs_indirect(rdx_ctx* ctx, uint32_t* keys, uint32_t* values, const uint32_t* count_dev, uint64_t capacity,
+                            int bits) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (!valid_bits(bits)) return fail(ctx, RDX_ERR_ARG, "WgpuRadixSort: bits must be 16, 24 or 32 (got %d)", bits);
+  if (capacity == 0) return RDX_OK;
+  if (capacity > rdx::kMaxSegmentKeys)
+    return fail(ctx, RDX_ERR_CAPACITY, "WgpuRadixSort: capacity %llu (at most %u)", (unsigned long long)capacity, rdx::kMaxSegmentKeys);
+  cudaSetDevice(ctx->device);
+  if (!is_device_ptr(keys) || !is_device_ptr(values) || !is_device_ptr(count_dev))
+    return fail(ctx, RDX_ERR_ARG, "WgpuRadixSort.sortIndirect: keys, values and count must be device memory");
+  const int passes = bits / 8;
+  const uint32_t tiles = tiles_of(capacity);
+  auto layout = [&](Arena& a, uint64_t** so, uint32_t** st, rdx::SortScratch* sc) {
+    *so = a.take<uint64_t>(2);
+    *st = a.take<uint32_t>(2);
+    *sc = take_sort_scratch(a, 1, passes, tiles, capacity);
+  };
+  uint32_t* st;
+  uint64_t* so;
+  rdx::SortScratch sc;
+  Arena dry(nullptr);
+  layout(dry, &so, &st, &sc);
+  int s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  layout(a, &so, &st, &sc);
+  Phase sorting(ctx, RDX_PHASE_SORT);
+  RDX_CUDA(rdx::launch_indirect_segments(count_dev, capacity, so, st, ctx->stream), "segments");
+  rdx::SortSegments segs{so, st, 1, tiles};
+  RDX_CUDA(rdx::sort_segments(keys, values, keys, values, segs, bits, sc, ctx->error_flag, ctx->stream), "sort launch");
+  ctx->launches += 1 + sort_launches(bits, tiles);
+  return RDX_OK;
+}
+
+int rdx_compact(rdx_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t invalid, uint32_t* keys_out,
+                uint32_t* values_out, uint32_t* count_out) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (n > rdx::kMaxSegmentKeys) return fail(ctx, RDX_ERR_CAPACITY, "WgpuCompact: %llu keys", (unsigned long long)n);
+  if ((!keys && n) || !keys_out || !values_out || !count_out) return fail(ctx, RDX_ERR_ARG, "a buffer is NULL");
+  cudaSetDevice(ctx->device);
+  const bool hk = n && !is_device_ptr(keys), hko = !is_device_ptr(keys_out), hvo = !is_device_ptr(values_out),
+             hc = !is_device_ptr(count_out);
+  auto layout = [&](Arena& a, const uint32_t** k, uint32_t** ko, uint32_t** vo, uint32_t** c, uint32_t** lb) {
+    *k = hk ? a.take<uint32_t>(n) : keys;
+    *ko = hko ? a.take<uint32_t>(n) : keys_out;
+    *vo = hvo ? a.take<uint32_t>(n) : values_out;
+    *c = hc ? a.take<uint32_t>(1) : count_out;
+    *lb = a.take<uint32_t>(n / 4096 + 2);
+  };
+  const uint32_t* k;
+  uint32_t *ko, *vo, *c, *lb;
+  Arena dry(nullptr);
+  layout(dry, &k, &ko, &vo, &c, &lb);
+  int s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  layout(a, &k, &ko, &vo, &c, &lb);
+  if (hk) RDX_CUDA(cudaMemcpyAsync((void*)k, keys, n * 4, cudaMemcpyHostToDevice, ctx->stream), "copy in");
+  RDX_CUDA(rdx::launch_compact(k, n, invalid, ko, vo, c, lb, ctx->error_flag, ctx->stream), "compact launch");
+  ctx->launches += n ? 1 : 0;
+  if (hc) RDX_CUDA(cudaMemcpyAsync(count_out, c, 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  if (hko || hvo) {
+    // only the first *count_out pairs are meaningful: copy them all (n), the rest is unspecified
+    if (hko) RDX_CUDA(cudaMemcpyAsync(keys_out, ko, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+    if (hvo) RDX_CUDA(cudaMemcpyAsync(values_out, vo, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  }
+  return hk || hko || hvo || hc ? finish(ctx) : RDX_OK;
+}
+
+int rdx_splat_sort(rdx_ctx* ctx, const uint32_t* keys, uint64_t count, int bits, uint32_t* values, uint32_t* count_out,
+                   uint32_t* draw_args) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (!valid_bits(bits)) return fail(ctx, RDX_ERR_ARG, "WgpuSplatSorter: bits must be 16, 24 or 32 (got %d)", bits);
+  if (count > rdx::kMaxSegmentKeys) return fail(ctx, RDX_ERR_CAPACITY, "WgpuSplatSorter: %llu keys", (unsigned long long)count);
+  if ((!keys && count) || !values || !count_out) return fail(ctx, RDX_ERR_ARG, "a buffer is NULL");
+  cudaSetDevice(ctx->device);
+  const uint32_t invalid = bits == 32 ? 0xffffffffu : ((1u << bits) - 1u);
+  const bool hk = count && !is_device_ptr(keys), hv = !is_device_ptr(values), hc = !is_device_ptr(count_out),
+             ha = draw_args && !is_device_ptr(draw_args);
+  const int passes = bits / 8;
+  const uint32_t tiles = tiles_of(count);
+  auto layout = [&](Arena& a, const uint32_t** k, uint32_t** v, uint32_t** c, uint32_t** args, uint32_t** kc,
+                    uint32_t** vc, uint32_t** lb, uint64_t** so, uint32_t** st, rdx::SortScratch* sc) {
+    *k = hk ? a.take<uint32_t>(count) : keys;
+    *v = hv ? a.take<uint32_t>(count) : values;
+    *c = hc ? a.take<uint32_t>(1) : count_out;
+    *args = ha ? a.take<uint32_t>(5) : draw_args;
+    *kc = a.take<uint32_t>(count);
+    *vc = a.take<uint32_t>(count);
+    *lb = a.take<uint32_t>(count / 4096 + 2);
+    *so = a.take<uint64_t>(2);
+    *st = a.take<uint32_t>(2);
+    *sc = take_sort_scratch(a, 1, passes, tiles, count);
+  };
+  const uint32_t* k;
+  uint32_t *v, *c, *args, *kc, *vc, *lb, *st;
+  uint64_t* so;
+  rdx::SortScratch sc;
+  Arena dry(nullptr);
+  layout(dry, &k, &v, &c, &args, &kc, &vc, &lb, &so, &st, &sc);
+  int s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  layout(a, &k, &v, &c, &args, &kc, &vc, &lb, &so, &st, &sc);
+  if (hk) RDX_CUDA(cudaMemcpyAsync((void*)k, keys, count * 4, cudaMemcpyHostToDevice, ctx->stream), "copy in");
+  // compact -> sortIndirect -> draw args (WgpuSplatSorter.ts:64-71)
+  Phase sorting(ctx, RDX_PHASE_SORT);
+  RDX_CUDA(rdx::launch_compact(k, count, invalid, kc, vc, c, lb, ctx->error_flag, ctx->stream), "compact launch");
+  ctx->launches += count ? 1 : 0;
+  if (count > 0) {
+    RDX_CUDA(rdx::launch_indirect_segments(c, count, so, st, ctx->stream), "segments");
+    rdx::SortSegments segs{so, st, 1, tiles};
+    RDX_CUDA(rdx::sort_segments(kc, vc, nullptr, v, segs, bits, sc, ctx->error_flag, ctx->stream), "sort launch");
+    ctx->launches += 1 + sort_launches(bits, tiles);
+  }
+  if (args) {
+    RDX_CUDA(rdx::launch_draw_args(c, args, ctx->stream), "draw args");
+    ctx->launches += 1;
+  }
+  sorting.end();
+  if (hc) RDX_CUDA(cudaMemcpyAsync(count_out, c, 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  if (ha) RDX_CUDA(cudaMemcpyAsync(draw_args, args, 20, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  if (hv && count) RDX_CUDA(cudaMemcpyAsync(values, v, count * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  return hk || hv || hc || ha ? finish(ctx) : RDX_OK;
+}
+
+static int project_common(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
+                          const rdx_params* params, int sort_bits, int pass, int cull_keys, const rdx_outputs* out,
+                          uint32_t* ordering, uint32_t* visible, bool sort) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (!valid_bits(sort_bits)) return fail(ctx, RDX_ERR_ARG, "sortBits must be 16, 24 or 32 (got %d)", sort_bits);
+  if (pass != RDX_PASS_FULL && pass != RDX_PASS_KEYS) return fail(ctx, RDX_ERR_ARG, "pass %d", pass);
+  int s = check_camera(ctx, camera);
+  if (s != RDX_OK) return s;
+  s = check_objects(ctx, objects, n_objects);
+  if (s != RDX_OK) return s;
+  rdx_params defaults;
+  rdx_params_default(&defaults);
+  const rdx_params* prm = params ? params : &defaults;
+  rdx_outputs none{};
+  const rdx_outputs* o = out ? out : &none;
+  cudaSetDevice(ctx->device);
+  uint64_t n = 0;
+  for (int i = 0; i < n_objects; i++) n += objects[i].count;
+  const uint64_t E = (uint64_t)camera->eyes;
+  const int passes = sort_bits / 8;
+  const uint32_t tiles = tiles_of(n);
+  if (sort && n > 0 && !ordering) return fail(ctx, RDX_ERR_ARG, "ordering is NULL");
+  const bool host_order = sort && ordering && !is_device_ptr(ordering);
+  const bool host_visible = sort && visible && !is_device_ptr(visible);
+
+  int status = RDX_OK;
+  ProjectCall call;
+  OutPlan plan;
+  uint32_t *keys = nullptr, *ord = nullptr, *vis = nullptr, *st = nullptr;
+  uint64_t* so = nullptr;
+  rdx::ProjDesc* dev_descs = nullptr;
+  rdx::SortScratch sc{};
+  auto layout = [&](Arena& a) {
+    call = ProjectCall();
+    plan = OutPlan();
+    status = plan_project(ctx, a, objects, n_objects, camera, prm, sort_bits, pass, cull_keys, call);
+    dev_descs = a.take<rdx::ProjDesc>(call.descs.size());
+    rdx::ProjOutputs& d = plan.dev;
+    if (pass == RDX_PASS_FULL) {
+      d.mean2d = stage_out(ctx, a, o->mean2d, E * n * 8, 8, plan, &status);
+      d.conic = stage_out(ctx, a, o->conic, E * n * 12, 4, plan, &status);
+      d.depth = stage_out(ctx, a, o->depth, E * n * 4, 4, plan, &status);
+      d.opacity = stage_out(ctx, a, o->opacity, E * n * 4, 4, plan, &status);
+      d.rgb = stage_out(ctx, a, o->rgb, E * n * 12, 4, plan, &status);
+      d.radii = stage_out(ctx, a, o->radii, E * n * 12, 4, plan, &status);
+      d.words = stage_out(ctx, a, o->words, E * n * 16, 16, plan, &status);
+    }
+    d.keys = stage_out(ctx, a, o->keys, n * 4, 4, plan, &status);
+    if (sort) {
+      if (!d.keys) d.keys = a.take<uint32_t>(n);
+      keys = d.keys;
+      ord = host_order ? a.take<uint32_t>(n) : ordering;
+      vis = a.take<uint32_t>(1);
+      so = a.take<uint64_t>(2);
+      st = a.take<uint32_t>(2);
+      sc = take_sort_scratch(a, 1, passes, tiles, n);
+    }
+  };
+  Arena dry(nullptr);
+  layout(dry);
+  if (status != RDX_OK) return status;
+  s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  {
+    Phase copying(ctx, RDX_PHASE_COPY_IN);  // staging copies of host tables are issued by layout()
+    layout(a);
+  }
+  if (status != RDX_OK) return status;
+  {
+    Phase projecting(ctx, RDX_PHASE_PROJECT);
+    s = run_project(ctx, dev_descs, call, plan.dev);
+  }
+  if (s != RDX_OK) return s;
+  if (sort && n > 0) {
+    s = single_segment(ctx, so, st, n);
+    if (s != RDX_OK) return s;
+    Phase sorting(ctx, RDX_PHASE_SORT);
+    rdx::SortSegments segs{so, st, 1, tiles};
+    RDX_CUDA(rdx::sort_segments(keys, nullptr, nullptr, ord, segs, sort_bits, sc, ctx->error_flag, ctx->stream),
+             "sort launch");
+    RDX_CUDA(rdx::launch_visible(so, sc.ref_hidden, 1, vis, ctx->stream), "visible");
+    ctx->launches += sort_launches(sort_bits, tiles) + 1;
+  }
+  if (sort && visible) {
+    if (n == 0) {
+      RDX_CUDA(cudaMemsetAsync(vis, 0, 4, ctx->stream), "visible");
+    }
+    RDX_CUDA(cudaMemcpyAsync(visible, vis, 4, host_visible ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream),
+             "visible copy");
+  }
+  Phase copying_out(ctx, RDX_PHASE_COPY_OUT);
+  s = copy_back(ctx, plan);
+  if (s != RDX_OK) return s;
+  if (host_order && n) RDX_CUDA(cudaMemcpyAsync(ordering, ord, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  copying_out.end();
+  bool host_in = false;
+  for (int i = 0; i < n_objects && !host_in; i++) {
+    const rdx_table& t = *objects[i].table;
+    host_in = t.layout == RDX_LAYOUT_RAW ? any_host({t.centers, t.log_scales, t.quats, t.opacities, t.colors})
+                                         : any_host({t.ext_a, t.ext_b});
+  }
+  return host_in || !plan.back.empty() || host_order || host_visible ? finish(ctx) : RDX_OK;
+}
+
+int rdx_project(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
+                const rdx_params* params, int sort_bits, int pass, int cull_keys, const rdx_outputs* out) {
+  return project_common(ctx, objects, n_objects, camera, params, sort_bits, pass, cull_keys, out, nullptr, nullptr, false);
+}
+
+int rdx_frame(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera, const rdx_params* params,
+              int sort_bits, const rdx_outputs* out, uint32_t* ordering, uint32_t* visible) {
+  return project_common(ctx, objects, n_objects, camera, params, sort_bits, RDX_PASS_FULL, 1, out, ordering, visible, true);
+}
+
+}  // extern "C"

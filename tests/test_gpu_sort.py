@@ -1,0 +1,144 @@
+"""The CUDA sorts against SortKeys.sort (the oracle): the reference's grid of
+widths and counts (test/gpu/renderTests.ts:31-57), compaction then an
+indirect sort (renderTests.ts:59-90), the splat sorter (renderTests.ts:369-390),
+keys from distances, host and device buffers, and ties."""
+import numpy as np
+import pytest
+import torch
+
+import radix_b200 as rb
+from oracle import oracle as orc
+from radix_b200.synthetic import Mulberry32
+from tests.parity import host, to_cuda, u32
+
+pytestmark = pytest.mark.gpu
+BITS = (16, 24, 32)
+
+
+def random_keys(n, bits, seed):
+    return (Mulberry32(seed).uniform(max(n, 1)) * 2.0 ** bits).astype(np.uint64).astype(np.uint32)
+
+
+@pytest.mark.parametrize("bits", BITS)
+@pytest.mark.parametrize("count", [0, 1, 4095, 4096, 4097, 70000, 1_000_003])
+def test_radix_sort_pairs_equals_sort_keys(ctx, bits, count):
+    keys = random_keys(count, bits, 7 + count + bits)
+    vals = np.arange(max(count, 1), dtype=np.uint32)
+    kt, vt = to_cuda(keys.view(np.int32)), to_cuda(vals.view(np.int32))
+    rb.RadixSort(kt, vt, ctx).sort(count, bits)
+    expected, _ = orc.sort(keys, count, bits)
+    got = u32(vt)[:count]
+    np.testing.assert_array_equal(got, expected[:count])
+    np.testing.assert_array_equal(u32(kt)[:count], keys[expected[:count]])
+
+
+@pytest.mark.parametrize("bits", BITS)
+def test_sort_keys_sort_ordering_visible_and_untouched_tail(ctx, bits):
+    n = 300_000
+    keys = random_keys(n, bits, 3)
+    keys[::7] = rb.SortKeys.invalid(bits)
+    ordering = torch.full((rb.align_capacity(n),), 12345, dtype=torch.int32, device="cuda")
+    got, visible = rb.SortKeys.sort(to_cuda(keys.view(np.int32)), n, bits, ordering=ordering, ctx=ctx)
+    expected, exp_visible = orc.sort(keys, n, bits)
+    assert visible == exp_visible
+    np.testing.assert_array_equal(u32(got)[:n], expected[:n])
+    assert (host(got)[n:] == 12345).all()
+
+
+def test_sort_from_and_to_host_memory(ctx):
+    n = 50_000
+    keys = random_keys(n, 24, 5)
+    ordering = np.zeros(rb.align_capacity(n), dtype=np.uint32)
+    got, visible = rb.SortKeys.sort(keys, n, 24, ordering=ordering, ctx=ctx)
+    expected, exp_visible = orc.sort(keys, n, 24)
+    assert got is ordering and visible == exp_visible
+    np.testing.assert_array_equal(ordering, expected)
+
+
+def test_sort_short_ordering_raises_the_reference_message(ctx):
+    with pytest.raises(rb.RadixError, match="SortKeys.sort: ordering holds 10 of 20 indices"):
+        rb.SortKeys.sort(np.zeros(20, dtype=np.uint32), 20, 32, ordering=np.zeros(10, dtype=np.uint32), ctx=ctx)
+    with pytest.raises(rb.RadixError, match="bits must be 16, 24 or 32"):
+        rb.SortKeys.sort(np.zeros(20, dtype=np.uint32), 20, 20, ctx=ctx)
+
+
+@pytest.mark.parametrize("pattern", ["equal", "three", "descending", "ascending", "upper_bits"])
+def test_sort_ties_and_patterns(ctx, pattern):
+    n = 200_000
+    if pattern == "equal":
+        keys = np.full(n, 0x1234, dtype=np.uint32)
+    elif pattern == "three":
+        keys = (random_keys(n, 32, 9) % 3).astype(np.uint32) * 0x01010101
+    elif pattern == "descending":
+        keys = np.arange(n, 0, -1, dtype=np.uint32)
+    elif pattern == "ascending":
+        keys = np.arange(n, dtype=np.uint32)
+    else:  # bits above the width: the 16-bit layout ignores them
+        keys = random_keys(n, 32, 11)
+    bits = 16 if pattern == "upper_bits" else 32
+    got, visible = rb.SortKeys.sort(to_cuda(keys.view(np.int32)), n, bits, ctx=ctx)
+    expected, exp_visible = orc.sort(keys, n, bits)
+    assert visible == exp_visible
+    np.testing.assert_array_equal(u32(got)[:n], expected[:n])
+
+
+@pytest.mark.parametrize("bits", BITS)
+def test_compact_then_sort_indirect_equals_sort_keys(ctx, bits):
+    n = 20000
+    rng = Mulberry32(11)
+    u = rng.uniform(n)
+    v = rng.uniform(n)
+    keys = np.where(u < 0.3, rb.SortKeys.invalid(bits), (v * 0xFF * 2 ** (bits - 8)).astype(np.uint64)).astype(np.uint32)
+    ck, cv, count = rb.Compact(ctx, invalid=rb.SortKeys.invalid(bits)).compact(to_cuda(keys.view(np.int32)))
+    rb.RadixSort(ck, cv, ctx).sort_indirect(count, bits)
+    ordering, visible = orc.sort(keys, n, bits)
+    assert int(u32(count)[0]) == visible
+    np.testing.assert_array_equal(u32(cv)[:visible], ordering[:visible])
+
+
+def test_compact_keeps_input_order(ctx):
+    n = 1_000_000
+    keys = random_keys(n, 32, 4)
+    keys[Mulberry32(2).uniform(n) < 0.5] = 0xFFFFFFFF
+    ck, cv, count = rb.Compact(ctx).compact(to_cuda(keys.view(np.int32)))
+    idx = np.flatnonzero(keys != 0xFFFFFFFF)
+    assert int(u32(count)[0]) == idx.size
+    np.testing.assert_array_equal(u32(cv)[:idx.size], idx)
+    np.testing.assert_array_equal(u32(ck)[:idx.size], keys[idx])
+
+
+@pytest.mark.parametrize("bits", BITS)
+def test_splat_sorter_values_count_and_draw_args(ctx, bits):
+    n = 123_457
+    keys = random_keys(n, bits - 1, 13)
+    keys[Mulberry32(5).uniform(n) < 0.25] = rb.SortKeys.invalid(bits)
+    sorter = rb.SplatSorter(ctx)
+    values, count, args = sorter.sort(to_cuda(keys.view(np.int32)), n, bits)
+    ordering, visible = orc.sort(keys, n, bits)
+    assert sorter.read_count() == visible
+    q = rb.SplatSorter.QUADS_PER_INSTANCE
+    assert list(u32(args)) == [6 * q, -(-visible // q), 0, 0, 0]
+    np.testing.assert_array_equal(u32(values)[:visible], ordering[:visible])
+
+
+@pytest.mark.parametrize("bits", BITS)
+def test_keys_compute_bit_exact(ctx, bits):
+    rng = Mulberry32(21)
+    d = np.concatenate([
+        np.exp(rng.uniform(100_000) * 80 - 40),
+        [0.0, -0.0, 1e-45, 1e-40, 1.0, 2.0 ** -32, 2.0 ** 32, 3e38, 4e38, 1e300, np.inf, -np.inf, np.nan, -1.0],
+    ])
+    got = u32(rb.SortKeys.compute(to_cuda(d), bits, ctx))
+    np.testing.assert_array_equal(got, orc.sort_keys(d, bits))
+    d32 = d.astype(np.float32)
+    got32 = u32(rb.SortKeys.compute(to_cuda(d32), bits, ctx))
+    np.testing.assert_array_equal(got32, np.array([orc.sort_key_f32(x, bits) for x in d32], dtype=np.uint32))
+
+
+def test_sort_large_random_32bit(ctx):
+    n = 4_000_000
+    keys = random_keys(n, 32, 99)
+    got, visible = rb.SortKeys.sort(to_cuda(keys.view(np.int32)), n, 32, ctx=ctx)
+    expected, exp_visible = orc.sort(keys, n, 32)
+    assert visible == exp_visible
+    np.testing.assert_array_equal(u32(got)[:n], expected[:n])
