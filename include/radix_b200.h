@@ -178,7 +178,7 @@ typedef struct rdx_outputs {
 /* A context on CUDA device `device`: its stream, scratch and error state. */
 int rdx_ctx_create(int device, rdx_ctx** out);
 int rdx_ctx_destroy(rdx_ctx* ctx);
-/* Run on `stream` (a cudaStream_t; NULL: the context's own stream). */
+/* Run on `stream` (a cudaStream_t, cudaStreamLegacy included; NULL: the context's own stream). */
 int rdx_ctx_set_stream(rdx_ctx* ctx, void* stream);
 /* Wait for the context's stream; reports a device-side timeout flag. */
 int rdx_ctx_synchronize(rdx_ctx* ctx);

@@ -88,7 +88,10 @@ class Context:
         try:
             torch = _torch()
             if torch.cuda.is_available():
-                _abi.lib().rdx_ctx_set_stream(self.handle, ctypes.c_void_p(torch.cuda.current_stream(self.device).cuda_stream))
+                h = torch.cuda.current_stream(self.device).cuda_stream
+                # torch's default stream is the legacy default stream: handle 0 there,
+                # cudaStreamLegacy (0x1) for the C ABI, where NULL means the context's own
+                _abi.lib().rdx_ctx_set_stream(self.handle, ctypes.c_void_p(h if h else 0x1))
         except ImportError:
             pass
 

@@ -433,8 +433,8 @@ Camera setup_camera(const rdx_camera& cam) {
       for (int col = 0; col < 3; col++) c.fh3[v][r * 3 + col] = fh[col * 4 + r];
     }
     memcpy(e.proj, cam.eye[v].projection, sizeof(e.proj));
-    e.focal[0] = (float)(cam.width * 0.5 * e.proj[0]);
-    e.focal[1] = (float)(cam.height * 0.5 * e.proj[5]);
+    e.focal_d[0] = cam.width * 0.5 * e.proj[0];
+    e.focal_d[1] = cam.height * 0.5 * e.proj[5];
     e.proj11 = (float)e.proj[5];
     e.ortho = cam.eye[v].ortho ? 1 : 0;
   }
@@ -475,7 +475,7 @@ rdx::ProjDesc make_desc(const rdx_camera& cam, const Camera& c, const rdx_object
       for (int col = 0; col < 3; col++) {
         double s = c.fh3[v][r * 3 + 0] * a3[0 * 3 + col] + c.fh3[v][r * 3 + 1] * a3[1 * 3 + col] +
                    c.fh3[v][r * 3 + 2] * a3[2 * 3 + col];
-        d.eye[v].w[r * 3 + col] = (float)s;
+        d.eye[v].wd[r * 3 + col] = s;
       }
     }
   }

@@ -118,7 +118,7 @@ __device__ __forceinline__ int sh_basis_band(int band, double x, double y, doubl
 
 struct Splat {
   float3 center;
-  float3 scales;
+  float3 log_scales;
   float4 quat;
   float opacity;
   float3 rgb;
@@ -169,8 +169,7 @@ __global__ void __launch_bounds__(kProjThreads) k_project(const ProjDesc* __rest
     s.center = make_float3(__uint_as_float(A.x), __uint_as_float(A.y), __uint_as_float(A.z));
     s.opacity = (float)(A.w >> 24) * (1.0f / 128.0f);
     decode_ext_rgb_f64(B.x, base);
-    s.scales = make_float3(expf(half_bits_to_float(B.y)), expf(half_bits_to_float(B.y >> 16)),
-                           expf(half_bits_to_float(B.z)));
+    s.log_scales = make_float3(half_bits_to_float(B.y), half_bits_to_float(B.y >> 16), half_bits_to_float(B.z));
     s.quat = decode_quat_oct32(B.w);
     if constexpr (K > 0) {
 #pragma unroll
@@ -187,7 +186,7 @@ __global__ void __launch_bounds__(kProjThreads) k_project(const ProjDesc* __rest
     const float* cp = tb.centers + i * 3;
     const float* lp = tb.log_scales + i * 3;
     s.center = make_float3(__ldg(cp), __ldg(cp + 1), __ldg(cp + 2));
-    s.scales = make_float3(expf(__ldg(lp)), expf(__ldg(lp + 1)), expf(__ldg(lp + 2)));
+    s.log_scales = make_float3(__ldg(lp), __ldg(lp + 1), __ldg(lp + 2));
     s.quat = __ldg(reinterpret_cast<const float4*>(tb.quats) + i);
     s.opacity = __ldg(tb.opacities + i);
     float col[(1 + K) * 3];
@@ -250,51 +249,57 @@ __global__ void __launch_bounds__(kProjThreads) k_project(const ProjDesc* __rest
   const double hz = affine_row(sd.a + 8, cx, cy, cz);
   const double distance = __dsqrt_rn(dadd(dadd(dmul(hx, hx), dmul(hy, hy)), dmul(hz, hz)));
 
-  // ---- prepareSplat: LoD stretch (projection.tsl.ts:42-64) ----
-  float opacity = s.opacity;
-  float inflate = 1.0f;
-  if (opacity > 1.0f) {
-    opacity = fminf(opacity * 4.0f - 3.0f, 5.0f);
+  // ---- prepareSplat: LoD stretch (projection.tsl.ts:42-64), float64 ----
+  double opacity_d = s.opacity;
+  double inflate2 = 1.0;  // inflate^2 multiplies the covariance
+  if (opacity_d > 1.0) {
+    opacity_d = fmin(opacity_d * 4.0 - 3.0, 5.0);
     if (p.lod_inflate) {
-      inflate = expf((opacity * opacity - 1.0f) * (1.0f / (3.0f * 2.718281828459045f)));
-      opacity = 1.0f;
+      inflate2 = exp((opacity_d * opacity_d - 1.0) * (2.0 / (3.0 * 2.718281828459045)));
+      opacity_d = 1.0;
     }
   }
-  const float sx = s.scales.x * inflate, sy = s.scales.y * inflate, sz = s.scales.z * inflate;
-  const float std_dev = opacity > 1.0f ? p.max_std_dev + (opacity - 1.0f) * 0.7f : p.max_std_dev;
-  const bool degenerate = (sx == 0.0f && sy == 0.0f && sz == 0.0f) || sd.degenerate;
-  const bool invisible = opacity <= 0.0f || opacity < p.min_alpha || degenerate;
+  const float opacity = (float)opacity_d;
+  // scale^2 = exp(2 ln s), float64: the covariance needs more than float32
+  // carries when its off-diagonal cancels
+  const double s2x = exp(2.0 * (double)s.log_scales.x) * inflate2;
+  const double s2y = exp(2.0 * (double)s.log_scales.y) * inflate2;
+  const double s2z = exp(2.0 * (double)s.log_scales.z) * inflate2;
+  const float std_dev = opacity_d > 1.0 ? (float)((double)p.max_std_dev + (opacity_d - 1.0) * 0.7) : p.max_std_dev;
+  const bool degenerate = (s2x == 0.0 && s2y == 0.0 && s2z == 0.0) || sd.degenerate;
+  const bool invisible = opacity_d <= 0.0 || opacity_d < (double)p.min_alpha || degenerate;
 
-  // rotation R(q), row-major (src/gpu/math.tsl.ts:26-44 without the scales)
-  float qx = s.quat.x, qy = s.quat.y, qz = s.quat.z, qw = s.quat.w;
+  // rotation R(q), row-major, float64 (src/gpu/math.tsl.ts:26-44 without the scales)
+  double qx = s.quat.x, qy = s.quat.y, qz = s.quat.z, qw = s.quat.w;
   {
-    const float ql2 = qx * qx + qy * qy + qz * qz + qw * qw;
-    if (ql2 > 0.0f) {
-      const float inv = rsqrtf(ql2);
+    const double ql2 = qx * qx + qy * qy + qz * qz + qw * qw;
+    if (ql2 > 0.0) {
+      const double inv = 1.0 / sqrt(ql2);
       qx *= inv;
       qy *= inv;
       qz *= inv;
       qw *= inv;
     } else {
-      qx = qy = qz = 0.0f;
-      qw = 1.0f;
+      qx = qy = qz = 0.0;
+      qw = 1.0;
     }
   }
-  const float R[9] = {1.0f - 2.0f * (qy * qy + qz * qz), 2.0f * (qx * qy - qw * qz), 2.0f * (qx * qz + qw * qy),
-                      2.0f * (qx * qy + qw * qz), 1.0f - 2.0f * (qx * qx + qz * qz), 2.0f * (qy * qz - qw * qx),
-                      2.0f * (qx * qz - qw * qy), 2.0f * (qy * qz + qw * qx), 1.0f - 2.0f * (qx * qx + qy * qy)};
+  const double R[9] = {1.0 - 2.0 * (qy * qy + qz * qz), 2.0 * (qx * qy - qw * qz), 2.0 * (qx * qz + qw * qy),
+                       2.0 * (qx * qy + qw * qz), 1.0 - 2.0 * (qx * qx + qz * qz), 2.0 * (qy * qz - qw * qx),
+                       2.0 * (qx * qz - qw * qy), 2.0 * (qy * qz + qw * qx), 1.0 - 2.0 * (qx * qx + qy * qy)};
 
   // ---- sort guard (only with params.sort_guard > 0; projection.tsl.ts:145-155) ----
   bool guarded = true;
   if (p.sort_guard > 0.0f) {
     // head-space covariance diagonal: |row_r(A3 R S)|^2
+    const float sx = (float)sqrt(s2x), sy = (float)sqrt(s2y), sz = (float)sqrt(s2z);
     float ext2 = 0.0f;
 #pragma unroll
     for (int r = 0; r < 3; r++) {
       const float a0 = (float)sd.a[r * 4 + 0], a1 = (float)sd.a[r * 4 + 1], a2 = (float)sd.a[r * 4 + 2];
-      const float g0 = (a0 * R[0] + a1 * R[3] + a2 * R[6]) * sx;
-      const float g1 = (a0 * R[1] + a1 * R[4] + a2 * R[7]) * sy;
-      const float g2 = (a0 * R[2] + a1 * R[5] + a2 * R[8]) * sz;
+      const float g0 = (a0 * (float)R[0] + a1 * (float)R[3] + a2 * (float)R[6]) * sx;
+      const float g1 = (a0 * (float)R[1] + a1 * (float)R[4] + a2 * (float)R[7]) * sy;
+      const float g2 = (a0 * (float)R[2] + a1 * (float)R[5] + a2 * (float)R[8]) * sz;
       ext2 = fmaxf(ext2, g0 * g0 + g1 * g1 + g2 * g2);
     }
     const float radius = sqrtf(ext2) * p.max_std_dev;
@@ -330,7 +335,7 @@ __global__ void __launch_bounds__(kProjThreads) k_project(const ProjDesc* __rest
       const double limit = dmul(fmin((double)p.clip_xy, 2.0), clw);
       bool ok = !(invisible || ez >= 0.0 || clz < dmul(sd.ndc_z_min, clw) || clz >= clw || fabs(clx) > limit ||
                   fabs(cly) > limit);
-      const float fz = (float)ez, fx = (float)ex, fy = (float)ey;
+      const float fz = (float)ez;
       float blur = p.blur_amount;
       if (p.focal_distance > 0.0f && p.aperture_tan > 0.0f && fz < 0.0f) {
         const float depth = -fz;
@@ -347,46 +352,52 @@ __global__ void __launch_bounds__(kProjThreads) k_project(const ProjDesc* __rest
       }
       const float ndcx = (float)ndcx_d, ndcy = (float)ndcy_d;
       float a = 0.f, b = 0.f, d = 0.f, det = 0.f, opacity_c = 0.f, scale1 = 0.f, scale2 = 0.f, angle = 0.f;
+      double a_d = 0.0, b_d = 0.0, d_d = 0.0, det_d = 1.0;
       if (ok) {
-        // J (projections.tsl.ts:108-118)
-        float j1x, j1y, j2x = 0.f, j2y = 0.f;
+        // J (projections.tsl.ts:108-118), float64
+        double j1x, j1y, j2x = 0.0, j2y = 0.0;
         if (e.ortho) {
-          j1x = e.focal[0];
-          j1y = e.focal[1];
+          j1x = e.focal_d[0];
+          j1y = e.focal_d[1];
         } else {
-          const float inv_z = 1.0f / fz;
-          j1x = e.focal[0] * inv_z;
-          j1y = e.focal[1] * inv_z;
-          j2x = -(j1x * fx) * inv_z;
-          j2y = -(j1y * fy) * inv_z;
+          const double inv_z = 1.0 / ez;
+          j1x = e.focal_d[0] * inv_z;
+          j1y = e.focal_d[1] * inv_z;
+          j2x = -(j1x * ex) * inv_z;
+          j2y = -(j1y * ey) * inv_z;
         }
-        // rows of J^T W (W = object -> eye 3x3)
-        const float* W = e.w;
-        const float w0x = j1x * W[0] + j2x * W[6], w0y = j1x * W[1] + j2x * W[7], w0z = j1x * W[2] + j2x * W[8];
-        const float w1x = j1y * W[3] + j2y * W[6], w1y = j1y * W[4] + j2y * W[7], w1z = j1y * W[5] + j2y * W[8];
-        // rows of J^T W R
-        const float u00 = w0x * R[0] + w0y * R[3] + w0z * R[6];
-        const float u01 = w0x * R[1] + w0y * R[4] + w0z * R[7];
-        const float u02 = w0x * R[2] + w0y * R[5] + w0z * R[8];
-        const float u10 = w1x * R[0] + w1y * R[3] + w1z * R[6];
-        const float u11 = w1x * R[1] + w1y * R[4] + w1z * R[7];
-        const float u12 = w1x * R[2] + w1y * R[5] + w1z * R[8];
-        const float t00 = u00 * sx, t01 = u01 * sy, t02 = u02 * sz;
-        const float t10 = u10 * sx, t11 = u11 * sy, t12 = u12 * sz;
-        const float ra = t00 * t00 + t01 * t01 + t02 * t02;
-        const float rd = t10 * t10 + t11 * t11 + t12 * t12;
-        b = t00 * t10 + t01 * t11 + t02 * t12;
-        const float m0 = (u01 * u12 - u02 * u11) * sy * sz;
-        const float m1 = (u02 * u10 - u00 * u12) * sx * sz;
-        const float m2 = (u00 * u11 - u01 * u10) * sx * sy;
-        const float det_t = m0 * m0 + m1 * m1 + m2 * m2;
-        const float pre = p.pre_blur_amount, full = p.pre_blur_amount + blur;
-        const float det_orig = det_t + pre * (ra + rd) + pre * pre;
-        det = det_t + full * (ra + rd) + full * full;
-        a = ra + full;
-        d = rd + full;
-        opacity_c = opacity * sqrtf(fmaxf(0.0f, det_orig / det));
-        const float contribution = opacity_c * 6.283185307179586f * sqrtf(fmaxf(0.0f, det));
+        // rows of J^T W (W = object -> eye 3x3), then of J^T W R
+        const double* W = e.wd;
+        const double w0x = j1x * W[0] + j2x * W[6], w0y = j1x * W[1] + j2x * W[7], w0z = j1x * W[2] + j2x * W[8];
+        const double w1x = j1y * W[3] + j2y * W[6], w1y = j1y * W[4] + j2y * W[7], w1z = j1y * W[5] + j2y * W[8];
+        const double u00 = w0x * R[0] + w0y * R[3] + w0z * R[6];
+        const double u01 = w0x * R[1] + w0y * R[4] + w0z * R[7];
+        const double u02 = w0x * R[2] + w0y * R[5] + w0z * R[8];
+        const double u10 = w1x * R[0] + w1y * R[3] + w1z * R[6];
+        const double u11 = w1x * R[1] + w1y * R[4] + w1z * R[7];
+        const double u12 = w1x * R[2] + w1y * R[5] + w1z * R[8];
+        // cov2D = T T^T with T = U S: a = sum u0k^2 s_k^2, d = sum u1k^2 s_k^2, b = sum u0k u1k s_k^2
+        const double ra = u00 * u00 * s2x + u01 * u01 * s2y + u02 * u02 * s2z;
+        const double rd = u10 * u10 * s2x + u11 * u11 * s2y + u12 * u12 * s2z;
+        const double rb = u00 * u10 * s2x + u01 * u11 * s2y + u02 * u12 * s2z;
+        // det(T T^T) by Cauchy-Binet: sum over column pairs of (s_j s_k (u0 x u1)_l)^2
+        const double m0 = u01 * u12 - u02 * u11;
+        const double m1 = u02 * u10 - u00 * u12;
+        const double m2 = u00 * u11 - u01 * u10;
+        const double det_t = m0 * m0 * (s2y * s2z) + m1 * m1 * (s2x * s2z) + m2 * m2 * (s2x * s2y);
+        const double pre = p.pre_blur_amount, full = (double)p.pre_blur_amount + (double)blur;
+        const double det_orig = det_t + pre * (ra + rd) + pre * pre;
+        det_d = det_t + full * (ra + rd) + full * full;
+        a_d = ra + full;
+        d_d = rd + full;
+        b_d = rb;
+        const double opacity_cd = opacity_d * sqrt(fmax(0.0, det_orig / det_d));
+        opacity_c = (float)opacity_cd;
+        const double contribution = opacity_cd * 6.283185307179586 * sqrt(fmax(0.0, det_d));
+        a = (float)a_d;
+        b = (float)b_d;
+        d = (float)d_d;
+        det = (float)det_d;
         // boundFromCov (projection.tsl.ts:223-240)
         const float half = (a - d) * 0.5f;
         const float eigen1 = (a + d) * 0.5f + sqrtf(half * half + b * b);
@@ -415,19 +426,19 @@ __global__ void __launch_bounds__(kProjThreads) k_project(const ProjDesc* __rest
           angle = atan2f(vy, vx);
           if (angle < 0.0f) angle += 3.14159265358979f;
         }
-        ok = opacity_c >= p.min_alpha && contribution >= p.min_contribution && bound_ok;
+        ok = opacity_cd >= (double)p.min_alpha && contribution >= (double)p.min_contribution && bound_ok;
       }
       const uint64_t ei = (uint64_t)v * sd.out_n + gi;
       if (ok) {
-        const float inv_det = 1.0f / det;
+        const double inv_det = 1.0 / det_d;
         if (out.mean2d) {
           reinterpret_cast<float2*>(out.mean2d)[ei] =
               make_float2((float)((ndcx_d + 1.0) * 0.5 * sd.width), (float)((ndcy_d + 1.0) * 0.5 * sd.height));
         }
         if (out.conic) {
-          out.conic[ei * 3 + 0] = d * inv_det;
-          out.conic[ei * 3 + 1] = -b * inv_det;
-          out.conic[ei * 3 + 2] = a * inv_det;
+          out.conic[ei * 3 + 0] = (float)(d_d * inv_det);
+          out.conic[ei * 3 + 1] = (float)(-b_d * inv_det);
+          out.conic[ei * 3 + 2] = (float)(a_d * inv_det);
         }
         if (out.depth) out.depth[ei] = -fz;
         if (out.opacity) out.opacity[ei] = opacity_c;

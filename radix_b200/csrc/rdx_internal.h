@@ -98,8 +98,8 @@ struct DevParams {
 struct DevEye {
   double from_head[12];  // rows of the 3x4 head -> eye transform
   double proj[16];       // column-major projection
-  float w[9];            // object -> eye 3x3, row-major (from_head3 * a3)
-  float focal[2];
+  double wd[9];          // object -> eye 3x3, row-major (from_head3 * a3)
+  double focal_d[2];     // size / 2 * (P00, P11)
   float proj11;          // projection element (1, 1) for the depth of field
   int identity;          // from_head is exactly the identity
   int ortho;
