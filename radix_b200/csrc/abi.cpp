@@ -44,6 +44,11 @@ struct rdx_ctx {
   size_t ring_off = 0;
   cudaEvent_t ring_event = nullptr;
   bool ring_used = false;
+  // Lookback words of the onesweep passes, tagged with a per-call epoch so
+  // they never need clearing; zeroed once when (re)allocated
+  uint64_t* lookback = nullptr;
+  size_t lookback_words = 0;
+  uint32_t epoch = 0;
 };
 
 static const size_t kRingBytes = 4u << 20;
@@ -183,20 +188,57 @@ bool valid_bits(int bits) { return bits == 16 || bits == 24 || bits == 32; }
 
 uint32_t tiles_of(uint64_t n) { return (uint32_t)((n + rdx::kSortTile - 1) / rdx::kSortTile); }
 
-// Sort scratch for `segments` segments of `total` keys, max_tiles tiles, `passes` passes
-rdx::SortScratch take_sort_scratch(Arena& a, int segments, int passes, uint32_t max_tiles, uint64_t total) {
-  rdx::SortScratch s;
-  // hist, ref_hidden and counters contiguous (one memset)
+// Sort scratch for `segments` segments of `total` keys
+rdx::SortScratch take_sort_scratch(Arena& a, int segments, int passes, uint64_t total) {
+  rdx::SortScratch s{};
+  // hist, valid, ref_hidden and counters contiguous (one memset)
   uint32_t* small = a.take<uint32_t>(rdx::sort_small_state_words(segments, passes));
-  s.hist = small;
-  s.ref_hidden = small ? small + (size_t)segments * passes * rdx::kRadix : nullptr;
-  s.counters = small ? s.ref_hidden + segments : nullptr;
-  s.lookback = a.take<uint32_t>((size_t)passes * max_tiles * rdx::kRadix);
+  if (small) {
+    s.hist = small;
+    s.valid = small + (size_t)segments * passes * rdx::kRadix;
+    s.ref_hidden = s.valid + segments;
+    s.counters = s.ref_hidden + segments;
+  }
+  s.vbegin = a.take<uint64_t>(segments);
+  s.vend = a.take<uint64_t>(segments);
+  s.vtiles = a.take<uint32_t>(segments + 1);
   s.keys_a = a.take<uint32_t>(total);
   s.vals_a = a.take<uint32_t>(total);
   s.keys_b = a.take<uint32_t>(passes > 2 ? total : 0);
   s.vals_b = a.take<uint32_t>(passes > 2 ? total : 0);
   return s;
+}
+
+// Segment descriptors in the arena
+struct SegBufs {
+  uint64_t* begin;
+  uint64_t* end;
+  uint32_t* tiles;
+};
+
+SegBufs take_segs(Arena& a, int segments) {
+  SegBufs b;
+  b.begin = a.take<uint64_t>(segments);
+  b.end = a.take<uint64_t>(segments);
+  b.tiles = a.take<uint32_t>(segments + 1);
+  return b;
+}
+
+// Grow the context's lookback words to `words` (zeroed: epoch 0 is never used)
+int ensure_lookback(rdx_ctx* ctx, size_t words) {
+  if (words <= ctx->lookback_words) return RDX_OK;
+  RDX_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+  if (ctx->lookback) cudaFree(ctx->lookback);
+  ctx->lookback = nullptr;
+  ctx->lookback_words = 0;
+  const size_t want = words + words / 4 + 4096;
+  if (cudaMalloc(&ctx->lookback, want * 8) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, RDX_ERR_NOMEM, "could not allocate %zu lookback words", want);
+  }
+  RDX_CUDA(cudaMemsetAsync(ctx->lookback, 0, want * 8, ctx->stream), "lookback clear");
+  ctx->lookback_words = want;
+  return RDX_OK;
 }
 
 // ---- float64 matrices, column-major (the same sums, in the same order, as the oracle) ----
@@ -260,9 +302,6 @@ int mat4_invert(const double m[16], double out[16]) {
 }
 
 const int kShCoeffs[5] = {0, 3, 8, 15, 24};
-
-// Kernels of one sort_segments call: the histogram and one onesweep per pass
-uint64_t sort_launches(int bits, uint32_t max_tiles) { return max_tiles ? 1 + (uint64_t)(bits / 8) : 0; }
 
 // ---- tables: checks and staging ----
 
@@ -479,6 +518,14 @@ rdx::ProjDesc make_desc(const rdx_camera& cam, const Camera& c, const rdx_object
       }
     }
   }
+  const rdx::DevTable& t = table;
+  auto a16 = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+  bool tma = t.layout == RDX_LAYOUT_RAW ? a16(t.centers) && a16(t.log_scales) && a16(t.quats) && a16(t.opacities) && a16(t.colors)
+                                        : a16(t.ext_a) && a16(t.ext_b);
+  if (t.layout == RDX_LAYOUT_EXT)
+    for (int c = 0; c < (kShCoeffs[t.sh_degree] + 3) / 4; c++) tma = tma && a16(t.ext_sh[c]);
+  d.tma_ok = tma ? 1 : 0;
+  d.segment = 0;
   d.width = cam.width;
   d.height = cam.height;
   d.ndc_z_min = cam.ndc_z_min;
@@ -522,7 +569,7 @@ int plan_project(rdx_ctx* ctx, Arena& a, const rdx_object* objects, int n_object
     uint32_t tiles = 0;
     for (auto& d : kv.second) {
       d.first_tile = tiles;
-      tiles += (uint32_t)((d.count + rdx::kProjThreads - 1) / rdx::kProjThreads);
+      tiles += (uint32_t)((d.count + rdx::kProjTile - 1) / rdx::kProjTile);
       call.descs.push_back(d);
     }
     call.group_tiles.push_back(tiles);
@@ -547,7 +594,8 @@ int check_objects(rdx_ctx* ctx, const rdx_object* objects, int n_objects) {
 }
 
 // Enqueue a projection whose plan, descriptor slot and output pointers are ready
-int run_project(rdx_ctx* ctx, rdx::ProjDesc* dev_descs, const ProjectCall& call, const rdx::ProjOutputs& out) {
+int run_project(rdx_ctx* ctx, rdx::ProjDesc* dev_descs, const ProjectCall& call, const rdx::ProjOutputs& out,
+                const rdx::ProjHist& hist) {
   if (!call.descs.empty()) {
     int st = upload(ctx, dev_descs, call.descs.data(), call.descs.size() * sizeof(rdx::ProjDesc));
     if (st != RDX_OK) return st;
@@ -555,11 +603,37 @@ int run_project(rdx_ctx* ctx, rdx::ProjDesc* dev_descs, const ProjectCall& call,
   for (size_t g = 0; g + 1 < call.groups.size(); g++) {
     const int start = call.groups[g];
     const int count = call.groups[g + 1] - start;
-    RDX_CUDA(rdx::launch_project(dev_descs + start, call.descs.data() + start, count, call.group_tiles[g], out,
-                                 ctx->stream),
+    RDX_CUDA(rdx::launch_project(dev_descs + start, call.descs.data() + start, count, call.group_tiles[g], out, hist,
+                                 ctx->error_flag, ctx->stream),
              "projection launch");
     if (call.group_tiles[g]) ctx->launches += 1;
   }
+  return RDX_OK;
+}
+
+// Enqueue one sort (every pass) with a fresh lookback epoch
+int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
+             const SegBufs& sb, int segments, uint32_t max_tiles, int bits, const rdx::SortScratch& sc,
+             bool hist_ready) {
+  const int passes = bits / 8;
+  int st = ensure_lookback(ctx, (size_t)passes * max_tiles * rdx::kRadix);
+  if (st != RDX_OK) return st;
+  if (++ctx->epoch == 0) ctx->epoch = 1;  // 0 marks a cleared word
+  rdx::SortCall c{};
+  c.keys_in = keys_in;
+  c.vals_in = vals_in;
+  c.keys_out = keys_out;
+  c.vals_out = vals_out;
+  c.segs = rdx::SortSegments{sb.begin, sb.end, sb.tiles, segments, max_tiles};
+  c.bits = bits;
+  c.hist_ready = hist_ready;
+  c.scratch = sc;
+  c.lookback = ctx->lookback;
+  c.epoch = ctx->epoch;
+  c.error_flag = ctx->error_flag;
+  int launches = 0;
+  RDX_CUDA(rdx::sort_segments(c, ctx->stream, &launches), "sort launch");
+  ctx->launches += (uint64_t)launches;
   return RDX_OK;
 }
 
@@ -622,6 +696,7 @@ int rdx_ctx_destroy(rdx_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->arena) cudaFree(ctx->arena);
+  if (ctx->lookback) cudaFree(ctx->lookback);
   if (ctx->error_flag) cudaFree(ctx->error_flag);
   if (ctx->error_host) cudaFreeHost(ctx->error_host);
   for (auto& p : ctx->pending) {
@@ -652,10 +727,11 @@ int rdx_ctx_reserve(rdx_ctx* ctx, uint64_t max_keys) {
   if (!ctx) return RDX_ERR_ARG;
   cudaSetDevice(ctx->device);
   Arena a(nullptr);
-  take_sort_scratch(a, 1, 4, tiles_of(max_keys), max_keys);
-  a.take<uint32_t>(max_keys * 3);  // keys / compacted pairs of a frame or splat sort
-  a.take<uint64_t>(4);
-  return ensure_arena(ctx, a.used);
+  take_sort_scratch(a, 1, 4, max_keys);
+  take_segs(a, 1);
+  a.take<uint32_t>(max_keys * 3);  // keys / staged buffers of a frame or splat sort
+  int st = ensure_arena(ctx, a.used);
+  return st != RDX_OK ? st : ensure_lookback(ctx, (size_t)4 * tiles_of(max_keys) * rdx::kRadix);
 }
 
 int rdx_ctx_set_profiling(rdx_ctx* ctx, int on) {
@@ -750,11 +826,12 @@ int rdx_sort_keys_compute_f32(rdx_ctx* ctx, const float* distances, uint64_t n, 
 }
 
 // The single-segment descriptors of a sort of n keys, written on the device
-static int single_segment(rdx_ctx* ctx, uint64_t* seg_off, uint32_t* seg_tiles, uint64_t n) {
-  const uint64_t off[2] = {0, n};
+static int single_segment(rdx_ctx* ctx, const SegBufs& sb, uint64_t n) {
+  const uint64_t begin[1] = {0}, end[1] = {n};
   const uint32_t tiles[2] = {0, tiles_of(n)};
-  int st = upload(ctx, seg_off, off, sizeof(off));
-  return st != RDX_OK ? st : upload(ctx, seg_tiles, tiles, sizeof(tiles));
+  int st = upload(ctx, sb.begin, begin, sizeof(begin));
+  if (st == RDX_OK) st = upload(ctx, sb.end, end, sizeof(end));
+  return st != RDX_OK ? st : upload(ctx, sb.tiles, tiles, sizeof(tiles));
 }
 
 int rdx_sort(rdx_ctx* ctx, const uint32_t* keys, uint64_t count, int bits, uint32_t* ordering, uint64_t ordering_len,
@@ -782,35 +859,33 @@ int rdx_sort(rdx_ctx* ctx, const uint32_t* keys, uint64_t count, int bits, uint3
   const bool host_visible = visible && !is_device_ptr(visible);
   const int passes = bits / 8;
   const uint32_t tiles = tiles_of(count);
-  auto layout = [&](Arena& a, const uint32_t** k, uint32_t** o, uint32_t** vis, uint64_t** so, uint32_t** st,
-                    rdx::SortScratch* sc) {
-    *k = host_keys ? a.take<uint32_t>(count) : keys;
-    *o = host_order ? a.take<uint32_t>(count) : ordering;
-    *vis = a.take<uint32_t>(1);
-    *so = a.take<uint64_t>(2);
-    *st = a.take<uint32_t>(2);
-    *sc = take_sort_scratch(a, 1, passes, tiles, count);
-  };
   const uint32_t* k;
-  uint32_t *o, *vis, *st;
-  uint64_t* so;
+  uint32_t *o, *vis;
+  SegBufs sb;
   rdx::SortScratch sc;
+  auto layout = [&](Arena& a) {
+    k = host_keys ? a.take<uint32_t>(count) : keys;
+    o = host_order ? a.take<uint32_t>(count) : ordering;
+    vis = a.take<uint32_t>(1);
+    sb = take_segs(a, 1);
+    sc = take_sort_scratch(a, 1, passes, count);
+  };
   Arena dry(nullptr);
-  layout(dry, &k, &o, &vis, &so, &st, &sc);
+  layout(dry);
   int s = ensure_arena(ctx, dry.used);
   if (s != RDX_OK) return s;
   Arena a(ctx->arena);
-  layout(a, &k, &o, &vis, &so, &st, &sc);
+  layout(a);
   if (host_keys) RDX_CUDA(cudaMemcpyAsync((void*)k, keys, count * 4, cudaMemcpyHostToDevice, ctx->stream), "copy in");
-  s = single_segment(ctx, so, st, count);
+  s = single_segment(ctx, sb, count);
   if (s != RDX_OK) return s;
-  rdx::SortSegments segs{so, st, 1, tiles};
-  Phase sorting(ctx, RDX_PHASE_SORT);
-  RDX_CUDA(rdx::sort_segments(k, nullptr, nullptr, o, segs, bits, sc, ctx->error_flag, ctx->stream), "sort launch");
-  ctx->launches += sort_launches(bits, tiles);
-  sorting.end();
+  {
+    Phase sorting(ctx, RDX_PHASE_SORT);
+    s = run_sort(ctx, k, nullptr, nullptr, o, sb, 1, tiles, bits, sc, false);
+    if (s != RDX_OK) return s;
+  }
   if (visible) {
-    RDX_CUDA(rdx::launch_visible(so, sc.ref_hidden, 1, vis, ctx->stream), "visible");
+    RDX_CUDA(rdx::launch_visible(sb.begin, sb.end, sc.ref_hidden, sc.valid, 1, vis, ctx->stream), "visible");
     ctx->launches += 1;
     RDX_CUDA(cudaMemcpyAsync(visible, vis, 4, host_visible ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream),
              "visible copy");
@@ -830,31 +905,29 @@ int rdx_sort_pairs(rdx_ctx* ctx, uint32_t* keys, uint32_t* values, uint64_t coun
   const bool host_k = !is_device_ptr(keys), host_v = !is_device_ptr(values);
   const int passes = bits / 8;
   const uint32_t tiles = tiles_of(count);
-  auto layout = [&](Arena& a, uint32_t** k, uint32_t** v, uint64_t** so, uint32_t** st, rdx::SortScratch* sc) {
-    *k = host_k ? a.take<uint32_t>(count) : keys;
-    *v = host_v ? a.take<uint32_t>(count) : values;
-    *so = a.take<uint64_t>(2);
-    *st = a.take<uint32_t>(2);
-    *sc = take_sort_scratch(a, 1, passes, tiles, count);
-  };
-  uint32_t *k, *v, *st;
-  uint64_t* so;
+  uint32_t *k, *v;
+  SegBufs sb;
   rdx::SortScratch sc;
+  auto layout = [&](Arena& a) {
+    k = host_k ? a.take<uint32_t>(count) : keys;
+    v = host_v ? a.take<uint32_t>(count) : values;
+    sb = take_segs(a, 1);
+    sc = take_sort_scratch(a, 1, passes, count);
+  };
   Arena dry(nullptr);
-  layout(dry, &k, &v, &so, &st, &sc);
+  layout(dry);
   int s = ensure_arena(ctx, dry.used);
   if (s != RDX_OK) return s;
   Arena a(ctx->arena);
-  layout(a, &k, &v, &so, &st, &sc);
+  layout(a);
   if (host_k) RDX_CUDA(cudaMemcpyAsync(k, keys, count * 4, cudaMemcpyHostToDevice, ctx->stream), "copy in");
   if (host_v) RDX_CUDA(cudaMemcpyAsync(v, values, count * 4, cudaMemcpyHostToDevice, ctx->stream), "copy in");
-  s = single_segment(ctx, so, st, count);
+  s = single_segment(ctx, sb, count);
   if (s != RDX_OK) return s;
-  rdx::SortSegments segs{so, st, 1, tiles};
   {
     Phase sorting(ctx, RDX_PHASE_SORT);
-    RDX_CUDA(rdx::sort_segments(k, v, k, v, segs, bits, sc, ctx->error_flag, ctx->stream), "sort launch");
-    ctx->launches += sort_launches(bits, tiles);
+    s = run_sort(ctx, k, v, k, v, sb, 1, tiles, bits, sc, false);
+    if (s != RDX_OK) return s;
   }
   if (host_k) RDX_CUDA(cudaMemcpyAsync(keys, k, count * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
   if (host_v) RDX_CUDA(cudaMemcpyAsync(values, v, count * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
@@ -873,26 +946,22 @@ int rdx_sort_pairs_indirect(rdx_ctx* ctx, uint32_t* keys, uint32_t* values, cons
     return fail(ctx, RDX_ERR_ARG, "WgpuRadixSort.sortIndirect: keys, values and count must be device memory");
   const int passes = bits / 8;
   const uint32_t tiles = tiles_of(capacity);
-  auto layout = [&](Arena& a, uint64_t** so, uint32_t** st, rdx::SortScratch* sc) {
-    *so = a.take<uint64_t>(2);
-    *st = a.take<uint32_t>(2);
-    *sc = take_sort_scratch(a, 1, passes, tiles, capacity);
-  };
-  uint32_t* st;
-  uint64_t* so;
+  SegBufs sb;
   rdx::SortScratch sc;
+  auto layout = [&](Arena& a) {
+    sb = take_segs(a, 1);
+    sc = take_sort_scratch(a, 1, passes, capacity);
+  };
   Arena dry(nullptr);
-  layout(dry, &so, &st, &sc);
+  layout(dry);
   int s = ensure_arena(ctx, dry.used);
   if (s != RDX_OK) return s;
   Arena a(ctx->arena);
-  layout(a, &so, &st, &sc);
+  layout(a);
   Phase sorting(ctx, RDX_PHASE_SORT);
-  RDX_CUDA(rdx::launch_indirect_segments(count_dev, capacity, so, st, ctx->stream), "segments");
-  rdx::SortSegments segs{so, st, 1, tiles};
-  RDX_CUDA(rdx::sort_segments(keys, values, keys, values, segs, bits, sc, ctx->error_flag, ctx->stream), "sort launch");
-  ctx->launches += 1 + sort_launches(bits, tiles);
-  return RDX_OK;
+  RDX_CUDA(rdx::launch_indirect_segments(count_dev, capacity, sb.begin, sb.end, sb.tiles, ctx->stream), "segments");
+  ctx->launches += 1;
+  return run_sort(ctx, keys, values, keys, values, sb, 1, tiles, bits, sc, false);
 }
 
 int rdx_compact(rdx_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t invalid, uint32_t* keys_out,
@@ -903,30 +972,28 @@ int rdx_compact(rdx_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t invalid
   cudaSetDevice(ctx->device);
   const bool hk = n && !is_device_ptr(keys), hko = !is_device_ptr(keys_out), hvo = !is_device_ptr(values_out),
              hc = !is_device_ptr(count_out);
-  auto layout = [&](Arena& a, const uint32_t** k, uint32_t** ko, uint32_t** vo, uint32_t** c, uint32_t** lb) {
-    *k = hk ? a.take<uint32_t>(n) : keys;
-    *ko = hko ? a.take<uint32_t>(n) : keys_out;
-    *vo = hvo ? a.take<uint32_t>(n) : values_out;
-    *c = hc ? a.take<uint32_t>(1) : count_out;
-    *lb = a.take<uint32_t>(n / 4096 + 2);
-  };
   const uint32_t* k;
   uint32_t *ko, *vo, *c, *lb;
+  auto layout = [&](Arena& a) {
+    k = hk ? a.take<uint32_t>(n) : keys;
+    ko = hko ? a.take<uint32_t>(n) : keys_out;
+    vo = hvo ? a.take<uint32_t>(n) : values_out;
+    c = hc ? a.take<uint32_t>(1) : count_out;
+    lb = a.take<uint32_t>(n / 4096 + 2);
+  };
   Arena dry(nullptr);
-  layout(dry, &k, &ko, &vo, &c, &lb);
+  layout(dry);
   int s = ensure_arena(ctx, dry.used);
   if (s != RDX_OK) return s;
   Arena a(ctx->arena);
-  layout(a, &k, &ko, &vo, &c, &lb);
+  layout(a);
   if (hk) RDX_CUDA(cudaMemcpyAsync((void*)k, keys, n * 4, cudaMemcpyHostToDevice, ctx->stream), "copy in");
   RDX_CUDA(rdx::launch_compact(k, n, invalid, ko, vo, c, lb, ctx->error_flag, ctx->stream), "compact launch");
   ctx->launches += n ? 1 : 0;
   if (hc) RDX_CUDA(cudaMemcpyAsync(count_out, c, 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
-  if (hko || hvo) {
-    // only the first *count_out pairs are meaningful: copy them all (n), the rest is unspecified
-    if (hko) RDX_CUDA(cudaMemcpyAsync(keys_out, ko, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
-    if (hvo) RDX_CUDA(cudaMemcpyAsync(values_out, vo, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
-  }
+  // only the first *count_out pairs are meaningful: all n are copied, the rest unspecified
+  if (hko) RDX_CUDA(cudaMemcpyAsync(keys_out, ko, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  if (hvo) RDX_CUDA(cudaMemcpyAsync(values_out, vo, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
   return hk || hko || hvo || hc ? finish(ctx) : RDX_OK;
 }
 
@@ -937,44 +1004,41 @@ int rdx_splat_sort(rdx_ctx* ctx, const uint32_t* keys, uint64_t count, int bits,
   if (count > rdx::kMaxSegmentKeys) return fail(ctx, RDX_ERR_CAPACITY, "WgpuSplatSorter: %llu keys", (unsigned long long)count);
   if ((!keys && count) || !values || !count_out) return fail(ctx, RDX_ERR_ARG, "a buffer is NULL");
   cudaSetDevice(ctx->device);
-  const uint32_t invalid = bits == 32 ? 0xffffffffu : ((1u << bits) - 1u);
   const bool hk = count && !is_device_ptr(keys), hv = !is_device_ptr(values), hc = !is_device_ptr(count_out),
              ha = draw_args && !is_device_ptr(draw_args);
   const int passes = bits / 8;
   const uint32_t tiles = tiles_of(count);
-  auto layout = [&](Arena& a, const uint32_t** k, uint32_t** v, uint32_t** c, uint32_t** args, uint32_t** kc,
-                    uint32_t** vc, uint32_t** lb, uint64_t** so, uint32_t** st, rdx::SortScratch* sc) {
-    *k = hk ? a.take<uint32_t>(count) : keys;
-    *v = hv ? a.take<uint32_t>(count) : values;
-    *c = hc ? a.take<uint32_t>(1) : count_out;
-    *args = ha ? a.take<uint32_t>(5) : draw_args;
-    *kc = a.take<uint32_t>(count);
-    *vc = a.take<uint32_t>(count);
-    *lb = a.take<uint32_t>(count / 4096 + 2);
-    *so = a.take<uint64_t>(2);
-    *st = a.take<uint32_t>(2);
-    *sc = take_sort_scratch(a, 1, passes, tiles, count);
-  };
   const uint32_t* k;
-  uint32_t *v, *c, *args, *kc, *vc, *lb, *st;
-  uint64_t* so;
+  uint32_t *v, *c, *args;
+  SegBufs sb;
   rdx::SortScratch sc;
+  auto layout = [&](Arena& a) {
+    k = hk ? a.take<uint32_t>(count) : keys;
+    v = hv ? a.take<uint32_t>(count) : values;
+    c = hc ? a.take<uint32_t>(1) : count_out;
+    args = ha ? a.take<uint32_t>(5) : draw_args;
+    sb = take_segs(a, 1);
+    sc = take_sort_scratch(a, 1, passes, count);
+  };
   Arena dry(nullptr);
-  layout(dry, &k, &v, &c, &args, &kc, &vc, &lb, &so, &st, &sc);
+  layout(dry);
   int s = ensure_arena(ctx, dry.used);
   if (s != RDX_OK) return s;
   Arena a(ctx->arena);
-  layout(a, &k, &v, &c, &args, &kc, &vc, &lb, &so, &st, &sc);
+  layout(a);
   if (hk) RDX_CUDA(cudaMemcpyAsync((void*)k, keys, count * 4, cudaMemcpyHostToDevice, ctx->stream), "copy in");
-  // compact -> sortIndirect -> draw args (WgpuSplatSorter.ts:64-71)
+  // WgpuSplatSorter.ts:64-71 compacts the invalid keys away, then sorts: here the
+  // first pass sends them to the tail, so values[0, count) is the same order
   Phase sorting(ctx, RDX_PHASE_SORT);
-  RDX_CUDA(rdx::launch_compact(k, count, invalid, kc, vc, c, lb, ctx->error_flag, ctx->stream), "compact launch");
-  ctx->launches += count ? 1 : 0;
   if (count > 0) {
-    RDX_CUDA(rdx::launch_indirect_segments(c, count, so, st, ctx->stream), "segments");
-    rdx::SortSegments segs{so, st, 1, tiles};
-    RDX_CUDA(rdx::sort_segments(kc, vc, nullptr, v, segs, bits, sc, ctx->error_flag, ctx->stream), "sort launch");
-    ctx->launches += 1 + sort_launches(bits, tiles);
+    s = single_segment(ctx, sb, count);
+    if (s != RDX_OK) return s;
+    s = run_sort(ctx, k, nullptr, nullptr, v, sb, 1, tiles, bits, sc, false);
+    if (s != RDX_OK) return s;
+    RDX_CUDA(rdx::launch_visible(sb.begin, sb.end, nullptr, sc.valid, 1, c, ctx->stream), "count");
+    ctx->launches += 1;
+  } else {
+    RDX_CUDA(cudaMemsetAsync(c, 0, 4, ctx->stream), "count");
   }
   if (args) {
     RDX_CUDA(rdx::launch_draw_args(c, args, ctx->stream), "draw args");
@@ -1015,8 +1079,8 @@ static int project_common(rdx_ctx* ctx, const rdx_object* objects, int n_objects
   int status = RDX_OK;
   ProjectCall call;
   OutPlan plan;
-  uint32_t *keys = nullptr, *ord = nullptr, *vis = nullptr, *st = nullptr;
-  uint64_t* so = nullptr;
+  uint32_t *keys = nullptr, *ord = nullptr, *vis = nullptr;
+  SegBufs sb{};
   rdx::ProjDesc* dev_descs = nullptr;
   rdx::SortScratch sc{};
   auto layout = [&](Arena& a) {
@@ -1040,9 +1104,8 @@ static int project_common(rdx_ctx* ctx, const rdx_object* objects, int n_objects
       keys = d.keys;
       ord = host_order ? a.take<uint32_t>(n) : ordering;
       vis = a.take<uint32_t>(1);
-      so = a.take<uint64_t>(2);
-      st = a.take<uint32_t>(2);
-      sc = take_sort_scratch(a, 1, passes, tiles, n);
+      sb = take_segs(a, 1);
+      sc = take_sort_scratch(a, 1, passes, n);
     }
   };
   Arena dry(nullptr);
@@ -1056,20 +1119,25 @@ static int project_common(rdx_ctx* ctx, const rdx_object* objects, int n_objects
     layout(a);
   }
   if (status != RDX_OK) return status;
+  // A frame's projection counts the digits of its valid keys for the sort
+  rdx::ProjHist hist{nullptr, nullptr, 0};
+  if (sort && n > 0) {
+    RDX_CUDA(cudaMemsetAsync(sc.hist, 0, rdx::sort_small_state_words(1, passes) * 4, ctx->stream), "sort state");
+    s = single_segment(ctx, sb, n);
+    if (s != RDX_OK) return s;
+    hist = rdx::ProjHist{sc.hist, sc.valid, passes};
+  }
   {
     Phase projecting(ctx, RDX_PHASE_PROJECT);
-    s = run_project(ctx, dev_descs, call, plan.dev);
+    s = run_project(ctx, dev_descs, call, plan.dev, hist);
   }
   if (s != RDX_OK) return s;
   if (sort && n > 0) {
-    s = single_segment(ctx, so, st, n);
-    if (s != RDX_OK) return s;
     Phase sorting(ctx, RDX_PHASE_SORT);
-    rdx::SortSegments segs{so, st, 1, tiles};
-    RDX_CUDA(rdx::sort_segments(keys, nullptr, nullptr, ord, segs, sort_bits, sc, ctx->error_flag, ctx->stream),
-             "sort launch");
-    RDX_CUDA(rdx::launch_visible(so, sc.ref_hidden, 1, vis, ctx->stream), "visible");
-    ctx->launches += sort_launches(sort_bits, tiles) + 1;
+    s = run_sort(ctx, keys, nullptr, nullptr, ord, sb, 1, tiles, sort_bits, sc, true);
+    if (s != RDX_OK) return s;
+    RDX_CUDA(rdx::launch_visible(sb.begin, sb.end, nullptr, sc.valid, 1, vis, ctx->stream), "visible");
+    ctx->launches += 1;
   }
   if (sort && visible) {
     if (n == 0) {

@@ -86,6 +86,31 @@ __device__ __forceinline__ float4 decode_quat_oct32(uint32_t code) {
   return make_float4(x * s, y * s, z * s, c);
 }
 
+// QuatOct32 in float64 (the oracle's precision): src/core/encoding.ts:49-67, 101-110
+__device__ __forceinline__ void decode_quat_oct32_f64(uint32_t code, double q[4]) {
+  const uint32_t axis = code & 0xfffffu;
+  double x = 0.0, y = 0.0, z = 0.0;
+  if (axis != 0u) {
+    x = (double)(axis & 1023u) / 1023.0 * 2.0 - 1.0;
+    y = (double)((axis >> 10) & 1023u) / 1023.0 * 2.0 - 1.0;
+    z = 1.0 - fabs(x) - fabs(y);
+    const double t = fmax(-z, 0.0);
+    x += x >= 0.0 ? -t : t;
+    y += y >= 0.0 ? -t : t;
+    const double len = sqrt(x * x + y * y + z * z);
+    x /= len;
+    y /= len;
+    z /= len;
+  }
+  const double angle = (double)((code >> 20) & 4095u) / 4095.0 * 3.14159265358979323846;
+  double s, c;
+  sincos(angle / 2.0, &s, &c);
+  q[0] = x * s;
+  q[1] = y * s;
+  q[2] = z * s;
+  q[3] = c;
+}
+
 // ---- the ewa words (src/render/projection.tsl.ts:277-311) ----
 
 __device__ __forceinline__ uint32_t encode_fixed16(float v) {

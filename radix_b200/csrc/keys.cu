@@ -26,17 +26,19 @@ __global__ void k_keys_f32(const float* __restrict__ d, uint64_t n, int bits, ui
   }
 }
 
-__global__ void k_visible(const uint64_t* seg_off, const uint32_t* ref_hidden, int segments, uint32_t* visible) {
+__global__ void k_visible(const uint64_t* begin, const uint64_t* end, const uint32_t* ref_hidden,
+                          const uint32_t* valid, int segments, uint32_t* visible) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < segments) visible[s] = (uint32_t)(seg_off[s + 1] - seg_off[s]) - ref_hidden[s];
+  if (s < segments) visible[s] = ref_hidden ? (uint32_t)(end[s] - begin[s]) - ref_hidden[s] : valid[s];
 }
 
-__global__ void k_indirect_segments(const uint32_t* count, uint64_t capacity, uint64_t* seg_off, uint32_t* seg_tiles) {
+__global__ void k_indirect_segments(const uint32_t* count, uint64_t capacity, uint64_t* begin, uint64_t* end,
+                                    uint32_t* tiles) {
   const uint64_t c = min((uint64_t)*count, capacity);
-  seg_off[0] = 0;
-  seg_off[1] = c;
-  seg_tiles[0] = 0;
-  seg_tiles[1] = (uint32_t)((c + kSortTile - 1) / kSortTile);
+  begin[0] = 0;
+  end[0] = c;
+  tiles[0] = 0;
+  tiles[1] = (uint32_t)((c + kSortTile - 1) / kSortTile);
 }
 
 __global__ void k_draw_args(const uint32_t* count, uint32_t* args) {
@@ -158,9 +160,9 @@ cudaError_t launch_keys_f32(const float* d, uint64_t n, int bits, uint32_t* keys
   return cudaGetLastError();
 }
 
-cudaError_t launch_visible(const uint64_t* seg_off, const uint32_t* ref_hidden, int segments, uint32_t* visible,
-                           cudaStream_t s) {
-  k_visible<<<(segments + 127) / 128, 128, 0, s>>>(seg_off, ref_hidden, segments, visible);
+cudaError_t launch_visible(const uint64_t* begin, const uint64_t* end, const uint32_t* ref_hidden,
+                           const uint32_t* valid, int segments, uint32_t* visible, cudaStream_t s) {
+  k_visible<<<(segments + 127) / 128, 128, 0, s>>>(begin, end, ref_hidden, valid, segments, visible);
   return cudaGetLastError();
 }
 
@@ -174,9 +176,9 @@ cudaError_t launch_compact(const uint32_t* keys, uint64_t n, uint32_t invalid, u
   return cudaGetLastError();
 }
 
-cudaError_t launch_indirect_segments(const uint32_t* count, uint64_t capacity, uint64_t* seg_off, uint32_t* seg_tiles,
-                                     cudaStream_t s) {
-  k_indirect_segments<<<1, 1, 0, s>>>(count, capacity, seg_off, seg_tiles);
+cudaError_t launch_indirect_segments(const uint32_t* count, uint64_t capacity, uint64_t* begin, uint64_t* end,
+                                     uint32_t* tiles, cudaStream_t s) {
+  k_indirect_segments<<<1, 1, 0, s>>>(count, capacity, begin, end, tiles);
   return cudaGetLastError();
 }
 

@@ -21,53 +21,72 @@ constexpr uint32_t kMaxSegmentKeys = (1u << 30) - 1u;
 // Bounded device waits: polls of a lookback word before the kernel gives up
 constexpr uint32_t kSpinLimit = 1u << 22;
 
-// Segments of one sort, in device memory: seg_off[S + 1] element offsets,
-// seg_tiles[S + 1] the running count of 4096-key tiles. A sort of one array
-// is one segment.
+// Segments of one sort, in device memory: segment s is [begin[s], end[s]);
+// tiles[S + 1] is the running count of 4096-key tiles. A sort of one array is
+// one segment.
 struct SortSegments {
-  const uint64_t* seg_off;
-  const uint32_t* seg_tiles;
+  const uint64_t* begin;
+  const uint64_t* end;
+  const uint32_t* tiles;
   int count;            // S
-  uint32_t max_tiles;   // grid size: at least seg_tiles[S]
+  uint32_t max_tiles;   // grid size: at least tiles[S]
 };
 
-// Device scratch of a sort (all in one context allocation)
+// Device scratch of a sort (carved from a context's arena)
 struct SortScratch {
-  uint32_t* hist;        // [S][passes][256]
+  uint32_t* hist;        // [S][passes][256] digit counts of the valid keys
+  uint32_t* valid;       // [S] keys below 2^bits - 1
   uint32_t* ref_hidden;  // [S] keys the reference's visible count leaves out
   uint32_t* counters;    // [passes] tile counters
-  uint32_t* lookback;    // [passes][max_tiles][256]
+  uint64_t* vbegin;      // [S] segments of the valid keys (passes after the first)
+  uint64_t* vend;        // [S]
+  uint32_t* vtiles;      // [S + 1]
   uint32_t* keys_a;      // [n] ping-pong
   uint32_t* vals_a;
   uint32_t* keys_b;
   uint32_t* vals_b;
 };
 
+// hist, valid, ref_hidden and counters are contiguous: words zeroed before a sort
+size_t sort_small_state_words(int segments, int passes);
+
 // Sort segments of keys_in (values: vals_in, or each key's index within its
 // segment when vals_in is null) into keys_out / vals_out (keys_out may be null:
-// values only). The result is stable and ascending by the low `bits` bits.
-// Everything is enqueued on `stream`; error_flag (device) is set on a timeout.
-cudaError_t sort_segments(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
-                          uint32_t* vals_out, const SortSegments& segs, int bits,
-                          const SortScratch& scratch, uint32_t* error_flag, cudaStream_t stream);
-
-// Bytes of memset-zeroed state at the head of the scratch (hist, ref_hidden, counters)
-size_t sort_small_state_words(int segments, int passes);
+// values only), stable and ascending by the low `bits` bits; the largest key
+// 2^bits - 1 goes to each segment's tail in input order. hist_ready: the
+// small state already holds the histogram and valid counts (a frame's
+// projection wrote them); else it is zeroed and counted here. The lookback
+// words [passes][max_tiles][256] are tagged with `epoch`, new for every call.
+struct SortCall {
+  const uint32_t* keys_in;
+  const uint32_t* vals_in;
+  uint32_t* keys_out;
+  uint32_t* vals_out;
+  SortSegments segs;
+  int bits;
+  bool hist_ready;  // (then the largest keys must be left out of it: outputs may not alias inputs)
+  bool no_drop;     // rank the largest key like the others
+  SortScratch scratch;
+  uint64_t* lookback;
+  uint32_t epoch;
+  uint32_t* error_flag;
+};
+cudaError_t sort_segments(const SortCall& call, cudaStream_t stream, int* launches);
 
 // ---- keys, compaction ----
 
 cudaError_t launch_keys_f64(const double* d, uint64_t n, int bits, uint32_t* keys, cudaStream_t s);
 cudaError_t launch_keys_f32(const float* d, uint64_t n, int bits, uint32_t* keys, cudaStream_t s);
-// visible[s] = seg_len - ref_hidden[s]
-cudaError_t launch_visible(const uint64_t* seg_off, const uint32_t* ref_hidden, int segments,
-                           uint32_t* visible, cudaStream_t s);
+// visible[s] = (end - begin) - ref_hidden[s], or valid[s] (ref_hidden null)
+cudaError_t launch_visible(const uint64_t* begin, const uint64_t* end, const uint32_t* ref_hidden,
+                           const uint32_t* valid, int segments, uint32_t* visible, cudaStream_t s);
 // Order-preserving compaction of keys != invalid; lookback: [tiles] zeroed here
 cudaError_t launch_compact(const uint32_t* keys, uint64_t n, uint32_t invalid, uint32_t* keys_out,
                            uint32_t* vals_out, uint32_t* count_out, uint32_t* lookback,
                            uint32_t* error_flag, cudaStream_t s);
-// seg_off = {0, min(*count, capacity)}, seg_tiles = {0, tiles}
-cudaError_t launch_indirect_segments(const uint32_t* count, uint64_t capacity, uint64_t* seg_off,
-                                     uint32_t* seg_tiles, cudaStream_t s);
+// One segment [0, min(*count, capacity)) and its tiles
+cudaError_t launch_indirect_segments(const uint32_t* count, uint64_t capacity, uint64_t* begin, uint64_t* end,
+                                     uint32_t* tiles, cudaStream_t s);
 cudaError_t launch_draw_args(const uint32_t* count, uint32_t* args, cudaStream_t s);
 
 // ---- projection ----
@@ -122,8 +141,10 @@ struct ProjDesc {
   int sort_bits;
   int cull_keys;
   int keys_only;
-  uint32_t first_tile;   // running count of 256-splat tiles before this object
-  uint32_t reserved2;
+  uint32_t first_tile;   // running count of projection tiles before this object
+  int tma_ok;            // every column 16-byte aligned: tiles staged by TMA bulk copies
+  int segment;           // the sort segment the keys belong to (a view of a batch)
+  int reserved3;
 };
 
 struct ProjOutputs {
@@ -137,10 +158,20 @@ struct ProjOutputs {
   uint32_t* keys;
 };
 
-constexpr int kProjThreads = 256;
+// Splats per projection tile (= threads per block)
+constexpr int kProjTile = 128;
 
-// One launch over every descriptor (a collection): descs in device memory
+// Where a frame's projection accumulates the digit histogram of its valid keys
+// (hist [segments][passes][256]) and their count per segment; hist == null: none
+struct ProjHist {
+  uint32_t* hist;
+  uint32_t* valid;
+  int passes;
+};
+
+// One persistent launch over every descriptor of one table kind (descs in device memory)
 cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host, int n_desc,
-                           uint32_t total_tiles, const ProjOutputs& out, cudaStream_t stream);
+                           uint32_t total_tiles, const ProjOutputs& out, const ProjHist& hist,
+                           uint32_t* error_flag, cudaStream_t stream);
 
 }  // namespace rdx

@@ -1,15 +1,21 @@
-// Stable LSD radix sort of uint32 keys with uint32 values for sm_100a: an
-// upfront histogram kernel (every digit place in one read of the keys), then
-// one onesweep kernel per 8-bit digit place. Each onesweep tile ranks its
-// keys with warp match-based multisplit in shared memory, publishes its digit
-// counts and finds its global offsets by decoupled lookback (single pass, no
-// separate scan kernel), then scatters keys and values through shared memory
-// so that writes of one digit run are contiguous.
+// Stable LSD radix sort of uint32 keys with uint32 values for sm_100a: a
+// histogram of every digit place in one read of the keys (or supplied by the
+// projection that wrote the keys), then one onesweep kernel per 8-bit digit
+// place. Each onesweep tile ranks its keys with warp match-based multisplit in
+// shared memory, publishes its digit counts and finds its global offsets by
+// decoupled lookback (single pass, no separate scan kernel), then scatters
+// keys and values through shared memory so writes of one digit run are
+// contiguous.
+//
+// The largest key of a width (2^bits - 1, the invalid key of SortKeys) sorts
+// after every other key, its copies in input order. The first pass therefore
+// writes them straight to the tail of each segment's output, and the later
+// passes sort only the rest: a frame's culled splats cost one pass, not four.
 //
 // Replaces WgpuRadixSort (src/wgpu/WgpuRadixSort.ts:43-361: 3 dispatches per
-// pass, histogram / scanBlocks / scatter with 8 one-bit splits) and
-// SortKeys.sort (src/core/sort.ts:64-163). Any stable ascending sort yields the
-// order of those two; the digit width here is the reference GPU sort's 8 bits.
+// pass, histogram / scanBlocks / scatter with 8 one-bit splits), WgpuCompact
+// + sortIndirect as the splat sorter uses them, and SortKeys.sort
+// (src/core/sort.ts:64-163). Any stable ascending sort yields their order.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -18,19 +24,21 @@
 namespace rdx {
 namespace {
 
-constexpr uint32_t kFlagAggregate = 1u << 30;
-constexpr uint32_t kFlagInclusive = 2u << 30;
-constexpr uint32_t kFlagMask = 3u << 30;
-constexpr uint32_t kCountMask = (1u << 30) - 1u;
+// Lookback word: epoch (32) | flag (2) | count (30)
+constexpr uint64_t kFlagAggregate = 1ull << 30;
+constexpr uint64_t kFlagInclusive = 2ull << 30;
+constexpr uint64_t kFlagMask = 3ull << 30;
+constexpr uint64_t kCountMask = (1ull << 30) - 1ull;
+constexpr uint32_t kNotRanked = 0xffffu;  // the digit of an item outside the ranking
 
-__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
-  uint32_t v;
-  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+__device__ __forceinline__ uint64_t ld_relaxed64(const uint64_t* p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
   return v;
 }
 
-__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
-  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_relaxed64(uint64_t* p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -43,7 +51,7 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 __device__ __forceinline__ int segment_of(const uint32_t* seg_tiles, int count, uint32_t tile) {
   int lo = 0, hi = count - 1;
   while (lo < hi) {
-    int mid = (lo + hi + 1) >> 1;
+    const int mid = (lo + hi + 1) >> 1;
     if (seg_tiles[mid] <= tile) {
       lo = mid;
     } else {
@@ -54,13 +62,13 @@ __device__ __forceinline__ int segment_of(const uint32_t* seg_tiles, int count, 
 }
 
 // Exclusive scan over the 256 threads of a block (64-bit lanes); `sums` is
-// 8 words of shared memory. Returns the thread's exclusive prefix.
-__device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* sums) {
+// 8 words of shared memory. Returns the thread's exclusive prefix; *total the sum.
+__device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* sums, uint64_t* total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint64_t x = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+    const uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
     if (lane >= o) x += y;
   }
   if (lane == 31) sums[warp] = x;
@@ -69,162 +77,217 @@ __device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* s
     uint64_t s = lane < kSortWarps ? sums[lane] : 0;
 #pragma unroll
     for (int o = 1; o < kSortWarps; o <<= 1) {
-      uint64_t y = __shfl_up_sync(0xffffffffu, s, o);
+      const uint64_t y = __shfl_up_sync(0xffffffffu, s, o);
       if (lane >= o) s += y;
     }
     if (lane < kSortWarps) sums[lane] = s;  // inclusive warp totals
   }
   __syncthreads();
-  uint64_t before = warp > 0 ? sums[warp - 1] : 0;
+  *total = sums[kSortWarps - 1];
+  const uint64_t before = warp > 0 ? sums[warp - 1] : 0;
   return before + x - v;
 }
 
-// ---- upfront histogram: every digit place of every segment, one read ----
+// Warp-aggregated shared-memory histogram increment
+__device__ __forceinline__ void hist_add(uint32_t* h, uint32_t d, bool valid) {
+  uint32_t active = __ballot_sync(0xffffffffu, valid);
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int round = 0; round < 2; round++) {
+    if (!active) break;
+    const int leader = __ffs(active) - 1;
+    const uint32_t dl = __shfl_sync(0xffffffffu, d, leader);
+    const uint32_t m = __ballot_sync(0xffffffffu, valid && d == dl) & active;
+    if (lane == leader) atomicAdd(&h[dl], (uint32_t)__popc(m));
+    active &= ~m;
+  }
+  if (active & (1u << lane)) atomicAdd(&h[d], 1u);
+}
+
+// ---- histogram of every digit place (valid keys), the reference's hidden count ----
 
 template <int PASSES>
-__global__ void __launch_bounds__(kSortThreads) k_sort_hist(
-    const uint32_t* __restrict__ keys, uint32_t key_mask, int ref_shift, uint32_t ref_top,
-    SortSegments segs, int tiles_per_block, uint32_t* __restrict__ hist,
-    uint32_t* __restrict__ ref_hidden, uint32_t* __restrict__ lookback) {
+__global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint32_t* __restrict__ keys, uint32_t key_mask,
+                                                            int ref_shift, uint32_t ref_top, int drop,
+                                                            SortSegments segs, int tiles_per_block,
+                                                            uint32_t* __restrict__ hist,
+                                                            uint32_t* __restrict__ valid_count,
+                                                            uint32_t* __restrict__ ref_hidden) {
   __shared__ uint32_t sh[PASSES][kRadix];
-  __shared__ uint32_t s_hidden;
+  __shared__ uint32_t s_hidden, s_valid;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
-  const uint32_t total_tiles = segs.seg_tiles[segs.count];
+  const uint32_t total_tiles = segs.tiles[segs.count];
   const uint32_t tile0 = blockIdx.x * (uint32_t)tiles_per_block;
   if (tile0 >= total_tiles) return;
   const uint32_t tile_end = min(tile0 + (uint32_t)tiles_per_block, total_tiles);
-
 #pragma unroll
   for (int p = 0; p < PASSES; p++) sh[p][tid] = 0;
-  if (tid == 0) s_hidden = 0;
+  if (tid == 0) s_hidden = s_valid = 0;
   __syncthreads();
 
-  int seg = segment_of(segs.seg_tiles, segs.count, tile0);
-  uint32_t hidden = 0;
+  int seg = segment_of(segs.tiles, segs.count, tile0);
+  uint32_t hidden = 0, nvalid = 0;
   auto flush = [&](int s) {
     __syncthreads();
 #pragma unroll
     for (int p = 0; p < PASSES; p++) {
-      uint32_t c = sh[p][tid];
+      const uint32_t c = sh[p][tid];
       if (c) atomicAdd(&hist[((size_t)s * PASSES + p) * kRadix + tid], c);
       sh[p][tid] = 0;
     }
-    uint32_t h = __reduce_add_sync(0xffffffffu, hidden);
+    const uint32_t h = __reduce_add_sync(0xffffffffu, hidden);
+    const uint32_t v = __reduce_add_sync(0xffffffffu, nvalid);
     if (lane == 0 && h) atomicAdd(&s_hidden, h);
-    hidden = 0;
+    if (lane == 0 && v) atomicAdd(&s_valid, v);
+    hidden = nvalid = 0;
     __syncthreads();
     if (tid == 0) {
       if (s_hidden) atomicAdd(&ref_hidden[s], s_hidden);
-      s_hidden = 0;
+      if (s_valid) atomicAdd(&valid_count[s], s_valid);
+      s_hidden = s_valid = 0;
     }
     __syncthreads();
   };
 
   for (uint32_t tile = tile0; tile < tile_end; tile++) {
-    while (tile >= segs.seg_tiles[seg + 1]) {
+    while (tile >= segs.tiles[seg + 1]) {
       flush(seg);
       seg++;
     }
-    // Zero this tile's lookback words of every pass (read by the onesweep kernels)
-#pragma unroll
-    for (int p = 0; p < PASSES; p++) lookback[((size_t)p * segs.max_tiles + tile) * kRadix + tid] = 0u;
-    const uint64_t seg_begin = segs.seg_off[seg];
-    const uint64_t base = seg_begin + (uint64_t)(tile - segs.seg_tiles[seg]) * kSortTile;
-    const uint32_t n = (uint32_t)min((uint64_t)kSortTile, segs.seg_off[seg + 1] - base);
+    const uint64_t base = segs.begin[seg] + (uint64_t)(tile - segs.tiles[seg]) * kSortTile;
+    const uint32_t n = (uint32_t)min((uint64_t)kSortTile, segs.end[seg] - base);
 #pragma unroll 4
     for (int j = 0; j < kSortItems; j++) {
       const uint32_t pos = (uint32_t)j * kSortThreads + tid;
-      const bool valid = pos < n;
-      const uint32_t active = __ballot_sync(0xffffffffu, valid);
-      if (valid) {
-        const uint32_t k = __ldg(&keys[base + pos]) & key_mask;
-        hidden += (k >> ref_shift) == ref_top;
-        const int leader = __ffs(active) - 1;
+      const bool in = pos < n;
+      const uint32_t k = in ? __ldg(&keys[base + pos]) & key_mask : key_mask;
+      hidden += in && (k >> ref_shift) == ref_top;
+      const bool valid = in && (!drop || k != key_mask);
+      nvalid += valid;
 #pragma unroll
-        for (int p = 0; p < PASSES; p++) {
-          const uint32_t d = (k >> (8 * p)) & 0xffu;
-          const uint32_t first = __shfl_sync(active, d, leader);
-          if (__all_sync(active, d == first)) {
-            if (lane == leader) atomicAdd(&sh[p][d], (uint32_t)__popc(active));
-          } else {
-            atomicAdd(&sh[p][d], 1u);
-          }
-        }
-      }
+      for (int p = 0; p < PASSES; p++) hist_add(sh[p], (k >> (8 * p)) & 0xffu, valid);
     }
   }
   flush(seg);
 }
 
+// Segments of the valid keys after the first pass: [begin, begin + valid)
+__global__ void k_compacted_segments(SortSegments full, const uint32_t* __restrict__ valid_count, uint64_t* begin,
+                                     uint64_t* end, uint32_t* tiles) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint32_t t = 0;
+  for (int s = 0; s < full.count; s++) {
+    const uint64_t b = full.begin[s];
+    const uint64_t v = min((uint64_t)valid_count[s], full.end[s] - b);
+    begin[s] = b;
+    end[s] = b + v;
+    tiles[s] = t;
+    t += (uint32_t)((v + kSortTile - 1) / kSortTile);
+  }
+  tiles[full.count] = t;
+}
+
 // ---- onesweep: one digit place ----
 
+struct PassArgs {
+  const uint32_t* keys_in;
+  const uint32_t* vals_in;   // null in the first pass: each key's index within its segment
+  uint32_t* keys_out;        // null: values only
+  uint32_t* vals_out;
+  uint32_t* tail_keys;       // first pass: where the largest keys go (final outputs; keys may be null)
+  uint32_t* tail_vals;
+  int drop;                  // route the largest key to the tail (outputs do not alias inputs)
+  uint32_t key_mask;
+  int shift;
+  SortSegments segs;         // full segments (first pass) or the valid keys' segments
+  const uint32_t* hist;      // [S][passes][256] of the valid keys
+  const uint32_t* valid_count;
+  int passes;
+  int place;
+  uint64_t* lookback;        // [max_tiles][256] of this pass
+  uint32_t epoch;
+  uint32_t* counter;
+  uint32_t* error_flag;
+};
+
 template <bool FIRST, bool WRITE_KEYS>
-__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(
-    const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-    uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t key_mask, int shift,
-    SortSegments segs, const uint32_t* __restrict__ hist, int passes, int place,
-    uint32_t* __restrict__ lookback, uint32_t* __restrict__ counter, uint32_t* __restrict__ error_flag) {
+__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(PassArgs a) {
   __shared__ uint32_t s_whist[kSortWarps][kRadix];
   __shared__ uint32_t s_exchange[kSortTile];
   __shared__ uint32_t s_tile_start[kRadix];
   __shared__ uint32_t s_dest[kRadix];
   __shared__ uint64_t s_sums[kSortWarps];
+  __shared__ uint32_t s_tail_warp[kSortWarps];
+  __shared__ uint32_t s_valid_before;
   __shared__ uint32_t s_tile;
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
 
-  if (tid == 0) s_tile = atomicAdd(counter, 1u);
+  if (tid == 0) s_tile = atomicAdd(a.counter, 1u);
 #pragma unroll
   for (int w = 0; w < kSortWarps; w++) s_whist[w][tid] = 0;
+  if (tid == 0) s_valid_before = 0;
   __syncthreads();
   const uint32_t tile = s_tile;
-  const uint32_t total_tiles = segs.seg_tiles[segs.count];
-  if (tile >= total_tiles) return;  // an indirect sort sized for its capacity
+  const uint32_t total_tiles = a.segs.tiles[a.segs.count];
+  if (tile >= total_tiles) return;  // grid sized for the capacity
 
-  const int seg = segment_of(segs.seg_tiles, segs.count, tile);
-  const uint32_t local_tile = tile - segs.seg_tiles[seg];
-  const uint64_t seg_begin = segs.seg_off[seg];
+  const int seg = segment_of(a.segs.tiles, a.segs.count, tile);
+  const uint32_t local_tile = tile - a.segs.tiles[seg];
+  const uint64_t seg_begin = a.segs.begin[seg];
+  const uint64_t seg_end = a.segs.end[seg];
   const uint64_t base = seg_begin + (uint64_t)local_tile * kSortTile;
-  const uint32_t n = (uint32_t)min((uint64_t)kSortTile, segs.seg_off[seg + 1] - base);
+  const uint32_t n = (uint32_t)min((uint64_t)kSortTile, seg_end - base);
 
   // Load: warp w holds tile positions [w * 512, (w + 1) * 512), item j at j * 32 + lane
-  uint32_t key[kSortItems], val[kSortItems];
+  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
   const uint32_t warp_base = (uint32_t)warp * (kSortItems * 32);
 #pragma unroll
   for (int j = 0; j < kSortItems; j++) {
     const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
     if (pos < n) {
-      key[j] = __ldg(&keys_in[base + pos]) & key_mask;
-      val[j] = FIRST && vals_in == nullptr ? (uint32_t)(base - seg_begin) + pos : __ldg(&vals_in[base + pos]);
+      key[j] = __ldg(&a.keys_in[base + pos]) & a.key_mask;
+      val[j] = FIRST && a.vals_in == nullptr ? (uint32_t)(base - seg_begin) + pos : __ldg(&a.vals_in[base + pos]);
     } else {
-      key[j] = 0xffffffffu;  // padding: digit 255, after every real key of the tile
-      val[j] = 0;
+      key[j] = 0u;
+      val[j] = 0u;
     }
   }
 
-  // Rank: items in position order, equal digits counted by their lowest lane
-  uint32_t rank[kSortItems];  // rank within the warp's digit, then the local position
+  // Rank the valid keys: items in position order, equal digits counted by
+  // their lowest lane. Largest keys (first pass) are ranked among themselves.
   const uint32_t lt = lanemask_lt();
+  uint32_t tail_count = 0;
 #pragma unroll
   for (int j = 0; j < kSortItems; j++) {
-    const uint32_t d = (key[j] >> shift) & 0xffu;
+    const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+    const bool in = pos < n;
+    const bool tail = FIRST && a.drop && in && key[j] == a.key_mask;
+    const bool ranked = in && !tail;
+    const uint32_t d = ranked ? (key[j] >> a.shift) & 0xffu : kNotRanked;
     const uint32_t peers = __match_any_sync(0xffffffffu, d);
     const int leader = __ffs(peers) - 1;
     uint32_t old = 0;
-    if (lane == leader) {
+    if (lane == leader && d != kNotRanked) {
       old = s_whist[warp][d];
       s_whist[warp][d] = old + (uint32_t)__popc(peers);
     }
     old = __shfl_sync(0xffffffffu, old, leader);
     rank[j] = old + (uint32_t)__popc(peers & lt);
+    if (FIRST) {
+      const uint32_t tb = __ballot_sync(0xffffffffu, tail);
+      if (tail) rank[j] = tail_count + (uint32_t)__popc(tb & lt);
+      tail_count += (uint32_t)__popc(tb);
+    }
     __syncwarp();
   }
+  if (FIRST && lane == 0) s_tail_warp[warp] = tail_count;
   __syncthreads();
 
-  // Thread d owns digit d: warp counts -> exclusive over warps, tile total
+  // Thread d owns digit d: warp counts -> exclusive over warps, the tile's count
   const uint32_t d = (uint32_t)tid;
   uint32_t total = 0;
 #pragma unroll
@@ -233,14 +296,16 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(
     s_whist[w][d] = total;
     total += c;
   }
-  const uint32_t real = total - (d == 0xffu ? (uint32_t)kSortTile - n : 0u);
-  uint32_t* my_word = &lookback[(size_t)tile * kRadix + d];
-  st_relaxed(my_word, (local_tile == 0 ? kFlagInclusive : kFlagAggregate) | real);
+  uint64_t* my_word = &a.lookback[(size_t)tile * kRadix + d];
+  const uint64_t ep = (uint64_t)a.epoch << 32;
+  st_relaxed64(my_word, ep | (local_tile == 0 ? kFlagInclusive : kFlagAggregate) | total);
 
   // Tile-local digit starts (low word) and the segment's digit offsets (high word) in one scan
-  const uint32_t seg_count = hist[((size_t)seg * passes + place) * kRadix + d];
-  const uint64_t both = block_exclusive_scan(((uint64_t)seg_count << 32) | total, s_sums);
+  const uint32_t seg_count = a.hist[((size_t)seg * a.passes + a.place) * kRadix + d];
+  uint64_t both_total;
+  const uint64_t both = block_exclusive_scan(((uint64_t)seg_count << 32) | total, s_sums, &both_total);
   const uint32_t tile_start = (uint32_t)both;
+  const uint32_t tile_valid = (uint32_t)both_total;
   const uint32_t seg_digit = (uint32_t)(both >> 32);
   s_tile_start[d] = tile_start;
 
@@ -250,118 +315,170 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(
     uint32_t t = tile - 1;
     uint32_t spins = 0;
     while (true) {
-      const uint32_t v = ld_relaxed(&lookback[(size_t)t * kRadix + d]);
-      const uint32_t flag = v & kFlagMask;
+      const uint64_t v = ld_relaxed64(&a.lookback[(size_t)t * kRadix + d]);
+      const uint64_t flag = (v >> 32) == a.epoch ? (v & kFlagMask) : 0;
       if (flag == 0) {
         if (++spins > kSpinLimit) {
-          atomicExch(error_flag, 1u);
+          atomicExch(a.error_flag, 1u);
           break;
         }
         if (spins > 32) __nanosleep(32);
         continue;
       }
-      prefix += v & kCountMask;
+      prefix += (uint32_t)(v & kCountMask);
       if (flag == kFlagInclusive) break;
       t--;
     }
-    st_relaxed(my_word, kFlagInclusive | (prefix + real));
+    st_relaxed64(my_word, ep | kFlagInclusive | (prefix + total));
   }
   s_dest[d] = (uint32_t)seg_begin + seg_digit + prefix - tile_start;
+  if (FIRST && prefix) atomicAdd(&s_valid_before, prefix);
   __syncthreads();
 
-  // Local sort of the keys in shared memory
+  // First pass: the largest keys to the tail of the segment, in input order
+  if (FIRST) {
+    const uint32_t seg_valid = min(a.valid_count[seg], (uint32_t)(seg_end - seg_begin));
+    const uint32_t tail_before = local_tile * (uint32_t)kSortTile - s_valid_before;
+    uint32_t warp_before = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; w++) warp_before += w < warp ? s_tail_warp[w] : 0u;
+    const uint64_t tail_base = seg_begin + seg_valid + tail_before + warp_before;
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+      const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+      if (a.drop && pos < n && key[j] == a.key_mask) {
+        const uint64_t dst = tail_base + rank[j];
+        if (dst < seg_end) {
+          a.tail_vals[dst] = val[j];
+          if (a.tail_keys) a.tail_keys[dst] = key[j];
+        }
+      }
+    }
+  }
+
+  // Local sort of the valid keys in shared memory
 #pragma unroll
   for (int j = 0; j < kSortItems; j++) {
-    const uint32_t dj = (key[j] >> shift) & 0xffu;
-    rank[j] += s_tile_start[dj] + s_whist[warp][dj];
-    s_exchange[rank[j]] = key[j];
+    const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+    const bool ranked = pos < n && !(FIRST && a.drop && key[j] == a.key_mask);
+    if (ranked) {
+      const uint32_t dj = (key[j] >> a.shift) & 0xffu;
+      rank[j] += s_tile_start[dj] + s_whist[warp][dj];
+      s_exchange[rank[j]] = key[j];
+    } else {
+      rank[j] = 0xffffffffu;
+    }
   }
   __syncthreads();
   // Destinations stay inside the segment even if a bounded wait gave up
-  const uint32_t seg_end = (uint32_t)segs.seg_off[seg + 1];
   uint32_t dest[kSortItems];
 #pragma unroll
   for (int k = 0; k < kSortItems; k++) {
     const uint32_t i = (uint32_t)k * kSortThreads + tid;
-    const uint32_t kk = s_exchange[i];
-    dest[k] = s_dest[(kk >> shift) & 0xffu] + i;
-    if (i >= n || dest[k] >= seg_end || dest[k] < (uint32_t)seg_begin) dest[k] = 0xffffffffu;
-    if (WRITE_KEYS && dest[k] != 0xffffffffu) keys_out[dest[k]] = kk;
+    dest[k] = 0xffffffffu;
+    if (i < tile_valid) {
+      const uint32_t kk = s_exchange[i];
+      const uint32_t dst = s_dest[(kk >> a.shift) & 0xffu] + i;
+      if (dst >= (uint32_t)seg_begin && dst < (uint32_t)seg_end) {
+        dest[k] = dst;
+        if (WRITE_KEYS) a.keys_out[dst] = kk;
+      }
+    }
   }
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < kSortItems; j++) s_exchange[rank[j]] = val[j];
+  for (int j = 0; j < kSortItems; j++) {
+    if (rank[j] != 0xffffffffu) s_exchange[rank[j]] = val[j];
+  }
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < kSortItems; k++) {
     const uint32_t i = (uint32_t)k * kSortThreads + tid;
-    if (dest[k] != 0xffffffffu) vals_out[dest[k]] = s_exchange[i];
+    if (dest[k] != 0xffffffffu) a.vals_out[dest[k]] = s_exchange[i];
   }
-}
-
-template <bool FIRST, bool WRITE_KEYS>
-void launch_onesweep(const uint32_t* ki, const uint32_t* vi, uint32_t* ko, uint32_t* vo, uint32_t mask,
-                     int place, const SortSegments& segs, const SortScratch& sc, int passes,
-                     uint32_t* error_flag, cudaStream_t stream) {
-  k_onesweep<FIRST, WRITE_KEYS><<<segs.max_tiles, kSortThreads, 0, stream>>>(
-      ki, vi, ko, vo, mask, 8 * place, segs, sc.hist, passes, place,
-      sc.lookback + (size_t)place * segs.max_tiles * kRadix, sc.counters + place, error_flag);
 }
 
 }  // namespace
 
 size_t sort_small_state_words(int segments, int passes) {
-  return (size_t)segments * passes * kRadix + (size_t)segments + (size_t)passes;
+  // hist [S][passes][256], valid [S], ref_hidden [S], counters [passes]
+  return (size_t)segments * passes * kRadix + 2 * (size_t)segments + (size_t)passes;
 }
 
-cudaError_t sort_segments(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
-                          uint32_t* vals_out, const SortSegments& segs, int bits,
-                          const SortScratch& sc, uint32_t* error_flag, cudaStream_t stream) {
-  const int passes = bits / 8;
-  const uint32_t mask = bits == 32 ? 0xffffffffu : ((1u << bits) - 1u);
+cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches) {
+  const int passes = c.bits / 8;
+  const uint32_t mask = c.bits == 32 ? 0xffffffffu : ((1u << c.bits) - 1u);
   // The reference's visible count: keys whose top digit of its own layout is all ones
-  const int ref_shift = bits == 16 ? 0 : (bits == 24 ? 11 : 16);
-  const uint32_t ref_top = bits == 24 ? 0x1fffu : 0xffffu;
-  if (segs.max_tiles == 0) return cudaSuccess;
-
-  // hist, ref_hidden and counters are contiguous
-  cudaError_t err = cudaMemsetAsync(sc.hist, 0, sort_small_state_words(segs.count, passes) * 4, stream);
-  if (err != cudaSuccess) return err;
-  const int target_blocks = 148 * 4;
-  int tpb = (int)((segs.max_tiles + target_blocks - 1) / target_blocks);
-  if (tpb < 1) tpb = 1;
-  const int hist_blocks = (int)((segs.max_tiles + tpb - 1) / tpb);
-  switch (passes) {
-    case 2:
-      k_sort_hist<2><<<hist_blocks, kSortThreads, 0, stream>>>(keys_in, mask, ref_shift, ref_top, segs, tpb,
-                                                              sc.hist, sc.ref_hidden, sc.lookback);
-      break;
-    case 3:
-      k_sort_hist<3><<<hist_blocks, kSortThreads, 0, stream>>>(keys_in, mask, ref_shift, ref_top, segs, tpb,
-                                                              sc.hist, sc.ref_hidden, sc.lookback);
-      break;
-    default:
-      k_sort_hist<4><<<hist_blocks, kSortThreads, 0, stream>>>(keys_in, mask, ref_shift, ref_top, segs, tpb,
-                                                              sc.hist, sc.ref_hidden, sc.lookback);
-      break;
+  const int ref_shift = c.bits == 16 ? 0 : (c.bits == 24 ? 11 : 16);
+  const uint32_t ref_top = c.bits == 24 ? 0x1fffu : 0xffffu;
+  const SortScratch& sc = c.scratch;
+  if (c.segs.max_tiles == 0) return cudaSuccess;
+  // In place (a WgpuRadixSort): the first pass may not write the tail while
+  // other tiles still read there, so the largest key is ranked like any other
+  const int drop = c.keys_out != c.keys_in && c.vals_out != c.vals_in && !c.no_drop ? 1 : 0;
+  int n_launch = 0;
+  if (!c.hist_ready) {
+    cudaError_t err = cudaMemsetAsync(sc.hist, 0, sort_small_state_words(c.segs.count, passes) * 4, stream);
+    if (err != cudaSuccess) return err;
+    const int target_blocks = 148 * 4;
+    int tpb = (int)((c.segs.max_tiles + target_blocks - 1) / target_blocks);
+    if (tpb < 1) tpb = 1;
+    const int hist_blocks = (int)((c.segs.max_tiles + tpb - 1) / tpb);
+    switch (passes) {
+      case 2:
+        k_sort_hist<2><<<hist_blocks, kSortThreads, 0, stream>>>(c.keys_in, mask, ref_shift, ref_top, drop, c.segs, tpb,
+                                                                sc.hist, sc.valid, sc.ref_hidden);
+        break;
+      case 3:
+        k_sort_hist<3><<<hist_blocks, kSortThreads, 0, stream>>>(c.keys_in, mask, ref_shift, ref_top, drop, c.segs, tpb,
+                                                                sc.hist, sc.valid, sc.ref_hidden);
+        break;
+      default:
+        k_sort_hist<4><<<hist_blocks, kSortThreads, 0, stream>>>(c.keys_in, mask, ref_shift, ref_top, drop, c.segs, tpb,
+                                                                sc.hist, sc.valid, sc.ref_hidden);
+        break;
+    }
+    n_launch++;
   }
-  // Ping-pong: pass 0 from the input, the last pass into the output
-  const uint32_t* ki = keys_in;
-  const uint32_t* vi = vals_in;
+  k_compacted_segments<<<1, 1, 0, stream>>>(c.segs, sc.valid, sc.vbegin, sc.vend, sc.vtiles);
+  n_launch++;
+  SortSegments vsegs{sc.vbegin, sc.vend, sc.vtiles, c.segs.count, c.segs.max_tiles};
+
+  PassArgs a{};
+  a.key_mask = mask;
+  a.hist = sc.hist;
+  a.valid_count = sc.valid;
+  a.passes = passes;
+  a.epoch = c.epoch;
+  a.error_flag = c.error_flag;
+  a.tail_keys = c.keys_out;
+  a.tail_vals = c.vals_out;
+  a.drop = drop;
+  const uint32_t* ki = c.keys_in;
+  const uint32_t* vi = c.vals_in;
   for (int place = 0; place < passes; place++) {
     const bool last = place == passes - 1;
-    uint32_t* ko = last ? keys_out : (place % 2 == 0 ? sc.keys_a : sc.keys_b);
-    uint32_t* vo = last ? vals_out : (place % 2 == 0 ? sc.vals_a : sc.vals_b);
+    a.keys_in = ki;
+    a.vals_in = vi;
+    a.keys_out = last ? c.keys_out : (place % 2 == 0 ? sc.keys_a : sc.keys_b);
+    a.vals_out = last ? c.vals_out : (place % 2 == 0 ? sc.vals_a : sc.vals_b);
+    a.shift = 8 * place;
+    a.segs = place == 0 ? c.segs : vsegs;
+    a.place = place;
+    a.lookback = c.lookback + (size_t)place * c.segs.max_tiles * kRadix;
+    a.counter = sc.counters + place;
     if (place == 0) {
-      launch_onesweep<true, true>(ki, vi, ko, vo, mask, place, segs, sc, passes, error_flag, stream);
-    } else if (last && ko == nullptr) {
-      launch_onesweep<false, false>(ki, vi, ko, vo, mask, place, segs, sc, passes, error_flag, stream);
+      k_onesweep<true, true><<<c.segs.max_tiles, kSortThreads, 0, stream>>>(a);
+    } else if (last && a.keys_out == nullptr) {
+      k_onesweep<false, false><<<c.segs.max_tiles, kSortThreads, 0, stream>>>(a);
     } else {
-      launch_onesweep<false, true>(ki, vi, ko, vo, mask, place, segs, sc, passes, error_flag, stream);
+      k_onesweep<false, true><<<c.segs.max_tiles, kSortThreads, 0, stream>>>(a);
     }
-    ki = ko;
-    vi = vo;
+    n_launch++;
+    ki = a.keys_out;
+    vi = a.vals_out;
   }
+  if (launches) *launches += n_launch;
   return cudaGetLastError();
 }
 
