@@ -11,12 +11,14 @@
 // (src/render/projections.tsl.ts:95-148) and SplatProjection.write
 // (src/render/SplatProjection.ts:141-153).
 //
-// Structure: a persistent grid; each block walks its 128-splat tiles. A tile's
-// columns are staged into shared memory by TMA bulk copies
-// (cp.async.bulk + mbarrier), two stages deep, so HBM streams while the
-// previous tile computes. Phase 1 (every splat): the centre in float64, the
-// key distance and the centre culls; splats culled in every eye are finished
-// there. Phase 2 (a compacted list of the rest): SH, covariance and ewa.
+// Structure: a persistent grid of independent warps; no block-wide barrier
+// until the end. A warp walks 32-splat chunks. Phase 1 (a lane per splat):
+// the centre, opacity and scales are read, the centre transformed in float64,
+// the key distance and the centre culls computed; splats culled in every eye
+// are finished there. The others go to a warp-private queue in shared memory
+// (their SH rows and quaternions prefetched into L2). Whenever 32 are queued,
+// phase 2 runs a lane per queued splat: SH, covariance and ewa. Culled splats'
+// SH rows and quaternions are never read, and phase 2's lanes are all busy.
 //
 // Precision: the head-space centre, the key distance and the centre culls are
 // float64 with explicitly rounded operations, so keys and cull decisions equal
@@ -36,116 +38,16 @@
 namespace rdx {
 namespace {
 
-constexpr int kTile = kProjTile;  // splats per tile = threads per block
-constexpr int kStages = 2;
-constexpr uint32_t kWaitLimit = 1u << 24;  // polls of a stage's mbarrier before giving up
+constexpr int kWarps = 4;              // warps per block
+constexpr int kThreads = kWarps * 32;  // 128
+constexpr int kChunk = kProjTile;      // splats per chunk (a warp's phase 1)
+constexpr int kQueue = 64;             // candidate ring of a warp
+static_assert(kChunk == 32, "a chunk is one warp wide");
 
 template <int DEG>
 struct ShCount {
   static constexpr int value = DEG == 0 ? 0 : (DEG == 1 ? 3 : (DEG == 2 ? 8 : (DEG == 3 ? 15 : 24)));
 };
-
-// Byte offsets of the columns of one tile in a shared-memory stage (all 16-aligned)
-template <int LAYOUT, int DEG, int CDT>
-struct Stage {
-  static constexpr int K = ShCount<DEG>::value;
-  static constexpr int kColorRow = (1 + K) * 3 * (CDT == RDX_DTYPE_F16 ? 2 : 4);
-  static constexpr int kCenters = 0;
-  static constexpr int kLogScales = kCenters + kTile * 12;
-  static constexpr int kQuats = kLogScales + kTile * 12;
-  static constexpr int kOpacities = kQuats + kTile * 16;
-  static constexpr int kColors = kOpacities + kTile * 4;
-  static constexpr int kRawBytes = kColors + (kTile * kColorRow + 15) / 16 * 16;
-  static constexpr int kTexels = (K + 3) / 4;
-  static constexpr int kExtA = 0;
-  static constexpr int kExtB = kTile * 16;
-  static constexpr int kExtSh = 2 * kTile * 16;
-  static constexpr int kExtBytes = (2 + kTexels) * kTile * 16;
-  static constexpr int kBytes = ((LAYOUT == RDX_LAYOUT_RAW ? kRawBytes : kExtBytes) + 127) / 128 * 128;
-};
-
-// The column copies of one tile: shared-memory offset, source, bytes
-struct TileCopies {
-  int n;
-  int dst[8];
-  const unsigned char* src[8];
-  uint32_t bytes[8];
-};
-
-template <int LAYOUT, int DEG, int CDT>
-__device__ __forceinline__ void tile_copies(const DevTable& t, uint64_t i0, uint32_t cnt, TileCopies& c) {
-  using S = Stage<LAYOUT, DEG, CDT>;
-  c.n = 0;
-  auto add = [&](int dst, const void* base, uint32_t row) {
-    c.dst[c.n] = dst;
-    c.src[c.n] = reinterpret_cast<const unsigned char*>(base) + i0 * row;
-    c.bytes[c.n] = cnt * row;
-    c.n++;
-  };
-  if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
-    add(S::kCenters, t.centers, 12);
-    add(S::kLogScales, t.log_scales, 12);
-    add(S::kQuats, t.quats, 16);
-    add(S::kOpacities, t.opacities, 4);
-    add(S::kColors, t.colors, S::kColorRow);
-  } else {
-    add(S::kExtA, t.ext_a, 16);
-    add(S::kExtB, t.ext_b, 16);
-#pragma unroll
-    for (int k = 0; k < S::kTexels; k++) add(S::kExtSh + k * kTile * 16, t.ext_sh[k], 16);
-  }
-}
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// Issue the bulk copies of a full, 16-byte aligned tile (one thread)
-__device__ __forceinline__ void issue_tma(uint64_t* bar, unsigned char* stage, const TileCopies& c) {
-  uint32_t total = 0;
-  for (int k = 0; k < c.n; k++) total += c.bytes[k];
-  const uint32_t b = smem_addr(bar);
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(total) : "memory");
-  for (int k = 0; k < c.n; k++) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_addr(stage + c.dst[k])),
-        "l"(c.src[k]), "r"(c.bytes[k]), "r"(b)
-        : "memory");
-  }
-}
-
-// Bounded wait for a stage's phase; false if it gave up
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t b = smem_addr(bar);
-  for (uint32_t i = 0; i < kWaitLimit; i++) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(b), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-// The tile copied by the block's threads: partial tiles, unaligned tables
-__device__ __forceinline__ void manual_copy(unsigned char* stage, const TileCopies& c) {
-  for (int k = 0; k < c.n; k++) {
-    const uint32_t bytes = c.bytes[k];
-    const unsigned char* src = c.src[k];
-    unsigned char* dst = stage + c.dst[k];
-    if ((bytes & 3u) == 0 && ((uintptr_t)src & 3u) == 0) {
-      for (uint32_t w = threadIdx.x; w < bytes / 4; w += kTile)
-        reinterpret_cast<uint32_t*>(dst)[w] = __ldg(reinterpret_cast<const unsigned int*>(src) + w);
-    } else {
-      for (uint32_t w = threadIdx.x; w < bytes / 2; w += kTile)
-        reinterpret_cast<unsigned short*>(dst)[w] = __ldg(reinterpret_cast<const unsigned short*>(src) + w);
-    }
-  }
-}
 
 // The 3DGS basis of band `band` along unit (x, y, z) in float64
 // (src/gpu/sh.tsl.ts:60-102, src/core/sh.ts:376-407), n values into `basis`
@@ -188,26 +90,30 @@ __device__ __forceinline__ int sh_basis_band(int band, double x, double y, doubl
   return 9;
 }
 
-template <int LAYOUT, int DEG, int CDT>
-__device__ __forceinline__ void read_centre(const unsigned char* st, int j, float& x, float& y, float& z, float& opacity,
-                                            float ls[3]) {
-  using S = Stage<LAYOUT, DEG, CDT>;
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// Phase 1's fields of row i: centre, opacity, ln scales
+template <int LAYOUT>
+__device__ __forceinline__ void load_head(const DevTable& t, uint64_t i, float c[3], float& opacity, float ls[3]) {
   if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
-    const float* c = reinterpret_cast<const float*>(st + S::kCenters) + j * 3;
-    const float* l = reinterpret_cast<const float*>(st + S::kLogScales) + j * 3;
-    x = c[0];
-    y = c[1];
-    z = c[2];
-    ls[0] = l[0];
-    ls[1] = l[1];
-    ls[2] = l[2];
-    opacity = reinterpret_cast<const float*>(st + S::kOpacities)[j];
+    const float* cp = t.centers + i * 3;
+    const float* lp = t.log_scales + i * 3;
+    c[0] = __ldg(cp);
+    c[1] = __ldg(cp + 1);
+    c[2] = __ldg(cp + 2);
+    ls[0] = __ldg(lp);
+    ls[1] = __ldg(lp + 1);
+    ls[2] = __ldg(lp + 2);
+    opacity = __ldg(t.opacities + i);
   } else {
-    const uint4 A = reinterpret_cast<const uint4*>(st + S::kExtA)[j];
-    const uint4 B = reinterpret_cast<const uint4*>(st + S::kExtB)[j];
-    x = __uint_as_float(A.x);
-    y = __uint_as_float(A.y);
-    z = __uint_as_float(A.z);
+    // src/core/splats.ts:10-24; src/gpu/splats.tsl.ts:63-71
+    const uint4 A = __ldg(reinterpret_cast<const uint4*>(t.ext_a) + i);
+    const uint4 B = __ldg(reinterpret_cast<const uint4*>(t.ext_b) + i);
+    c[0] = __uint_as_float(A.x);
+    c[1] = __uint_as_float(A.y);
+    c[2] = __uint_as_float(A.z);
     opacity = (float)(A.w >> 24) * (1.0f / 128.0f);
     ls[0] = half_bits_to_float(B.y);
     ls[1] = half_bits_to_float(B.y >> 16);
@@ -215,37 +121,107 @@ __device__ __forceinline__ void read_centre(const unsigned char* st, int j, floa
   }
 }
 
-template <int LAYOUT, int DEG, int CDT>
-__device__ __forceinline__ void read_quat(const unsigned char* st, int j, double q[4]) {
-  using S = Stage<LAYOUT, DEG, CDT>;
+// Phase 1's columns of the chunk starting at row j0 into L2 (a 128-byte line per lane)
+template <int LAYOUT>
+__device__ __forceinline__ void prefetch_head(const DevTable& t, uint64_t j0, uint64_t count, int lane) {
+  const unsigned char* base;
+  uint64_t off, size;
   if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
-    const float4 v = reinterpret_cast<const float4*>(st + S::kQuats)[j];
+    // centres and ln scales: 384 bytes each (3 lines), opacities 128 bytes (1 line)
+    if (lane < 3) {
+      base = reinterpret_cast<const unsigned char*>(t.centers);
+      off = j0 * 12 + (uint64_t)lane * 128;
+      size = count * 12;
+    } else if (lane < 6) {
+      base = reinterpret_cast<const unsigned char*>(t.log_scales);
+      off = j0 * 12 + (uint64_t)(lane - 3) * 128;
+      size = count * 12;
+    } else if (lane < 7) {
+      base = reinterpret_cast<const unsigned char*>(t.opacities);
+      off = j0 * 4;
+      size = count * 4;
+    } else {
+      return;
+    }
+  } else {
+    // ext_a and ext_b: 512 bytes each (4 lines)
+    if (lane >= 8) return;
+    base = reinterpret_cast<const unsigned char*>(lane < 4 ? t.ext_a : t.ext_b);
+    off = j0 * 16 + (uint64_t)(lane & 3) * 128;
+    size = count * 16;
+  }
+  if (off < size) prefetch_l2(base + off);
+}
+
+template <int DEG, int CDT>
+struct ColorRow {
+  static constexpr int kValues = (1 + ShCount<DEG>::value) * 3;
+  static constexpr int kBytes = kValues * (CDT == RDX_DTYPE_F16 ? 2 : 4);
+  static constexpr int kVec = kBytes % 16 == 0 ? 16 : (kBytes % 8 == 0 ? 8 : (kBytes % 4 == 0 ? 4 : 2));
+};
+
+// Phase 2's rows of a queued splat into L2 while the queue fills
+template <int LAYOUT, int DEG, int CDT>
+__device__ __forceinline__ void prefetch_rows(const DevTable& t, uint64_t i) {
+  if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
+    prefetch_l2(t.quats + i * 4);
+    const unsigned char* row = reinterpret_cast<const unsigned char*>(t.colors) + i * ColorRow<DEG, CDT>::kBytes;
+#pragma unroll
+    for (int off = 0; off < ColorRow<DEG, CDT>::kBytes; off += 128) prefetch_l2(row + off);
+    prefetch_l2(row + ColorRow<DEG, CDT>::kBytes - 1);
+  } else {
+#pragma unroll
+    for (int k = 0; k < (ShCount<DEG>::value + 3) / 4; k++) prefetch_l2(t.ext_sh[k] + i * 4);
+  }
+}
+
+template <int LAYOUT>
+__device__ __forceinline__ void load_quat(const DevTable& t, uint64_t i, double q[4]) {
+  if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(t.quats) + i);
     q[0] = v.x;
     q[1] = v.y;
     q[2] = v.z;
     q[3] = v.w;
   } else {
-    decode_quat_oct32_f64(reinterpret_cast<const uint4*>(st + S::kExtB)[j].w, q);
+    decode_quat_oct32_f64(__ldg(reinterpret_cast<const uint4*>(t.ext_b) + i).w, q);
   }
 }
 
-// Base rgb + SH (float64) of splat j, clamped at 0 when the table has SH
+template <int BYTES>
+__device__ __forceinline__ void load_vec(const unsigned char* p, unsigned char* dst) {
+  if constexpr (BYTES == 16) {
+    *reinterpret_cast<uint4*>(dst) = __ldg(reinterpret_cast<const uint4*>(p));
+  } else if constexpr (BYTES == 8) {
+    *reinterpret_cast<uint2*>(dst) = __ldg(reinterpret_cast<const uint2*>(p));
+  } else if constexpr (BYTES == 4) {
+    *reinterpret_cast<uint32_t*>(dst) = __ldg(reinterpret_cast<const unsigned int*>(p));
+  } else {
+    *reinterpret_cast<unsigned short*>(dst) = __ldg(reinterpret_cast<const unsigned short*>(p));
+  }
+}
+
+// Base rgb + SH (float64) of row i seen along (dx, dy, dz), clamped at 0 when
+// the table has SH (GpuShReader.apply); without SH no clamp
 template <int LAYOUT, int DEG, int CDT>
-__device__ __forceinline__ void colour(const unsigned char* st, int j, double dx, double dy, double dz, int cap,
+__device__ __forceinline__ void colour(const DevTable& t, uint64_t i, double dx, double dy, double dz, int cap,
                                        double rgb[3]) {
-  using S = Stage<LAYOUT, DEG, CDT>;
-  constexpr int K = S::K;
+  constexpr int K = ShCount<DEG>::value;
   double acc[3] = {0.0, 0.0, 0.0};
   const double l2 = dx * dx + dy * dy + dz * dz;
   const double inv = l2 > 0.0 ? 1.0 / sqrt(l2) : 0.0;
   const double x = dx * inv, y = dy * inv, z = dz * inv;
   if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
-    const unsigned char* row = st + S::kColors + j * S::kColorRow;
+    using CR = ColorRow<DEG, CDT>;
+    alignas(16) unsigned char buf[(CR::kBytes + 15) / 16 * 16];
+    const unsigned char* row = reinterpret_cast<const unsigned char*>(t.colors) + i * CR::kBytes;
+#pragma unroll
+    for (int b = 0; b < CR::kBytes; b += CR::kVec) load_vec<CR::kVec>(row + b, buf + b);
     auto value = [&](int v) -> double {
       if constexpr (CDT == RDX_DTYPE_F16) {
-        return (double)__half2float(reinterpret_cast<const __half*>(row)[v]);
+        return (double)__half2float(*reinterpret_cast<const __half*>(buf + v * 2));
       } else {
-        return (double)reinterpret_cast<const float*>(row)[v];
+        return (double)*reinterpret_cast<const float*>(buf + v * 4);
       }
     };
     rgb[0] = value(0);
@@ -270,8 +246,17 @@ __device__ __forceinline__ void colour(const unsigned char* st, int j, double dx
       }
     }
   } else {
-    decode_ext_rgb_f64(reinterpret_cast<const uint4*>(st + S::kExtB)[j].x, rgb);
+    decode_ext_rgb_f64(__ldg(reinterpret_cast<const uint4*>(t.ext_b) + i).x, rgb);
     if constexpr (K > 0) {
+      uint32_t words[(K + 3) / 4 * 4];
+#pragma unroll
+      for (int k = 0; k < (K + 3) / 4; k++) {
+        const uint4 T = __ldg(reinterpret_cast<const uint4*>(t.ext_sh[k]) + i);
+        words[k * 4 + 0] = T.x;
+        words[k * 4 + 1] = T.y;
+        words[k * 4 + 2] = T.z;
+        words[k * 4 + 3] = T.w;
+      }
 #pragma unroll
       for (int band = 1; band <= DEG; band++) {
         if (band <= cap) {
@@ -280,10 +265,8 @@ __device__ __forceinline__ void colour(const unsigned char* st, int j, double dx
 #pragma unroll
           for (int k = 0; k < 9; k++) {
             if (k < nb) {
-              const int ci = band * band - 1 + k;
-              const uint32_t* words = reinterpret_cast<const uint32_t*>(st + S::kExtSh + (ci >> 2) * kTile * 16) + j * 4;
               double c[3];
-              decode_ext_rgb_f64(words[ci & 3], c);
+              decode_ext_rgb_f64(words[band * band - 1 + k], c);
               acc[0] = fma(c[0], basis[k], acc[0]);
               acc[1] = fma(c[1], basis[k], acc[1]);
               acc[2] = fma(c[2], basis[k], acc[2]);
@@ -316,273 +299,78 @@ __device__ __forceinline__ void hist_add(uint32_t* h, uint32_t d, bool valid) {
   if (active & (1u << lane)) atomicAdd(&h[d], 1u);
 }
 
-struct PerEye {  // float64 centre culls of one splat in one eye (phase 1 -> 2)
-  double ex, ey, ez, clx, cly, clw;
+// A warp's shared memory: its descriptor, its candidate queue (a ring), its histogram
+template <int EYES>
+struct WarpSmem {
+  ProjDesc desc;
+  uint32_t idx[kQueue];    // row of the object
+  uint32_t key[kQueue];    // the splat's valid key
+  float c[3][kQueue];      // object-space centre
+  uint32_t eye_ok[kQueue]; // eyes whose centre culls passed
+  double e[EYES][6][kQueue];  // per eye: centre ex, ey, ez and clip x, y, w (float64)
+  uint32_t hist[kMaxPasses][kRadix];
+  uint32_t valid;
 };
 
 template <int LAYOUT, int DEG, int CDT, int EYES, bool HIST>
-__global__ void __launch_bounds__(kTile) k_project(const ProjDesc* __restrict__ descs, int n_desc, uint32_t total_tiles,
-                                                   ProjOutputs out, ProjHist hist, uint32_t* __restrict__ error_flag) {
-  using S = Stage<LAYOUT, DEG, CDT>;
-  extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ uint64_t s_bar[kStages];
-  __shared__ int s_manual[kStages];
-  __shared__ ProjDesc sd;
-  __shared__ int s_desc;
-  __shared__ int s_abort;
-  __shared__ uint16_t s_list[kTile];
-  __shared__ int s_warp_count[kTile / 32];
-  __shared__ uint32_t s_key[kTile];
-  __shared__ uint32_t s_keyval[kTile];   // the valid key of a candidate
-  __shared__ double s_centre[3][kTile];  // object-space centre of a candidate
-  __shared__ PerEye s_eye[EYES][kTile];
-  __shared__ uint8_t s_eye_ok[kTile];
-  __shared__ uint32_t s_hist[HIST ? kMaxPasses : 1][kRadix];
-  __shared__ uint32_t s_valid;
+__global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict__ descs, int n_desc, uint32_t total_chunks,
+                                                      ProjOutputs out, ProjHist hist) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  WarpSmem<EYES>& W = reinterpret_cast<WarpSmem<EYES>*>(smem_raw)[warp];
+  const ProjDesc& sd = W.desc;
+  const uint32_t lt = (1u << lane) - 1u;
 
-  const int tid = threadIdx.x;
-  const int lane = tid & 31, warp = tid >> 5;
-  unsigned char* stage[kStages] = {smem, smem + S::kBytes};
-
-  if (tid == 0) {
-    for (int s = 0; s < kStages; s++) {
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_bar[s])) : "memory");
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    s_abort = 0;
-    s_valid = 0;
-  }
   if constexpr (HIST) {
-    for (int w = tid; w < kMaxPasses * kRadix; w += kTile) (&s_hist[0][0])[w] = 0;
+    for (int w = lane; w < kMaxPasses * kRadix; w += 32) (&W.hist[0][0])[w] = 0;
+    if (lane == 0) W.valid = 0;
   }
+  __syncwarp();
 
-  // tile t -> descriptor (objects are contiguous runs of tiles)
-  auto desc_of = [&](uint32_t t) {
-    int lo = 0, hi = n_desc - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (descs[mid].first_tile <= t) {
-        lo = mid;
-      } else {
-        hi = mid - 1;
-      }
-    }
-    return lo;
-  };
-  // fill stage s with tile t (thread 0)
-  auto issue = [&](int s, uint32_t t) {
-    const ProjDesc& D = descs[desc_of(t)];
-    const uint64_t i0 = (uint64_t)(t - D.first_tile) * kTile;
-    const uint32_t cnt = (uint32_t)min((uint64_t)kTile, D.count - i0);
-    TileCopies c;
-    tile_copies<LAYOUT, DEG, CDT>(D.table, i0, cnt, c);
-    const bool tma = cnt == (uint32_t)kTile && D.tma_ok;
-    s_manual[s] = tma ? 0 : 1;
-    if (tma) issue_tma(&s_bar[s], stage[s], c);
-  };
-
-  __syncthreads();
-  const uint32_t stride = gridDim.x;
-  if (tid == 0) {
-    for (int s = 0; s < kStages; s++) {
-      const uint32_t t = blockIdx.x + s * stride;
-      if (t < total_tiles) issue(s, t);
-    }
-  }
-  uint32_t parity[kStages] = {0u, 0u};
   int cur_desc = -1;
-  int hist_seg = -1;
+  int cur_seg = -1;
+  uint32_t head = 0, queued = 0;
 
-  for (uint32_t k = 0;; k++) {
-    const uint32_t t = blockIdx.x + k * stride;
-    if (t >= total_tiles) break;
-    const int s = (int)(k % kStages);
-    if (tid == 0) s_desc = desc_of(t);
-    __syncthreads();
-    if (s_desc != cur_desc) {
-      if constexpr (HIST) {
-        // a new sort segment: flush the block's histogram of the previous one
-        if (hist_seg >= 0 && descs[s_desc].segment != hist_seg) {
-          for (int w = tid; w < hist.passes * kRadix; w += kTile) {
-            const uint32_t c = (&s_hist[0][0])[w];
-            if (c) atomicAdd(&hist.hist[(size_t)hist_seg * hist.passes * kRadix + w], c);
-            (&s_hist[0][0])[w] = 0;
-          }
-          if (tid == 0 && s_valid) {
-            atomicAdd(&hist.valid[hist_seg], s_valid);
-            s_valid = 0;
-          }
+  auto flush_hist = [&]() {
+    if constexpr (HIST) {
+      __syncwarp();
+      if (cur_seg >= 0) {
+        for (int w = lane; w < hist.passes * kRadix; w += 32) {
+          const uint32_t c = (&W.hist[0][0])[w];
+          if (c) atomicAdd(&hist.hist[(size_t)cur_seg * hist.passes * kRadix + w], c);
+          (&W.hist[0][0])[w] = 0;
         }
+        if (lane == 0 && W.valid) atomicAdd(&hist.valid[cur_seg], W.valid);
+        if (lane == 0) W.valid = 0;
       }
-      const uint32_t* src = reinterpret_cast<const uint32_t*>(&descs[s_desc]);
-      uint32_t* dst = reinterpret_cast<uint32_t*>(&sd);
-      for (int w = tid; w < (int)(sizeof(ProjDesc) / 4); w += kTile) dst[w] = src[w];
-      cur_desc = s_desc;
-      __syncthreads();
-      hist_seg = sd.segment;
+      __syncwarp();
     }
-    const uint64_t i0 = (uint64_t)(t - sd.first_tile) * kTile;
-    const int cnt = (int)min((uint64_t)kTile, sd.count - i0);
-    unsigned char* st = stage[s];
-    if (s_manual[s]) {
-      TileCopies c;
-      tile_copies<LAYOUT, DEG, CDT>(sd.table, i0, (uint32_t)cnt, c);
-      manual_copy(st, c);
-      __syncthreads();
-    } else {
-      const bool ok = mbar_wait(&s_bar[s], parity[s]);
-      parity[s] ^= 1u;
-      if (!ok) {
-        atomicExch(error_flag, 2u);
-        s_abort = 1;
-      }
-      __syncthreads();
-      if (s_abort) return;  // every thread: the wait gave up (a TMA never completed)
+  };
+  auto count_key = [&](uint32_t key, bool final_key) {
+    if constexpr (HIST) {
+      const bool valid = final_key && key != invalid_key(sd.sort_bits);
+      for (int pl = 0; pl < hist.passes; pl++) hist_add(W.hist[pl], (key >> (8 * pl)) & 0xffu, valid);
+      const uint32_t nv = (uint32_t)__popc(__ballot_sync(0xffffffffu, valid));
+      if (lane == 0) W.valid += nv;
     }
+  };
+
+  // ---- phase 2: SH, covariance and ewa of nb queued splats (a lane each) ----
+  auto process = [&](uint32_t nb) {
     const DevParams& p = sd.params;
-    const int j = tid;
-    const bool live = j < cnt;
-    const uint64_t gi = sd.out_offset + i0 + (uint64_t)j;
-
-    // ---- phase 1: every splat: centre, distance, centre culls ----
-    bool candidate = false;
-    uint32_t key = invalid_key(sd.sort_bits);
-    if (live) {
-      float cxf, cyf, czf, opac, ls[3];
-      read_centre<LAYOUT, DEG, CDT>(st, j, cxf, cyf, czf, opac, ls);
-      const double cx = cxf, cy = cyf, cz = czf;
-      const double hx = affine_row(sd.a + 0, cx, cy, cz);
-      const double hy = affine_row(sd.a + 4, cx, cy, cz);
-      const double hz = affine_row(sd.a + 8, cx, cy, cz);
-      const double distance = __dsqrt_rn(dadd(dadd(dmul(hx, hx), dmul(hy, hy)), dmul(hz, hz)));
-      // prepareSplat's opacity (projection.tsl.ts:42-64) and cullInvisible (66-69)
-      double op = opac;
-      if (op > 1.0) {
-        op = fmin(op * 4.0 - 3.0, 5.0);
-        if (p.lod_inflate) op = 1.0;
-      }
-      // exp(2 ln s) underflows to 0 below ln s = -372.6: a degenerate (zero) covariance
-      const bool degenerate = sd.degenerate || (ls[0] < -372.6f && ls[1] < -372.6f && ls[2] < -372.6f);
-      const bool invisible = op <= 0.0 || op < (double)p.min_alpha || degenerate;
-      bool guarded = true;
-      if (p.sort_guard > 0.0f && !invisible) {
-        // inSortGuard (projection.tsl.ts:145-155), cov form, float32
-        double q[4];
-        read_quat<LAYOUT, DEG, CDT>(st, j, q);
-        float qx = (float)q[0], qy = (float)q[1], qz = (float)q[2], qw = (float)q[3];
-        const float ql2 = qx * qx + qy * qy + qz * qz + qw * qw;
-        const float qi = ql2 > 0.0f ? rsqrtf(ql2) : 0.0f;
-        qx *= qi;
-        qy *= qi;
-        qz *= qi;
-        qw = ql2 > 0.0f ? qw * qi : 1.0f;
-        const float R[9] = {1.f - 2.f * (qy * qy + qz * qz), 2.f * (qx * qy - qw * qz), 2.f * (qx * qz + qw * qy),
-                            2.f * (qx * qy + qw * qz), 1.f - 2.f * (qx * qx + qz * qz), 2.f * (qy * qz - qw * qx),
-                            2.f * (qx * qz - qw * qy), 2.f * (qy * qz + qw * qx), 1.f - 2.f * (qx * qx + qy * qy)};
-        float inflate = 1.0f;
-        if (opac > 1.0f && p.lod_inflate) {
-          const float o = fminf(opac * 4.0f - 3.0f, 5.0f);
-          inflate = expf((o * o - 1.0f) * (1.0f / (3.0f * 2.718281828459045f)));
-        }
-        const float sx = expf(ls[0]) * inflate, sy = expf(ls[1]) * inflate, sz = expf(ls[2]) * inflate;
-        float ext2 = 0.0f;
-#pragma unroll
-        for (int r = 0; r < 3; r++) {
-          const float a0 = (float)sd.a[r * 4 + 0], a1 = (float)sd.a[r * 4 + 1], a2 = (float)sd.a[r * 4 + 2];
-          const float g0 = (a0 * R[0] + a1 * R[3] + a2 * R[6]) * sx;
-          const float g1 = (a0 * R[1] + a1 * R[4] + a2 * R[7]) * sy;
-          const float g2 = (a0 * R[2] + a1 * R[5] + a2 * R[8]) * sz;
-          ext2 = fmaxf(ext2, g0 * g0 + g1 * g1 + g2 * g2);
-        }
-        const float radius = sqrtf(ext2) * p.max_std_dev;
-        const double* P = sd.eye[0].proj;
-        const float clx = (float)(P[0] * hx + P[4] * hy + P[8] * hz + P[12]);
-        const float cly = (float)(P[1] * hx + P[5] * hy + P[9] * hz + P[13]);
-        const float clw = (float)(P[3] * hx + P[7] * hy + P[11] * hz + P[15]);
-        const float w = fmaxf(clw, 1e-6f);
-        const float rx = (float)P[0] * radius / w, ry = (float)P[5] * radius / w;
-        const bool inside =
-            fabsf(clx / w) - rx <= p.sort_guard + 1.0f && fabsf(cly / w) - ry <= p.sort_guard + 1.0f;
-        const bool near_head = -(float)hz <= radius;
-        guarded = (float)hz < radius && (inside || near_head);
-      }
-      const uint32_t kv = key_of_bits(__float_as_uint(__double2float_rn(distance)), sd.sort_bits);
-      const bool cull_keys = sd.cull_keys && !sd.keys_only;
-      if (!cull_keys && !invisible && guarded) key = kv;
-      uint32_t eye_ok = 0;
-      if (!sd.keys_only && !invisible) {
-#pragma unroll
-        for (int v = 0; v < EYES; v++) {
-          const DevEye& e = sd.eye[v];
-          double ex = hx, ey = hy, ez = hz;
-          if (!e.identity) {
-            ex = affine_row(e.from_head + 0, hx, hy, hz);
-            ey = affine_row(e.from_head + 4, hx, hy, hz);
-            ez = affine_row(e.from_head + 8, hx, hy, hz);
-          }
-          const double* P = e.proj;
-          const double clx = dadd(dadd(dadd(dmul(P[0], ex), dmul(P[4], ey)), dmul(P[8], ez)), P[12]);
-          const double cly = dadd(dadd(dadd(dmul(P[1], ex), dmul(P[5], ey)), dmul(P[9], ez)), P[13]);
-          const double clz = dadd(dadd(dadd(dmul(P[2], ex), dmul(P[6], ey)), dmul(P[10], ez)), P[14]);
-          const double clw = dadd(dadd(dadd(dmul(P[3], ex), dmul(P[7], ey)), dmul(P[11], ez)), P[15]);
-          // cullDepth and cullClipXY (projection.tsl.ts:132-140)
-          const double limit = dmul(fmin((double)p.clip_xy, 2.0), clw);
-          const bool culled = ez >= 0.0 || clz < dmul(sd.ndc_z_min, clw) || clz >= clw || fabs(clx) > limit ||
-                              fabs(cly) > limit;
-          if (!culled) {
-            eye_ok |= 1u << v;
-            s_eye[v][j] = PerEye{ex, ey, ez, clx, cly, clw};
-          }
-        }
-      }
-      candidate = eye_ok != 0;
-      s_eye_ok[j] = (uint8_t)eye_ok;
-      if (candidate) {
-        s_centre[0][j] = cx;
-        s_centre[1][j] = cy;
-        s_centre[2][j] = cz;
-        s_keyval[j] = kv;
-      } else if (!sd.keys_only) {
-        // culled in every eye: zeros, as a zero opacity byte marks a culled eye
-#pragma unroll
-        for (int v = 0; v < EYES; v++) {
-          const uint64_t ei = (uint64_t)v * sd.out_n + gi;
-          if (out.mean2d) reinterpret_cast<float2*>(out.mean2d)[ei] = make_float2(0.f, 0.f);
-          if (out.conic) out.conic[ei * 3 + 0] = out.conic[ei * 3 + 1] = out.conic[ei * 3 + 2] = 0.f;
-          if (out.depth) out.depth[ei] = 0.f;
-          if (out.opacity) out.opacity[ei] = 0.f;
-          if (out.rgb) out.rgb[ei * 3 + 0] = out.rgb[ei * 3 + 1] = out.rgb[ei * 3 + 2] = 0.f;
-          if (out.radii) out.radii[ei * 3 + 0] = out.radii[ei * 3 + 1] = out.radii[ei * 3 + 2] = 0.f;
-          if (out.words) reinterpret_cast<uint4*>(out.words)[gi * EYES + v] = make_uint4(0u, 0u, 0u, 0u);
-        }
-      }
-    }
-    s_key[j] = key;
-    // compact the candidates, in tile order
-    const uint32_t ballot = __ballot_sync(0xffffffffu, candidate);
-    if (lane == 0) s_warp_count[warp] = __popc(ballot);
-    __syncthreads();
-    int before = 0, n_cand = 0;
-#pragma unroll
-    for (int w = 0; w < kTile / 32; w++) {
-      const int c = s_warp_count[w];
-      if (w < warp) before += c;
-      n_cand += c;
-    }
-    if (candidate) s_list[before + __popc(ballot & ((1u << lane) - 1u))] = (uint16_t)j;
-    __syncthreads();
-
-    // ---- phase 2: the candidates: SH, covariance, ewa (float64) ----
-    if (tid < n_cand) {
-      const int c = s_list[tid];
-      const uint64_t gc = sd.out_offset + i0 + (uint64_t)c;
-      float cxf, cyf, czf, opac, ls[3];
-      read_centre<LAYOUT, DEG, CDT>(st, c, cxf, cyf, czf, opac, ls);
+    const bool busy = (uint32_t)lane < nb;
+    const uint32_t q = (head + (uint32_t)lane) & (kQueue - 1);
+    uint32_t key_out = invalid_key(sd.sort_bits);
+    bool any_visible = false;
+    if (busy) {
+      const uint64_t i = W.idx[q];
+      const uint64_t gi = sd.out_offset + i;
+      float cf[3], opac, ls[3];
+      load_head<LAYOUT>(sd.table, i, cf, opac, ls);
       double rgb[3];
-      const int cap = min(p.max_sh_degree, DEG);
-      colour<LAYOUT, DEG, CDT>(st, c, s_centre[0][c] - sd.origin[0], s_centre[1][c] - sd.origin[1],
-                               s_centre[2][c] - sd.origin[2], cap, rgb);
-      // prepareSplat (float64)
+      colour<LAYOUT, DEG, CDT>(sd.table, i, (double)W.c[0][q] - sd.origin[0], (double)W.c[1][q] - sd.origin[1],
+                               (double)W.c[2][q] - sd.origin[2], min(p.max_sh_degree, DEG), rgb);
+      // prepareSplat (projection.tsl.ts:42-64), float64
       double op = opac, inflate2 = 1.0;
       if (op > 1.0) {
         op = fmin(op * 4.0 - 3.0, 5.0);
@@ -595,42 +383,34 @@ __global__ void __launch_bounds__(kTile) k_project(const ProjDesc* __restrict__ 
       const double s2x = exp(2.0 * (double)ls[0]) * inflate2;
       const double s2y = exp(2.0 * (double)ls[1]) * inflate2;
       const double s2z = exp(2.0 * (double)ls[2]) * inflate2;
-      double q[4];
-      read_quat<LAYOUT, DEG, CDT>(st, c, q);
+      double qv[4];
+      load_quat<LAYOUT>(sd.table, i, qv);
       {
-        const double ql2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+        const double ql2 = qv[0] * qv[0] + qv[1] * qv[1] + qv[2] * qv[2] + qv[3] * qv[3];
         if (ql2 > 0.0) {
           const double qi = 1.0 / sqrt(ql2);
-          q[0] *= qi;
-          q[1] *= qi;
-          q[2] *= qi;
-          q[3] *= qi;
+          qv[0] *= qi;
+          qv[1] *= qi;
+          qv[2] *= qi;
+          qv[3] *= qi;
         } else {
-          q[0] = q[1] = q[2] = 0.0;
-          q[3] = 1.0;
+          qv[0] = qv[1] = qv[2] = 0.0;
+          qv[3] = 1.0;
         }
       }
-      const double qx = q[0], qy = q[1], qz = q[2], qw = q[3];
+      const double qx = qv[0], qy = qv[1], qz = qv[2], qw = qv[3];
+      // R(q), row-major (src/gpu/math.tsl.ts:26-44 without the scales)
       const double R[9] = {1.0 - 2.0 * (qy * qy + qz * qz), 2.0 * (qx * qy - qw * qz), 2.0 * (qx * qz + qw * qy),
                            2.0 * (qx * qy + qw * qz), 1.0 - 2.0 * (qx * qx + qz * qz), 2.0 * (qy * qz - qw * qx),
                            2.0 * (qx * qz - qw * qy), 2.0 * (qy * qz + qw * qx), 1.0 - 2.0 * (qx * qx + qy * qy)};
-      const uint32_t eye_ok = s_eye_ok[c];
-      bool any_visible = false;
+      const uint32_t eye_ok = W.eye_ok[q];
 #pragma unroll
       for (int v = 0; v < EYES; v++) {
         const DevEye& e = sd.eye[v];
-        const uint64_t ei = (uint64_t)v * sd.out_n + gc;
+        const uint64_t ei = (uint64_t)v * sd.out_n + gi;
         bool ok = (eye_ok >> v) & 1u;
-        double ex = 0, ey = 0, ez = -1, clx = 0, cly = 0, clw = 1;
-        if (ok) {
-          const PerEye pe = s_eye[v][c];
-          ex = pe.ex;
-          ey = pe.ey;
-          ez = pe.ez;
-          clx = pe.clx;
-          cly = pe.cly;
-          clw = pe.clw;
-        }
+        const double ex = W.e[v][0][q], ey = W.e[v][1][q], ez = W.e[v][2][q];
+        const double clx = W.e[v][3][q], cly = W.e[v][4][q], clw = W.e[v][5][q];
         // depth of field (projection.tsl.ts:117-125)
         float blur = p.blur_amount;
         const float fz = (float)ez;
@@ -656,9 +436,9 @@ __global__ void __launch_bounds__(kTile) k_project(const ProjDesc* __restrict__ 
             j2x = -(j1x * ex) * inv_z;
             j2y = -(j1y * ey) * inv_z;
           }
-          const double* W = e.wd;  // object -> eye 3x3
-          const double w0x = j1x * W[0] + j2x * W[6], w0y = j1x * W[1] + j2x * W[7], w0z = j1x * W[2] + j2x * W[8];
-          const double w1x = j1y * W[3] + j2y * W[6], w1y = j1y * W[4] + j2y * W[7], w1z = j1y * W[5] + j2y * W[8];
+          const double* Wm = e.wd;  // object -> eye 3x3
+          const double w0x = j1x * Wm[0] + j2x * Wm[6], w0y = j1x * Wm[1] + j2x * Wm[7], w0z = j1x * Wm[2] + j2x * Wm[8];
+          const double w1x = j1y * Wm[3] + j2y * Wm[6], w1y = j1y * Wm[4] + j2y * Wm[7], w1z = j1y * Wm[5] + j2y * Wm[8];
           const double u00 = w0x * R[0] + w0y * R[3] + w0z * R[6];
           const double u01 = w0x * R[1] + w0y * R[4] + w0z * R[7];
           const double u02 = w0x * R[2] + w0y * R[5] + w0z * R[8];
@@ -743,7 +523,7 @@ __global__ void __launch_bounds__(kTile) k_project(const ProjDesc* __restrict__ 
             wv.y = encode_depth20(fz) | (encode_angle12(angle) << 20);
             wv.z = encode_ext_rgb((float)rgb[0], (float)rgb[1], (float)rgb[2]);
             wv.w = encode_opacity8(stored) | (encode_log_scale12(scale1) << 8) | (encode_log_scale12(scale2) << 20);
-            reinterpret_cast<uint4*>(out.words)[gc * EYES + v] = wv;
+            reinterpret_cast<uint4*>(out.words)[gi * EYES + v] = wv;
           }
           any_visible = true;
         } else {
@@ -753,41 +533,201 @@ __global__ void __launch_bounds__(kTile) k_project(const ProjDesc* __restrict__ 
           if (out.opacity) out.opacity[ei] = 0.f;
           if (out.rgb) out.rgb[ei * 3 + 0] = out.rgb[ei * 3 + 1] = out.rgb[ei * 3 + 2] = 0.f;
           if (out.radii) out.radii[ei * 3 + 0] = out.radii[ei * 3 + 1] = out.radii[ei * 3 + 2] = 0.f;
-          if (out.words) reinterpret_cast<uint4*>(out.words)[gc * EYES + v] = make_uint4(0u, 0u, 0u, 0u);
+          if (out.words) reinterpret_cast<uint4*>(out.words)[gi * EYES + v] = make_uint4(0u, 0u, 0u, 0u);
         }
       }
-      if (sd.cull_keys && any_visible) s_key[c] = s_keyval[c];
-    }
-    __syncthreads();
-
-    // ---- keys (coalesced) and their digit histogram ----
-    if (live && out.keys) out.keys[gi] = s_key[j];
-    if constexpr (HIST) {
-      const uint32_t kk = s_key[j];
-      const bool valid = live && kk != invalid_key(sd.sort_bits);
-      for (int pl = 0; pl < hist.passes; pl++) hist_add(s_hist[pl], (kk >> (8 * pl)) & 0xffu, valid);
-      const uint32_t nv = (uint32_t)__popc(__ballot_sync(0xffffffffu, valid));
-      if (lane == 0 && nv) atomicAdd(&s_valid, nv);
-    }
-    __syncthreads();  // stage s is free
-    if (tid == 0) {
-      const uint32_t tn = t + kStages * stride;
-      if (tn < total_tiles) issue(s, tn);
-    }
-  }
-  if constexpr (HIST) {
-    __syncthreads();
-    if (hist_seg >= 0) {
-      for (int w = tid; w < hist.passes * kRadix; w += kTile) {
-        const uint32_t c = (&s_hist[0][0])[w];
-        if (c) atomicAdd(&hist.hist[(size_t)hist_seg * hist.passes * kRadix + w], c);
+      // SplatProjection.write (SplatProjection.ts:150-151): culled in every eye -> invalid
+      if (sd.cull_keys) {
+        key_out = any_visible ? W.key[q] : invalid_key(sd.sort_bits);
+        if (out.keys) out.keys[gi] = key_out;
       }
-      if (tid == 0 && s_valid) atomicAdd(&hist.valid[hist_seg], s_valid);
     }
+    if (sd.cull_keys) count_key(key_out, busy);
+    head = (head + nb) & (kQueue - 1);
+    queued -= nb;
+    __syncwarp();
+  };
+
+  const uint32_t gw = blockIdx.x * kWarps + (uint32_t)warp;
+  const uint32_t nw = gridDim.x * kWarps;
+  for (uint32_t chunk = gw; chunk < total_chunks; chunk += nw) {
+    int di = 0;
+    if (lane == 0) {
+      int lo = 0, hi = n_desc - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (descs[mid].first_tile <= chunk) {
+          lo = mid;
+        } else {
+          hi = mid - 1;
+        }
+      }
+      di = lo;
+    }
+    di = __shfl_sync(0xffffffffu, di, 0);
+    if (di != cur_desc) {
+      if (queued) process(queued);  // the queue holds one object's splats
+      const int seg = descs[di].segment;
+      if (seg != cur_seg) {
+        flush_hist();
+        cur_seg = seg;
+      }
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(&descs[di]);
+      uint32_t* dst = reinterpret_cast<uint32_t*>(&W.desc);
+      for (int w = lane; w < (int)(sizeof(ProjDesc) / 4); w += 32) dst[w] = src[w];
+      __syncwarp();
+      cur_desc = di;
+    }
+    const DevParams& p = sd.params;
+    // keys only: culled splats keep their keys (SplatProjection.ts:150-151 applies to a full projection)
+    const bool cull_keys = sd.cull_keys && !sd.keys_only;
+    const uint64_t i0 = (uint64_t)(chunk - sd.first_tile) * kChunk;
+    const uint64_t i = i0 + (uint64_t)lane;
+    const bool live = i < sd.count;
+    const uint64_t gi = sd.out_offset + i;
+    if (i0 + (uint64_t)nw * kChunk < sd.count) prefetch_head<LAYOUT>(sd.table, i0 + (uint64_t)nw * kChunk, sd.count, lane);
+
+    // ---- phase 1: centre, distance, centre culls ----
+    bool candidate = false;
+    uint32_t key = invalid_key(sd.sort_bits), kv = 0, eye_ok = 0;
+    float cf[3] = {0.f, 0.f, 0.f};
+    double pe[EYES][6];
+    if (live) {
+      float opac, ls[3];
+      load_head<LAYOUT>(sd.table, i, cf, opac, ls);
+      const double cx = cf[0], cy = cf[1], cz = cf[2];
+      const double hx = affine_row(sd.a + 0, cx, cy, cz);
+      const double hy = affine_row(sd.a + 4, cx, cy, cz);
+      const double hz = affine_row(sd.a + 8, cx, cy, cz);
+      const double distance = __dsqrt_rn(dadd(dadd(dmul(hx, hx), dmul(hy, hy)), dmul(hz, hz)));
+      // prepareSplat's opacity (projection.tsl.ts:42-64) and cullInvisible (66-69)
+      double op = opac;
+      if (op > 1.0) {
+        op = fmin(op * 4.0 - 3.0, 5.0);
+        if (p.lod_inflate) op = 1.0;
+      }
+      // exp(2 ln s) underflows to 0 below ln s = -372.6: a degenerate (zero) covariance
+      const bool degenerate = sd.degenerate || (ls[0] < -372.6f && ls[1] < -372.6f && ls[2] < -372.6f);
+      const bool invisible = op <= 0.0 || op < (double)p.min_alpha || degenerate;
+      bool guarded = true;
+      if (p.sort_guard > 0.0f && !invisible) {
+        // inSortGuard (projection.tsl.ts:145-155), cov form, float32
+        double qd[4];
+        load_quat<LAYOUT>(sd.table, i, qd);
+        float qx = (float)qd[0], qy = (float)qd[1], qz = (float)qd[2], qw = (float)qd[3];
+        const float ql2 = qx * qx + qy * qy + qz * qz + qw * qw;
+        const float qi = ql2 > 0.0f ? rsqrtf(ql2) : 0.0f;
+        qx *= qi;
+        qy *= qi;
+        qz *= qi;
+        qw = ql2 > 0.0f ? qw * qi : 1.0f;
+        const float R[9] = {1.f - 2.f * (qy * qy + qz * qz), 2.f * (qx * qy - qw * qz), 2.f * (qx * qz + qw * qy),
+                            2.f * (qx * qy + qw * qz), 1.f - 2.f * (qx * qx + qz * qz), 2.f * (qy * qz - qw * qx),
+                            2.f * (qx * qz - qw * qy), 2.f * (qy * qz + qw * qx), 1.f - 2.f * (qx * qx + qy * qy)};
+        float inflate = 1.0f;
+        if (opac > 1.0f && p.lod_inflate) {
+          const float o = fminf(opac * 4.0f - 3.0f, 5.0f);
+          inflate = expf((o * o - 1.0f) * (1.0f / (3.0f * 2.718281828459045f)));
+        }
+        const float sx = expf(ls[0]) * inflate, sy = expf(ls[1]) * inflate, sz = expf(ls[2]) * inflate;
+        float ext2 = 0.0f;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          const float a0 = (float)sd.a[r * 4 + 0], a1 = (float)sd.a[r * 4 + 1], a2 = (float)sd.a[r * 4 + 2];
+          const float g0 = (a0 * R[0] + a1 * R[3] + a2 * R[6]) * sx;
+          const float g1 = (a0 * R[1] + a1 * R[4] + a2 * R[7]) * sy;
+          const float g2 = (a0 * R[2] + a1 * R[5] + a2 * R[8]) * sz;
+          ext2 = fmaxf(ext2, g0 * g0 + g1 * g1 + g2 * g2);
+        }
+        const float radius = sqrtf(ext2) * p.max_std_dev;
+        const double* P = sd.eye[0].proj;
+        const float clx = (float)(P[0] * hx + P[4] * hy + P[8] * hz + P[12]);
+        const float cly = (float)(P[1] * hx + P[5] * hy + P[9] * hz + P[13]);
+        const float clw = (float)(P[3] * hx + P[7] * hy + P[11] * hz + P[15]);
+        const float w = fmaxf(clw, 1e-6f);
+        const float rx = (float)P[0] * radius / w, ry = (float)P[5] * radius / w;
+        const bool inside =
+            fabsf(clx / w) - rx <= p.sort_guard + 1.0f && fabsf(cly / w) - ry <= p.sort_guard + 1.0f;
+        const bool near_head = -(float)hz <= radius;
+        guarded = (float)hz < radius && (inside || near_head);
+      }
+      kv = key_of_bits(__float_as_uint(__double2float_rn(distance)), sd.sort_bits);
+      if (!cull_keys && !invisible && guarded) key = kv;
+      if (!sd.keys_only && !invisible) {
+#pragma unroll
+        for (int v = 0; v < EYES; v++) {
+          const DevEye& e = sd.eye[v];
+          double ex = hx, ey = hy, ez = hz;
+          if (!e.identity) {
+            ex = affine_row(e.from_head + 0, hx, hy, hz);
+            ey = affine_row(e.from_head + 4, hx, hy, hz);
+            ez = affine_row(e.from_head + 8, hx, hy, hz);
+          }
+          const double* P = e.proj;
+          const double clx = dadd(dadd(dadd(dmul(P[0], ex), dmul(P[4], ey)), dmul(P[8], ez)), P[12]);
+          const double cly = dadd(dadd(dadd(dmul(P[1], ex), dmul(P[5], ey)), dmul(P[9], ez)), P[13]);
+          const double clz = dadd(dadd(dadd(dmul(P[2], ex), dmul(P[6], ey)), dmul(P[10], ez)), P[14]);
+          const double clw = dadd(dadd(dadd(dmul(P[3], ex), dmul(P[7], ey)), dmul(P[11], ez)), P[15]);
+          // cullDepth and cullClipXY (projection.tsl.ts:132-140)
+          const double limit = dmul(fmin((double)p.clip_xy, 2.0), clw);
+          const bool culled = ez >= 0.0 || clz < dmul(sd.ndc_z_min, clw) || clz >= clw || fabs(clx) > limit ||
+                              fabs(cly) > limit;
+          if (!culled) eye_ok |= 1u << v;
+          pe[v][0] = ex;
+          pe[v][1] = ey;
+          pe[v][2] = ez;
+          pe[v][3] = clx;
+          pe[v][4] = cly;
+          pe[v][5] = clw;
+        }
+      }
+      candidate = eye_ok != 0;
+      if (candidate) {
+        prefetch_rows<LAYOUT, DEG, CDT>(sd.table, i);
+      } else if (!sd.keys_only) {
+        // culled in every eye: zeros, as a zero opacity byte marks a culled eye
+#pragma unroll
+        for (int v = 0; v < EYES; v++) {
+          const uint64_t ei = (uint64_t)v * sd.out_n + gi;
+          if (out.mean2d) reinterpret_cast<float2*>(out.mean2d)[ei] = make_float2(0.f, 0.f);
+          if (out.conic) out.conic[ei * 3 + 0] = out.conic[ei * 3 + 1] = out.conic[ei * 3 + 2] = 0.f;
+          if (out.depth) out.depth[ei] = 0.f;
+          if (out.opacity) out.opacity[ei] = 0.f;
+          if (out.rgb) out.rgb[ei * 3 + 0] = out.rgb[ei * 3 + 1] = out.rgb[ei * 3 + 2] = 0.f;
+          if (out.radii) out.radii[ei * 3 + 0] = out.radii[ei * 3 + 1] = out.radii[ei * 3 + 2] = 0.f;
+          if (out.words) reinterpret_cast<uint4*>(out.words)[gi * EYES + v] = make_uint4(0u, 0u, 0u, 0u);
+        }
+      }
+    }
+    // keys known now: every key without cullKeys, culled splats' with it
+    const bool key_final = live && (!cull_keys || !candidate);
+    if (key_final && out.keys) out.keys[gi] = key;
+    count_key(key, key_final);
+    // enqueue the candidates, in row order
+    const uint32_t ballot = __ballot_sync(0xffffffffu, candidate);
+    if (candidate) {
+      const uint32_t q = (head + queued + (uint32_t)__popc(ballot & lt)) & (kQueue - 1);
+      W.idx[q] = (uint32_t)i;
+      W.key[q] = kv;
+      W.c[0][q] = cf[0];
+      W.c[1][q] = cf[1];
+      W.c[2][q] = cf[2];
+      W.eye_ok[q] = eye_ok;
+#pragma unroll
+      for (int v = 0; v < EYES; v++) {
+#pragma unroll
+        for (int f = 0; f < 6; f++) W.e[v][f][q] = pe[v][f];
+      }
+    }
+    queued += (uint32_t)__popc(ballot);
+    __syncwarp();
+    if (queued >= 32) process(32);
   }
+  if (queued) process(queued);
+  flush_hist();
 }
 
-using ProjKernel = void (*)(const ProjDesc*, int, uint32_t, ProjOutputs, ProjHist, uint32_t*);
+using ProjKernel = void (*)(const ProjDesc*, int, uint32_t, ProjOutputs, ProjHist);
 
 struct Picked {
   ProjKernel fn;
@@ -796,7 +736,7 @@ struct Picked {
 
 template <int LAYOUT, int DEG, int CDT, int EYES, bool HIST>
 Picked picked() {
-  return {k_project<LAYOUT, DEG, CDT, EYES, HIST>, kStages * Stage<LAYOUT, DEG, CDT>::kBytes};
+  return {k_project<LAYOUT, DEG, CDT, EYES, HIST>, (int)(kWarps * sizeof(WarpSmem<EYES>))};
 }
 
 template <int LAYOUT, int DEG, int CDT>
@@ -824,9 +764,10 @@ Picked pick_kernel(int layout, int degree, int cdt, int eyes, bool hist) {
 
 }  // namespace
 
-cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host, int n_desc, uint32_t total_tiles,
+cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host, int n_desc, uint32_t total_chunks,
                            const ProjOutputs& out, const ProjHist& hist, uint32_t* error_flag, cudaStream_t stream) {
-  if (total_tiles == 0 || n_desc == 0) return cudaSuccess;
+  (void)error_flag;  // no device wait in this kernel
+  if (total_chunks == 0 || n_desc == 0) return cudaSuccess;
   // One kernel per launch: the caller groups objects by table kind
   const ProjDesc& d0 = descs_host[0];
   const Picked k =
@@ -836,11 +777,12 @@ cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host
   int device = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&device);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, kTile, k.smem);
+  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, kThreads, k.smem);
   if (err != cudaSuccess) return err;
   if (per_sm < 1) per_sm = 1;
-  const uint32_t grid = min(total_tiles, (uint32_t)(sms * per_sm));
-  k.fn<<<grid, kTile, k.smem, stream>>>(descs_dev, n_desc, total_tiles, out, hist, error_flag);
+  const uint32_t want = (total_chunks + kWarps - 1) / kWarps;
+  const uint32_t grid = min(want, (uint32_t)(sms * per_sm));
+  k.fn<<<grid, kThreads, k.smem, stream>>>(descs_dev, n_desc, total_chunks, out, hist);
   return cudaGetLastError();
 }
 

@@ -158,8 +158,8 @@ struct ProjOutputs {
   uint32_t* keys;
 };
 
-// Splats per projection tile (= threads per block)
-constexpr int kProjTile = 128;
+// Splats per projection chunk (one warp)
+constexpr int kProjTile = 32;
 
 // Where a frame's projection accumulates the digit histogram of its valid keys
 // (hist [segments][passes][256]) and their count per segment; hist == null: none
