@@ -44,11 +44,11 @@ struct rdx_ctx {
   size_t ring_off = 0;
   cudaEvent_t ring_event = nullptr;
   bool ring_used = false;
-  // Lookback words of the onesweep passes, tagged with a per-call epoch so
-  // they never need clearing; zeroed once when (re)allocated
+  // Lookback words of the onesweep passes, tagged with a per-sort epoch so
+  // they never need clearing; zeroed once when (re)allocated. The epoch is a
+  // device word (error_flag + 1) that each sort advances on the device.
   uint64_t* lookback = nullptr;
   size_t lookback_words = 0;
-  uint32_t epoch = 0;
 };
 
 static const size_t kRingBytes = 4u << 20;
@@ -611,14 +611,13 @@ int run_project(rdx_ctx* ctx, rdx::ProjDesc* dev_descs, const ProjectCall& call,
   return RDX_OK;
 }
 
-// Enqueue one sort (every pass) with a fresh lookback epoch
+// Enqueue one sort (every pass); it takes a fresh lookback epoch on the device
 int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
              const SegBufs& sb, int segments, uint32_t max_tiles, int bits, const rdx::SortScratch& sc,
              bool hist_ready) {
   const int passes = bits / 8;
   int st = ensure_lookback(ctx, (size_t)passes * max_tiles * rdx::kRadix);
   if (st != RDX_OK) return st;
-  if (++ctx->epoch == 0) ctx->epoch = 1;  // 0 marks a cleared word
   rdx::SortCall c{};
   c.keys_in = keys_in;
   c.vals_in = vals_in;
@@ -629,7 +628,7 @@ int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uin
   c.hist_ready = hist_ready;
   c.scratch = sc;
   c.lookback = ctx->lookback;
-  c.epoch = ctx->epoch;
+  c.epoch = ctx->error_flag + 1;
   c.error_flag = ctx->error_flag;
   int launches = 0;
   RDX_CUDA(rdx::sort_segments(c, ctx->stream, &launches), "sort launch");
@@ -678,8 +677,8 @@ int rdx_ctx_create(int device, rdx_ctx** out) {
   rdx_ctx* ctx = new rdx_ctx();
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaMalloc(&ctx->error_flag, 4) != cudaSuccess || cudaMallocHost(&ctx->error_host, 4) != cudaSuccess ||
-      cudaMemset(ctx->error_flag, 0, 4) != cudaSuccess || cudaMallocHost(&ctx->ring, kRingBytes) != cudaSuccess ||
+      cudaMalloc(&ctx->error_flag, 8) != cudaSuccess || cudaMallocHost(&ctx->error_host, 4) != cudaSuccess ||
+      cudaMemset(ctx->error_flag, 0, 8) != cudaSuccess || cudaMallocHost(&ctx->ring, kRingBytes) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ring_event, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
     rdx_ctx_destroy(ctx);

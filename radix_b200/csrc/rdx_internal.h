@@ -56,7 +56,9 @@ size_t sort_small_state_words(int segments, int passes);
 // 2^bits - 1 goes to each segment's tail in input order. hist_ready: the
 // small state already holds the histogram and valid counts (a frame's
 // projection wrote them); else it is zeroed and counted here. The lookback
-// words [passes][max_tiles][256] are tagged with `epoch`, new for every call.
+// words [passes][max_tiles][256] are tagged with the epoch in the device word
+// `epoch`, which the sort advances on the device before its first pass (zero
+// it with the lookback words; it needs no host update between calls).
 struct SortCall {
   const uint32_t* keys_in;
   const uint32_t* vals_in;
@@ -68,7 +70,7 @@ struct SortCall {
   bool no_drop;     // rank the largest key like the others
   SortScratch scratch;
   uint64_t* lookback;
-  uint32_t epoch;
+  uint32_t* epoch;
   uint32_t* error_flag;
 };
 cudaError_t sort_segments(const SortCall& call, cudaStream_t stream, int* launches);

@@ -173,9 +173,13 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint32_t* __re
 }
 
 // Segments of the valid keys after the first pass: [begin, begin + valid)
+// Also advances the lookback epoch: the word is bumped on the device, so a
+// sort replayed from a CUDA graph still tags its words with a new epoch
 __global__ void k_compacted_segments(SortSegments full, const uint32_t* __restrict__ valid_count, uint64_t* begin,
-                                     uint64_t* end, uint32_t* tiles) {
+                                     uint64_t* end, uint32_t* tiles, uint32_t* epoch) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const uint32_t e = *epoch + 1u;
+  *epoch = e == 0u ? 1u : e;  // 0 marks a cleared word
   uint32_t t = 0;
   for (int s = 0; s < full.count; s++) {
     const uint64_t b = full.begin[s];
@@ -206,7 +210,7 @@ struct PassArgs {
   int passes;
   int place;
   uint64_t* lookback;        // [max_tiles][256] of this pass
-  uint32_t epoch;
+  const uint32_t* epoch;     // this sort's lookback epoch (device word)
   uint32_t* counter;
   uint32_t* error_flag;
 };
@@ -297,7 +301,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(PassArgs a) {
     total += c;
   }
   uint64_t* my_word = &a.lookback[(size_t)tile * kRadix + d];
-  const uint64_t ep = (uint64_t)a.epoch << 32;
+  const uint32_t epoch = *a.epoch;
+  const uint64_t ep = (uint64_t)epoch << 32;
   st_relaxed64(my_word, ep | (local_tile == 0 ? kFlagInclusive : kFlagAggregate) | total);
 
   // Tile-local digit starts (low word) and the segment's digit offsets (high word) in one scan
@@ -316,7 +321,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(PassArgs a) {
     uint32_t spins = 0;
     while (true) {
       const uint64_t v = ld_relaxed64(&a.lookback[(size_t)t * kRadix + d]);
-      const uint64_t flag = (v >> 32) == a.epoch ? (v & kFlagMask) : 0;
+      const uint64_t flag = (v >> 32) == epoch ? (v & kFlagMask) : 0;
       if (flag == 0) {
         if (++spins > kSpinLimit) {
           atomicExch(a.error_flag, 1u);
@@ -440,7 +445,7 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     }
     n_launch++;
   }
-  k_compacted_segments<<<1, 1, 0, stream>>>(c.segs, sc.valid, sc.vbegin, sc.vend, sc.vtiles);
+  k_compacted_segments<<<1, 1, 0, stream>>>(c.segs, sc.valid, sc.vbegin, sc.vend, sc.vtiles, c.epoch);
   n_launch++;
   SortSegments vsegs{sc.vbegin, sc.vend, sc.vtiles, c.segs.count, c.segs.max_tiles};
 
