@@ -290,6 +290,26 @@ int rdx_frame(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_
               const rdx_params* params, int sort_bits, const rdx_outputs* out,
               uint32_t* ordering, uint32_t* visible);
 
+/* ---- sorting without allocating ---- */
+
+/*
+ * SortKeys.sort for callers that may not allocate GPU memory: hosts that own
+ * the whole device memory budget, or frame loops where an allocation's device
+ * synchronisation would stall. Same order and visible count as rdx_sort, for
+ * up to 2^20 keys (RDX_ERR_CAPACITY beyond), with scratch in a fixed device
+ * array of the library (about 18 MB on every GPU that loads it, until exit)
+ * instead of allocated memory; it allocates nothing and takes no context.
+ * keys, ordering and visible (may be NULL) must be device memory
+ * (RDX_ERR_ARG otherwise). The work is enqueued on `stream` (NULL: the legacy
+ * default stream); *visible becomes 0xffffffff if a bounded device wait gave
+ * up. The first call on a device looks up the array's device address, so make
+ * it before capturing a stream. All calls share the array: calls that overlap
+ * on the GPU race; issue them one after another.
+ * No counterpart in the reference: its sorts allocate their buffers.
+ */
+int rdx_sort_noalloc(const uint32_t* keys, uint64_t count, int bits, uint32_t* ordering,
+                     uint64_t ordering_len, uint32_t* visible, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -142,6 +142,8 @@ SIGNATURES = {
     "rdx_project": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_object), ctypes.c_int, ctypes.POINTER(rdx_camera),
                                    ctypes.POINTER(rdx_params), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                    ctypes.POINTER(rdx_outputs)]),
+    "rdx_sort_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                                        ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_frame": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_object), ctypes.c_int, ctypes.POINTER(rdx_camera),
                                  ctypes.POINTER(rdx_params), ctypes.c_int, ctypes.POINTER(rdx_outputs), ctypes.c_void_p,
                                  ctypes.c_void_p]),
