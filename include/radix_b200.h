@@ -199,7 +199,8 @@ int rdx_version(void);
 #define RDX_PHASE_SORT 1    /* histogram + onesweep passes (+ compaction) */
 #define RDX_PHASE_COPY_IN 2 /* host -> device staging */
 #define RDX_PHASE_COPY_OUT 3
-#define RDX_PHASES 4
+#define RDX_PHASE_BATCH 4   /* one replay of a batch's CUDA graph */
+#define RDX_PHASES 5
 int rdx_ctx_set_profiling(rdx_ctx* ctx, int on);
 int rdx_ctx_phase_times(rdx_ctx* ctx, double* ms, uint64_t* runs);
 /* Kernels this context has launched since it was created. */
@@ -289,6 +290,51 @@ int rdx_project(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rd
 int rdx_frame(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
               const rdx_params* params, int sort_bits, const rdx_outputs* out,
               uint32_t* ordering, uint32_t* visible);
+
+/* ---- batched frames: many views of many collections ---- */
+
+/* One view of a batch: a collection (objects, as for rdx_frame) and its camera. */
+typedef struct rdx_view {
+  const rdx_object* objects;
+  int n_objects;
+  int reserved;
+  const rdx_camera* camera;
+} rdx_view;
+
+/*
+ * Several frames in one call: each view is the SplatRenderer.update of its own
+ * collection and camera (SplatRenderer.ts:412-456), run as one projection
+ * launch per table kind and one segmented sort with a segment per view. View
+ * v's splats are output rows [first_v, first_v + n_v), first_v = n_0 + ... +
+ * n_{v-1}, n_v its objects' counts summed; eye e of row r is output e * N + r
+ * (N = all rows; every view has the same number of eyes). ordering[first_v + i]
+ * is view v's i-th splat back to front, an index within the view; visible[v]
+ * its drawn count (n_views words). The results equal n_views rdx_frame calls.
+ */
+int rdx_frame_batched(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx_params* params,
+                      int sort_bits, const rdx_outputs* out, uint32_t* ordering, uint32_t* visible);
+
+/*
+ * A batched frame captured once in a CUDA graph and replayed: rdx_batch_create
+ * plans it, allocates its scratch (descriptors, keys, sort state, lookback)
+ * and captures its kernels; every rdx_batch_launch is one cudaGraphLaunch on
+ * the context's stream. Tables, outputs, ordering and visible must be device
+ * memory that stays valid while the batch exists. rdx_batch_update replaces
+ * the cameras, object matrices and parameters (same views, tables and counts)
+ * for the launches enqueued after it, without capturing again.
+ * rdx_batch_synchronize waits for the stream and reports RDX_ERR_TIMEOUT if a
+ * bounded device wait gave up. No counterpart in the reference: it dispatches
+ * every object and view separately (SplatProjector.ts:106-139).
+ */
+typedef struct rdx_batch rdx_batch;
+int rdx_batch_create(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx_params* params,
+                     int sort_bits, const rdx_outputs* out, uint32_t* ordering, uint32_t* visible,
+                     rdx_batch** batch);
+int rdx_batch_update(rdx_batch* batch, const rdx_view* views, int n_views, const rdx_params* params);
+int rdx_batch_launch(rdx_batch* batch);
+int rdx_batch_synchronize(rdx_batch* batch);
+int rdx_batch_launches(const rdx_batch* batch, uint64_t* launches);  /* kernels per launch */
+int rdx_batch_destroy(rdx_batch* batch);
 
 /* ---- sorting without allocating ---- */
 

@@ -25,7 +25,8 @@ from .camera import IDENTITY, Camera, look_at, perspective
 
 __all__ = [
     "Context", "SortKeys", "RadixSort", "Compact", "SplatSorter", "SplatParams", "Table", "SplatObject",
-    "Camera", "look_at", "perspective", "project_collection", "frame", "RadixError", "align_capacity",
+    "Camera", "look_at", "perspective", "project_collection", "frame", "frame_batched", "Batch", "RadixError",
+    "align_capacity",
 ]
 
 ROW_ELEMENTS = 4096  # TextureLayout.ROW_ELEMENTS (src/core/layout.ts:28-30)
@@ -111,7 +112,7 @@ class Context:
         ms = (ctypes.c_double * _abi.RDX_PHASES)()
         runs = (ctypes.c_uint64 * _abi.RDX_PHASES)()
         _abi.check(_abi.lib().rdx_ctx_phase_times(self.handle, ms, runs), self.handle)
-        names = ("project", "sort", "copy_in", "copy_out")
+        names = ("project", "sort", "copy_in", "copy_out", "batch")
         return {names[i]: (ms[i], runs[i]) for i in range(_abi.RDX_PHASES)}
 
     def launches(self):
@@ -450,3 +451,114 @@ def frame(objects, camera, params=None, sort_bits=24, outputs=DEFAULT_OUTPUTS, d
     res["ordering"] = ordering
     res["visible"] = vis_host.value if vis_host is not None else visible
     return res
+
+
+def _c_views(views):
+    """views: [(objects, camera)] -> (rdx_view array, objects kept alive)."""
+    arr = (_abi.rdx_view * len(views))()
+    keep = []
+    for v, (objects, camera) in enumerate(views):
+        objs, k = _c_objects(objects)
+        cam = camera.to_c(_abi)
+        keep += [objs, k, cam]
+        arr[v].objects = ctypes.cast(objs, ctypes.POINTER(_abi.rdx_object))
+        arr[v].n_objects = len(objects)
+        arr[v].camera = ctypes.pointer(cam)
+    return arr, keep
+
+
+def _batch_rows(views):
+    n = sum(o.count for objects, _ in views for o in objects)
+    eyes = len(views[0][1].eyes)
+    return n, eyes
+
+
+def frame_batched(views, params=None, sort_bits=24, outputs=DEFAULT_OUTPUTS, device="cuda", ctx=None,
+                  out=None, ordering=None, visible=None):
+    """Several frames at once: views = [(objects, camera)]. View v's splats
+    are rows first_v .. first_v + n_v - 1 of the outputs (eye e of row r at
+    [e][r]); 'ordering'[first_v + i] is view v's i-th splat back to front (an
+    index within the view) and 'visible'[v] its drawn count. Same results as
+    one `frame` per view, in one projection launch per table kind and one
+    segmented sort."""
+    torch = _torch()
+    params = params or SplatParams()
+    n, eyes = _batch_rows(views)
+    if out is None:
+        out = _alloc_outputs(tuple(outputs), n, eyes, device)
+    if ordering is None:
+        ordering = _alloc_outputs(("keys",), n, 1, device)["keys"]
+    if visible is None:
+        visible = torch.zeros(len(views), dtype=torch.int32, device=device) if device is not None \
+            else np.zeros(len(views), dtype=np.uint32)
+    arr, keep = _c_views(views)
+    prm = params.to_c()
+    c = ctx or default_context(0)
+    c.call("rdx_frame_batched", arr, len(views), ctypes.byref(prm), sort_bits, ctypes.byref(_c_outputs(out)),
+           _ptr(ordering), _ptr(visible))
+    del keep
+    res = dict(out)
+    res["ordering"] = ordering
+    res["visible"] = visible
+    return res
+
+
+class Batch:
+    """A batched frame captured once in a CUDA graph: `launch()` replays it
+    (one cudaGraphLaunch); `update(views)` swaps cameras, object matrices and
+    params for later launches. Everything lives in device memory."""
+
+    def __init__(self, views, params=None, sort_bits=24, outputs=DEFAULT_OUTPUTS, device="cuda", ctx=None):
+        torch = _torch()
+        self.ctx = ctx or default_context(0)
+        self.sort_bits = sort_bits
+        n, eyes = _batch_rows(views)
+        self.out = _alloc_outputs(tuple(outputs), n, eyes, device)
+        self.ordering = torch.empty(n, dtype=torch.int32, device=device)
+        self.visible = torch.zeros(len(views), dtype=torch.int32, device=device)
+        self._views = views
+        arr, keep = _c_views(views)
+        prm = (params or SplatParams()).to_c()
+        h = ctypes.c_void_p()
+        self.ctx.call("rdx_batch_create", arr, len(views), ctypes.byref(prm), sort_bits, ctypes.byref(_c_outputs(self.out)),
+                      _ptr(self.ordering), _ptr(self.visible), ctypes.byref(h))
+        del keep
+        self.handle = h
+
+    def _call(self, name, *args):
+        self.ctx._bind_stream()  # the batch runs on its context's stream
+        _abi.check(getattr(_abi.lib(), name)(self.handle, *args), self.ctx.handle)
+
+    def update(self, views, params=None):
+        arr, keep = _c_views(views)
+        prm = (params or SplatParams()).to_c()
+        self._call("rdx_batch_update", arr, len(views), ctypes.byref(prm))
+        del keep
+
+    def launch(self):
+        self._call("rdx_batch_launch")
+
+    def synchronize(self):
+        self._call("rdx_batch_synchronize")
+
+    def launches(self):
+        n = ctypes.c_uint64(0)
+        self._call("rdx_batch_launches", ctypes.byref(n))
+        return n.value
+
+    def results(self):
+        res = dict(self.out)
+        res["ordering"] = self.ordering
+        res["visible"] = self.visible
+        return res
+
+    def close(self):
+        if self.handle:
+            _abi.lib().rdx_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

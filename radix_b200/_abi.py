@@ -28,7 +28,8 @@ RDX_PHASE_PROJECT = 0
 RDX_PHASE_SORT = 1
 RDX_PHASE_COPY_IN = 2
 RDX_PHASE_COPY_OUT = 3
-RDX_PHASES = 4
+RDX_PHASE_BATCH = 4
+RDX_PHASES = 5
 
 c_u32p = ctypes.POINTER(ctypes.c_uint32)
 c_f32p = ctypes.POINTER(ctypes.c_float)
@@ -102,6 +103,15 @@ class rdx_object(ctypes.Structure):
     ]
 
 
+class rdx_view(ctypes.Structure):
+    _fields_ = [
+        ("objects", ctypes.POINTER(rdx_object)),
+        ("n_objects", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("camera", ctypes.POINTER(rdx_camera)),
+    ]
+
+
 class rdx_outputs(ctypes.Structure):
     _fields_ = [
         ("mean2d", ctypes.c_void_p),
@@ -147,6 +157,16 @@ SIGNATURES = {
     "rdx_frame": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_object), ctypes.c_int, ctypes.POINTER(rdx_camera),
                                  ctypes.POINTER(rdx_params), ctypes.c_int, ctypes.POINTER(rdx_outputs), ctypes.c_void_p,
                                  ctypes.c_void_p]),
+    "rdx_frame_batched": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_view), ctypes.c_int, ctypes.POINTER(rdx_params),
+                                         ctypes.c_int, ctypes.POINTER(rdx_outputs), ctypes.c_void_p, ctypes.c_void_p]),
+    "rdx_batch_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_view), ctypes.c_int, ctypes.POINTER(rdx_params),
+                                        ctypes.c_int, ctypes.POINTER(rdx_outputs), ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.POINTER(ctypes.c_void_p)]),
+    "rdx_batch_update": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_view), ctypes.c_int, ctypes.POINTER(rdx_params)]),
+    "rdx_batch_launch": (ctypes.c_int, [ctypes.c_void_p]),
+    "rdx_batch_synchronize": (ctypes.c_int, [ctypes.c_void_p]),
+    "rdx_batch_launches": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64)]),
+    "rdx_batch_destroy": (ctypes.c_int, [ctypes.c_void_p]),
 }
 
 _lib = None

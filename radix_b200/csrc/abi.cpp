@@ -135,7 +135,7 @@ struct Phase {
   int phase;
   cudaEvent_t start = nullptr;
   Phase(rdx_ctx* c, int p) : ctx(c), phase(p) {
-    if (!ctx->profiling) return;
+    if (!ctx || !ctx->profiling) return;
     start = take_event(ctx);
     if (start) cudaEventRecord(start, ctx->stream);
   }
@@ -540,29 +540,47 @@ struct ProjectCall {
   std::vector<rdx::ProjDesc> descs;
   std::vector<int> groups;  // start of each group of one kernel kind in descs (+ end)
   std::vector<uint32_t> group_tiles;
+  std::vector<uint64_t> seg_begin, seg_end;  // rows of each view (its sort segment)
   uint64_t n = 0;
 };
 
-int plan_project(rdx_ctx* ctx, Arena& a, const rdx_object* objects, int n_objects, const rdx_camera* cam,
-                 const rdx_params* params, int bits, int pass, int cull_keys, ProjectCall& call) {
+// One view of a frame: a collection seen by a camera
+struct ViewRef {
+  const rdx_object* objects;
+  int n_objects;
+  const rdx_camera* camera;
+};
+
+// Descriptors of every (view, object) pair, grouped by kernel kind (one launch
+// per kind). View v's rows follow view v-1's; eye e of row r is output
+// e * n + r; the keys of view v are sort segment v.
+int plan_views(rdx_ctx* ctx, Arena& a, const ViewRef* views, int n_views, const rdx_params* params, int bits, int pass,
+               int cull_keys, ProjectCall& call) {
   int status = RDX_OK;
-  const Camera c = setup_camera(*cam);
   std::map<const rdx_table*, rdx::DevTable> staged;
   uint64_t n = 0;
-  for (int i = 0; i < n_objects; i++) n += objects[i].count;
+  for (int v = 0; v < n_views; v++)
+    for (int i = 0; i < views[v].n_objects; i++) n += views[v].objects[i].count;
   call.n = n;
-  // group by kernel kind, keeping the collection's output offsets
   std::map<int, std::vector<rdx::ProjDesc>> by_kind;
   uint64_t offset = 0;
-  for (int i = 0; i < n_objects; i++) {
-    const rdx_object& o = objects[i];
-    const rdx_table& t = *o.table;
-    if (!staged.count(o.table)) staged[o.table] = stage_table(ctx, a, t, &status);
-    const int kind = t.layout * 100 + t.sh_degree * 10 + (t.layout == RDX_LAYOUT_RAW ? t.color_dtype : 0);
-    if (o.count > 0) {
-      by_kind[kind].push_back(make_desc(*cam, c, o, staged[o.table], *params, offset, n, bits, pass, cull_keys));
+  for (int v = 0; v < n_views; v++) {
+    const ViewRef& vw = views[v];
+    const Camera c = setup_camera(*vw.camera);
+    call.seg_begin.push_back(offset);
+    for (int i = 0; i < vw.n_objects; i++) {
+      const rdx_object& o = vw.objects[i];
+      const rdx_table& t = *o.table;
+      if (!staged.count(o.table)) staged[o.table] = stage_table(ctx, a, t, &status);
+      const int kind = t.layout * 100 + t.sh_degree * 10 + (t.layout == RDX_LAYOUT_RAW ? t.color_dtype : 0);
+      if (o.count > 0) {
+        rdx::ProjDesc d = make_desc(*vw.camera, c, o, staged[o.table], *params, offset, n, bits, pass, cull_keys);
+        d.segment = v;
+        by_kind[kind].push_back(d);
+      }
+      offset += o.count;
     }
-    offset += o.count;
+    call.seg_end.push_back(offset);
   }
   for (auto& kv : by_kind) {
     call.groups.push_back((int)call.descs.size());
@@ -578,6 +596,17 @@ int plan_project(rdx_ctx* ctx, Arena& a, const rdx_object* objects, int n_object
   return status;
 }
 
+// Sort tiles of the views' segments (each segment starts a new tile)
+uint32_t segment_tiles(const ProjectCall& call, std::vector<uint32_t>* prefix) {
+  uint32_t t = 0;
+  for (size_t v = 0; v < call.seg_begin.size(); v++) {
+    if (prefix) prefix->push_back(t);
+    t += tiles_of(call.seg_end[v] - call.seg_begin[v]);
+  }
+  if (prefix) prefix->push_back(t);
+  return t;
+}
+
 int check_objects(rdx_ctx* ctx, const rdx_object* objects, int n_objects) {
   if (n_objects < 0 || (n_objects > 0 && !objects)) return fail(ctx, RDX_ERR_ARG, "objects is NULL");
   uint64_t n = 0;
@@ -590,24 +619,6 @@ int check_objects(rdx_ctx* ctx, const rdx_object* objects, int n_objects) {
     n += objects[i].count;
   }
   if (n > rdx::kMaxSegmentKeys) return fail(ctx, RDX_ERR_CAPACITY, "%llu splats (at most %u)", (unsigned long long)n, rdx::kMaxSegmentKeys);
-  return RDX_OK;
-}
-
-// Enqueue a projection whose plan, descriptor slot and output pointers are ready
-int run_project(rdx_ctx* ctx, rdx::ProjDesc* dev_descs, const ProjectCall& call, const rdx::ProjOutputs& out,
-                const rdx::ProjHist& hist) {
-  if (!call.descs.empty()) {
-    int st = upload(ctx, dev_descs, call.descs.data(), call.descs.size() * sizeof(rdx::ProjDesc));
-    if (st != RDX_OK) return st;
-  }
-  for (size_t g = 0; g + 1 < call.groups.size(); g++) {
-    const int start = call.groups[g];
-    const int count = call.groups[g + 1] - start;
-    RDX_CUDA(rdx::launch_project(dev_descs + start, call.descs.data() + start, count, call.group_tiles[g], out, hist,
-                                 ctx->error_flag, ctx->stream),
-             "projection launch");
-    if (call.group_tiles[g]) ctx->launches += 1;
-  }
   return RDX_OK;
 }
 
@@ -1050,15 +1061,109 @@ int rdx_splat_sort(rdx_ctx* ctx, const uint32_t* keys, uint64_t count, int bits,
   return hk || hv || hc || ha ? finish(ctx) : RDX_OK;
 }
 
-static int project_common(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
-                          const rdx_params* params, int sort_bits, int pass, int cull_keys, const rdx_outputs* out,
-                          uint32_t* ordering, uint32_t* visible, bool sort) {
-  if (!ctx) return RDX_ERR_ARG;
+}  // extern "C"
+
+namespace {
+
+// The device side of a planned frame: every pointer its kernels use
+struct FrameDev {
+  rdx::ProjDesc* descs = nullptr;
+  rdx::ProjOutputs out{};
+  SegBufs sb{};
+  rdx::SortScratch sc{};
+  uint32_t* ord = nullptr;
+  uint32_t* vis = nullptr;         // [views]
+  uint64_t* lookback = nullptr;
+  uint32_t* error_flag = nullptr;  // word 0: the error flag, word 1: the lookback epoch
+};
+
+// Enqueue a planned frame on `stream`: the projection (with the key histogram
+// when sorting), then the segmented sort and the visible counts. It reads and
+// writes no host memory, so the same sequence can be captured in a CUDA graph.
+// `timing` (may be null) gets phase timings.
+cudaError_t enqueue_frame(rdx_ctx* timing, const ProjectCall& call, const FrameDev& fd, int bits, bool sort,
+                          cudaStream_t stream, uint64_t* launches) {
+  const int views = (int)call.seg_begin.size();
+  const int passes = bits / 8;
+  const bool sorting = sort && call.n > 0;
+  cudaError_t e;
+  rdx::ProjHist hist{nullptr, nullptr, 0};
+  if (sorting) {
+    e = cudaMemsetAsync(fd.sc.hist, 0, rdx::sort_small_state_words(views, passes) * 4, stream);
+    if (e != cudaSuccess) return e;
+    hist = rdx::ProjHist{fd.sc.hist, fd.sc.valid, passes};
+  }
+  {
+    Phase projecting(timing, RDX_PHASE_PROJECT);
+    for (size_t g = 0; g + 1 < call.groups.size(); g++) {
+      const int start = call.groups[g];
+      const int count = call.groups[g + 1] - start;
+      e = rdx::launch_project(fd.descs + start, call.descs.data() + start, count, call.group_tiles[g], fd.out, hist,
+                              fd.error_flag, stream);
+      if (e != cudaSuccess) return e;
+      if (call.group_tiles[g]) *launches += 1;
+    }
+  }
+  if (sorting) {
+    Phase sorting_phase(timing, RDX_PHASE_SORT);
+    rdx::SortCall c{};
+    c.keys_in = fd.out.keys;
+    c.vals_out = fd.ord;
+    c.segs = rdx::SortSegments{fd.sb.begin, fd.sb.end, fd.sb.tiles, views, segment_tiles(call, nullptr)};
+    c.bits = bits;
+    c.hist_ready = true;  // the projection counted the digits of the valid keys
+    c.scratch = fd.sc;
+    c.lookback = fd.lookback;
+    c.epoch = fd.error_flag + 1;
+    c.error_flag = fd.error_flag;
+    int n_launch = 0;
+    e = rdx::sort_segments(c, stream, &n_launch);
+    *launches += (uint64_t)n_launch;
+    if (e != cudaSuccess) return e;
+    e = rdx::launch_visible(fd.sb.begin, fd.sb.end, nullptr, fd.sc.valid, views, fd.vis, stream);
+    *launches += 1;
+    if (e != cudaSuccess) return e;
+  } else if (sort && fd.vis) {
+    e = cudaMemsetAsync(fd.vis, 0, (size_t)views * 4, stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// Argument checks shared by the frame entry points; *n = rows of all views
+int check_views(rdx_ctx* ctx, const ViewRef* views, int n_views, int sort_bits, int pass, uint64_t* n) {
   if (!valid_bits(sort_bits)) return fail(ctx, RDX_ERR_ARG, "sortBits must be 16, 24 or 32 (got %d)", sort_bits);
   if (pass != RDX_PASS_FULL && pass != RDX_PASS_KEYS) return fail(ctx, RDX_ERR_ARG, "pass %d", pass);
-  int s = check_camera(ctx, camera);
-  if (s != RDX_OK) return s;
-  s = check_objects(ctx, objects, n_objects);
+  if (n_views < 1 || !views) return fail(ctx, RDX_ERR_ARG, "no views");
+  *n = 0;
+  for (int v = 0; v < n_views; v++) {
+    int s = check_camera(ctx, views[v].camera);
+    if (s != RDX_OK) return s;
+    if (views[v].camera->eyes != views[0].camera->eyes)
+      return fail(ctx, RDX_ERR_ARG, "view %d has %d eyes, view 0 has %d: a batch shares one eye count", v,
+                  views[v].camera->eyes, views[0].camera->eyes);
+    s = check_objects(ctx, views[v].objects, views[v].n_objects);
+    if (s != RDX_OK) return s;
+    for (int i = 0; i < views[v].n_objects; i++) *n += views[v].objects[i].count;
+  }
+  return RDX_OK;
+}
+
+// Segment descriptors of the views' keys, uploaded through the ring
+int upload_segments(rdx_ctx* ctx, const ProjectCall& call, const SegBufs& sb) {
+  std::vector<uint32_t> tiles;
+  segment_tiles(call, &tiles);
+  const size_t v = call.seg_begin.size();
+  int st = upload(ctx, sb.begin, call.seg_begin.data(), v * 8);
+  if (st == RDX_OK) st = upload(ctx, sb.end, call.seg_end.data(), v * 8);
+  return st != RDX_OK ? st : upload(ctx, sb.tiles, tiles.data(), (v + 1) * 4);
+}
+
+int frame_common(rdx_ctx* ctx, const ViewRef* views, int n_views, const rdx_params* params, int sort_bits, int pass,
+                 int cull_keys, const rdx_outputs* out, uint32_t* ordering, uint32_t* visible, bool sort) {
+  if (!ctx) return RDX_ERR_ARG;
+  uint64_t n = 0;
+  int s = check_views(ctx, views, n_views, sort_bits, pass, &n);
   if (s != RDX_OK) return s;
   rdx_params defaults;
   rdx_params_default(&defaults);
@@ -1066,11 +1171,8 @@ static int project_common(rdx_ctx* ctx, const rdx_object* objects, int n_objects
   rdx_outputs none{};
   const rdx_outputs* o = out ? out : &none;
   cudaSetDevice(ctx->device);
-  uint64_t n = 0;
-  for (int i = 0; i < n_objects; i++) n += objects[i].count;
-  const uint64_t E = (uint64_t)camera->eyes;
+  const uint64_t E = (uint64_t)views[0].camera->eyes;
   const int passes = sort_bits / 8;
-  const uint32_t tiles = tiles_of(n);
   if (sort && n > 0 && !ordering) return fail(ctx, RDX_ERR_ARG, "ordering is NULL");
   const bool host_order = sort && ordering && !is_device_ptr(ordering);
   const bool host_visible = sort && visible && !is_device_ptr(visible);
@@ -1078,15 +1180,13 @@ static int project_common(rdx_ctx* ctx, const rdx_object* objects, int n_objects
   int status = RDX_OK;
   ProjectCall call;
   OutPlan plan;
-  uint32_t *keys = nullptr, *ord = nullptr, *vis = nullptr;
-  SegBufs sb{};
-  rdx::ProjDesc* dev_descs = nullptr;
-  rdx::SortScratch sc{};
+  FrameDev fd;
   auto layout = [&](Arena& a) {
     call = ProjectCall();
     plan = OutPlan();
-    status = plan_project(ctx, a, objects, n_objects, camera, prm, sort_bits, pass, cull_keys, call);
-    dev_descs = a.take<rdx::ProjDesc>(call.descs.size());
+    fd = FrameDev();
+    status = plan_views(ctx, a, views, n_views, prm, sort_bits, pass, cull_keys, call);
+    fd.descs = a.take<rdx::ProjDesc>(call.descs.size());
     rdx::ProjOutputs& d = plan.dev;
     if (pass == RDX_PASS_FULL) {
       d.mean2d = stage_out(ctx, a, o->mean2d, E * n * 8, 8, plan, &status);
@@ -1100,12 +1200,12 @@ static int project_common(rdx_ctx* ctx, const rdx_object* objects, int n_objects
     d.keys = stage_out(ctx, a, o->keys, n * 4, 4, plan, &status);
     if (sort) {
       if (!d.keys) d.keys = a.take<uint32_t>(n);
-      keys = d.keys;
-      ord = host_order ? a.take<uint32_t>(n) : ordering;
-      vis = a.take<uint32_t>(1);
-      sb = take_segs(a, 1);
-      sc = take_sort_scratch(a, 1, passes, n);
+      fd.ord = host_order ? a.take<uint32_t>(n) : ordering;
+      fd.vis = a.take<uint32_t>((size_t)n_views);
+      fd.sb = take_segs(a, n_views);
+      fd.sc = take_sort_scratch(a, n_views, passes, n);
     }
+    fd.out = d;
   };
   Arena dry(nullptr);
   layout(dry);
@@ -1118,55 +1218,295 @@ static int project_common(rdx_ctx* ctx, const rdx_object* objects, int n_objects
     layout(a);
   }
   if (status != RDX_OK) return status;
-  // A frame's projection counts the digits of its valid keys for the sort
-  rdx::ProjHist hist{nullptr, nullptr, 0};
   if (sort && n > 0) {
-    RDX_CUDA(cudaMemsetAsync(sc.hist, 0, rdx::sort_small_state_words(1, passes) * 4, ctx->stream), "sort state");
-    s = single_segment(ctx, sb, n);
+    s = ensure_lookback(ctx, (size_t)passes * segment_tiles(call, nullptr) * rdx::kRadix);
     if (s != RDX_OK) return s;
-    hist = rdx::ProjHist{sc.hist, sc.valid, passes};
-  }
-  {
-    Phase projecting(ctx, RDX_PHASE_PROJECT);
-    s = run_project(ctx, dev_descs, call, plan.dev, hist);
-  }
-  if (s != RDX_OK) return s;
-  if (sort && n > 0) {
-    Phase sorting(ctx, RDX_PHASE_SORT);
-    s = run_sort(ctx, keys, nullptr, nullptr, ord, sb, 1, tiles, sort_bits, sc, true);
+    s = upload_segments(ctx, call, fd.sb);
     if (s != RDX_OK) return s;
-    RDX_CUDA(rdx::launch_visible(sb.begin, sb.end, nullptr, sc.valid, 1, vis, ctx->stream), "visible");
-    ctx->launches += 1;
   }
+  if (!call.descs.empty()) {
+    s = upload(ctx, fd.descs, call.descs.data(), call.descs.size() * sizeof(rdx::ProjDesc));
+    if (s != RDX_OK) return s;
+  }
+  fd.lookback = ctx->lookback;
+  fd.error_flag = ctx->error_flag;
+  RDX_CUDA(enqueue_frame(ctx, call, fd, sort_bits, sort, ctx->stream, &ctx->launches), "frame launch");
   if (sort && visible) {
-    if (n == 0) {
-      RDX_CUDA(cudaMemsetAsync(vis, 0, 4, ctx->stream), "visible");
-    }
-    RDX_CUDA(cudaMemcpyAsync(visible, vis, 4, host_visible ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream),
+    RDX_CUDA(cudaMemcpyAsync(visible, fd.vis, (size_t)n_views * 4,
+                             host_visible ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream),
              "visible copy");
   }
   Phase copying_out(ctx, RDX_PHASE_COPY_OUT);
   s = copy_back(ctx, plan);
   if (s != RDX_OK) return s;
-  if (host_order && n) RDX_CUDA(cudaMemcpyAsync(ordering, ord, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
+  if (host_order && n) RDX_CUDA(cudaMemcpyAsync(ordering, fd.ord, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
   copying_out.end();
   bool host_in = false;
-  for (int i = 0; i < n_objects && !host_in; i++) {
-    const rdx_table& t = *objects[i].table;
-    host_in = t.layout == RDX_LAYOUT_RAW ? any_host({t.centers, t.log_scales, t.quats, t.opacities, t.colors})
-                                         : any_host({t.ext_a, t.ext_b});
+  for (int v = 0; v < n_views && !host_in; v++) {
+    for (int i = 0; i < views[v].n_objects && !host_in; i++) {
+      const rdx_table& t = *views[v].objects[i].table;
+      host_in = t.layout == RDX_LAYOUT_RAW ? any_host({t.centers, t.log_scales, t.quats, t.opacities, t.colors})
+                                           : any_host({t.ext_a, t.ext_b});
+    }
   }
   return host_in || !plan.back.empty() || host_order || host_visible ? finish(ctx) : RDX_OK;
 }
 
+}  // namespace
+
+// A batched frame captured once in a CUDA graph (device memory only)
+struct rdx_batch {
+  rdx_ctx* ctx = nullptr;
+  int bits = 32;
+  int eyes = 1;
+  std::vector<int> view_objects;             // objects of each view
+  std::vector<const rdx_table*> tables;      // of each (view, object)
+  std::vector<uint64_t> counts;
+  ProjectCall call;
+  FrameDev fd;
+  char* arena = nullptr;                     // descriptors, segments, sort scratch, keys
+  uint64_t* lookback = nullptr;
+  uint32_t* words = nullptr;                 // error flag, lookback epoch
+  uint32_t* error_host = nullptr;
+  rdx::ProjDesc* staging = nullptr;          // pinned copy of the descriptors for updates
+  cudaEvent_t staged = nullptr;              // the last update's copy is done
+  bool staged_used = false;
+  cudaStream_t capture = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t graph_launches = 0;               // kernels in the graph
+};
+
+namespace {
+
+void free_batch(rdx_batch* b) {
+  if (!b) return;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  if (b->capture) cudaStreamDestroy(b->capture);
+  if (b->staged) cudaEventDestroy(b->staged);
+  if (b->staging) cudaFreeHost(b->staging);
+  if (b->error_host) cudaFreeHost(b->error_host);
+  if (b->words) cudaFree(b->words);
+  if (b->lookback) cudaFree(b->lookback);
+  if (b->arena) cudaFree(b->arena);
+  delete b;
+}
+
+bool all_device(const rdx_table& t) {
+  if (t.layout == RDX_LAYOUT_RAW) {
+    for (const void* p : {(const void*)t.centers, (const void*)t.log_scales, (const void*)t.quats,
+                          (const void*)t.opacities, t.colors})
+      if (!is_device_ptr(p)) return false;
+    return true;
+  }
+  if (!is_device_ptr(t.ext_a) || !is_device_ptr(t.ext_b)) return false;
+  for (int c = 0; c < (kShCoeffs[t.sh_degree] + 3) / 4; c++)
+    if (!is_device_ptr(t.ext_sh[c])) return false;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
 int rdx_project(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
                 const rdx_params* params, int sort_bits, int pass, int cull_keys, const rdx_outputs* out) {
-  return project_common(ctx, objects, n_objects, camera, params, sort_bits, pass, cull_keys, out, nullptr, nullptr, false);
+  const ViewRef view{objects, n_objects, camera};
+  return frame_common(ctx, &view, 1, params, sort_bits, pass, cull_keys, out, nullptr, nullptr, false);
 }
 
 int rdx_frame(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera, const rdx_params* params,
               int sort_bits, const rdx_outputs* out, uint32_t* ordering, uint32_t* visible) {
-  return project_common(ctx, objects, n_objects, camera, params, sort_bits, RDX_PASS_FULL, 1, out, ordering, visible, true);
+  const ViewRef view{objects, n_objects, camera};
+  return frame_common(ctx, &view, 1, params, sort_bits, RDX_PASS_FULL, 1, out, ordering, visible, true);
+}
+
+int rdx_frame_batched(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx_params* params, int sort_bits,
+                      const rdx_outputs* out, uint32_t* ordering, uint32_t* visible) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (n_views < 1 || !views) return fail(ctx, RDX_ERR_ARG, "no views");
+  std::vector<ViewRef> refs;
+  for (int v = 0; v < n_views; v++) refs.push_back({views[v].objects, views[v].n_objects, views[v].camera});
+  return frame_common(ctx, refs.data(), n_views, params, sort_bits, RDX_PASS_FULL, 1, out, ordering, visible, true);
+}
+
+int rdx_batch_create(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx_params* params, int sort_bits,
+                     const rdx_outputs* out, uint32_t* ordering, uint32_t* visible, rdx_batch** batch) {
+  if (!ctx || !batch) return RDX_ERR_ARG;
+  *batch = nullptr;
+  if (n_views < 1 || !views) return fail(ctx, RDX_ERR_ARG, "no views");
+  std::vector<ViewRef> refs;
+  for (int v = 0; v < n_views; v++) refs.push_back({views[v].objects, views[v].n_objects, views[v].camera});
+  uint64_t n = 0;
+  int s = check_views(ctx, refs.data(), n_views, sort_bits, RDX_PASS_FULL, &n);
+  if (s != RDX_OK) return s;
+  if (n == 0) return fail(ctx, RDX_ERR_ARG, "a batch draws no splats");
+  cudaSetDevice(ctx->device);
+  rdx_outputs none{};
+  const rdx_outputs* o = out ? out : &none;
+  for (const void* p : {(const void*)o->mean2d, (const void*)o->conic, (const void*)o->depth, (const void*)o->opacity,
+                        (const void*)o->rgb, (const void*)o->radii, (const void*)o->words, (const void*)o->keys,
+                        (const void*)ordering, (const void*)visible})
+    if (p && !is_device_ptr(p)) return fail(ctx, RDX_ERR_ARG, "a batch takes device memory only (an output is host memory)");
+  if (!ordering) return fail(ctx, RDX_ERR_ARG, "ordering is NULL");
+  for (const ViewRef& r : refs)
+    for (int i = 0; i < r.n_objects; i++)
+      if (!all_device(*r.objects[i].table)) return fail(ctx, RDX_ERR_ARG, "a batch takes device memory only (a table column is host memory)");
+  rdx_params defaults;
+  rdx_params_default(&defaults);
+  const rdx_params* prm = params ? params : &defaults;
+  const uint64_t E = (uint64_t)refs[0].camera->eyes;
+  const int passes = sort_bits / 8;
+
+  rdx_batch* b = new rdx_batch();
+  b->ctx = ctx;
+  b->bits = sort_bits;
+  b->eyes = (int)E;
+  for (const ViewRef& r : refs) {
+    b->view_objects.push_back(r.n_objects);
+    for (int i = 0; i < r.n_objects; i++) {
+      b->tables.push_back(r.objects[i].table);
+      b->counts.push_back(r.objects[i].count);
+    }
+  }
+  int status = RDX_OK;
+  auto layout = [&](Arena& a) {
+    b->call = ProjectCall();
+    b->fd = FrameDev();
+    status = plan_views(ctx, a, refs.data(), n_views, prm, sort_bits, RDX_PASS_FULL, 1, b->call);
+    FrameDev& fd = b->fd;
+    fd.descs = a.take<rdx::ProjDesc>(b->call.descs.size());
+    fd.out = rdx::ProjOutputs{o->mean2d, o->conic, o->depth, o->opacity, o->rgb, o->radii, o->words, o->keys};
+    if (!fd.out.keys) fd.out.keys = a.take<uint32_t>(n);
+    fd.ord = ordering;
+    fd.vis = visible ? visible : a.take<uint32_t>((size_t)n_views);
+    fd.sb = take_segs(a, n_views);
+    fd.sc = take_sort_scratch(a, n_views, passes, n);
+  };
+  Arena dry(nullptr);
+  layout(dry);
+  auto bail = [&](int code) {
+    free_batch(b);
+    return code;
+  };
+  if (status != RDX_OK) return bail(status);
+  const uint32_t max_tiles = segment_tiles(b->call, nullptr);
+  const size_t lookback_words = (size_t)passes * max_tiles * rdx::kRadix;
+  const size_t ndesc = b->call.descs.size();
+  if (cudaMalloc(&b->arena, dry.used + 256) != cudaSuccess || cudaMalloc(&b->lookback, lookback_words * 8) != cudaSuccess ||
+      cudaMalloc(&b->words, 8) != cudaSuccess || cudaMallocHost(&b->error_host, 4) != cudaSuccess ||
+      cudaMallocHost(&b->staging, ndesc * sizeof(rdx::ProjDesc) + 1) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->capture, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    return bail(fail(ctx, RDX_ERR_NOMEM, "could not allocate a batch's device memory"));
+  }
+  Arena a(b->arena);
+  layout(a);
+  if (status != RDX_OK) return bail(status);
+  b->fd.lookback = b->lookback;
+  b->fd.error_flag = b->words;
+  // descriptors and segments stay in the batch's memory; the graph only reads them
+  std::vector<uint32_t> tiles;
+  segment_tiles(b->call, &tiles);
+  cudaError_t e = cudaMemsetAsync(b->lookback, 0, lookback_words * 8, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->words, 0, 8, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->fd.descs, b->call.descs.data(), ndesc * sizeof(rdx::ProjDesc), cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->fd.sb.begin, b->call.seg_begin.data(), (size_t)n_views * 8, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->fd.sb.end, b->call.seg_end.data(), (size_t)n_views * 8, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->fd.sb.tiles, tiles.data(), tiles.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "batch set-up"));
+  // capture the frame's kernels once
+  e = cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "cudaStreamBeginCapture"));
+  cudaError_t le = enqueue_frame(nullptr, b->call, b->fd, sort_bits, true, b->capture, &b->graph_launches);
+  e = cudaStreamEndCapture(b->capture, &b->graph);
+  if (le != cudaSuccess) return bail(cuda_fail(ctx, le, "batch capture"));
+  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "cudaStreamEndCapture"));
+  e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "cudaGraphInstantiate"));
+  *batch = b;
+  return RDX_OK;
+}
+
+int rdx_batch_update(rdx_batch* b, const rdx_view* views, int n_views, const rdx_params* params) {
+  if (!b) return RDX_ERR_ARG;
+  rdx_ctx* ctx = b->ctx;
+  if (!views || n_views != (int)b->view_objects.size())
+    return fail(ctx, RDX_ERR_ARG, "a batch update keeps the views (%d, got %d)", (int)b->view_objects.size(), n_views);
+  std::vector<ViewRef> refs;
+  size_t k = 0;
+  for (int v = 0; v < n_views; v++) {
+    if (views[v].n_objects != b->view_objects[v]) return fail(ctx, RDX_ERR_ARG, "view %d: the objects changed", v);
+    int s = check_camera(ctx, views[v].camera);
+    if (s != RDX_OK) return s;
+    if (views[v].camera->eyes != b->eyes) return fail(ctx, RDX_ERR_ARG, "view %d: the eye count changed", v);
+    for (int i = 0; i < views[v].n_objects; i++, k++) {
+      if (views[v].objects[i].table != b->tables[k] || views[v].objects[i].count != b->counts[k])
+        return fail(ctx, RDX_ERR_ARG, "view %d object %d: a batch update keeps tables and counts", v, i);
+    }
+    refs.push_back({views[v].objects, views[v].n_objects, views[v].camera});
+  }
+  rdx_params defaults;
+  rdx_params_default(&defaults);
+  ProjectCall call;
+  Arena dry(nullptr);
+  int s = plan_views(ctx, dry, refs.data(), n_views, params ? params : &defaults, b->bits, RDX_PASS_FULL, 1, call);
+  if (s != RDX_OK) return s;
+  cudaSetDevice(ctx->device);
+  if (b->staged_used) RDX_CUDA(cudaEventSynchronize(b->staged), "batch staging wait");
+  const size_t bytes = call.descs.size() * sizeof(rdx::ProjDesc);
+  memcpy(b->staging, call.descs.data(), bytes);
+  RDX_CUDA(cudaMemcpyAsync(b->fd.descs, b->staging, bytes, cudaMemcpyHostToDevice, ctx->stream), "batch update");
+  RDX_CUDA(cudaEventRecord(b->staged, ctx->stream), "batch update event");
+  b->staged_used = true;
+  b->call.descs = call.descs;
+  return RDX_OK;
+}
+
+int rdx_batch_launch(rdx_batch* b) {
+  if (!b) return RDX_ERR_ARG;
+  rdx_ctx* ctx = b->ctx;
+  cudaSetDevice(ctx->device);
+  Phase frame(ctx, RDX_PHASE_BATCH);
+  RDX_CUDA(cudaGraphLaunch(b->exec, ctx->stream), "cudaGraphLaunch");
+  ctx->launches += b->graph_launches;
+  return RDX_OK;
+}
+
+int rdx_batch_synchronize(rdx_batch* b) {
+  if (!b) return RDX_ERR_ARG;
+  rdx_ctx* ctx = b->ctx;
+  cudaSetDevice(ctx->device);
+  RDX_CUDA(cudaMemcpyAsync(b->error_host, b->words, 4, cudaMemcpyDeviceToHost, ctx->stream), "error flag");
+  RDX_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+  if (*b->error_host) {
+    *b->error_host = 0;
+    cudaMemsetAsync(b->words, 0, 4, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    return fail(ctx, RDX_ERR_TIMEOUT, "a device wait gave up (lookback of a tile never published)");
+  }
+  return RDX_OK;
+}
+
+int rdx_batch_launches(const rdx_batch* b, uint64_t* launches) {
+  if (!b || !launches) return RDX_ERR_ARG;
+  *launches = b->graph_launches;
+  return RDX_OK;
+}
+
+int rdx_batch_destroy(rdx_batch* b) {
+  if (!b) return RDX_OK;
+  cudaSetDevice(b->ctx->device);
+  cudaStreamSynchronize(b->ctx->stream);
+  free_batch(b);
+  return RDX_OK;
 }
 
 }  // extern "C"
