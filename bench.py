@@ -42,6 +42,9 @@ def parse():
     p.add_argument("--n", type=int, default=N_SPLATS)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--workload", default="frame", choices=["frame", "batched", "stereo"],
+                   help="frame: 4M SH-3 splats, one view (the headline); batched: 16 scenes x 64 views in one "
+                        "CUDA graph; stereo: 16M SH-3 fp16 splats, two eyes")
     return p.parse_args()
 
 
@@ -198,10 +201,192 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def timed(step, steps, warmup, world, local, after_warmup=None):
+    """W untimed steps, then K steps between barriers, timed with CUDA events
+    on the current stream; returns (max over ranks of the total ms, clocks)."""
+    import torch
+    import torch.distributed as dist
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    if after_warmup:
+        after_warmup()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(steps):
+        step()
+    stop.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clock_info = clocks.stop()
+    ms = start.elapsed_time(stop)
+    if world > 1:
+        t = torch.tensor([ms], device=torch.device("cuda", local), dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms, clock_info
+
+
+def run_batched(args, world, rank, local, device):
+    """16 scenes (log-uniform 50k-2M splats, SH 3 fp32), 64 views on a sphere
+    of radius 4 (view v sees scene v mod 16): one CUDA-graph launch per step."""
+    import numpy as np
+    import torch
+
+    import radix_b200 as rb
+    from radix_b200 import synthetic as syn
+    counts = syn.batched_counts(16, seed=2)
+    tables = []
+    for s, c in enumerate(counts):
+        d = syn.mixture_table(c, seed=100 + s, sh_degree=SH_DEGREE, device=device)
+        tables.append(rb.Table.raw(*(torch.from_numpy(np.ascontiguousarray(d[k])).to(device) for k in
+                                     ("centers", "log_scales", "quats", "opacities", "colors")), SH_DEGREE))
+    cams = syn.sphere_cameras(64, seed=1)
+    views = [([rb.SplatObject(tables[v % 16])], cams[v]) for v in range(64)]
+    n_views = sum(counts[v % 16] for v in range(64))
+    names = ("mean2d", "conic", "depth", "opacity", "rgb", "keys")
+    ctx = rb.Context(local)
+    batch = rb.Batch(views, None, BITS, names, device=device, ctx=ctx)
+    graph_kernels = batch.launches()
+    ms_total, clock_info = timed(batch.launch, args.steps, args.warmup, world, local)
+    batch.synchronize()
+    ms_step = ms_total / args.steps
+    # the projection / sort split of the same batch, from the direct call's phase events
+    out = rb._alloc_outputs(names, n_views, 1, device)
+    ordering = torch.empty(n_views, dtype=torch.int32, device=device)
+    visible = torch.zeros(64, dtype=torch.int32, device=device)
+    for _ in range(2):
+        rb.frame_batched(views, None, BITS, names, ctx=ctx, out=out, ordering=ordering, visible=visible)
+    torch.cuda.synchronize()
+    ctx.set_profiling(True)
+    ctx.phase_times()
+    for _ in range(5):
+        rb.frame_batched(views, None, BITS, names, ctx=ctx, out=out, ordering=ordering, visible=visible)
+    phases = ctx.phase_times()
+    ctx.set_profiling(False)
+    proj_ms = phases["project"][0] / max(phases["project"][1], 1)
+    sort_ms = phases["sort"][0] / max(phases["sort"][1], 1)
+    peak, peak_kind = peak_hbm()
+    achieved = PROJECT_BYTES * n_views / (proj_ms / 1e3) / 1e9
+    batch.close()
+    return {
+        "metric": "Msplat-views/s (batched project+SH+key+sort)",
+        "value": world * n_views * args.steps / (ms_total / 1e3) / 1e6, "unit": "Msplat-views/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic (seeded mulberry32 + Box-Muller)",
+        "config": {"workload": "batched: 16 scenes (log-uniform 50k-2M splats, SH 3 fp32, Gaussian mixtures), "
+                               "64 views on a sphere of radius 4, 1920x1080 fov 50, 32-bit keys, "
+                               "one CUDA-graph launch (projection + segmented sort) per step",
+                   "scenes": counts, "splat_views": n_views, "bits": BITS, "parallelism": f"replicas{world}",
+                   "l2": "inputs 2 GB > 126 MB L2 (no flush)", "frame_bytes_per_splat_view": FRAME_BYTES,
+                   "hbm_frac_frame": FRAME_BYTES * n_views / (ms_step / 1e3) / 1e9 / peak,
+                   "project_ms": proj_ms, "sort_ms": sort_ms},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_project (raw, SH 3, 1 eye), all 64 views in one launch",
+                     "bytes_per_splat": PROJECT_BYTES, "peak_kind": peak_kind},
+        "e2e": None, "e2e_note": "a graph batch takes device memory only",
+        "gpu_launches": graph_kernels * args.steps,
+        "clocks": clock_info,
+    }
+
+
+def run_stereo(args, world, rank, local, device):
+    """16M splats, SH 3 stored as fp16, two eyes 2064x2208 fov 100 with a
+    64 mm baseline, one key per splat from the head."""
+    import numpy as np
+    import torch
+
+    import radix_b200 as rb
+    from radix_b200 import synthetic as syn
+    n = 16_000_000 if args.n == N_SPLATS else args.n
+    d = syn.mixture_table(n, seed=0, sh_degree=SH_DEGREE, color_dtype=np.float16, device=device)
+    cols = {k: torch.from_numpy(np.ascontiguousarray(d[k])).to(device)
+            for k in ("centers", "log_scales", "quats", "opacities", "colors")}
+    del d
+    table = rb.Table.raw(cols["centers"], cols["log_scales"], cols["quats"], cols["opacities"], cols["colors"],
+                         SH_DEGREE)
+    cam = syn.stereo_camera()
+    names = ("mean2d", "conic", "depth", "opacity", "rgb", "keys")
+    out = rb._alloc_outputs(names, n, 2, device)
+    ordering = torch.empty(n, dtype=torch.int32, device=device)
+    visible = torch.zeros(1, dtype=torch.int32, device=device)
+    ctx = rb.Context(local)
+    ctx.reserve(n)
+    obj = [rb.SplatObject(table)]
+
+    def step():
+        rb.frame(obj, cam, None, BITS, names, ctx=ctx, out=out, ordering=ordering, visible=visible)
+
+    marks = {}
+
+    def start_counting():
+        ctx.set_profiling(True)
+        ctx.phase_times()
+        marks["launches"] = ctx.launches()
+
+    ms_total, clock_info = timed(step, args.steps, args.warmup, world, local, start_counting)
+    launches = ctx.launches() - marks["launches"]
+    phases = ctx.phase_times()
+    ctx.set_profiling(False)
+    runs = args.steps
+    proj_ms = phases["project"][0] / max(phases["project"][1], 1)
+    sort_ms = phases["sort"][0] / max(phases["sort"][1], 1)
+    ms_step = ms_total / args.steps
+    in_bytes = 12 + 12 + 16 + 4 + 96
+    proj_bytes = in_bytes + 2 * 40 + 4
+    frame_bytes = in_bytes + 2 * 40 + 8 + 16 * (BITS // 8) + 4
+    peak, peak_kind = peak_hbm()
+    achieved = proj_bytes * n / (proj_ms / 1e3) / 1e9
+    return {
+        "metric": "Msplats/s (stereo project+SH+key+sort)",
+        "value": world * n * args.steps / (ms_total / 1e3) / 1e6, "unit": "Msplats/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16 SH, f32+f64 maths",
+        "data": "synthetic (seeded mulberry32 + Box-Muller)",
+        "config": {"workload": f"stereo: {n} splats, SH 3 stored fp16, two eyes 2064x2208 fov 100, 64 mm "
+                               "baseline, one key per splat from the head, 32-bit keys",
+                   "n": n, "eyes": 2, "bits": BITS, "parallelism": f"replicas{world}",
+                   "l2": "inputs 2.2 GB > 126 MB L2 (no flush)", "frame_bytes_per_splat": frame_bytes,
+                   "hbm_frac_frame": frame_bytes * n / (ms_step / 1e3) / 1e9 / peak,
+                   "project_ms": proj_ms, "sort_ms": sort_ms, "phase_runs": runs},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_project (raw, SH 3 fp16, 2 eyes)",
+                     "bytes_per_splat": proj_bytes, "peak_kind": peak_kind},
+        "e2e": None, "e2e_note": "device-resident tables; the headline workload carries the host end-to-end number",
+        "gpu_launches": launches,
+        "clocks": clock_info,
+    }
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload != "frame":
+        import torch
+        import torch.distributed as dist
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        device = torch.device("cuda", local)
+        if world > 1:
+            from datetime import timedelta
+            dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
+        run = run_batched if args.workload == "batched" else run_stereo
+        line = run(args, world, rank, local, device)
+        if rank == 0:
+            print(json.dumps(line))
+        if world > 1:
+            dist.destroy_process_group()
         return
     import torch
     import torch.distributed as dist
