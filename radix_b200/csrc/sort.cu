@@ -30,6 +30,7 @@ constexpr uint64_t kFlagInclusive = 2ull << 30;
 constexpr uint64_t kFlagMask = 3ull << 30;
 constexpr uint64_t kCountMask = (1ull << 30) - 1ull;
 constexpr uint32_t kNotRanked = 0xffffu;  // the digit of an item outside the ranking
+constexpr int kSortBlocksPerSm = 4;       // onesweep blocks resident per SM (register budget)
 
 __device__ __forceinline__ uint64_t ld_relaxed64(const uint64_t* p) {
   uint64_t v;
@@ -45,6 +46,21 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   uint32_t m;
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
   return m;
+}
+
+// Lanes whose item has the same digit as this lane's (ranked items only; the
+// unranked ones group among themselves): one ballot per digit bit, cheaper
+// than a general match over 32-bit values
+__device__ __forceinline__ uint32_t peers_of(uint32_t d, bool ranked) {
+  const uint32_t r = __ballot_sync(0xffffffffu, ranked);
+  uint32_t peers = ranked ? r : ~r;
+#pragma unroll
+  for (int b = 0; b < 8; b++) {
+    const bool bit = (d >> b) & 1u;
+    const uint32_t m = __ballot_sync(0xffffffffu, bit);
+    peers &= bit ? m : ~m;
+  }
+  return peers;
 }
 
 // Segment holding `tile` (seg_tiles is non-decreasing, seg_tiles[0] = 0)
@@ -216,9 +232,10 @@ struct PassArgs {
 };
 
 template <bool FIRST, bool WRITE_KEYS>
-__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(PassArgs a) {
+__global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(PassArgs a) {
   __shared__ uint32_t s_whist[kSortWarps][kRadix];
   __shared__ uint32_t s_exchange[kSortTile];
+  __shared__ uint32_t s_vals[kSortTile];  // the tile's values, copied in asynchronously
   __shared__ uint32_t s_tile_start[kRadix];
   __shared__ uint32_t s_dest[kRadix];
   __shared__ uint64_t s_sums[kSortWarps];
@@ -246,20 +263,31 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(PassArgs a) {
   const uint64_t base = seg_begin + (uint64_t)local_tile * kSortTile;
   const uint32_t n = (uint32_t)min((uint64_t)kSortTile, seg_end - base);
 
-  // Load: warp w holds tile positions [w * 512, (w + 1) * 512), item j at j * 32 + lane
-  uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+  // Load: warp w holds tile positions [w * 512, (w + 1) * 512), item j at j * 32 + lane.
+  // Keys go to registers; values go straight to shared memory (cp.async, no
+  // registers held) and are waited for only before they are scattered. In the
+  // first pass without values, a value is the key's index within its segment.
+  const bool gen_vals = FIRST && a.vals_in == nullptr;
+  uint32_t key[kSortItems], rank[kSortItems];
   const uint32_t warp_base = (uint32_t)warp * (kSortItems * 32);
 #pragma unroll
   for (int j = 0; j < kSortItems; j++) {
     const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
     if (pos < n) {
       key[j] = __ldg(&a.keys_in[base + pos]) & a.key_mask;
-      val[j] = FIRST && a.vals_in == nullptr ? (uint32_t)(base - seg_begin) + pos : __ldg(&a.vals_in[base + pos]);
+      if (!gen_vals) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(&s_vals[pos])),
+                     "l"(&a.vals_in[base + pos])
+                     : "memory");
+      }
     } else {
       key[j] = 0u;
-      val[j] = 0u;
     }
   }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  auto value_at = [&](uint32_t pos) -> uint32_t {
+    return gen_vals ? (uint32_t)(base - seg_begin) + pos : s_vals[pos];
+  };
 
   // Rank the valid keys: items in position order, equal digits counted by
   // their lowest lane. Largest keys (first pass) are ranked among themselves.
@@ -272,7 +300,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(PassArgs a) {
     const bool tail = FIRST && a.drop && in && key[j] == a.key_mask;
     const bool ranked = in && !tail;
     const uint32_t d = ranked ? (key[j] >> a.shift) & 0xffu : kNotRanked;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t peers = peers_of(d, ranked);
     const int leader = __ffs(peers) - 1;
     uint32_t old = 0;
     if (lane == leader && d != kNotRanked) {
@@ -338,7 +366,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(PassArgs a) {
   }
   s_dest[d] = (uint32_t)seg_begin + seg_digit + prefix - tile_start;
   if (FIRST && prefix) atomicAdd(&s_valid_before, prefix);
-  __syncthreads();
+  asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's value copies have landed
+  __syncthreads();                                   // and every thread's
 
   // First pass: the largest keys to the tail of the segment, in input order
   if (FIRST) {
@@ -354,7 +383,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(PassArgs a) {
       if (a.drop && pos < n && key[j] == a.key_mask) {
         const uint64_t dst = tail_base + rank[j];
         if (dst < seg_end) {
-          a.tail_vals[dst] = val[j];
+          a.tail_vals[dst] = value_at(pos);
           if (a.tail_keys) a.tail_keys[dst] = key[j];
         }
       }
@@ -393,7 +422,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(PassArgs a) {
   __syncthreads();
 #pragma unroll
   for (int j = 0; j < kSortItems; j++) {
-    if (rank[j] != 0xffffffffu) s_exchange[rank[j]] = val[j];
+    if (rank[j] != 0xffffffffu) s_exchange[rank[j]] = value_at(warp_base + (uint32_t)j * 32 + lane);
   }
   __syncthreads();
 #pragma unroll
