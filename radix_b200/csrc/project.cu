@@ -550,23 +550,39 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
 
   const uint32_t gw = blockIdx.x * kWarps + (uint32_t)warp;
   const uint32_t nw = gridDim.x * kWarps;
-  for (uint32_t chunk = gw; chunk < total_chunks; chunk += nw) {
-    int di = 0;
-    if (lane == 0) {
-      int lo = 0, hi = n_desc - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (descs[mid].first_tile <= chunk) {
-          lo = mid;
-        } else {
-          hi = mid - 1;
+  // One loop with a single site for each phase keeps the kernel's code small
+  // (phase 2 is large; inlined at several sites it thrashes the instruction
+  // cache). Each turn either runs phase 2 on a batch of queued splats or
+  // phase 1 on the next chunk.
+  uint32_t chunk = gw;
+  int di = -1;  // descriptor of `chunk` (-1: not looked up yet)
+  while (true) {
+    const bool have_chunk = chunk < total_chunks;
+    if (have_chunk && di < 0) {
+      int d = 0;
+      if (lane == 0) {
+        int lo = 0, hi = n_desc - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (descs[mid].first_tile <= chunk) {
+            lo = mid;
+          } else {
+            hi = mid - 1;
+          }
         }
+        d = lo;
       }
-      di = lo;
+      di = __shfl_sync(0xffffffffu, d, 0);
     }
-    di = __shfl_sync(0xffffffffu, di, 0);
+    // full batches; the rest before the object changes (the queue holds one object's splats) and at the end
+    const bool switching = !have_chunk || di != cur_desc;
+    const uint32_t nb = queued >= 32 ? 32u : (switching ? queued : 0u);
+    if (nb) {
+      process(nb);
+      continue;
+    }
+    if (!have_chunk) break;
     if (di != cur_desc) {
-      if (queued) process(queued);  // the queue holds one object's splats
       const int seg = descs[di].segment;
       if (seg != cur_seg) {
         flush_hist();
@@ -721,9 +737,9 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
     }
     queued += (uint32_t)__popc(ballot);
     __syncwarp();
-    if (queued >= 32) process(32);
+    chunk += nw;
+    di = -1;
   }
-  if (queued) process(queued);
   flush_hist();
 }
 
