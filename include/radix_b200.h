@@ -291,6 +291,42 @@ int rdx_frame(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_
               const rdx_params* params, int sort_bits, const rdx_outputs* out,
               uint32_t* ordering, uint32_t* visible);
 
+/* ---- the projection's gradient ---- */
+
+/* Upstream gradients, laid out as rdx_project's outputs (float32, device
+   memory; NULL: zero), and the forward's opacity output, which says which
+   eyes drew each splat (nonzero: drawn). */
+typedef struct rdx_grads_in {
+  const float* mean2d;      /* [E][n][2]: dL/d(mean2d), pixels */
+  const float* conic;       /* [E][n][3] */
+  const float* depth;       /* [E][n] */
+  const float* opacity;     /* [E][n] */
+  const float* rgb;         /* [E][n][3] */
+  const float* fwd_opacity; /* [E][n], required */
+} rdx_grads_in;
+
+/* One object's gradient rows, float32 device memory in the table's shapes
+   (rows [0, count) are written; NULL: not wanted). */
+typedef struct rdx_table_grads {
+  float* centers;     /* [count][3] */
+  float* log_scales;  /* [count][3] */
+  float* quats;       /* [count][4]: of the stored, unnormalised quaternion */
+  float* opacities;   /* [count] */
+  float* colors;      /* [count][1 + K][3]: base rgb, then the SH coefficients (float32 also for float16 tables) */
+} rdx_table_grads;
+
+/*
+ * The gradient of rdx_project's full pass (mean2d, conic, depth, opacity,
+ * rgb) with respect to raw tables' fields, computed in float64 by one thread
+ * per splat; grads[k] receives object k's rows. Same objects, camera and
+ * params as the forward. An eye that culled a splat contributes nothing; the
+ * rgb clamp (max(base + SH, 0)) passes a gradient only where it is open.
+ * RDX_ERR_UNSUPPORTED for ext tables (quantised words have no gradient).
+ * No counterpart in the reference, which renders only.
+ */
+int rdx_project_backward(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
+                         const rdx_params* params, const rdx_grads_in* upstream, const rdx_table_grads* grads);
+
 /* ---- batched frames: many views of many collections ---- */
 
 /* One view of a batch: a collection (objects, as for rdx_frame) and its camera. */

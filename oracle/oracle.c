@@ -760,13 +760,14 @@ static void project_one(const orc_splat* s, const object_setup* o, const eye_set
   if (out->distance) out->distance[gi] = distance;
 }
 
-int orc_project(const rdx_object* objects, int n_objects, const rdx_camera* cam, const rdx_params* params,
-                int sort_bits, int cull_keys, int threads, const orc_outputs* out) {
-  if (cam->eyes < 1 || cam->eyes > 2) return -1;
-  eye_setup eyes[2];
+/* SplatCamera.setViews (splatCamera.ts:119-138) and setTransforms
+   (splatTransform.tsl.ts:78-107, splatGenerator.ts:105-112); returns the
+   objects' set-ups (caller frees) and their total count */
+static object_setup* setup_frame(const rdx_object* objects, int n_objects, const rdx_camera* cam,
+                                 const rdx_params* params, eye_setup eyes[2], uint64_t* total) {
   double head_world[16];
   orc_mat4_invert(cam->head, head_world);
-  for (int v = 0; v < cam->eyes; v++) { /* splatCamera.ts:119-138 */
+  for (int v = 0; v < cam->eyes; v++) {
     eye_setup* e = &eyes[v];
     e->identity = mat_equal(cam->eye[v].view, cam->head);
     if (e->identity) {
@@ -783,7 +784,7 @@ int orc_project(const rdx_object* objects, int n_objects, const rdx_camera* cam,
   }
   object_setup* objs = (object_setup*)calloc((size_t)(n_objects > 0 ? n_objects : 1), sizeof(object_setup));
   uint64_t n = 0;
-  for (int i = 0; i < n_objects; i++) { /* splatTransform.tsl.ts:78-107, splatGenerator.ts:105-112 */
+  for (int i = 0; i < n_objects; i++) {
     object_setup* o = &objs[i];
     orc_mat4_mul(cam->head, objects[i].world, o->a);
     m3_from_m4(o->a, o->a3);
@@ -796,6 +797,16 @@ int orc_project(const rdx_object* objects, int n_objects, const rdx_camera* cam,
     o->offset = n;
     n += objects[i].count;
   }
+  *total = n;
+  return objs;
+}
+
+int orc_project(const rdx_object* objects, int n_objects, const rdx_camera* cam, const rdx_params* params,
+                int sort_bits, int cull_keys, int threads, const orc_outputs* out) {
+  if (cam->eyes < 1 || cam->eyes > 2) return -1;
+  eye_setup eyes[2];
+  uint64_t n = 0;
+  object_setup* objs = setup_frame(objects, n_objects, cam, params, eyes, &n);
 #ifdef _OPENMP
   int nt = threads > 0 ? threads : omp_get_max_threads();
 #pragma omp parallel for schedule(static, 4096) num_threads(nt)
@@ -842,5 +853,342 @@ int orc_encode_ext_table(const rdx_table* raw, uint32_t* ext_a, uint32_t* ext_b,
     /* the padding word of a last texel is 0 */
     for (int c = k; c < ((k + 3) / 4) * 4; c++) ext_sh[c >> 2][i * 4 + (uint64_t)(c & 3)] = 0u;
   }
+  return 0;
+}
+
+/* ---- gradients of the projection (raw tables) ---- */
+
+void orc_sh_basis_grad(const double d[3], double g[24][3]) {
+  const double x = d[0], y = d[1], z = d[2];
+  const double xx = x * x, yy = y * y, zz = z * z;
+  const double c1 = 0.4886025, c2a = 1.0925484, c2b = 0.3153916, c2c = 0.5462742;
+  const double c3a = 0.5900436, c3b = 2.8906114, c3c = 0.4570458, c3d = 0.3731763, c3e = 1.4453057;
+  const double c4a = 2.5033429, c4b = 1.7701308, c4c = 0.9461747, c4d = 0.6690465, c4e = 0.1057855,
+               c4f = 0.4730873, c4g = 0.6258357;
+  double t[24][3] = {
+      {0, -c1, 0},
+      {0, 0, c1},
+      {-c1, 0, 0},
+      {c2a * y, c2a * x, 0},
+      {0, -c2a * z, -c2a * y},
+      {-2 * c2b * x, -2 * c2b * y, 4 * c2b * z},
+      {-c2a * z, 0, -c2a * x},
+      {2 * c2c * x, -2 * c2c * y, 0},
+      {-6 * c3a * x * y, -3 * c3a * (xx - yy), 0},
+      {c3b * y * z, c3b * x * z, c3b * x * y},
+      {2 * c3c * x * y, -c3c * (4 * zz - xx - 3 * yy), -8 * c3c * y * z},
+      {-6 * c3d * x * z, -6 * c3d * y * z, c3d * (6 * zz - 3 * xx - 3 * yy)},
+      {-c3c * (4 * zz - 3 * xx - yy), 2 * c3c * x * y, -8 * c3c * x * z},
+      {2 * c3e * x * z, -2 * c3e * y * z, c3e * (xx - yy)},
+      {-3 * c3a * (xx - yy), 6 * c3a * x * y, 0},
+      {c4a * (3 * xx * y - yy * y), c4a * (xx * x - 3 * x * yy), 0},
+      {-6 * c4b * x * y * z, -3 * c4b * z * (xx - yy), -c4b * y * (3 * xx - yy)},
+      {c4c * y * (7 * zz - 1), c4c * x * (7 * zz - 1), 14 * c4c * x * y * z},
+      {0, -c4d * z * (7 * zz - 3), -c4d * y * (21 * zz - 3)},
+      {0, 0, c4e * (140 * zz * z - 60 * z)},
+      {-c4d * z * (7 * zz - 3), 0, -c4d * x * (21 * zz - 3)},
+      {2 * c4f * x * (7 * zz - 1), -2 * c4f * y * (7 * zz - 1), 14 * c4f * z * (xx - yy)},
+      {-3 * c4b * z * (xx - yy), 6 * c4b * x * y * z, -c4b * x * (xx - 3 * yy)},
+      {c4g * (4 * xx * x - 12 * x * yy), c4g * (4 * yy * y - 12 * xx * y), 0},
+  };
+  memcpy(g, t, sizeof(t));
+}
+
+/* m (3x3 row-major) times a vector / its transpose times a vector */
+static void m3_tvec(const double m[9], const double v[3], double out[3]) {
+  for (int c = 0; c < 3; c++) out[c] = m[0 * 3 + c] * v[0] + m[1 * 3 + c] * v[1] + m[2 * 3 + c] * v[2];
+}
+
+/* One visible splat's gradient: the forward of project_one in the
+   covariance-matrix form, then its adjoint, summed over the eyes that draw it */
+static void backward_one(const orc_splat* s, const object_setup* o, const eye_setup* eyes, int n_eyes,
+                         const rdx_camera* cam, const uint8_t* vis, uint64_t gi, uint64_t n, const orc_grads_in* gin,
+                         double g_center[3], double g_ls[3], double g_quat[4], double* g_opacity, double g_colors[75]) {
+  const rdx_params* p = &o->params;
+  memset(g_center, 0, 3 * sizeof(double));
+  memset(g_ls, 0, 3 * sizeof(double));
+  memset(g_quat, 0, 4 * sizeof(double));
+  *g_opacity = 0.0;
+  memset(g_colors, 0, 75 * sizeof(double));
+  int any = 0;
+  for (int v = 0; v < n_eyes; v++) any |= vis[v];
+  if (!any) return;
+
+  /* ---- forward ---- */
+  double qn[4] = {s->quat[0], s->quat[1], s->quat[2], s->quat[3]};
+  const double ql = sqrt(qn[0] * qn[0] + qn[1] * qn[1] + qn[2] * qn[2] + qn[3] * qn[3]);
+  const int qvalid = ql > 0;
+  if (qvalid) {
+    for (int c = 0; c < 4; c++) qn[c] /= ql;
+  } else {
+    qn[0] = qn[1] = qn[2] = 0.0;
+    qn[3] = 1.0;
+  }
+  const double qx = qn[0], qy = qn[1], qz = qn[2], qw = qn[3];
+  const double R[9] = {1 - 2 * (qy * qy + qz * qz), 2 * (qx * qy - qw * qz), 2 * (qx * qz + qw * qy),
+                       2 * (qx * qy + qw * qz), 1 - 2 * (qx * qx + qz * qz), 2 * (qy * qz - qw * qx),
+                       2 * (qx * qz - qw * qy), 2 * (qy * qz + qw * qx), 1 - 2 * (qx * qx + qy * qy)};
+  double M[9], Mt[9], cov[9];
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) M[r * 3 + c] = R[r * 3 + c] * s->scales[c];
+  m3_transpose(M, Mt);
+  m3_mul(M, Mt, cov);
+  double a3t[9], tmp[9], acov[9];
+  m3_transpose(o->a3, a3t);
+  m3_mul(o->a3, cov, tmp);
+  m3_mul(tmp, a3t, acov); /* A cov A^T, before the LoD inflation */
+  double opacity = s->opacity, infl2 = 1.0, dop_do = 1.0;
+  int op_const = 0;
+  if (opacity > 1.0) {
+    const double raw = opacity * 4.0 - 3.0;
+    dop_do = raw < 5.0 ? 4.0 : 0.0;
+    opacity = fmin(raw, 5.0);
+    if (p->lod_inflate) {
+      infl2 = exp(2.0 * (opacity * opacity - 1.0) / (3.0 * E_CONST));
+      op_const = 1;
+    }
+  }
+  const double op_used = op_const ? 1.0 : opacity;
+  double covh[9];
+  for (int k = 0; k < 9; k++) covh[k] = acov[k] * infl2;
+  double ch[3];
+  xform_point(o->a, s->center, ch);
+
+  double g_covh[9] = {0}, g_ch[3] = {0}, g_op = 0.0, g_rgb[3] = {0, 0, 0};
+  for (int v = 0; v < n_eyes; v++) {
+    if (!vis[v]) continue;
+    const eye_setup* e = &eyes[v];
+    const uint64_t ei = (uint64_t)v * n + gi;
+    double ce[3];
+    if (e->identity) {
+      memcpy(ce, ch, sizeof(ce));
+    } else {
+      xform_point(e->from_head, ch, ce);
+    }
+    double clip[4];
+    clip_of(e->proj, ce, clip);
+    const double ndc0 = clip[0] / clip[3], ndc1 = clip[1] / clip[3];
+    double cov3[9];
+    if (e->identity) {
+      memcpy(cov3, covh, sizeof(cov3));
+    } else {
+      double ft[9], t2[9];
+      m3_transpose(e->from_head3, ft);
+      m3_mul(e->from_head3, covh, t2);
+      m3_mul(t2, ft, cov3);
+    }
+    double J[9] = {0};
+    const double z = ce[2];
+    if (e->ortho) {
+      J[0] = e->focal[0];
+      J[4] = e->focal[1];
+    } else {
+      J[0] = e->focal[0] / z;
+      J[4] = e->focal[1] / z;
+      J[6] = -(e->focal[0] * ce[0]) / (z * z);
+      J[7] = -(e->focal[1] * ce[1]) / (z * z);
+    }
+    double Jt[9], t3[9], cov2[9];
+    m3_transpose(J, Jt);
+    m3_mul(Jt, cov3, t3);
+    m3_mul(t3, J, cov2);
+    /* depth of field: blur as a function of the depth (projection.tsl.ts:117-125) */
+    double blur = p->blur_amount, dblur_ddepth = 0.0;
+    if (p->focal_distance > 0.0f && p->aperture_tan > 0.0f && z < 0.0) {
+      const double depth = -z;
+      const double fp = cam->height * 0.5 * e->proj[5];
+      const double dist = depth - (double)p->focal_distance;
+      const double coc_view = fabs(dist) * (double)p->aperture_tan;
+      const double coc = e->ortho ? coc_view * fp : coc_view * fp / depth;
+      const double dcoc = e->ortho ? (dist >= 0 ? 1.0 : -1.0) * p->aperture_tan * fp
+                                   : ((dist >= 0 ? 1.0 : -1.0) * p->aperture_tan * fp / depth - coc / depth);
+      const double maxr2 = (double)p->max_pixel_radius * p->max_pixel_radius;
+      const double c2 = coc * coc;
+      if (c2 > blur && c2 < maxr2) dblur_ddepth = 2.0 * coc * dcoc;
+      blur = fmin(fmax(c2, blur), maxr2);
+    }
+    const double pre = p->pre_blur_amount;
+    const double a0 = cov2[0] + pre, d0 = cov2[4] + pre, b = cov2[1];
+    const double det_orig = a0 * d0 - b * b;
+    const double a = a0 + blur, d = d0 + blur;
+    const double det = a * d - b * b;
+    const double r = det_orig / det;
+
+    /* ---- adjoint ---- */
+    const double gm0 = gin->mean2d ? gin->mean2d[ei * 2] : 0.0, gm1 = gin->mean2d ? gin->mean2d[ei * 2 + 1] : 0.0;
+    const double gc0 = gin->conic ? gin->conic[ei * 3] : 0.0, gc1 = gin->conic ? gin->conic[ei * 3 + 1] : 0.0,
+                 gc2 = gin->conic ? gin->conic[ei * 3 + 2] : 0.0;
+    const double gd = gin->depth ? gin->depth[ei] : 0.0;
+    const double go = gin->opacity ? gin->opacity[ei] : 0.0;
+    if (gin->rgb)
+      for (int c = 0; c < 3; c++) g_rgb[c] += gin->rgb[ei * 3 + c];
+    /* conic = (d, -b, a) / det */
+    double G_a = gc2 / det, G_d = gc0 / det, G_b = -gc1 / det;
+    double G_det = (-gc0 * d + gc1 * b - gc2 * a) / (det * det);
+    /* opacity = op sqrt(det_orig / det) */
+    double G_det_orig = 0.0;
+    if (r > 0.0) {
+      const double sr = sqrt(r);
+      g_op += go * sr;
+      const double G_r = go * op_used / (2.0 * sr);
+      G_det_orig = G_r / det;
+      G_det += -G_r * r / det;
+    }
+    G_a += G_det * d;
+    G_d += G_det * a;
+    G_b += -2.0 * b * G_det;
+    const double G_a0 = G_a + G_det_orig * d0, G_d0 = G_d + G_det_orig * a0;
+    G_b += -2.0 * b * G_det_orig;
+    const double G_blur = G_a + G_d;
+    /* cov2 = J^T cov3 J, read at [0], [1] and [4] */
+    double G2[9] = {0};
+    G2[0] = G_a0;
+    G2[1] = G_b;
+    G2[4] = G_d0;
+    double G2s[9], JG[9], g_cov3[9], tmpg[9];
+    for (int k = 0; k < 9; k++) G2s[k] = G2[k] + G2[(k % 3) * 3 + k / 3]; /* G2 + G2^T */
+    m3_mul(J, G2, JG);
+    m3_mul(JG, Jt, g_cov3); /* J G2 J^T */
+    double CJ[9], g_J[9];
+    m3_mul(cov3, J, tmpg);
+    memcpy(CJ, tmpg, sizeof(CJ));
+    m3_mul(CJ, G2s, g_J); /* cov3 J (G2 + G2^T) */
+    double g_ce[3] = {0, 0, 0};
+    if (!e->ortho) {
+      const double fx = e->focal[0], fy = e->focal[1];
+      g_ce[0] += g_J[6] * (-fx / (z * z));
+      g_ce[1] += g_J[7] * (-fy / (z * z));
+      g_ce[2] += g_J[0] * (-fx / (z * z)) + g_J[4] * (-fy / (z * z)) + g_J[6] * (2.0 * fx * ce[0] / (z * z * z)) +
+                 g_J[7] * (2.0 * fy * ce[1] / (z * z * z));
+    }
+    g_ce[2] += -G_blur * dblur_ddepth; /* depth = -z */
+    /* mean2d = (ndc + 1) / 2 * size, ndc = clip.xy / clip.w */
+    const double g_n0 = gm0 * 0.5 * cam->width, g_n1 = gm1 * 0.5 * cam->height;
+    const double g_cl[4] = {g_n0 / clip[3], g_n1 / clip[3], 0.0, -(g_n0 * ndc0 + g_n1 * ndc1) / clip[3]};
+    for (int c = 0; c < 3; c++)
+      for (int rr = 0; rr < 4; rr++) g_ce[c] += e->proj[c * 4 + rr] * g_cl[rr];
+    g_ce[2] += -gd;
+    /* cov3 = F covh F^T, ce = F ch + f */
+    if (e->identity) {
+      for (int k = 0; k < 9; k++) g_covh[k] += g_cov3[k];
+      for (int c = 0; c < 3; c++) g_ch[c] += g_ce[c];
+    } else {
+      double ft[9], t4[9], t5[9], gh[3];
+      m3_transpose(e->from_head3, ft);
+      m3_mul(ft, g_cov3, t4);
+      m3_mul(t4, e->from_head3, t5);
+      for (int k = 0; k < 9; k++) g_covh[k] += t5[k];
+      m3_tvec(e->from_head3, g_ce, gh);
+      for (int c = 0; c < 3; c++) g_ch[c] += gh[c];
+    }
+  }
+  /* ch = A c + t */
+  double gc_[3];
+  m3_tvec(o->a3, g_ch, gc_);
+  for (int c = 0; c < 3; c++) g_center[c] += gc_[c];
+  /* covh = infl2 A cov A^T */
+  double g_infl2 = 0.0;
+  for (int k = 0; k < 9; k++) g_infl2 += g_covh[k] * acov[k];
+  double t6[9], t7[9], g_cov[9];
+  m3_mul(a3t, g_covh, t6);
+  m3_mul(t6, o->a3, t7);
+  for (int k = 0; k < 9; k++) g_cov[k] = t7[k] * infl2;
+  /* cov = M M^T: g_M = (g_cov + g_cov^T) M */
+  double gcs[9], g_M[9];
+  for (int k = 0; k < 9; k++) gcs[k] = g_cov[k] + g_cov[(k % 3) * 3 + k / 3];
+  m3_mul(gcs, M, g_M);
+  double g_R[9];
+  for (int r = 0; r < 3; r++)
+    for (int c = 0; c < 3; c++) {
+      g_R[r * 3 + c] = g_M[r * 3 + c] * s->scales[c];
+      g_ls[c] += g_M[r * 3 + c] * R[r * 3 + c] * s->scales[c]; /* d s / d ln s = s */
+    }
+  /* R(q) of the normalised quaternion, then the normalisation */
+  if (qvalid) {
+    const double* G = g_R;
+    double gq[4];
+    gq[0] = G[1] * 2 * qy + G[2] * 2 * qz + G[3] * 2 * qy + G[4] * -4 * qx + G[5] * -2 * qw + G[6] * 2 * qz +
+            G[7] * 2 * qw + G[8] * -4 * qx;
+    gq[1] = G[0] * -4 * qy + G[1] * 2 * qx + G[2] * 2 * qw + G[3] * 2 * qx + G[5] * 2 * qz + G[6] * -2 * qw +
+            G[7] * 2 * qz + G[8] * -4 * qy;
+    gq[2] = G[0] * -4 * qz + G[1] * -2 * qw + G[2] * 2 * qx + G[3] * 2 * qw + G[4] * -4 * qz + G[5] * 2 * qy +
+            G[6] * 2 * qx + G[7] * 2 * qy;
+    gq[3] = G[1] * -2 * qz + G[2] * 2 * qy + G[3] * 2 * qz + G[5] * -2 * qx + G[6] * -2 * qy + G[7] * 2 * qx;
+    const double dotq = gq[0] * qx + gq[1] * qy + gq[2] * qz + gq[3] * qw;
+    for (int c = 0; c < 4; c++) g_quat[c] = (gq[c] - qn[c] * dotq) / ql;
+  }
+  /* opacity: the LoD stretch and inflation (projection.tsl.ts:42-64) */
+  if (op_const) {
+    const double g_opl = g_infl2 * infl2 * 4.0 * opacity / (3.0 * E_CONST);
+    *g_opacity = g_opl * dop_do;
+  } else {
+    *g_opacity = g_op * dop_do;
+  }
+  /* colour: rgb = max(base + SH, 0) with SH (GpuShReader.apply), base alone without */
+  const int degree = s->sh_degree < p->max_sh_degree ? s->sh_degree : p->max_sh_degree;
+  if (s->sh_degree < 1) {
+    for (int c = 0; c < 3; c++) g_colors[c] = g_rgb[c];
+    return;
+  }
+  double sh[3] = {0, 0, 0}, dir[3] = {0, 0, 0}, len = 0.0;
+  double dv[3] = {s->center[0] - o->origin[0], s->center[1] - o->origin[1], s->center[2] - o->origin[2]};
+  if (degree >= 1) {
+    len = sqrt(dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2]);
+    if (len > 0)
+      for (int c = 0; c < 3; c++) dir[c] = dv[c] / len;
+    orc_sh_evaluate(s->sh, dir, degree, sh);
+  }
+  double gm[3];
+  for (int c = 0; c < 3; c++) {
+    gm[c] = s->rgb[c] + sh[c] > 0.0 ? g_rgb[c] : 0.0;
+    g_colors[c] = gm[c];
+  }
+  if (degree >= 1 && len > 0) {
+    double basis[24], db[24][3], g_dir[3] = {0, 0, 0};
+    orc_sh_basis(dir, basis);
+    orc_sh_basis_grad(dir, db);
+    for (int k = 0; k < SH_COEFFS[degree]; k++) {
+      for (int c = 0; c < 3; c++) {
+        g_colors[3 + k * 3 + c] = gm[c] * basis[k];
+        for (int j = 0; j < 3; j++) g_dir[j] += gm[c] * s->sh[k * 3 + c] * db[k][j];
+      }
+    }
+    const double dd = g_dir[0] * dir[0] + g_dir[1] * dir[1] + g_dir[2] * dir[2];
+    for (int j = 0; j < 3; j++) g_center[j] += (g_dir[j] - dir[j] * dd) / len;
+  }
+}
+
+int orc_project_backward(const rdx_object* objects, int n_objects, const rdx_camera* cam, const rdx_params* params,
+                         const orc_grads_in* gin, const orc_grads_out* gout, int threads) {
+  if (cam->eyes < 1 || cam->eyes > 2) return -1;
+  for (int i = 0; i < n_objects; i++)
+    if (objects[i].table->layout != RDX_LAYOUT_RAW) return -1;
+  eye_setup eyes[2];
+  uint64_t n = 0;
+  object_setup* objs = setup_frame(objects, n_objects, cam, params, eyes, &n);
+#ifdef _OPENMP
+  int nt = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(static, 1024) num_threads(nt)
+#endif
+  for (int64_t gi = 0; gi < (int64_t)n; gi++) {
+    int oi = 0;
+    while (oi + 1 < n_objects && (uint64_t)gi >= objs[oi + 1].offset) oi++;
+    orc_splat s;
+    orc_load_splat(objects[oi].table, (uint64_t)gi - objs[oi].offset, &s);
+    /* the forward's cull decisions, per eye */
+    uint8_t vis[2] = {0, 0};
+    orc_outputs one;
+    memset(&one, 0, sizeof(one));
+    one.visible = vis;
+    project_one(&s, &objs[oi], eyes, cam->eyes, cam, 32, 1, 0, 1, &one);
+    double gcen[3], gls[3], gq[4], gop, gcol[75];
+    backward_one(&s, &objs[oi], eyes, cam->eyes, cam, vis, (uint64_t)gi, n, gin, gcen, gls, gq, &gop, gcol);
+    if (gout->centers) memcpy(gout->centers + gi * 3, gcen, sizeof(gcen));
+    if (gout->log_scales) memcpy(gout->log_scales + gi * 3, gls, sizeof(gls));
+    if (gout->quats) memcpy(gout->quats + gi * 4, gq, sizeof(gq));
+    if (gout->opacities) gout->opacities[gi] = gop;
+    if (gout->colors) memcpy(gout->colors + gi * 75, gcol, sizeof(gcol));
+  }
+  free(objs);
   return 0;
 }

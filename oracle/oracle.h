@@ -78,6 +78,39 @@ int orc_project(const rdx_object* objects, int n_objects, const rdx_camera* came
                 const rdx_params* params, int sort_bits, int cull_keys, int threads,
                 const orc_outputs* out);
 
+/* d(basis)/d(x, y, z) of the 24 basis functions above, as polynomials in x, y, z */
+void orc_sh_basis_grad(const double dir[3], double out[24][3]);
+
+/* Upstream gradients of a projection, laid out as orc_outputs (NULL: zero) */
+typedef struct orc_grads_in {
+  const double* mean2d;
+  const double* conic;
+  const double* depth;
+  const double* opacity;
+  const double* rgb;
+} orc_grads_in;
+
+/* Gradients of the collection's rows (raw tables): centers [n][3],
+   log_scales [n][3], quats [n][4] (of the stored, unnormalised quaternion),
+   opacities [n], colors [n][75] (base rgb, then the coefficients of bands
+   1..4, coefficient-major RGB; beyond the table's degree: 0) */
+typedef struct orc_grads_out {
+  double* centers;
+  double* log_scales;
+  double* quats;
+  double* opacities;
+  double* colors;
+} orc_grads_out;
+
+/*
+ * The analytic gradient of orc_project's mean2d, conic, depth, opacity and
+ * rgb outputs (full pass) with respect to a raw table's fields, in float64.
+ * An eye that culls a splat contributes nothing. Returns -1 for an ext table.
+ */
+int orc_project_backward(const rdx_object* objects, int n_objects, const rdx_camera* camera,
+                         const rdx_params* params, const orc_grads_in* gin, const orc_grads_out* gout,
+                         int threads);
+
 /* Word codecs of the ewa projection (src/render/projection.tsl.ts:283-294) */
 uint32_t orc_encode_depth20(double view_z);
 uint32_t orc_encode_angle12(double angle);

@@ -20,6 +20,14 @@ def build():
     return LIB_PATH
 
 
+class orc_grads_in(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name in ("mean2d", "conic", "depth", "opacity", "rgb")]
+
+
+class orc_grads_out(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name in ("centers", "log_scales", "quats", "opacities", "colors")]
+
+
 class orc_outputs(ctypes.Structure):
     _fields_ = [(name, ctypes.c_void_p) for name in
                 ("mean2d", "conic", "depth", "opacity", "rgb", "radii", "words", "keys", "distance", "visible")]
@@ -55,6 +63,10 @@ def lib():
             "orc_project": (i, [ctypes.POINTER(_abi.rdx_object), i, ctypes.POINTER(_abi.rdx_camera),
                                 ctypes.POINTER(_abi.rdx_params), i, i, i, ctypes.POINTER(orc_outputs)]),
             "orc_encode_ext_table": (i, [ctypes.POINTER(_abi.rdx_table), vp, vp, vp]),
+            "orc_sh_basis_grad": (None, [vp, vp]),
+            "orc_project_backward": (i, [ctypes.POINTER(_abi.rdx_object), i, ctypes.POINTER(_abi.rdx_camera),
+                                         ctypes.POINTER(_abi.rdx_params), ctypes.POINTER(orc_grads_in),
+                                         ctypes.POINTER(orc_grads_out), i]),
             "orc_params_default": (None, [ctypes.POINTER(_abi.rdx_params)]),
             "orc_encode_depth20": (u32, [f64]),
             "orc_encode_angle12": (u32, [f64]),
@@ -192,3 +204,33 @@ def encode_ext(raw):
     if lib().orc_encode_ext_table(ctypes.byref(t.c), _p(a), _p(b), ptrs) != 0:
         raise ValueError("orc_encode_ext_table failed")
     return a, b, sh
+
+
+def project_backward(objects, camera, upstream, params=None, threads=0):
+    """float64 gradient of the projection's mean2d / conic / depth / opacity /
+    rgb (upstream: dict of arrays shaped as project()'s outputs, missing =
+    zero) with respect to the raw tables' rows: dict of centers [n][3],
+    log_scales [n][3], quats [n][4], opacities [n] and colors [n][75]."""
+    import radix_b200 as rb
+    params = params or rb.SplatParams()
+    n = sum(o.count for o in objects)
+    ups = {k: np.ascontiguousarray(v, dtype=np.float64) for k, v in upstream.items() if v is not None}
+    gin = orc_grads_in(**{k: _p(v) for k, v in ups.items()})
+    out = {"centers": np.zeros((n, 3)), "log_scales": np.zeros((n, 3)), "quats": np.zeros((n, 4)),
+           "opacities": np.zeros(n), "colors": np.zeros((n, 75))}
+    gout = orc_grads_out(**{k: _p(v) for k, v in out.items()})
+    objs, keep = rb._c_objects(objects)
+    cam = camera.to_c(_abi)
+    prm = params.to_c()
+    st = lib().orc_project_backward(objs, len(objects), ctypes.byref(cam), ctypes.byref(prm), ctypes.byref(gin),
+                                    ctypes.byref(gout), threads)
+    del keep, ups
+    if st != 0:
+        raise ValueError("orc_project_backward failed (ext tables have no gradient)")
+    return out
+
+
+def sh_basis_grad(d):
+    out = np.zeros((24, 3))
+    lib().orc_sh_basis_grad(_p(np.ascontiguousarray(d, dtype=np.float64)), _p(out))
+    return out

@@ -25,7 +25,8 @@ from .camera import IDENTITY, Camera, look_at, perspective
 
 __all__ = [
     "Context", "SortKeys", "RadixSort", "Compact", "SplatSorter", "SplatParams", "Table", "SplatObject",
-    "Camera", "look_at", "perspective", "project_collection", "frame", "frame_batched", "Batch", "RadixError",
+    "Camera", "look_at", "perspective", "project_collection", "project_backward", "frame", "frame_batched", "Batch",
+    "RadixError",
     "align_capacity",
 ]
 
@@ -451,6 +452,43 @@ def frame(objects, camera, params=None, sort_bits=24, outputs=DEFAULT_OUTPUTS, d
     res["ordering"] = ordering
     res["visible"] = vis_host.value if vis_host is not None else visible
     return res
+
+
+GRAD_OUTPUTS = ("mean2d", "conic", "depth", "opacity", "rgb")
+
+
+def project_backward(objects, camera, upstream, fwd_opacity, params=None, ctx=None, grads=None):
+    """The gradient of `project_collection`'s full pass (raw tables, CUDA
+    tensors): upstream = {output: dL/d(output)} laid out as the forward's
+    outputs (missing: zero), fwd_opacity = the forward's 'opacity' output.
+    Returns one dict per object: centers [count][3], log_scales [count][3],
+    quats [count][4], opacities [count], colors [count][1+K][3] (float32)."""
+    torch = _torch()
+    params = params or SplatParams()
+    if grads is None:
+        grads = []
+        for o in objects:
+            dev = torch.device("cuda", torch.cuda.current_device())
+            k = (int(o.table.c.sh_degree) + 1) ** 2
+            grads.append({"centers": torch.empty((o.count, 3), device=dev), "log_scales": torch.empty((o.count, 3), device=dev),
+                          "quats": torch.empty((o.count, 4), device=dev), "opacities": torch.empty(o.count, device=dev),
+                          "colors": torch.empty((o.count, k, 3), device=dev)})
+    gin = _abi.rdx_grads_in()
+    for name in GRAD_OUTPUTS:
+        if upstream.get(name) is not None:
+            setattr(gin, name, _ptr(upstream[name]))
+    gin.fwd_opacity = _ptr(fwd_opacity)
+    gout = (_abi.rdx_table_grads * max(1, len(objects)))()
+    for i, g in enumerate(grads):
+        for name, t in g.items():
+            setattr(gout[i], name, _ptr(t))
+    objs, keep = _c_objects(objects)
+    cam = camera.to_c(_abi)
+    prm = params.to_c()
+    c = ctx or default_context(0)
+    c.call("rdx_project_backward", objs, len(objects), ctypes.byref(cam), ctypes.byref(prm), ctypes.byref(gin), gout)
+    del keep
+    return grads
 
 
 def _c_views(views):

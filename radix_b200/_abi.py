@@ -112,6 +112,14 @@ class rdx_view(ctypes.Structure):
     ]
 
 
+class rdx_grads_in(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name in ("mean2d", "conic", "depth", "opacity", "rgb", "fwd_opacity")]
+
+
+class rdx_table_grads(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_void_p) for name in ("centers", "log_scales", "quats", "opacities", "colors")]
+
+
 class rdx_outputs(ctypes.Structure):
     _fields_ = [
         ("mean2d", ctypes.c_void_p),
@@ -157,6 +165,9 @@ SIGNATURES = {
     "rdx_frame": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_object), ctypes.c_int, ctypes.POINTER(rdx_camera),
                                  ctypes.POINTER(rdx_params), ctypes.c_int, ctypes.POINTER(rdx_outputs), ctypes.c_void_p,
                                  ctypes.c_void_p]),
+    "rdx_project_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_object), ctypes.c_int,
+                                            ctypes.POINTER(rdx_camera), ctypes.POINTER(rdx_params),
+                                            ctypes.POINTER(rdx_grads_in), ctypes.POINTER(rdx_table_grads)]),
     "rdx_frame_batched": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_view), ctypes.c_int, ctypes.POINTER(rdx_params),
                                          ctypes.c_int, ctypes.POINTER(rdx_outputs), ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_batch_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_view), ctypes.c_int, ctypes.POINTER(rdx_params),

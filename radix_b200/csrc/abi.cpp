@@ -518,13 +518,6 @@ rdx::ProjDesc make_desc(const rdx_camera& cam, const Camera& c, const rdx_object
       }
     }
   }
-  const rdx::DevTable& t = table;
-  auto a16 = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
-  bool tma = t.layout == RDX_LAYOUT_RAW ? a16(t.centers) && a16(t.log_scales) && a16(t.quats) && a16(t.opacities) && a16(t.colors)
-                                        : a16(t.ext_a) && a16(t.ext_b);
-  if (t.layout == RDX_LAYOUT_EXT)
-    for (int c = 0; c < (kShCoeffs[t.sh_degree] + 3) / 4; c++) tma = tma && a16(t.ext_sh[c]);
-  d.tma_ok = tma ? 1 : 0;
   d.segment = 0;
   d.width = cam.width;
   d.height = cam.height;
@@ -576,6 +569,7 @@ int plan_views(rdx_ctx* ctx, Arena& a, const ViewRef* views, int n_views, const 
       if (o.count > 0) {
         rdx::ProjDesc d = make_desc(*vw.camera, c, o, staged[o.table], *params, offset, n, bits, pass, cull_keys);
         d.segment = v;
+        d.object = i;
         by_kind[kind].push_back(d);
       }
       offset += o.count;
@@ -1320,6 +1314,72 @@ int rdx_frame(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_
               int sort_bits, const rdx_outputs* out, uint32_t* ordering, uint32_t* visible) {
   const ViewRef view{objects, n_objects, camera};
   return frame_common(ctx, &view, 1, params, sort_bits, RDX_PASS_FULL, 1, out, ordering, visible, true);
+}
+
+int rdx_project_backward(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
+                         const rdx_params* params, const rdx_grads_in* upstream, const rdx_table_grads* grads) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (!upstream || !grads) return fail(ctx, RDX_ERR_ARG, "upstream or grads is NULL");
+  if (!upstream->fwd_opacity) return fail(ctx, RDX_ERR_ARG, "the forward's opacity output is required");
+  const ViewRef view{objects, n_objects, camera};
+  uint64_t n = 0;
+  int s = check_views(ctx, &view, 1, 32, RDX_PASS_FULL, &n);
+  if (s != RDX_OK) return s;
+  for (int i = 0; i < n_objects; i++) {
+    if (objects[i].table->layout != RDX_LAYOUT_RAW)
+      return fail(ctx, RDX_ERR_UNSUPPORTED, "object %d: only raw tables have a gradient", i);
+    if (!all_device(*objects[i].table)) return fail(ctx, RDX_ERR_ARG, "the gradient takes device memory only (object %d's table)", i);
+    const rdx_table_grads& g = grads[i];
+    for (const void* p : {(const void*)g.centers, (const void*)g.log_scales, (const void*)g.quats,
+                          (const void*)g.opacities, (const void*)g.colors})
+      if (p && !is_device_ptr(p)) return fail(ctx, RDX_ERR_ARG, "object %d: a gradient buffer is host memory", i);
+    if (g.quats && !aligned(g.quats, 16)) return fail(ctx, RDX_ERR_ARG, "object %d: quats gradient not 16-byte aligned", i);
+  }
+  for (const void* p : {(const void*)upstream->mean2d, (const void*)upstream->conic, (const void*)upstream->depth,
+                        (const void*)upstream->opacity, (const void*)upstream->rgb, (const void*)upstream->fwd_opacity})
+    if (p && !is_device_ptr(p)) return fail(ctx, RDX_ERR_ARG, "an upstream gradient is host memory");
+  if (n == 0) return RDX_OK;
+  rdx_params defaults;
+  rdx_params_default(&defaults);
+  cudaSetDevice(ctx->device);
+  ProjectCall call;
+  rdx::ProjDesc* descs = nullptr;
+  rdx::GradsOut* gdev = nullptr;
+  int status = RDX_OK;
+  auto layout = [&](Arena& a) {
+    call = ProjectCall();
+    status = plan_views(ctx, a, &view, 1, params ? params : &defaults, 32, RDX_PASS_FULL, 1, call);
+    descs = a.take<rdx::ProjDesc>(call.descs.size());
+    gdev = a.take<rdx::GradsOut>(call.descs.size());
+  };
+  Arena dry(nullptr);
+  layout(dry);
+  if (status != RDX_OK) return status;
+  s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  layout(a);
+  if (status != RDX_OK) return status;
+  std::vector<rdx::GradsOut> gh;
+  for (const rdx::ProjDesc& d : call.descs) {
+    const rdx_table_grads& g = grads[d.object];
+    gh.push_back(rdx::GradsOut{g.centers, g.log_scales, g.quats, g.opacities, g.colors});
+  }
+  s = upload(ctx, descs, call.descs.data(), call.descs.size() * sizeof(rdx::ProjDesc));
+  if (s == RDX_OK) s = upload(ctx, gdev, gh.data(), gh.size() * sizeof(rdx::GradsOut));
+  if (s != RDX_OK) return s;
+  const rdx::GradsIn in{upstream->mean2d, upstream->conic, upstream->depth, upstream->opacity, upstream->rgb,
+                        upstream->fwd_opacity};
+  Phase backward(ctx, RDX_PHASE_PROJECT);
+  for (size_t g = 0; g + 1 < call.groups.size(); g++) {
+    const int start = call.groups[g];
+    const int count = call.groups[g + 1] - start;
+    RDX_CUDA(rdx::launch_project_backward(descs + start, gdev + start, call.descs.data() + start, count,
+                                          call.group_tiles[g], in, ctx->stream),
+             "backward launch");
+    if (call.group_tiles[g]) ctx->launches += 1;
+  }
+  return RDX_OK;
 }
 
 int rdx_frame_batched(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx_params* params, int sort_bits,

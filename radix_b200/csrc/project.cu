@@ -412,14 +412,14 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
         const double ex = W.e[v][0][q], ey = W.e[v][1][q], ez = W.e[v][2][q];
         const double clx = W.e[v][3][q], cly = W.e[v][4][q], clw = W.e[v][5][q];
         // depth of field (projection.tsl.ts:117-125)
-        float blur = p.blur_amount;
+        double blur = p.blur_amount;
         const float fz = (float)ez;
-        if (p.focal_distance > 0.0f && p.aperture_tan > 0.0f && fz < 0.0f) {
-          const float depth = -fz;
-          const float coc_view = fabsf(depth - p.focal_distance) * p.aperture_tan;
-          const float focal_pixels = (float)sd.height * 0.5f * e.proj11;
-          const float coc = e.ortho ? coc_view * focal_pixels : coc_view * focal_pixels / depth;
-          blur = fminf(fmaxf(coc * coc, blur), p.max_pixel_radius * p.max_pixel_radius);
+        if (p.focal_distance > 0.0f && p.aperture_tan > 0.0f && ez < 0.0) {
+          const double depth = -ez;
+          const double coc_view = fabs(depth - (double)p.focal_distance) * (double)p.aperture_tan;
+          const double focal_pixels = sd.height * 0.5 * e.proj[5];
+          const double coc = e.ortho ? coc_view * focal_pixels : coc_view * focal_pixels / depth;
+          blur = fmin(fmax(coc * coc, blur), (double)p.max_pixel_radius * p.max_pixel_radius);
         }
         double a_d = 0.0, b_d = 0.0, d_d = 0.0, det_d = 1.0, opacity_cd = 0.0;
         float scale1 = 0.f, scale2 = 0.f, angle = 0.f;
@@ -452,7 +452,7 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
           const double m1 = u02 * u10 - u00 * u12;
           const double m2 = u00 * u11 - u01 * u10;
           const double det_t = m0 * m0 * (s2y * s2z) + m1 * m1 * (s2x * s2z) + m2 * m2 * (s2x * s2y);
-          const double pre = p.pre_blur_amount, full = (double)p.pre_blur_amount + (double)blur;
+          const double pre = p.pre_blur_amount, full = (double)p.pre_blur_amount + blur;
           const double det_orig = det_t + pre * (ra + rd) + pre * pre;
           det_d = det_t + full * (ra + rd) + full * full;
           a_d = ra + full;

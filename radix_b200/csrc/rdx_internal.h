@@ -144,7 +144,7 @@ struct ProjDesc {
   int cull_keys;
   int keys_only;
   uint32_t first_tile;   // running count of projection tiles before this object
-  int tma_ok;            // every column 16-byte aligned: tiles staged by TMA bulk copies
+  int object;            // index of the object in its view's collection
   int segment;           // the sort segment the keys belong to (a view of a batch)
   int reserved3;
 };
@@ -172,6 +172,32 @@ struct ProjHist {
 };
 
 // One persistent launch over every descriptor of one table kind (descs in device memory)
+// ---- the projection's gradient (raw tables) ----
+
+// Upstream gradients laid out as the forward's outputs ([E][n]...; null: zero)
+// and the forward's opacity output, which marks the eyes that drew a splat
+struct GradsIn {
+  const float* mean2d;
+  const float* conic;
+  const float* depth;
+  const float* opacity;
+  const float* rgb;
+  const float* fwd_opacity;
+};
+
+// One object's gradient rows (float32, the table's shapes; null: not wanted)
+struct GradsOut {
+  float* centers;
+  float* log_scales;
+  float* quats;
+  float* opacities;
+  float* colors;
+};
+
+// grads_dev[k] belongs to descs_dev[k]; one launch per table kind
+cudaError_t launch_project_backward(const ProjDesc* descs_dev, const GradsOut* grads_dev, const ProjDesc* descs_host,
+                                    int n_desc, uint32_t total_chunks, const GradsIn& in, cudaStream_t stream);
+
 cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host, int n_desc,
                            uint32_t total_tiles, const ProjOutputs& out, const ProjHist& hist,
                            uint32_t* error_flag, cudaStream_t stream);
