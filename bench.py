@@ -42,9 +42,9 @@ def parse():
     p.add_argument("--n", type=int, default=N_SPLATS)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--workload", default="frame", choices=["frame", "batched", "stereo"],
+    p.add_argument("--workload", default="frame", choices=["frame", "batched", "stereo", "backward"],
                    help="frame: 4M SH-3 splats, one view (the headline); batched: 16 scenes x 64 views in one "
-                        "CUDA graph; stereo: 16M SH-3 fp16 splats, two eyes")
+                        "CUDA graph; stereo: 16M SH-3 fp16 splats, two eyes; backward: the projection's gradient, 1M")
     return p.parse_args()
 
 
@@ -365,6 +365,73 @@ def run_stereo(args, world, rank, local, device):
     }
 
 
+def run_backward(args, world, rank, local, device):
+    """1M splats of the SH-3 mixture: the forward projection (mean2d, conic,
+    depth, opacity, rgb) and its gradient with respect to the table, upstream
+    gradients N(0, 1); timed separately, the backward is the step."""
+    import numpy as np
+    import torch
+
+    import radix_b200 as rb
+    from radix_b200 import synthetic as syn
+    n = 1_000_000 if args.n == N_SPLATS else args.n
+    d = syn.mixture_table(n, seed=0, sh_degree=SH_DEGREE, device=device)
+    cols = {k: torch.from_numpy(np.ascontiguousarray(d[k])).to(device)
+            for k in ("centers", "log_scales", "quats", "opacities", "colors")}
+    table = rb.Table.raw(cols["centers"], cols["log_scales"], cols["quats"], cols["opacities"], cols["colors"],
+                         SH_DEGREE)
+    obj = [rb.SplatObject(table)]
+    cam = syn.scale_camera()
+    ctx = rb.Context(local)
+    names = ("mean2d", "conic", "depth", "opacity", "rgb")
+    out = rb._alloc_outputs(names, n, 1, device)
+    g = torch.Generator(device=device).manual_seed(1)
+    up = {k: torch.randn(out[k].shape, device=device, generator=g) for k in ("mean2d", "conic", "opacity", "rgb")}
+    grads = [{"centers": torch.empty((n, 3), device=device), "log_scales": torch.empty((n, 3), device=device),
+              "quats": torch.empty((n, 4), device=device), "opacities": torch.empty(n, device=device),
+              "colors": torch.empty((n, (SH_DEGREE + 1) ** 2, 3), device=device)}]
+
+    def forward():
+        rb.project_collection(obj, cam, None, BITS, "full", True, names, ctx=ctx, out=out)
+
+    def backward():
+        rb.project_backward(obj, cam, up, out["opacity"], None, ctx=ctx, grads=grads)
+
+    marks = {}
+
+    def start_counting():
+        marks["launches"] = ctx.launches()
+
+    fwd_ms, _ = timed(forward, args.steps, args.warmup, world, local)
+    ms_total, clock_info = timed(backward, args.steps, args.warmup, world, local, start_counting)
+    launches = ctx.launches() - marks["launches"]
+    ms_step = ms_total / args.steps
+    fwd_step = fwd_ms / args.steps
+    in_bytes = 12 + 12 + 16 + 4 + 192
+    bwd_bytes = in_bytes + 36 + 4 + in_bytes  # table re-read, upstream + forward opacity, gradients
+    peak, peak_kind = peak_hbm()
+    achieved = bwd_bytes * n / (ms_step / 1e3) / 1e9
+    return {
+        "metric": "Msplats/s (projection backward)",
+        "value": world * n * args.steps / (ms_total / 1e3) / 1e6, "unit": "Msplats/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 adjoint, f32 I/O",
+        "data": "synthetic (seeded mulberry32 + Box-Muller; upstream N(0, 1))",
+        "config": {"workload": f"backward: {n} splats, SH 3 fp32, Gaussian-mixture centres, 1920x1080 fov 50; "
+                               "gradient of mean2d/conic/opacity/rgb w.r.t. centres, ln scales, quaternions, "
+                               "opacities and colour rows",
+                   "n": n, "parallelism": f"replicas{world}", "l2": "inputs 236 MB > 126 MB L2 (no flush)",
+                   "forward_ms": fwd_step, "backward_over_forward": ms_step / fwd_step,
+                   "backward_bytes_per_splat": bwd_bytes},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_project_backward (raw, SH 3, 1 eye)",
+                     "bytes_per_splat": bwd_bytes, "peak_kind": peak_kind},
+        "e2e": None, "e2e_note": "device-resident tensors (a training step's layout)",
+        "gpu_launches": launches,
+        "clocks": clock_info,
+    }
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -381,7 +448,7 @@ def main():
         if world > 1:
             from datetime import timedelta
             dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
-        run = run_batched if args.workload == "batched" else run_stereo
+        run = {"batched": run_batched, "stereo": run_stereo, "backward": run_backward}[args.workload]
         line = run(args, world, rank, local, device)
         if rank == 0:
             print(json.dumps(line))

@@ -406,14 +406,16 @@ DEFAULT_OUTPUTS = ("mean2d", "conic", "depth", "opacity", "rgb", "keys")
 
 
 def project_collection(objects, camera, params=None, sort_bits=24, pass_="full", cull_keys=False,
-                       outputs=DEFAULT_OUTPUTS, device="cuda", ctx=None):
+                       outputs=DEFAULT_OUTPUTS, device="cuda", ctx=None, out=None):
     """projectCollection with the ewa method: outputs (per eye [E][n][...],
-    words [n][4E], keys [n]) as CUDA tensors (device=None: numpy)."""
+    words [n][4E], keys [n]) as CUDA tensors (device=None: numpy), or into
+    `out` (a dict of such arrays) when given."""
     params = params or SplatParams()
     n = sum(o.count for o in objects)
     eyes = len(camera.eyes)
     names = ("keys",) if pass_ == "keys" else tuple(outputs)
-    out = _alloc_outputs(names, n, eyes, device)
+    if out is None:
+        out = _alloc_outputs(names, n, eyes, device)
     objs, keep = _c_objects(objects)
     cam = camera.to_c(_abi)
     prm = params.to_c()

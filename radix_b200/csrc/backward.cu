@@ -23,6 +23,7 @@ namespace rdx {
 namespace {
 
 constexpr int kBwdThreads = 128;
+constexpr int kBwdBlocksPerSm = 3;  // up to 168 registers a thread
 
 template <int DEG>
 struct Coeffs {
@@ -94,7 +95,7 @@ __device__ __forceinline__ double colour_value(const void* colors, uint64_t i, i
 }
 
 template <int DEG, int CDT, int EYES>
-__global__ void __launch_bounds__(kBwdThreads) k_project_backward(const ProjDesc* __restrict__ descs,
+__global__ void __launch_bounds__(kBwdThreads, kBwdBlocksPerSm) k_project_backward(const ProjDesc* __restrict__ descs,
                                                                   const GradsOut* __restrict__ grads, int n_desc,
                                                                   uint32_t total_chunks, GradsIn in) {
   constexpr int K = Coeffs<DEG>::value;
@@ -128,6 +129,17 @@ __global__ void __launch_bounds__(kBwdThreads) k_project_backward(const ProjDesc
     if (__ldg(in.fwd_opacity + (uint64_t)v * sd.out_n + gi) != 0.0f) drawn |= 1u << v;
   }
   any = drawn != 0;
+  if (!any) {  // drawn by no eye: the outputs are constants
+    if (go_.centers) go_.centers[i * 3] = go_.centers[i * 3 + 1] = go_.centers[i * 3 + 2] = 0.0f;
+    if (go_.log_scales) go_.log_scales[i * 3] = go_.log_scales[i * 3 + 1] = go_.log_scales[i * 3 + 2] = 0.0f;
+    if (go_.quats) reinterpret_cast<float4*>(go_.quats)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (go_.opacities) go_.opacities[i] = 0.0f;
+    if (go_.colors) {
+#pragma unroll
+      for (int c = 0; c < kRow; c++) go_.colors[i * kRow + c] = 0.0f;
+    }
+    return;
+  }
 
   // the splat
   const double cx = __ldg(tb.centers + i * 3), cy = __ldg(tb.centers + i * 3 + 1), cz = __ldg(tb.centers + i * 3 + 2);
