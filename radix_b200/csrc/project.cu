@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
           const double coc = e.ortho ? coc_view * focal_pixels : coc_view * focal_pixels / depth;
           blur = fmin(fmax(coc * coc, blur), (double)p.max_pixel_radius * p.max_pixel_radius);
         }
-        double a_d = 0.0, b_d = 0.0, d_d = 0.0, det_d = 1.0, opacity_cd = 0.0;
+        double a_d = 0.0, b_d = 0.0, d_d = 0.0, det_d = 1.0, inv_det = 1.0, opacity_cd = 0.0;
         float scale1 = 0.f, scale2 = 0.f, angle = 0.f;
         if (ok) {
           // J (projections.tsl.ts:108-118)
@@ -457,8 +457,13 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
           det_d = det_t + full * (ra + rd) + full * full;
           a_d = ra + full;
           d_d = rd + full;
-          opacity_cd = op * sqrt(fmax(0.0, det_orig / det_d));
-          const double contribution = opacity_cd * 6.283185307179586 * sqrt(fmax(0.0, det_d));
+          inv_det = 1.0 / det_d;
+          opacity_cd = op * sqrt(fmax(0.0, det_orig * inv_det));
+          // contribution >= minContribution holds for any non-NaN value when the bound is <= 0, and a NaN
+          // opacity already fails the minAlpha test: the square root is needed only for a positive bound
+          const bool contributes =
+              p.min_contribution <= 0.0f ||
+              opacity_cd * 6.283185307179586 * sqrt(fmax(0.0, det_d)) >= (double)p.min_contribution;
           // boundFromCov (projection.tsl.ts:223-240)
           const float a = (float)a_d, b = (float)b_d, d = (float)d_d, det = (float)det_d;
           const float half = (a - d) * 0.5f;
@@ -467,7 +472,7 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
           scale1 = fminf(p.max_pixel_radius, std_dev * sqrtf(fmaxf(eigen1, 0.0f)));
           scale2 = fminf(p.max_pixel_radius, std_dev * sqrtf(eigen2));
           const bool bound_ok = scale1 >= p.min_pixel_radius || scale2 >= p.min_pixel_radius;
-          if (bound_ok) {
+          if (bound_ok && (out.radii || out.words)) {  // the angle is an output of the words and radii only
             float vx, vy;
             if (fabsf(a - eigen1) >= fabsf(d - eigen1)) {
               vx = b;
@@ -488,12 +493,11 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
             angle = atan2f(vy, vx);
             if (angle < 0.0f) angle += 3.14159265358979f;
           }
-          ok = opacity_cd >= (double)p.min_alpha && contribution >= (double)p.min_contribution && bound_ok;
+          ok = opacity_cd >= (double)p.min_alpha && contributes && bound_ok;
         }
         if (ok) {
           const double inv_w = 1.0 / clw;
           const double ndcx = clx * inv_w, ndcy = cly * inv_w;
-          const double inv_det = 1.0 / det_d;
           if (out.mean2d) {
             reinterpret_cast<float2*>(out.mean2d)[ei] =
                 make_float2((float)((ndcx + 1.0) * 0.5 * sd.width), (float)((ndcy + 1.0) * 0.5 * sd.height));
