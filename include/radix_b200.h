@@ -39,8 +39,14 @@ extern "C" {
 #define RDX_ERR_NOMEM 6        /* device or pinned host allocation failed */
 
 /* Splat table layouts */
-#define RDX_LAYOUT_RAW 0  /* float32 columns (3DGS parameters) */
-#define RDX_LAYOUT_EXT 1  /* Radix extSplats (2 x uint32x4) + extSh texels */
+#define RDX_LAYOUT_RAW 0     /* float32 columns (3DGS parameters) */
+#define RDX_LAYOUT_EXT 1     /* Radix extSplats (2 x uint32x4) */
+#define RDX_LAYOUT_PACKED 2  /* Radix packedSplats (uint32x4) */
+#define RDX_LAYOUT_COV 3     /* Radix covSplats (2 x uint32x4) */
+
+/* SH codecs of the ext / packed / cov layouts (src/core/sh.ts:13-24) */
+#define RDX_SH_EXT 0     /* one ext rgb word per coefficient */
+#define RDX_SH_PACKED 1  /* per band a scale byte, then a sint8 per value */
 
 /* Element types of a raw table's colour block */
 #define RDX_DTYPE_F32 0
@@ -65,17 +71,25 @@ typedef struct rdx_ctx rdx_ctx;
  *                1..sh_degree, coefficient-major RGB (src/core/sh.ts:7-11).
  *   Rows of colors must start 4-byte aligned; other columns as their type.
  *
- * RDX_LAYOUT_EXT: Radix's ArrayData columns, drop-in
- *   ext_a, ext_b uint32 [count][4]    (src/core/splats.ts:10-24)
- *   ext_sh[t]    uint32 [count][4]    texel channel t (extShA, extShB, ...),
- *                one ext rgb word per SH coefficient (src/core/sh.ts:114-135);
- *                ceil(K / 4) channels for degree sh_degree.
+ * RDX_LAYOUT_EXT / RDX_LAYOUT_COV: Radix's ArrayData columns, drop-in
+ *   ext_a, ext_b uint32 [count][4]    extA / extB, or covA / covB
+ *                (src/core/splats.ts:10-32)
+ * RDX_LAYOUT_PACKED:
+ *   packed       uint32 [count][4]    (src/core/splats.ts:28-32)
+ *   packed_encoding  rgbMin, rgbMax, lnScaleMin, lnScaleMax (the bundle's
+ *                meta.encoding; defaults 0, 1, -12, 9)
+ * SH of these layouts, in codec sh_codec (src/core/sh.ts:13-24):
+ *   ext_sh[t]    uint32 [count][4]    per-splat texel channel t (<codec>ShA,
+ *                <codec>ShB, ...), or, when sh_palette is set,
+ *   sh_palette   uint32 [entries * sh_stride][4]  an ShPalette's shEntries,
+ *   sh_label     uint16 [count]       each splat's entry (labels past
+ *                sh_palette_size read the last entry).
  */
 typedef struct rdx_table {
-  int32_t layout;      /* RDX_LAYOUT_RAW or RDX_LAYOUT_EXT */
+  int32_t layout;      /* RDX_LAYOUT_* */
   int32_t sh_degree;   /* 0..4: SH bands stored above the base colour */
   int32_t color_dtype; /* raw only: RDX_DTYPE_F32 or RDX_DTYPE_F16 */
-  int32_t reserved;
+  int32_t sh_codec;    /* ext / packed / cov: RDX_SH_EXT or RDX_SH_PACKED */
   uint64_t count;
   const float* centers;
   const float* log_scales;
@@ -85,6 +99,12 @@ typedef struct rdx_table {
   const uint32_t* ext_a;
   const uint32_t* ext_b;
   const uint32_t* ext_sh[6];
+  const uint32_t* packed;
+  float packed_encoding[4];
+  const uint32_t* sh_palette;
+  const uint16_t* sh_label;
+  uint32_t sh_stride;        /* texels per palette entry */
+  uint32_t sh_palette_size;  /* palette entries */
 } rdx_table;
 
 /*

@@ -234,10 +234,15 @@ uint32_t orc_encode_oct(const double v[3], int bits) { /* encoding.ts:33-47 */
   return code == 0 ? all_ones : code;
 }
 
-void orc_decode_quat_oct32(uint32_t code, double q[4]) { /* encoding.ts:101-110, axis 10+10, angle 12 */
+/* A quaternion code: an octahedral axis of axis_bits + axis_bits, then the
+   angle 0..pi in angle_bits (encoding.ts:73-111; QuatOct32 = 10 + 10 + 12,
+   QuatOct24 = 8 + 8 + 8) */
+void orc_decode_quat_oct(uint32_t code, int axis_bits, int angle_bits, double q[4]) {
+  const uint32_t axis_mask = (uint32_t)((1ull << (2 * axis_bits)) - 1u);
+  const uint32_t angle_max = (1u << angle_bits) - 1u;
   double axis[3];
-  orc_decode_oct(code & 0xfffffu, 10, axis);
-  double angle = (double)((code >> 20) & 4095u) / 4095.0 * PI;
+  orc_decode_oct(code & axis_mask, axis_bits, axis);
+  double angle = (double)((code >> (2 * axis_bits)) & angle_max) / (double)angle_max * PI;
   double s = sin(angle / 2.0);
   q[0] = axis[0] * s;
   q[1] = axis[1] * s;
@@ -245,14 +250,23 @@ void orc_decode_quat_oct32(uint32_t code, double q[4]) { /* encoding.ts:101-110,
   q[3] = cos(angle / 2.0);
 }
 
-uint32_t orc_encode_quat_oct32(const double q[4]) { /* encoding.ts:86-99 */
+uint32_t orc_encode_quat_oct(const double q[4], int axis_bits, int angle_bits) {
   double len = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
   if (!(len > 0)) return 0;
   double s = (q[3] < 0 ? -1.0 : 1.0) / len;
   double axis[3] = {q[0] * s, q[1] * s, q[2] * s};
   double angle = 2.0 * acos(fmin(1.0, q[3] * s));
-  uint32_t angle_code = (uint32_t)js_round(angle / PI * 4095.0);
-  return orc_encode_oct(axis, 10) | (angle_code << 20);
+  uint32_t angle_code = (uint32_t)js_round(angle / PI * (double)((1u << angle_bits) - 1u));
+  return orc_encode_oct(axis, axis_bits) | (angle_code << (2 * axis_bits));
+}
+
+void orc_decode_quat_oct32(uint32_t code, double q[4]) { orc_decode_quat_oct(code, 10, 12, q); }
+
+uint32_t orc_encode_quat_oct32(const double q[4]) { return orc_encode_quat_oct(q, 10, 12); }
+
+static uint32_t encode_unorm8(double v) { /* encoding.ts:204-206 */
+  double r = js_round(v * 255.0);
+  return (uint32_t)(r < 0 ? 0 : (r > 255 ? 255 : r));
 }
 
 /* ---- spherical harmonics: src/core/sh.ts:362-407 ---- */
@@ -311,10 +325,61 @@ static double load_color(const rdx_table* t, uint64_t i, int j) {
   return (double)((const float*)t->colors)[at];
 }
 
+/* SH scale byte: 0 = zero, else 2^((code - 192) / 16) (sh.ts:70-87) */
+static double decode_sh_scale(uint32_t code) { return code == 0 ? 0.0 : pow(2.0, ((double)code - 192.0) / 16.0); }
+
+static uint32_t encode_sh_scale(double max) {
+  if (!(max > 0)) return 0;
+  double c = ceil(log2(max) * 16.0) + 192.0;
+  uint32_t code = (uint32_t)(c < 1 ? 1 : (c > 255 ? 255 : c));
+  while (code < 255 && decode_sh_scale(code) < max) code++;
+  return code;
+}
+
+static const int PACKED_BAND_BYTES[4] = {10, 16, 22, 28}; /* sh.ts:62 */
+
+/* Word j of splat i's SH entry: per-splat texel channels, or its palette
+   entry (sh.tsl.ts:219-233; a label past the palette reads its last entry) */
+static uint32_t sh_word(const rdx_table* t, uint64_t i, int j) {
+  if (t->sh_palette) {
+    uint64_t label = t->sh_label[i];
+    if (t->sh_palette_size > 0 && label >= t->sh_palette_size) label = t->sh_palette_size - 1;
+    return t->sh_palette[(label * t->sh_stride) * 4 + (uint64_t)j];
+  }
+  return t->ext_sh[j >> 2][i * 4 + (uint64_t)(j & 3)];
+}
+
+/* The coefficients of splat i's entry in the table's codec (sh.ts:137-170) */
+static void load_sh_words(const rdx_table* t, uint64_t i, double* sh) {
+  const int deg = t->sh_degree;
+  if (t->sh_codec == RDX_SH_PACKED) {
+    int byte = 0;
+    for (int band = 0; band < deg; band++) {
+      const int first = SH_COEFFS[band] * 3, end = SH_COEFFS[band + 1] * 3;
+      uint32_t code = (sh_word(t, i, byte >> 2) >> ((byte & 3) * 8)) & 0xffu;
+      double scale = decode_sh_scale(code) / 127.0;
+      for (int v = first; v < end; v++) {
+        int b = byte + 1 + v - first;
+        int32_t sb = (int32_t)((sh_word(t, i, b >> 2) >> ((b & 3) * 8)) & 0xffu);
+        if (sb > 127) sb -= 256;
+        sh[v] = (double)sb * scale;
+      }
+      byte += PACKED_BAND_BYTES[band];
+    }
+  } else {
+    for (int c = 0; c < SH_COEFFS[deg]; c++) orc_decode_ext_rgb(sh_word(t, i, c), &sh[c * 3]);
+  }
+}
+
+static double decode_correlation(double e) { /* splats.ts:231-233 */
+  return e == 0.0 ? 0.0 : (e > 0 ? -1.0 : 1.0) * exp(-fabs(e));
+}
+
 void orc_load_splat(const rdx_table* t, uint64_t i, orc_splat* s) {
   s->sh_degree = t->sh_degree;
+  s->has_cov = 0;
   const int k = SH_COEFFS[t->sh_degree];
-  if (t->layout == RDX_LAYOUT_EXT) { /* splats.ts:188-197 */
+  if (t->layout == RDX_LAYOUT_EXT || t->layout == RDX_LAYOUT_COV) { /* splats.ts:188-197, 249-266 */
     const uint32_t* a = t->ext_a + i * 4;
     const uint32_t* b = t->ext_b + i * 4;
     for (int c = 0; c < 3; c++) {
@@ -324,14 +389,42 @@ void orc_load_splat(const rdx_table* t, uint64_t i, orc_splat* s) {
     }
     s->opacity = (double)(a[3] >> 24) / 128.0; /* encoding.ts:213-215 */
     orc_decode_ext_rgb(b[0], s->rgb);
-    s->scales[0] = exp(orc_decode_half(b[1] & 0xffffu));
-    s->scales[1] = exp(orc_decode_half(b[1] >> 16));
-    s->scales[2] = exp(orc_decode_half(b[2] & 0xffffu));
-    orc_decode_quat_oct32(b[3], s->quat);
-    for (int c = 0; c < k; c++) { /* sh.ts:114-135: one ext rgb word per coefficient */
-      uint32_t w = t->ext_sh[c >> 2][i * 4 + (uint64_t)(c & 3)];
-      orc_decode_ext_rgb(w, &s->sh[c * 3]);
+    if (t->layout == RDX_LAYOUT_EXT) {
+      s->scales[0] = exp(orc_decode_half(b[1] & 0xffffu));
+      s->scales[1] = exp(orc_decode_half(b[1] >> 16));
+      s->scales[2] = exp(orc_decode_half(b[2] & 0xffffu));
+      orc_decode_quat_oct32(b[3], s->quat);
+    } else {
+      const double xx = exp(orc_decode_half(b[1] & 0xffffu)), yy = exp(orc_decode_half(b[1] >> 16)),
+                   zz = exp(orc_decode_half(b[2] & 0xffffu));
+      s->cov[0] = xx;
+      s->cov[1] = yy;
+      s->cov[2] = zz;
+      s->cov[3] = decode_correlation(orc_decode_half(b[2] >> 16)) * sqrt(xx * yy);
+      s->cov[4] = decode_correlation(orc_decode_half(b[3] & 0xffffu)) * sqrt(xx * zz);
+      s->cov[5] = decode_correlation(orc_decode_half(b[3] >> 16)) * sqrt(yy * zz);
+      s->has_cov = 1;
+      s->scales[0] = s->scales[1] = s->scales[2] = 1.0;
+      s->quat[0] = s->quat[1] = s->quat[2] = 0.0;
+      s->quat[3] = 1.0;
     }
+    if (k) load_sh_words(t, i, s->sh);
+  } else if (t->layout == RDX_LAYOUT_PACKED) { /* packedCodec.decode, splats.ts:288-306 */
+    const uint32_t* p = t->packed + i * 4;
+    const double rmin = t->packed_encoding[0], rmax = t->packed_encoding[1];
+    const double lmin = t->packed_encoding[2], lmax = t->packed_encoding[3];
+    const double range = rmax - rmin, step = (lmax - lmin) / 254.0;
+    for (int c = 0; c < 3; c++) s->rgb[c] = rmin + ((double)((p[0] >> (8 * c)) & 0xffu) / 255.0) * range;
+    s->opacity = (double)(p[0] >> 24) / 255.0;
+    s->center[0] = orc_decode_half(p[1] & 0xffffu);
+    s->center[1] = orc_decode_half(p[1] >> 16);
+    s->center[2] = orc_decode_half(p[2] & 0xffffu);
+    for (int c = 0; c < 3; c++) {
+      uint32_t code = (p[3] >> (8 * c)) & 0xffu;
+      s->scales[c] = code == 0 ? 0.0 : exp(lmin + (double)(code - 1) * step);
+    }
+    orc_decode_quat_oct((p[2] >> 16) | ((p[3] >> 24) << 16), 8, 8, s->quat);
+    if (k) load_sh_words(t, i, s->sh);
   } else {
     for (int c = 0; c < 3; c++) {
       s->center[c] = t->centers[i * 3 + c];
@@ -576,6 +669,10 @@ static void project_one(const orc_splat* s, const object_setup* o, const eye_set
   double Mt[9], cov[9];
   m3_transpose(M, Mt);
   m3_mul(M, Mt, cov);
+  if (s->has_cov) { /* cov layout: the stored covariance (splats.tsl.ts:104-118) */
+    const double c6[9] = {s->cov[0], s->cov[3], s->cov[4], s->cov[3], s->cov[1], s->cov[5], s->cov[4], s->cov[5], s->cov[2]};
+    memcpy(cov, c6, sizeof(cov));
+  }
   /* transformCov: splatTransform.tsl.ts:120-140 */
   double ch[3];
   xform_point(o->a, s->center, ch);
@@ -1190,5 +1287,129 @@ int orc_project_backward(const rdx_object* objects, int n_objects, const rdx_cam
     if (gout->colors) memcpy(gout->colors + gi * 75, gcol, sizeof(gcol));
   }
   free(objs);
+  return 0;
+}
+
+/* ---- fixtures of the packed and cov layouts and of the SH codecs ---- */
+
+/* packedCodec.encode (splats.ts:279-286) of a raw table */
+int orc_encode_packed_table(const rdx_table* raw, const float encoding[4], uint32_t* packed) {
+  if (raw->layout != RDX_LAYOUT_RAW) return -1;
+  const double rmin = encoding[0], rmax = encoding[1], lmin = encoding[2], lmax = encoding[3];
+  const double range = rmax - rmin, step = (lmax - lmin) / 254.0;
+  for (uint64_t i = 0; i < raw->count; i++) {
+    orc_splat s;
+    orc_load_splat(raw, i, &s);
+    uint32_t* p = packed + i * 4;
+    uint32_t rgb = 0;
+    for (int c = 0; c < 3; c++) rgb |= encode_unorm8((s.rgb[c] - rmin) / range) << (8 * c);
+    const uint32_t quat = orc_encode_quat_oct(s.quat, 8, 8);
+    p[0] = rgb | (encode_unorm8(s.opacity) << 24);
+    p[1] = orc_encode_half(s.center[0]) | (orc_encode_half(s.center[1]) << 16);
+    p[2] = orc_encode_half(s.center[2]) | ((quat & 0xffffu) << 16);
+    uint32_t w = 0;
+    for (int c = 0; c < 3; c++) {
+      const double v = s.scales[c];
+      uint32_t code = 0;
+      if (v > 0) {
+        double r = js_round((log(v) - lmin) / step) + 1.0;
+        code = (uint32_t)(r < 1 ? 1 : (r > 255 ? 255 : r));
+      }
+      w |= code << (8 * c);
+    }
+    p[3] = w | ((quat >> 16) << 24);
+  }
+  return 0;
+}
+
+static double encode_correlation(double value, double a, double b) { /* splats.ts:223-229 */
+  double c = value / sqrt(a * b);
+  c = c < -1 ? -1 : (c > 1 ? 1 : c);
+  if (c == 0 || !isfinite(c)) return 0.0;
+  double l = log(fabs(c));
+  l = l < -100 ? -100 : (l > -1e-7 ? -1e-7 : l);
+  return (c > 0 ? 1.0 : -1.0) * l;
+}
+
+/* storeCovFields (splats.ts:236-243) of a raw table: the covariance of its
+   scales and rotation, the base rgb and the LoD opacity byte */
+int orc_encode_cov_table(const rdx_table* raw, uint32_t* cov_a, uint32_t* cov_b) {
+  if (raw->layout != RDX_LAYOUT_RAW) return -1;
+  for (uint64_t i = 0; i < raw->count; i++) {
+    orc_splat s;
+    orc_load_splat(raw, i, &s);
+    double qx = s.quat[0], qy = s.quat[1], qz = s.quat[2], qw = s.quat[3];
+    double ql = sqrt(qx * qx + qy * qy + qz * qz + qw * qw);
+    if (ql > 0) {
+      qx /= ql;
+      qy /= ql;
+      qz /= ql;
+      qw /= ql;
+    } else {
+      qx = qy = qz = 0;
+      qw = 1;
+    }
+    const double sx = s.scales[0], sy = s.scales[1], sz = s.scales[2];
+    const double M[9] = {
+        sx * (1 - 2 * (qy * qy + qz * qz)), sy * 2 * (qx * qy - qw * qz), sz * 2 * (qx * qz + qw * qy),
+        sx * 2 * (qx * qy + qw * qz), sy * (1 - 2 * (qx * qx + qz * qz)), sz * 2 * (qy * qz - qw * qx),
+        sx * 2 * (qx * qz - qw * qy), sy * 2 * (qy * qz + qw * qx), sz * (1 - 2 * (qx * qx + qy * qy)),
+    };
+    double Mt[9], cov[9];
+    m3_transpose(M, Mt);
+    m3_mul(M, Mt, cov);
+    const double xx = cov[0], yy = cov[4], zz = cov[8];
+    uint32_t* a = cov_a + i * 4;
+    uint32_t* b = cov_b + i * 4;
+    for (int c = 0; c < 3; c++) {
+      float f = (float)s.center[c];
+      memcpy(&a[c], &f, 4);
+    }
+    a[3] = encode_lod_opacity(s.opacity) << 24;
+    b[0] = orc_encode_ext_rgb(s.rgb);
+    b[1] = orc_encode_half(log(xx)) | (orc_encode_half(log(yy)) << 16);
+    b[2] = orc_encode_half(log(zz)) | (orc_encode_half(encode_correlation(cov[1], xx, yy)) << 16);
+    b[3] = orc_encode_half(encode_correlation(cov[2], xx, zz)) | (orc_encode_half(encode_correlation(cov[5], yy, zz)) << 16);
+  }
+  return 0;
+}
+
+int orc_sh_words(int codec, int degree) {
+  static const int PACKED_BYTES[5] = {0, 10, 26, 48, 76};
+  if (degree < 0 || degree > 4) return 0;
+  return codec == RDX_SH_PACKED ? (PACKED_BYTES[degree] + 3) / 4 : SH_COEFFS[degree];
+}
+
+/* The codec words of a raw table's SH coefficients (sh.ts:137-160), [count][stride] */
+int orc_encode_sh(const rdx_table* raw, int codec, uint32_t* words, int stride) {
+  if (raw->layout != RDX_LAYOUT_RAW) return -1;
+  const int deg = raw->sh_degree;
+  if (stride < orc_sh_words(codec, deg)) return -1;
+  for (uint64_t i = 0; i < raw->count; i++) {
+    orc_splat s;
+    orc_load_splat(raw, i, &s);
+    uint32_t* out = words + i * (uint64_t)stride;
+    memset(out, 0, (size_t)stride * 4);
+    if (codec == RDX_SH_PACKED) {
+      int byte = 0;
+      for (int band = 0; band < deg; band++) {
+        const int first = SH_COEFFS[band] * 3, end = SH_COEFFS[band + 1] * 3;
+        double max = 0.0;
+        for (int v = first; v < end; v++) max = fmax(max, fabs(s.sh[v]));
+        const uint32_t code = encode_sh_scale(max);
+        const double scale = decode_sh_scale(code);
+        out[byte >> 2] |= code << ((byte & 3) * 8);
+        for (int v = first; v < end; v++) {
+          int b = byte + 1 + v - first;
+          double q = scale > 0 ? js_round(s.sh[v] / scale * 127.0) : 0.0;
+          int32_t qi = (int32_t)(q < -127 ? -127 : (q > 127 ? 127 : q));
+          out[b >> 2] |= ((uint32_t)qi & 0xffu) << ((b & 3) * 8);
+        }
+        byte += PACKED_BAND_BYTES[band];
+      }
+    } else {
+      for (int c = 0; c < SH_COEFFS[deg]; c++) out[c] = orc_encode_ext_rgb(&s.sh[c * 3]);
+    }
+  }
   return 0;
 }

@@ -38,6 +38,8 @@ void orc_decode_oct(uint32_t code, int bits, double out[3]);
 uint32_t orc_encode_oct(const double v[3], int bits);
 void orc_decode_quat_oct32(uint32_t code, double q[4]);
 uint32_t orc_encode_quat_oct32(const double q[4]);
+void orc_decode_quat_oct(uint32_t code, int axis_bits, int angle_bits, double q[4]);
+uint32_t orc_encode_quat_oct(const double q[4], int axis_bits, int angle_bits);
 
 /* src/core/sh.ts:362-407 */
 void orc_sh_basis(const double dir[3], double out[24]);
@@ -52,6 +54,8 @@ typedef struct orc_splat {
   double rgb[3];
   double sh[24 * 3];
   int sh_degree;
+  double cov[6];      /* cov layout: xx, yy, zz, xy, xz, yz (then scales and quat are unused) */
+  int has_cov;
 } orc_splat;
 void orc_load_splat(const rdx_table* table, uint64_t index, orc_splat* out);
 
@@ -118,6 +122,14 @@ uint32_t orc_encode_angle12(double angle);
 /* A raw table encoded as Radix's ext layout (src/core/splats.ts:150-181 store
    path, src/core/sh.ts:114-135 ext SH), for fixtures of the ext reader */
 int orc_encode_ext_table(const rdx_table* raw, uint32_t* ext_a, uint32_t* ext_b, uint32_t* const* ext_sh);
+
+/* Fixtures: packedCodec.encode (src/core/splats.ts:279-286) and
+   storeCovFields (splats.ts:236-243) of a raw table, and its SH coefficients
+   in a codec (src/core/sh.ts:137-160), `stride` words per splat */
+int orc_encode_packed_table(const rdx_table* raw, const float encoding[4], uint32_t* packed);
+int orc_encode_cov_table(const rdx_table* raw, uint32_t* cov_a, uint32_t* cov_b);
+int orc_sh_words(int codec, int degree);
+int orc_encode_sh(const rdx_table* raw, int codec, uint32_t* words, int stride);
 
 /* The reference's defaults (src/render/splatParams.ts:68-72) */
 void orc_params_default(rdx_params* p);

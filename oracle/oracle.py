@@ -28,6 +28,12 @@ class orc_grads_out(ctypes.Structure):
     _fields_ = [(name, ctypes.c_void_p) for name in ("centers", "log_scales", "quats", "opacities", "colors")]
 
 
+class orc_splat(ctypes.Structure):
+    _fields_ = [("center", ctypes.c_double * 3), ("scales", ctypes.c_double * 3), ("quat", ctypes.c_double * 4),
+                ("opacity", ctypes.c_double), ("rgb", ctypes.c_double * 3), ("sh", ctypes.c_double * 72),
+                ("sh_degree", ctypes.c_int), ("cov", ctypes.c_double * 6), ("has_cov", ctypes.c_int)]
+
+
 class orc_outputs(ctypes.Structure):
     _fields_ = [(name, ctypes.c_void_p) for name in
                 ("mean2d", "conic", "depth", "opacity", "rgb", "radii", "words", "keys", "distance", "visible")]
@@ -64,6 +70,13 @@ def lib():
                                 ctypes.POINTER(_abi.rdx_params), i, i, i, ctypes.POINTER(orc_outputs)]),
             "orc_encode_ext_table": (i, [ctypes.POINTER(_abi.rdx_table), vp, vp, vp]),
             "orc_sh_basis_grad": (None, [vp, vp]),
+            "orc_load_splat": (None, [ctypes.POINTER(_abi.rdx_table), ctypes.c_uint64, ctypes.POINTER(orc_splat)]),
+            "orc_encode_packed_table": (i, [ctypes.POINTER(_abi.rdx_table), vp, vp]),
+            "orc_encode_cov_table": (i, [ctypes.POINTER(_abi.rdx_table), vp, vp]),
+            "orc_sh_words": (i, [i, i]),
+            "orc_encode_sh": (i, [ctypes.POINTER(_abi.rdx_table), i, vp, i]),
+            "orc_decode_quat_oct": (None, [u32, i, i, vp]),
+            "orc_encode_quat_oct": (u32, [vp, i, i]),
             "orc_project_backward": (i, [ctypes.POINTER(_abi.rdx_object), i, ctypes.POINTER(_abi.rdx_camera),
                                          ctypes.POINTER(_abi.rdx_params), ctypes.POINTER(orc_grads_in),
                                          ctypes.POINTER(orc_grads_out), i]),
@@ -234,3 +247,63 @@ def sh_basis_grad(d):
     out = np.zeros((24, 3))
     lib().orc_sh_basis_grad(_p(np.ascontiguousarray(d, dtype=np.float64)), _p(out))
     return out
+
+
+def encode_packed(raw, encoding=(0.0, 1.0, -12.0, 9.0)):
+    """packedCodec.encode of a numpy raw table dict: [n][4] uint32."""
+    import radix_b200 as rb
+    t = rb.Table.from_dict(raw)
+    out = np.zeros((t.count, 4), dtype=np.uint32)
+    enc = np.asarray(encoding, dtype=np.float32)
+    if lib().orc_encode_packed_table(ctypes.byref(t.c), _p(enc), _p(out)) != 0:
+        raise ValueError("orc_encode_packed_table failed")
+    return out
+
+
+def encode_cov(raw):
+    """storeCovFields of a numpy raw table dict: (covA, covB), [n][4] uint32 each."""
+    import radix_b200 as rb
+    t = rb.Table.from_dict(raw)
+    a = np.zeros((t.count, 4), dtype=np.uint32)
+    b = np.zeros((t.count, 4), dtype=np.uint32)
+    if lib().orc_encode_cov_table(ctypes.byref(t.c), _p(a), _p(b)) != 0:
+        raise ValueError("orc_encode_cov_table failed")
+    return a, b
+
+
+def encode_sh(raw, codec):
+    """A raw table's SH coefficients as codec words ("ext" / "packed"):
+    [n][texels * 4] uint32, zero padded to whole texels."""
+    import radix_b200 as rb
+    t = rb.Table.from_dict(raw)
+    c = _abi.RDX_SH_PACKED if codec == "packed" else _abi.RDX_SH_EXT
+    words = lib().orc_sh_words(c, raw["sh_degree"])
+    stride = (words + 3) // 4 * 4
+    out = np.zeros((t.count, max(stride, 4)), dtype=np.uint32)
+    if lib().orc_encode_sh(ctypes.byref(t.c), c, _p(out), out.shape[1]) != 0:
+        raise ValueError("orc_encode_sh failed")
+    return out[:, :stride] if stride else out[:, :0]
+
+
+def sh_channels(words):
+    """Codec words [n][4 * texels] as per-splat texel channels [n][4] each."""
+    return [np.ascontiguousarray(words[:, 4 * k:4 * k + 4]) for k in range(words.shape[1] // 4)]
+
+
+def sh_palette(words, stride):
+    """Entries' codec words [size][4 * texels] as an ShPalette's shEntries:
+    [size * stride][4], each entry `stride` texels (the tail zero)."""
+    size, w = words.shape
+    out = np.zeros((size, stride, 4), dtype=np.uint32)
+    out[:, :w // 4, :] = words.reshape(size, w // 4, 4)
+    return out.reshape(size * stride, 4)
+
+
+def load_splat(table, i):
+    """orc_load_splat of row i of a radix_b200.Table (numpy columns): a dict."""
+    sp = orc_splat()
+    lib().orc_load_splat(ctypes.byref(table.c), i, ctypes.byref(sp))
+    k = ((sp.sh_degree + 1) ** 2 - 1) * 3
+    return {"center": np.array(sp.center[:]), "scales": np.array(sp.scales[:]), "quat": np.array(sp.quat[:]),
+            "opacity": sp.opacity, "rgb": np.array(sp.rgb[:]), "sh": np.array(sp.sh[:k]),
+            "cov": np.array(sp.cov[:]) if sp.has_cov else None}

@@ -320,18 +320,59 @@ class Table:
         t.opacities, t.colors = _ptr(opacities), _ptr(colors)
         return cls(t, [centers, log_scales, quats, opacities, colors])
 
+    @staticmethod
+    def _sh(t, keep, sh, sh_degree, sh_codec, palette):
+        t.sh_degree = sh_degree
+        t.sh_codec = _abi.RDX_SH_PACKED if sh_codec == "packed" else _abi.RDX_SH_EXT
+        if palette is not None:
+            entries, labels, stride = palette
+            t.sh_palette, t.sh_label = _ptr(entries), _ptr(labels)
+            t.sh_stride = int(stride)
+            t.sh_palette_size = int(entries.shape[0]) // int(stride)
+            keep += [entries, labels]
+        for i, ch in enumerate(sh):
+            t.ext_sh[i] = _ptr(ch)
+        keep += list(sh)
+
     @classmethod
-    def ext(cls, ext_a, ext_b, ext_sh=(), sh_degree=0):
-        """extA / extB uint32x4 columns (src/core/splats.ts:10-24) and the extSh
-        texel channels (src/core/sh.ts:114-135), each [count][4] uint32."""
+    def ext(cls, ext_a, ext_b, ext_sh=(), sh_degree=0, sh_codec="ext", palette=None):
+        """extA / extB uint32x4 columns (src/core/splats.ts:10-24) and the SH
+        texel channels of codec sh_codec ("ext" or "packed"), each [count][4]
+        uint32, or palette = (entries [size * stride][4] uint32, labels [count]
+        uint16, stride) (src/core/sh.ts:13-24, 432-527)."""
         t = _abi.rdx_table()
         t.layout = _abi.RDX_LAYOUT_EXT
-        t.sh_degree = sh_degree
         t.count = int(ext_a.shape[0])
         t.ext_a, t.ext_b = _ptr(ext_a), _ptr(ext_b)
-        for i, ch in enumerate(ext_sh):
-            t.ext_sh[i] = _ptr(ch)
-        return cls(t, [ext_a, ext_b, *ext_sh])
+        keep = [ext_a, ext_b]
+        cls._sh(t, keep, ext_sh, sh_degree, sh_codec, palette)
+        return cls(t, keep)
+
+    @classmethod
+    def cov(cls, cov_a, cov_b, sh=(), sh_degree=0, sh_codec="ext", palette=None):
+        """covA / covB uint32x4 columns (src/core/splats.ts:25-27), SH as for ext."""
+        t = _abi.rdx_table()
+        t.layout = _abi.RDX_LAYOUT_COV
+        t.count = int(cov_a.shape[0])
+        t.ext_a, t.ext_b = _ptr(cov_a), _ptr(cov_b)
+        keep = [cov_a, cov_b]
+        cls._sh(t, keep, sh, sh_degree, sh_codec, palette)
+        return cls(t, keep)
+
+    PACKED_ENCODING = (0.0, 1.0, -12.0, 9.0)  # Splats.DEFAULT_PACKED_ENCODING (src/core/splats.ts:97)
+
+    @classmethod
+    def packed(cls, packed, encoding=PACKED_ENCODING, sh=(), sh_degree=0, sh_codec="ext", palette=None):
+        """The packed uint32x4 column (src/core/splats.ts:28-32) and its
+        encoding (rgbMin, rgbMax, lnScaleMin, lnScaleMax), SH as for ext."""
+        t = _abi.rdx_table()
+        t.layout = _abi.RDX_LAYOUT_PACKED
+        t.count = int(packed.shape[0])
+        t.packed = _ptr(packed)
+        t.packed_encoding[:] = [float(x) for x in encoding]
+        keep = [packed]
+        cls._sh(t, keep, sh, sh_degree, sh_codec, palette)
+        return cls(t, keep)
 
     @classmethod
     def from_dict(cls, d, to=None):

@@ -20,6 +20,10 @@ RDX_ERR_NOMEM = 6
 
 RDX_LAYOUT_RAW = 0
 RDX_LAYOUT_EXT = 1
+RDX_LAYOUT_PACKED = 2
+RDX_LAYOUT_COV = 3
+RDX_SH_EXT = 0
+RDX_SH_PACKED = 1
 RDX_DTYPE_F32 = 0
 RDX_DTYPE_F16 = 1
 RDX_PASS_FULL = 0
@@ -41,7 +45,7 @@ class rdx_table(ctypes.Structure):
         ("layout", ctypes.c_int32),
         ("sh_degree", ctypes.c_int32),
         ("color_dtype", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("sh_codec", ctypes.c_int32),
         ("count", ctypes.c_uint64),
         ("centers", ctypes.c_void_p),
         ("log_scales", ctypes.c_void_p),
@@ -51,6 +55,12 @@ class rdx_table(ctypes.Structure):
         ("ext_a", ctypes.c_void_p),
         ("ext_b", ctypes.c_void_p),
         ("ext_sh", ctypes.c_void_p * 6),
+        ("packed", ctypes.c_void_p),
+        ("packed_encoding", ctypes.c_float * 4),
+        ("sh_palette", ctypes.c_void_p),
+        ("sh_label", ctypes.c_void_p),
+        ("sh_stride", ctypes.c_uint32),
+        ("sh_palette_size", ctypes.c_uint32),
     ]
 
 

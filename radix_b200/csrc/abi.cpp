@@ -305,8 +305,15 @@ const int kShCoeffs[5] = {0, 3, 8, 15, 24};
 
 // ---- tables: checks and staging ----
 
+// SH texels per entry of a codec and degree (src/core/sh.ts:13-24)
+int sh_texels(int codec, int degree) {
+  static const int kPackedTexels[5] = {0, 1, 2, 3, 5};
+  if (degree <= 0) return 0;
+  return codec == RDX_SH_PACKED ? kPackedTexels[degree] : (kShCoeffs[degree] + 3) / 4;
+}
+
 struct TableBytes {
-  size_t centers, scales, quats, opacities, colors, ext, sh_texels;
+  size_t centers, scales, quats, opacities, colors, words, sh_texels;
 };
 
 TableBytes table_bytes(const rdx_table& t, uint64_t n) {
@@ -319,8 +326,8 @@ TableBytes table_bytes(const rdx_table& t, uint64_t n) {
     b.opacities = n * 4;
     b.colors = n * (size_t)(1 + k) * 3 * (t.color_dtype == RDX_DTYPE_F16 ? 2 : 4);
   } else {
-    b.ext = n * 16;
-    b.sh_texels = (size_t)((k + 3) / 4);
+    b.words = n * 16;  // one uint32x4 per splat and column
+    b.sh_texels = (size_t)sh_texels(t.sh_codec, t.sh_degree);
   }
   return b;
 }
@@ -331,28 +338,49 @@ size_t color_vec_bytes(const rdx_table& t) {
   return row % 16 == 0 ? 16 : (row % 8 == 0 ? 8 : (row % 4 == 0 ? 4 : 2));
 }
 
+const char* layout_name(int layout) {
+  switch (layout) {
+    case RDX_LAYOUT_EXT: return "ext";
+    case RDX_LAYOUT_PACKED: return "packed";
+    case RDX_LAYOUT_COV: return "cov";
+    default: return "raw";
+  }
+}
+
 int check_table(rdx_ctx* ctx, const rdx_table* t, int index) {
   if (!t) return fail(ctx, RDX_ERR_ARG, "object %d has no table", index);
-  if (t->layout != RDX_LAYOUT_RAW && t->layout != RDX_LAYOUT_EXT)
-    return fail(ctx, RDX_ERR_UNSUPPORTED, "table layout %d (raw 0 or ext 1)", t->layout);
+  if (t->layout < RDX_LAYOUT_RAW || t->layout > RDX_LAYOUT_COV)
+    return fail(ctx, RDX_ERR_UNSUPPORTED, "table layout %d (raw 0, ext 1, packed 2, cov 3)", t->layout);
   if (t->sh_degree < 0 || t->sh_degree > 4) return fail(ctx, RDX_ERR_ARG, "sh_degree %d (0 to 4)", t->sh_degree);
   if (t->layout == RDX_LAYOUT_RAW) {
     if (t->color_dtype != RDX_DTYPE_F32 && t->color_dtype != RDX_DTYPE_F16)
       return fail(ctx, RDX_ERR_ARG, "color_dtype %d", t->color_dtype);
     if (!t->centers || !t->log_scales || !t->quats || !t->opacities || !t->colors)
       return fail(ctx, RDX_ERR_ARG, "raw table of object %d: a column is NULL", index);
+    return RDX_OK;
+  }
+  const char* name = layout_name(t->layout);
+  if (t->layout == RDX_LAYOUT_PACKED) {
+    if (!t->packed) return fail(ctx, RDX_ERR_ARG, "packed table of object %d: the packed column is NULL", index);
+    if (!(t->packed_encoding[1] > t->packed_encoding[0]) || !(t->packed_encoding[3] > t->packed_encoding[2]))
+      return fail(ctx, RDX_ERR_ARG, "packed table of object %d: encoding ranges are empty", index);
+  } else if (!t->ext_a || !t->ext_b) {
+    return fail(ctx, RDX_ERR_ARG, "%s table of object %d: word column A or B is NULL", name, index);
+  }
+  if (t->sh_codec != RDX_SH_EXT && t->sh_codec != RDX_SH_PACKED)
+    return fail(ctx, RDX_ERR_ARG, "%s table of object %d: SH codec %d (ext 0, packed 1)", name, index, t->sh_codec);
+  const int texels = sh_texels(t->sh_codec, t->sh_degree);
+  if (t->sh_palette) {
+    if (!t->sh_label) return fail(ctx, RDX_ERR_ARG, "%s table of object %d: a palette without labels", name, index);
+    if (t->sh_palette_size == 0 || t->sh_stride < (uint32_t)texels)
+      return fail(ctx, RDX_ERR_ARG, "%s table of object %d: palette stride %u below the codec's %d texels", name, index,
+                  t->sh_stride, texels);
   } else {
-    if (!t->ext_a || !t->ext_b) return fail(ctx, RDX_ERR_ARG, "ext table of object %d: extA or extB is NULL", index);
-    for (int c = 0; c < (kShCoeffs[t->sh_degree] + 3) / 4; c++)
-      if (!t->ext_sh[c]) return fail(ctx, RDX_ERR_ARG, "ext table of object %d: SH texel channel %d is NULL", index, c);
+    for (int c = 0; c < texels; c++)
+      if (!t->ext_sh[c]) return fail(ctx, RDX_ERR_ARG, "%s table of object %d: SH texel channel %d is NULL", name, index, c);
   }
   return RDX_OK;
 }
-
-// A table whose columns are on the device: the caller's pointers, or staged copies of host columns
-struct Staged {
-  rdx::DevTable dev;
-};
 
 template <class T>
 const T* stage_column(rdx_ctx* ctx, Arena& a, const T* src, size_t bytes, size_t align, int* status) {
@@ -369,11 +397,13 @@ const T* stage_column(rdx_ctx* ctx, Arena& a, const T* src, size_t bytes, size_t
   return reinterpret_cast<const T*>(dst);
 }
 
+// A table whose columns are on the device: the caller's pointers, or staged copies of host columns
 rdx::DevTable stage_table(rdx_ctx* ctx, Arena& a, const rdx_table& t, int* status) {
   rdx::DevTable d{};
   d.layout = t.layout;
   d.sh_degree = t.sh_degree;
   d.color_dtype = t.color_dtype;
+  d.sh_codec = t.sh_codec;
   const uint64_t n = t.count;
   const TableBytes b = table_bytes(t, n);
   if (t.layout == RDX_LAYOUT_RAW) {
@@ -382,12 +412,43 @@ rdx::DevTable stage_table(rdx_ctx* ctx, Arena& a, const rdx_table& t, int* statu
     d.quats = stage_column(ctx, a, t.quats, b.quats, 16, status);
     d.opacities = stage_column(ctx, a, t.opacities, b.opacities, 4, status);
     d.colors = stage_column(ctx, a, reinterpret_cast<const char*>(t.colors), b.colors, color_vec_bytes(t), status);
+    return d;
+  }
+  if (t.layout == RDX_LAYOUT_PACKED) {
+    d.packed = stage_column(ctx, a, t.packed, b.words, 16, status);
+    for (int c = 0; c < 4; c++) d.packed_encoding[c] = t.packed_encoding[c];
   } else {
-    d.ext_a = stage_column(ctx, a, t.ext_a, b.ext, 16, status);
-    d.ext_b = stage_column(ctx, a, t.ext_b, b.ext, 16, status);
-    for (size_t c = 0; c < b.sh_texels; c++) d.ext_sh[c] = stage_column(ctx, a, t.ext_sh[c], b.ext, 16, status);
+    d.ext_a = stage_column(ctx, a, t.ext_a, b.words, 16, status);
+    d.ext_b = stage_column(ctx, a, t.ext_b, b.words, 16, status);
+  }
+  if (t.sh_palette) {
+    d.sh_palette = stage_column(ctx, a, t.sh_palette, (size_t)t.sh_palette_size * t.sh_stride * 16, 16, status);
+    d.sh_label = stage_column(ctx, a, t.sh_label, n * 2, 2, status);
+    d.sh_stride = t.sh_stride;
+    d.sh_palette_size = t.sh_palette_size;
+  } else {
+    for (size_t c = 0; c < b.sh_texels; c++) d.ext_sh[c] = stage_column(ctx, a, t.ext_sh[c], b.words, 16, status);
   }
   return d;
+}
+
+// Every column of the table is device memory
+bool all_device(const rdx_table& t) {
+  if (t.layout == RDX_LAYOUT_RAW) {
+    for (const void* p : {(const void*)t.centers, (const void*)t.log_scales, (const void*)t.quats,
+                          (const void*)t.opacities, t.colors})
+      if (!is_device_ptr(p)) return false;
+    return true;
+  }
+  if (t.layout == RDX_LAYOUT_PACKED) {
+    if (!is_device_ptr(t.packed)) return false;
+  } else if (!is_device_ptr(t.ext_a) || !is_device_ptr(t.ext_b)) {
+    return false;
+  }
+  if (t.sh_palette) return is_device_ptr(t.sh_palette) && is_device_ptr(t.sh_label);
+  for (int c = 0; c < sh_texels(t.sh_codec, t.sh_degree); c++)
+    if (!is_device_ptr(t.ext_sh[c])) return false;
+  return true;
 }
 
 rdx::DevParams dev_params(const rdx_params& p) {
@@ -565,7 +626,7 @@ int plan_views(rdx_ctx* ctx, Arena& a, const ViewRef* views, int n_views, const 
       const rdx_object& o = vw.objects[i];
       const rdx_table& t = *o.table;
       if (!staged.count(o.table)) staged[o.table] = stage_table(ctx, a, t, &status);
-      const int kind = t.layout * 100 + t.sh_degree * 10 + (t.layout == RDX_LAYOUT_RAW ? t.color_dtype : 0);
+      const int kind = t.layout * 100 + t.sh_degree * 10 + (t.layout == RDX_LAYOUT_RAW ? t.color_dtype : t.sh_codec);
       if (o.count > 0) {
         rdx::ProjDesc d = make_desc(*vw.camera, c, o, staged[o.table], *params, offset, n, bits, pass, cull_keys);
         d.segment = v;
@@ -1239,8 +1300,7 @@ int frame_common(rdx_ctx* ctx, const ViewRef* views, int n_views, const rdx_para
   for (int v = 0; v < n_views && !host_in; v++) {
     for (int i = 0; i < views[v].n_objects && !host_in; i++) {
       const rdx_table& t = *views[v].objects[i].table;
-      host_in = t.layout == RDX_LAYOUT_RAW ? any_host({t.centers, t.log_scales, t.quats, t.opacities, t.colors})
-                                           : any_host({t.ext_a, t.ext_b});
+      host_in = !all_device(t);
     }
   }
   return host_in || !plan.back.empty() || host_order || host_visible ? finish(ctx) : RDX_OK;
@@ -1285,19 +1345,6 @@ void free_batch(rdx_batch* b) {
   if (b->lookback) cudaFree(b->lookback);
   if (b->arena) cudaFree(b->arena);
   delete b;
-}
-
-bool all_device(const rdx_table& t) {
-  if (t.layout == RDX_LAYOUT_RAW) {
-    for (const void* p : {(const void*)t.centers, (const void*)t.log_scales, (const void*)t.quats,
-                          (const void*)t.opacities, t.colors})
-      if (!is_device_ptr(p)) return false;
-    return true;
-  }
-  if (!is_device_ptr(t.ext_a) || !is_device_ptr(t.ext_b)) return false;
-  for (int c = 0; c < (kShCoeffs[t.sh_degree] + 3) / 4; c++)
-    if (!is_device_ptr(t.ext_sh[c])) return false;
-  return true;
 }
 
 }  // namespace

@@ -86,13 +86,18 @@ __device__ __forceinline__ float4 decode_quat_oct32(uint32_t code) {
   return make_float4(x * s, y * s, z * s, c);
 }
 
-// QuatOct32 in float64 (the oracle's precision): src/core/encoding.ts:49-67, 101-110
-__device__ __forceinline__ void decode_quat_oct32_f64(uint32_t code, double q[4]) {
-  const uint32_t axis = code & 0xfffffu;
+// A quaternion code in float64 (the oracle's precision): an octahedral axis
+// of AXIS + AXIS bits, then the angle 0..pi in ANGLE bits
+// (src/core/encoding.ts:49-67, 101-110; QuatOct32 = 10 + 10 + 12, QuatOct24 = 8 + 8 + 8)
+template <int AXIS, int ANGLE>
+__device__ __forceinline__ void decode_quat_oct_f64(uint32_t code, double q[4]) {
+  constexpr uint32_t kMax = (1u << AXIS) - 1u;
+  constexpr uint32_t kAngleMax = (1u << ANGLE) - 1u;
+  const uint32_t axis = code & ((1u << (2 * AXIS)) - 1u);
   double x = 0.0, y = 0.0, z = 0.0;
   if (axis != 0u) {
-    x = (double)(axis & 1023u) / 1023.0 * 2.0 - 1.0;
-    y = (double)((axis >> 10) & 1023u) / 1023.0 * 2.0 - 1.0;
+    x = (double)(axis & kMax) / (double)kMax * 2.0 - 1.0;
+    y = (double)((axis >> AXIS) & kMax) / (double)kMax * 2.0 - 1.0;
     z = 1.0 - fabs(x) - fabs(y);
     const double t = fmax(-z, 0.0);
     x += x >= 0.0 ? -t : t;
@@ -102,7 +107,7 @@ __device__ __forceinline__ void decode_quat_oct32_f64(uint32_t code, double q[4]
     y /= len;
     z /= len;
   }
-  const double angle = (double)((code >> 20) & 4095u) / 4095.0 * 3.14159265358979323846;
+  const double angle = (double)((code >> (2 * AXIS)) & kAngleMax) / (double)kAngleMax * 3.14159265358979323846;
   double s, c;
   sincos(angle / 2.0, &s, &c);
   q[0] = x * s;
@@ -110,6 +115,8 @@ __device__ __forceinline__ void decode_quat_oct32_f64(uint32_t code, double q[4]
   q[2] = z * s;
   q[3] = c;
 }
+
+__device__ __forceinline__ void decode_quat_oct32_f64(uint32_t code, double q[4]) { decode_quat_oct_f64<10, 12>(code, q); }
 
 // ---- the ewa words (src/render/projection.tsl.ts:277-311) ----
 

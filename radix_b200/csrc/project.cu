@@ -94,9 +94,15 @@ __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
 
-// Phase 1's fields of row i: centre, opacity, ln scales
+// The template parameter VAR is the raw layout's colour type (RDX_DTYPE_*),
+// and the SH codec (RDX_SH_*) of the other layouts.
+
+// Phase 1's fields of row i: centre, opacity, ln scales in float64 (-inf: a
+// zero scale). `zero` is set when the splat's covariance is zero (every
+// scale, or every variance, underflows to 0): cullInvisible's zero cov.
 template <int LAYOUT>
-__device__ __forceinline__ void load_head(const DevTable& t, uint64_t i, float c[3], float& opacity, float ls[3]) {
+__device__ __forceinline__ void load_head(const DevTable& t, uint64_t i, float c[3], float& opacity, double ls[3],
+                                          bool& zero) {
   if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
     const float* cp = t.centers + i * 3;
     const float* lp = t.log_scales + i * 3;
@@ -107,17 +113,38 @@ __device__ __forceinline__ void load_head(const DevTable& t, uint64_t i, float c
     ls[1] = __ldg(lp + 1);
     ls[2] = __ldg(lp + 2);
     opacity = __ldg(t.opacities + i);
+  } else if constexpr (LAYOUT == RDX_LAYOUT_PACKED) {
+    // packedCodec.decode (src/core/splats.ts:288-306), src/gpu/splats.tsl.ts:141-154
+    const uint4 P = __ldg(reinterpret_cast<const uint4*>(t.packed) + i);
+    c[0] = half_bits_to_float(P.y);
+    c[1] = half_bits_to_float(P.y >> 16);
+    c[2] = half_bits_to_float(P.z);
+    opacity = (float)(P.x >> 24) * (1.0f / 255.0f);
+    const double lmin = t.packed_encoding[2];
+    const double step = ((double)t.packed_encoding[3] - lmin) / 254.0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const uint32_t code = (P.w >> (8 * k)) & 0xffu;
+      ls[k] = code == 0u ? -INFINITY : lmin + (double)(code - 1u) * step;
+    }
   } else {
-    // src/core/splats.ts:10-24; src/gpu/splats.tsl.ts:63-71
+    // extA / covA and extB / covB (src/core/splats.ts:10-32; src/gpu/splats.tsl.ts:63-71, 104-118)
     const uint4 A = __ldg(reinterpret_cast<const uint4*>(t.ext_a) + i);
     const uint4 B = __ldg(reinterpret_cast<const uint4*>(t.ext_b) + i);
     c[0] = __uint_as_float(A.x);
     c[1] = __uint_as_float(A.y);
     c[2] = __uint_as_float(A.z);
     opacity = (float)(A.w >> 24) * (1.0f / 128.0f);
+    // ext: ln scales; cov: ln variances (the same half fields)
     ls[0] = half_bits_to_float(B.y);
     ls[1] = half_bits_to_float(B.y >> 16);
     ls[2] = half_bits_to_float(B.z);
+  }
+  if constexpr (LAYOUT == RDX_LAYOUT_COV) {
+    zero = ls[0] == -INFINITY && ls[1] == -INFINITY && ls[2] == -INFINITY;  // exp(-inf) variances
+  } else {
+    // exp(2 ln s) underflows to 0 below ln s = -372.6
+    zero = ls[0] < -372.6 && ls[1] < -372.6 && ls[2] < -372.6;
   }
 }
 
@@ -143,8 +170,13 @@ __device__ __forceinline__ void prefetch_head(const DevTable& t, uint64_t j0, ui
     } else {
       return;
     }
+  } else if constexpr (LAYOUT == RDX_LAYOUT_PACKED) {
+    if (lane >= 4) return;  // 512 bytes
+    base = reinterpret_cast<const unsigned char*>(t.packed);
+    off = j0 * 16 + (uint64_t)lane * 128;
+    size = count * 16;
   } else {
-    // ext_a and ext_b: 512 bytes each (4 lines)
+    // A and B: 512 bytes each (4 lines)
     if (lane >= 8) return;
     base = reinterpret_cast<const unsigned char*>(lane < 4 ? t.ext_a : t.ext_b);
     off = j0 * 16 + (uint64_t)(lane & 3) * 128;
@@ -153,25 +185,44 @@ __device__ __forceinline__ void prefetch_head(const DevTable& t, uint64_t j0, ui
   if (off < size) prefetch_l2(base + off);
 }
 
-template <int DEG, int CDT>
+template <int DEG, int VAR>
 struct ColorRow {
   static constexpr int kValues = (1 + ShCount<DEG>::value) * 3;
-  static constexpr int kBytes = kValues * (CDT == RDX_DTYPE_F16 ? 2 : 4);
+  static constexpr int kBytes = kValues * (VAR == RDX_DTYPE_F16 ? 2 : 4);
   static constexpr int kVec = kBytes % 16 == 0 ? 16 : (kBytes % 8 == 0 ? 8 : (kBytes % 4 == 0 ? 4 : 2));
 };
 
+// Texels of an SH entry in codec VAR: ext one word per coefficient, packed
+// 10 / 26 / 48 / 76 bytes for degree 1 / 2 / 3 / 4 (src/core/sh.ts:13-24)
+template <int DEG, int VAR>
+struct ShTexels {
+  static constexpr int value = VAR == RDX_SH_PACKED ? (DEG == 0 ? 0 : (DEG == 1 ? 1 : (DEG == 2 ? 2 : (DEG == 3 ? 3 : 5))))
+                                                    : (ShCount<DEG>::value + 3) / 4;
+};
+
+// Texel k of splat i's SH entry: its per-splat channel, or its palette entry
+// (sh.tsl.ts:219-233; a label past the palette reads the last entry)
+__device__ __forceinline__ const uint4* sh_texel(const DevTable& t, uint64_t i, int k) {
+  if (t.sh_palette) {
+    uint64_t label = __ldg(t.sh_label + i);
+    if (label >= t.sh_palette_size) label = t.sh_palette_size - 1;
+    return reinterpret_cast<const uint4*>(t.sh_palette) + label * t.sh_stride + (uint64_t)k;
+  }
+  return reinterpret_cast<const uint4*>(t.ext_sh[k]) + i;
+}
+
 // Phase 2's rows of a queued splat into L2 while the queue fills
-template <int LAYOUT, int DEG, int CDT>
+template <int LAYOUT, int DEG, int VAR>
 __device__ __forceinline__ void prefetch_rows(const DevTable& t, uint64_t i) {
   if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
     prefetch_l2(t.quats + i * 4);
-    const unsigned char* row = reinterpret_cast<const unsigned char*>(t.colors) + i * ColorRow<DEG, CDT>::kBytes;
+    const unsigned char* row = reinterpret_cast<const unsigned char*>(t.colors) + i * ColorRow<DEG, VAR>::kBytes;
 #pragma unroll
-    for (int off = 0; off < ColorRow<DEG, CDT>::kBytes; off += 128) prefetch_l2(row + off);
-    prefetch_l2(row + ColorRow<DEG, CDT>::kBytes - 1);
+    for (int off = 0; off < ColorRow<DEG, VAR>::kBytes; off += 128) prefetch_l2(row + off);
+    prefetch_l2(row + ColorRow<DEG, VAR>::kBytes - 1);
   } else {
 #pragma unroll
-    for (int k = 0; k < (ShCount<DEG>::value + 3) / 4; k++) prefetch_l2(t.ext_sh[k] + i * 4);
+    for (int k = 0; k < ShTexels<DEG, VAR>::value; k++) prefetch_l2(sh_texel(t, i, k));
   }
 }
 
@@ -183,9 +234,32 @@ __device__ __forceinline__ void load_quat(const DevTable& t, uint64_t i, double 
     q[1] = v.y;
     q[2] = v.z;
     q[3] = v.w;
-  } else {
+  } else if constexpr (LAYOUT == RDX_LAYOUT_PACKED) {
+    const uint4 P = __ldg(reinterpret_cast<const uint4*>(t.packed) + i);
+    decode_quat_oct_f64<8, 8>((P.z >> 16) | ((P.w >> 24) << 16), q);
+  } else if constexpr (LAYOUT == RDX_LAYOUT_EXT) {
     decode_quat_oct32_f64(__ldg(reinterpret_cast<const uint4*>(t.ext_b) + i).w, q);
+  } else {
+    q[0] = q[1] = q[2] = 0.0;  // the cov layout stores no rotation
+    q[3] = 1.0;
   }
+}
+
+// covB's object-space covariance: xx, yy, zz, xy, xz, yz (src/core/splats.ts:223-266)
+__device__ __forceinline__ double decode_correlation(double e) {
+  return e == 0.0 ? 0.0 : (e > 0.0 ? -1.0 : 1.0) * exp(-fabs(e));
+}
+
+__device__ __forceinline__ void load_cov(const DevTable& t, uint64_t i, double cov[6]) {
+  const uint4 B = __ldg(reinterpret_cast<const uint4*>(t.ext_b) + i);
+  const double xx = exp((double)half_bits_to_float(B.y)), yy = exp((double)half_bits_to_float(B.y >> 16)),
+               zz = exp((double)half_bits_to_float(B.z));
+  cov[0] = xx;
+  cov[1] = yy;
+  cov[2] = zz;
+  cov[3] = decode_correlation(half_bits_to_float(B.z >> 16)) * sqrt(xx * yy);
+  cov[4] = decode_correlation(half_bits_to_float(B.w)) * sqrt(xx * zz);
+  cov[5] = decode_correlation(half_bits_to_float(B.w >> 16)) * sqrt(yy * zz);
 }
 
 template <int BYTES>
@@ -203,7 +277,7 @@ __device__ __forceinline__ void load_vec(const unsigned char* p, unsigned char* 
 
 // Base rgb + SH (float64) of row i seen along (dx, dy, dz), clamped at 0 when
 // the table has SH (GpuShReader.apply); without SH no clamp
-template <int LAYOUT, int DEG, int CDT>
+template <int LAYOUT, int DEG, int VAR>
 __device__ __forceinline__ void colour(const DevTable& t, uint64_t i, double dx, double dy, double dz, int cap,
                                        double rgb[3]) {
   constexpr int K = ShCount<DEG>::value;
@@ -212,13 +286,13 @@ __device__ __forceinline__ void colour(const DevTable& t, uint64_t i, double dx,
   const double inv = l2 > 0.0 ? 1.0 / sqrt(l2) : 0.0;
   const double x = dx * inv, y = dy * inv, z = dz * inv;
   if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
-    using CR = ColorRow<DEG, CDT>;
+    using CR = ColorRow<DEG, VAR>;
     alignas(16) unsigned char buf[(CR::kBytes + 15) / 16 * 16];
     const unsigned char* row = reinterpret_cast<const unsigned char*>(t.colors) + i * CR::kBytes;
 #pragma unroll
     for (int b = 0; b < CR::kBytes; b += CR::kVec) load_vec<CR::kVec>(row + b, buf + b);
     auto value = [&](int v) -> double {
-      if constexpr (CDT == RDX_DTYPE_F16) {
+      if constexpr (VAR == RDX_DTYPE_F16) {
         return (double)__half2float(*reinterpret_cast<const __half*>(buf + v * 2));
       } else {
         return (double)*reinterpret_cast<const float*>(buf + v * 4);
@@ -246,27 +320,52 @@ __device__ __forceinline__ void colour(const DevTable& t, uint64_t i, double dx,
       }
     }
   } else {
-    decode_ext_rgb_f64(__ldg(reinterpret_cast<const uint4*>(t.ext_b) + i).x, rgb);
-    if constexpr (K > 0) {
-      uint32_t words[(K + 3) / 4 * 4];
+    if constexpr (LAYOUT == RDX_LAYOUT_PACKED) {
+      // rgbMin + byte / 255 * (rgbMax - rgbMin)
+      const uint32_t w = __ldg(reinterpret_cast<const uint4*>(t.packed) + i).x;
+      const double rmin = t.packed_encoding[0], range = (double)t.packed_encoding[1] - rmin;
 #pragma unroll
-      for (int k = 0; k < (K + 3) / 4; k++) {
-        const uint4 T = __ldg(reinterpret_cast<const uint4*>(t.ext_sh[k]) + i);
+      for (int c = 0; c < 3; c++) rgb[c] = rmin + ((double)((w >> (8 * c)) & 0xffu) / 255.0) * range;
+    } else {
+      decode_ext_rgb_f64(__ldg(reinterpret_cast<const uint4*>(t.ext_b) + i).x, rgb);
+    }
+    if constexpr (K > 0) {
+      constexpr int kTexels = ShTexels<DEG, VAR>::value;
+      uint32_t words[kTexels * 4];
+#pragma unroll
+      for (int k = 0; k < kTexels; k++) {
+        const uint4 T = __ldg(sh_texel(t, i, k));
         words[k * 4 + 0] = T.x;
         words[k * 4 + 1] = T.y;
         words[k * 4 + 2] = T.z;
         words[k * 4 + 3] = T.w;
       }
+      auto byte_at = [&](int b) -> uint32_t { return (words[b >> 2] >> ((b & 3) * 8)) & 0xffu; };
 #pragma unroll
       for (int band = 1; band <= DEG; band++) {
         if (band <= cap) {
           double basis[9];
           const int nb = sh_basis_band(band, x, y, z, basis);
+          // packed: the band's scale byte, then its sint8 values (sh.ts:156-168)
+          constexpr int kStart[5] = {0, 0, 10, 26, 48};
+          double scale = 0.0;
+          if constexpr (VAR == RDX_SH_PACKED) {
+            const uint32_t code = byte_at(kStart[band]);
+            scale = code == 0u ? 0.0 : exp2(((double)code - 192.0) / 16.0) / 127.0;
+          }
 #pragma unroll
           for (int k = 0; k < 9; k++) {
             if (k < nb) {
               double c[3];
-              decode_ext_rgb_f64(words[band * band - 1 + k], c);
+              if constexpr (VAR == RDX_SH_PACKED) {
+#pragma unroll
+                for (int ch = 0; ch < 3; ch++) {
+                  const int b = kStart[band] + 1 + k * 3 + ch;
+                  c[ch] = (double)(int)(signed char)byte_at(b) * scale;
+                }
+              } else {
+                decode_ext_rgb_f64(words[band * band - 1 + k], c);
+              }
               acc[0] = fma(c[0], basis[k], acc[0]);
               acc[1] = fma(c[1], basis[k], acc[1]);
               acc[2] = fma(c[2], basis[k], acc[2]);
@@ -312,7 +411,7 @@ struct WarpSmem {
   uint32_t valid;
 };
 
-template <int LAYOUT, int DEG, int CDT, int EYES, bool HIST>
+template <int LAYOUT, int DEG, int VAR, int EYES, bool HIST>
 __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict__ descs, int n_desc, uint32_t total_chunks,
                                                       ProjOutputs out, ProjHist hist) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -365,10 +464,12 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
     if (busy) {
       const uint64_t i = W.idx[q];
       const uint64_t gi = sd.out_offset + i;
-      float cf[3], opac, ls[3];
-      load_head<LAYOUT>(sd.table, i, cf, opac, ls);
+      float cf[3], opac;
+      double ls[3];
+      bool zero_cov;
+      load_head<LAYOUT>(sd.table, i, cf, opac, ls, zero_cov);
       double rgb[3];
-      colour<LAYOUT, DEG, CDT>(sd.table, i, (double)W.c[0][q] - sd.origin[0], (double)W.c[1][q] - sd.origin[1],
+      colour<LAYOUT, DEG, VAR>(sd.table, i, (double)W.c[0][q] - sd.origin[0], (double)W.c[1][q] - sd.origin[1],
                                (double)W.c[2][q] - sd.origin[2], min(p.max_sh_degree, DEG), rgb);
       // prepareSplat (projection.tsl.ts:42-64), float64
       double op = opac, inflate2 = 1.0;
@@ -380,12 +481,19 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
         }
       }
       const float std_dev = op > 1.0 ? (float)((double)p.max_std_dev + (op - 1.0) * 0.7) : p.max_std_dev;
-      const double s2x = exp(2.0 * (double)ls[0]) * inflate2;
-      const double s2y = exp(2.0 * (double)ls[1]) * inflate2;
-      const double s2z = exp(2.0 * (double)ls[2]) * inflate2;
-      double qv[4];
-      load_quat<LAYOUT>(sd.table, i, qv);
-      {
+      // scales^2 = exp(2 ln s) (the cov layout: the stored covariance), both times the LoD inflation
+      double s2x = 0.0, s2y = 0.0, s2z = 0.0, cv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+      double R[9] = {1.0, 0.0, 0.0, 0.0, 1.0, 0.0, 0.0, 0.0, 1.0};
+      if constexpr (LAYOUT == RDX_LAYOUT_COV) {
+        load_cov(sd.table, i, cv);
+#pragma unroll
+        for (int k = 0; k < 6; k++) cv[k] *= inflate2;
+      } else {
+        s2x = exp(2.0 * ls[0]) * inflate2;
+        s2y = exp(2.0 * ls[1]) * inflate2;
+        s2z = exp(2.0 * ls[2]) * inflate2;
+        double qv[4];
+        load_quat<LAYOUT>(sd.table, i, qv);
         const double ql2 = qv[0] * qv[0] + qv[1] * qv[1] + qv[2] * qv[2] + qv[3] * qv[3];
         if (ql2 > 0.0) {
           const double qi = 1.0 / sqrt(ql2);
@@ -397,12 +505,18 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
           qv[0] = qv[1] = qv[2] = 0.0;
           qv[3] = 1.0;
         }
+        const double qx = qv[0], qy = qv[1], qz = qv[2], qw = qv[3];
+        // R(q), row-major (src/gpu/math.tsl.ts:26-44 without the scales)
+        R[0] = 1.0 - 2.0 * (qy * qy + qz * qz);
+        R[1] = 2.0 * (qx * qy - qw * qz);
+        R[2] = 2.0 * (qx * qz + qw * qy);
+        R[3] = 2.0 * (qx * qy + qw * qz);
+        R[4] = 1.0 - 2.0 * (qx * qx + qz * qz);
+        R[5] = 2.0 * (qy * qz - qw * qx);
+        R[6] = 2.0 * (qx * qz - qw * qy);
+        R[7] = 2.0 * (qy * qz + qw * qx);
+        R[8] = 1.0 - 2.0 * (qx * qx + qy * qy);
       }
-      const double qx = qv[0], qy = qv[1], qz = qv[2], qw = qv[3];
-      // R(q), row-major (src/gpu/math.tsl.ts:26-44 without the scales)
-      const double R[9] = {1.0 - 2.0 * (qy * qy + qz * qz), 2.0 * (qx * qy - qw * qz), 2.0 * (qx * qz + qw * qy),
-                           2.0 * (qx * qy + qw * qz), 1.0 - 2.0 * (qx * qx + qz * qz), 2.0 * (qy * qz - qw * qx),
-                           2.0 * (qx * qz - qw * qy), 2.0 * (qy * qz + qw * qx), 1.0 - 2.0 * (qx * qx + qy * qy)};
       const uint32_t eye_ok = W.eye_ok[q];
 #pragma unroll
       for (int v = 0; v < EYES; v++) {
@@ -439,19 +553,34 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
           const double* Wm = e.wd;  // object -> eye 3x3
           const double w0x = j1x * Wm[0] + j2x * Wm[6], w0y = j1x * Wm[1] + j2x * Wm[7], w0z = j1x * Wm[2] + j2x * Wm[8];
           const double w1x = j1y * Wm[3] + j2y * Wm[6], w1y = j1y * Wm[4] + j2y * Wm[7], w1z = j1y * Wm[5] + j2y * Wm[8];
-          const double u00 = w0x * R[0] + w0y * R[3] + w0z * R[6];
-          const double u01 = w0x * R[1] + w0y * R[4] + w0z * R[7];
-          const double u02 = w0x * R[2] + w0y * R[5] + w0z * R[8];
-          const double u10 = w1x * R[0] + w1y * R[3] + w1z * R[6];
-          const double u11 = w1x * R[1] + w1y * R[4] + w1z * R[7];
-          const double u12 = w1x * R[2] + w1y * R[5] + w1z * R[8];
-          const double ra = u00 * u00 * s2x + u01 * u01 * s2y + u02 * u02 * s2z;
-          const double rd = u10 * u10 * s2x + u11 * u11 * s2y + u12 * u12 * s2z;
-          b_d = u00 * u10 * s2x + u01 * u11 * s2y + u02 * u12 * s2z;
-          const double m0 = u01 * u12 - u02 * u11;
-          const double m1 = u02 * u10 - u00 * u12;
-          const double m2 = u00 * u11 - u01 * u10;
-          const double det_t = m0 * m0 * (s2y * s2z) + m1 * m1 * (s2x * s2z) + m2 * m2 * (s2x * s2y);
+          double ra, rd, det_t;
+          if constexpr (LAYOUT == RDX_LAYOUT_COV) {
+            // cov2D = M Sigma M^T with the rows w0, w1 of M (float64: its det cancels less than float32 needs)
+            const double sw0x = cv[0] * w0x + cv[3] * w0y + cv[4] * w0z;
+            const double sw0y = cv[3] * w0x + cv[1] * w0y + cv[5] * w0z;
+            const double sw0z = cv[4] * w0x + cv[5] * w0y + cv[2] * w0z;
+            const double sw1x = cv[0] * w1x + cv[3] * w1y + cv[4] * w1z;
+            const double sw1y = cv[3] * w1x + cv[1] * w1y + cv[5] * w1z;
+            const double sw1z = cv[4] * w1x + cv[5] * w1y + cv[2] * w1z;
+            ra = w0x * sw0x + w0y * sw0y + w0z * sw0z;
+            rd = w1x * sw1x + w1y * sw1y + w1z * sw1z;
+            b_d = w0x * sw1x + w0y * sw1y + w0z * sw1z;
+            det_t = ra * rd - b_d * b_d;
+          } else {
+            const double u00 = w0x * R[0] + w0y * R[3] + w0z * R[6];
+            const double u01 = w0x * R[1] + w0y * R[4] + w0z * R[7];
+            const double u02 = w0x * R[2] + w0y * R[5] + w0z * R[8];
+            const double u10 = w1x * R[0] + w1y * R[3] + w1z * R[6];
+            const double u11 = w1x * R[1] + w1y * R[4] + w1z * R[7];
+            const double u12 = w1x * R[2] + w1y * R[5] + w1z * R[8];
+            ra = u00 * u00 * s2x + u01 * u01 * s2y + u02 * u02 * s2z;
+            rd = u10 * u10 * s2x + u11 * u11 * s2y + u12 * u12 * s2z;
+            b_d = u00 * u10 * s2x + u01 * u11 * s2y + u02 * u12 * s2z;
+            const double m0 = u01 * u12 - u02 * u11;
+            const double m1 = u02 * u10 - u00 * u12;
+            const double m2 = u00 * u11 - u01 * u10;
+            det_t = m0 * m0 * (s2y * s2z) + m1 * m1 * (s2x * s2z) + m2 * m2 * (s2x * s2y);
+          }
           const double pre = p.pre_blur_amount, full = (double)p.pre_blur_amount + blur;
           const double det_orig = det_t + pre * (ra + rd) + pre * pre;
           det_d = det_t + full * (ra + rd) + full * full;
@@ -613,8 +742,10 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
     float cf[3] = {0.f, 0.f, 0.f};
     double pe[EYES][6];
     if (live) {
-      float opac, ls[3];
-      load_head<LAYOUT>(sd.table, i, cf, opac, ls);
+      float opac;
+      double ls[3];
+      bool zero_cov;
+      load_head<LAYOUT>(sd.table, i, cf, opac, ls, zero_cov);
       const double cx = cf[0], cy = cf[1], cz = cf[2];
       const double hx = affine_row(sd.a + 0, cx, cy, cz);
       const double hy = affine_row(sd.a + 4, cx, cy, cz);
@@ -626,38 +757,51 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
         op = fmin(op * 4.0 - 3.0, 5.0);
         if (p.lod_inflate) op = 1.0;
       }
-      // exp(2 ln s) underflows to 0 below ln s = -372.6: a degenerate (zero) covariance
-      const bool degenerate = sd.degenerate || (ls[0] < -372.6f && ls[1] < -372.6f && ls[2] < -372.6f);
+      const bool degenerate = sd.degenerate || zero_cov;
       const bool invisible = op <= 0.0 || op < (double)p.min_alpha || degenerate;
       bool guarded = true;
       if (p.sort_guard > 0.0f && !invisible) {
-        // inSortGuard (projection.tsl.ts:145-155), cov form, float32
-        double qd[4];
-        load_quat<LAYOUT>(sd.table, i, qd);
-        float qx = (float)qd[0], qy = (float)qd[1], qz = (float)qd[2], qw = (float)qd[3];
-        const float ql2 = qx * qx + qy * qy + qz * qz + qw * qw;
-        const float qi = ql2 > 0.0f ? rsqrtf(ql2) : 0.0f;
-        qx *= qi;
-        qy *= qi;
-        qz *= qi;
-        qw = ql2 > 0.0f ? qw * qi : 1.0f;
-        const float R[9] = {1.f - 2.f * (qy * qy + qz * qz), 2.f * (qx * qy - qw * qz), 2.f * (qx * qz + qw * qy),
-                            2.f * (qx * qy + qw * qz), 1.f - 2.f * (qx * qx + qz * qz), 2.f * (qy * qz - qw * qx),
-                            2.f * (qx * qz - qw * qy), 2.f * (qy * qz + qw * qx), 1.f - 2.f * (qx * qx + qy * qy)};
+        // inSortGuard (projection.tsl.ts:145-155), cov form, float32: the head-space
+        // covariance's largest diagonal element
         float inflate = 1.0f;
         if (opac > 1.0f && p.lod_inflate) {
           const float o = fminf(opac * 4.0f - 3.0f, 5.0f);
           inflate = expf((o * o - 1.0f) * (1.0f / (3.0f * 2.718281828459045f)));
         }
-        const float sx = expf(ls[0]) * inflate, sy = expf(ls[1]) * inflate, sz = expf(ls[2]) * inflate;
         float ext2 = 0.0f;
+        if constexpr (LAYOUT == RDX_LAYOUT_COV) {
+          double cv[6];
+          load_cov(sd.table, i, cv);
 #pragma unroll
-        for (int r = 0; r < 3; r++) {
-          const float a0 = (float)sd.a[r * 4 + 0], a1 = (float)sd.a[r * 4 + 1], a2 = (float)sd.a[r * 4 + 2];
-          const float g0 = (a0 * R[0] + a1 * R[3] + a2 * R[6]) * sx;
-          const float g1 = (a0 * R[1] + a1 * R[4] + a2 * R[7]) * sy;
-          const float g2 = (a0 * R[2] + a1 * R[5] + a2 * R[8]) * sz;
-          ext2 = fmaxf(ext2, g0 * g0 + g1 * g1 + g2 * g2);
+          for (int r = 0; r < 3; r++) {
+            const float a0 = (float)sd.a[r * 4 + 0], a1 = (float)sd.a[r * 4 + 1], a2 = (float)sd.a[r * 4 + 2];
+            const float v = a0 * a0 * (float)cv[0] + a1 * a1 * (float)cv[1] + a2 * a2 * (float)cv[2] +
+                            2.0f * (a0 * a1 * (float)cv[3] + a0 * a2 * (float)cv[4] + a1 * a2 * (float)cv[5]);
+            ext2 = fmaxf(ext2, v * inflate * inflate);
+          }
+        } else {
+          double qd[4];
+          load_quat<LAYOUT>(sd.table, i, qd);
+          float qx = (float)qd[0], qy = (float)qd[1], qz = (float)qd[2], qw = (float)qd[3];
+          const float ql2 = qx * qx + qy * qy + qz * qz + qw * qw;
+          const float qi = ql2 > 0.0f ? rsqrtf(ql2) : 0.0f;
+          qx *= qi;
+          qy *= qi;
+          qz *= qi;
+          qw = ql2 > 0.0f ? qw * qi : 1.0f;
+          const float R[9] = {1.f - 2.f * (qy * qy + qz * qz), 2.f * (qx * qy - qw * qz), 2.f * (qx * qz + qw * qy),
+                              2.f * (qx * qy + qw * qz), 1.f - 2.f * (qx * qx + qz * qz), 2.f * (qy * qz - qw * qx),
+                              2.f * (qx * qz - qw * qy), 2.f * (qy * qz + qw * qx), 1.f - 2.f * (qx * qx + qy * qy)};
+          const float sx = expf((float)ls[0]) * inflate, sy = expf((float)ls[1]) * inflate,
+                      sz = expf((float)ls[2]) * inflate;
+#pragma unroll
+          for (int r = 0; r < 3; r++) {
+            const float a0 = (float)sd.a[r * 4 + 0], a1 = (float)sd.a[r * 4 + 1], a2 = (float)sd.a[r * 4 + 2];
+            const float g0 = (a0 * R[0] + a1 * R[3] + a2 * R[6]) * sx;
+            const float g1 = (a0 * R[1] + a1 * R[4] + a2 * R[7]) * sy;
+            const float g2 = (a0 * R[2] + a1 * R[5] + a2 * R[8]) * sz;
+            ext2 = fmaxf(ext2, g0 * g0 + g1 * g1 + g2 * g2);
+          }
         }
         const float radius = sqrtf(ext2) * p.max_std_dev;
         const double* P = sd.eye[0].proj;
@@ -703,7 +847,7 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
       }
       candidate = eye_ok != 0;
       if (candidate) {
-        prefetch_rows<LAYOUT, DEG, CDT>(sd.table, i);
+        prefetch_rows<LAYOUT, DEG, VAR>(sd.table, i);
       } else if (!sd.keys_only) {
         // culled in every eye: zeros, as a zero opacity byte marks a culled eye
 #pragma unroll
@@ -754,32 +898,44 @@ struct Picked {
   int smem;
 };
 
-template <int LAYOUT, int DEG, int CDT, int EYES, bool HIST>
+template <int LAYOUT, int DEG, int VAR, int EYES, bool HIST>
 Picked picked() {
-  return {k_project<LAYOUT, DEG, CDT, EYES, HIST>, (int)(kWarps * sizeof(WarpSmem<EYES>))};
+  return {k_project<LAYOUT, DEG, VAR, EYES, HIST>, (int)(kWarps * sizeof(WarpSmem<EYES>))};
 }
 
-template <int LAYOUT, int DEG, int CDT>
+template <int LAYOUT, int DEG, int VAR>
 Picked pick_eyes(int eyes, bool hist) {
-  if (eyes == 2) return hist ? picked<LAYOUT, DEG, CDT, 2, true>() : picked<LAYOUT, DEG, CDT, 2, false>();
-  return hist ? picked<LAYOUT, DEG, CDT, 1, true>() : picked<LAYOUT, DEG, CDT, 1, false>();
+  if (eyes == 2) return hist ? picked<LAYOUT, DEG, VAR, 2, true>() : picked<LAYOUT, DEG, VAR, 2, false>();
+  return hist ? picked<LAYOUT, DEG, VAR, 1, true>() : picked<LAYOUT, DEG, VAR, 1, false>();
 }
 
-template <int LAYOUT, int CDT>
+template <int LAYOUT, int VAR>
 Picked pick_degree(int degree, int eyes, bool hist) {
   switch (degree) {
-    case 0: return pick_eyes<LAYOUT, 0, CDT>(eyes, hist);
-    case 1: return pick_eyes<LAYOUT, 1, CDT>(eyes, hist);
-    case 2: return pick_eyes<LAYOUT, 2, CDT>(eyes, hist);
-    case 3: return pick_eyes<LAYOUT, 3, CDT>(eyes, hist);
-    default: return pick_eyes<LAYOUT, 4, CDT>(eyes, hist);
+    case 0: return pick_eyes<LAYOUT, 0, VAR>(eyes, hist);
+    case 1: return pick_eyes<LAYOUT, 1, VAR>(eyes, hist);
+    case 2: return pick_eyes<LAYOUT, 2, VAR>(eyes, hist);
+    case 3: return pick_eyes<LAYOUT, 3, VAR>(eyes, hist);
+    default: return pick_eyes<LAYOUT, 4, VAR>(eyes, hist);
   }
 }
 
-Picked pick_kernel(int layout, int degree, int cdt, int eyes, bool hist) {
-  if (layout == RDX_LAYOUT_EXT) return pick_degree<RDX_LAYOUT_EXT, RDX_DTYPE_F32>(degree, eyes, hist);
-  if (cdt == RDX_DTYPE_F16) return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F16>(degree, eyes, hist);
-  return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F32>(degree, eyes, hist);
+template <int LAYOUT>
+Picked pick_codec(int degree, int codec, int eyes, bool hist) {
+  // without SH the codec is immaterial: one kernel
+  if (codec == RDX_SH_PACKED && degree > 0) return pick_degree<LAYOUT, RDX_SH_PACKED>(degree, eyes, hist);
+  return pick_degree<LAYOUT, RDX_SH_EXT>(degree, eyes, hist);
+}
+
+Picked pick_kernel(const DevTable& t, int eyes, bool hist) {
+  switch (t.layout) {
+    case RDX_LAYOUT_EXT: return pick_codec<RDX_LAYOUT_EXT>(t.sh_degree, t.sh_codec, eyes, hist);
+    case RDX_LAYOUT_PACKED: return pick_codec<RDX_LAYOUT_PACKED>(t.sh_degree, t.sh_codec, eyes, hist);
+    case RDX_LAYOUT_COV: return pick_codec<RDX_LAYOUT_COV>(t.sh_degree, t.sh_codec, eyes, hist);
+    default:
+      if (t.color_dtype == RDX_DTYPE_F16) return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F16>(t.sh_degree, eyes, hist);
+      return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F32>(t.sh_degree, eyes, hist);
+  }
 }
 
 }  // namespace
@@ -790,8 +946,7 @@ cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host
   if (total_chunks == 0 || n_desc == 0) return cudaSuccess;
   // One kernel per launch: the caller groups objects by table kind
   const ProjDesc& d0 = descs_host[0];
-  const Picked k =
-      pick_kernel(d0.table.layout, d0.table.sh_degree, d0.table.color_dtype, d0.eyes, hist.hist != nullptr);
+  const Picked k = pick_kernel(d0.table, d0.eyes, hist.hist != nullptr);
   cudaError_t err = cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem);
   if (err != cudaSuccess) return err;
   int device = 0, sms = 0, per_sm = 0;

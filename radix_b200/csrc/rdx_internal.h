@@ -97,7 +97,7 @@ struct DevTable {
   int layout;
   int sh_degree;
   int color_dtype;
-  int reserved;
+  int sh_codec;
   const float* centers;
   const float* log_scales;
   const float* quats;
@@ -106,6 +106,12 @@ struct DevTable {
   const uint32_t* ext_a;
   const uint32_t* ext_b;
   const uint32_t* ext_sh[6];
+  const uint32_t* packed;
+  float packed_encoding[4];
+  const uint32_t* sh_palette;  // SH from a palette when set (entries of sh_stride texels)
+  const uint16_t* sh_label;
+  uint32_t sh_stride;
+  uint32_t sh_palette_size;
 };
 
 struct DevParams {
