@@ -6,8 +6,10 @@ python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 One process per GPU (torchrun for N > 1): each rank runs its own replica of
 the workload (the path shards by object and view; no collective is needed),
 timed on the device with CUDA events between barriers; the time is the max
-over ranks and `value` counts the splats of every rank. Rank 0 prints one JSON
-line. --impl reference times the reference's CPU path (the float64 port of
+over ranks and `value` counts the splats of every rank. A step is one CUDA
+graph launch of the frame (rb.Batch with one view); the same frame through
+rb.frame, which plans on the host every call, is timed beside it. Rank 0
+prints one JSON line. --impl reference times the reference's CPU path (the float64 port of
 SortKeys.compute / SortKeys.sort and of the projection) on the host cores.
 """
 import argparse
@@ -482,39 +484,29 @@ def main():
     visible = torch.zeros(1, dtype=torch.int32, device=device)
     ctx.reserve(n)
 
-    def step():
+    def frame_step():
         rb.frame(obj, cam, None, BITS, names, ctx=ctx, out=out, ordering=ordering, visible=visible)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    ctx.set_profiling(True)
-    ctx.phase_times()
-    launches0 = ctx.launches()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    clocks = Clocks(local)
-    start = torch.cuda.Event(enable_timing=True)
-    stop = torch.cuda.Event(enable_timing=True)
-    start.record()
-    for _ in range(args.steps):
-        step()
-    stop.record()
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    clock_info = clocks.stop()
-    ms_total = start.elapsed_time(stop)
-    launches = ctx.launches() - launches0
-    phases = ctx.phase_times()
-    ctx.set_profiling(False)
-    if world > 1:
-        t = torch.tensor([ms_total], device=device, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    # The frame captured once in a CUDA graph (rb.Batch with one view): each
+    # step is one graph launch of the projection and the sort
+    batch = rb.Batch([(obj, cam)], None, BITS, names, device=device, ctx=ctx)
+    graph_kernels = batch.launches()
+    ms_total, clock_info = timed(batch.launch, args.steps, args.warmup, world, local)
+    batch.synchronize()
+    launches = graph_kernels * args.steps
     ms_step = ms_total / args.steps
     value = world * n * args.steps / (ms_total / 1e3) / 1e6
+    # the same frame through rb.frame (host planning every call), and its phase split
+    frame_ms, _ = timed(frame_step, args.steps, args.warmup, world, local)
+
+    def start_profiling():
+        ctx.set_profiling(True)
+        ctx.phase_times()
+
+    timed(frame_step, args.steps, 1, world, local, start_profiling)
+    phases = ctx.phase_times()
+    ctx.set_profiling(False)
+    batch.close()
 
     # end to end through the public API: pinned host tables in, the order and
     # the visible count out, copies inside the timed region
@@ -561,7 +553,9 @@ def main():
                    "l2": "inputs 944 MB > 126 MB L2 (no flush)",
                    "frame_bytes_per_splat": FRAME_BYTES,
                    "hbm_frac_frame": FRAME_BYTES * n / (ms_step / 1e3) / 1e9 / peak,
-                   "project_ms": proj_avg, "sort_ms": sort_ms / max(sort_runs, 1)},
+                   "project_ms": proj_avg, "sort_ms": sort_ms / max(sort_runs, 1),
+                   "step": "one CUDA-graph launch of the frame (rb.Batch, one view)",
+                   "rb_frame_ms": frame_ms / args.steps},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "k_project (raw, SH 3, 1 eye)",
                      "bytes_per_splat": PROJECT_BYTES, "peak_kind": peak_kind},
