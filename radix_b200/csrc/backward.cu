@@ -94,53 +94,18 @@ __device__ __forceinline__ double colour_value(const void* colors, uint64_t i, i
   }
 }
 
+// The gradient of row i of an object (drawn: the eyes whose forward drew it, not 0)
 template <int DEG, int CDT, int EYES>
-__global__ void __launch_bounds__(kBwdThreads, kBwdBlocksPerSm) k_project_backward(const ProjDesc* __restrict__ descs,
-                                                                  const GradsOut* __restrict__ grads, int n_desc,
-                                                                  uint32_t total_chunks, GradsIn in) {
+__device__ __forceinline__ void splat_backward(const ProjDesc& sd, const GradsOut& go_, const GradsIn& in, uint64_t i,
+                                               uint32_t drawn) {
   constexpr int K = Coeffs<DEG>::value;
   constexpr int kRow = (1 + K) * 3;
-  const uint64_t t = (uint64_t)blockIdx.x * kBwdThreads + threadIdx.x;
-  const uint32_t chunk = (uint32_t)(t / kProjTile);
-  if (chunk >= total_chunks) return;
-  int lo = 0, hi = n_desc - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (descs[mid].first_tile <= chunk) {
-      lo = mid;
-    } else {
-      hi = mid - 1;
-    }
-  }
-  const ProjDesc& sd = descs[lo];
-  const GradsOut go_ = grads[lo];
-  const uint64_t i = (uint64_t)(chunk - sd.first_tile) * kProjTile + t % kProjTile;
-  if (i >= sd.count) return;
   const uint64_t gi = sd.out_offset + i;
   const DevParams& p = sd.params;
   const DevTable& tb = sd.table;
 
   double g_c[3] = {0.0, 0.0, 0.0}, g_S[3] = {0.0, 0.0, 0.0}, g_R[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   double g_op = 0.0, g_rgb[3] = {0.0, 0.0, 0.0};
-  bool any = false;
-  uint32_t drawn = 0;
-#pragma unroll
-  for (int v = 0; v < EYES; v++) {
-    if (__ldg(in.fwd_opacity + (uint64_t)v * sd.out_n + gi) != 0.0f) drawn |= 1u << v;
-  }
-  any = drawn != 0;
-  if (!any) {  // drawn by no eye: the outputs are constants
-    if (go_.centers) go_.centers[i * 3] = go_.centers[i * 3 + 1] = go_.centers[i * 3 + 2] = 0.0f;
-    if (go_.log_scales) go_.log_scales[i * 3] = go_.log_scales[i * 3 + 1] = go_.log_scales[i * 3 + 2] = 0.0f;
-    if (go_.quats) reinterpret_cast<float4*>(go_.quats)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (go_.opacities) go_.opacities[i] = 0.0f;
-    if (go_.colors) {
-#pragma unroll
-      for (int c = 0; c < kRow; c++) go_.colors[i * kRow + c] = 0.0f;
-    }
-    return;
-  }
-
   // the splat
   const double cx = __ldg(tb.centers + i * 3), cy = __ldg(tb.centers + i * 3 + 1), cz = __ldg(tb.centers + i * 3 + 2);
   const double ls0 = __ldg(tb.log_scales + i * 3), ls1 = __ldg(tb.log_scales + i * 3 + 1),
@@ -185,7 +150,7 @@ __global__ void __launch_bounds__(kBwdThreads, kBwdBlocksPerSm) k_project_backwa
   const double hy = affine_row(sd.a + 4, cx, cy, cz);
   const double hz = affine_row(sd.a + 8, cx, cy, cz);
 
-  if (any) {
+  {
 #pragma unroll
     for (int v = 0; v < EYES; v++) {
       if (!((drawn >> v) & 1u)) continue;
@@ -330,7 +295,7 @@ __global__ void __launch_bounds__(kBwdThreads, kBwdBlocksPerSm) k_project_backwa
     g_ls[k] = g_S[k] * S[k];
     g_infl2 += g_S[k] * S[k] / (2.0 * infl2);
   }
-  if (qvalid && any) {
+  if (qvalid) {
     const double* G = g_R;
     double gq[4];
     gq[0] = 2.0 * (G[1] * qy + G[2] * qz + G[3] * qy - 2.0 * G[4] * qx - G[5] * qw + G[6] * qz + G[7] * qw -
@@ -417,6 +382,89 @@ __global__ void __launch_bounds__(kBwdThreads, kBwdBlocksPerSm) k_project_backwa
   if (go_.opacities) go_.opacities[i] = (float)g_o;
 }
 
+constexpr int kBwdWarps = kBwdThreads / 32;
+constexpr int kBwdQueue = 64;  // drawn rows waiting in a warp's queue
+
+// Persistent warps over 32-row chunks: rows no eye drew get zero gradients at
+// once (coalesced), drawn rows are queued and their gradients computed 32 at
+// a time, so every lane of the float64 work is busy whatever the cull pattern.
+template <int DEG, int CDT, int EYES>
+__global__ void __launch_bounds__(kBwdThreads, kBwdBlocksPerSm) k_project_backward(const ProjDesc* __restrict__ descs,
+                                                                  const GradsOut* __restrict__ grads, int n_desc,
+                                                                  uint32_t total_chunks, GradsIn in) {
+  constexpr int kRow = (1 + Coeffs<DEG>::value) * 3;
+  __shared__ uint32_t s_row[kBwdWarps][kBwdQueue];
+  __shared__ uint8_t s_drawn[kBwdWarps][kBwdQueue];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t gw = blockIdx.x * kBwdWarps + (uint32_t)warp, nw = gridDim.x * kBwdWarps;
+  int cur = -1, di = -1;
+  uint32_t head = 0, queued = 0, chunk = gw;
+  while (true) {
+    const bool have = chunk < total_chunks;
+    if (have && di < 0) {
+      int d = 0;
+      if (lane == 0) {
+        int lo = 0, hi = n_desc - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (descs[mid].first_tile <= chunk) {
+            lo = mid;
+          } else {
+            hi = mid - 1;
+          }
+        }
+        d = lo;
+      }
+      di = __shfl_sync(0xffffffffu, d, 0);
+    }
+    // one site for the gradient: full batches, the rest before the object changes and at the end
+    const uint32_t nb = queued >= 32 ? 32u : ((!have || di != cur) ? queued : 0u);
+    if (nb) {
+      if ((uint32_t)lane < nb) {
+        const uint32_t q = (head + (uint32_t)lane) & (kBwdQueue - 1);
+        splat_backward<DEG, CDT, EYES>(descs[cur], grads[cur], in, s_row[warp][q], s_drawn[warp][q]);
+      }
+      head = (head + nb) & (kBwdQueue - 1);
+      queued -= nb;
+      __syncwarp();
+      continue;
+    }
+    if (!have) break;
+    cur = di;
+    const ProjDesc& sd = descs[cur];
+    const uint64_t i = (uint64_t)(chunk - sd.first_tile) * kProjTile + (uint64_t)lane;
+    const bool live = i < sd.count;
+    uint32_t drawn = 0;
+    if (live) {
+      const uint64_t gi = sd.out_offset + i;
+#pragma unroll
+      for (int v = 0; v < EYES; v++)
+        if (__ldg(in.fwd_opacity + (uint64_t)v * sd.out_n + gi) != 0.0f) drawn |= 1u << v;
+      if (!drawn) {  // drawn by no eye: the outputs are constants
+        const GradsOut go_ = grads[cur];
+        if (go_.centers) go_.centers[i * 3] = go_.centers[i * 3 + 1] = go_.centers[i * 3 + 2] = 0.0f;
+        if (go_.log_scales) go_.log_scales[i * 3] = go_.log_scales[i * 3 + 1] = go_.log_scales[i * 3 + 2] = 0.0f;
+        if (go_.quats) reinterpret_cast<float4*>(go_.quats)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (go_.opacities) go_.opacities[i] = 0.0f;
+        if (go_.colors) {
+#pragma unroll
+          for (int c = 0; c < kRow; c++) go_.colors[i * kRow + c] = 0.0f;
+        }
+      }
+    }
+    const uint32_t ballot = __ballot_sync(0xffffffffu, drawn != 0u);
+    if (drawn) {
+      const uint32_t q = (head + queued + (uint32_t)__popc(ballot & ((1u << lane) - 1u))) & (kBwdQueue - 1);
+      s_row[warp][q] = (uint32_t)i;
+      s_drawn[warp][q] = (uint8_t)drawn;
+    }
+    queued += (uint32_t)__popc(ballot);
+    __syncwarp();
+    chunk += nw;
+    di = -1;
+  }
+}
+
 using BwdKernel = void (*)(const ProjDesc*, const GradsOut*, int, uint32_t, GradsIn);
 
 template <int DEG, int CDT>
@@ -443,8 +491,11 @@ cudaError_t launch_project_backward(const ProjDesc* descs_dev, const GradsOut* g
   const ProjDesc& d0 = descs_host[0];
   const BwdKernel k = d0.table.color_dtype == RDX_DTYPE_F16 ? pick_degree<RDX_DTYPE_F16>(d0.table.sh_degree, d0.eyes)
                                                             : pick_degree<RDX_DTYPE_F32>(d0.table.sh_degree, d0.eyes);
-  const uint64_t threads = (uint64_t)total_chunks * kProjTile;
-  const uint32_t blocks = (uint32_t)((threads + kBwdThreads - 1) / kBwdThreads);
+  int device = 0, sms = 0;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const uint32_t want = (total_chunks + kBwdWarps - 1) / kBwdWarps;
+  const uint32_t blocks = min(want, (uint32_t)(sms * kBwdBlocksPerSm));
   k<<<blocks, kBwdThreads, 0, stream>>>(descs_dev, grads_dev, n_desc, total_chunks, in);
   return cudaGetLastError();
 }
