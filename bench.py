@@ -44,9 +44,10 @@ def parse():
     p.add_argument("--n", type=int, default=N_SPLATS)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--workload", default="frame", choices=["frame", "batched", "stereo", "backward"],
+    p.add_argument("--workload", default="frame", choices=["frame", "batched", "stereo", "backward", "ply"],
                    help="frame: 4M SH-3 splats, one view (the headline); batched: 16 scenes x 64 views in one "
-                        "CUDA graph; stereo: 16M SH-3 fp16 splats, two eyes; backward: the projection's gradient, 1M")
+                        "CUDA graph; stereo: 16M SH-3 fp16 splats, two eyes; backward: the projection's gradient, 1M; "
+                        "ply: decoding a 1M-splat PLY file")
     return p.parse_args()
 
 
@@ -434,6 +435,64 @@ def run_backward(args, world, rank, local, device):
     }
 
 
+def run_ply(args, world, rank, local, device):
+    """A 1M-splat SH-3 standard 3DGS PLY file (62 float properties, 248 B a
+    splat) in device memory decoded into a raw table each step."""
+    import numpy as np
+    import torch
+
+    import radix_b200 as rb
+    from radix_b200 import synthetic as syn
+    n = 1_000_000 if args.n == N_SPLATS else args.n
+    d = syn.mixture_table(n, seed=0, sh_degree=SH_DEGREE, device=device)
+    k = (SH_DEGREE + 1) ** 2 - 1
+    names = ["x", "y", "z", "f_dc_0", "f_dc_1", "f_dc_2"] + [f"f_rest_{i}" for i in range(3 * k)] + \
+        ["opacity", "scale_0", "scale_1", "scale_2", "rot_0", "rot_1", "rot_2", "rot_3"]
+    header = ("ply\nformat binary_little_endian 1.0\nelement vertex %d\n" % n +
+              "".join(f"property float {nm}\n" for nm in names) + "end_header\n").encode()
+    c0 = 0.28209479177387814
+    op = np.clip(d["opacities"].astype(np.float64), 1e-6, 1 - 1e-6)
+    cols = [d["centers"], (d["colors"][:, 0].astype(np.float64) - 0.5) / c0]
+    cols += [d["colors"][:, 1:, ch] for ch in range(3)]
+    cols += [np.log(op / (1 - op))[:, None], d["log_scales"], d["quats"][:, 3:4], d["quats"][:, :3]]
+    body = np.concatenate([np.asarray(x, dtype=np.float32).reshape(n, -1) for x in cols], axis=1)
+    raw = np.concatenate([np.frombuffer(header, dtype=np.uint8), body.view(np.uint8).reshape(-1)])
+    data = torch.from_numpy(raw).to(device)
+    del d, body
+    ctx = rb.Context(local)
+    table, out = rb.decode_ply(data, ctx=ctx)
+    record = 4 * len(names)
+    row = (k + 1) * 3 * 4
+
+    def step():
+        rb.decode_ply(data, ctx=ctx)
+
+    marks = {}
+
+    def start_counting():
+        marks["launches"] = ctx.launches()
+
+    ms_total, clock_info = timed(step, args.steps, args.warmup, world, local, start_counting)
+    launches = ctx.launches() - marks["launches"]
+    ms_step = ms_total / args.steps
+    peak, peak_kind = peak_hbm()
+    bytes_per = record + 12 + 12 + 16 + 4 + row
+    achieved = bytes_per * n / (ms_step / 1e3) / 1e9
+    return {
+        "metric": "Msplats/s (PLY decode)", "value": world * n * args.steps / (ms_total / 1e3) / 1e6,
+        "unit": "Msplats/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 in, f64 maths, f32 out",
+        "data": "synthetic (a PLY file written from the seeded SH-3 mixture)",
+        "config": {"workload": f"PLY decode: {n} splats, standard 3DGS, SH 3 ({record} B records) in device memory "
+                               "to a raw float32 table", "n": n, "parallelism": f"replicas{world}",
+                   "bytes_per_splat": bytes_per, "note": "each step includes the header read on the host"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_decode_ply", "bytes_per_splat": bytes_per, "peak_kind": peak_kind},
+        "e2e": None, "e2e_note": "device-resident file bytes",
+        "gpu_launches": launches, "clocks": clock_info,
+    }
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -450,7 +509,7 @@ def main():
         if world > 1:
             from datetime import timedelta
             dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
-        run = {"batched": run_batched, "stereo": run_stereo, "backward": run_backward}[args.workload]
+        run = {"batched": run_batched, "stereo": run_stereo, "backward": run_backward, "ply": run_ply}[args.workload]
         line = run(args, world, rank, local, device)
         if rank == 0:
             print(json.dumps(line))

@@ -347,6 +347,30 @@ typedef struct rdx_table_grads {
 int rdx_project_backward(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
                          const rdx_params* params, const rdx_grads_in* upstream, const rdx_table_grads* grads);
 
+/* ---- PLY files to raw tables ---- */
+
+/* What a PLY file holds (its header): splats, SH degree (from its f_rest_*
+   properties, ply.ts shDegree) and kind: 0 standard 3DGS, 1 RGB point
+   cloud, 2 SuperSplat / PlayCanvas compressed */
+typedef struct rdx_ply_info {
+  uint64_t count;
+  int32_t sh_degree;
+  int32_t kind;
+} rdx_ply_info;
+int rdx_ply_read_info(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx_ply_info* info);
+
+/*
+ * PlyFile.read (src/core/ply.ts:58-264) of a binary PLY file (host or device
+ * bytes) into the columns of a raw table with `count` rows: centers [3],
+ * log_scales [3], quats [4] (normalised x y z w; 16-byte aligned), opacities,
+ * colors [1 + K][3] (base rgb = 0.5 + SH_C0 f_dc, then the SH coefficients
+ * coefficient-major) of degree sh_degree (-1: the file's; at most the file's).
+ * Any output may be NULL. Errors carry the reference's texts ("PLY has no
+ * vertex element", "PLY vertex lacks ...", "PLY file ended unexpectedly" ...).
+ */
+int rdx_decode_ply(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, int sh_degree, float* centers,
+                   float* log_scales, float* quats, float* opacities, float* colors);
+
 /* ---- batched frames: many views of many collections ---- */
 
 /* One view of a batch: a collection (objects, as for rdx_frame) and its camera. */

@@ -15,6 +15,7 @@
 #include "oracle.h"
 
 #include <math.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
@@ -1410,6 +1411,268 @@ int orc_encode_sh(const rdx_table* raw, int codec, uint32_t* words, int stride) 
     } else {
       for (int c = 0; c < SH_COEFFS[deg]; c++) out[c] = orc_encode_ext_rgb(&s.sh[c * 3]);
     }
+  }
+  return 0;
+}
+
+/* ---- PLY files: PlyFile.read (src/core/ply.ts:58-264) in float64 ---- */
+
+typedef struct ply_prop {
+  char name[64];
+  int type; /* 0 char .. 7 double, -1 list */
+  int offset;
+} ply_prop;
+
+typedef struct ply_elem {
+  char name[64];
+  uint64_t count;
+  int n_props;
+  ply_prop props[256];
+  int record;
+} ply_elem;
+
+static const int PLY_BYTES[8] = {1, 1, 2, 2, 4, 4, 4, 8};
+static const double PLY_SCALE[8] = {127, 255, 32767, 65535, 2147483647.0, 4294967295.0, 1, 1}; /* ply.ts:33-42 */
+
+static int ply_type_of(const char* s) { /* ply.ts:413-423 */
+  static const char* names[8] = {"char", "uchar", "short", "ushort", "int", "uint", "float", "double"};
+  static const char* aliases[8] = {"int8", "uint8", "int16", "uint16", "int32", "uint32", "float32", "float64"};
+  for (int t = 0; t < 8; t++)
+    if (!strcmp(s, names[t]) || !strcmp(s, aliases[t])) return t;
+  return -2;
+}
+
+static const ply_prop* ply_find(const ply_elem* e, const char* name) {
+  for (int i = 0; i < e->n_props; i++)
+    if (e->props[i].type >= 0 && !strcmp(e->props[i].name, name)) return &e->props[i];
+  return NULL;
+}
+
+static double ply_read(const uint8_t* rec, const ply_prop* p, int little, int normalized) { /* ply.ts:446-469 */
+  const uint8_t* at = rec + p->offset;
+  const int n = PLY_BYTES[p->type];
+  uint64_t bits = 0;
+  for (int b = 0; b < n; b++) bits |= (uint64_t)at[b] << (8 * (little ? b : n - 1 - b));
+  double v;
+  switch (p->type) {
+    case 0: v = (double)(int8_t)bits; break;
+    case 1: v = (double)(uint8_t)bits; break;
+    case 2: v = (double)(int16_t)bits; break;
+    case 3: v = (double)(uint16_t)bits; break;
+    case 4: v = (double)(int32_t)bits; break;
+    case 5: v = (double)(uint32_t)bits; break;
+    case 6: {
+      uint32_t u = (uint32_t)bits;
+      float f;
+      memcpy(&f, &u, 4);
+      v = f;
+      break;
+    }
+    default: {
+      double dd;
+      memcpy(&dd, &bits, 8);
+      v = dd;
+    }
+  }
+  return normalized ? v / PLY_SCALE[p->type] : v;
+}
+
+static int ply_degree(int rest) { return rest >= 72 ? 4 : rest >= 45 ? 3 : rest >= 24 ? 2 : rest > 0 ? 1 : 0; }
+
+int orc_ply_decode(const uint8_t* bytes, uint64_t nbytes, int sh_degree, double* centers, double* log_scales,
+                   double* quats, double* opacities, double* colors, uint64_t* count_out, int* degree_out,
+                   int* kind_out) {
+  const uint64_t head = nbytes < 65536 ? nbytes : 65536;
+  if (head < 3 || memcmp(bytes, "ply", 3) != 0) return -1;
+  /* the header lines up to end_header */
+  uint64_t pos = 0, header_len = 0;
+  int little = -1;
+  static ply_elem elems[16];
+  int n_elems = 0;
+  char line[512];
+  while (pos < head) {
+    uint64_t e = pos;
+    while (e < head && bytes[e] != '\n') e++;
+    if (e >= head) return -1;
+    uint64_t len = e - pos;
+    if (len && bytes[e - 1] == '\r') len--;
+    if (len >= sizeof(line)) len = sizeof(line) - 1;
+    memcpy(line, bytes + pos, len);
+    line[len] = 0;
+    pos = e + 1;
+    if (!strcmp(line, "end_header")) {
+      header_len = pos;
+      break;
+    }
+    char f0[64] = "", f1[64] = "", f2[64] = "", f3[64] = "", f4[64] = "";
+    int nf = sscanf(line, "%63s %63s %63s %63s %63s", f0, f1, f2, f3, f4);
+    if (nf <= 0) continue;
+    if (!strcmp(f0, "format")) {
+      if (!strcmp(f1, "binary_little_endian")) little = 1;
+      else if (!strcmp(f1, "binary_big_endian")) little = 0;
+      else return -1;
+    } else if (!strcmp(f0, "element") && nf >= 3 && n_elems < 16) {
+      ply_elem* el = &elems[n_elems++];
+      memset(el, 0, sizeof(*el));
+      snprintf(el->name, sizeof(el->name), "%s", f1);
+      el->count = strtoull(f2, NULL, 10);
+    } else if (!strcmp(f0, "property") && n_elems > 0) {
+      ply_elem* el = &elems[n_elems - 1];
+      if (el->n_props >= 256) return -1;
+      ply_prop* p = &el->props[el->n_props++];
+      if (!strcmp(f1, "list")) {
+        snprintf(p->name, sizeof(p->name), "%s", f4);
+        p->type = -1;
+        p->offset = -1;
+      } else {
+        snprintf(p->name, sizeof(p->name), "%s", f2);
+        p->type = ply_type_of(f1);
+        if (p->type < 0) return -1;
+        p->offset = el->record;
+        el->record += PLY_BYTES[p->type];
+      }
+    }
+  }
+  if (!header_len || little < 0) return -1;
+  const ply_elem *vertex = NULL, *chunk = NULL, *sh = NULL;
+  uint64_t offs[16], off = header_len;
+  for (int i = 0; i < n_elems; i++) {
+    offs[i] = off;
+    off += elems[i].count * (uint64_t)elems[i].record;
+    if (!strcmp(elems[i].name, "vertex") && !vertex) vertex = &elems[i];
+    if (!strcmp(elems[i].name, "chunk") && !chunk) chunk = &elems[i];
+    if (!strcmp(elems[i].name, "sh") && !sh) sh = &elems[i];
+  }
+  if (!vertex) return -1;
+  const uint64_t vo = offs[vertex - elems];
+  if (vo + vertex->count * (uint64_t)vertex->record > nbytes) return -1;
+  const uint64_t n = vertex->count;
+  *count_out = n;
+  char name[64];
+  static const char* packed_names[4] = {"packed_position", "packed_rotation", "packed_scale", "packed_color"};
+  int compressed = chunk != NULL;
+  for (int k = 0; k < 4 && compressed; k++) compressed = ply_find(vertex, packed_names[k]) != NULL;
+  int degree = 0, rest = 0;
+  if (compressed) {
+    if (sh)
+      for (;;) {
+        snprintf(name, sizeof(name), "f_rest_%d", rest);
+        if (!ply_find(sh, name)) break;
+        rest++;
+      }
+    degree = (sh && sh->count >= n) ? ply_degree(rest) : 0;
+    *kind_out = 2;
+  } else {
+    for (;;) {
+      snprintf(name, sizeof(name), "f_rest_%d", rest);
+      if (!ply_find(vertex, name)) break;
+      rest++;
+    }
+    *kind_out = ply_find(vertex, "scale_0") ? 0 : 1;
+    degree = *kind_out == 0 ? ply_degree(rest) : 0;
+  }
+  *degree_out = degree;
+  if (sh_degree < 0) sh_degree = degree;
+  if (sh_degree > degree) return -1;
+  const int kvals = SH_COEFFS[sh_degree] * 3, row = 3 + kvals, per = rest / 3;
+  for (uint64_t i = 0; i < n; i++) {
+    const uint8_t* v = bytes + vo + i * (uint64_t)vertex->record;
+    double c[3], ls[3], q[4], op, rgb[3];
+    double* col = colors ? colors + i * (uint64_t)row : NULL;
+    if (compressed) { /* ply.ts:222-262 */
+      static const char* cn[18] = {"min_x", "min_y", "min_z", "max_x", "max_y", "max_z",
+                                   "min_scale_x", "min_scale_y", "min_scale_z", "max_scale_x", "max_scale_y", "max_scale_z",
+                                   "min_r", "min_g", "min_b", "max_r", "max_g", "max_b"};
+      const double defaults[6] = {0, 0, 0, 1, 1, 1};
+      const uint8_t* ch = bytes + offs[chunk - elems] + (i / 256) * (uint64_t)chunk->record;
+      double r[18];
+      for (int k = 0; k < 18; k++) {
+        const ply_prop* p = ply_find(chunk, cn[k]);
+        r[k] = p ? ply_read(ch, p, little, 0) : defaults[k >= 12 ? k - 12 : 0];
+      }
+      uint32_t words[4];
+      for (int k = 0; k < 4; k++) words[k] = (uint32_t)ply_read(v, ply_find(vertex, packed_names[k]), little, 0);
+      const uint32_t pw = words[0], rw = words[1], lw = words[2], kw = words[3];
+      c[0] = r[0] + (r[3] - r[0]) * ((double)((pw >> 21) & 2047) / 2047);
+      c[1] = r[1] + (r[4] - r[1]) * ((double)((pw >> 11) & 1023) / 1023);
+      c[2] = r[2] + (r[5] - r[2]) * ((double)(pw & 2047) / 2047);
+      ls[0] = r[6] + (r[9] - r[6]) * ((double)((lw >> 21) & 2047) / 2047);
+      ls[1] = r[7] + (r[10] - r[7]) * ((double)((lw >> 11) & 1023) / 1023);
+      ls[2] = r[8] + (r[11] - r[8]) * ((double)(lw & 2047) / 2047);
+      const double a = ((double)((rw >> 20) & 1023) / 1023 - 0.5) * sqrt(2.0);
+      const double b = ((double)((rw >> 10) & 1023) / 1023 - 0.5) * sqrt(2.0);
+      const double cc = ((double)(rw & 1023) / 1023 - 0.5) * sqrt(2.0);
+      const double m = sqrt(fmax(0.0, 1 - a * a - b * b - cc * cc));
+      const uint32_t largest = rw >> 30;
+      q[3] = largest == 0 ? m : a;
+      q[0] = largest == 0 ? a : largest == 1 ? m : b;
+      q[1] = largest <= 1 ? b : largest == 2 ? m : cc;
+      q[2] = largest <= 2 ? cc : m;
+      rgb[0] = r[12] + (r[15] - r[12]) * ((double)((kw >> 24) & 255) / 255);
+      rgb[1] = r[13] + (r[16] - r[13]) * ((double)((kw >> 16) & 255) / 255);
+      rgb[2] = r[14] + (r[17] - r[14]) * ((double)((kw >> 8) & 255) / 255);
+      op = (double)(kw & 255) / 255;
+      if (col) {
+        const uint8_t* srec = (sh && degree > 0) ? bytes + offs[sh - elems] + i * (uint64_t)sh->record : NULL;
+        for (int x = 0; x < kvals; x++) {
+          double val = 0.0;
+          if (srec) {
+            snprintf(name, sizeof(name), "f_rest_%d", (x % 3) * per + x / 3);
+            const ply_prop* p = ply_find(sh, name);
+            const uint32_t byte = srec[p ? p->offset : 0];
+            val = ((byte == 0 ? 0 : byte == 255 ? 1 : (byte + 0.5) / 256) - 0.5) * 8; /* ply.ts:267-270 */
+          }
+          col[3 + x] = val;
+        }
+      }
+    } else {
+      c[0] = ply_read(v, ply_find(vertex, "x"), little, 0);
+      c[1] = ply_read(v, ply_find(vertex, "y"), little, 0);
+      c[2] = ply_read(v, ply_find(vertex, "z"), little, 0);
+      if (*kind_out == 0) { /* ply.ts:129-146 */
+        for (int k = 0; k < 3; k++) {
+          snprintf(name, sizeof(name), "scale_%d", k);
+          ls[k] = ply_read(v, ply_find(vertex, name), little, 0);
+        }
+        q[0] = ply_read(v, ply_find(vertex, "rot_1"), little, 0);
+        q[1] = ply_read(v, ply_find(vertex, "rot_2"), little, 0);
+        q[2] = ply_read(v, ply_find(vertex, "rot_3"), little, 0);
+        q[3] = ply_read(v, ply_find(vertex, "rot_0"), little, 0);
+        op = 1.0 / (1.0 + exp(-ply_read(v, ply_find(vertex, "opacity"), little, 0)));
+        for (int k = 0; k < 3; k++) {
+          snprintf(name, sizeof(name), "f_dc_%d", k);
+          rgb[k] = 0.5 + 0.28209479177387814 * ply_read(v, ply_find(vertex, name), little, 0);
+        }
+        if (col)
+          for (int x = 0; x < kvals; x++) {
+            snprintf(name, sizeof(name), "f_rest_%d", (x % 3) * per + x / 3);
+            col[3 + x] = ply_read(v, ply_find(vertex, name), little, 0);
+          }
+      } else { /* a point cloud: ply.ts:147-155 */
+        ls[0] = ls[1] = ls[2] = log(0.001);
+        q[0] = q[1] = q[2] = 0;
+        q[3] = 1;
+        const ply_prop* alpha = ply_find(vertex, "alpha");
+        op = alpha ? ply_read(v, alpha, little, 1) : 1.0;
+        rgb[0] = ply_read(v, ply_find(vertex, "red"), little, 1);
+        rgb[1] = ply_read(v, ply_find(vertex, "green"), little, 1);
+        rgb[2] = ply_read(v, ply_find(vertex, "blue"), little, 1);
+        if (col)
+          for (int x = 0; x < kvals; x++) col[3 + x] = 0.0;
+      }
+    }
+    const double len = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]); /* math.ts:12-27 */
+    if (len > 0) {
+      for (int k = 0; k < 4; k++) q[k] /= len;
+    } else {
+      q[0] = q[1] = q[2] = 0;
+      q[3] = 1;
+    }
+    if (centers) memcpy(centers + i * 3, c, sizeof(c));
+    if (log_scales) memcpy(log_scales + i * 3, ls, sizeof(ls));
+    if (quats) memcpy(quats + i * 4, q, sizeof(q));
+    if (opacities) opacities[i] = op;
+    if (col) memcpy(col, rgb, sizeof(rgb));
   }
   return 0;
 }

@@ -131,6 +131,14 @@ int orc_encode_cov_table(const rdx_table* raw, uint32_t* cov_a, uint32_t* cov_b)
 int orc_sh_words(int codec, int degree);
 int orc_encode_sh(const rdx_table* raw, int codec, uint32_t* words, int stride);
 
+/* PlyFile.read (src/core/ply.ts:58-264) in float64 into raw-table columns
+   (centers [n][3], log_scales [n][3], quats [n][4] normalised x y z w,
+   opacities [n], colors [n][1 + K][3] of degree sh_degree, -1: the file's);
+   the count, the file's SH degree and kind (0 standard, 1 point cloud,
+   2 compressed) come back. -1 on a malformed file. */
+int orc_ply_decode(const uint8_t* bytes, uint64_t nbytes, int sh_degree, double* centers, double* log_scales,
+                   double* quats, double* opacities, double* colors, uint64_t* count, int* degree, int* kind);
+
 /* The reference's defaults (src/render/splatParams.ts:68-72) */
 void orc_params_default(rdx_params* p);
 

@@ -70,6 +70,7 @@ def lib():
                                 ctypes.POINTER(_abi.rdx_params), i, i, i, ctypes.POINTER(orc_outputs)]),
             "orc_encode_ext_table": (i, [ctypes.POINTER(_abi.rdx_table), vp, vp, vp]),
             "orc_sh_basis_grad": (None, [vp, vp]),
+            "orc_ply_decode": (i, [vp, ctypes.c_uint64, i, vp, vp, vp, vp, vp, vp, vp, vp]),
             "orc_load_splat": (None, [ctypes.POINTER(_abi.rdx_table), ctypes.c_uint64, ctypes.POINTER(orc_splat)]),
             "orc_encode_packed_table": (i, [ctypes.POINTER(_abi.rdx_table), vp, vp]),
             "orc_encode_cov_table": (i, [ctypes.POINTER(_abi.rdx_table), vp, vp]),
@@ -307,3 +308,26 @@ def load_splat(table, i):
     return {"center": np.array(sp.center[:]), "scales": np.array(sp.scales[:]), "quat": np.array(sp.quat[:]),
             "opacity": sp.opacity, "rgb": np.array(sp.rgb[:]), "sh": np.array(sp.sh[:k]),
             "cov": np.array(sp.cov[:]) if sp.has_cov else None}
+
+
+def ply_decode(data, sh_degree=-1):
+    """orc_ply_decode of PLY bytes: a dict of float64 raw-table columns plus
+    count, sh_degree (the file's) and kind (0 standard, 1 points, 2 compressed)."""
+    buf = np.frombuffer(bytes(data), dtype=np.uint8)
+    n = ctypes.c_uint64(0)
+    deg = ctypes.c_int(0)
+    kind = ctypes.c_int(0)
+    if lib().orc_ply_decode(_p(buf), buf.size, -1, None, None, None, None, None, ctypes.byref(n), ctypes.byref(deg),
+                            ctypes.byref(kind)) != 0:
+        raise ValueError("orc_ply_decode: malformed PLY")
+    d = deg.value if sh_degree < 0 else sh_degree
+    count = n.value
+    row = ((d + 1) ** 2) * 3
+    out = {"centers": np.zeros((count, 3)), "log_scales": np.zeros((count, 3)), "quats": np.zeros((count, 4)),
+           "opacities": np.zeros(count), "colors": np.zeros((count, row // 3, 3))}
+    if lib().orc_ply_decode(_p(buf), buf.size, d, _p(out["centers"]), _p(out["log_scales"]), _p(out["quats"]),
+                            _p(out["opacities"]), _p(out["colors"]), ctypes.byref(n), ctypes.byref(deg),
+                            ctypes.byref(kind)) != 0:
+        raise ValueError("orc_ply_decode: malformed PLY")
+    out.update(count=count, sh_degree=deg.value, kind=kind.value, degree=d)
+    return out

@@ -130,6 +130,10 @@ class rdx_table_grads(ctypes.Structure):
     _fields_ = [(name, ctypes.c_void_p) for name in ("centers", "log_scales", "quats", "opacities", "colors")]
 
 
+class rdx_ply_info(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_uint64), ("sh_degree", ctypes.c_int32), ("kind", ctypes.c_int32)]
+
+
 class rdx_outputs(ctypes.Structure):
     _fields_ = [
         ("mean2d", ctypes.c_void_p),
@@ -178,6 +182,9 @@ SIGNATURES = {
     "rdx_project_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_object), ctypes.c_int,
                                             ctypes.POINTER(rdx_camera), ctypes.POINTER(rdx_params),
                                             ctypes.POINTER(rdx_grads_in), ctypes.POINTER(rdx_table_grads)]),
+    "rdx_ply_read_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(rdx_ply_info)]),
+    "rdx_decode_ply": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_frame_batched": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_view), ctypes.c_int, ctypes.POINTER(rdx_params),
                                          ctypes.c_int, ctypes.POINTER(rdx_outputs), ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_batch_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_view), ctypes.c_int, ctypes.POINTER(rdx_params),

@@ -1429,6 +1429,85 @@ int rdx_project_backward(rdx_ctx* ctx, const rdx_object* objects, int n_objects,
   return RDX_OK;
 }
 
+// The header of a PLY file (host or device bytes) into desc
+static int read_ply_header(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx::PlyDesc* d) {
+  if (!bytes || nbytes == 0) return fail(ctx, RDX_ERR_ARG, "Invalid PLY header");
+  const size_t head = (size_t)std::min<uint64_t>(nbytes, 64 * 1024);  // HEADER_MAX_BYTES (ply.ts:16)
+  std::vector<unsigned char> buf(head);
+  if (is_device_ptr(bytes)) {
+    RDX_CUDA(cudaMemcpy(buf.data(), bytes, head, cudaMemcpyDeviceToHost), "PLY header copy");
+  } else {
+    memcpy(buf.data(), bytes, head);
+  }
+  const char* err = rdx::parse_ply_header(buf.data(), head, nbytes, d);
+  return err ? fail(ctx, RDX_ERR_ARG, "%s", err) : RDX_OK;
+}
+
+int rdx_ply_read_info(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx_ply_info* info) {
+  if (!ctx || !info) return RDX_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  rdx::PlyDesc d;
+  int s = read_ply_header(ctx, bytes, nbytes, &d);
+  if (s != RDX_OK) return s;
+  info->count = d.count;
+  info->sh_degree = d.sh_degree;
+  info->kind = d.kind;
+  return RDX_OK;
+}
+
+int rdx_decode_ply(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, int sh_degree, float* centers, float* log_scales,
+                   float* quats, float* opacities, float* colors) {
+  if (!ctx) return RDX_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  rdx::PlyDesc d;
+  int s = read_ply_header(ctx, bytes, nbytes, &d);
+  if (s != RDX_OK) return s;
+  if (sh_degree < 0) sh_degree = d.sh_degree;
+  if (sh_degree > d.sh_degree)
+    return fail(ctx, RDX_ERR_ARG, "the file has SH degree %d, not %d", d.sh_degree, sh_degree);
+  d.out_degree = sh_degree;
+  const uint64_t n = d.count;
+  const size_t row = (size_t)(1 + kShCoeffs[sh_degree]) * 3;
+  const bool host_in = !is_device_ptr(bytes);
+  if (quats && is_device_ptr(quats) && !aligned(quats, 16)) return fail(ctx, RDX_ERR_ARG, "quats is not 16-byte aligned");
+  OutPlan plan;
+  const unsigned char* dev_bytes = nullptr;
+  float *c = nullptr, *l = nullptr, *q = nullptr, *o = nullptr, *col = nullptr;
+  int status = RDX_OK;
+  auto layout = [&](Arena& a) {
+    plan = OutPlan();
+    dev_bytes = host_in ? a.take<unsigned char>(nbytes) : reinterpret_cast<const unsigned char*>(bytes);
+    c = stage_out(ctx, a, centers, n * 12, 4, plan, &status);
+    l = stage_out(ctx, a, log_scales, n * 12, 4, plan, &status);
+    q = stage_out(ctx, a, quats, n * 16, 16, plan, &status);
+    o = stage_out(ctx, a, opacities, n * 4, 4, plan, &status);
+    col = stage_out(ctx, a, colors, n * row * 4, 4, plan, &status);
+  };
+  Arena dry(nullptr);
+  layout(dry);
+  if (status != RDX_OK) return status;
+  s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  layout(a);
+  if (status != RDX_OK) return status;
+  if (host_in) RDX_CUDA(cudaMemcpyAsync((void*)dev_bytes, bytes, nbytes, cudaMemcpyHostToDevice, ctx->stream), "PLY copy");
+  // the header's byte offsets into device addresses
+  d.vertex = dev_bytes + (uintptr_t)d.vertex;
+  if (d.kind == rdx::kPlyCompressed) {
+    d.chunk = dev_bytes + (uintptr_t)d.chunk;
+    if (d.sh) d.sh = dev_bytes + (uintptr_t)d.sh;
+  }
+  {
+    Phase decoding(ctx, RDX_PHASE_PROJECT);
+    RDX_CUDA(rdx::launch_decode_ply(d, c, l, q, o, col, ctx->stream), "PLY decode launch");
+    if (n) ctx->launches += 1;
+  }
+  s = copy_back(ctx, plan);
+  if (s != RDX_OK) return s;
+  return host_in || !plan.back.empty() ? finish(ctx) : RDX_OK;
+}
+
 int rdx_frame_batched(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx_params* params, int sort_bits,
                       const rdx_outputs* out, uint32_t* ordering, uint32_t* visible) {
   if (!ctx) return RDX_ERR_ARG;

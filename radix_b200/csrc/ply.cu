@@ -1,0 +1,397 @@
+// PLY files to raw tables on the device: the splat values of PlyFile.read
+// (src/core/ply.ts:58-164) for standard 3DGS files and RGB point clouds, and
+// of its compressed reader (ply.ts:170-264, SuperSplat / PlayCanvas chunks),
+// written as float32 columns (centres, ln scales, normalised quaternions
+// x y z w, opacities, base rgb + SH coefficient-major) instead of Radix's
+// quantised layouts. The header is read on the host; one thread decodes a
+// splat, in float64, and rounds once to float32.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "rdx_internal.h"
+
+namespace rdx {
+
+namespace {
+
+constexpr double kShC0 = 0.28209479177387814;  // ply.ts:15
+constexpr int kTypeBytes[8] = {1, 1, 2, 2, 4, 4, 4, 8};  // host copy (the header's record sizes)
+
+__device__ __forceinline__ int type_bytes(int t) { return t <= 1 ? 1 : (t <= 3 ? 2 : (t <= 6 ? 4 : 8)); }
+
+// TYPES[type].scale of a normalised read (ply.ts:33-42)
+__device__ __forceinline__ double type_scale(int t) {
+  switch (t) {
+    case 0: return 127.0;
+    case 1: return 255.0;
+    case 2: return 32767.0;
+    case 3: return 65535.0;
+    case 4: return 2147483647.0;
+    case 5: return 4294967295.0;
+    default: return 1.0;
+  }
+}
+
+// One scalar of a record, in the file's byte order (byte loads: records need not be aligned)
+__device__ __forceinline__ double read_value(const unsigned char* rec, PlyProp p, bool little, bool normalized) {
+  const unsigned char* at = rec + p.offset;
+  const int n = type_bytes(p.type);
+  uint64_t bits = 0;
+  for (int b = 0; b < n; b++) {
+    const uint64_t byte = at[b];
+    bits |= little ? byte << (8 * b) : byte << (8 * (n - 1 - b));
+  }
+  double v;
+  switch (p.type) {
+    case 0: v = (double)(int8_t)(uint8_t)bits; break;
+    case 1: v = (double)(uint8_t)bits; break;
+    case 2: v = (double)(int16_t)(uint16_t)bits; break;
+    case 3: v = (double)(uint16_t)bits; break;
+    case 4: v = (double)(int32_t)(uint32_t)bits; break;
+    case 5: v = (double)(uint32_t)bits; break;
+    case 6: v = (double)__uint_as_float((uint32_t)bits); break;
+    default: v = __longlong_as_double((long long)bits); break;
+  }
+  return normalized ? v / type_scale(p.type) : v;
+}
+
+__device__ __forceinline__ uint32_t read_word(const unsigned char* rec, PlyProp p, bool little) {
+  const unsigned char* at = rec + p.offset;
+  return little ? (uint32_t)at[0] | ((uint32_t)at[1] << 8) | ((uint32_t)at[2] << 16) | ((uint32_t)at[3] << 24)
+                : (uint32_t)at[3] | ((uint32_t)at[2] << 8) | ((uint32_t)at[1] << 16) | ((uint32_t)at[0] << 24);
+}
+
+// splat-transform's SH byte over [-4, 4] (ply.ts:267-270)
+__device__ __forceinline__ double compressed_sh(uint32_t byte) {
+  return ((byte == 0u ? 0.0 : (byte == 255u ? 1.0 : ((double)byte + 0.5) / 256.0)) - 0.5) * 8.0;
+}
+
+__global__ void k_decode_ply(const PlyDesc d, float* __restrict__ centers, float* __restrict__ log_scales,
+                             float* __restrict__ quats, float* __restrict__ opacities, float* __restrict__ colors) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= d.count) return;
+  const bool little = d.little != 0;
+  const int kvals = (d.out_degree == 0 ? 0 : (d.out_degree == 1 ? 3 : (d.out_degree == 2 ? 8 : (d.out_degree == 3 ? 15 : 24)))) * 3;
+  const int row = 3 + kvals;
+  double c[3], ls[3], q[4], op, rgb[3];
+  float* col = colors ? colors + i * (uint64_t)row : nullptr;
+  if (d.kind == kPlyCompressed) {
+    const unsigned char* v = d.vertex + i * d.record;
+    const unsigned char* ch = d.chunk + (i / 256) * d.chunk_record;
+    double r[18];
+    const double defaults[6] = {0.0, 0.0, 0.0, 1.0, 1.0, 1.0};
+    for (int k = 0; k < 18; k++)
+      r[k] = d.chunk_prop[k].offset >= 0 ? read_value(ch, d.chunk_prop[k], little, false) : defaults[k >= 12 ? k - 12 : 0];
+    const uint32_t p = read_word(v, d.packed[0], little);
+    c[0] = r[0] + (r[3] - r[0]) * ((double)((p >> 21) & 2047u) / 2047.0);
+    c[1] = r[1] + (r[4] - r[1]) * ((double)((p >> 11) & 1023u) / 1023.0);
+    c[2] = r[2] + (r[5] - r[2]) * ((double)(p & 2047u) / 2047.0);
+    const uint32_t l = read_word(v, d.packed[2], little);
+    ls[0] = r[6] + (r[9] - r[6]) * ((double)((l >> 21) & 2047u) / 2047.0);
+    ls[1] = r[7] + (r[10] - r[7]) * ((double)((l >> 11) & 1023u) / 1023.0);
+    ls[2] = r[8] + (r[11] - r[8]) * ((double)(l & 2047u) / 2047.0);
+    const uint32_t w = read_word(v, d.packed[1], little);
+    const double sq = 1.4142135623730951;
+    const double a = ((double)((w >> 20) & 1023u) / 1023.0 - 0.5) * sq;
+    const double b = ((double)((w >> 10) & 1023u) / 1023.0 - 0.5) * sq;
+    const double cc = ((double)(w & 1023u) / 1023.0 - 0.5) * sq;
+    const double m = sqrt(fmax(0.0, 1.0 - a * a - b * b - cc * cc));
+    const uint32_t largest = w >> 30;
+    q[3] = largest == 0u ? m : a;
+    q[0] = largest == 0u ? a : (largest == 1u ? m : b);
+    q[1] = largest <= 1u ? b : (largest == 2u ? m : cc);
+    q[2] = largest <= 2u ? cc : m;
+    const uint32_t k = read_word(v, d.packed[3], little);
+    rgb[0] = r[12] + (r[15] - r[12]) * ((double)((k >> 24) & 255u) / 255.0);
+    rgb[1] = r[13] + (r[16] - r[13]) * ((double)((k >> 16) & 255u) / 255.0);
+    rgb[2] = r[14] + (r[17] - r[14]) * ((double)((k >> 8) & 255u) / 255.0);
+    op = (double)(k & 255u) / 255.0;
+    if (col) {
+      const unsigned char* s = d.sh ? d.sh + i * d.sh_record : nullptr;
+      for (int x = 0; x < kvals; x++) col[3 + x] = s ? (float)compressed_sh(s[d.sh_byte[x]]) : 0.0f;
+    }
+  } else {
+    const unsigned char* v = d.vertex + i * d.record;
+    for (int k = 0; k < 3; k++) c[k] = read_value(v, d.xyz[k], little, false);
+    if (d.kind == kPlyStandard) {
+      for (int k = 0; k < 3; k++) ls[k] = read_value(v, d.scale[k], little, false);
+      // (rot_1, rot_2, rot_3, rot_0) = (x, y, z, w)
+      q[0] = read_value(v, d.rot[1], little, false);
+      q[1] = read_value(v, d.rot[2], little, false);
+      q[2] = read_value(v, d.rot[3], little, false);
+      q[3] = read_value(v, d.rot[0], little, false);
+      op = 1.0 / (1.0 + exp(-read_value(v, d.opacity, little, false)));
+      for (int k = 0; k < 3; k++) rgb[k] = 0.5 + kShC0 * read_value(v, d.color[k], little, false);
+      if (col)
+        for (int x = 0; x < kvals; x++) col[3 + x] = (float)read_value(v, d.rest[x], little, false);
+    } else {
+      const double point = log(0.001);  // POINT_SCALE (ply.ts:18)
+      ls[0] = ls[1] = ls[2] = point;
+      q[0] = q[1] = q[2] = 0.0;
+      q[3] = 1.0;
+      op = d.alpha.offset >= 0 ? read_value(v, d.alpha, little, true) : 1.0;
+      for (int k = 0; k < 3; k++) rgb[k] = read_value(v, d.color[k], little, true);
+      if (col)
+        for (int x = 0; x < kvals; x++) col[3 + x] = 0.0f;
+    }
+  }
+  // SplatMath.normalizeQuat (math.ts:12-27)
+  const double len = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  if (len > 0.0) {
+    for (int k = 0; k < 4; k++) q[k] /= len;
+  } else {
+    q[0] = q[1] = q[2] = 0.0;
+    q[3] = 1.0;
+  }
+  if (centers)
+    for (int k = 0; k < 3; k++) centers[i * 3 + k] = (float)c[k];
+  if (log_scales)
+    for (int k = 0; k < 3; k++) log_scales[i * 3 + k] = (float)ls[k];
+  if (quats) reinterpret_cast<float4*>(quats)[i] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+  if (opacities) opacities[i] = (float)op;
+  if (col)
+    for (int k = 0; k < 3; k++) col[k] = (float)rgb[k];
+}
+
+// ---- the header (ply.ts:362-444) ----
+
+struct Prop {
+  std::string name;
+  int type;
+  bool list;
+  int offset;
+};
+
+struct Element {
+  std::string name;
+  uint64_t count;
+  std::vector<Prop> props;
+  uint32_t record;
+};
+
+int ply_type(const std::string& name) {
+  static const char* names[8] = {"char", "uchar", "short", "ushort", "int", "uint", "float", "double"};
+  static const char* aliases[8] = {"int8", "uint8", "int16", "uint16", "int32", "uint32", "float32", "float64"};
+  for (int t = 0; t < 8; t++)
+    if (name == names[t] || name == aliases[t]) return t;
+  return -1;
+}
+
+int shdeg(int rest) { return rest >= 72 ? 4 : rest >= 45 ? 3 : rest >= 24 ? 2 : rest > 0 ? 1 : 0; }
+
+const Prop* find(const Element& e, const std::string& name) {
+  for (const Prop& p : e.props)
+    if (p.name == name && !p.list) return &p;
+  return nullptr;
+}
+
+PlyProp pp(const Prop* p) { return p ? PlyProp{p->offset, p->type} : PlyProp{-1, 6}; }
+
+std::string g_error;
+
+}  // namespace
+
+const char* parse_ply_header(const unsigned char* head, uint64_t head_bytes, uint64_t nbytes, PlyDesc* d) {
+  memset(d, 0, sizeof(*d));
+  std::string text((const char*)head, (size_t)head_bytes);
+  size_t end = text.find("end_header\n");
+  size_t end_r = text.find("end_header\r\n");
+  if (text.compare(0, 3, "ply") != 0 || (end == std::string::npos && end_r == std::string::npos))
+    return "Invalid PLY header";
+  uint64_t header_len;
+  if (end != std::string::npos && (end_r == std::string::npos || end < end_r)) {
+    header_len = end + strlen("end_header\n");
+  } else {
+    end = end_r;
+    header_len = end_r + strlen("end_header\r\n");
+  }
+  int little = -1;
+  std::vector<Element> elements;
+  size_t pos = text.find('\n') + 1;
+  while (pos < end) {
+    size_t nl = text.find('\n', pos);
+    std::string line = text.substr(pos, nl - pos);
+    pos = nl + 1;
+    if (!line.empty() && line.back() == '\r') line.pop_back();
+    std::vector<std::string> f;
+    size_t i = 0;
+    while (i < line.size()) {
+      while (i < line.size() && (line[i] == ' ' || line[i] == '\t')) i++;
+      size_t j = i;
+      while (j < line.size() && line[j] != ' ' && line[j] != '\t') j++;
+      if (j > i) f.push_back(line.substr(i, j - i));
+      i = j;
+    }
+    if (f.empty()) continue;
+    if (f[0] == "format") {
+      if (f.size() < 2 || (f[1] != "binary_little_endian" && f[1] != "binary_big_endian")) {
+        g_error = "Unsupported PLY format " + (f.size() > 1 ? f[1] : std::string());
+        return g_error.c_str();
+      }
+      little = f[1] == "binary_little_endian" ? 1 : 0;
+    } else if (f[0] == "element" && f.size() >= 3) {
+      elements.push_back(Element{f[1], (uint64_t)strtoull(f[2].c_str(), nullptr, 10), {}, 0});
+    } else if (f[0] == "property") {
+      if (elements.empty()) return "PLY property outside an element";
+      Element& e = elements.back();
+      if (f.size() >= 5 && f[1] == "list") {
+        e.props.push_back(Prop{f[4], ply_type(f[3]), true, -1});
+      } else if (f.size() >= 3) {
+        const int t = ply_type(f[1]);
+        if (t < 0) {
+          g_error = "Unsupported PLY property type " + f[1];
+          return g_error.c_str();
+        }
+        e.props.push_back(Prop{f[2], t, false, (int)e.record});
+        e.record += (uint32_t)kTypeBytes[t];
+      }
+    }
+  }
+  if (little < 0) return "PLY header has no format line";
+  d->little = little;
+  auto offset_of = [&](const Element* el, uint64_t* out) -> const char* {
+    uint64_t off = header_len;
+    for (const Element& b : elements) {
+      if (&b == el) break;
+      for (const Prop& p : b.props)
+        if (p.list) {
+          g_error = "PLY element " + b.name + " before " + el->name + " has list properties";
+          return g_error.c_str();
+        }
+      off += b.count * b.record;
+    }
+    if (off + el->count * el->record > nbytes) return "PLY file ended unexpectedly";
+    *out = off;
+    return nullptr;
+  };
+  const Element* vertex = nullptr;
+  const Element* chunk = nullptr;
+  const Element* sh = nullptr;
+  for (const Element& e : elements) {
+    if (e.name == "vertex" && !vertex) vertex = &e;
+    if (e.name == "chunk" && !chunk) chunk = &e;
+    if (e.name == "sh" && !sh) sh = &e;
+  }
+  if (!vertex) return "PLY has no vertex element";
+  d->count = vertex->count;
+  d->record = vertex->record;
+  uint64_t off = 0;
+  const char* err;
+  const char* packed_names[4] = {"packed_position", "packed_rotation", "packed_scale", "packed_color"};
+  bool compressed = chunk != nullptr;
+  for (int k = 0; k < 4 && compressed; k++) compressed = find(*vertex, packed_names[k]) != nullptr;
+  if (compressed) {
+    for (const Element* el : {chunk, vertex})
+      for (const Prop& p : el->props)
+        if (p.list) {
+          g_error = "PLY " + el->name + " list properties are not supported";
+          return g_error.c_str();
+        }
+    static const char* chunk_names[18] = {"min_x", "min_y", "min_z", "max_x", "max_y", "max_z",
+                                          "min_scale_x", "min_scale_y", "min_scale_z", "max_scale_x", "max_scale_y", "max_scale_z",
+                                          "min_r", "min_g", "min_b", "max_r", "max_g", "max_b"};
+    std::string missing;
+    for (int k = 0; k < 12; k++)
+      if (!find(*chunk, chunk_names[k])) missing += (missing.empty() ? "" : ", ") + std::string(chunk_names[k]);
+    if (!missing.empty()) {
+      g_error = "PLY chunk lacks " + missing;
+      return g_error.c_str();
+    }
+    const uint64_t chunks = (vertex->count + 255) / 256;
+    if (chunk->count < chunks) {
+      g_error = "PLY has " + std::to_string(chunk->count) + " chunks for " + std::to_string(vertex->count) + " splats";
+      return g_error.c_str();
+    }
+    d->kind = kPlyCompressed;
+    for (int k = 0; k < 18; k++) d->chunk_prop[k] = pp(find(*chunk, chunk_names[k]));
+    for (int k = 0; k < 4; k++) {
+      const Prop* p = find(*vertex, packed_names[k]);
+      if (kTypeBytes[p->type] != 4) return "PLY packed words must be 32-bit";
+      d->packed[k] = pp(p);
+    }
+    uint64_t coff = 0;
+    if ((err = offset_of(chunk, &coff))) return err;
+    d->chunk = (const unsigned char*)(uintptr_t)coff;
+    d->chunk_record = chunk->record;
+    int rest = 0;
+    if (sh)
+      while (find(*sh, "f_rest_" + std::to_string(rest))) rest++;
+    d->sh_degree = (sh && sh->count >= vertex->count) ? shdeg(rest) : 0;
+    if (sh && d->sh_degree > 0) {
+      uint64_t soff = 0;
+      if ((err = offset_of(sh, &soff))) return err;
+      d->sh = (const unsigned char*)(uintptr_t)soff;
+      d->sh_record = sh->record;
+      const int per = rest / 3;
+      const int vals = (d->sh_degree == 1 ? 3 : d->sh_degree == 2 ? 8 : d->sh_degree == 3 ? 15 : 24) * 3;
+      for (int v = 0; v < vals; v++) {
+        const Prop* p = find(*sh, "f_rest_" + std::to_string((v % 3) * per + v / 3));
+        d->sh_byte[v] = p ? p->offset : 0;
+      }
+    }
+  } else {
+    static const char* standard[14] = {"x", "y", "z", "scale_0", "scale_1", "scale_2", "rot_0", "rot_1", "rot_2", "rot_3",
+                                       "opacity", "f_dc_0", "f_dc_1", "f_dc_2"};
+    static const char* cloud[6] = {"x", "y", "z", "red", "green", "blue"};
+    bool is_standard = true, is_cloud = true, any_standard = false;
+    for (const char* n : standard) {
+      const bool h = find(*vertex, n) != nullptr;
+      is_standard = is_standard && h;
+      any_standard = any_standard || h;
+    }
+    for (const char* n : cloud) is_cloud = is_cloud && find(*vertex, n) != nullptr;
+    if (!is_standard && !is_cloud) {
+      std::string missing;
+      if (any_standard) {
+        for (const char* n : standard)
+          if (!find(*vertex, n)) missing += (missing.empty() ? "" : ", ") + std::string(n);
+      } else {
+        for (const char* n : cloud)
+          if (!find(*vertex, n)) missing += (missing.empty() ? "" : ", ") + std::string(n);
+      }
+      g_error = "PLY vertex lacks " + missing;
+      return g_error.c_str();
+    }
+    for (const Prop& p : vertex->props)
+      if (p.list) return "PLY vertex list properties are not supported";
+    d->kind = is_standard ? kPlyStandard : kPlyPoints;
+    for (int k = 0; k < 3; k++) d->xyz[k] = pp(find(*vertex, standard[k]));
+    if (is_standard) {
+      for (int k = 0; k < 3; k++) d->scale[k] = pp(find(*vertex, standard[3 + k]));
+      for (int k = 0; k < 4; k++) d->rot[k] = pp(find(*vertex, standard[6 + k]));
+      d->opacity = pp(find(*vertex, "opacity"));
+      for (int k = 0; k < 3; k++) d->color[k] = pp(find(*vertex, standard[11 + k]));
+      int rest = 0;
+      while (find(*vertex, "f_rest_" + std::to_string(rest))) rest++;
+      d->sh_degree = shdeg(rest);
+      const int per = rest / 3;
+      const int vals = (d->sh_degree == 0 ? 0 : d->sh_degree == 1 ? 3 : d->sh_degree == 2 ? 8 : d->sh_degree == 3 ? 15 : 24) * 3;
+      for (int v = 0; v < vals; v++) d->rest[v] = pp(find(*vertex, "f_rest_" + std::to_string((v % 3) * per + v / 3)));
+    } else {
+      for (int k = 0; k < 3; k++) d->color[k] = pp(find(*vertex, cloud[3 + k]));
+      d->alpha = pp(find(*vertex, "alpha"));
+      d->sh_degree = 0;
+    }
+  }
+  if ((err = offset_of(vertex, &off))) return err;
+  d->vertex = (const unsigned char*)(uintptr_t)off;
+  d->out_degree = d->sh_degree;
+  return nullptr;
+}
+
+cudaError_t launch_decode_ply(const PlyDesc& desc, float* centers, float* log_scales, float* quats, float* opacities,
+                              float* colors, cudaStream_t stream) {
+  if (desc.count == 0) return cudaSuccess;
+  const uint32_t threads = 128;
+  const uint64_t blocks = (desc.count + threads - 1) / threads;
+  k_decode_ply<<<(unsigned)blocks, threads, 0, stream>>>(desc, centers, log_scales, quats, opacities, colors);
+  return cudaGetLastError();
+}
+
+}  // namespace rdx

@@ -178,6 +178,48 @@ struct ProjHist {
 };
 
 // One persistent launch over every descriptor of one table kind (descs in device memory)
+// ---- PLY files (src/core/ply.ts) to raw tables ----
+
+constexpr int kPlyRest = 72;  // f_rest_* values of SH degree 4
+
+// A scalar property of a record: byte offset (-1: absent) and type
+// (0 char, 1 uchar, 2 short, 3 ushort, 4 int, 5 uint, 6 float, 7 double)
+struct PlyProp {
+  int32_t offset;
+  int32_t type;
+};
+
+enum PlyKind { kPlyStandard = 0, kPlyPoints = 1, kPlyCompressed = 2 };
+
+// Where a file's values are, with the header already read on the host
+struct PlyDesc {
+  int32_t kind;
+  int32_t little;           // binary_little_endian
+  int32_t sh_degree;        // of the file
+  int32_t out_degree;       // of the rows written
+  uint64_t count;           // splats
+  const unsigned char* vertex;  // the first vertex record (device memory)
+  uint32_t record;          // bytes per vertex record
+  PlyProp xyz[3], scale[3], rot[4], opacity, color[3], alpha;
+  PlyProp rest[kPlyRest];   // coefficient-major (value 3k + c is f_rest_{c * N + k})
+  // compressed files: per-chunk ranges and packed words
+  const unsigned char* chunk;
+  uint32_t chunk_record;
+  PlyProp chunk_prop[18];   // min/max x y z, min/max scale x y z, min/max r g b (absent: 0, 0, 0, 1, 1, 1)
+  PlyProp packed[4];        // packed_position, packed_rotation, packed_scale, packed_color
+  const unsigned char* sh;  // the sh element (null: none)
+  uint32_t sh_record;
+  int32_t sh_byte[kPlyRest]; // coefficient-major byte offsets in an sh record
+};
+
+// Host: read a PLY header (the first bytes of a file of nbytes) into desc;
+// 0 or an error text. vertex, chunk and sh are byte offsets into the file.
+const char* parse_ply_header(const unsigned char* head, uint64_t head_bytes, uint64_t nbytes, PlyDesc* desc);
+
+// Device: rows [0, count) of a raw table of degree out_degree
+cudaError_t launch_decode_ply(const PlyDesc& desc, float* centers, float* log_scales, float* quats, float* opacities,
+                              float* colors, cudaStream_t stream);
+
 // ---- the projection's gradient (raw tables) ----
 
 // Upstream gradients laid out as the forward's outputs ([E][n]...; null: zero)
