@@ -72,9 +72,33 @@ __device__ __forceinline__ double compressed_sh(uint32_t byte) {
   return ((byte == 0u ? 0.0 : (byte == 255u ? 1.0 : ((double)byte + 0.5) / 256.0)) - 0.5) * 8.0;
 }
 
+// STAGED: the block's vertex records are first copied into shared memory
+// with coalesced word loads, then each thread parses its record there
+template <bool STAGED>
 __global__ void k_decode_ply(const PlyDesc d, float* __restrict__ centers, float* __restrict__ log_scales,
                              float* __restrict__ quats, float* __restrict__ opacities, float* __restrict__ colors) {
-  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  const uint64_t r0 = (uint64_t)blockIdx.x * blockDim.x;
+  const uint64_t i = r0 + threadIdx.x;
+  const unsigned char* staged = nullptr;
+  if constexpr (STAGED) {
+    // s[x] holds byte x of the block's records; the copy's words are aligned
+    // in both memories (the buffer starts at the source's offset mod 4)
+    const uint64_t rows = min((uint64_t)blockDim.x, d.count - r0);
+    const unsigned char* src = d.vertex + r0 * d.record;
+    const uint64_t len = rows * d.record;
+    const uint32_t off = (uint32_t)((uintptr_t)src & 3u);
+    unsigned char* buf = s_raw + off;
+    const uint64_t head = min((uint64_t)((4u - off) & 3u), len);
+    const uint64_t words = (len - head) / 4;
+    for (uint64_t b = threadIdx.x; b < head; b += blockDim.x) buf[b] = src[b];
+    const uint32_t* sw = reinterpret_cast<const uint32_t*>(src + head);
+    uint32_t* dw = reinterpret_cast<uint32_t*>(buf + head);
+    for (uint64_t w = threadIdx.x; w < words; w += blockDim.x) dw[w] = __ldg(sw + w);
+    for (uint64_t b = head + words * 4 + threadIdx.x; b < len; b += blockDim.x) buf[b] = src[b];
+    __syncthreads();
+    staged = buf;
+  }
   if (i >= d.count) return;
   const bool little = d.little != 0;
   const int kvals = (d.out_degree == 0 ? 0 : (d.out_degree == 1 ? 3 : (d.out_degree == 2 ? 8 : (d.out_degree == 3 ? 15 : 24)))) * 3;
@@ -117,7 +141,7 @@ __global__ void k_decode_ply(const PlyDesc d, float* __restrict__ centers, float
       for (int x = 0; x < kvals; x++) col[3 + x] = s ? (float)compressed_sh(s[d.sh_byte[x]]) : 0.0f;
     }
   } else {
-    const unsigned char* v = d.vertex + i * d.record;
+    const unsigned char* v = STAGED ? staged + (i - r0) * d.record : d.vertex + i * d.record;
     for (int k = 0; k < 3; k++) c[k] = read_value(v, d.xyz[k], little, false);
     if (d.kind == kPlyStandard) {
       for (int k = 0; k < 3; k++) ls[k] = read_value(v, d.scale[k], little, false);
@@ -390,7 +414,13 @@ cudaError_t launch_decode_ply(const PlyDesc& desc, float* centers, float* log_sc
   if (desc.count == 0) return cudaSuccess;
   const uint32_t threads = 128;
   const uint64_t blocks = (desc.count + threads - 1) / threads;
-  k_decode_ply<<<(unsigned)blocks, threads, 0, stream>>>(desc, centers, log_scales, quats, opacities, colors);
+  // standard files and point clouds: records staged through shared memory when a block's fit in 48 KB
+  const size_t smem = (size_t)threads * desc.record + 4;
+  if (desc.kind != kPlyCompressed && smem <= 48 * 1024) {
+    k_decode_ply<true><<<(unsigned)blocks, threads, smem, stream>>>(desc, centers, log_scales, quats, opacities, colors);
+  } else {
+    k_decode_ply<false><<<(unsigned)blocks, threads, 0, stream>>>(desc, centers, log_scales, quats, opacities, colors);
+  }
   return cudaGetLastError();
 }
 
