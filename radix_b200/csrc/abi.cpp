@@ -191,21 +191,25 @@ uint32_t tiles_of(uint64_t n) { return (uint32_t)((n + rdx::kSortTile - 1) / rdx
 // Sort scratch for `segments` segments of `total` keys
 rdx::SortScratch take_sort_scratch(Arena& a, int segments, int passes, uint64_t total) {
   rdx::SortScratch s{};
-  // hist, valid, ref_hidden and counters contiguous (one memset)
-  uint32_t* small = a.take<uint32_t>(rdx::sort_small_state_words(segments, passes));
+  // hist, valid, ref_hidden, counters and tile_valid contiguous (one memset); each
+  // segment adds at most one partial tile
+  const uint32_t max_tiles = tiles_of(total) + (uint32_t)segments;
+  uint32_t* small = a.take<uint32_t>(rdx::sort_small_state_words(segments, passes, max_tiles));
   if (small) {
     s.hist = small;
     s.valid = small + (size_t)segments * passes * rdx::kRadix;
     s.ref_hidden = s.valid + segments;
     s.counters = s.ref_hidden + segments;
+    s.tile_valid = s.counters + passes + 1;
   }
   s.vbegin = a.take<uint64_t>(segments);
   s.vend = a.take<uint64_t>(segments);
   s.vtiles = a.take<uint32_t>(segments + 1);
+  // Ping-pong pairs: the partition and every pass but the last write one of them
   s.keys_a = a.take<uint32_t>(total);
   s.vals_a = a.take<uint32_t>(total);
-  s.keys_b = a.take<uint32_t>(passes > 2 ? total : 0);
-  s.vals_b = a.take<uint32_t>(passes > 2 ? total : 0);
+  s.keys_b = a.take<uint32_t>(total);
+  s.vals_b = a.take<uint32_t>(total);
   return s;
 }
 
@@ -1144,7 +1148,8 @@ cudaError_t enqueue_frame(rdx_ctx* timing, const ProjectCall& call, const FrameD
   cudaError_t e;
   rdx::ProjHist hist{nullptr, nullptr, 0};
   if (sorting) {
-    e = cudaMemsetAsync(fd.sc.hist, 0, rdx::sort_small_state_words(views, passes) * 4, stream);
+    e = cudaMemsetAsync(fd.sc.hist, 0, rdx::sort_small_state_words(views, passes, segment_tiles(call, nullptr)) * 4,
+                        stream);
     if (e != cudaSuccess) return e;
     hist = rdx::ProjHist{fd.sc.hist, fd.sc.valid, passes};
   }

@@ -28,6 +28,7 @@ __global__ void k_keys_f32(const float* __restrict__ d, uint64_t n, int bits, ui
 
 __global__ void k_visible(const uint64_t* begin, const uint64_t* end, const uint32_t* ref_hidden,
                           const uint32_t* valid, int segments, uint32_t* visible) {
+  pdl_wait();
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s < segments) visible[s] = ref_hidden ? (uint32_t)(end[s] - begin[s]) - ref_hidden[s] : valid[s];
 }
@@ -162,8 +163,7 @@ cudaError_t launch_keys_f32(const float* d, uint64_t n, int bits, uint32_t* keys
 
 cudaError_t launch_visible(const uint64_t* begin, const uint64_t* end, const uint32_t* ref_hidden,
                            const uint32_t* valid, int segments, uint32_t* visible, cudaStream_t s) {
-  k_visible<<<(segments + 127) / 128, 128, 0, s>>>(begin, end, ref_hidden, valid, segments, visible);
-  return cudaGetLastError();
+  return launch_after(k_visible, (segments + 127) / 128, 128, 0, s, begin, end, ref_hidden, valid, segments, visible);
 }
 
 cudaError_t launch_compact(const uint32_t* keys, uint64_t n, uint32_t invalid, uint32_t* keys_out, uint32_t* vals_out,

@@ -32,8 +32,8 @@ constexpr int kMaxDevices = 64;
 
 // Byte offsets inside the array (every region 256-byte aligned)
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
-constexpr size_t kSmallOff = 0;  // hist, valid, ref_hidden, counters (zeroed per call)
-constexpr size_t kSmallBytes = align256((size_t)(kMaxPasses * kRadix + 2 + kMaxPasses) * 4);
+constexpr size_t kSmallOff = 0;  // hist, valid, ref_hidden, counters, tile counts (zeroed per call)
+constexpr size_t kSmallBytes = align256((size_t)(kMaxPasses * kRadix + 2 + kMaxPasses + 1 + kNoAllocMaxTiles) * 4);
 constexpr size_t kSegOff = kSmallOff + kSmallBytes;  // begin, end, tiles[2], vbegin, vend, vtiles[2]
 constexpr size_t kSegBytes = 256;
 constexpr size_t kFlagOff = kSegOff + kSegBytes;  // error flag, visible, lookback epoch
@@ -117,6 +117,7 @@ extern "C" int rdx_sort_noalloc(const uint32_t* keys, uint64_t count, int bits, 
   sc.valid = small + (size_t)passes * kRadix;
   sc.ref_hidden = sc.valid + 1;
   sc.counters = sc.ref_hidden + 1;
+  sc.tile_valid = sc.counters + passes + 1;
   uint64_t* seg64 = reinterpret_cast<uint64_t*>(b + kSegOff);
   uint64_t* begin = seg64;
   uint64_t* end = seg64 + 1;

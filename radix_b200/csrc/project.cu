@@ -425,6 +425,7 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
     if (lane == 0) W.valid = 0;
   }
   __syncwarp();
+  pdl_trigger();  // the sort's set-up kernel may be placed now; it waits for this grid to complete
 
   int cur_desc = -1;
   int cur_seg = -1;

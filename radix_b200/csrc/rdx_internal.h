@@ -4,9 +4,40 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "../../include/radix_b200.h"
 
 namespace rdx {
+
+// ---- programmatic dependent launch ----
+// A kernel launched with launch_after() may start while the kernel before it
+// in the stream is still running, once every block of that kernel has called
+// pdl_trigger() (or exited); it calls pdl_wait() before it touches anything
+// the earlier kernel writes, which returns when that kernel has completed and
+// its writes are visible. Both are no-ops in a kernel launched plainly, and
+// the launch attribute has no effect when the previous operation in the
+// stream is not a kernel (a copy or a memset keeps full ordering).
+#ifdef __CUDACC__
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... Params, typename... Args>
+cudaError_t launch_after(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                         Args&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+#endif
 
 // ---- sort ----
 
@@ -37,7 +68,8 @@ struct SortScratch {
   uint32_t* hist;        // [S][passes][256] digit counts of the valid keys
   uint32_t* valid;       // [S] keys below 2^bits - 1
   uint32_t* ref_hidden;  // [S] keys the reference's visible count leaves out
-  uint32_t* counters;    // [passes] tile counters
+  uint32_t* counters;    // [passes + 1] tile counters (the last: the partition's)
+  uint32_t* tile_valid;  // [max_tiles] valid keys of each tile
   uint64_t* vbegin;      // [S] segments of the valid keys (passes after the first)
   uint64_t* vend;        // [S]
   uint32_t* vtiles;      // [S + 1]
@@ -47,8 +79,8 @@ struct SortScratch {
   uint32_t* vals_b;
 };
 
-// hist, valid, ref_hidden and counters are contiguous: words zeroed before a sort
-size_t sort_small_state_words(int segments, int passes);
+// hist, valid, ref_hidden, counters and tile_valid are contiguous: words zeroed before a sort
+size_t sort_small_state_words(int segments, int passes, uint32_t max_tiles);
 
 // Sort segments of keys_in (values: vals_in, or each key's index within its
 // segment when vals_in is null) into keys_out / vals_out (keys_out may be null:

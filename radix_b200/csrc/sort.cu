@@ -8,9 +8,12 @@
 // contiguous.
 //
 // The largest key of a width (2^bits - 1, the invalid key of SortKeys) sorts
-// after every other key, its copies in input order. The first pass therefore
-// writes them straight to the tail of each segment's output, and the later
-// passes sort only the rest: a frame's culled splats cost one pass, not four.
+// after every other key, its copies in input order. When outputs do not alias
+// inputs, a stable partition kernel (offsets from per-tile valid counts
+// counted before it, no digit ranking) first writes them straight to the tail
+// of each segment's output and packs the other keys, in order, at the
+// segment's front; every digit pass then sorts only those: a frame's culled
+// splats are read twice and written once, never ranked.
 //
 // Replaces WgpuRadixSort (src/wgpu/WgpuRadixSort.ts:43-361: 3 dispatches per
 // pass, histogram / scanBlocks / scatter with 8 one-bit splits), WgpuCompact
@@ -128,9 +131,10 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint32_t* __re
                                                             SortSegments segs, int tiles_per_block,
                                                             uint32_t* __restrict__ hist,
                                                             uint32_t* __restrict__ valid_count,
-                                                            uint32_t* __restrict__ ref_hidden) {
+                                                            uint32_t* __restrict__ ref_hidden,
+                                                            uint32_t* __restrict__ tile_valid) {
   __shared__ uint32_t sh[PASSES][kRadix];
-  __shared__ uint32_t s_hidden, s_valid;
+  __shared__ uint32_t s_hidden, s_valid, s_tile_valid;
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const uint32_t total_tiles = segs.tiles[segs.count];
@@ -139,7 +143,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint32_t* __re
   const uint32_t tile_end = min(tile0 + (uint32_t)tiles_per_block, total_tiles);
 #pragma unroll
   for (int p = 0; p < PASSES; p++) sh[p][tid] = 0;
-  if (tid == 0) s_hidden = s_valid = 0;
+  if (tid == 0) s_hidden = s_valid = s_tile_valid = 0;
   __syncthreads();
 
   int seg = segment_of(segs.tiles, segs.count, tile0);
@@ -173,6 +177,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint32_t* __re
     }
     const uint64_t base = segs.begin[seg] + (uint64_t)(tile - segs.tiles[seg]) * kSortTile;
     const uint32_t n = (uint32_t)min((uint64_t)kSortTile, segs.end[seg] - base);
+    uint32_t in_tile = 0;
 #pragma unroll 4
     for (int j = 0; j < kSortItems; j++) {
       const uint32_t pos = (uint32_t)j * kSortThreads + tid;
@@ -180,32 +185,171 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint32_t* __re
       const uint32_t k = in ? __ldg(&keys[base + pos]) & key_mask : key_mask;
       hidden += in && (k >> ref_shift) == ref_top;
       const bool valid = in && (!drop || k != key_mask);
-      nvalid += valid;
+      in_tile += valid;
 #pragma unroll
       for (int p = 0; p < PASSES; p++) hist_add(sh[p], (k >> (8 * p)) & 0xffu, valid);
+    }
+    nvalid += in_tile;
+    // the tile's valid keys, for the partition's offsets
+    const uint32_t w = __reduce_add_sync(0xffffffffu, in_tile);
+    if (lane == 0 && w) atomicAdd(&s_tile_valid, w);
+    __syncthreads();
+    if (tid == 0) {
+      tile_valid[tile] = s_tile_valid;
+      s_tile_valid = 0;
     }
   }
   flush(seg);
 }
 
-// Segments of the valid keys after the first pass: [begin, begin + valid)
-// Also advances the lookback epoch: the word is bumped on the device, so a
-// sort replayed from a CUDA graph still tags its words with a new epoch
-__global__ void k_compacted_segments(SortSegments full, const uint32_t* __restrict__ valid_count, uint64_t* begin,
-                                     uint64_t* end, uint32_t* tiles, uint32_t* epoch) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const uint32_t e = *epoch + 1u;
-  *epoch = e == 0u ? 1u : e;  // 0 marks a cleared word
-  uint32_t t = 0;
-  for (int s = 0; s < full.count; s++) {
-    const uint64_t b = full.begin[s];
-    const uint64_t v = min((uint64_t)valid_count[s], full.end[s] - b);
-    begin[s] = b;
-    end[s] = b + v;
-    tiles[s] = t;
-    t += (uint32_t)((v + kSortTile - 1) / kSortTile);
+// Set-up of the digit passes. Block 0's first thread writes the segments of
+// the valid keys, [begin, begin + valid), and advances the lookback epoch: the
+// word is bumped on the device, so a sort replayed from a CUDA graph still tags
+// its words with a new epoch. With `keys` (a histogram that came without tile
+// counts, as a frame's projection gives it), every block also counts the valid
+// keys of tiles blockIdx.x, blockIdx.x + gridDim.x, ... into tile_valid.
+__global__ void __launch_bounds__(kSortThreads) k_sort_setup(SortSegments full, const uint32_t* __restrict__ valid_count,
+                                                             uint64_t* begin, uint64_t* end, uint32_t* tiles,
+                                                             uint32_t* epoch, const uint32_t* __restrict__ keys,
+                                                             uint32_t key_mask, uint32_t* __restrict__ tile_valid) {
+  __shared__ uint32_t s_count;
+  pdl_wait();
+  pdl_trigger();
+  const int tid = threadIdx.x;
+  if (tid == 0 && blockIdx.x == 0) {
+    const uint32_t e = *epoch + 1u;
+    *epoch = e == 0u ? 1u : e;  // 0 marks a cleared word
+    uint32_t t = 0;
+    for (int s = 0; s < full.count; s++) {
+      const uint64_t b = full.begin[s];
+      const uint64_t v = min((uint64_t)valid_count[s], full.end[s] - b);
+      begin[s] = b;
+      end[s] = b + v;
+      tiles[s] = t;
+      t += (uint32_t)((v + kSortTile - 1) / kSortTile);
+    }
+    tiles[full.count] = t;
   }
-  tiles[full.count] = t;
+  if (keys == nullptr) return;
+  const uint32_t total_tiles = full.tiles[full.count];
+  for (uint32_t tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+    const int seg = segment_of(full.tiles, full.count, tile);
+    const uint64_t base = full.begin[seg] + (uint64_t)(tile - full.tiles[seg]) * kSortTile;
+    const uint32_t n = (uint32_t)min((uint64_t)kSortTile, full.end[seg] - base);
+    if (tid == 0) s_count = 0;
+    __syncthreads();
+    uint32_t c = 0;
+#pragma unroll
+    for (int j = 0; j < kSortItems; j++) {
+      const uint32_t pos = (uint32_t)j * kSortThreads + tid;
+      c += pos < n && (__ldg(&keys[base + pos]) & key_mask) != key_mask;
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((tid & 31) == 0 && c) atomicAdd(&s_count, c);
+    __syncthreads();
+    if (tid == 0) tile_valid[tile] = s_count;
+  }
+}
+
+// ---- stable partition: the valid keys packed at each segment's front ----
+
+struct PartArgs {
+  const uint32_t* keys_in;
+  const uint32_t* vals_in;  // null: each key's index within its segment
+  uint32_t* keys_front;     // valid keys at begin[s] + their rank among the segment's valid keys
+  uint32_t* vals_front;
+  uint32_t* tail_keys;      // largest keys (final outputs; may be null) at begin[s] + valid[s] + rank
+  uint32_t* tail_vals;
+  uint32_t key_mask;
+  SortSegments segs;
+  const uint32_t* valid_count;
+  const uint32_t* tile_valid;  // [tiles] valid keys of each tile, complete before this kernel
+  uint32_t* counter;
+};
+
+constexpr int kPartBlocksPerSm = 8;
+
+// Each tile's offsets come from the valid counts of the segment's earlier
+// tiles, which the histogram or the set-up kernel wrote: no tile waits for another.
+__global__ void __launch_bounds__(kSortThreads, kPartBlocksPerSm) k_partition(PartArgs a) {
+  __shared__ uint32_t s_warp_valid[kSortWarps];
+  __shared__ uint32_t s_warp_prefix[kSortWarps];
+  __shared__ uint32_t s_tile;
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  pdl_wait();
+  pdl_trigger();
+  if (tid == 0) s_tile = atomicAdd(a.counter, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  if (tile >= a.segs.tiles[a.segs.count]) return;
+  const int seg = segment_of(a.segs.tiles, a.segs.count, tile);
+  const uint32_t first = a.segs.tiles[seg];
+  const uint32_t local_tile = tile - first;
+  const uint64_t seg_begin = a.segs.begin[seg];
+  const uint64_t seg_end = a.segs.end[seg];
+  const uint64_t base = seg_begin + (uint64_t)local_tile * kSortTile;
+  const uint32_t n = (uint32_t)min((uint64_t)kSortTile, seg_end - base);
+  const uint32_t warp_base = (uint32_t)warp * (kSortItems * 32);
+  const uint32_t lt = lanemask_lt();
+
+  // Warp w holds tile positions [w * 512, (w + 1) * 512), item j at j * 32 + lane
+  uint32_t key[kSortItems];
+#pragma unroll
+  for (int j = 0; j < kSortItems; j++) {
+    const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+    key[j] = pos < n ? __ldg(&a.keys_in[base + pos]) & a.key_mask : a.key_mask;
+  }
+  // Valid keys of the segment's earlier tiles (loads in flight with the keys')
+  uint32_t before = 0;
+#pragma unroll 4
+  for (uint32_t t = first + (uint32_t)tid; t < tile; t += kSortThreads) before += __ldg(&a.tile_valid[t]);
+  uint32_t warp_valid = 0;
+#pragma unroll
+  for (int j = 0; j < kSortItems; j++) warp_valid += (uint32_t)__popc(__ballot_sync(0xffffffffu, key[j] != a.key_mask));
+  before = __reduce_add_sync(0xffffffffu, before);
+  if (lane == 0) {
+    s_warp_valid[warp] = warp_valid;
+    s_warp_prefix[warp] = before;
+  }
+  __syncthreads();
+  uint32_t valid_before = 0, warp_before = 0;
+#pragma unroll
+  for (int w = 0; w < kSortWarps; w++) {
+    warp_before += w < warp ? s_warp_valid[w] : 0u;
+    valid_before += s_warp_prefix[w];
+  }
+
+  // Valid keys to the front in order; the largest keys to the tail in order
+  const uint32_t seg_valid = min(a.valid_count[seg], (uint32_t)(seg_end - seg_begin));
+  const uint64_t front = seg_begin + valid_before;
+  const uint64_t tail = seg_begin + seg_valid + ((uint64_t)local_tile * kSortTile - valid_before);
+  uint32_t run = warp_before;
+#pragma unroll
+  for (int j = 0; j < kSortItems; j++) {
+    const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+    const bool valid = key[j] != a.key_mask;
+    const uint32_t vb = __ballot_sync(0xffffffffu, valid);
+    const uint32_t r = run + (uint32_t)__popc(vb & lt);  // valid keys of the tile before this one
+    run += (uint32_t)__popc(vb);
+    if (pos < n) {
+      const uint32_t value = a.vals_in ? __ldg(&a.vals_in[base + pos]) : (uint32_t)(base - seg_begin) + pos;
+      if (valid) {
+        const uint64_t dst = front + r;
+        if (dst < seg_begin + seg_valid) {
+          a.keys_front[dst] = key[j];
+          a.vals_front[dst] = value;
+        }
+      } else {
+        const uint64_t dst = tail + (pos - r);
+        if (dst < seg_end) {
+          a.tail_vals[dst] = value;
+          if (a.tail_keys) a.tail_keys[dst] = key[j];
+        }
+      }
+    }
+  }
 }
 
 // ---- onesweep: one digit place ----
@@ -215,14 +359,10 @@ struct PassArgs {
   const uint32_t* vals_in;   // null in the first pass: each key's index within its segment
   uint32_t* keys_out;        // null: values only
   uint32_t* vals_out;
-  uint32_t* tail_keys;       // first pass: where the largest keys go (final outputs; keys may be null)
-  uint32_t* tail_vals;
-  int drop;                  // route the largest key to the tail (outputs do not alias inputs)
   uint32_t key_mask;
   int shift;
   SortSegments segs;         // full segments (first pass) or the valid keys' segments
-  const uint32_t* hist;      // [S][passes][256] of the valid keys
-  const uint32_t* valid_count;
+  const uint32_t* hist;      // [S][passes][256] of the keys sorted
   int passes;
   int place;
   uint64_t* lookback;        // [max_tiles][256] of this pass
@@ -239,18 +379,17 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   __shared__ uint32_t s_tile_start[kRadix];
   __shared__ uint32_t s_dest[kRadix];
   __shared__ uint64_t s_sums[kSortWarps];
-  __shared__ uint32_t s_tail_warp[kSortWarps];
-  __shared__ uint32_t s_valid_before;
   __shared__ uint32_t s_tile;
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
 
-  if (tid == 0) s_tile = atomicAdd(a.counter, 1u);
 #pragma unroll
   for (int w = 0; w < kSortWarps; w++) s_whist[w][tid] = 0;
-  if (tid == 0) s_valid_before = 0;
+  pdl_wait();     // the previous pass (or the set-up) has completed
+  pdl_trigger();  // the next pass may start placing its blocks
+  if (tid == 0) s_tile = atomicAdd(a.counter, 1u);
   __syncthreads();
   const uint32_t tile = s_tile;
   const uint32_t total_tiles = a.segs.tiles[a.segs.count];
@@ -289,16 +428,12 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
     return gen_vals ? (uint32_t)(base - seg_begin) + pos : s_vals[pos];
   };
 
-  // Rank the valid keys: items in position order, equal digits counted by
-  // their lowest lane. Largest keys (first pass) are ranked among themselves.
+  // Rank the keys: items in position order, equal digits counted by their lowest lane
   const uint32_t lt = lanemask_lt();
-  uint32_t tail_count = 0;
 #pragma unroll
   for (int j = 0; j < kSortItems; j++) {
     const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
-    const bool in = pos < n;
-    const bool tail = FIRST && a.drop && in && key[j] == a.key_mask;
-    const bool ranked = in && !tail;
+    const bool ranked = pos < n;
     const uint32_t d = ranked ? (key[j] >> a.shift) & 0xffu : kNotRanked;
     const uint32_t peers = peers_of(d, ranked);
     const int leader = __ffs(peers) - 1;
@@ -309,14 +444,8 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
     }
     old = __shfl_sync(0xffffffffu, old, leader);
     rank[j] = old + (uint32_t)__popc(peers & lt);
-    if (FIRST) {
-      const uint32_t tb = __ballot_sync(0xffffffffu, tail);
-      if (tail) rank[j] = tail_count + (uint32_t)__popc(tb & lt);
-      tail_count += (uint32_t)__popc(tb);
-    }
     __syncwarp();
   }
-  if (FIRST && lane == 0) s_tail_warp[warp] = tail_count;
   __syncthreads();
 
   // Thread d owns digit d: warp counts -> exclusive over warps, the tile's count
@@ -338,7 +467,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   uint64_t both_total;
   const uint64_t both = block_exclusive_scan(((uint64_t)seg_count << 32) | total, s_sums, &both_total);
   const uint32_t tile_start = (uint32_t)both;
-  const uint32_t tile_valid = (uint32_t)both_total;
+  const uint32_t tile_count = (uint32_t)both_total;
   const uint32_t seg_digit = (uint32_t)(both >> 32);
   s_tile_start[d] = tile_start;
 
@@ -365,37 +494,14 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
     st_relaxed64(my_word, ep | kFlagInclusive | (prefix + total));
   }
   s_dest[d] = (uint32_t)seg_begin + seg_digit + prefix - tile_start;
-  if (FIRST && prefix) atomicAdd(&s_valid_before, prefix);
   asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's value copies have landed
   __syncthreads();                                   // and every thread's
 
-  // First pass: the largest keys to the tail of the segment, in input order
-  if (FIRST) {
-    const uint32_t seg_valid = min(a.valid_count[seg], (uint32_t)(seg_end - seg_begin));
-    const uint32_t tail_before = local_tile * (uint32_t)kSortTile - s_valid_before;
-    uint32_t warp_before = 0;
-#pragma unroll
-    for (int w = 0; w < kSortWarps; w++) warp_before += w < warp ? s_tail_warp[w] : 0u;
-    const uint64_t tail_base = seg_begin + seg_valid + tail_before + warp_before;
-#pragma unroll
-    for (int j = 0; j < kSortItems; j++) {
-      const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
-      if (a.drop && pos < n && key[j] == a.key_mask) {
-        const uint64_t dst = tail_base + rank[j];
-        if (dst < seg_end) {
-          a.tail_vals[dst] = value_at(pos);
-          if (a.tail_keys) a.tail_keys[dst] = key[j];
-        }
-      }
-    }
-  }
-
-  // Local sort of the valid keys in shared memory
+  // Local sort of the tile's keys in shared memory
 #pragma unroll
   for (int j = 0; j < kSortItems; j++) {
     const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
-    const bool ranked = pos < n && !(FIRST && a.drop && key[j] == a.key_mask);
-    if (ranked) {
+    if (pos < n) {
       const uint32_t dj = (key[j] >> a.shift) & 0xffu;
       rank[j] += s_tile_start[dj] + s_whist[warp][dj];
       s_exchange[rank[j]] = key[j];
@@ -410,7 +516,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   for (int k = 0; k < kSortItems; k++) {
     const uint32_t i = (uint32_t)k * kSortThreads + tid;
     dest[k] = 0xffffffffu;
-    if (i < tile_valid) {
+    if (i < tile_count) {
       const uint32_t kk = s_exchange[i];
       const uint32_t dst = s_dest[(kk >> a.shift) & 0xffu] + i;
       if (dst >= (uint32_t)seg_begin && dst < (uint32_t)seg_end) {
@@ -434,9 +540,9 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
 
 }  // namespace
 
-size_t sort_small_state_words(int segments, int passes) {
-  // hist [S][passes][256], valid [S], ref_hidden [S], counters [passes]
-  return (size_t)segments * passes * kRadix + 2 * (size_t)segments + (size_t)passes;
+size_t sort_small_state_words(int segments, int passes, uint32_t max_tiles) {
+  // hist [S][passes][256], valid [S], ref_hidden [S], counters [passes + 1], tile_valid [max_tiles]
+  return (size_t)segments * passes * kRadix + 2 * (size_t)segments + (size_t)passes + 1 + max_tiles;
 }
 
 cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches) {
@@ -447,12 +553,13 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
   const uint32_t ref_top = c.bits == 24 ? 0x1fffu : 0xffffu;
   const SortScratch& sc = c.scratch;
   if (c.segs.max_tiles == 0) return cudaSuccess;
-  // In place (a WgpuRadixSort): the first pass may not write the tail while
+  // In place (a WgpuRadixSort): the partition may not write the tail while
   // other tiles still read there, so the largest key is ranked like any other
   const int drop = c.keys_out != c.keys_in && c.vals_out != c.vals_in && !c.no_drop ? 1 : 0;
   int n_launch = 0;
   if (!c.hist_ready) {
-    cudaError_t err = cudaMemsetAsync(sc.hist, 0, sort_small_state_words(c.segs.count, passes) * 4, stream);
+    cudaError_t err =
+        cudaMemsetAsync(sc.hist, 0, sort_small_state_words(c.segs.count, passes, c.segs.max_tiles) * 4, stream);
     if (err != cudaSuccess) return err;
     const int target_blocks = 148 * 4;
     int tpb = (int)((c.segs.max_tiles + target_blocks - 1) / target_blocks);
@@ -461,53 +568,77 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     switch (passes) {
       case 2:
         k_sort_hist<2><<<hist_blocks, kSortThreads, 0, stream>>>(c.keys_in, mask, ref_shift, ref_top, drop, c.segs, tpb,
-                                                                sc.hist, sc.valid, sc.ref_hidden);
+                                                                sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid);
         break;
       case 3:
         k_sort_hist<3><<<hist_blocks, kSortThreads, 0, stream>>>(c.keys_in, mask, ref_shift, ref_top, drop, c.segs, tpb,
-                                                                sc.hist, sc.valid, sc.ref_hidden);
+                                                                sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid);
         break;
       default:
         k_sort_hist<4><<<hist_blocks, kSortThreads, 0, stream>>>(c.keys_in, mask, ref_shift, ref_top, drop, c.segs, tpb,
-                                                                sc.hist, sc.valid, sc.ref_hidden);
+                                                                sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid);
         break;
     }
     n_launch++;
   }
-  k_compacted_segments<<<1, 1, 0, stream>>>(c.segs, sc.valid, sc.vbegin, sc.vend, sc.vtiles, c.epoch);
+  // The partition's offsets need each tile's valid keys: the histogram kernel
+  // counted them, a frame's projection did not
+  const bool count_tiles = drop && c.hist_ready;
+  const uint32_t setup_blocks = count_tiles ? min(c.segs.max_tiles, (uint32_t)(148 * 8)) : 1u;
+  cudaError_t err = launch_after(k_sort_setup, setup_blocks, kSortThreads, 0, stream, c.segs,
+                                 (const uint32_t*)sc.valid, sc.vbegin, sc.vend, sc.vtiles, c.epoch,
+                                 count_tiles ? c.keys_in : (const uint32_t*)nullptr, mask, sc.tile_valid);
+  if (err != cudaSuccess) return err;
   n_launch++;
   SortSegments vsegs{sc.vbegin, sc.vend, sc.vtiles, c.segs.count, c.segs.max_tiles};
 
   PassArgs a{};
   a.key_mask = mask;
   a.hist = sc.hist;
-  a.valid_count = sc.valid;
   a.passes = passes;
   a.epoch = c.epoch;
   a.error_flag = c.error_flag;
-  a.tail_keys = c.keys_out;
-  a.tail_vals = c.vals_out;
-  a.drop = drop;
   const uint32_t* ki = c.keys_in;
   const uint32_t* vi = c.vals_in;
+  if (drop) {
+    // Valid keys packed into the A buffers, the largest keys to the outputs' tails
+    PartArgs p{};
+    p.keys_in = c.keys_in;
+    p.vals_in = c.vals_in;
+    p.keys_front = sc.keys_a;
+    p.vals_front = sc.vals_a;
+    p.tail_keys = c.keys_out;
+    p.tail_vals = c.vals_out;
+    p.key_mask = mask;
+    p.segs = c.segs;
+    p.valid_count = sc.valid;
+    p.tile_valid = sc.tile_valid;
+    p.counter = sc.counters + passes;
+    err = launch_after(k_partition, c.segs.max_tiles, kSortThreads, 0, stream, p);
+    if (err != cudaSuccess) return err;
+    n_launch++;
+    ki = sc.keys_a;
+    vi = sc.vals_a;
+  }
   for (int place = 0; place < passes; place++) {
     const bool last = place == passes - 1;
+    // Ping-pong: after the partition the passes read A, B, A, ...; without it the first reads the input
+    const bool to_a = drop ? place % 2 == 1 : place % 2 == 0;
     a.keys_in = ki;
     a.vals_in = vi;
-    a.keys_out = last ? c.keys_out : (place % 2 == 0 ? sc.keys_a : sc.keys_b);
-    a.vals_out = last ? c.vals_out : (place % 2 == 0 ? sc.vals_a : sc.vals_b);
+    a.keys_out = last ? c.keys_out : (to_a ? sc.keys_a : sc.keys_b);
+    a.vals_out = last ? c.vals_out : (to_a ? sc.vals_a : sc.vals_b);
     a.shift = 8 * place;
-    a.segs = place == 0 ? c.segs : vsegs;
+    a.segs = place == 0 && !drop ? c.segs : vsegs;
     a.place = place;
     a.lookback = c.lookback + (size_t)place * c.segs.max_tiles * kRadix;
     a.counter = sc.counters + place;
-    if (place == 0) {
-      k_onesweep<true, true><<<c.segs.max_tiles, kSortThreads, 0, stream>>>(a);
-    } else if (last && a.keys_out == nullptr) {
-      k_onesweep<false, false><<<c.segs.max_tiles, kSortThreads, 0, stream>>>(a);
-    } else {
-      k_onesweep<false, true><<<c.segs.max_tiles, kSortThreads, 0, stream>>>(a);
-    }
+    const bool first = place == 0 && !drop;
+    void (*kernel)(PassArgs) = first                             ? k_onesweep<true, true>
+                               : (last && a.keys_out == nullptr) ? k_onesweep<false, false>
+                                                                 : k_onesweep<false, true>;
+    err = launch_after(kernel, c.segs.max_tiles, kSortThreads, 0, stream, a);
+    if (err != cudaSuccess) return err;
     n_launch++;
     ki = a.keys_out;
     vi = a.vals_out;
