@@ -44,6 +44,8 @@ def parse():
     p.add_argument("--n", type=int, default=N_SPLATS)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--bits", type=int, default=32, choices=[16, 24, 32],
+                   help="sort-key width (32 for the headline; 24 is the reference's default)")
     p.add_argument("--workload", default="frame", choices=["frame", "batched", "stereo", "backward", "ply"],
                    help="frame: 4M SH-3 splats, one view (the headline); batched: 16 scenes x 64 views in one "
                         "CUDA graph; stereo: 16M SH-3 fp16 splats, two eyes; backward: the projection's gradient, 1M; "
@@ -196,7 +198,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded mulberry32)",
         "config": {"workload": f"project+SH+key+sort, {n} splats (a bounded sample of the 4M SH-3 workload), "
-                               "1920x1080 fov 50, 32-bit keys", "n": n, "sh_degree": SH_DEGREE, "bits": BITS},
+                               f"1920x1080 fov 50, {BITS}-bit keys", "n": n, "sh_degree": SH_DEGREE, "bits": BITS},
         "cpu_baseline": {"value": value, "unit": "Msplats/s", "cores": threads, "kind": "port",
                          "sample": f"{n} splats per step; float64 projection on {threads} threads, sort on 1"},
         "e2e": {"value": value, "unit": "Msplats/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -285,7 +287,7 @@ def run_batched(args, world, rank, local, device):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (seeded mulberry32 + Box-Muller)",
         "config": {"workload": "batched: 16 scenes (log-uniform 50k-2M splats, SH 3 fp32, Gaussian mixtures), "
-                               "64 views on a sphere of radius 4, 1920x1080 fov 50, 32-bit keys, "
+                               f"64 views on a sphere of radius 4, 1920x1080 fov 50, {BITS}-bit keys, "
                                "one CUDA-graph launch (projection + segmented sort) per step",
                    "scenes": counts, "splat_views": n_views, "bits": BITS, "parallelism": f"replicas{world}",
                    "l2": "inputs 2 GB > 126 MB L2 (no flush)", "frame_bytes_per_splat_view": FRAME_BYTES,
@@ -354,7 +356,7 @@ def run_stereo(args, world, rank, local, device):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16 SH, f32+f64 maths",
         "data": "synthetic (seeded mulberry32 + Box-Muller)",
         "config": {"workload": f"stereo: {n} splats, SH 3 stored fp16, two eyes 2064x2208 fov 100, 64 mm "
-                               "baseline, one key per splat from the head, 32-bit keys",
+                               f"baseline, one key per splat from the head, {BITS}-bit keys",
                    "n": n, "eyes": 2, "bits": BITS, "parallelism": f"replicas{world}",
                    "l2": "inputs 2.2 GB > 126 MB L2 (no flush)", "frame_bytes_per_splat": frame_bytes,
                    "hbm_frac_frame": frame_bytes * n / (ms_step / 1e3) / 1e9 / peak,
@@ -494,7 +496,10 @@ def run_ply(args, world, rank, local, device):
 
 
 def main():
+    global BITS, FRAME_BYTES
     args = parse()
+    BITS = args.bits
+    FRAME_BYTES = 236 + 40 + 8 + 16 * (BITS // 8) + 4
     if args.impl == "reference":
         run_reference(args)
         return
@@ -607,7 +612,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded mulberry32 + Box-Muller)",
         "config": {"workload": "project+SH+key+sort, 4M splats, SH degree 3 fp32, Gaussian-mixture centres, "
-                               "1920x1080 fov 50, 32-bit keys, stable order",
+                               f"1920x1080 fov 50, {BITS}-bit keys, stable order",
                    "n": n, "sh_degree": SH_DEGREE, "bits": BITS, "parallelism": f"replicas{world}",
                    "l2": "inputs 944 MB > 126 MB L2 (no flush)",
                    "frame_bytes_per_splat": FRAME_BYTES,

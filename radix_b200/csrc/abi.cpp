@@ -684,7 +684,7 @@ int check_objects(rdx_ctx* ctx, const rdx_object* objects, int n_objects) {
 // Enqueue one sort (every pass); it takes a fresh lookback epoch on the device
 int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
              const SegBufs& sb, int segments, uint32_t max_tiles, int bits, const rdx::SortScratch& sc,
-             bool hist_ready) {
+             bool zeroed) {
   const int passes = bits / 8;
   int st = ensure_lookback(ctx, (size_t)passes * max_tiles * rdx::kRadix);
   if (st != RDX_OK) return st;
@@ -695,7 +695,7 @@ int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uin
   c.vals_out = vals_out;
   c.segs = rdx::SortSegments{sb.begin, sb.end, sb.tiles, segments, max_tiles};
   c.bits = bits;
-  c.hist_ready = hist_ready;
+  c.zeroed = zeroed;
   c.scratch = sc;
   c.lookback = ctx->lookback;
   c.epoch = ctx->error_flag + 1;
@@ -1136,8 +1136,8 @@ struct FrameDev {
   uint32_t* error_flag = nullptr;  // word 0: the error flag, word 1: the lookback epoch
 };
 
-// Enqueue a planned frame on `stream`: the projection (with the key histogram
-// when sorting), then the segmented sort and the visible counts. It reads and
+// Enqueue a planned frame on `stream`: the projection, then the segmented sort
+// (its small state zeroed before the projection) and the visible counts. It reads and
 // writes no host memory, so the same sequence can be captured in a CUDA graph.
 // `timing` (may be null) gets phase timings.
 cudaError_t enqueue_frame(rdx_ctx* timing, const ProjectCall& call, const FrameDev& fd, int bits, bool sort,
@@ -1146,19 +1146,17 @@ cudaError_t enqueue_frame(rdx_ctx* timing, const ProjectCall& call, const FrameD
   const int passes = bits / 8;
   const bool sorting = sort && call.n > 0;
   cudaError_t e;
-  rdx::ProjHist hist{nullptr, nullptr, 0};
   if (sorting) {
     e = cudaMemsetAsync(fd.sc.hist, 0, rdx::sort_small_state_words(views, passes, segment_tiles(call, nullptr)) * 4,
                         stream);
     if (e != cudaSuccess) return e;
-    hist = rdx::ProjHist{fd.sc.hist, fd.sc.valid, passes};
   }
   {
     Phase projecting(timing, RDX_PHASE_PROJECT);
     for (size_t g = 0; g + 1 < call.groups.size(); g++) {
       const int start = call.groups[g];
       const int count = call.groups[g + 1] - start;
-      e = rdx::launch_project(fd.descs + start, call.descs.data() + start, count, call.group_tiles[g], fd.out, hist,
+      e = rdx::launch_project(fd.descs + start, call.descs.data() + start, count, call.group_tiles[g], fd.out,
                               fd.error_flag, stream);
       if (e != cudaSuccess) return e;
       if (call.group_tiles[g]) *launches += 1;
@@ -1171,7 +1169,7 @@ cudaError_t enqueue_frame(rdx_ctx* timing, const ProjectCall& call, const FrameD
     c.vals_out = fd.ord;
     c.segs = rdx::SortSegments{fd.sb.begin, fd.sb.end, fd.sb.tiles, views, segment_tiles(call, nullptr)};
     c.bits = bits;
-    c.hist_ready = true;  // the projection counted the digits of the valid keys
+    c.zeroed = true;  // zeroed before the projection, so the projection and the sort's kernels run back to back
     c.scratch = fd.sc;
     c.lookback = fd.lookback;
     c.epoch = fd.error_flag + 1;

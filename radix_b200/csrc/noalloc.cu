@@ -143,7 +143,7 @@ extern "C" int rdx_sort_noalloc(const uint32_t* keys, uint64_t count, int bits, 
   const uint32_t max_tiles = (uint32_t)((count + kSortTile - 1) / kSortTile);
   c.segs = SortSegments{begin, end, tiles, 1, max_tiles};
   c.bits = bits;
-  c.hist_ready = false;  // the sort zeroes and counts its histogram itself
+  c.zeroed = false;  // the sort zeroes its small state itself
   c.scratch = sc;
   c.lookback = reinterpret_cast<uint64_t*>(b + kLookbackOff);
   c.epoch = epoch;

@@ -1,7 +1,6 @@
 // Fused per-splat projection for sm_100a: table decode, SH colour from the
 // head (object space), object -> head transform, ewa projection per eye, the
-// reference's words, float outputs, the back-to-front sort key and (for a
-// frame) the histogram of the keys' digits for the sort that follows.
+// reference's words, float outputs and the back-to-front sort key.
 //
 // Restates, fused: SplatProjector.build (src/render/SplatProjector.ts:153-194),
 // SplatGenerator.fromSplats.withSh (src/gpu/splatGenerator.ts:152-158),
@@ -382,23 +381,7 @@ __device__ __forceinline__ void colour(const DevTable& t, uint64_t i, double dx,
   }
 }
 
-// Warp-aggregated shared-memory histogram increment: lanes sharing a digit add once
-__device__ __forceinline__ void hist_add(uint32_t* h, uint32_t d, bool valid) {
-  uint32_t active = __ballot_sync(0xffffffffu, valid);
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int round = 0; round < 2; round++) {
-    if (!active) break;
-    const int leader = __ffs(active) - 1;
-    const uint32_t dl = __shfl_sync(0xffffffffu, d, leader);
-    const uint32_t m = __ballot_sync(0xffffffffu, valid && d == dl) & active;
-    if (lane == leader) atomicAdd(&h[dl], (uint32_t)__popc(m));
-    active &= ~m;
-  }
-  if (active & (1u << lane)) atomicAdd(&h[d], 1u);
-}
-
-// A warp's shared memory: its descriptor, its candidate queue (a ring), its histogram
+// A warp's shared memory: its descriptor and its candidate queue (a ring)
 template <int EYES>
 struct WarpSmem {
   ProjDesc desc;
@@ -407,53 +390,21 @@ struct WarpSmem {
   float c[3][kQueue];      // object-space centre
   uint32_t eye_ok[kQueue]; // eyes whose centre culls passed
   double e[EYES][6][kQueue];  // per eye: centre ex, ey, ez and clip x, y, w (float64)
-  uint32_t hist[kMaxPasses][kRadix];
-  uint32_t valid;
 };
 
-template <int LAYOUT, int DEG, int VAR, int EYES, bool HIST>
+template <int LAYOUT, int DEG, int VAR, int EYES>
 __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict__ descs, int n_desc, uint32_t total_chunks,
-                                                      ProjOutputs out, ProjHist hist) {
+                                                      ProjOutputs out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   WarpSmem<EYES>& W = reinterpret_cast<WarpSmem<EYES>*>(smem_raw)[warp];
   const ProjDesc& sd = W.desc;
   const uint32_t lt = (1u << lane) - 1u;
 
-  if constexpr (HIST) {
-    for (int w = lane; w < kMaxPasses * kRadix; w += 32) (&W.hist[0][0])[w] = 0;
-    if (lane == 0) W.valid = 0;
-  }
-  __syncwarp();
-  pdl_trigger();  // the sort's set-up kernel may be placed now; it waits for this grid to complete
+  pdl_trigger();  // the sort's first kernel may be placed now; it waits for this grid to complete
 
   int cur_desc = -1;
-  int cur_seg = -1;
   uint32_t head = 0, queued = 0;
-
-  auto flush_hist = [&]() {
-    if constexpr (HIST) {
-      __syncwarp();
-      if (cur_seg >= 0) {
-        for (int w = lane; w < hist.passes * kRadix; w += 32) {
-          const uint32_t c = (&W.hist[0][0])[w];
-          if (c) atomicAdd(&hist.hist[(size_t)cur_seg * hist.passes * kRadix + w], c);
-          (&W.hist[0][0])[w] = 0;
-        }
-        if (lane == 0 && W.valid) atomicAdd(&hist.valid[cur_seg], W.valid);
-        if (lane == 0) W.valid = 0;
-      }
-      __syncwarp();
-    }
-  };
-  auto count_key = [&](uint32_t key, bool final_key) {
-    if constexpr (HIST) {
-      const bool valid = final_key && key != invalid_key(sd.sort_bits);
-      for (int pl = 0; pl < hist.passes; pl++) hist_add(W.hist[pl], (key >> (8 * pl)) & 0xffu, valid);
-      const uint32_t nv = (uint32_t)__popc(__ballot_sync(0xffffffffu, valid));
-      if (lane == 0) W.valid += nv;
-    }
-  };
 
   // ---- phase 2: SH, covariance and ewa of nb queued splats (a lane each) ----
   auto process = [&](uint32_t nb) {
@@ -676,7 +627,6 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
         if (out.keys) out.keys[gi] = key_out;
       }
     }
-    if (sd.cull_keys) count_key(key_out, busy);
     head = (head + nb) & (kQueue - 1);
     queued -= nb;
     __syncwarp();
@@ -717,11 +667,6 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
     }
     if (!have_chunk) break;
     if (di != cur_desc) {
-      const int seg = descs[di].segment;
-      if (seg != cur_seg) {
-        flush_hist();
-        cur_seg = seg;
-      }
       const uint32_t* src = reinterpret_cast<const uint32_t*>(&descs[di]);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&W.desc);
       for (int w = lane; w < (int)(sizeof(ProjDesc) / 4); w += 32) dst[w] = src[w];
@@ -867,7 +812,6 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
     // keys known now: every key without cullKeys, culled splats' with it
     const bool key_final = live && (!cull_keys || !candidate);
     if (key_final && out.keys) out.keys[gi] = key;
-    count_key(key, key_final);
     // enqueue the candidates, in row order
     const uint32_t ballot = __ballot_sync(0xffffffffu, candidate);
     if (candidate) {
@@ -889,65 +833,63 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
     chunk += nw;
     di = -1;
   }
-  flush_hist();
 }
 
-using ProjKernel = void (*)(const ProjDesc*, int, uint32_t, ProjOutputs, ProjHist);
+using ProjKernel = void (*)(const ProjDesc*, int, uint32_t, ProjOutputs);
 
 struct Picked {
   ProjKernel fn;
   int smem;
 };
 
-template <int LAYOUT, int DEG, int VAR, int EYES, bool HIST>
+template <int LAYOUT, int DEG, int VAR, int EYES>
 Picked picked() {
-  return {k_project<LAYOUT, DEG, VAR, EYES, HIST>, (int)(kWarps * sizeof(WarpSmem<EYES>))};
+  return {k_project<LAYOUT, DEG, VAR, EYES>, (int)(kWarps * sizeof(WarpSmem<EYES>))};
 }
 
 template <int LAYOUT, int DEG, int VAR>
-Picked pick_eyes(int eyes, bool hist) {
-  if (eyes == 2) return hist ? picked<LAYOUT, DEG, VAR, 2, true>() : picked<LAYOUT, DEG, VAR, 2, false>();
-  return hist ? picked<LAYOUT, DEG, VAR, 1, true>() : picked<LAYOUT, DEG, VAR, 1, false>();
+Picked pick_eyes(int eyes) {
+  return eyes == 2 ? picked<LAYOUT, DEG, VAR, 2>() : picked<LAYOUT, DEG, VAR, 1>();
 }
 
 template <int LAYOUT, int VAR>
-Picked pick_degree(int degree, int eyes, bool hist) {
+Picked pick_degree(int degree, int eyes) {
   switch (degree) {
-    case 0: return pick_eyes<LAYOUT, 0, VAR>(eyes, hist);
-    case 1: return pick_eyes<LAYOUT, 1, VAR>(eyes, hist);
-    case 2: return pick_eyes<LAYOUT, 2, VAR>(eyes, hist);
-    case 3: return pick_eyes<LAYOUT, 3, VAR>(eyes, hist);
-    default: return pick_eyes<LAYOUT, 4, VAR>(eyes, hist);
+    case 0: return pick_eyes<LAYOUT, 0, VAR>(eyes);
+    case 1: return pick_eyes<LAYOUT, 1, VAR>(eyes);
+    case 2: return pick_eyes<LAYOUT, 2, VAR>(eyes);
+    case 3: return pick_eyes<LAYOUT, 3, VAR>(eyes);
+    default: return pick_eyes<LAYOUT, 4, VAR>(eyes);
   }
 }
 
 template <int LAYOUT>
-Picked pick_codec(int degree, int codec, int eyes, bool hist) {
+Picked pick_codec(int degree, int codec, int eyes) {
   // without SH the codec is immaterial: one kernel
-  if (codec == RDX_SH_PACKED && degree > 0) return pick_degree<LAYOUT, RDX_SH_PACKED>(degree, eyes, hist);
-  return pick_degree<LAYOUT, RDX_SH_EXT>(degree, eyes, hist);
+  if (codec == RDX_SH_PACKED && degree > 0) return pick_degree<LAYOUT, RDX_SH_PACKED>(degree, eyes);
+  return pick_degree<LAYOUT, RDX_SH_EXT>(degree, eyes);
 }
 
-Picked pick_kernel(const DevTable& t, int eyes, bool hist) {
+Picked pick_kernel(const DevTable& t, int eyes) {
   switch (t.layout) {
-    case RDX_LAYOUT_EXT: return pick_codec<RDX_LAYOUT_EXT>(t.sh_degree, t.sh_codec, eyes, hist);
-    case RDX_LAYOUT_PACKED: return pick_codec<RDX_LAYOUT_PACKED>(t.sh_degree, t.sh_codec, eyes, hist);
-    case RDX_LAYOUT_COV: return pick_codec<RDX_LAYOUT_COV>(t.sh_degree, t.sh_codec, eyes, hist);
+    case RDX_LAYOUT_EXT: return pick_codec<RDX_LAYOUT_EXT>(t.sh_degree, t.sh_codec, eyes);
+    case RDX_LAYOUT_PACKED: return pick_codec<RDX_LAYOUT_PACKED>(t.sh_degree, t.sh_codec, eyes);
+    case RDX_LAYOUT_COV: return pick_codec<RDX_LAYOUT_COV>(t.sh_degree, t.sh_codec, eyes);
     default:
-      if (t.color_dtype == RDX_DTYPE_F16) return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F16>(t.sh_degree, eyes, hist);
-      return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F32>(t.sh_degree, eyes, hist);
+      if (t.color_dtype == RDX_DTYPE_F16) return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F16>(t.sh_degree, eyes);
+      return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F32>(t.sh_degree, eyes);
   }
 }
 
 }  // namespace
 
 cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host, int n_desc, uint32_t total_chunks,
-                           const ProjOutputs& out, const ProjHist& hist, uint32_t* error_flag, cudaStream_t stream) {
+                           const ProjOutputs& out, uint32_t* error_flag, cudaStream_t stream) {
   (void)error_flag;  // no device wait in this kernel
   if (total_chunks == 0 || n_desc == 0) return cudaSuccess;
   // One kernel per launch: the caller groups objects by table kind
   const ProjDesc& d0 = descs_host[0];
-  const Picked k = pick_kernel(d0.table, d0.eyes, hist.hist != nullptr);
+  const Picked k = pick_kernel(d0.table, d0.eyes);
   cudaError_t err = cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem);
   if (err != cudaSuccess) return err;
   int device = 0, sms = 0, per_sm = 0;
@@ -958,7 +900,7 @@ cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host
   if (per_sm < 1) per_sm = 1;
   const uint32_t want = (total_chunks + kWarps - 1) / kWarps;
   const uint32_t grid = min(want, (uint32_t)(sms * per_sm));
-  k.fn<<<grid, kThreads, k.smem, stream>>>(descs_dev, n_desc, total_chunks, out, hist);
+  k.fn<<<grid, kThreads, k.smem, stream>>>(descs_dev, n_desc, total_chunks, out);
   return cudaGetLastError();
 }
 

@@ -85,9 +85,9 @@ size_t sort_small_state_words(int segments, int passes, uint32_t max_tiles);
 // Sort segments of keys_in (values: vals_in, or each key's index within its
 // segment when vals_in is null) into keys_out / vals_out (keys_out may be null:
 // values only), stable and ascending by the low `bits` bits; the largest key
-// 2^bits - 1 goes to each segment's tail in input order. hist_ready: the
-// small state already holds the histogram and valid counts (a frame's
-// projection wrote them); else it is zeroed and counted here. The lookback
+// 2^bits - 1 goes to each segment's tail in input order. zeroed: the caller
+// has zeroed the small state (sort_small_state_words from scratch.hist), so
+// the sort starts with a kernel; else it zeroes it first. The lookback
 // words [passes][max_tiles][256] are tagged with the epoch in the device word
 // `epoch`, which the sort advances on the device before its first pass (zero
 // it with the lookback words; it needs no host update between calls).
@@ -98,7 +98,7 @@ struct SortCall {
   uint32_t* vals_out;
   SortSegments segs;
   int bits;
-  bool hist_ready;  // (then the largest keys must be left out of it: outputs may not alias inputs)
+  bool zeroed;      // the small state is zeroed already
   bool no_drop;     // rank the largest key like the others
   SortScratch scratch;
   uint64_t* lookback;
@@ -201,13 +201,6 @@ struct ProjOutputs {
 // Splats per projection chunk (one warp)
 constexpr int kProjTile = 32;
 
-// Where a frame's projection accumulates the digit histogram of its valid keys
-// (hist [segments][passes][256]) and their count per segment; hist == null: none
-struct ProjHist {
-  uint32_t* hist;
-  uint32_t* valid;
-  int passes;
-};
 
 // One persistent launch over every descriptor of one table kind (descs in device memory)
 // ---- PLY files (src/core/ply.ts) to raw tables ----
@@ -279,7 +272,7 @@ cudaError_t launch_project_backward(const ProjDesc* descs_dev, const GradsOut* g
                                     int n_desc, uint32_t total_chunks, const GradsIn& in, cudaStream_t stream);
 
 cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host, int n_desc,
-                           uint32_t total_tiles, const ProjOutputs& out, const ProjHist& hist,
+                           uint32_t total_tiles, const ProjOutputs& out,
                            uint32_t* error_flag, cudaStream_t stream);
 
 }  // namespace rdx

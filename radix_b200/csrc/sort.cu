@@ -9,8 +9,8 @@
 //
 // The largest key of a width (2^bits - 1, the invalid key of SortKeys) sorts
 // after every other key, its copies in input order. When outputs do not alias
-// inputs, a stable partition kernel (offsets from per-tile valid counts
-// counted before it, no digit ranking) first writes them straight to the tail
+// inputs, a stable partition kernel (offsets from per-tile valid counts that
+// the counting kernel wrote, no digit ranking) first writes them straight to the tail
 // of each segment's output and packs the other keys, in order, at the
 // segment's front; every digit pass then sorts only those: a frame's culled
 // splats are read twice and written once, never ranked.
@@ -34,6 +34,7 @@ constexpr uint64_t kFlagMask = 3ull << 30;
 constexpr uint64_t kCountMask = (1ull << 30) - 1ull;
 constexpr uint32_t kNotRanked = 0xffffu;  // the digit of an item outside the ranking
 constexpr int kSortBlocksPerSm = 4;       // onesweep blocks resident per SM (register budget)
+constexpr int kCountBlocksPerSm = 6;      // counting blocks resident per SM
 
 __device__ __forceinline__ uint64_t ld_relaxed64(const uint64_t* p) {
   uint64_t v;
@@ -107,8 +108,12 @@ __device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* s
   return before + x - v;
 }
 
-// Warp-aggregated shared-memory histogram increment
-__device__ __forceinline__ void hist_add(uint32_t* h, uint32_t d, bool valid) {
+// ---- counting: every digit place's histogram, valid keys per tile and segment ----
+
+// Per-warp histogram increment, two 16-bit bins a word (a warp adds at most
+// 512 keys, so a bin cannot carry into its neighbour): lanes sharing a digit
+// add once
+__device__ __forceinline__ void hist_add16(uint32_t* h, uint32_t d, bool valid) {
   uint32_t active = __ballot_sync(0xffffffffu, valid);
   const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -117,137 +122,87 @@ __device__ __forceinline__ void hist_add(uint32_t* h, uint32_t d, bool valid) {
     const int leader = __ffs(active) - 1;
     const uint32_t dl = __shfl_sync(0xffffffffu, d, leader);
     const uint32_t m = __ballot_sync(0xffffffffu, valid && d == dl) & active;
-    if (lane == leader) atomicAdd(&h[dl], (uint32_t)__popc(m));
+    if (lane == leader) atomicAdd(&h[dl >> 1], (uint32_t)__popc(m) << ((dl & 1u) * 16));
     active &= ~m;
   }
-  if (active & (1u << lane)) atomicAdd(&h[d], 1u);
+  if (active & (1u << lane)) atomicAdd(&h[d >> 1], 1u << ((d & 1u) * 16));
 }
 
-// ---- histogram of every digit place (valid keys), the reference's hidden count ----
-
+// One block per tile: the tile's keys in one read give every digit place's
+// histogram of the valid keys (per-warp shared-memory histograms, summed into
+// the segment's by one global atomic per non-zero bin), the tile's valid count
+// (the partition's offsets), the segment's valid count and the reference's
+// hidden count. Block 0 also advances the lookback epoch: the word is bumped
+// on the device, so a sort replayed from a CUDA graph still tags its words
+// with a new epoch.
 template <int PASSES>
-__global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint32_t* __restrict__ keys, uint32_t key_mask,
-                                                            int ref_shift, uint32_t ref_top, int drop,
-                                                            SortSegments segs, int tiles_per_block,
-                                                            uint32_t* __restrict__ hist,
-                                                            uint32_t* __restrict__ valid_count,
-                                                            uint32_t* __restrict__ ref_hidden,
-                                                            uint32_t* __restrict__ tile_valid) {
-  __shared__ uint32_t sh[PASSES][kRadix];
-  __shared__ uint32_t s_hidden, s_valid, s_tile_valid;
+__global__ void __launch_bounds__(kSortThreads, kCountBlocksPerSm)
+    k_sort_count(const uint32_t* __restrict__ keys, uint32_t key_mask, int ref_shift, uint32_t ref_top, int drop,
+                 SortSegments segs, uint32_t* __restrict__ hist, uint32_t* __restrict__ valid_count,
+                 uint32_t* __restrict__ ref_hidden, uint32_t* __restrict__ tile_valid, uint32_t* epoch) {
+  __shared__ uint32_t sh[kSortWarps][PASSES][kRadix / 2];
+  __shared__ uint32_t s_valid[kSortWarps], s_hidden[kSortWarps];
   const int tid = threadIdx.x;
   const int lane = tid & 31;
-  const uint32_t total_tiles = segs.tiles[segs.count];
-  const uint32_t tile0 = blockIdx.x * (uint32_t)tiles_per_block;
-  if (tile0 >= total_tiles) return;
-  const uint32_t tile_end = min(tile0 + (uint32_t)tiles_per_block, total_tiles);
+  const int warp = tid >> 5;
 #pragma unroll
-  for (int p = 0; p < PASSES; p++) sh[p][tid] = 0;
-  if (tid == 0) s_hidden = s_valid = s_tile_valid = 0;
-  __syncthreads();
-
-  int seg = segment_of(segs.tiles, segs.count, tile0);
-  uint32_t hidden = 0, nvalid = 0;
-  auto flush = [&](int s) {
-    __syncthreads();
-#pragma unroll
-    for (int p = 0; p < PASSES; p++) {
-      const uint32_t c = sh[p][tid];
-      if (c) atomicAdd(&hist[((size_t)s * PASSES + p) * kRadix + tid], c);
-      sh[p][tid] = 0;
-    }
-    const uint32_t h = __reduce_add_sync(0xffffffffu, hidden);
-    const uint32_t v = __reduce_add_sync(0xffffffffu, nvalid);
-    if (lane == 0 && h) atomicAdd(&s_hidden, h);
-    if (lane == 0 && v) atomicAdd(&s_valid, v);
-    hidden = nvalid = 0;
-    __syncthreads();
-    if (tid == 0) {
-      if (s_hidden) atomicAdd(&ref_hidden[s], s_hidden);
-      if (s_valid) atomicAdd(&valid_count[s], s_valid);
-      s_hidden = s_valid = 0;
-    }
-    __syncthreads();
-  };
-
-  for (uint32_t tile = tile0; tile < tile_end; tile++) {
-    while (tile >= segs.tiles[seg + 1]) {
-      flush(seg);
-      seg++;
-    }
-    const uint64_t base = segs.begin[seg] + (uint64_t)(tile - segs.tiles[seg]) * kSortTile;
-    const uint32_t n = (uint32_t)min((uint64_t)kSortTile, segs.end[seg] - base);
-    uint32_t in_tile = 0;
-#pragma unroll 4
-    for (int j = 0; j < kSortItems; j++) {
-      const uint32_t pos = (uint32_t)j * kSortThreads + tid;
-      const bool in = pos < n;
-      const uint32_t k = in ? __ldg(&keys[base + pos]) & key_mask : key_mask;
-      hidden += in && (k >> ref_shift) == ref_top;
-      const bool valid = in && (!drop || k != key_mask);
-      in_tile += valid;
-#pragma unroll
-      for (int p = 0; p < PASSES; p++) hist_add(sh[p], (k >> (8 * p)) & 0xffu, valid);
-    }
-    nvalid += in_tile;
-    // the tile's valid keys, for the partition's offsets
-    const uint32_t w = __reduce_add_sync(0xffffffffu, in_tile);
-    if (lane == 0 && w) atomicAdd(&s_tile_valid, w);
-    __syncthreads();
-    if (tid == 0) {
-      tile_valid[tile] = s_tile_valid;
-      s_tile_valid = 0;
-    }
-  }
-  flush(seg);
-}
-
-// Set-up of the digit passes. Block 0's first thread writes the segments of
-// the valid keys, [begin, begin + valid), and advances the lookback epoch: the
-// word is bumped on the device, so a sort replayed from a CUDA graph still tags
-// its words with a new epoch. With `keys` (a histogram that came without tile
-// counts, as a frame's projection gives it), every block also counts the valid
-// keys of tiles blockIdx.x, blockIdx.x + gridDim.x, ... into tile_valid.
-__global__ void __launch_bounds__(kSortThreads) k_sort_setup(SortSegments full, const uint32_t* __restrict__ valid_count,
-                                                             uint64_t* begin, uint64_t* end, uint32_t* tiles,
-                                                             uint32_t* epoch, const uint32_t* __restrict__ keys,
-                                                             uint32_t key_mask, uint32_t* __restrict__ tile_valid) {
-  __shared__ uint32_t s_count;
+  for (int w = lane; w < PASSES * kRadix / 2; w += 32) (&sh[warp][0][0])[w] = 0;
   pdl_wait();
   pdl_trigger();
-  const int tid = threadIdx.x;
   if (tid == 0 && blockIdx.x == 0) {
     const uint32_t e = *epoch + 1u;
     *epoch = e == 0u ? 1u : e;  // 0 marks a cleared word
-    uint32_t t = 0;
-    for (int s = 0; s < full.count; s++) {
-      const uint64_t b = full.begin[s];
-      const uint64_t v = min((uint64_t)valid_count[s], full.end[s] - b);
-      begin[s] = b;
-      end[s] = b + v;
-      tiles[s] = t;
-      t += (uint32_t)((v + kSortTile - 1) / kSortTile);
-    }
-    tiles[full.count] = t;
   }
-  if (keys == nullptr) return;
-  const uint32_t total_tiles = full.tiles[full.count];
-  for (uint32_t tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
-    const int seg = segment_of(full.tiles, full.count, tile);
-    const uint64_t base = full.begin[seg] + (uint64_t)(tile - full.tiles[seg]) * kSortTile;
-    const uint32_t n = (uint32_t)min((uint64_t)kSortTile, full.end[seg] - base);
-    if (tid == 0) s_count = 0;
-    __syncthreads();
+  const uint32_t tile = blockIdx.x;
+  if (tile >= segs.tiles[segs.count]) return;  // grid sized for the capacity
+  const int seg = segment_of(segs.tiles, segs.count, tile);
+  const uint64_t base = segs.begin[seg] + (uint64_t)(tile - segs.tiles[seg]) * kSortTile;
+  const uint32_t n = (uint32_t)min((uint64_t)kSortTile, segs.end[seg] - base);
+  const uint32_t warp_base = (uint32_t)warp * (kSortItems * 32);
+  uint32_t key[kSortItems];
+#pragma unroll
+  for (int j = 0; j < kSortItems; j++) {
+    const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+    key[j] = pos < n ? __ldg(&keys[base + pos]) & key_mask : key_mask;
+  }
+  __syncwarp();
+  uint32_t nvalid = 0, hidden = 0;
+#pragma unroll
+  for (int j = 0; j < kSortItems; j++) {
+    const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+    const bool in = pos < n;
+    hidden += in && (key[j] >> ref_shift) == ref_top;
+    const bool valid = in && (!drop || key[j] != key_mask);
+    nvalid += valid;
+#pragma unroll
+    for (int p = 0; p < PASSES; p++) hist_add16(sh[warp][p], (key[j] >> (8 * p)) & 0xffu, valid);
+  }
+  nvalid = __reduce_add_sync(0xffffffffu, nvalid);
+  hidden = __reduce_add_sync(0xffffffffu, hidden);
+  if (lane == 0) {
+    s_valid[warp] = nvalid;
+    s_hidden[warp] = hidden;
+  }
+  __syncthreads();
+  // thread d sums bin d of every place over the warps
+  const uint32_t d = (uint32_t)tid;
+#pragma unroll
+  for (int p = 0; p < PASSES; p++) {
     uint32_t c = 0;
 #pragma unroll
-    for (int j = 0; j < kSortItems; j++) {
-      const uint32_t pos = (uint32_t)j * kSortThreads + tid;
-      c += pos < n && (__ldg(&keys[base + pos]) & key_mask) != key_mask;
+    for (int w = 0; w < kSortWarps; w++) c += (sh[w][p][d >> 1] >> ((d & 1u) * 16)) & 0xffffu;
+    if (c) atomicAdd(&hist[((size_t)seg * PASSES + p) * kRadix + d], c);
+  }
+  if (tid == 0) {
+    uint32_t v = 0, h = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; w++) {
+      v += s_valid[w];
+      h += s_hidden[w];
     }
-    c = __reduce_add_sync(0xffffffffu, c);
-    if ((tid & 31) == 0 && c) atomicAdd(&s_count, c);
-    __syncthreads();
-    if (tid == 0) tile_valid[tile] = s_count;
+    tile_valid[tile] = v;
+    if (v) atomicAdd(&valid_count[seg], v);
+    if (h) atomicAdd(&ref_hidden[seg], h);
   }
 }
 
@@ -265,12 +220,15 @@ struct PartArgs {
   const uint32_t* valid_count;
   const uint32_t* tile_valid;  // [tiles] valid keys of each tile, complete before this kernel
   uint32_t* counter;
+  uint64_t* vbegin;            // out (block 0): the valid keys' segments for the digit passes
+  uint64_t* vend;
+  uint32_t* vtiles;
 };
 
 constexpr int kPartBlocksPerSm = 8;
 
 // Each tile's offsets come from the valid counts of the segment's earlier
-// tiles, which the histogram or the set-up kernel wrote: no tile waits for another.
+// tiles, which the counting kernel wrote: no tile waits for another.
 __global__ void __launch_bounds__(kSortThreads, kPartBlocksPerSm) k_partition(PartArgs a) {
   __shared__ uint32_t s_warp_valid[kSortWarps];
   __shared__ uint32_t s_warp_prefix[kSortWarps];
@@ -280,6 +238,19 @@ __global__ void __launch_bounds__(kSortThreads, kPartBlocksPerSm) k_partition(Pa
   const int warp = tid >> 5;
   pdl_wait();
   pdl_trigger();
+  if (tid == 0 && blockIdx.x == 0) {
+    // The valid keys' segments [begin, begin + valid) and their tiles
+    uint32_t t = 0;
+    for (int s = 0; s < a.segs.count; s++) {
+      const uint64_t b = a.segs.begin[s];
+      const uint64_t v = min((uint64_t)a.valid_count[s], a.segs.end[s] - b);
+      a.vbegin[s] = b;
+      a.vend[s] = b + v;
+      a.vtiles[s] = t;
+      t += (uint32_t)((v + kSortTile - 1) / kSortTile);
+    }
+    a.vtiles[a.segs.count] = t;
+  }
   if (tid == 0) s_tile = atomicAdd(a.counter, 1u);
   __syncthreads();
   const uint32_t tile = s_tile;
@@ -557,40 +528,29 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
   // other tiles still read there, so the largest key is ranked like any other
   const int drop = c.keys_out != c.keys_in && c.vals_out != c.vals_in && !c.no_drop ? 1 : 0;
   int n_launch = 0;
-  if (!c.hist_ready) {
-    cudaError_t err =
-        cudaMemsetAsync(sc.hist, 0, sort_small_state_words(c.segs.count, passes, c.segs.max_tiles) * 4, stream);
+  cudaError_t err;
+  if (!c.zeroed) {
+    err = cudaMemsetAsync(sc.hist, 0, sort_small_state_words(c.segs.count, passes, c.segs.max_tiles) * 4, stream);
     if (err != cudaSuccess) return err;
-    const int target_blocks = 148 * 4;
-    int tpb = (int)((c.segs.max_tiles + target_blocks - 1) / target_blocks);
-    if (tpb < 1) tpb = 1;
-    const int hist_blocks = (int)((c.segs.max_tiles + tpb - 1) / tpb);
-    switch (passes) {
-      case 2:
-        k_sort_hist<2><<<hist_blocks, kSortThreads, 0, stream>>>(c.keys_in, mask, ref_shift, ref_top, drop, c.segs, tpb,
-                                                                sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid);
-        break;
-      case 3:
-        k_sort_hist<3><<<hist_blocks, kSortThreads, 0, stream>>>(c.keys_in, mask, ref_shift, ref_top, drop, c.segs, tpb,
-                                                                sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid);
-        break;
-      default:
-        k_sort_hist<4><<<hist_blocks, kSortThreads, 0, stream>>>(c.keys_in, mask, ref_shift, ref_top, drop, c.segs, tpb,
-                                                                sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid);
-        break;
-    }
-    n_launch++;
   }
-  // The partition's offsets need each tile's valid keys: the histogram kernel
-  // counted them, a frame's projection did not
-  const bool count_tiles = drop && c.hist_ready;
-  const uint32_t setup_blocks = count_tiles ? min(c.segs.max_tiles, (uint32_t)(148 * 8)) : 1u;
-  cudaError_t err = launch_after(k_sort_setup, setup_blocks, kSortThreads, 0, stream, c.segs,
-                                 (const uint32_t*)sc.valid, sc.vbegin, sc.vend, sc.vtiles, c.epoch,
-                                 count_tiles ? c.keys_in : (const uint32_t*)nullptr, mask, sc.tile_valid);
+  switch (passes) {
+    case 2:
+      err = launch_after(k_sort_count<2>, c.segs.max_tiles, kSortThreads, 0, stream, c.keys_in, mask, ref_shift, ref_top,
+                         drop, c.segs, sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid, c.epoch);
+      break;
+    case 3:
+      err = launch_after(k_sort_count<3>, c.segs.max_tiles, kSortThreads, 0, stream, c.keys_in, mask, ref_shift, ref_top,
+                         drop, c.segs, sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid, c.epoch);
+      break;
+    default:
+      err = launch_after(k_sort_count<4>, c.segs.max_tiles, kSortThreads, 0, stream, c.keys_in, mask, ref_shift, ref_top,
+                         drop, c.segs, sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid, c.epoch);
+      break;
+  }
   if (err != cudaSuccess) return err;
   n_launch++;
-  SortSegments vsegs{sc.vbegin, sc.vend, sc.vtiles, c.segs.count, c.segs.max_tiles};
+  // Without the partition every key is valid: the digit passes use the segments as given
+  SortSegments vsegs = drop ? SortSegments{sc.vbegin, sc.vend, sc.vtiles, c.segs.count, c.segs.max_tiles} : c.segs;
 
   PassArgs a{};
   a.key_mask = mask;
@@ -614,6 +574,9 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     p.valid_count = sc.valid;
     p.tile_valid = sc.tile_valid;
     p.counter = sc.counters + passes;
+    p.vbegin = sc.vbegin;
+    p.vend = sc.vend;
+    p.vtiles = sc.vtiles;
     err = launch_after(k_partition, c.segs.max_tiles, kSortThreads, 0, stream, p);
     if (err != cudaSuccess) return err;
     n_launch++;
@@ -629,7 +592,7 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     a.keys_out = last ? c.keys_out : (to_a ? sc.keys_a : sc.keys_b);
     a.vals_out = last ? c.vals_out : (to_a ? sc.vals_a : sc.vals_b);
     a.shift = 8 * place;
-    a.segs = place == 0 && !drop ? c.segs : vsegs;
+    a.segs = vsegs;
     a.place = place;
     a.lookback = c.lookback + (size_t)place * c.segs.max_tiles * kRadix;
     a.counter = sc.counters + place;
