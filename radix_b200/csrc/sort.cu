@@ -34,7 +34,7 @@ constexpr uint64_t kFlagMask = 3ull << 30;
 constexpr uint64_t kCountMask = (1ull << 30) - 1ull;
 constexpr uint32_t kNotRanked = 0xffffu;  // the digit of an item outside the ranking
 constexpr int kSortBlocksPerSm = 4;       // onesweep blocks resident per SM (register budget)
-constexpr int kCountBlocksPerSm = 6;      // counting blocks resident per SM
+constexpr int kCountBlocksPerSm = 8;      // counting blocks resident per SM (one wave at 4M keys)
 
 __device__ __forceinline__ uint64_t ld_relaxed64(const uint64_t* p) {
   uint64_t v;
@@ -111,21 +111,22 @@ __device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* s
 // ---- counting: every digit place's histogram, valid keys per tile and segment ----
 
 // Per-warp histogram increment, two 16-bit bins a word (a warp adds at most
-// 512 keys, so a bin cannot carry into its neighbour): lanes sharing a digit
-// add once
+// 512 keys, so a bin cannot carry into its neighbour). When every valid lane
+// has the same digit (the high places of depth keys: few exponents) one lane
+// adds them all; otherwise each lane adds its own (the hardware serialises
+// the few lanes that share a bin).
 __device__ __forceinline__ void hist_add16(uint32_t* h, uint32_t d, bool valid) {
-  uint32_t active = __ballot_sync(0xffffffffu, valid);
+  const uint32_t active = __ballot_sync(0xffffffffu, valid);
+  if (!active) return;
   const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int round = 0; round < 2; round++) {
-    if (!active) break;
-    const int leader = __ffs(active) - 1;
-    const uint32_t dl = __shfl_sync(0xffffffffu, d, leader);
-    const uint32_t m = __ballot_sync(0xffffffffu, valid && d == dl) & active;
-    if (lane == leader) atomicAdd(&h[dl >> 1], (uint32_t)__popc(m) << ((dl & 1u) * 16));
-    active &= ~m;
+  const int first = __ffs(active) - 1;
+  const uint32_t d0 = __shfl_sync(0xffffffffu, d, first);
+  const uint32_t same = __ballot_sync(0xffffffffu, valid && d == d0);
+  if (same == active) {
+    if (lane == first) atomicAdd(&h[d0 >> 1], (uint32_t)__popc(active) << ((d0 & 1u) * 16));
+  } else if (valid) {
+    atomicAdd(&h[d >> 1], 1u << ((d & 1u) * 16));
   }
-  if (active & (1u << lane)) atomicAdd(&h[d >> 1], 1u << ((d & 1u) * 16));
 }
 
 // One block per tile: the tile's keys in one read give every digit place's
