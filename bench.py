@@ -46,10 +46,10 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--bits", type=int, default=32, choices=[16, 24, 32],
                    help="sort-key width (32 for the headline; 24 is the reference's default)")
-    p.add_argument("--workload", default="frame", choices=["frame", "batched", "stereo", "backward", "ply"],
+    p.add_argument("--workload", default="frame", choices=["frame", "batched", "stereo", "backward", "ply", "spz"],
                    help="frame: 4M SH-3 splats, one view (the headline); batched: 16 scenes x 64 views in one "
                         "CUDA graph; stereo: 16M SH-3 fp16 splats, two eyes; backward: the projection's gradient, 1M; "
-                        "ply: decoding a 1M-splat PLY file")
+                        "ply: decoding a 1M-splat PLY file; spz: decoding a 1M-splat SPZ file from host bytes")
     return p.parse_args()
 
 
@@ -495,6 +495,64 @@ def run_ply(args, world, rank, local, device):
     }
 
 
+def run_spz(args, world, rank, local, device):
+    """A 1M-splat SH-3 SPZ file (version 3, gzip) in host memory decoded into a
+    raw table on the GPU each step: the host inflates the container, the device
+    decodes the byte columns. The device decode is timed alone beside it."""
+    import torch
+
+    import radix_b200 as rb
+    from radix_b200 import synthetic as syn
+    from tests import spz_fixtures as sf
+    n = 1_000_000 if args.n == N_SPLATS else args.n
+    d = syn.mixture_table(n, seed=0, sh_degree=SH_DEGREE)
+    raw = sf.gzip_spz(d, version=3)
+    del d
+    ctx = rb.Context(local)
+    rb.decode_spz(raw, ctx=ctx)
+    k = (SH_DEGREE + 1) ** 2 - 1
+    payload = n * (9 + 1 + 3 + 3 + 4 + 3 * k)
+
+    def step():
+        rb.decode_spz(raw, ctx=ctx)
+
+    marks = {}
+
+    def start_counting():
+        marks["launches"] = ctx.launches()
+
+    ms_total, clock_info = timed(step, args.steps, args.warmup, world, local, start_counting)
+    launches = ctx.launches() - marks["launches"]
+    ms_step = ms_total / args.steps
+    # the device decode alone: phase events around its launch, outside the timed region
+    ctx.set_profiling(True)
+    ctx.phase_times()
+    for _ in range(5):
+        rb.decode_spz(raw, ctx=ctx)
+    torch.cuda.synchronize()
+    kt, kr = ctx.phase_times()["project"]
+    ctx.set_profiling(False)
+    kernel_ms = kt / max(kr, 1)
+    peak, peak_kind = peak_hbm()
+    bytes_per = payload // n + 12 + 12 + 16 + 4 + (k + 1) * 3 * 4
+    achieved = bytes_per * n / (kernel_ms / 1e3) / 1e9
+    value = world * n * args.steps / (ms_total / 1e3) / 1e6
+    return {
+        "metric": "Msplats/s (SPZ decode, host bytes to a device table)", "value": value,
+        "unit": "Msplats/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 in, f64 maths, f32 out",
+        "data": "synthetic (an SPZ file written from the seeded SH-3 mixture)",
+        "config": {"workload": f"SPZ decode: {n} splats, version 3 in gzip ({len(raw)} B file, {payload} B of columns), "
+                               "SH 3, host bytes to a raw float32 table on the GPU", "n": n,
+                   "parallelism": f"replicas{world}", "file_bytes": len(raw), "kernel_ms": kernel_ms,
+                   "note": "a step: gzip inflated on one host thread (zlib), columns copied, decoded on the GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_decode_spz", "bytes_per_splat": bytes_per, "peak_kind": peak_kind},
+        "e2e": {"value": value, "unit": "Msplats/s", "h2d_bytes_per_step": payload, "d2h_bytes_per_step": 0},
+        "gpu_launches": launches, "clocks": clock_info,
+    }
+
+
 def main():
     global BITS, FRAME_BYTES
     args = parse()
@@ -514,7 +572,8 @@ def main():
         if world > 1:
             from datetime import timedelta
             dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
-        run = {"batched": run_batched, "stereo": run_stereo, "backward": run_backward, "ply": run_ply}[args.workload]
+        run = {"batched": run_batched, "stereo": run_stereo, "backward": run_backward, "ply": run_ply,
+               "spz": run_spz}[args.workload]
         line = run(args, world, rank, local, device)
         if rank == 0:
             print(json.dumps(line))

@@ -371,6 +371,38 @@ int rdx_ply_read_info(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx_ply_
 int rdx_decode_ply(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, int sh_degree, float* centers,
                    float* log_scales, float* quats, float* opacities, float* colors);
 
+/* ---- SPZ files to raw tables ---- */
+
+/* What an SPZ file holds (its header; unpackSpz, src/core/spz.ts:141-263):
+   splats, version (1-4), SH degree (0-4), fractional bits of its fixed-point
+   centres, flags, and container: 0 gzip (versions 1-4), 1 SPZ 4's NGSP
+   container (zstd streams). */
+typedef struct rdx_spz_info {
+  uint64_t count;
+  int32_t version;
+  int32_t sh_degree;
+  int32_t fractional_bits;
+  int32_t flags;
+  int32_t container;
+  int32_t reserved;
+} rdx_spz_info;
+int rdx_spz_read_info(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx_spz_info* info);
+
+/*
+ * SpzFile.read (src/core/spz.ts:265-348) of an SPZ file in HOST memory (the
+ * container is unpacked on the host: zlib for gzip, libzstd for SPZ 4) into the
+ * columns of a raw table with `count` rows, decoded on the device: centers [3],
+ * log_scales [3] (byte / 16 - 10), quats [4] (normalised x y z w; 16-byte
+ * aligned), opacities (alpha / 255), colors [1 + K][3] (base rgb
+ * (b / 255 - 0.5) SH_C0 / 0.15 + 0.5, then (b - 128) / 128 coefficient-major)
+ * of degree sh_degree (-1: the file's; at most the file's). Any output may be
+ * NULL. Trailers (LoD tree, PBR) and extension records are not decoded. Errors
+ * carry the reference's texts ("Invalid SPZ file", "Unsupported SPZ version
+ * ...", "SPZ 4 stream ... sizes don't match its header" ...).
+ */
+int rdx_decode_spz(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, int sh_degree, float* centers,
+                   float* log_scales, float* quats, float* opacities, float* colors);
+
 /* ---- batched frames: many views of many collections ---- */
 
 /* One view of a batch: a collection (objects, as for rdx_frame) and its camera. */

@@ -1676,3 +1676,82 @@ int orc_ply_decode(const uint8_t* bytes, uint64_t nbytes, int sh_degree, double*
   }
   return 0;
 }
+
+/* ---- SPZ: src/core/spz.ts:285-348 (per splat), 571-586 (smallest three) ---- */
+
+static const int SPZ_SH_VECTORS[5] = {0, 3, 8, 15, 24};
+
+/* decodeSmallestThree: the largest component's index in the top 2 bits, then
+   the other three from the highest index down, 10 bits each (sign bit 9,
+   magnitude over sqrt(1/2) in bits 0-8) from the low bits up */
+static void spz_smallest_three(uint32_t packed, double q[4]) {
+  const int largest = (int)(packed >> 30);
+  uint32_t rest = packed;
+  double sum = 0.0;
+  for (int i = 3; i >= 0; i--) {
+    if (i == largest) continue;
+    const double mag = (double)(rest & 511u) / 511.0;
+    const double v = 0.7071067811865476 * mag * ((rest >> 9) & 1u ? -1.0 : 1.0);
+    rest >>= 10;
+    q[i] = v;
+    sum += v * v;
+  }
+  q[largest] = sqrt(fmax(1.0 - sum, 0.0));
+}
+
+int orc_spz_decode(int version, uint64_t count, int sh_degree, int fractional_bits, const uint8_t* centers,
+                   const uint8_t* alphas, const uint8_t* colors, const uint8_t* scales, const uint8_t* rotations,
+                   const uint8_t* sh, int out_degree, double* out_centers, double* out_log_scales, double* out_quats,
+                   double* out_opacities, double* out_colors) {
+  if (version < 1 || version > 4 || sh_degree < 0 || sh_degree > 4 || out_degree < 0 || out_degree > sh_degree)
+    return -1;
+  const double color_scale = 0.28209479177387814 / 0.15;
+  /* fixed = 1 / (1 << fractionalBits) with a 32-bit shift, as JS evaluates it */
+  const int32_t unit = (int32_t)(1u << (fractional_bits & 31));
+  const double fixed = 1.0 / (double)unit;
+  const int file_k = SPZ_SH_VECTORS[sh_degree], out_k = SPZ_SH_VECTORS[out_degree];
+  for (uint64_t i = 0; i < count; i++) {
+    if (out_centers) {
+      for (int c = 0; c < 3; c++) {
+        double v;
+        if (version == 1) {
+          const uint8_t* p = centers + i * 6 + c * 2;
+          v = orc_decode_half((uint32_t)p[0] | ((uint32_t)p[1] << 8));
+        } else {
+          const uint8_t* p = centers + i * 9 + c * 3;
+          int32_t code = (int32_t)((uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16));
+          if (code & 0x800000) code -= 0x1000000;
+          v = (double)code * fixed;
+        }
+        out_centers[i * 3 + c] = v;
+      }
+    }
+    if (out_opacities) out_opacities[i] = (double)alphas[i] / 255.0;
+    if (out_log_scales)
+      for (int c = 0; c < 3; c++) out_log_scales[i * 3 + c] = (double)scales[i * 3 + c] / 16.0 - 10.0;
+    if (out_quats) {
+      double q[4];
+      if (version >= 3) {
+        const uint8_t* p = rotations + i * 4;
+        spz_smallest_three((uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24), q);
+      } else {
+        const uint8_t* p = rotations + i * 3;
+        q[0] = (double)p[0] / 127.5 - 1.0;
+        q[1] = (double)p[1] / 127.5 - 1.0;
+        q[2] = (double)p[2] / 127.5 - 1.0;
+        q[3] = sqrt(fmax(0.0, 1.0 - q[0] * q[0] - q[1] * q[1] - q[2] * q[2]));
+      }
+      /* the raw table's quaternions are normalised */
+      const double l2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+      const double inv = l2 > 0.0 ? 1.0 / sqrt(l2) : 0.0;
+      for (int c = 0; c < 4; c++) out_quats[i * 4 + c] = l2 > 0.0 ? q[c] * inv : (c == 3 ? 1.0 : 0.0);
+    }
+    if (out_colors) {
+      double* row = out_colors + i * (size_t)(1 + out_k) * 3;
+      for (int c = 0; c < 3; c++) row[c] = ((double)colors[i * 3 + c] / 255.0 - 0.5) * color_scale + 0.5;
+      for (int k = 0; k < out_k; k++)
+        for (int c = 0; c < 3; c++) row[3 + k * 3 + c] = ((double)sh[(i * file_k + k) * 3 + c] - 128.0) / 128.0;
+    }
+  }
+  return 0;
+}

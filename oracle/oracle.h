@@ -139,6 +139,19 @@ int orc_encode_sh(const rdx_table* raw, int codec, uint32_t* words, int stride);
 int orc_ply_decode(const uint8_t* bytes, uint64_t nbytes, int sh_degree, double* centers, double* log_scales,
                    double* quats, double* opacities, double* colors, uint64_t* count, int* degree, int* kind);
 
+/* SpzFile.read's per-splat decode (src/core/spz.ts:285-348) of an SPZ file's
+   byte columns (a gzip payload's after its 16-byte header, or an NGSP file's
+   decompressed streams) in float64 into raw-table columns: centers [n][3]
+   (v1: halves; else 24-bit fixed point over 2^fractional_bits), log_scales
+   [n][3] (byte / 16 - 10), quats [n][4] normalised x y z w (v3 and later:
+   smallest three; else 3 bytes of x y z, w >= 0), opacities [n] (alpha / 255),
+   colors [n][1 + K][3] of degree out_degree (base rgb (b / 255 - 0.5) SH_C0 /
+   0.15 + 0.5, then (b - 128) / 128 coefficient-major). -1 on bad arguments. */
+int orc_spz_decode(int version, uint64_t count, int sh_degree, int fractional_bits, const uint8_t* centers,
+                   const uint8_t* alphas, const uint8_t* colors, const uint8_t* scales, const uint8_t* rotations,
+                   const uint8_t* sh, int out_degree, double* out_centers, double* out_log_scales, double* out_quats,
+                   double* out_opacities, double* out_colors);
+
 /* The reference's defaults (src/render/splatParams.ts:68-72) */
 void orc_params_default(rdx_params* p);
 

@@ -71,6 +71,7 @@ def lib():
             "orc_encode_ext_table": (i, [ctypes.POINTER(_abi.rdx_table), vp, vp, vp]),
             "orc_sh_basis_grad": (None, [vp, vp]),
             "orc_ply_decode": (i, [vp, ctypes.c_uint64, i, vp, vp, vp, vp, vp, vp, vp, vp]),
+            "orc_spz_decode": (i, [i, ctypes.c_uint64, i, i, vp, vp, vp, vp, vp, vp, i, vp, vp, vp, vp, vp]),
             "orc_load_splat": (None, [ctypes.POINTER(_abi.rdx_table), ctypes.c_uint64, ctypes.POINTER(orc_splat)]),
             "orc_encode_packed_table": (i, [ctypes.POINTER(_abi.rdx_table), vp, vp]),
             "orc_encode_cov_table": (i, [ctypes.POINTER(_abi.rdx_table), vp, vp]),
@@ -330,4 +331,139 @@ def ply_decode(data, sh_degree=-1):
                             ctypes.byref(kind)) != 0:
         raise ValueError("orc_ply_decode: malformed PLY")
     out.update(count=count, sh_degree=deg.value, kind=kind.value, degree=d)
+    return out
+
+
+# ---- SPZ (src/core/spz.ts): the two containers unpacked here, the splats decoded by orc_spz_decode ----
+
+SPZ_MAGIC = 0x5053474E  # "NGSP" little-endian
+SPZ_SH_VECTORS = {0: 0, 1: 3, 2: 8, 3: 15, 4: 24}
+
+
+def zstd_lib():
+    """libzstd (the system's shared library), for SPZ 4's streams; None when absent."""
+    try:
+        z = ctypes.CDLL("libzstd.so.1")
+    except OSError:
+        return None
+    z.ZSTD_decompress.restype = ctypes.c_size_t
+    z.ZSTD_decompress.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t]
+    z.ZSTD_isError.restype = ctypes.c_uint
+    z.ZSTD_isError.argtypes = [ctypes.c_size_t]
+    z.ZSTD_compress.restype = ctypes.c_size_t
+    z.ZSTD_compress.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+    z.ZSTD_compressBound.restype = ctypes.c_size_t
+    z.ZSTD_compressBound.argtypes = [ctypes.c_size_t]
+    return z
+
+
+def _le32(b, at):
+    return int.from_bytes(b[at:at + 4], "little")
+
+
+def _spz_check(version, degree, latest):
+    if version < 1 or version > latest or degree not in SPZ_SH_VECTORS:
+        raise ValueError(f"Unsupported SPZ version {version} or SH degree {degree}")
+
+
+def spz_unpack(data):
+    """unpackSpz (src/core/spz.ts:141-263): the header and byte columns of an
+    SPZ file in either container, with the reference's error texts."""
+    import zlib
+    raw = bytes(data)
+    if len(raw) >= 4 and _le32(raw, 0) == SPZ_MAGIC:
+        if len(raw) < 32:
+            raise ValueError("SPZ file ended unexpectedly")
+        version, count = _le32(raw, 4), _le32(raw, 8)
+        degree, fb, flags, nstreams = raw[12], raw[13], raw[14], raw[15]
+        toc_at = _le32(raw, 16)
+        if version != 4:
+            raise ValueError(f"Unsupported SPZ version {version} in the NGSP container")
+        _spz_check(version, degree, 4)
+        if count > 0x7FFFFFFF:
+            raise ValueError(f"Invalid SPZ point count {count}")
+        if toc_at < 32:
+            raise ValueError("SPZ 4 table of contents inside the header")
+        sizes = [count * b for b in (9, 1, 3, 3, 4, SPZ_SH_VECTORS[degree] * 3)]
+        present = [k for k, size in enumerate(sizes) if size > 0]
+        if nstreams != len(present):
+            raise ValueError(f"SPZ 4 file with {nstreams} streams, {len(present)} expected")
+        if len(raw) < toc_at + nstreams * 16:
+            raise ValueError("SPZ file ended unexpectedly")
+        total = toc_at + nstreams * 16
+        comp = []
+        for k in range(nstreams):
+            low, high, size_low, size_high = (_le32(raw, toc_at + k * 16 + a) for a in (0, 4, 8, 12))
+            if high >= 1 << 21 or size_high != 0 or size_low != sizes[present[k]]:
+                raise ValueError(f"SPZ 4 stream {k} sizes don't match its header")
+            comp.append(high * 2 ** 32 + low)
+            total += comp[-1]
+        if count * 9 > total * 1024:
+            raise ValueError(f"Invalid SPZ point count {count} for {total} bytes")
+        z = zstd_lib()
+        if z is None:
+            raise ValueError("SPZ 4 needs libzstd")
+        cols = [b""] * 6
+        at = toc_at + nstreams * 16
+        for k in range(nstreams):
+            if at + comp[k] > len(raw):
+                raise ValueError("SPZ file ended unexpectedly")
+            src = np.frombuffer(raw[at:at + comp[k]], dtype=np.uint8)
+            dst = np.zeros(max(sizes[present[k]], 1), dtype=np.uint8)
+            got = z.ZSTD_decompress(_p(dst), sizes[present[k]], _p(src), comp[k])
+            if z.ZSTD_isError(got) or got != sizes[present[k]]:
+                raise ValueError(f"SPZ 4 stream {k} does not decompress to its size")
+            cols[present[k]] = dst[:sizes[present[k]]].tobytes()
+            at += comp[k]
+        if at != len(raw):
+            raise ValueError("SPZ 4 file has bytes after its last stream")
+        return {"container": "ngsp", "version": version, "count": count, "sh_degree": degree,
+                "fractional_bits": fb, "flags": flags, "centers": cols[0], "alphas": cols[1], "colors": cols[2],
+                "scales": cols[3], "rotations": cols[4], "sh": cols[5]}
+    if raw[:2] != b"\x1f\x8b":
+        raise ValueError("Invalid SPZ file")
+    d = zlib.decompressobj(wbits=31)
+    payload = d.decompress(raw)
+    while d.eof and d.unused_data:  # concatenated gzip members
+        rest = d.unused_data
+        d = zlib.decompressobj(wbits=31)
+        payload += d.decompress(rest)
+    if len(payload) < 16:
+        raise ValueError("SPZ file ended unexpectedly")
+    if _le32(payload, 0) != SPZ_MAGIC:
+        raise ValueError("Invalid SPZ file")
+    version, count = _le32(payload, 4), _le32(payload, 8)
+    degree, fb, flags = payload[12], payload[13], payload[14]
+    _spz_check(version, degree, 4)
+    sizes = [count * (6 if version == 1 else 9), count, count * 3, count * 3, count * (4 if version >= 3 else 3),
+             count * SPZ_SH_VECTORS[degree] * 3]
+    at, cols = 16, []
+    for size in sizes:
+        if at + size > len(payload):
+            raise ValueError("SPZ file ended unexpectedly")
+        cols.append(payload[at:at + size])
+        at += size
+    return {"container": "gzip", "version": version, "count": count, "sh_degree": degree, "fractional_bits": fb,
+            "flags": flags, "centers": cols[0], "alphas": cols[1], "colors": cols[2], "scales": cols[3],
+            "rotations": cols[4], "sh": cols[5]}
+
+
+def spz_decode(data, sh_degree=-1):
+    """SpzFile.read's splats (src/core/spz.ts:265-348) as float64 raw-table
+    columns (orc_spz_decode), plus the header fields."""
+    u = spz_unpack(data)
+    deg = u["sh_degree"] if sh_degree < 0 else sh_degree
+    if deg > u["sh_degree"]:
+        raise ValueError(f"the file has SH degree {u['sh_degree']}, not {deg}")
+    n = u["count"]
+    out = {"centers": np.zeros((n, 3)), "log_scales": np.zeros((n, 3)), "quats": np.zeros((n, 4)),
+           "opacities": np.zeros(n), "colors": np.zeros((n, (deg + 1) ** 2, 3))}
+    cols = [np.frombuffer(u[k], dtype=np.uint8) if len(u[k]) else np.zeros(1, dtype=np.uint8)
+            for k in ("centers", "alphas", "colors", "scales", "rotations", "sh")]
+    if lib().orc_spz_decode(u["version"], n, u["sh_degree"], u["fractional_bits"], *(_p(c) for c in cols), deg,
+                            _p(out["centers"]), _p(out["log_scales"]), _p(out["quats"]), _p(out["opacities"]),
+                            _p(out["colors"])) != 0:
+        raise ValueError("orc_spz_decode: bad arguments")
+    out.update({k: u[k] for k in ("container", "version", "count", "sh_degree", "fractional_bits", "flags")})
+    out["degree"] = deg
     return out

@@ -26,7 +26,7 @@ from .camera import IDENTITY, Camera, look_at, perspective
 __all__ = [
     "Context", "SortKeys", "RadixSort", "Compact", "SplatSorter", "SplatParams", "Table", "SplatObject",
     "Camera", "look_at", "perspective", "project_collection", "project_backward", "frame", "frame_batched", "Batch",
-    "RadixError", "decode_ply", "ply_info",
+    "RadixError", "decode_ply", "ply_info", "decode_spz", "spz_info",
     "align_capacity",
 ]
 
@@ -649,11 +649,51 @@ PLY_KINDS = ("standard", "points", "compressed")
 
 
 def _bytes_arg(data):
-    """(pointer, size, keep-alive) of PLY bytes: bytes / bytearray / numpy uint8 / a CUDA uint8 tensor."""
+    """(pointer, size, keep-alive) of file bytes: bytes / bytearray / numpy uint8 / a uint8 tensor."""
     if _is_torch(data):
         return _ptr(data), int(data.numel() * data.element_size()), data
     arr = np.frombuffer(bytes(data), dtype=np.uint8) if not isinstance(data, np.ndarray) else data
     return arr.ctypes.data, int(arr.nbytes), arr
+
+
+SPZ_CONTAINERS = ("gzip", "ngsp")
+
+
+def spz_info(data, ctx=None):
+    """unpackSpz's view of an SPZ file's header (host bytes): {count, version,
+    sh_degree, fractional_bits, flags, container}."""
+    c = ctx or default_context(0)
+    if _is_torch(data) and data.is_cuda:
+        raise RadixError(_abi.RDX_ERR_ARG, "SPZ bytes must be in host memory (the container is unpacked on the host)")
+    ptr, size, keep = _bytes_arg(data)
+    info = _abi.rdx_spz_info()
+    c.call("rdx_spz_read_info", ctypes.c_void_p(ptr), size, ctypes.byref(info))
+    del keep
+    return {"count": int(info.count), "version": int(info.version), "sh_degree": int(info.sh_degree),
+            "fractional_bits": int(info.fractional_bits), "flags": int(info.flags),
+            "container": SPZ_CONTAINERS[info.container]}
+
+
+def decode_spz(data, sh_degree=-1, device="cuda", ctx=None):
+    """SpzFile.read (src/core/spz.ts) of an SPZ file (host bytes, gzip or SPZ 4)
+    decoded on the GPU into a raw Table of float32 columns (centres, ln scales,
+    normalised quaternions, opacities, base rgb + SH of degree sh_degree, -1:
+    the file's)."""
+    torch = _torch()
+    info = spz_info(data, ctx)
+    deg = info["sh_degree"] if sh_degree < 0 else sh_degree
+    n = info["count"]
+    dev = torch.device(device)
+    cols = {"centers": torch.empty((n, 3), device=dev), "log_scales": torch.empty((n, 3), device=dev),
+            "quats": torch.empty((n, 4), device=dev), "opacities": torch.empty(n, device=dev),
+            "colors": torch.empty((n, (deg + 1) ** 2, 3), device=dev)}
+    c = ctx or default_context(0)
+    ptr, size, keep = _bytes_arg(data)
+    c.call("rdx_decode_spz", ctypes.c_void_p(ptr), size, deg, *(ctypes.c_void_p(_ptr(cols[k])) for k in
+                                                                  ("centers", "log_scales", "quats", "opacities",
+                                                                   "colors")))
+    del keep
+    return Table.raw(cols["centers"], cols["log_scales"], cols["quats"], cols["opacities"], cols["colors"], deg), cols
 
 
 def ply_info(data, ctx=None):

@@ -134,6 +134,12 @@ class rdx_ply_info(ctypes.Structure):
     _fields_ = [("count", ctypes.c_uint64), ("sh_degree", ctypes.c_int32), ("kind", ctypes.c_int32)]
 
 
+class rdx_spz_info(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_uint64), ("version", ctypes.c_int32), ("sh_degree", ctypes.c_int32),
+                ("fractional_bits", ctypes.c_int32), ("flags", ctypes.c_int32), ("container", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
 class rdx_outputs(ctypes.Structure):
     _fields_ = [
         ("mean2d", ctypes.c_void_p),
@@ -184,6 +190,9 @@ SIGNATURES = {
                                             ctypes.POINTER(rdx_grads_in), ctypes.POINTER(rdx_table_grads)]),
     "rdx_ply_read_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(rdx_ply_info)]),
     "rdx_decode_ply": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "rdx_spz_read_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(rdx_spz_info)]),
+    "rdx_decode_spz": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_frame_batched": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_view), ctypes.c_int, ctypes.POINTER(rdx_params),
                                          ctypes.c_int, ctypes.POINTER(rdx_outputs), ctypes.c_void_p, ctypes.c_void_p]),

@@ -17,7 +17,7 @@ LIB = os.path.join(LIB_DIR, "libradix_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "--expt-relaxed-constexpr"]
-SOURCES = ["sort.cu", "keys.cu", "project.cu", "backward.cu", "ply.cu", "noalloc.cu", "abi.cpp"]
+SOURCES = ["sort.cu", "keys.cu", "project.cu", "backward.cu", "ply.cu", "spz.cu", "noalloc.cu", "abi.cpp"]
 
 
 def _compile(src, verbose):
@@ -48,7 +48,8 @@ def build(verbose=False):
                 print(f"== {src}\n{log}")
     newest = max(os.path.getmtime(o) for o in objs)
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < newest:
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static"]
+        # zlib inflates gzip SPZ files; libzstd (SPZ 4) is opened at run time with dlopen
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lz", "-ldl"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -14,6 +14,8 @@
 #include <algorithm>
 #include <map>
 #include <string>
+#include <memory>
+#include <new>
 #include <vector>
 
 #include "../../include/radix_b200.h"
@@ -1509,6 +1511,84 @@ int rdx_decode_ply(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, int sh_degr
   s = copy_back(ctx, plan);
   if (s != RDX_OK) return s;
   return host_in || !plan.back.empty() ? finish(ctx) : RDX_OK;
+}
+
+static int read_spz_header(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx::SpzDesc* d) {
+  if (!bytes || nbytes == 0) return fail(ctx, RDX_ERR_ARG, "Invalid SPZ file");
+  if (is_device_ptr(bytes))
+    return fail(ctx, RDX_ERR_ARG, "SPZ bytes must be in host memory (the container is unpacked on the host)");
+  const char* err = rdx::spz_header(reinterpret_cast<const unsigned char*>(bytes), nbytes, d);
+  return err ? fail(ctx, RDX_ERR_ARG, "%s", err) : RDX_OK;
+}
+
+int rdx_spz_read_info(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx_spz_info* info) {
+  if (!ctx || !info) return RDX_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  rdx::SpzDesc d;
+  int s = read_spz_header(ctx, bytes, nbytes, &d);
+  if (s != RDX_OK) return s;
+  info->count = d.count;
+  info->version = d.version;
+  info->sh_degree = d.sh_degree;
+  info->fractional_bits = d.fractional_bits;
+  info->flags = d.flags;
+  info->container = d.container;
+  info->reserved = 0;
+  return RDX_OK;
+}
+
+int rdx_decode_spz(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, int sh_degree, float* centers, float* log_scales,
+                   float* quats, float* opacities, float* colors) {
+  if (!ctx) return RDX_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  rdx::SpzDesc d;
+  int s = read_spz_header(ctx, bytes, nbytes, &d);
+  if (s != RDX_OK) return s;
+  if (sh_degree < 0) sh_degree = d.sh_degree;
+  if (sh_degree > d.sh_degree)
+    return fail(ctx, RDX_ERR_ARG, "the file has SH degree %d, not %d", d.sh_degree, sh_degree);
+  d.out_degree = sh_degree;
+  const uint64_t n = d.count;
+  const size_t row = (size_t)(1 + kShCoeffs[sh_degree]) * 3;
+  if (quats && is_device_ptr(quats) && !aligned(quats, 16)) return fail(ctx, RDX_ERR_ARG, "quats is not 16-byte aligned");
+  // The columns unpacked on the host first: a bad stream fails before any device work
+  std::unique_ptr<unsigned char[]> payload(new (std::nothrow) unsigned char[d.payload ? d.payload : 1]);
+  if (!payload) return fail(ctx, RDX_ERR_NOMEM, "could not allocate %llu bytes for the SPZ columns",
+                            (unsigned long long)d.payload);
+  const char* err = rdx::spz_unpack(reinterpret_cast<const unsigned char*>(bytes), nbytes, d, payload.get());
+  if (err) return fail(ctx, RDX_ERR_ARG, "%s", err);
+  OutPlan plan;
+  unsigned char* dev_payload = nullptr;
+  float *c = nullptr, *l = nullptr, *q = nullptr, *o = nullptr, *col = nullptr;
+  int status = RDX_OK;
+  auto layout = [&](Arena& a) {
+    plan = OutPlan();
+    dev_payload = a.take<unsigned char>(d.payload);
+    c = stage_out(ctx, a, centers, n * 12, 4, plan, &status);
+    l = stage_out(ctx, a, log_scales, n * 12, 4, plan, &status);
+    q = stage_out(ctx, a, quats, n * 16, 16, plan, &status);
+    o = stage_out(ctx, a, opacities, n * 4, 4, plan, &status);
+    col = stage_out(ctx, a, colors, n * row * 4, 4, plan, &status);
+  };
+  Arena dry(nullptr);
+  layout(dry);
+  if (status != RDX_OK) return status;
+  s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  layout(a);
+  if (status != RDX_OK) return status;
+  // pageable source: the copy has left `payload` when the call returns
+  if (d.payload) RDX_CUDA(cudaMemcpyAsync(dev_payload, payload.get(), d.payload, cudaMemcpyHostToDevice, ctx->stream), "SPZ copy");
+  d.base = dev_payload;
+  {
+    Phase decoding(ctx, RDX_PHASE_PROJECT);
+    RDX_CUDA(rdx::launch_decode_spz(d, c, l, q, o, col, ctx->stream), "SPZ decode launch");
+    if (n) ctx->launches += 1;
+  }
+  s = copy_back(ctx, plan);
+  if (s != RDX_OK) return s;
+  return finish(ctx);
 }
 
 int rdx_frame_batched(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx_params* params, int sort_bits,

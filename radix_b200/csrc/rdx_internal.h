@@ -202,6 +202,35 @@ struct ProjOutputs {
 constexpr int kProjTile = 32;
 
 
+// ---- SPZ files (src/core/spz.ts) to raw tables ----
+
+// An SPZ file's header and the layout of its byte columns once unpacked on the
+// host: centers, alphas, colors, scales, rotations, SH, back to back
+struct SpzDesc {
+  uint64_t count = 0;
+  int container = 0;  // 0: gzip (versions 1-4), 1: SPZ 4's NGSP container
+  int version = 0;
+  int sh_degree = 0;
+  int fractional_bits = 0;
+  int flags = 0;
+  int out_degree = 0;
+  int n_streams = 0;           // NGSP: zstd streams (non-empty columns)
+  uint64_t toc_at = 0;         // NGSP: byte offset of the table of contents
+  uint64_t col_off[6] = {};    // in the unpacked payload
+  uint64_t col_size[6] = {};
+  uint64_t payload = 0;        // unpacked bytes
+  const unsigned char* base = nullptr;  // device address of the unpacked payload (set before a launch)
+};
+constexpr int kSpzGzip = 0;
+constexpr int kSpzNgsp = 1;
+// An SPZ file's header from host bytes: null, or the reference's error text
+const char* spz_header(const unsigned char* bytes, uint64_t nbytes, SpzDesc* d);
+// The file's columns unpacked on the host into payload (d.payload bytes): gzip
+// inflated by zlib, NGSP streams by libzstd (loaded when first needed): null or an error text
+const char* spz_unpack(const unsigned char* bytes, uint64_t nbytes, const SpzDesc& d, unsigned char* payload);
+cudaError_t launch_decode_spz(const SpzDesc& d, float* centers, float* log_scales, float* quats, float* opacities,
+                              float* colors, cudaStream_t stream);
+
 // One persistent launch over every descriptor of one table kind (descs in device memory)
 // ---- PLY files (src/core/ply.ts) to raw tables ----
 
