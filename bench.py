@@ -206,6 +206,25 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def max_over_ranks(value, world, device):
+    """The largest of a per-rank float over the process group's ranks (the
+    value itself for one rank): every rank gets it."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replicas_throughput(units_per_rank, steps, world, ms_total):
+    """Whole-job throughput in millions of units per second: `world` replicas,
+    each processing units_per_rank units a step, `steps` steps in ms_total
+    (the slowest rank's time)."""
+    return world * units_per_rank * steps / (ms_total / 1e3) / 1e6
+
+
 def timed(step, steps, warmup, world, local, after_warmup=None):
     """W untimed steps, then K steps between barriers, timed with CUDA events
     on the current stream; returns (max over ranks of the total ms, clocks)."""
@@ -230,11 +249,7 @@ def timed(step, steps, warmup, world, local, after_warmup=None):
     if world > 1:
         dist.barrier()
     clock_info = clocks.stop()
-    ms = start.elapsed_time(stop)
-    if world > 1:
-        t = torch.tensor([ms], device=torch.device("cuda", local), dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(start.elapsed_time(stop), world, torch.device("cuda", local))
     return ms, clock_info
 
 
@@ -282,7 +297,7 @@ def run_batched(args, world, rank, local, device):
     batch.close()
     return {
         "metric": "Msplat-views/s (batched project+SH+key+sort)",
-        "value": world * n_views * args.steps / (ms_total / 1e3) / 1e6, "unit": "Msplat-views/s",
+        "value": replicas_throughput(n_views, args.steps, world, ms_total), "unit": "Msplat-views/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
         "data": "synthetic (seeded mulberry32 + Box-Muller)",
@@ -351,7 +366,7 @@ def run_stereo(args, world, rank, local, device):
     achieved = proj_bytes * n / (proj_ms / 1e3) / 1e9
     return {
         "metric": "Msplats/s (stereo project+SH+key+sort)",
-        "value": world * n * args.steps / (ms_total / 1e3) / 1e6, "unit": "Msplats/s",
+        "value": replicas_throughput(n, args.steps, world, ms_total), "unit": "Msplats/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16 SH, f32+f64 maths",
         "data": "synthetic (seeded mulberry32 + Box-Muller)",
@@ -418,7 +433,7 @@ def run_backward(args, world, rank, local, device):
     achieved = bwd_bytes * n / (ms_step / 1e3) / 1e9
     return {
         "metric": "Msplats/s (projection backward)",
-        "value": world * n * args.steps / (ms_total / 1e3) / 1e6, "unit": "Msplats/s",
+        "value": replicas_throughput(n, args.steps, world, ms_total), "unit": "Msplats/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 adjoint, f32 I/O",
         "data": "synthetic (seeded mulberry32 + Box-Muller; upstream N(0, 1))",
@@ -481,7 +496,7 @@ def run_ply(args, world, rank, local, device):
     bytes_per = record + 12 + 12 + 16 + 4 + row
     achieved = bytes_per * n / (ms_step / 1e3) / 1e9
     return {
-        "metric": "Msplats/s (PLY decode)", "value": world * n * args.steps / (ms_total / 1e3) / 1e6,
+        "metric": "Msplats/s (PLY decode)", "value": replicas_throughput(n, args.steps, world, ms_total),
         "unit": "Msplats/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 in, f64 maths, f32 out",
         "data": "synthetic (a PLY file written from the seeded SH-3 mixture)",
@@ -536,7 +551,7 @@ def run_spz(args, world, rank, local, device):
     peak, peak_kind = peak_hbm()
     bytes_per = payload // n + 12 + 12 + 16 + 4 + (k + 1) * 3 * 4
     achieved = bytes_per * n / (kernel_ms / 1e3) / 1e9
-    value = world * n * args.steps / (ms_total / 1e3) / 1e6
+    value = replicas_throughput(n, args.steps, world, ms_total)
     return {
         "metric": "Msplats/s (SPZ decode, host bytes to a device table)", "value": value,
         "unit": "Msplats/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
@@ -618,7 +633,7 @@ def main():
     batch.synchronize()
     launches = graph_kernels * args.steps
     ms_step = ms_total / args.steps
-    value = world * n * args.steps / (ms_total / 1e3) / 1e6
+    value = replicas_throughput(n, args.steps, world, ms_total)
     # the same frame through rb.frame (host planning every call), and its phase split
     frame_ms, _ = timed(frame_step, args.steps, args.warmup, world, local)
 
@@ -652,12 +667,8 @@ def main():
             rb.frame(hobj, cam, None, BITS, names, ctx=ctx, out=out, ordering=host_order)
         e1.record()
         torch.cuda.synchronize()
-        e_ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([e_ms], device=device, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
-        e2e = {"value": world * n * e2e_steps / (e_ms / 1e3) / 1e6, "unit": "Msplats/s",
+        e_ms = max_over_ranks(e0.elapsed_time(e1), world, device)
+        e2e = {"value": replicas_throughput(n, e2e_steps, world, e_ms), "unit": "Msplats/s",
                "h2d_bytes_per_step": bi, "d2h_bytes_per_step": bo, "ms_per_step": e_ms / e2e_steps}
 
     peak, peak_kind = peak_hbm()
