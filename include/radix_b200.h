@@ -403,6 +403,43 @@ int rdx_spz_read_info(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx_spz_
 int rdx_decode_spz(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, int sh_degree, float* centers,
                    float* log_scales, float* quats, float* opacities, float* colors);
 
+/* ---- RDX files (the reference's own container) to device arrays ---- */
+
+/* What an RDX file holds (its header piece; src/core/rdx.ts:19-40, 162-170):
+   elements, rows per chunk, chunks, serialized channels, and the header's JSON
+   text (bundle definitions and metas) */
+typedef struct rdx_rdxfile_info {
+  uint64_t count;
+  uint64_t chunk_size;
+  int32_t n_chunks;
+  int32_t n_channels;
+  uint64_t header_json_bytes;
+} rdx_rdxfile_info;
+/* One serialized channel, in payload order: bundle and label names, its
+   ArrayFormats name ("uint32x4", "float16", ...) and bytes per element */
+typedef struct rdx_rdxfile_channel {
+  char bundle[64];
+  char label[64];
+  char format[16];
+  int32_t element_bytes;
+  int32_t reserved;
+} rdx_rdxfile_channel;
+/* Fills info; then up to `capacity` channels and up to json_capacity bytes of
+   the header's JSON (either may be NULL). Host bytes only. */
+int rdx_rdxfile_read_info(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx_rdxfile_info* info,
+                          rdx_rdxfile_channel* channels, int capacity, char* header_json, uint64_t json_capacity);
+
+/*
+ * RdxFile.read of a whole file in HOST memory (header then every chunk;
+ * decodeRdxChunk, src/core/rdx.ts:181-205): channels[k] (n_channels pointers,
+ * host or device, NULL to skip) receives channel k's count * element_bytes
+ * bytes. Payloads are inflated on the host and transposed back on the device.
+ * Errors carry the reference's texts ("Not an RDX piece of the expected
+ * type", "RDX version ... is not 1", "Chunk at ...: ... holds ... bytes,
+ * expected ...").
+ */
+int rdx_decode_rdxfile(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, void* const* channels);
+
 /* ---- batched frames: many views of many collections ---- */
 
 /* One view of a batch: a collection (objects, as for rdx_frame) and its camera. */

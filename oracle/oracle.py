@@ -467,3 +467,59 @@ def spz_decode(data, sh_degree=-1):
     out.update({k: u[k] for k in ("container", "version", "count", "sh_degree", "fractional_bits", "flags")})
     out["degree"] = deg
     return out
+
+
+# ---- RDX files (src/core/rdx.ts:62-205): containers, byte-transposed gzip payloads ----
+
+RDX_HEADER_MAGIC = 0x48584452  # "RDXH"
+RDX_CHUNK_MAGIC = 0x43584452   # "RDXC"
+_RDX_SCALARS = {"uint8": 1, "sint8": 1, "unorm8": 1, "snorm8": 1, "uint16": 2, "sint16": 2, "float16": 2,
+                "uint32": 4, "sint32": 4, "float32": 4}
+
+
+def _rdx_container(raw, at, magic):
+    """decodeContainer: (meta, [payload bytes], byte length) of the piece at `at`."""
+    import json
+    if len(raw) - at < 16 or _le32(raw, at) != magic:
+        raise ValueError("Not an RDX piece of the expected type")
+    meta_len, count = _le32(raw, at + 4), _le32(raw, at + 8)
+    meta = json.loads(raw[at + 16:at + 16 + meta_len].decode())
+    sizes_at = at + 16 + (meta_len + 15) // 16 * 16
+    off = sizes_at + (count * 4 + 15) // 16 * 16
+    payloads = []
+    for i in range(count):
+        size = _le32(raw, sizes_at + 4 * i)
+        if off + size > len(raw):
+            raise ValueError("RDX file ended unexpectedly")
+        payloads.append(raw[off:off + size])
+        off += (size + 15) // 16 * 16
+    return meta, payloads, off - at
+
+
+def rdxfile_read(data):
+    """RdxFile.read of a whole file: (header, {bundle: {label: uint8 array [count, element bytes]}})."""
+    import zlib
+    raw = bytes(data)
+    header, _, length = _rdx_container(raw, 0, RDX_HEADER_MAGIC)
+    if header.get("version") != 1:
+        raise ValueError(f"RDX version {header.get('version')} is not 1")
+    count = header["count"]
+    chans = []
+    for name, b in header["bundles"].items():
+        for label, fmt in b["def"]["channels"].items():
+            scalar, _, comps = fmt.partition("x")
+            chans.append((name, label, _RDX_SCALARS[scalar] * (int(comps) if comps else 1)))
+    out = {name: {} for name, _, _ in chans}
+    for name, label, eb in chans:
+        out[name][label] = np.zeros((count, eb), dtype=np.uint8)
+    at = length
+    for size in header["chunks"]:
+        meta, payloads, _ = _rdx_container(raw, at, RDX_CHUNK_MAGIC)
+        start, n = meta["start"], meta["count"]
+        for (name, label, eb), p in zip(chans, payloads):
+            t = np.frombuffer(zlib.decompress(p, 31), dtype=np.uint8)
+            if t.size != n * eb:
+                raise ValueError(f"Chunk at {start}: {name}.{label} holds {t.size} bytes, expected {n * eb}")
+            out[name][label][start:start + n] = t.reshape(eb, n).T
+        at += size
+    return header, out

@@ -26,7 +26,8 @@ from .camera import IDENTITY, Camera, look_at, perspective
 __all__ = [
     "Context", "SortKeys", "RadixSort", "Compact", "SplatSorter", "SplatParams", "Table", "SplatObject",
     "Camera", "look_at", "perspective", "project_collection", "project_backward", "frame", "frame_batched", "Batch",
-    "RadixError", "decode_ply", "ply_info", "decode_spz", "spz_info",
+    "RadixError", "decode_ply", "ply_info", "decode_spz", "spz_info", "rdxfile_info", "decode_rdxfile",
+    "rdxfile_table",
     "align_capacity",
 ]
 
@@ -694,6 +695,83 @@ def decode_spz(data, sh_degree=-1, device="cuda", ctx=None):
                                                                    "colors")))
     del keep
     return Table.raw(cols["centers"], cols["log_scales"], cols["quats"], cols["opacities"], cols["colors"], deg), cols
+
+
+def rdxfile_info(data, ctx=None):
+    """An RDX file's header (src/core/rdx.ts): {count, chunk_size, chunks,
+    channels: [(bundle, label, format, element_bytes)] in payload order,
+    header: the header's JSON as a dict}. Host bytes only."""
+    import json
+    c = ctx or default_context(0)
+    if _is_torch(data) and data.is_cuda:
+        raise RadixError(_abi.RDX_ERR_ARG, "RDX bytes must be in host memory (the payloads are inflated on the host)")
+    ptr, size, keep = _bytes_arg(data)
+    info = _abi.rdx_rdxfile_info()
+    c.call("rdx_rdxfile_read_info", ctypes.c_void_p(ptr), size, ctypes.byref(info), None, 0, None, 0)
+    chans = (_abi.rdx_rdxfile_channel * max(info.n_channels, 1))()
+    text = ctypes.create_string_buffer(int(info.header_json_bytes) + 1)
+    c.call("rdx_rdxfile_read_info", ctypes.c_void_p(ptr), size, ctypes.byref(info), chans, info.n_channels, text,
+           info.header_json_bytes)
+    del keep
+    channels = [(ch.bundle.decode(), ch.label.decode(), ch.format.decode(), int(ch.element_bytes))
+                for ch in chans[:info.n_channels]]
+    return {"count": int(info.count), "chunk_size": int(info.chunk_size), "chunks": int(info.n_chunks),
+            "channels": channels, "header": json.loads(text.raw[:info.header_json_bytes].decode())}
+
+
+def decode_rdxfile(data, device="cuda", ctx=None):
+    """RdxFile.read of a whole RDX file (host bytes): (info, {bundle: {label:
+    uint8 tensor [count, element_bytes]}}), every serialized channel decoded
+    on the GPU (inflated on the host, bytes transposed back on the device)."""
+    torch = _torch()
+    info = rdxfile_info(data, ctx)
+    n = info["count"]
+    dev = torch.device(device)
+    out, ptrs = {}, []
+    for bundle, label, fmt, eb in info["channels"]:
+        t = torch.empty((n, eb), dtype=torch.uint8, device=dev)
+        out.setdefault(bundle, {})[label] = t
+        ptrs.append(_ptr(t) if n else None)
+    c = ctx or default_context(0)
+    ptr, size, keep = _bytes_arg(data)
+    arr = (ctypes.c_void_p * max(len(ptrs), 1))(*ptrs)
+    c.call("rdx_decode_rdxfile", ctypes.c_void_p(ptr), size, arr)
+    del keep
+    return info, out
+
+
+def _words(t):
+    """A uint8 [count, 16] channel as int32 [count, 4] words."""
+    return t.view(_torch().int32).reshape(t.shape[0], -1)
+
+
+def rdxfile_table(data, device="cuda", ctx=None):
+    """A Table over an RDX file's splats: its extSplats, covSplats or
+    packedSplats bundle (src/core/splats.ts:69-77; packedSplats' meta.encoding)
+    and its per-splat SH bundle ("extSh" or "packedSh", meta {codec, degree},
+    src/core/sh.ts:230-240), decoded on the GPU. Returns (table, channels)."""
+    info, ch = decode_rdxfile(data, device, ctx)
+    bundles = info["header"]["bundles"]
+    sh, deg, codec = (), 0, "ext"
+    for name in ("extSh", "packedSh"):
+        if name in ch:
+            meta = bundles[name].get("meta", {})
+            codec = meta.get("codec", name[:-2])
+            deg = int(meta.get("degree", 0))
+            sh = [_words(t) for t in ch[name].values()]
+            break
+    if "extSplats" in ch:
+        t = Table.ext(_words(ch["extSplats"]["extA"]), _words(ch["extSplats"]["extB"]), sh, deg, codec)
+    elif "covSplats" in ch:
+        t = Table.cov(_words(ch["covSplats"]["covA"]), _words(ch["covSplats"]["covB"]), sh, deg, codec)
+    elif "packedSplats" in ch:
+        e = dict(zip(("rgbMin", "rgbMax", "lnScaleMin", "lnScaleMax"), Table.PACKED_ENCODING))
+        e.update(bundles["packedSplats"].get("meta", {}).get("encoding", {}))
+        enc = (e["rgbMin"], e["rgbMax"], e["lnScaleMin"], e["lnScaleMax"])
+        t = Table.packed(_words(ch["packedSplats"]["packed"]), enc, sh, deg, codec)
+    else:
+        raise RadixError(_abi.RDX_ERR_ARG, "the RDX file has no extSplats, covSplats or packedSplats bundle")
+    return t, ch
 
 
 def ply_info(data, ctx=None):

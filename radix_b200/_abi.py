@@ -140,6 +140,16 @@ class rdx_spz_info(ctypes.Structure):
                 ("reserved", ctypes.c_int32)]
 
 
+class rdx_rdxfile_info(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_uint64), ("chunk_size", ctypes.c_uint64), ("n_chunks", ctypes.c_int32),
+                ("n_channels", ctypes.c_int32), ("header_json_bytes", ctypes.c_uint64)]
+
+
+class rdx_rdxfile_channel(ctypes.Structure):
+    _fields_ = [("bundle", ctypes.c_char * 64), ("label", ctypes.c_char * 64), ("format", ctypes.c_char * 16),
+                ("element_bytes", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
 class rdx_outputs(ctypes.Structure):
     _fields_ = [
         ("mean2d", ctypes.c_void_p),
@@ -194,6 +204,11 @@ SIGNATURES = {
     "rdx_spz_read_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(rdx_spz_info)]),
     "rdx_decode_spz": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "rdx_rdxfile_read_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                             ctypes.POINTER(rdx_rdxfile_info), ctypes.POINTER(rdx_rdxfile_channel),
+                                             ctypes.c_int, ctypes.c_char_p, ctypes.c_uint64]),
+    "rdx_decode_rdxfile": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                          ctypes.POINTER(ctypes.c_void_p)]),
     "rdx_frame_batched": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_view), ctypes.c_int, ctypes.POINTER(rdx_params),
                                          ctypes.c_int, ctypes.POINTER(rdx_outputs), ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_batch_create": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_view), ctypes.c_int, ctypes.POINTER(rdx_params),

@@ -17,7 +17,7 @@ LIB = os.path.join(LIB_DIR, "libradix_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "--expt-relaxed-constexpr"]
-SOURCES = ["sort.cu", "keys.cu", "project.cu", "backward.cu", "ply.cu", "spz.cu", "noalloc.cu", "abi.cpp"]
+SOURCES = ["sort.cu", "keys.cu", "project.cu", "backward.cu", "ply.cu", "spz.cu", "rdxfile.cu", "noalloc.cu", "abi.cpp"]
 
 
 def _compile(src, verbose):

@@ -1591,6 +1591,105 @@ int rdx_decode_spz(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, int sh_degr
   return finish(ctx);
 }
 
+static int read_rdxfile_header(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx::RdxFile* f) {
+  if (!bytes || nbytes == 0) return fail(ctx, RDX_ERR_ARG, "Not an RDX piece of the expected type");
+  if (is_device_ptr(bytes))
+    return fail(ctx, RDX_ERR_ARG, "RDX bytes must be in host memory (the payloads are inflated on the host)");
+  const char* err = rdx::rdxfile_header(reinterpret_cast<const unsigned char*>(bytes), nbytes, f);
+  return err ? fail(ctx, RDX_ERR_ARG, "%s", err) : RDX_OK;
+}
+
+int rdx_rdxfile_read_info(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx_rdxfile_info* info,
+                          rdx_rdxfile_channel* channels, int capacity, char* header_json, uint64_t json_capacity) {
+  if (!ctx || !info) return RDX_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  rdx::RdxFile f;
+  int s = read_rdxfile_header(ctx, bytes, nbytes, &f);
+  if (s != RDX_OK) return s;
+  info->count = f.count;
+  info->chunk_size = f.chunk_size;
+  info->n_chunks = (int32_t)f.chunk_bytes.size();
+  info->n_channels = (int32_t)f.channels.size();
+  info->header_json_bytes = f.header_json.size();
+  for (int k = 0; channels && k < capacity && k < (int)f.channels.size(); k++) {
+    const rdx::RdxChannel& c = f.channels[k];
+    if (c.bundle.size() >= sizeof(channels[k].bundle) || c.label.size() >= sizeof(channels[k].label) ||
+        c.format.size() >= sizeof(channels[k].format))
+      return fail(ctx, RDX_ERR_ARG, "RDX channel name too long: %s.%s", c.bundle.c_str(), c.label.c_str());
+    memset(&channels[k], 0, sizeof(channels[k]));
+    memcpy(channels[k].bundle, c.bundle.data(), c.bundle.size());
+    memcpy(channels[k].label, c.label.data(), c.label.size());
+    memcpy(channels[k].format, c.format.data(), c.format.size());
+    channels[k].element_bytes = c.element_bytes;
+  }
+  if (header_json && json_capacity) {
+    const size_t nj = std::min<size_t>(f.header_json.size(), json_capacity);
+    memcpy(header_json, f.header_json.data(), nj);
+  }
+  return RDX_OK;
+}
+
+int rdx_decode_rdxfile(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, void* const* channels) {
+  if (!ctx) return RDX_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  rdx::RdxFile f;
+  int s = read_rdxfile_header(ctx, bytes, nbytes, &f);
+  if (s != RDX_OK) return s;
+  const int nc = (int)f.channels.size();
+  std::vector<char> wanted(nc > 0 ? nc : 1);
+  for (int k = 0; k < nc; k++) wanted[k] = channels && channels[k];
+  // Every payload inflated on the host first: a bad chunk fails before any device work
+  std::vector<unsigned char> staged;
+  std::vector<rdx::RdxSpan> spans;
+  static_assert(sizeof(bool) == sizeof(char), "wanted flags");
+  const char* err = rdx::rdxfile_unpack(reinterpret_cast<const unsigned char*>(bytes), nbytes, f,
+                                        reinterpret_cast<const bool*>(wanted.data()), &staged, &spans);
+  if (err) return fail(ctx, RDX_ERR_ARG, "%s", err);
+  OutPlan plan;
+  std::vector<unsigned char*> outs(nc > 0 ? nc : 1, nullptr);
+  unsigned char* dev_staged = nullptr;
+  rdx::RdxPiece* dev_pieces = nullptr;
+  int status = RDX_OK;
+  auto layout = [&](Arena& a) {
+    plan = OutPlan();
+    dev_staged = a.take<unsigned char>(staged.size());
+    dev_pieces = a.take<rdx::RdxPiece>(spans.size());
+    for (int k = 0; k < nc; k++)
+      outs[k] = wanted[k] ? stage_out(ctx, a, reinterpret_cast<unsigned char*>(channels[k]),
+                                      f.count * (uint64_t)f.channels[k].element_bytes, 1, plan, &status)
+                          : nullptr;
+  };
+  Arena dry(nullptr);
+  layout(dry);
+  if (status != RDX_OK) return status;
+  s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  layout(a);
+  if (status != RDX_OK) return status;
+  std::vector<rdx::RdxPiece> pieces;
+  uint32_t max_count = 0;
+  for (const rdx::RdxSpan& sp : spans) {
+    pieces.push_back({sp.src, outs[sp.channel] + sp.start * (uint64_t)sp.bytes, sp.count, sp.bytes});
+    max_count = std::max(max_count, sp.count);
+  }
+  if (!staged.empty())
+    RDX_CUDA(cudaMemcpyAsync(dev_staged, staged.data(), staged.size(), cudaMemcpyHostToDevice, ctx->stream), "RDX copy");
+  if (!pieces.empty())
+    RDX_CUDA(cudaMemcpyAsync(dev_pieces, pieces.data(), pieces.size() * sizeof(rdx::RdxPiece), cudaMemcpyHostToDevice,
+                             ctx->stream),
+             "RDX pieces");
+  {
+    Phase decoding(ctx, RDX_PHASE_PROJECT);
+    RDX_CUDA(rdx::launch_untranspose(dev_pieces, (int)pieces.size(), max_count, dev_staged, ctx->stream),
+             "RDX transpose launch");
+    if (!pieces.empty()) ctx->launches += (uint64_t)((pieces.size() + 65534) / 65535);
+  }
+  s = copy_back(ctx, plan);
+  if (s != RDX_OK) return s;
+  return finish(ctx);
+}
+
 int rdx_frame_batched(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx_params* params, int sort_bits,
                       const rdx_outputs* out, uint32_t* ordering, uint32_t* visible) {
   if (!ctx) return RDX_ERR_ARG;

@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
 #include <utility>
+#include <vector>
 
 #include "../../include/radix_b200.h"
 
@@ -230,6 +232,44 @@ const char* spz_header(const unsigned char* bytes, uint64_t nbytes, SpzDesc* d);
 const char* spz_unpack(const unsigned char* bytes, uint64_t nbytes, const SpzDesc& d, unsigned char* payload);
 cudaError_t launch_decode_spz(const SpzDesc& d, float* centers, float* log_scales, float* quats, float* opacities,
                               float* colors, cudaStream_t stream);
+
+// ---- RDX files (src/core/rdx.ts): serialized ArrayData bundles ----
+
+struct RdxChannel {
+  std::string bundle, label, format;
+  int element_bytes;
+};
+struct RdxFile {
+  uint64_t count = 0;
+  uint64_t chunk_size = 0;
+  uint64_t header_bytes = 0;  // where chunk 0 starts
+  std::vector<RdxChannel> channels;   // payload order
+  std::vector<uint64_t> chunk_bytes;
+  std::string header_json;
+};
+// One chunk's channel inflated on the host: its transposed bytes at `src` of the staged buffer
+struct RdxSpan {
+  uint64_t src;
+  int channel;
+  uint64_t start;
+  uint32_t count;
+  uint32_t bytes;
+};
+// The same on the device: where its elements go
+struct RdxPiece {
+  uint64_t src;
+  unsigned char* dst;
+  uint32_t count;
+  uint32_t bytes;
+};
+// An RDX file's header from host bytes: null, or the reference's error text
+const char* rdxfile_header(const unsigned char* bytes, uint64_t nbytes, RdxFile* f);
+// Every chunk's payloads of the wanted channels inflated into `staged`: null or an error text
+const char* rdxfile_unpack(const unsigned char* bytes, uint64_t nbytes, const RdxFile& f, const bool* wanted,
+                           std::vector<unsigned char>* staged, std::vector<RdxSpan>* spans);
+// The staged bytes transposed back into the pieces' destinations (one launch per 65535 pieces)
+cudaError_t launch_untranspose(const RdxPiece* pieces_dev, int n_pieces, uint32_t max_count, const unsigned char* staged,
+                               cudaStream_t stream);
 
 // One persistent launch over every descriptor of one table kind (descs in device memory)
 // ---- PLY files (src/core/ply.ts) to raw tables ----

@@ -1,0 +1,400 @@
+// RDX files (src/core/rdx.ts): the serialized bundles of an ArrayData in
+// chunks of rows. Every piece is a container - u32 magic, u32 metaLength,
+// u32 payloadCount, u32 0, JSON meta, u32 payloadSize[payloadCount], the
+// payloads, each section 16-byte aligned. The header piece ("RDXH") names the
+// bundles, their channels and formats, in payload order; each chunk ("RDXC")
+// holds { start, count } and, per channel, that channel's elements gzipped
+// with their bytes transposed (byte b of every element together).
+//
+// The host parses the JSON and inflates the payloads (DEFLATE is sequential);
+// the device transposes the bytes back, every chunk and channel in one launch,
+// into the caller's channel arrays.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include <zlib.h>
+
+#include <algorithm>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "rdx_internal.h"
+
+namespace rdx {
+namespace {
+
+constexpr uint32_t kHeaderMagic = 0x48584452u;  // "RDXH"
+constexpr uint32_t kChunkMagic = 0x43584452u;   // "RDXC"
+constexpr int kRdxVersion = 1;
+
+char g_error[256];
+
+const char* error_text(const char* fmt, const char* a = "", const char* b = "", uint64_t x = 0, uint64_t y = 0) {
+  snprintf(g_error, sizeof(g_error), fmt, a, b, (unsigned long long)x, (unsigned long long)y);
+  return g_error;
+}
+
+uint32_t le32(const unsigned char* p) { return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24); }
+uint64_t align16(uint64_t n) { return (n + 15) & ~(uint64_t)15; }
+
+// ---- a small JSON reader: objects keep their key order ----
+
+struct Json {
+  enum Kind { kNull, kBool, kNum, kStr, kArr, kObj } kind = kNull;
+  bool b = false;
+  double num = 0.0;
+  std::string str;
+  std::vector<Json> arr;
+  std::vector<std::pair<std::string, Json>> obj;
+  const Json* get(const char* key) const {
+    if (kind != kObj) return nullptr;
+    for (const auto& kv : obj)
+      if (kv.first == key) return &kv.second;
+    return nullptr;
+  }
+};
+
+struct JsonReader {
+  const char* p;
+  const char* end;
+  int depth = 0;
+  void ws() {
+    while (p < end && (*p == ' ' || *p == '\t' || *p == '\n' || *p == '\r')) p++;
+  }
+  bool lit(const char* s) {
+    const size_t n = strlen(s);
+    if ((size_t)(end - p) < n || memcmp(p, s, n) != 0) return false;
+    p += n;
+    return true;
+  }
+  static void utf8(std::string& out, uint32_t c) {
+    if (c < 0x80) {
+      out += (char)c;
+    } else if (c < 0x800) {
+      out += (char)(0xC0 | (c >> 6));
+      out += (char)(0x80 | (c & 0x3F));
+    } else if (c < 0x10000) {
+      out += (char)(0xE0 | (c >> 12));
+      out += (char)(0x80 | ((c >> 6) & 0x3F));
+      out += (char)(0x80 | (c & 0x3F));
+    } else {
+      out += (char)(0xF0 | (c >> 18));
+      out += (char)(0x80 | ((c >> 12) & 0x3F));
+      out += (char)(0x80 | ((c >> 6) & 0x3F));
+      out += (char)(0x80 | (c & 0x3F));
+    }
+  }
+  bool hex4(uint32_t* v) {
+    if (end - p < 4) return false;
+    *v = 0;
+    for (int i = 0; i < 4; i++) {
+      const char c = *p++;
+      *v <<= 4;
+      if (c >= '0' && c <= '9') *v |= (uint32_t)(c - '0');
+      else if (c >= 'a' && c <= 'f') *v |= (uint32_t)(c - 'a' + 10);
+      else if (c >= 'A' && c <= 'F') *v |= (uint32_t)(c - 'A' + 10);
+      else return false;
+    }
+    return true;
+  }
+  bool string(std::string& out) {
+    if (p >= end || *p != '"') return false;
+    p++;
+    while (p < end && *p != '"') {
+      if (*p == '\\') {
+        if (++p >= end) return false;
+        const char e = *p++;
+        switch (e) {
+          case '"': out += '"'; break;
+          case '\\': out += '\\'; break;
+          case '/': out += '/'; break;
+          case 'b': out += '\b'; break;
+          case 'f': out += '\f'; break;
+          case 'n': out += '\n'; break;
+          case 'r': out += '\r'; break;
+          case 't': out += '\t'; break;
+          case 'u': {
+            uint32_t c;
+            if (!hex4(&c)) return false;
+            if (c >= 0xD800 && c < 0xDC00 && end - p >= 6 && p[0] == '\\' && p[1] == 'u') {
+              p += 2;
+              uint32_t lo;
+              if (!hex4(&lo)) return false;
+              c = 0x10000 + ((c - 0xD800) << 10) + (lo - 0xDC00);
+            }
+            utf8(out, c);
+            break;
+          }
+          default: return false;
+        }
+      } else {
+        out += *p++;
+      }
+    }
+    if (p >= end) return false;
+    p++;
+    return true;
+  }
+  bool value(Json& v) {
+    if (++depth > 64) return false;
+    ws();
+    if (p >= end) return false;
+    bool ok = true;
+    if (*p == '{') {
+      p++;
+      v.kind = Json::kObj;
+      ws();
+      if (p < end && *p == '}') {
+        p++;
+      } else {
+        while (ok) {
+          ws();
+          std::string key;
+          if (!string(key)) return false;
+          ws();
+          if (p >= end || *p++ != ':') return false;
+          v.obj.emplace_back(std::move(key), Json());
+          if (!value(v.obj.back().second)) return false;
+          ws();
+          if (p < end && *p == ',') {
+            p++;
+            continue;
+          }
+          if (p < end && *p == '}') {
+            p++;
+            break;
+          }
+          return false;
+        }
+      }
+    } else if (*p == '[') {
+      p++;
+      v.kind = Json::kArr;
+      ws();
+      if (p < end && *p == ']') {
+        p++;
+      } else {
+        while (true) {
+          v.arr.emplace_back();
+          if (!value(v.arr.back())) return false;
+          ws();
+          if (p < end && *p == ',') {
+            p++;
+            continue;
+          }
+          if (p < end && *p == ']') {
+            p++;
+            break;
+          }
+          return false;
+        }
+      }
+    } else if (*p == '"') {
+      v.kind = Json::kStr;
+      ok = string(v.str);
+    } else if (lit("true")) {
+      v.kind = Json::kBool;
+      v.b = true;
+    } else if (lit("false")) {
+      v.kind = Json::kBool;
+    } else if (lit("null")) {
+      v.kind = Json::kNull;
+    } else {
+      char* stop = nullptr;
+      std::string tok(p, (size_t)std::min<ptrdiff_t>(end - p, 64));
+      v.num = strtod(tok.c_str(), &stop);
+      if (stop == tok.c_str()) return false;
+      v.kind = Json::kNum;
+      p += stop - tok.c_str();
+    }
+    depth--;
+    return ok;
+  }
+};
+
+bool parse_json(const unsigned char* s, uint64_t n, Json* out) {
+  JsonReader r{reinterpret_cast<const char*>(s), reinterpret_cast<const char*>(s) + n};
+  if (!r.value(*out)) return false;
+  r.ws();
+  return r.p == r.end;
+}
+
+// Bytes of one element of an ArrayFormats name ("uint32x4", "float16", ...): 0 if invalid
+int element_bytes(const std::string& f) {
+  static const std::pair<const char*, int> kScalars[] = {{"uint8", 1},  {"sint8", 1},  {"unorm8", 1},  {"snorm8", 1},
+                                                         {"uint16", 2}, {"sint16", 2}, {"float16", 2}, {"uint32", 4},
+                                                         {"sint32", 4}, {"float32", 4}};
+  const size_t x = f.find('x');
+  const std::string scalar = f.substr(0, x);
+  int components = 1;
+  if (x != std::string::npos) {
+    const std::string c = f.substr(x + 1);
+    if (c.empty() || c.size() > 6 || c.find_first_not_of("0123456789") != std::string::npos) return 0;
+    components = atoi(c.c_str());
+    if (components < 1) return 0;
+  }
+  for (const auto& s : kScalars)
+    if (scalar == s.first) return s.second * components;
+  return 0;
+}
+
+// A container: its meta JSON and payload spans (offsets into `bytes`)
+const char* read_container(const unsigned char* bytes, uint64_t n, uint32_t magic, Json* meta,
+                           std::vector<std::pair<uint64_t, uint64_t>>* payloads, uint64_t* length) {
+  if (n < 16 || le32(bytes) != magic) return "Not an RDX piece of the expected type";
+  const uint64_t meta_len = le32(bytes + 4), count = le32(bytes + 8);
+  const uint64_t sizes_at = 16 + align16(meta_len);
+  if (16 + meta_len > n || sizes_at + count * 4 > n) return "RDX file ended unexpectedly";
+  if (!parse_json(bytes + 16, meta_len, meta)) return "RDX piece with malformed JSON meta";
+  uint64_t at = sizes_at + align16(count * 4);
+  payloads->clear();
+  for (uint64_t i = 0; i < count; i++) {
+    const uint64_t size = le32(bytes + sizes_at + i * 4);
+    if (at + size > n) return "RDX file ended unexpectedly";
+    payloads->emplace_back(at, size);
+    at += align16(size);
+  }
+  *length = at;
+  return nullptr;
+}
+
+uint64_t as_u64(const Json* v) { return v && v->kind == Json::kNum && v->num >= 0 ? (uint64_t)v->num : 0; }
+
+// Inflate one gzip payload completely: the bytes, or -1 on a bad stream
+int64_t gunzip_all(const unsigned char* in, uint64_t n, std::vector<unsigned char>* out) {
+  z_stream zs;
+  memset(&zs, 0, sizeof(zs));
+  if (inflateInit2(&zs, 16 + MAX_WBITS) != Z_OK) return -1;
+  out->clear();
+  unsigned char buf[1 << 16];
+  zs.next_in = const_cast<unsigned char*>(in);
+  zs.avail_in = (uInt)n;
+  int status = Z_OK;
+  while (status == Z_OK) {
+    zs.next_out = buf;
+    zs.avail_out = sizeof(buf);
+    status = inflate(&zs, Z_NO_FLUSH);
+    if (status != Z_OK && status != Z_STREAM_END) break;
+    out->insert(out->end(), buf, buf + (sizeof(buf) - zs.avail_out));
+    if (status == Z_OK && zs.avail_in == 0 && zs.avail_out != 0) {
+      status = Z_BUF_ERROR;
+      break;
+    }
+  }
+  inflateEnd(&zs);
+  return status == Z_STREAM_END ? (int64_t)out->size() : -1;
+}
+
+// ---- device: bytes transposed back ----
+
+constexpr int kTransposeThreads = 256;
+
+// Element i's byte b sits at src[b * count + i]: blockIdx.y picks the piece
+__global__ void __launch_bounds__(kTransposeThreads) k_untranspose(const RdxPiece* __restrict__ pieces,
+                                                                   const unsigned char* __restrict__ staged) {
+  const RdxPiece pc = pieces[blockIdx.y];
+  const unsigned char* src = staged + pc.src;
+  for (uint32_t i = blockIdx.x * kTransposeThreads + threadIdx.x; i < pc.count; i += gridDim.x * kTransposeThreads) {
+    unsigned char* d = pc.dst + (uint64_t)i * pc.bytes;
+    if (pc.bytes == 16 && (reinterpret_cast<uintptr_t>(d) & 15u) == 0) {
+      uint32_t w[4];
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        w[k] = (uint32_t)src[(uint64_t)(4 * k) * pc.count + i] | ((uint32_t)src[(uint64_t)(4 * k + 1) * pc.count + i] << 8) |
+               ((uint32_t)src[(uint64_t)(4 * k + 2) * pc.count + i] << 16) |
+               ((uint32_t)src[(uint64_t)(4 * k + 3) * pc.count + i] << 24);
+      }
+      *reinterpret_cast<uint4*>(d) = make_uint4(w[0], w[1], w[2], w[3]);
+    } else {
+      for (uint32_t b = 0; b < pc.bytes; b++) d[b] = src[(uint64_t)b * pc.count + i];
+    }
+  }
+}
+
+}  // namespace
+
+const char* rdxfile_header(const unsigned char* bytes, uint64_t nbytes, RdxFile* f) {
+  *f = RdxFile();
+  if (!bytes || nbytes < 16 || le32(bytes) != kHeaderMagic) return "Not an RDX piece of the expected type";
+  Json meta;
+  std::vector<std::pair<uint64_t, uint64_t>> payloads;
+  uint64_t length = 0;
+  const char* err = read_container(bytes, nbytes, kHeaderMagic, &meta, &payloads, &length);
+  if (err) return err;
+  f->header_bytes = length;
+  f->header_json.assign(reinterpret_cast<const char*>(bytes) + 16, le32(bytes + 4));
+  const Json* version = meta.get("version");
+  if (!version || version->kind != Json::kNum || version->num != kRdxVersion)
+    return error_text("RDX version %s is not 1", version && version->kind == Json::kNum ? std::to_string((long long)version->num).c_str() : "undefined");
+  f->count = as_u64(meta.get("count"));
+  f->chunk_size = as_u64(meta.get("chunkSize"));
+  const Json* bundles = meta.get("bundles");
+  if (!bundles || bundles->kind != Json::kObj) return "RDX header without bundles";
+  for (const auto& b : bundles->obj) {
+    const Json* def = b.second.get("def");
+    const Json* channels = def ? def->get("channels") : nullptr;
+    if (!channels || channels->kind != Json::kObj) return error_text("RDX bundle %s without channels", b.first.c_str());
+    for (const auto& c : channels->obj) {
+      if (c.second.kind != Json::kStr) return error_text("RDX channel %s.%s without a format", b.first.c_str(), c.first.c_str());
+      const int eb = element_bytes(c.second.str);
+      if (eb == 0) return error_text("Invalid array format \"%s\"", c.second.str.c_str());
+      f->channels.push_back({b.first, c.first, c.second.str, eb});
+    }
+  }
+  const Json* chunks = meta.get("chunks");
+  if (!chunks || chunks->kind != Json::kArr) return "RDX header without chunks";
+  uint64_t total = length;
+  for (const Json& c : chunks->arr) {
+    f->chunk_bytes.push_back(as_u64(&c));
+    total += f->chunk_bytes.back();
+  }
+  if (total > nbytes) return "RDX file ended unexpectedly";
+  return nullptr;
+}
+
+const char* rdxfile_unpack(const unsigned char* bytes, uint64_t nbytes, const RdxFile& f, const bool* wanted,
+                           std::vector<unsigned char>* staged, std::vector<RdxSpan>* spans) {
+  (void)nbytes;  // rdxfile_header checked that every chunk lies inside the file
+  staged->clear();
+  spans->clear();
+  uint64_t at = f.header_bytes;
+  std::vector<unsigned char> buf;
+  for (size_t ci = 0; ci < f.chunk_bytes.size(); ci++) {
+    Json meta;
+    std::vector<std::pair<uint64_t, uint64_t>> payloads;
+    uint64_t length = 0;
+    const char* err = read_container(bytes + at, f.chunk_bytes[ci], kChunkMagic, &meta, &payloads, &length);
+    if (err) return err;
+    const uint64_t start = as_u64(meta.get("start")), count = as_u64(meta.get("count"));
+    if (start + count > f.count) return error_text("RDX chunk at %s%s%llu runs past the %llu elements", "", "", start, f.count);
+    if (payloads.size() != f.channels.size())
+      return error_text("RDX chunk %s%s%llu holds %llu payloads", "", "", (uint64_t)ci, (uint64_t)payloads.size());
+    for (size_t k = 0; k < f.channels.size(); k++) {
+      const RdxChannel& ch = f.channels[k];
+      if (gunzip_all(bytes + at + payloads[k].first, payloads[k].second, &buf) < 0) return "RDX payload is not a gzip stream";
+      if (buf.size() != count * (uint64_t)ch.element_bytes)
+        return error_text("Chunk at %s: %s holds %llu bytes, expected %llu", std::to_string(start).c_str(),
+                          (ch.bundle + "." + ch.label).c_str(), (uint64_t)buf.size(), count * (uint64_t)ch.element_bytes);
+      if (!wanted[k] || count == 0) continue;
+      spans->push_back({staged->size(), (int)k, start, (uint32_t)count, (uint32_t)ch.element_bytes});
+      staged->insert(staged->end(), buf.begin(), buf.end());
+    }
+    at += f.chunk_bytes[ci];
+  }
+  return nullptr;
+}
+
+cudaError_t launch_untranspose(const RdxPiece* pieces_dev, int n_pieces, uint32_t max_count, const unsigned char* staged,
+                               cudaStream_t stream) {
+  if (n_pieces == 0 || max_count == 0) return cudaSuccess;
+  const uint32_t gx = std::min<uint32_t>((max_count + kTransposeThreads - 1) / kTransposeThreads, 1024u);
+  for (int first = 0; first < n_pieces; first += 65535) {
+    const int batch = std::min(n_pieces - first, 65535);
+    k_untranspose<<<dim3(gx, (unsigned)batch), kTransposeThreads, 0, stream>>>(pieces_dev + first, staged);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace rdx
