@@ -745,14 +745,17 @@ def _words(t):
     return t.view(_torch().int32).reshape(t.shape[0], -1)
 
 
-def rdxfile_table(data, device="cuda", ctx=None):
+def rdxfile_table(data, device="cuda", ctx=None, palette=None):
     """A Table over an RDX file's splats: its extSplats, covSplats or
     packedSplats bundle (src/core/splats.ts:69-77; packedSplats' meta.encoding)
-    and its per-splat SH bundle ("extSh" or "packedSh", meta {codec, degree},
-    src/core/sh.ts:230-240), decoded on the GPU. Returns (table, channels)."""
+    and its SH: a per-splat bundle ("extSh" or "packedSh", meta {codec,
+    degree}, src/core/sh.ts:230-240), or labels (bundle shLabel) into the
+    ShPalette that `palette` (the palette's own RDX file) holds (bundle
+    shPalette, meta {codec, degree, size, stride}, src/core/sh.ts:426-470).
+    Decoded on the GPU. Returns (table, channels)."""
     info, ch = decode_rdxfile(data, device, ctx)
     bundles = info["header"]["bundles"]
-    sh, deg, codec = (), 0, "ext"
+    sh, deg, codec, pal = (), 0, "ext", None
     for name in ("extSh", "packedSh"):
         if name in ch:
             meta = bundles[name].get("meta", {})
@@ -760,15 +763,27 @@ def rdxfile_table(data, device="cuda", ctx=None):
             deg = int(meta.get("degree", 0))
             sh = [_words(t) for t in ch[name].values()]
             break
+    if palette is not None:
+        if "shLabel" not in ch:
+            raise RadixError(_abi.RDX_ERR_ARG, "a palette was given but the RDX file has no shLabel bundle")
+        pinfo, pch = decode_rdxfile(palette, device, ctx)
+        if "shPalette" not in pch or "shEntries" not in pch["shPalette"]:
+            raise RadixError(_abi.RDX_ERR_ARG, "Not an SH palette: no shPalette.shEntries channel")
+        meta = pinfo["header"]["bundles"]["shPalette"].get("meta", {})
+        codec, deg = meta.get("codec", "ext"), int(meta.get("degree", 0))
+        labels = ch["shLabel"]["label"].view(_torch().int16).reshape(-1)
+        pal = (_words(pch["shPalette"]["shEntries"]), labels, int(meta["stride"]))
+        ch["shPalette"] = pch["shPalette"]
+    kw = {"palette": pal} if pal is not None else {}
     if "extSplats" in ch:
-        t = Table.ext(_words(ch["extSplats"]["extA"]), _words(ch["extSplats"]["extB"]), sh, deg, codec)
+        t = Table.ext(_words(ch["extSplats"]["extA"]), _words(ch["extSplats"]["extB"]), sh, deg, codec, **kw)
     elif "covSplats" in ch:
-        t = Table.cov(_words(ch["covSplats"]["covA"]), _words(ch["covSplats"]["covB"]), sh, deg, codec)
+        t = Table.cov(_words(ch["covSplats"]["covA"]), _words(ch["covSplats"]["covB"]), sh, deg, codec, **kw)
     elif "packedSplats" in ch:
         e = dict(zip(("rgbMin", "rgbMax", "lnScaleMin", "lnScaleMax"), Table.PACKED_ENCODING))
         e.update(bundles["packedSplats"].get("meta", {}).get("encoding", {}))
         enc = (e["rgbMin"], e["rgbMax"], e["lnScaleMin"], e["lnScaleMax"])
-        t = Table.packed(_words(ch["packedSplats"]["packed"]), enc, sh, deg, codec)
+        t = Table.packed(_words(ch["packedSplats"]["packed"]), enc, sh, deg, codec, **kw)
     else:
         raise RadixError(_abi.RDX_ERR_ARG, "the RDX file has no extSplats, covSplats or packedSplats bundle")
     return t, ch

@@ -116,3 +116,30 @@ def test_decoded_file_drawn_by_a_frame(ctx):
     expected, visible = orc.sort(o["keys"], n, 32)
     assert res["visible"] == visible
     np.testing.assert_array_equal(u32(res["ordering"])[:n], expected[:n])
+
+
+@pytest.mark.parametrize("codec", ["ext", "packed"])
+def test_palette_files(ctx, codec):
+    """Splats with an shLabel bundle and their ShPalette in its own RDX file."""
+    d = syn.mixture_table(60_000, seed=12, sh_degree=3)
+    n, deg = d["centers"].shape[0], 3
+    words = orc.encode_sh(d, codec)
+    size = 211
+    stride = 1 << (words.shape[1] // 4 - 1).bit_length()
+    labels = (np.arange(n) * 7 % size).astype(np.uint16)
+    entries = orc.sh_palette(np.ascontiguousarray(words[:size]), stride)
+    a, b = orc.encode_ext(d)[:2]
+    splats = rf.rdx_file({"extSplats": ({"extA": "uint32x4", "extB": "uint32x4"}, {}, {"extA": a, "extB": b}),
+                          "shLabel": ({"label": "uint16"}, {}, {"label": labels})}, n, 65536)
+    pal = rf.rdx_file({"shPalette": ({"shEntries": "uint32x4"},
+                                     {"codec": codec, "degree": deg, "size": size, "stride": stride},
+                                     {"shEntries": entries})}, entries.shape[0], 4096)
+    table, _ = rb.rdxfile_table(splats, palette=pal)
+    ref_table = rb.Table.ext(a, b, (), deg, codec, palette=(entries, labels, stride))
+    cam = syn.scale_camera()
+    gpu = rb.project_collection([rb.SplatObject(table)], cam, None, 32, cull_keys=True, outputs=ALL)
+    ref = orc.project([rb.SplatObject(ref_table)], cam, None, 32, True)
+    r = compare_projection(gpu, ref)
+    assert r["drawn"] > 0 and r["cull_disagreements"] == 0 and r["key_mismatches"] == 0, r
+    for name, e in r["errors"].items():
+        assert e < TOLERANCE, (name, e, r)
