@@ -190,6 +190,9 @@ bool valid_bits(int bits) { return bits == 16 || bits == 24 || bits == 32; }
 
 uint32_t tiles_of(uint64_t n) { return (uint32_t)((n + rdx::kSortTile - 1) / rdx::kSortTile); }
 
+// Lookback tiles a pass of a sort of max_tiles 4096-key tiles may use (small sorts: 1024-key tiles)
+size_t lookback_tiles(uint32_t max_tiles) { return std::max(max_tiles, rdx::sort_small_pass_tiles(max_tiles)); }
+
 // Sort scratch for `segments` segments of `total` keys
 rdx::SortScratch take_sort_scratch(Arena& a, int segments, int passes, uint64_t total) {
   rdx::SortScratch s{};
@@ -688,7 +691,7 @@ int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uin
              const SegBufs& sb, int segments, uint32_t max_tiles, int bits, const rdx::SortScratch& sc,
              bool zeroed) {
   const int passes = bits / 8;
-  int st = ensure_lookback(ctx, (size_t)passes * max_tiles * rdx::kRadix);
+  int st = ensure_lookback(ctx, (size_t)passes * lookback_tiles(max_tiles) * rdx::kRadix);
   if (st != RDX_OK) return st;
   rdx::SortCall c{};
   c.keys_in = keys_in;
@@ -700,6 +703,7 @@ int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uin
   c.zeroed = zeroed;
   c.scratch = sc;
   c.lookback = ctx->lookback;
+  c.lookback_words = ctx->lookback_words;
   c.epoch = ctx->error_flag + 1;
   c.error_flag = ctx->error_flag;
   int launches = 0;
@@ -802,7 +806,7 @@ int rdx_ctx_reserve(rdx_ctx* ctx, uint64_t max_keys) {
   take_segs(a, 1);
   a.take<uint32_t>(max_keys * 3);  // keys / staged buffers of a frame or splat sort
   int st = ensure_arena(ctx, a.used);
-  return st != RDX_OK ? st : ensure_lookback(ctx, (size_t)4 * tiles_of(max_keys) * rdx::kRadix);
+  return st != RDX_OK ? st : ensure_lookback(ctx, (size_t)4 * lookback_tiles(tiles_of(max_keys)) * rdx::kRadix);
 }
 
 int rdx_ctx_set_profiling(rdx_ctx* ctx, int on) {
@@ -1135,6 +1139,7 @@ struct FrameDev {
   uint32_t* ord = nullptr;
   uint32_t* vis = nullptr;         // [views]
   uint64_t* lookback = nullptr;
+  uint64_t lookback_words = 0;
   uint32_t* error_flag = nullptr;  // word 0: the error flag, word 1: the lookback epoch
 };
 
@@ -1174,6 +1179,7 @@ cudaError_t enqueue_frame(rdx_ctx* timing, const ProjectCall& call, const FrameD
     c.zeroed = true;  // zeroed before the projection, so the projection and the sort's kernels run back to back
     c.scratch = fd.sc;
     c.lookback = fd.lookback;
+    c.lookback_words = fd.lookback_words;
     c.epoch = fd.error_flag + 1;
     c.error_flag = fd.error_flag;
     int n_launch = 0;
@@ -1279,7 +1285,7 @@ int frame_common(rdx_ctx* ctx, const ViewRef* views, int n_views, const rdx_para
   }
   if (status != RDX_OK) return status;
   if (sort && n > 0) {
-    s = ensure_lookback(ctx, (size_t)passes * segment_tiles(call, nullptr) * rdx::kRadix);
+    s = ensure_lookback(ctx, (size_t)passes * lookback_tiles(segment_tiles(call, nullptr)) * rdx::kRadix);
     if (s != RDX_OK) return s;
     s = upload_segments(ctx, call, fd.sb);
     if (s != RDX_OK) return s;
@@ -1289,6 +1295,7 @@ int frame_common(rdx_ctx* ctx, const ViewRef* views, int n_views, const rdx_para
     if (s != RDX_OK) return s;
   }
   fd.lookback = ctx->lookback;
+  fd.lookback_words = ctx->lookback_words;
   fd.error_flag = ctx->error_flag;
   RDX_CUDA(enqueue_frame(ctx, call, fd, sort_bits, sort, ctx->stream, &ctx->launches), "frame launch");
   if (sort && visible) {
@@ -1760,7 +1767,7 @@ int rdx_batch_create(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx
   };
   if (status != RDX_OK) return bail(status);
   const uint32_t max_tiles = segment_tiles(b->call, nullptr);
-  const size_t lookback_words = (size_t)passes * max_tiles * rdx::kRadix;
+  const size_t lookback_words = (size_t)passes * lookback_tiles(max_tiles) * rdx::kRadix;
   const size_t ndesc = b->call.descs.size();
   if (cudaMalloc(&b->arena, dry.used + 256) != cudaSuccess || cudaMalloc(&b->lookback, lookback_words * 8) != cudaSuccess ||
       cudaMalloc(&b->words, 8) != cudaSuccess || cudaMallocHost(&b->error_host, 4) != cudaSuccess ||
@@ -1774,6 +1781,7 @@ int rdx_batch_create(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx
   layout(a);
   if (status != RDX_OK) return bail(status);
   b->fd.lookback = b->lookback;
+  b->fd.lookback_words = lookback_words;
   b->fd.error_flag = b->words;
   // descriptors and segments stay in the batch's memory; the graph only reads them
   std::vector<uint32_t> tiles;

@@ -146,6 +146,7 @@ extern "C" int rdx_sort_noalloc(const uint32_t* keys, uint64_t count, int bits, 
   c.zeroed = false;  // the sort zeroes its small state itself
   c.scratch = sc;
   c.lookback = reinterpret_cast<uint64_t*>(b + kLookbackOff);
+  c.lookback_words = kLookbackBytes / 8;
   c.epoch = epoch;
   c.error_flag = flag;
   if (sort_segments(c, s, nullptr) != cudaSuccess) return RDX_ERR_CUDA;

@@ -47,6 +47,10 @@ constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per onesweep tile
+// Sorts of at most kSmallSortTiles such tiles run their digit passes in tiles of
+// kSortThreads * kSmallItems keys (when their lookback words allow)
+constexpr int kSmallItems = 4;
+constexpr uint32_t kSmallSortTiles = 256;
 constexpr int kRadix = 256;
 constexpr int kMaxPasses = 4;
 // Lookback words: a 2-bit flag over a 30-bit count, so a segment holds < 2^30 keys
@@ -83,6 +87,9 @@ struct SortScratch {
 
 // hist, valid, ref_hidden, counters and tile_valid are contiguous: words zeroed before a sort
 size_t sort_small_state_words(int segments, int passes, uint32_t max_tiles);
+// The digit passes' tile count of a small sort (0: not small); lookback words
+// for passes * max(this, max_tiles) * kRadix let a sort use small tiles
+uint32_t sort_small_pass_tiles(uint32_t max_tiles);
 
 // Sort segments of keys_in (values: vals_in, or each key's index within its
 // segment when vals_in is null) into keys_out / vals_out (keys_out may be null:
@@ -104,6 +111,7 @@ struct SortCall {
   bool no_drop;     // rank the largest key like the others
   SortScratch scratch;
   uint64_t* lookback;
+  uint64_t lookback_words;  // its capacity
   uint32_t* epoch;
   uint32_t* error_flag;
 };

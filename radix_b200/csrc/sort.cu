@@ -223,7 +223,8 @@ struct PartArgs {
   uint32_t* counter;
   uint64_t* vbegin;            // out (block 0): the valid keys' segments for the digit passes
   uint64_t* vend;
-  uint32_t* vtiles;
+  uint32_t* vtiles;            // in tiles of pass_tile keys
+  uint32_t pass_tile;
 };
 
 constexpr int kPartBlocksPerSm = 8;
@@ -248,7 +249,7 @@ __global__ void __launch_bounds__(kSortThreads, kPartBlocksPerSm) k_partition(Pa
       a.vbegin[s] = b;
       a.vend[s] = b + v;
       a.vtiles[s] = t;
-      t += (uint32_t)((v + kSortTile - 1) / kSortTile);
+      t += (uint32_t)((v + a.pass_tile - 1) / a.pass_tile);
     }
     a.vtiles[a.segs.count] = t;
   }
@@ -343,11 +344,12 @@ struct PassArgs {
   uint32_t* error_flag;
 };
 
-template <bool FIRST, bool WRITE_KEYS>
+template <bool FIRST, bool WRITE_KEYS, int ITEMS>
 __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(PassArgs a) {
+  constexpr int TILE = kSortThreads * ITEMS;
   __shared__ uint32_t s_whist[kSortWarps][kRadix];
-  __shared__ uint32_t s_exchange[kSortTile];
-  __shared__ uint32_t s_vals[kSortTile];  // the tile's values, copied in asynchronously
+  __shared__ uint32_t s_exchange[TILE];
+  __shared__ uint32_t s_vals[TILE];  // the tile's values, copied in asynchronously
   __shared__ uint32_t s_tile_start[kRadix];
   __shared__ uint32_t s_dest[kRadix];
   __shared__ uint64_t s_sums[kSortWarps];
@@ -371,18 +373,18 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   const uint32_t local_tile = tile - a.segs.tiles[seg];
   const uint64_t seg_begin = a.segs.begin[seg];
   const uint64_t seg_end = a.segs.end[seg];
-  const uint64_t base = seg_begin + (uint64_t)local_tile * kSortTile;
-  const uint32_t n = (uint32_t)min((uint64_t)kSortTile, seg_end - base);
+  const uint64_t base = seg_begin + (uint64_t)local_tile * TILE;
+  const uint32_t n = (uint32_t)min((uint64_t)TILE, seg_end - base);
 
   // Load: warp w holds tile positions [w * 512, (w + 1) * 512), item j at j * 32 + lane.
   // Keys go to registers; values go straight to shared memory (cp.async, no
   // registers held) and are waited for only before they are scattered. In the
   // first pass without values, a value is the key's index within its segment.
   const bool gen_vals = FIRST && a.vals_in == nullptr;
-  uint32_t key[kSortItems], rank[kSortItems];
-  const uint32_t warp_base = (uint32_t)warp * (kSortItems * 32);
+  uint32_t key[ITEMS], rank[ITEMS];
+  const uint32_t warp_base = (uint32_t)warp * (ITEMS * 32);
 #pragma unroll
-  for (int j = 0; j < kSortItems; j++) {
+  for (int j = 0; j < ITEMS; j++) {
     const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
     if (pos < n) {
       key[j] = __ldg(&a.keys_in[base + pos]) & a.key_mask;
@@ -403,7 +405,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   // Rank the keys: items in position order, equal digits counted by their lowest lane
   const uint32_t lt = lanemask_lt();
 #pragma unroll
-  for (int j = 0; j < kSortItems; j++) {
+  for (int j = 0; j < ITEMS; j++) {
     const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
     const bool ranked = pos < n;
     const uint32_t d = ranked ? (key[j] >> a.shift) & 0xffu : kNotRanked;
@@ -471,7 +473,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
 
   // Local sort of the tile's keys in shared memory
 #pragma unroll
-  for (int j = 0; j < kSortItems; j++) {
+  for (int j = 0; j < ITEMS; j++) {
     const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
     if (pos < n) {
       const uint32_t dj = (key[j] >> a.shift) & 0xffu;
@@ -483,9 +485,9 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   }
   __syncthreads();
   // Destinations stay inside the segment even if a bounded wait gave up
-  uint32_t dest[kSortItems];
+  uint32_t dest[ITEMS];
 #pragma unroll
-  for (int k = 0; k < kSortItems; k++) {
+  for (int k = 0; k < ITEMS; k++) {
     const uint32_t i = (uint32_t)k * kSortThreads + tid;
     dest[k] = 0xffffffffu;
     if (i < tile_count) {
@@ -499,18 +501,22 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   }
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < kSortItems; j++) {
+  for (int j = 0; j < ITEMS; j++) {
     if (rank[j] != 0xffffffffu) s_exchange[rank[j]] = value_at(warp_base + (uint32_t)j * 32 + lane);
   }
   __syncthreads();
 #pragma unroll
-  for (int k = 0; k < kSortItems; k++) {
+  for (int k = 0; k < ITEMS; k++) {
     const uint32_t i = (uint32_t)k * kSortThreads + tid;
     if (dest[k] != 0xffffffffu) a.vals_out[dest[k]] = s_exchange[i];
   }
 }
 
 }  // namespace
+
+uint32_t sort_small_pass_tiles(uint32_t max_tiles) {
+  return max_tiles <= kSmallSortTiles ? max_tiles * (uint32_t)(kSortItems / kSmallItems) : 0u;
+}
 
 size_t sort_small_state_words(int segments, int passes, uint32_t max_tiles) {
   // hist [S][passes][256], valid [S], ref_hidden [S], counters [passes + 1], tile_valid [max_tiles]
@@ -550,8 +556,14 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
   }
   if (err != cudaSuccess) return err;
   n_launch++;
+  // Small sorts after a partition take their digit passes in 1024-key tiles: a
+  // pass's time is then one short tile's chain (its tile count at most four times
+  // the 4096-key count), when the lookback words hold the extra tiles
+  const uint32_t small_tiles = sort_small_pass_tiles(c.segs.max_tiles);
+  const bool small = drop && small_tiles != 0 && (uint64_t)passes * small_tiles * kRadix <= c.lookback_words;
+  const uint32_t pass_tiles = small ? small_tiles : c.segs.max_tiles;
   // Without the partition every key is valid: the digit passes use the segments as given
-  SortSegments vsegs = drop ? SortSegments{sc.vbegin, sc.vend, sc.vtiles, c.segs.count, c.segs.max_tiles} : c.segs;
+  SortSegments vsegs = drop ? SortSegments{sc.vbegin, sc.vend, sc.vtiles, c.segs.count, pass_tiles} : c.segs;
 
   PassArgs a{};
   a.key_mask = mask;
@@ -578,6 +590,7 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     p.vbegin = sc.vbegin;
     p.vend = sc.vend;
     p.vtiles = sc.vtiles;
+    p.pass_tile = small ? (uint32_t)(kSortThreads * kSmallItems) : (uint32_t)kSortTile;
     err = launch_after(k_partition, c.segs.max_tiles, kSortThreads, 0, stream, p);
     if (err != cudaSuccess) return err;
     n_launch++;
@@ -595,13 +608,14 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     a.shift = 8 * place;
     a.segs = vsegs;
     a.place = place;
-    a.lookback = c.lookback + (size_t)place * c.segs.max_tiles * kRadix;
+    a.lookback = c.lookback + (size_t)place * pass_tiles * kRadix;
     a.counter = sc.counters + place;
     const bool first = place == 0 && !drop;
-    void (*kernel)(PassArgs) = first                             ? k_onesweep<true, true>
-                               : (last && a.keys_out == nullptr) ? k_onesweep<false, false>
-                                                                 : k_onesweep<false, true>;
-    err = launch_after(kernel, c.segs.max_tiles, kSortThreads, 0, stream, a);
+    void (*kernel)(PassArgs) =
+        first ? k_onesweep<true, true, kSortItems>
+              : (last && a.keys_out == nullptr) ? (small ? k_onesweep<false, false, kSmallItems> : k_onesweep<false, false, kSortItems>)
+                                                : (small ? k_onesweep<false, true, kSmallItems> : k_onesweep<false, true, kSortItems>);
+    err = launch_after(kernel, pass_tiles, kSortThreads, 0, stream, a);
     if (err != cudaSuccess) return err;
     n_launch++;
     ki = a.keys_out;
