@@ -94,10 +94,12 @@ __device__ __forceinline__ double colour_value(const void* colors, uint64_t i, i
   }
 }
 
-// The gradient of row i of an object (drawn: the eyes whose forward drew it, not 0)
+// The gradient of row i of an object (drawn: the eyes whose forward drew it,
+// not 0). col: the row's colour values (base rgb, then the SH coefficients),
+// staged in shared memory; the row's colour gradient replaces them there.
 template <int DEG, int CDT, int EYES>
 __device__ __forceinline__ void splat_backward(const ProjDesc& sd, const GradsOut& go_, const GradsIn& in, uint64_t i,
-                                               uint32_t drawn) {
+                                               uint32_t drawn, float* col) {
   constexpr int K = Coeffs<DEG>::value;
   constexpr int kRow = (1 + K) * 3;
   const uint64_t gi = sd.out_offset + i;
@@ -316,12 +318,9 @@ __device__ __forceinline__ void splat_backward(const ProjDesc& sd, const GradsOu
   }
 
   // colour: rgb = max(base + SH, 0) with SH (GpuShReader.apply), the base alone without
-  float* gcol = go_.colors ? go_.colors + i * kRow : nullptr;
   if constexpr (K == 0) {
-    if (gcol) {
 #pragma unroll
-      for (int c = 0; c < 3; c++) gcol[c] = (float)g_rgb[c];
-    }
+    for (int c = 0; c < 3; c++) col[c] = (float)g_rgb[c];
   } else {
     const int cap = min(p.max_sh_degree, DEG);
     const int kc = cap <= 0 ? 0 : (cap == 1 ? 3 : (cap == 2 ? 8 : (cap == 3 ? 15 : 24)));
@@ -338,15 +337,15 @@ __device__ __forceinline__ void splat_backward(const ProjDesc& sd, const GradsOu
       for (int k = 0; k < K; k++) {
         if (k < kc) {
 #pragma unroll
-          for (int c = 0; c < 3; c++) sh[c] = fma(colour_value<DEG, CDT>(tb.colors, i, 3 + k * 3 + c), Y[k], sh[c]);
+          for (int c = 0; c < 3; c++) sh[c] = fma((double)col[3 + k * 3 + c], Y[k], sh[c]);
         }
       }
     }
     double gm[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      gm[c] = colour_value<DEG, CDT>(tb.colors, i, c) + sh[c] > 0.0 ? g_rgb[c] : 0.0;
-      if (gcol) gcol[c] = (float)gm[c];
+      gm[c] = (double)col[c] + sh[c] > 0.0 ? g_rgb[c] : 0.0;
+      col[c] = (float)gm[c];
     }
     double g_dir[3] = {0.0, 0.0, 0.0};
 #pragma unroll
@@ -354,9 +353,10 @@ __device__ __forceinline__ void splat_backward(const ProjDesc& sd, const GradsOu
       const bool used = dir_ok && k < kc;
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        if (gcol) gcol[3 + k * 3 + c] = used ? (float)(gm[c] * Y[k]) : 0.0f;
+        const double value = (double)col[3 + k * 3 + c];  // read before the gradient takes its place
+        col[3 + k * 3 + c] = used ? (float)(gm[c] * Y[k]) : 0.0f;
         if (used) {
-          const double ck = gm[c] * colour_value<DEG, CDT>(tb.colors, i, 3 + k * 3 + c);
+          const double ck = gm[c] * value;
           g_dir[0] += ck * G[k][0];
           g_dir[1] += ck * G[k][1];
           g_dir[2] += ck * G[k][2];
@@ -393,8 +393,10 @@ __global__ void __launch_bounds__(kBwdThreads, kBwdBlocksPerSm) k_project_backwa
                                                                   const GradsOut* __restrict__ grads, int n_desc,
                                                                   uint32_t total_chunks, GradsIn in) {
   constexpr int kRow = (1 + Coeffs<DEG>::value) * 3;
+  constexpr int kPitch = kRow | 1;  // odd: a lane reading its own row hits its own banks
   __shared__ uint32_t s_row[kBwdWarps][kBwdQueue];
   __shared__ uint8_t s_drawn[kBwdWarps][kBwdQueue];
+  __shared__ float s_col[kBwdWarps][32][kPitch];  // a batch's colour rows, then their gradients
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t gw = blockIdx.x * kBwdWarps + (uint32_t)warp, nw = gridDim.x * kBwdWarps;
   int cur = -1, di = -1;
@@ -420,10 +422,39 @@ __global__ void __launch_bounds__(kBwdThreads, kBwdBlocksPerSm) k_project_backwa
     // one site for the gradient: full batches, the rest before the object changes and at the end
     const uint32_t nb = queued >= 32 ? 32u : ((!have || di != cur) ? queued : 0u);
     if (nb) {
-      if ((uint32_t)lane < nb) {
-        const uint32_t q = (head + (uint32_t)lane) & (kBwdQueue - 1);
-        splat_backward<DEG, CDT, EYES>(descs[cur], grads[cur], in, s_row[warp][q], s_drawn[warp][q]);
+      // the batch's colour rows in by the whole warp (coalesced), the gradients out the same way
+      const uint32_t q = (head + (uint32_t)lane) & (kBwdQueue - 1);
+      const uint32_t my_row = (uint32_t)lane < nb ? s_row[warp][q] : 0u;
+      const void* colors = descs[cur].table.colors;
+      if constexpr (CDT == RDX_DTYPE_F16) {
+#pragma unroll 8
+        for (uint32_t r = 0; r < nb; r++) {
+          const uint64_t row = __shfl_sync(0xffffffffu, my_row, (int)r);
+          for (int e = lane; e < kRow; e += 32) s_col[warp][r][e] = (float)colour_value<DEG, CDT>(colors, row, e);
+        }
+      } else {
+        // float32 rows copied asynchronously: every row's loads in flight at once
+        for (uint32_t r = 0; r < nb; r++) {
+          const uint64_t row = __shfl_sync(0xffffffffu, my_row, (int)r);
+          const float* src = reinterpret_cast<const float*>(colors) + row * kRow;
+          for (int e = lane; e < kRow; e += 32)
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(&s_col[warp][r][e])),
+                         "l"(src + e)
+                         : "memory");
+        }
+        asm volatile("cp.async.commit_group;\n\tcp.async.wait_all;" ::: "memory");
       }
+      __syncwarp();
+      if ((uint32_t)lane < nb) splat_backward<DEG, CDT, EYES>(descs[cur], grads[cur], in, my_row, s_drawn[warp][q], s_col[warp][lane]);
+      __syncwarp();
+      float* gcol = grads[cur].colors;
+      if (gcol) {
+        for (uint32_t r = 0; r < nb; r++) {
+          const uint64_t row = __shfl_sync(0xffffffffu, my_row, (int)r);
+          for (int e = lane; e < kRow; e += 32) gcol[row * kRow + e] = s_col[warp][r][e];
+        }
+      }
+      __syncwarp();
       head = (head + nb) & (kBwdQueue - 1);
       queued -= nb;
       __syncwarp();
@@ -446,10 +477,16 @@ __global__ void __launch_bounds__(kBwdThreads, kBwdBlocksPerSm) k_project_backwa
         if (go_.log_scales) go_.log_scales[i * 3] = go_.log_scales[i * 3 + 1] = go_.log_scales[i * 3 + 2] = 0.0f;
         if (go_.quats) reinterpret_cast<float4*>(go_.quats)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
         if (go_.opacities) go_.opacities[i] = 0.0f;
-        if (go_.colors) {
-#pragma unroll
-          for (int c = 0; c < kRow; c++) go_.colors[i * kRow + c] = 0.0f;
-        }
+      }
+    }
+    // colour rows of the undrawn live rows zeroed by the whole warp (coalesced)
+    if (float* gcol = grads[cur].colors) {
+      uint32_t undrawn = __ballot_sync(0xffffffffu, live && !drawn);
+      const uint64_t i0 = (uint64_t)(chunk - sd.first_tile) * kProjTile;
+      while (undrawn) {
+        const int r = __ffs(undrawn) - 1;
+        undrawn &= undrawn - 1u;
+        for (int e = lane; e < kRow; e += 32) gcol[(i0 + (uint64_t)r) * kRow + e] = 0.0f;
       }
     }
     const uint32_t ballot = __ballot_sync(0xffffffffu, drawn != 0u);
