@@ -1,11 +1,12 @@
 // Stable LSD radix sort of uint32 keys with uint32 values for sm_100a: a
-// histogram of every digit place in one read of the keys (or supplied by the
-// projection that wrote the keys), then one onesweep kernel per 8-bit digit
-// place. Each onesweep tile ranks its keys with warp match-based multisplit in
-// shared memory, publishes its digit counts and finds its global offsets by
-// decoupled lookback (single pass, no separate scan kernel), then scatters
-// keys and values through shared memory so writes of one digit run are
-// contiguous.
+// counting kernel reads the keys once (every digit place's histogram, valid
+// keys per tile and per segment), then one onesweep kernel per 8-bit digit
+// place. Each onesweep tile ranks its keys with a warp multisplit (one ballot
+// per digit bit) in shared memory, publishes its digit counts and finds its
+// global offsets by decoupled lookback (single pass, no separate scan
+// kernel), then scatters keys and values through shared memory so writes of
+// one digit run are contiguous. Kernels after the first start by programmatic
+// dependent launch.
 //
 // The largest key of a width (2^bits - 1, the invalid key of SortKeys) sorts
 // after every other key, its copies in input order. When outputs do not alias
@@ -329,12 +330,12 @@ __global__ void __launch_bounds__(kSortThreads, kPartBlocksPerSm) k_partition(Pa
 
 struct PassArgs {
   const uint32_t* keys_in;
-  const uint32_t* vals_in;   // null in the first pass: each key's index within its segment
+  const uint32_t* vals_in;   // null (first pass of an in-place sort): each key's index within its segment
   uint32_t* keys_out;        // null: values only
   uint32_t* vals_out;
   uint32_t key_mask;
   int shift;
-  SortSegments segs;         // full segments (first pass) or the valid keys' segments
+  SortSegments segs;         // the valid keys' segments (after a partition) or the segments as given
   const uint32_t* hist;      // [S][passes][256] of the keys sorted
   int passes;
   int place;
