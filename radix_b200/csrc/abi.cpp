@@ -1153,17 +1153,16 @@ cudaError_t enqueue_frame(rdx_ctx* timing, const ProjectCall& call, const FrameD
   const int passes = bits / 8;
   const bool sorting = sort && call.n > 0;
   cudaError_t e;
-  if (sorting) {
-    e = cudaMemsetAsync(fd.sc.hist, 0, rdx::sort_small_state_words(views, passes, segment_tiles(call, nullptr)) * 4,
-                        stream);
-    if (e != cudaSuccess) return e;
-  }
   {
     Phase projecting(timing, RDX_PHASE_PROJECT);
     for (size_t g = 0; g + 1 < call.groups.size(); g++) {
       const int start = call.groups[g];
       const int count = call.groups[g + 1] - start;
-      e = rdx::launch_project(fd.descs + start, call.descs.data() + start, count, call.group_tiles[g], fd.out,
+      // the first launch zeroes the sort's small state (hist, counts, counters)
+      rdx::ProjOutputs out = fd.out;
+      out.zero = sorting && g == 0 ? fd.sc.hist : nullptr;
+      out.zero_words = out.zero ? rdx::sort_small_state_words(views, passes, segment_tiles(call, nullptr)) : 0;
+      e = rdx::launch_project(fd.descs + start, call.descs.data() + start, count, call.group_tiles[g], out,
                               fd.error_flag, stream);
       if (e != cudaSuccess) return e;
       if (call.group_tiles[g]) *launches += 1;
@@ -1216,15 +1215,6 @@ int check_views(rdx_ctx* ctx, const ViewRef* views, int n_views, int sort_bits, 
 }
 
 // Segment descriptors of the views' keys, uploaded through the ring
-int upload_segments(rdx_ctx* ctx, const ProjectCall& call, const SegBufs& sb) {
-  std::vector<uint32_t> tiles;
-  segment_tiles(call, &tiles);
-  const size_t v = call.seg_begin.size();
-  int st = upload(ctx, sb.begin, call.seg_begin.data(), v * 8);
-  if (st == RDX_OK) st = upload(ctx, sb.end, call.seg_end.data(), v * 8);
-  return st != RDX_OK ? st : upload(ctx, sb.tiles, tiles.data(), (v + 1) * 4);
-}
-
 int frame_common(rdx_ctx* ctx, const ViewRef* views, int n_views, const rdx_params* params, int sort_bits, int pass,
                  int cull_keys, const rdx_outputs* out, uint32_t* ordering, uint32_t* visible, bool sort) {
   if (!ctx) return RDX_ERR_ARG;
@@ -1247,12 +1237,22 @@ int frame_common(rdx_ctx* ctx, const ViewRef* views, int n_views, const rdx_para
   ProjectCall call;
   OutPlan plan;
   FrameDev fd;
+  // Descriptors and segment tables share one block, uploaded in one copy:
+  // descs | begin [views] | end [views] | tiles [views + 1], each 256-aligned
+  const auto align256 = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  size_t off_begin = 0, off_end = 0, off_tiles = 0, block_bytes = 0;
+  char* block = nullptr;
   auto layout = [&](Arena& a) {
     call = ProjectCall();
     plan = OutPlan();
     fd = FrameDev();
     status = plan_views(ctx, a, views, n_views, prm, sort_bits, pass, cull_keys, call);
-    fd.descs = a.take<rdx::ProjDesc>(call.descs.size());
+    off_begin = align256(call.descs.size() * sizeof(rdx::ProjDesc));
+    off_end = off_begin + align256((size_t)n_views * 8);
+    off_tiles = off_end + align256((size_t)n_views * 8);
+    block_bytes = sort ? off_tiles + ((size_t)n_views + 1) * 4 : off_begin;
+    block = a.take<char>(block_bytes);
+    fd.descs = reinterpret_cast<rdx::ProjDesc*>(block);
     rdx::ProjOutputs& d = plan.dev;
     if (pass == RDX_PASS_FULL) {
       d.mean2d = stage_out(ctx, a, o->mean2d, E * n * 8, 8, plan, &status);
@@ -1268,7 +1268,8 @@ int frame_common(rdx_ctx* ctx, const ViewRef* views, int n_views, const rdx_para
       if (!d.keys) d.keys = a.take<uint32_t>(n);
       fd.ord = host_order ? a.take<uint32_t>(n) : ordering;
       fd.vis = a.take<uint32_t>((size_t)n_views);
-      fd.sb = take_segs(a, n_views);
+      fd.sb = SegBufs{reinterpret_cast<uint64_t*>(block + off_begin), reinterpret_cast<uint64_t*>(block + off_end),
+                      reinterpret_cast<uint32_t*>(block + off_tiles)};
       fd.sc = take_sort_scratch(a, n_views, passes, n);
     }
     fd.out = d;
@@ -1287,11 +1288,18 @@ int frame_common(rdx_ctx* ctx, const ViewRef* views, int n_views, const rdx_para
   if (sort && n > 0) {
     s = ensure_lookback(ctx, (size_t)passes * lookback_tiles(segment_tiles(call, nullptr)) * rdx::kRadix);
     if (s != RDX_OK) return s;
-    s = upload_segments(ctx, call, fd.sb);
-    if (s != RDX_OK) return s;
   }
-  if (!call.descs.empty()) {
-    s = upload(ctx, fd.descs, call.descs.data(), call.descs.size() * sizeof(rdx::ProjDesc));
+  if (block_bytes && (!call.descs.empty() || (sort && n > 0))) {
+    std::vector<char> host(block_bytes, 0);
+    memcpy(host.data(), call.descs.data(), call.descs.size() * sizeof(rdx::ProjDesc));
+    if (sort) {
+      std::vector<uint32_t> tiles;
+      segment_tiles(call, &tiles);
+      memcpy(host.data() + off_begin, call.seg_begin.data(), (size_t)n_views * 8);
+      memcpy(host.data() + off_end, call.seg_end.data(), (size_t)n_views * 8);
+      memcpy(host.data() + off_tiles, tiles.data(), ((size_t)n_views + 1) * 4);
+    }
+    s = upload(ctx, block, host.data(), block_bytes);
     if (s != RDX_OK) return s;
   }
   fd.lookback = ctx->lookback;

@@ -402,6 +402,9 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
   const uint32_t lt = (1u << lane) - 1u;
 
   pdl_trigger();  // the sort's first kernel may be placed now; it waits for this grid to complete
+  if (blockIdx.x == 0 && out.zero) {
+    for (uint64_t w = threadIdx.x; w < out.zero_words; w += blockDim.x) out.zero[w] = 0u;
+  }
 
   int cur_desc = -1;
   uint32_t head = 0, queued = 0;

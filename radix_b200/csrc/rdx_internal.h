@@ -206,6 +206,10 @@ struct ProjOutputs {
   float* radii;
   uint32_t* words;
   uint32_t* keys;
+  // Words the launch's first block zeroes (the sort's small state, so that no
+  // memset separates the projection from the sort's kernels); may be null
+  uint32_t* zero;
+  uint64_t zero_words;
 };
 
 // Splats per projection chunk (one warp)
