@@ -142,3 +142,15 @@ def test_sort_large_random_32bit(ctx):
     expected, exp_visible = orc.sort(keys, n, 32)
     assert visible == exp_visible
     np.testing.assert_array_equal(u32(got)[:n], expected[:n])
+
+
+@pytest.mark.parametrize("n", [256 * 4096, 256 * 4096 + 1])
+def test_sort_keys_sort_at_the_small_tile_threshold(ctx, n):
+    """Up to 256 tiles of 4096 keys the digit passes run in 1024-key tiles; one
+    key more and they do not: both orders equal the oracle's."""
+    keys = random_keys(n, 32, 11)
+    keys[::3] = rb.SortKeys.invalid(32)
+    got, visible = rb.SortKeys.sort(to_cuda(keys.view(np.int32)), n, 32, ctx=ctx)
+    expected, exp_visible = orc.sort(keys, n, 32)
+    assert visible == exp_visible
+    np.testing.assert_array_equal(u32(got)[:n], expected[:n])
