@@ -143,3 +143,21 @@ def test_palette_files(ctx, codec):
     assert r["drawn"] > 0 and r["cull_disagreements"] == 0 and r["key_mismatches"] == 0, r
     for name, e in r["errors"].items():
         assert e < TOLERANCE, (name, e, r)
+
+
+def test_header_json_of_every_kind(ctx):
+    """The header's JSON reader: nested objects and arrays, numbers with
+    exponents, booleans, null, escapes and surrogate pairs, key order kept."""
+    meta = {"scene": "café \U0001F600 \"quoted\" \\ / \t", "list": [1, -2.5e3, 0.125, True, False, None],
+            "nested": {"z": {"y": []}, "a": {}}}
+    # names that reach the library's own reader escaped: a BMP character, a surrogate pair, a quote
+    bundle, label = "b\u00e9\u2603", 'x"\U0001F600'
+    raw = rf.rdx_file({bundle: ({label: "uint16x2"}, {"k": [1, {"m": "☃"}]},
+                                {label: np.arange(8, dtype=np.uint16).reshape(4, 2)})}, 4, 4096, meta=meta)
+    assert b"\\u2603" in raw and b"\\ud83d\\ude00" in raw and b'x\\"' in raw
+    info = rb.rdxfile_info(raw)
+    assert info["header"]["meta"] == meta
+    assert list(info["header"]["meta"]["nested"].keys()) == ["z", "a"]
+    assert info["channels"] == [(bundle, label, "uint16x2", 4)]
+    _, ch = rb.decode_rdxfile(raw)
+    np.testing.assert_array_equal(host(ch[bundle][label]).view(np.uint16).reshape(4, 2), np.arange(8).reshape(4, 2))
