@@ -23,7 +23,7 @@ namespace rdx {
 namespace {
 
 constexpr int kBwdThreads = 128;
-constexpr int kBwdBlocksPerSm = 3;  // up to 168 registers a thread
+constexpr int kBwdBlocksPerSm = 4;  // 128 registers a thread (some spills: faster than 3 blocks of 168)
 
 template <int DEG>
 struct Coeffs {
