@@ -29,7 +29,7 @@ constexpr uint32_t kHeaderMagic = 0x48584452u;  // "RDXH"
 constexpr uint32_t kChunkMagic = 0x43584452u;   // "RDXC"
 constexpr int kRdxVersion = 1;
 
-char g_error[256];
+thread_local char g_error[256];  // the last error text of this thread
 
 const char* error_text(const char* fmt, const char* a = "", const char* b = "", uint64_t x = 0, uint64_t y = 0) {
   snprintf(g_error, sizeof(g_error), fmt, a, b, (unsigned long long)x, (unsigned long long)y);

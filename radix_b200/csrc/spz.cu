@@ -32,7 +32,7 @@ constexpr int Z_STREAM_END_FINAL = 100;  // the last gzip member ended (not a zl
 
 __host__ __device__ __forceinline__ uint32_t le32(const unsigned char* p) { return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24); }
 
-char g_error[160];  // the last error text (each call that fails rewrites it)
+thread_local char g_error[160];  // the last error text of this thread (each call that fails rewrites it)
 
 const char* error_text(const char* fmt, uint64_t a = 0, uint64_t b = 0) {
   snprintf(g_error, sizeof(g_error), fmt, (unsigned long long)a, (unsigned long long)b);
