@@ -215,7 +215,7 @@ int rdx_version(void);
  * for the stream and returns, per phase, the summed milliseconds and the number
  * of timed runs since the last read, then clears them.
  */
-#define RDX_PHASE_PROJECT 0 /* the fused projection kernel(s) */
+#define RDX_PHASE_PROJECT 0 /* the fused projection kernel(s); the gradient and file decode kernels */
 #define RDX_PHASE_SORT 1    /* histogram + onesweep passes (+ compaction) */
 #define RDX_PHASE_COPY_IN 2 /* host -> device staging */
 #define RDX_PHASE_COPY_OUT 3

@@ -1452,10 +1452,22 @@ int rdx_project_backward(rdx_ctx* ctx, const rdx_object* objects, int n_objects,
 // The header of a PLY file (host or device bytes) into desc
 static int read_ply_header(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx::PlyDesc* d) {
   if (!bytes || nbytes == 0) return fail(ctx, RDX_ERR_ARG, "Invalid PLY header");
-  const size_t head = (size_t)std::min<uint64_t>(nbytes, 64 * 1024);  // HEADER_MAX_BYTES (ply.ts:16)
+  size_t head = (size_t)std::min<uint64_t>(nbytes, 64 * 1024);  // HEADER_MAX_BYTES (ply.ts:16)
   std::vector<unsigned char> buf(head);
   if (is_device_ptr(bytes)) {
+    // headers are mostly short: the first 4 KB, and the rest of the 64 KB only
+    // when those hold no end_header line (the parser reads up to the first one)
+    const size_t all = head;
+    head = std::min<size_t>(all, 4096);
     RDX_CUDA(cudaMemcpy(buf.data(), bytes, head, cudaMemcpyDeviceToHost), "PLY header copy");
+    const std::string first(reinterpret_cast<const char*>(buf.data()), head);
+    if (head < all && first.find("end_header\n") == std::string::npos &&
+        first.find("end_header\r\n") == std::string::npos) {
+      RDX_CUDA(cudaMemcpy(buf.data() + head, static_cast<const char*>(bytes) + head, all - head,
+                          cudaMemcpyDeviceToHost),
+               "PLY header copy");
+      head = all;
+    }
   } else {
     memcpy(buf.data(), bytes, head);
   }

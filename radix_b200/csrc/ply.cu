@@ -11,6 +11,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -72,33 +73,22 @@ __device__ __forceinline__ double compressed_sh(uint32_t byte) {
   return ((byte == 0u ? 0.0 : (byte == 255u ? 1.0 : ((double)byte + 0.5) / 256.0)) - 0.5) * 8.0;
 }
 
-// STAGED: the block's vertex records are first copied into shared memory
-// with coalesced word loads, then each thread parses its record there
-template <bool STAGED>
+// SplatMath.normalizeQuat (math.ts:12-27)
+__device__ __forceinline__ void normalize_quat(double q[4]) {
+  const double len = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  if (len > 0.0) {
+    for (int k = 0; k < 4; k++) q[k] /= len;
+  } else {
+    q[0] = q[1] = q[2] = 0.0;
+    q[3] = 1.0;
+  }
+}
+
+// Any file, one thread per splat reading its record in place (compressed
+// files, and records too long to stage)
 __global__ void k_decode_ply(const PlyDesc d, float* __restrict__ centers, float* __restrict__ log_scales,
                              float* __restrict__ quats, float* __restrict__ opacities, float* __restrict__ colors) {
-  extern __shared__ __align__(16) unsigned char s_raw[];
-  const uint64_t r0 = (uint64_t)blockIdx.x * blockDim.x;
-  const uint64_t i = r0 + threadIdx.x;
-  const unsigned char* staged = nullptr;
-  if constexpr (STAGED) {
-    // s[x] holds byte x of the block's records; the copy's words are aligned
-    // in both memories (the buffer starts at the source's offset mod 4)
-    const uint64_t rows = min((uint64_t)blockDim.x, d.count - r0);
-    const unsigned char* src = d.vertex + r0 * d.record;
-    const uint64_t len = rows * d.record;
-    const uint32_t off = (uint32_t)((uintptr_t)src & 3u);
-    unsigned char* buf = s_raw + off;
-    const uint64_t head = min((uint64_t)((4u - off) & 3u), len);
-    const uint64_t words = (len - head) / 4;
-    for (uint64_t b = threadIdx.x; b < head; b += blockDim.x) buf[b] = src[b];
-    const uint32_t* sw = reinterpret_cast<const uint32_t*>(src + head);
-    uint32_t* dw = reinterpret_cast<uint32_t*>(buf + head);
-    for (uint64_t w = threadIdx.x; w < words; w += blockDim.x) dw[w] = __ldg(sw + w);
-    for (uint64_t b = head + words * 4 + threadIdx.x; b < len; b += blockDim.x) buf[b] = src[b];
-    __syncthreads();
-    staged = buf;
-  }
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= d.count) return;
   const bool little = d.little != 0;
   const int kvals = (d.out_degree == 0 ? 0 : (d.out_degree == 1 ? 3 : (d.out_degree == 2 ? 8 : (d.out_degree == 3 ? 15 : 24)))) * 3;
@@ -141,7 +131,7 @@ __global__ void k_decode_ply(const PlyDesc d, float* __restrict__ centers, float
       for (int x = 0; x < kvals; x++) col[3 + x] = s ? (float)compressed_sh(s[d.sh_byte[x]]) : 0.0f;
     }
   } else {
-    const unsigned char* v = STAGED ? staged + (i - r0) * d.record : d.vertex + i * d.record;
+    const unsigned char* v = d.vertex + i * d.record;
     for (int k = 0; k < 3; k++) c[k] = read_value(v, d.xyz[k], little, false);
     if (d.kind == kPlyStandard) {
       for (int k = 0; k < 3; k++) ls[k] = read_value(v, d.scale[k], little, false);
@@ -165,14 +155,7 @@ __global__ void k_decode_ply(const PlyDesc d, float* __restrict__ centers, float
         for (int x = 0; x < kvals; x++) col[3 + x] = 0.0f;
     }
   }
-  // SplatMath.normalizeQuat (math.ts:12-27)
-  const double len = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
-  if (len > 0.0) {
-    for (int k = 0; k < 4; k++) q[k] /= len;
-  } else {
-    q[0] = q[1] = q[2] = 0.0;
-    q[3] = 1.0;
-  }
+  normalize_quat(q);
   if (centers)
     for (int k = 0; k < 3; k++) centers[i * 3 + k] = (float)c[k];
   if (log_scales)
@@ -181,6 +164,189 @@ __global__ void k_decode_ply(const PlyDesc d, float* __restrict__ centers, float
   if (opacities) opacities[i] = (float)op;
   if (col)
     for (int k = 0; k < 3; k++) col[k] = (float)rgb[k];
+}
+
+constexpr int kRowsThreads = 128;  // 4 warps, each staging 32 records
+constexpr uint32_t kRowsMaxRecord = 1024;  // 32 KB of shared memory a warp at most
+
+// One value of a staged record: a float32 word when every property the
+// decode reads is an aligned little-endian float32 (WORDS), else bytes
+__device__ __forceinline__ double staged_value(const uint32_t* sw, uint32_t base, PlyProp p, bool words, bool little,
+                                               bool normalized) {
+  if (words) return (double)__uint_as_float(sw[(base + (uint32_t)p.offset) >> 2]);
+  return read_value(reinterpret_cast<const unsigned char*>(sw) + base, p, little, normalized);
+}
+
+// An SH value as written: the float32 word itself, or the float32 of any other type
+__device__ __forceinline__ float staged_float(const uint32_t* sw, uint32_t base, PlyProp p, bool words, bool little) {
+  if (words) return __uint_as_float(sw[(base + (uint32_t)p.offset) >> 2]);
+  return (float)read_value(reinterpret_cast<const unsigned char*>(sw) + base, p, little, false);
+}
+
+// Shared-memory row pitch (floats) of the colour rows: rows of a multiple of 4
+// floats are written as 16-byte vectors, an odd number of vectors apart (the 8
+// lanes of each store phase then fill distinct banks); other rows an odd
+// number of floats apart
+template <int ROW>
+__host__ __device__ constexpr int row_pitch() {
+  return ROW % 4 == 0 ? ((ROW / 4) % 2 == 1 ? ROW : ROW + 4) : (ROW | 1);
+}
+
+// Standard files and RGB point clouds, one warp per 32 records: the warp
+// copies its records into shared memory with coalesced aligned word loads
+// (funnel-shifted when the records start off a word boundary), each lane
+// decodes one splat from there, and the colour rows (ROW floats a splat) go
+// back through the same shared memory so that the warp writes its 32 rows as
+// one contiguous span (16-byte stores when VEC: rows of a multiple of 4
+// floats and 16-byte aligned colours). `region` is the words of shared memory
+// each warp owns, a multiple of 4: at least 32 records and 32 rows of
+// row_pitch<ROW>() words.
+template <int ROW>
+__global__ void __launch_bounds__(kRowsThreads) k_decode_ply_rows(const PlyDesc d, uint32_t region, bool words,
+                                                                  bool vec, float* __restrict__ centers,
+                                                                  float* __restrict__ log_scales,
+                                                                  float* __restrict__ quats,
+                                                                  float* __restrict__ opacities,
+                                                                  float* __restrict__ colors) {
+  extern __shared__ __align__(16) uint32_t s_words[];
+  constexpr int kPitch = row_pitch<ROW>();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint64_t r0 = ((uint64_t)blockIdx.x * (kRowsThreads / 32) + (uint64_t)warp) * 32;
+  if (r0 >= d.count) return;  // the whole warp
+  const uint32_t rows = (uint32_t)min((uint64_t)32, d.count - r0);
+  uint32_t* sw = s_words + (size_t)warp * region;
+
+  // the records' bytes [0, len) into sw; every source word read holds at least one of them
+  const unsigned char* src = d.vertex + r0 * d.record;
+  const uint32_t len = rows * d.record;
+  const uint32_t shift = (uint32_t)((uintptr_t)src & 3u);
+  const uint32_t* aw = reinterpret_cast<const uint32_t*>(src - shift);
+  const uint32_t n_out = (len + 3) / 4, n_in = (len + shift + 3) / 4;
+  // kCopyBatch loads in flight per lane before their stores
+  constexpr uint32_t kCopyBatch = 16;
+  for (uint32_t j0 = lane; j0 < n_out; j0 += 32 * kCopyBatch) {
+    uint32_t lo[kCopyBatch], hi[kCopyBatch];
+#pragma unroll
+    for (uint32_t b = 0; b < kCopyBatch; b++) {
+      const uint32_t j = j0 + 32 * b;
+      lo[b] = j < n_out ? __ldg(aw + j) : 0u;
+      hi[b] = shift != 0 && j + 1 < n_in ? __ldg(aw + j + 1) : 0u;
+    }
+#pragma unroll
+    for (uint32_t b = 0; b < kCopyBatch; b++) {
+      const uint32_t j = j0 + 32 * b;
+      if (j < n_out) sw[j] = shift == 0 ? lo[b] : __funnelshift_r(lo[b], hi[b], 8 * shift);
+    }
+  }
+  __syncwarp();
+
+  const bool live = (uint32_t)lane < rows;
+  const uint64_t i = r0 + (uint64_t)lane;
+  const bool little = d.little != 0;
+  const uint32_t base = (uint32_t)lane * d.record;
+  constexpr int kVals = ROW - 3;
+  double c[3], ls[3], q[4], op, rgb[3];
+  float cv[ROW];
+  if (live) {
+    for (int k = 0; k < 3; k++) c[k] = staged_value(sw, base, d.xyz[k], words, little, false);
+    if (d.kind == kPlyStandard) {
+      for (int k = 0; k < 3; k++) ls[k] = staged_value(sw, base, d.scale[k], words, little, false);
+      // (rot_1, rot_2, rot_3, rot_0) = (x, y, z, w)
+      q[0] = staged_value(sw, base, d.rot[1], words, little, false);
+      q[1] = staged_value(sw, base, d.rot[2], words, little, false);
+      q[2] = staged_value(sw, base, d.rot[3], words, little, false);
+      q[3] = staged_value(sw, base, d.rot[0], words, little, false);
+      op = 1.0 / (1.0 + exp(-staged_value(sw, base, d.opacity, words, little, false)));
+      for (int k = 0; k < 3; k++) rgb[k] = 0.5 + kShC0 * staged_value(sw, base, d.color[k], words, little, false);
+#pragma unroll
+      for (int x = 0; x < kVals; x++) cv[3 + x] = staged_float(sw, base, d.rest[x], words, little);
+    } else {
+      const double point = log(0.001);  // POINT_SCALE (ply.ts:18)
+      ls[0] = ls[1] = ls[2] = point;
+      q[0] = q[1] = q[2] = 0.0;
+      q[3] = 1.0;
+      op = d.alpha.offset >= 0 ? staged_value(sw, base, d.alpha, words, little, true) : 1.0;
+      for (int k = 0; k < 3; k++) rgb[k] = staged_value(sw, base, d.color[k], words, little, true);
+#pragma unroll
+      for (int x = 0; x < kVals; x++) cv[3 + x] = 0.0f;
+    }
+    normalize_quat(q);
+    for (int k = 0; k < 3; k++) cv[k] = (float)rgb[k];
+    if (centers)
+      for (int k = 0; k < 3; k++) centers[i * 3 + k] = (float)c[k];
+    if (log_scales)
+      for (int k = 0; k < 3; k++) log_scales[i * 3 + k] = (float)ls[k];
+    if (quats) reinterpret_cast<float4*>(quats)[i] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+    if (opacities) opacities[i] = (float)op;
+  }
+  if (!colors) return;  // uniform
+  __syncwarp();  // every lane has read its record: the rows may overwrite them
+  float* srow = reinterpret_cast<float*>(sw);
+  if constexpr (ROW % 4 == 0) {
+    if (vec) {
+      constexpr int kQuads = ROW / 4;
+      if (live) {
+        float4* r4 = reinterpret_cast<float4*>(srow + lane * kPitch);
+#pragma unroll
+        for (int k = 0; k < kQuads; k++) r4[k] = make_float4(cv[4 * k], cv[4 * k + 1], cv[4 * k + 2], cv[4 * k + 3]);
+      }
+      __syncwarp();
+      const float4* s4 = reinterpret_cast<const float4*>(srow);
+      float4* d4 = reinterpret_cast<float4*>(colors + r0 * ROW);
+      const uint32_t total4 = rows * kQuads;
+      for (uint32_t j = lane; j < total4; j += 32) {
+        const uint32_t r = j / kQuads;
+        d4[j] = s4[r * (kPitch / 4) + (j - r * kQuads)];
+      }
+      return;
+    }
+  }
+  if (live) {
+#pragma unroll
+    for (int k = 0; k < ROW; k++) srow[lane * kPitch + k] = cv[k];
+  }
+  __syncwarp();
+  float* dst = colors + r0 * ROW;
+  const uint32_t total = rows * ROW;
+  for (uint32_t j = lane; j < total; j += 32) {
+    const uint32_t r = j / ROW;
+    dst[j] = srow[r * kPitch + (j - r * ROW)];
+  }
+}
+
+// Every value the staged decode reads is an aligned little-endian float32
+bool all_float_words(const PlyDesc& d) {
+  if (!d.little || d.record % 4) return false;
+  auto word = [](PlyProp p) { return p.offset < 0 || (p.type == 6 && p.offset % 4 == 0); };
+  bool ok = word(d.xyz[0]) && word(d.xyz[1]) && word(d.xyz[2]);
+  for (int k = 0; k < 3; k++) ok = ok && word(d.color[k]);
+  if (d.kind == kPlyStandard) {
+    for (int k = 0; k < 3; k++) ok = ok && word(d.scale[k]);
+    for (int k = 0; k < 4; k++) ok = ok && word(d.rot[k]);
+    ok = ok && word(d.opacity);
+    const int vals = (d.out_degree == 0 ? 0 : (d.out_degree == 1 ? 3 : (d.out_degree == 2 ? 8 : (d.out_degree == 3 ? 15 : 24)))) * 3;
+    for (int x = 0; x < vals; x++) ok = ok && word(d.rest[x]);
+  } else {
+    ok = ok && word(d.alpha);
+  }
+  return ok;
+}
+
+template <int ROW>
+cudaError_t launch_rows(const PlyDesc& d, float* centers, float* log_scales, float* quats, float* opacities,
+                        float* colors, cudaStream_t stream) {
+  const uint32_t record_words = (d.record + 3) / 4;
+  const uint32_t region = (std::max<uint32_t>(32 * record_words, 32 * row_pitch<ROW>()) + 3) & ~3u;
+  const size_t smem = (size_t)region * 4 * (kRowsThreads / 32);
+  cudaError_t e = cudaFuncSetAttribute(k_decode_ply_rows<ROW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  const uint64_t warps = (d.count + 31) / 32;
+  const uint64_t blocks = (warps + kRowsThreads / 32 - 1) / (kRowsThreads / 32);
+  const bool vec = ROW % 4 == 0 && ((uintptr_t)colors & 15u) == 0;
+  k_decode_ply_rows<ROW><<<(unsigned)blocks, kRowsThreads, smem, stream>>>(d, region, all_float_words(d), vec,
+                                                                           centers, log_scales, quats, opacities,
+                                                                           colors);
+  return cudaGetLastError();
 }
 
 // ---- the header (ply.ts:362-444) ----
@@ -217,7 +383,7 @@ const Prop* find(const Element& e, const std::string& name) {
 
 PlyProp pp(const Prop* p) { return p ? PlyProp{p->offset, p->type} : PlyProp{-1, 6}; }
 
-std::string g_error;
+thread_local std::string g_error;
 
 }  // namespace
 
@@ -412,15 +578,19 @@ const char* parse_ply_header(const unsigned char* head, uint64_t head_bytes, uin
 cudaError_t launch_decode_ply(const PlyDesc& desc, float* centers, float* log_scales, float* quats, float* opacities,
                               float* colors, cudaStream_t stream) {
   if (desc.count == 0) return cudaSuccess;
+  // standard files and point clouds: records staged a warp at a time
+  if (desc.kind != kPlyCompressed && desc.record <= kRowsMaxRecord) {
+    switch (desc.out_degree) {
+      case 0: return launch_rows<3>(desc, centers, log_scales, quats, opacities, colors, stream);
+      case 1: return launch_rows<12>(desc, centers, log_scales, quats, opacities, colors, stream);
+      case 2: return launch_rows<27>(desc, centers, log_scales, quats, opacities, colors, stream);
+      case 3: return launch_rows<48>(desc, centers, log_scales, quats, opacities, colors, stream);
+      default: return launch_rows<75>(desc, centers, log_scales, quats, opacities, colors, stream);
+    }
+  }
   const uint32_t threads = 128;
   const uint64_t blocks = (desc.count + threads - 1) / threads;
-  // standard files and point clouds: records staged through shared memory when a block's fit in 48 KB
-  const size_t smem = (size_t)threads * desc.record + 4;
-  if (desc.kind != kPlyCompressed && smem <= 48 * 1024) {
-    k_decode_ply<true><<<(unsigned)blocks, threads, smem, stream>>>(desc, centers, log_scales, quats, opacities, colors);
-  } else {
-    k_decode_ply<false><<<(unsigned)blocks, threads, 0, stream>>>(desc, centers, log_scales, quats, opacities, colors);
-  }
+  k_decode_ply<<<(unsigned)blocks, threads, 0, stream>>>(desc, centers, log_scales, quats, opacities, colors);
   return cudaGetLastError();
 }
 

@@ -10,8 +10,8 @@ import numpy as np
 SH_C0 = 0.28209479177387814
 
 
-def _header(elements, little=True):
-    lines = ["ply", f"format binary_{'little' if little else 'big'}_endian 1.0", "comment radix_b200 test fixture"]
+def _header(elements, little=True, comment="radix_b200 test fixture"):
+    lines = ["ply", f"format binary_{'little' if little else 'big'}_endian 1.0", f"comment {comment}"]
     for name, count, props in elements:
         lines.append(f"element {name} {count}")
         lines += [f"property {t} {p}" for p, t in props]
@@ -29,8 +29,9 @@ def _records(columns, little=True):
     return rec.tobytes()
 
 
-def standard_ply(d, little=True, extra_uchar=False):
-    """A standard 3DGS PLY of a raw table dict (float properties; opacity as a logit)."""
+def standard_ply(d, little=True, extra_uchar=False, comment="radix_b200 test fixture"):
+    """A standard 3DGS PLY of a raw table dict (float properties; opacity as a
+    logit); the comment's length sets where the records start."""
     n = d["centers"].shape[0]
     deg = d["sh_degree"]
     k = (deg + 1) ** 2 - 1
@@ -46,7 +47,7 @@ def standard_ply(d, little=True, extra_uchar=False):
     q = d["quats"]
     cols += [("rot_0", "f4", q[:, 3]), ("rot_1", "f4", q[:, 0]), ("rot_2", "f4", q[:, 1]), ("rot_3", "f4", q[:, 2])]
     types = {"f4": "float", "u1": "uchar"}
-    head = _header([("vertex", n, [(name, types[ch]) for name, ch, _ in cols])], little)
+    head = _header([("vertex", n, [(name, types[ch]) for name, ch, _ in cols])], little, comment)
     return head + _records(cols, little)
 
 

@@ -36,6 +36,60 @@ def test_standard_files(ctx, little):
     _check(pf.standard_ply(d, little, extra_uchar=True), sh_degree=1)
 
 
+@pytest.mark.parametrize("pad", [0, 1, 2, 3])
+def test_records_at_every_alignment(ctx, pad):
+    # a count that leaves the last warp of 32 records and the last block part-filled;
+    # the comment's length moves the records' start through the four byte offsets
+    d = syn.mixture_table(1003, seed=7, sh_degree=3)
+    raw = pf.standard_ply(d, comment="x" * pad)
+    _check(raw)
+    _check(raw, device_bytes=True)
+
+
+def test_header_longer_than_the_first_read(ctx):
+    # a device file whose header (a 6000-character comment) ends past the first 4 KB read
+    raw = pf.standard_ply(syn.mixture_table(300, seed=4, sh_degree=1), comment="c" * 6000)
+    assert raw.index(b"end_header") > 4096
+    _check(raw, device_bytes=True)
+    assert rb.ply_info(torch.from_numpy(np.frombuffer(raw, dtype=np.uint8).copy()).cuda())["count"] == 300
+
+
+@pytest.mark.parametrize("offset", [1, 2, 3])
+def test_device_bytes_off_a_word_boundary(ctx, offset):
+    raw = pf.standard_ply(syn.mixture_table(777, seed=8, sh_degree=2))
+    buf = torch.zeros(len(raw) + 8, dtype=torch.uint8, device="cuda")
+    buf[offset:offset + len(raw)] = torch.from_numpy(np.frombuffer(raw, dtype=np.uint8).copy()).cuda()
+    table, cols = rb.decode_ply(buf[offset:offset + len(raw)])
+    ref = orc.ply_decode(raw)
+    np.testing.assert_array_equal(host(cols["colors"]).reshape(ref["colors"].shape), ref["colors"].astype(np.float32))
+    np.testing.assert_array_equal(host(cols["centers"]).reshape(-1, 3), ref["centers"].astype(np.float32))
+
+
+@pytest.mark.parametrize("degree", [0, 1, 2, 3, 4])
+def test_every_row_width(ctx, degree):
+    # rows of 3, 12, 27, 48 and 75 floats from an SH-4 file, in both byte orders
+    d = syn.mixture_table(2500, seed=9, sh_degree=4)
+    _check(pf.standard_ply(d), sh_degree=degree)
+    _check(pf.standard_ply(d, little=False), sh_degree=degree)
+
+
+@pytest.mark.parametrize("degree", [1, 3])
+def test_colour_rows_off_a_16_byte_boundary(ctx, degree):
+    # rows of 12 and 48 floats into a colour column that is 4- but not 16-byte aligned
+    import ctypes
+    raw = pf.standard_ply(syn.mixture_table(1500, seed=12, sh_degree=3))
+    ref = orc.ply_decode(raw, degree)
+    n, row = 1500, ((degree + 1) ** 2) * 3
+    cols = torch.zeros(n * row + 4, device="cuda")
+    data = np.frombuffer(raw, dtype=np.uint8)
+    rb.default_context(0).call("rdx_decode_ply", ctypes.c_void_p(data.ctypes.data), len(raw), degree, None, None,
+                               None, None, ctypes.c_void_p(cols.data_ptr() + 4))
+    torch.cuda.synchronize()
+    got = host(cols[1:1 + n * row]).reshape(ref["colors"].shape)
+    np.testing.assert_array_equal(got, ref["colors"].astype(np.float32))
+    assert float(cols[0]) == 0.0 and np.all(host(cols[1 + n * row:]) == 0.0)
+
+
 def test_point_cloud_and_device_bytes(ctx):
     raw = pf.point_cloud_ply(5000, alpha=True)
     _check(raw)
