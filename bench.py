@@ -61,14 +61,15 @@ def peak_hbm():
     return FALLBACK_HBM_GBS, "fallback"
 
 
-def ncu_traffic(summary="project_kernel_4m_sh3.md"):
-    """DRAM bytes per launch of a kernel from its committed ncu summary, or None."""
+def ncu_traffic(summary="project_kernel_4m_sh3.md", scale=1.0):
+    """DRAM bytes per launch of a kernel from its committed ncu summary (times
+    `scale` where the summary captured a smaller launch of the same kernel), or None."""
     path = os.path.join(ROOT, "profiles", summary)
     if not os.path.exists(path):
         return None
     for line in open(path):
         if line.startswith("dram_bytes_per_launch:"):
-            return float(line.split(":")[1])
+            return float(line.split(":")[1].split()[0]) * scale
     return None
 
 
@@ -377,7 +378,8 @@ def run_stereo(args, world, rank, local, device):
                    "hbm_frac_frame": frame_bytes * n / (ms_step / 1e3) / 1e9 / peak,
                    "project_ms": proj_ms, "sort_ms": sort_ms, "phase_runs": runs},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_project (raw, SH 3 fp16, 2 eyes)",
+                     "traffic": ncu_traffic("project_kernel_stereo_2m.md", n / 2_000_000),
+                     "kernel": "k_project (raw, SH 3 fp16, 2 eyes)",
                      "bytes_per_splat": proj_bytes, "peak_kind": peak_kind},
         "e2e": None, "e2e_note": "device-resident tables; the headline workload carries the host end-to-end number",
         "gpu_launches": launches,
@@ -444,7 +446,8 @@ def run_backward(args, world, rank, local, device):
                    "forward_ms": fwd_step, "backward_over_forward": ms_step / fwd_step,
                    "backward_bytes_per_splat": bwd_bytes},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_project_backward (raw, SH 3, 1 eye)",
+                     "traffic": ncu_traffic("backward_kernel_1m_sh3.md", n / 1_000_000),
+                     "kernel": "k_project_backward (raw, SH 3, 1 eye)",
                      "bytes_per_splat": bwd_bytes, "peak_kind": peak_kind},
         "e2e": None, "e2e_note": "device-resident tensors (a training step's layout)",
         "gpu_launches": launches,
