@@ -84,6 +84,36 @@ __device__ __forceinline__ void normalize_quat(double q[4]) {
   }
 }
 
+// A standard file's or point cloud's splat (ply.ts:58-164) from its record:
+// value(p, normalized) reads property p as a double, rest(p) an SH value as
+// float32, and put(x, v) takes SH value x (coefficient-major) of the kvals kept
+template <class Value, class Rest, class Put>
+__device__ __forceinline__ void decode_plain(const PlyDesc& d, int kvals, Value value, Rest rest, Put put, double c[3],
+                                             double ls[3], double q[4], double& op, double rgb[3]) {
+  for (int k = 0; k < 3; k++) c[k] = value(d.xyz[k], false);
+  if (d.kind == kPlyStandard) {
+    for (int k = 0; k < 3; k++) ls[k] = value(d.scale[k], false);
+    // (rot_1, rot_2, rot_3, rot_0) = (x, y, z, w)
+    q[0] = value(d.rot[1], false);
+    q[1] = value(d.rot[2], false);
+    q[2] = value(d.rot[3], false);
+    q[3] = value(d.rot[0], false);
+    op = 1.0 / (1.0 + exp(-value(d.opacity, false)));
+    for (int k = 0; k < 3; k++) rgb[k] = 0.5 + kShC0 * value(d.color[k], false);
+#pragma unroll
+    for (int x = 0; x < kvals; x++) put(x, rest(d.rest[x]));
+  } else {
+    const double point = log(0.001);  // POINT_SCALE (ply.ts:18)
+    ls[0] = ls[1] = ls[2] = point;
+    q[0] = q[1] = q[2] = 0.0;
+    q[3] = 1.0;
+    op = d.alpha.offset >= 0 ? value(d.alpha, true) : 1.0;
+    for (int k = 0; k < 3; k++) rgb[k] = value(d.color[k], true);
+#pragma unroll
+    for (int x = 0; x < kvals; x++) put(x, 0.0f);
+  }
+}
+
 // Any file, one thread per splat reading its record in place (compressed
 // files, and records too long to stage)
 __global__ void k_decode_ply(const PlyDesc d, float* __restrict__ centers, float* __restrict__ log_scales,
@@ -132,28 +162,13 @@ __global__ void k_decode_ply(const PlyDesc d, float* __restrict__ centers, float
     }
   } else {
     const unsigned char* v = d.vertex + i * d.record;
-    for (int k = 0; k < 3; k++) c[k] = read_value(v, d.xyz[k], little, false);
-    if (d.kind == kPlyStandard) {
-      for (int k = 0; k < 3; k++) ls[k] = read_value(v, d.scale[k], little, false);
-      // (rot_1, rot_2, rot_3, rot_0) = (x, y, z, w)
-      q[0] = read_value(v, d.rot[1], little, false);
-      q[1] = read_value(v, d.rot[2], little, false);
-      q[2] = read_value(v, d.rot[3], little, false);
-      q[3] = read_value(v, d.rot[0], little, false);
-      op = 1.0 / (1.0 + exp(-read_value(v, d.opacity, little, false)));
-      for (int k = 0; k < 3; k++) rgb[k] = 0.5 + kShC0 * read_value(v, d.color[k], little, false);
-      if (col)
-        for (int x = 0; x < kvals; x++) col[3 + x] = (float)read_value(v, d.rest[x], little, false);
-    } else {
-      const double point = log(0.001);  // POINT_SCALE (ply.ts:18)
-      ls[0] = ls[1] = ls[2] = point;
-      q[0] = q[1] = q[2] = 0.0;
-      q[3] = 1.0;
-      op = d.alpha.offset >= 0 ? read_value(v, d.alpha, little, true) : 1.0;
-      for (int k = 0; k < 3; k++) rgb[k] = read_value(v, d.color[k], little, true);
-      if (col)
-        for (int x = 0; x < kvals; x++) col[3 + x] = 0.0f;
-    }
+    decode_plain(
+        d, kvals, [&](PlyProp p, bool normalized) { return read_value(v, p, little, normalized); },
+        [&](PlyProp p) { return (float)read_value(v, p, little, false); },
+        [&](int x, float f) {
+          if (col) col[3 + x] = f;
+        },
+        c, ls, q, op, rgb);
   }
   normalize_quat(q);
   if (centers)
@@ -248,28 +263,10 @@ __global__ void __launch_bounds__(kRowsThreads) k_decode_ply_rows(const PlyDesc 
   double c[3], ls[3], q[4], op, rgb[3];
   float cv[ROW];
   if (live) {
-    for (int k = 0; k < 3; k++) c[k] = staged_value(sw, base, d.xyz[k], words, little, false);
-    if (d.kind == kPlyStandard) {
-      for (int k = 0; k < 3; k++) ls[k] = staged_value(sw, base, d.scale[k], words, little, false);
-      // (rot_1, rot_2, rot_3, rot_0) = (x, y, z, w)
-      q[0] = staged_value(sw, base, d.rot[1], words, little, false);
-      q[1] = staged_value(sw, base, d.rot[2], words, little, false);
-      q[2] = staged_value(sw, base, d.rot[3], words, little, false);
-      q[3] = staged_value(sw, base, d.rot[0], words, little, false);
-      op = 1.0 / (1.0 + exp(-staged_value(sw, base, d.opacity, words, little, false)));
-      for (int k = 0; k < 3; k++) rgb[k] = 0.5 + kShC0 * staged_value(sw, base, d.color[k], words, little, false);
-#pragma unroll
-      for (int x = 0; x < kVals; x++) cv[3 + x] = staged_float(sw, base, d.rest[x], words, little);
-    } else {
-      const double point = log(0.001);  // POINT_SCALE (ply.ts:18)
-      ls[0] = ls[1] = ls[2] = point;
-      q[0] = q[1] = q[2] = 0.0;
-      q[3] = 1.0;
-      op = d.alpha.offset >= 0 ? staged_value(sw, base, d.alpha, words, little, true) : 1.0;
-      for (int k = 0; k < 3; k++) rgb[k] = staged_value(sw, base, d.color[k], words, little, true);
-#pragma unroll
-      for (int x = 0; x < kVals; x++) cv[3 + x] = 0.0f;
-    }
+    decode_plain(
+        d, kVals, [&](PlyProp p, bool normalized) { return staged_value(sw, base, p, words, little, normalized); },
+        [&](PlyProp p) { return staged_float(sw, base, p, words, little); }, [&](int x, float f) { cv[3 + x] = f; }, c,
+        ls, q, op, rgb);
     normalize_quat(q);
     for (int k = 0; k < 3; k++) cv[k] = (float)rgb[k];
     if (centers)

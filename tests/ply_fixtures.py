@@ -29,9 +29,10 @@ def _records(columns, little=True):
     return rec.tobytes()
 
 
-def standard_ply(d, little=True, extra_uchar=False, comment="radix_b200 test fixture"):
+def standard_ply(d, little=True, extra_uchar=False, comment="radix_b200 test fixture", extra_doubles=0):
     """A standard 3DGS PLY of a raw table dict (float properties; opacity as a
-    logit); the comment's length sets where the records start."""
+    logit); the comment's length sets where the records start, and
+    extra_doubles unread double properties lengthen each record."""
     n = d["centers"].shape[0]
     deg = d["sh_degree"]
     k = (deg + 1) ** 2 - 1
@@ -46,7 +47,8 @@ def standard_ply(d, little=True, extra_uchar=False, comment="radix_b200 test fix
     cols += [(f"scale_{c}", "f4", d["log_scales"][:, c]) for c in range(3)]
     q = d["quats"]
     cols += [("rot_0", "f4", q[:, 3]), ("rot_1", "f4", q[:, 0]), ("rot_2", "f4", q[:, 1]), ("rot_3", "f4", q[:, 2])]
-    types = {"f4": "float", "u1": "uchar"}
+    cols += [(f"extra_{e}", "f8", np.full(n, e + 0.5)) for e in range(extra_doubles)]
+    types = {"f4": "float", "u1": "uchar", "f8": "double"}
     head = _header([("vertex", n, [(name, types[ch]) for name, ch, _ in cols])], little, comment)
     return head + _records(cols, little)
 

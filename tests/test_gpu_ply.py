@@ -46,6 +46,14 @@ def test_records_at_every_alignment(ctx, pad):
     _check(raw, device_bytes=True)
 
 
+def test_records_too_long_to_stage(ctx):
+    # 59 floats and 130 doubles: 1276-byte records, decoded in place a thread per record
+    d = syn.mixture_table(700, seed=13, sh_degree=3)
+    raw = pf.standard_ply(d, extra_doubles=130)
+    _check(raw)
+    _check(raw, sh_degree=2, device_bytes=True)
+
+
 def test_header_longer_than_the_first_read(ctx):
     # a device file whose header (a 6000-character comment) ends past the first 4 KB read
     raw = pf.standard_ply(syn.mixture_table(300, seed=4, sh_degree=1), comment="c" * 6000)
