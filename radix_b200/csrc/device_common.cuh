@@ -7,6 +7,31 @@
 
 namespace rdx {
 
+// The bytes [src, src + len) into words of shared memory (dst[j] holds bytes
+// 4j to 4j + 3), copied by one warp with aligned word loads, funnel-shifted
+// pairs of them when src is off a word boundary; every word read holds at
+// least one of the bytes. kBatch loads a lane are in flight before their stores.
+__device__ __forceinline__ void warp_copy_bytes(const unsigned char* src, uint32_t len, uint32_t* dst, uint32_t lane) {
+  constexpr uint32_t kBatch = 16;
+  const uint32_t shift = (uint32_t)((uintptr_t)src & 3u);
+  const uint32_t* aw = reinterpret_cast<const uint32_t*>(src - shift);
+  const uint32_t n_out = (len + 3) / 4, n_in = (len + shift + 3) / 4;
+  for (uint32_t j0 = lane; j0 < n_out; j0 += 32 * kBatch) {
+    uint32_t lo[kBatch], hi[kBatch];
+#pragma unroll
+    for (uint32_t b = 0; b < kBatch; b++) {
+      const uint32_t j = j0 + 32 * b;
+      lo[b] = j < n_out ? __ldg(aw + j) : 0u;
+      hi[b] = shift != 0 && j + 1 < n_in ? __ldg(aw + j + 1) : 0u;
+    }
+#pragma unroll
+    for (uint32_t b = 0; b < kBatch; b++) {
+      const uint32_t j = j0 + 32 * b;
+      if (j < n_out) dst[j] = shift == 0 ? lo[b] : __funnelshift_r(lo[b], hi[b], 8 * shift);
+    }
+  }
+}
+
 // Non-contracted float64 arithmetic: the sort-key distance and the centre
 // culls round exactly as the float64 CPU oracle does.
 __device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }

@@ -15,6 +15,7 @@
 #include <string>
 #include <vector>
 
+#include "device_common.cuh"
 #include "rdx_internal.h"
 
 namespace rdx {
@@ -231,28 +232,8 @@ __global__ void __launch_bounds__(kRowsThreads) k_decode_ply_rows(const PlyDesc 
   const uint32_t rows = (uint32_t)min((uint64_t)32, d.count - r0);
   uint32_t* sw = s_words + (size_t)warp * region;
 
-  // the records' bytes [0, len) into sw; every source word read holds at least one of them
-  const unsigned char* src = d.vertex + r0 * d.record;
-  const uint32_t len = rows * d.record;
-  const uint32_t shift = (uint32_t)((uintptr_t)src & 3u);
-  const uint32_t* aw = reinterpret_cast<const uint32_t*>(src - shift);
-  const uint32_t n_out = (len + 3) / 4, n_in = (len + shift + 3) / 4;
-  // kCopyBatch loads in flight per lane before their stores
-  constexpr uint32_t kCopyBatch = 16;
-  for (uint32_t j0 = lane; j0 < n_out; j0 += 32 * kCopyBatch) {
-    uint32_t lo[kCopyBatch], hi[kCopyBatch];
-#pragma unroll
-    for (uint32_t b = 0; b < kCopyBatch; b++) {
-      const uint32_t j = j0 + 32 * b;
-      lo[b] = j < n_out ? __ldg(aw + j) : 0u;
-      hi[b] = shift != 0 && j + 1 < n_in ? __ldg(aw + j + 1) : 0u;
-    }
-#pragma unroll
-    for (uint32_t b = 0; b < kCopyBatch; b++) {
-      const uint32_t j = j0 + 32 * b;
-      if (j < n_out) sw[j] = shift == 0 ? lo[b] : __funnelshift_r(lo[b], hi[b], 8 * shift);
-    }
-  }
+  // the records' bytes [0, len) into sw
+  warp_copy_bytes(d.vertex + r0 * d.record, rows * d.record, sw, (uint32_t)lane);
   __syncwarp();
 
   const bool live = (uint32_t)lane < rows;

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 
+#include "device_common.cuh"
 #include "rdx_internal.h"
 
 namespace rdx {
@@ -28,6 +29,9 @@ __host__ __device__ constexpr int sh_vectors(int degree) {
   return degree <= 0 ? 0 : degree == 1 ? 3 : degree == 2 ? 8 : degree == 3 ? 15 : 24;
 }
 constexpr int kSpzThreads = 256;
+// A warp's staging words: 32 splats' base colour bytes (96) and SH bytes (72 a splat at most)
+constexpr uint32_t kSpzColourWords = 32 * 3 / 4;
+constexpr uint32_t kSpzStageWords = kSpzColourWords + 32 * 72 / 4;
 constexpr int Z_STREAM_END_FINAL = 100;  // the last gzip member ended (not a zlib status)
 
 __host__ __device__ __forceinline__ uint32_t le32(const unsigned char* p) { return (uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16) | ((uint32_t)p[3] << 24); }
@@ -130,40 +134,97 @@ __global__ void __launch_bounds__(kSpzThreads) k_decode_spz(SpzDesc d, float* __
   // fixed = 1 / (1 << fractionalBits) with a 32-bit shift, as JS evaluates it
   const double fixed = 1.0 / (double)(int32_t)(1u << (d.fractional_bits & 31));
   const double color_scale = 0.28209479177387814 / 0.15;  // SH_C0 / 0.15
+  // Every byte-valued column maps one byte (a 9-bit magnitude for version 3
+  // rotations) to its value: the block computes each mapping once, with the
+  // same rounded operations as for a single splat, and the splats look it up
+  __shared__ float s_color[256], s_alpha[256], s_scale[256], s_sh[256];
+  __shared__ double s_rot2[256], s_mag[512];
+  for (uint32_t b = threadIdx.x; b < 512; b += blockDim.x) {
+    if (b < 256) {
+      const double x = (double)b;
+      s_color[b] = (float)__dadd_rn(__dmul_rn(sub(__ddiv_rn(x, 255.0), 0.5), color_scale), 0.5);
+      s_alpha[b] = (float)__ddiv_rn(x, 255.0);
+      s_scale[b] = (float)sub(__ddiv_rn(x, 16.0), 10.0);
+      s_sh[b] = (float)((x - 128.0) / 128.0);
+      s_rot2[b] = sub(__ddiv_rn(x, 127.5), 1.0);
+    }
+    s_mag[b] = __ddiv_rn((double)b, 511.0);
+  }
+  __syncthreads();
+  __shared__ uint32_t s_stage[kSpzThreads / 32][kSpzStageWords];
+  const unsigned char* colour_bytes = reinterpret_cast<const unsigned char*>(s_stage[threadIdx.x >> 5]);
+  const unsigned char* sh_bytes = colour_bytes + kSpzColourWords * 4;
   const int file_k = sh_vectors(d.sh_degree), out_k = sh_vectors(d.out_degree);
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < d.count; i += (uint64_t)gridDim.x * blockDim.x) {
+  const uint32_t row_floats = (uint32_t)(1 + out_k) * 3;
+  // row = e / row_floats by a multiply-high (exact for e < 32 rows of at most 75 floats)
+  const uint32_t row_magic = (uint32_t)(((1ull << 32) + row_floats - 1) / row_floats);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+  // a warp per 32 splats: a lane per splat for the small columns, the whole
+  // warp for the 32 colour rows
+  for (uint64_t t = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; t * 32 < d.count; t += warps) {
+    const uint64_t i0 = t * 32, i = i0 + lane;
+    const uint32_t rows = (uint32_t)min((uint64_t)32, d.count - i0);
+    const bool live = i < d.count;
+    if (colors) {
+      // the warp's colour and SH bytes into shared memory with word loads,
+      // then its rows as one span in output order (consecutive lanes write
+      // consecutive floats)
+      warp_copy_bytes(col + i0 * 3, rows * 3, s_stage[threadIdx.x >> 5], lane);
+      warp_copy_bytes(shv + i0 * (uint64_t)file_k * 3, rows * (uint32_t)file_k * 3,
+                      s_stage[threadIdx.x >> 5] + kSpzColourWords, lane);
+      __syncwarp();
+      float* out = colors + i0 * row_floats;
+      const uint32_t total = rows * row_floats;
+      for (uint32_t e = lane; e < total; e += 32) {
+        const uint32_t r = __umulhi(e, row_magic), c = e - r * row_floats;
+        out[e] = c < 3 ? s_color[colour_bytes[r * 3 + c]] : s_sh[sh_bytes[r * (uint32_t)file_k * 3 + (c - 3)]];
+      }
+      __syncwarp();  // before the next tile's bytes replace these
+    }
+    if (!live) continue;
+    // The splat's bytes are all loaded before any of its stores (a float store may
+    // alias them as far as the compiler knows, which would order each load
+    // after the previous store and so chain their latencies)
+    const int cen_bytes = d.version == 1 ? 6 : 9, rot_bytes = d.version >= 3 ? 4 : 3;
+    uint32_t cb[9], sb[3], qb[4], ab = 0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) cb[k] = centers && k < cen_bytes ? cen[i * cen_bytes + k] : 0u;
+#pragma unroll
+    for (int k = 0; k < 3; k++) sb[k] = log_scales ? sca[i * 3 + k] : 0u;
+#pragma unroll
+    for (int k = 0; k < 4; k++) qb[k] = quats && k < rot_bytes ? rot[i * rot_bytes + k] : 0u;
+    if (opacities) ab = alp[i];
     if (centers) {
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         double v;
         if (d.version == 1) {
-          const unsigned char* p = cen + i * 6 + c * 2;
-          v = (double)__half2float(__ushort_as_half((unsigned short)(p[0] | (p[1] << 8))));
+          v = (double)__half2float(__ushort_as_half((unsigned short)(cb[c * 2] | (cb[c * 2 + 1] << 8))));
         } else {
-          const unsigned char* p = cen + i * 9 + c * 3;
-          int32_t code = (int32_t)((uint32_t)p[0] | ((uint32_t)p[1] << 8) | ((uint32_t)p[2] << 16));
+          int32_t code = (int32_t)(cb[c * 3] | (cb[c * 3 + 1] << 8) | (cb[c * 3 + 2] << 16));
           if (code & 0x800000) code -= 0x1000000;
           v = __dmul_rn((double)code, fixed);
         }
         centers[i * 3 + c] = (float)v;
       }
     }
-    if (opacities) opacities[i] = (float)__ddiv_rn((double)alp[i], 255.0);
+    if (opacities) opacities[i] = s_alpha[ab];
     if (log_scales) {
 #pragma unroll
-      for (int c = 0; c < 3; c++) log_scales[i * 3 + c] = (float)sub(__ddiv_rn((double)sca[i * 3 + c], 16.0), 10.0);
+      for (int c = 0; c < 3; c++) log_scales[i * 3 + c] = s_scale[sb[c]];
     }
     if (quats) {
       double q[4];
       if (d.version >= 3) {
-        const uint32_t packed = le32(rot + i * 4);
+        const uint32_t packed = qb[0] | (qb[1] << 8) | (qb[2] << 16) | (qb[3] << 24);
         const int largest = (int)(packed >> 30);
         uint32_t rest = packed;
         double sum = 0.0;
 #pragma unroll
         for (int k = 3; k >= 0; k--) {
           if (k == largest) continue;
-          const double mag = __ddiv_rn((double)(rest & 511u), 511.0);
+          const double mag = s_mag[rest & 511u];
           const double v = __dmul_rn(__dmul_rn(0.7071067811865476, mag), (rest >> 9) & 1u ? -1.0 : 1.0);
           rest >>= 10;
           q[k] = v;
@@ -174,9 +235,8 @@ __global__ void __launch_bounds__(kSpzThreads) k_decode_spz(SpzDesc d, float* __
         for (int k = 0; k < 4; k++)
           if (k == largest) q[k] = w;
       } else {
-        const unsigned char* p = rot + i * 3;
 #pragma unroll
-        for (int c = 0; c < 3; c++) q[c] = sub(__ddiv_rn((double)p[c], 127.5), 1.0);
+        for (int c = 0; c < 3; c++) q[c] = s_rot2[qb[c]];
         q[3] = __dsqrt_rn(
             fmax(0.0, sub(sub(sub(1.0, __dmul_rn(q[0], q[0])), __dmul_rn(q[1], q[1])), __dmul_rn(q[2], q[2]))));
       }
@@ -190,14 +250,6 @@ __global__ void __launch_bounds__(kSpzThreads) k_decode_spz(SpzDesc d, float* __
                           (float)__dmul_rn(q[3], inv));
       }
       reinterpret_cast<float4*>(quats)[i] = out;
-    }
-    if (colors) {
-      float* row = colors + i * (uint64_t)(1 + out_k) * 3;
-#pragma unroll
-      for (int c = 0; c < 3; c++)
-        row[c] = (float)__dadd_rn(__dmul_rn(sub(__ddiv_rn((double)col[i * 3 + c], 255.0), 0.5), color_scale), 0.5);
-      const unsigned char* sh = shv + i * (uint64_t)file_k * 3;
-      for (int v = 0; v < out_k * 3; v++) row[3 + v] = (float)(((double)sh[v] - 128.0) / 128.0);
     }
   }
 }
@@ -296,7 +348,13 @@ const char* spz_unpack(const unsigned char* bytes, uint64_t nbytes, const SpzDes
 cudaError_t launch_decode_spz(const SpzDesc& d, float* centers, float* log_scales, float* quats, float* opacities,
                               float* colors, cudaStream_t stream) {
   if (d.count == 0) return cudaSuccess;
-  const uint64_t blocks = std::min<uint64_t>((d.count + kSpzThreads - 1) / kSpzThreads, 148u * 16u);
+  // one wave of blocks (each builds its lookup tables once), warps looping over tiles of 32 splats
+  int device = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_decode_spz, kSpzThreads, 0);
+  const uint64_t wave = (uint64_t)std::max(sms, 1) * (uint64_t)std::max(per_sm, 1);
+  const uint64_t blocks = std::min<uint64_t>((d.count + kSpzThreads - 1) / kSpzThreads, wave);
   k_decode_spz<<<(unsigned)blocks, kSpzThreads, 0, stream>>>(d, centers, log_scales, quats, opacities, colors);
   return cudaGetLastError();
 }

@@ -77,17 +77,18 @@ def columns(d, version=3, fractional_bits=12, sh_degree=None):
     return [centers, alphas, colors, scales, rotations, sh], deg
 
 
-def gzip_spz(d, version=3, fractional_bits=12, sh_degree=None, members=1, flags=0x01, trailer=b""):
-    """A gzip SPZ (versions 1 to 4: 4 is version 3's layout) of a raw table dict."""
+def gzip_spz(d, version=3, fractional_bits=12, sh_degree=None, members=1, flags=0x01, trailer=b"", level=9):
+    """A gzip SPZ (versions 1 to 4: 4 is version 3's layout) of a raw table
+    dict, at gzip compression `level`."""
     cols, deg = columns(d, version, fractional_bits, sh_degree)
     n = d["centers"].shape[0]
     head = struct.pack("<IIIBBBB", SPZ_MAGIC, version, n, deg, fractional_bits, flags, 0)
     body = head + b"".join(cols) + trailer
     if members == 1:
-        return gzip.compress(body, mtime=0)
+        return gzip.compress(body, compresslevel=level, mtime=0)
     cut = len(body) // members
     parts = [body[i * cut:(i + 1) * cut if i < members - 1 else len(body)] for i in range(members)]
-    return b"".join(gzip.compress(p, mtime=0) for p in parts)
+    return b"".join(gzip.compress(p, compresslevel=level, mtime=0) for p in parts)
 
 
 def ngsp_spz(d, fractional_bits=12, sh_degree=None, records=b"", flags=0x01, level=3):

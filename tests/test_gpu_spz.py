@@ -46,6 +46,12 @@ def test_sh_degrees_lower_output_and_members(ctx, degree):
         _check(raw, sh_degree=degree - 1)
 
 
+def test_more_splats_than_one_sweep_of_the_grid(ctx):
+    # 1.25M splats: the decode's warps (4736 blocks of 8) take a second tile each
+    d = syn.mixture_table(1_250_000, seed=60, sh_degree=1)
+    _check(sf.gzip_spz(d, level=1))
+
+
 def test_ngsp_container(ctx):
     if orc.zstd_lib() is None:
         pytest.skip("libzstd is not on this machine")
