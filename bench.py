@@ -46,10 +46,12 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--bits", type=int, default=32, choices=[16, 24, 32],
                    help="sort-key width (32 for the headline; 24 is the reference's default)")
-    p.add_argument("--workload", default="frame", choices=["frame", "batched", "stereo", "backward", "ply", "spz"],
+    p.add_argument("--workload", default="frame",
+                   choices=["frame", "batched", "stereo", "backward", "ply", "spz", "rdx"],
                    help="frame: 4M SH-3 splats, one view (the headline); batched: 16 scenes x 64 views in one "
                         "CUDA graph; stereo: 16M SH-3 fp16 splats, two eyes; backward: the projection's gradient, 1M; "
-                        "ply: decoding a 1M-splat PLY file; spz: decoding a 1M-splat SPZ file from host bytes")
+                        "ply: decoding a 1M-splat PLY file; spz: decoding a 1M-splat SPZ file from host bytes; "
+                        "rdx: decoding a 1M-splat RDX file from host bytes")
     return p.parse_args()
 
 
@@ -583,6 +585,78 @@ def run_spz(args, world, rank, local, device):
     }
 
 
+def run_rdx(args, world, rank, local, device):
+    """A 1M-splat RDX file in host memory decoded into device channel arrays
+    each step: an extSplats bundle (extA, extB) and a degree-3 extSh bundle
+    (four channels), six uint32x4 channels in 64k-row chunks, every chunk's
+    channel byte-transposed and gzipped. The host inflates the payloads, the
+    device un-transposes them in one launch, which is timed alone beside it.
+    The words are the seeded SH-3 mixture's float32 columns, so the payloads
+    compress like splat data; the decode does not interpret them."""
+    import numpy as np
+    import torch
+
+    import radix_b200 as rb
+    from radix_b200 import synthetic as syn
+    from tests import rdx_fixtures as rf
+    n = 1_000_000 if args.n == N_SPLATS else args.n
+    d = syn.mixture_table(n, seed=0, sh_degree=SH_DEGREE)
+
+    def words(*cols):
+        rows = np.concatenate([np.asarray(c, np.float32).reshape(n, -1) for c in cols], 1)
+        return np.ascontiguousarray(rows).view(np.uint32)
+
+    sh = np.asarray(d["colors"][:, 1:, :], np.float32).reshape(n, -1)[:, :16]
+    chans = {"extA": words(d["centers"], d["opacities"]), "extB": words(d["log_scales"], d["quats"][:, 3])}
+    sh_chans = {f"extSh{chr(65 + c)}": np.ascontiguousarray(sh[:, 4 * c:4 * c + 4]).view(np.uint32) for c in range(4)}
+    bundles = {"extSplats": ({k: "uint32x4" for k in chans}, {}, chans),
+               "extSh": ({k: "uint32x4" for k in sh_chans}, {"codec": "ext", "degree": SH_DEGREE}, sh_chans)}
+    raw = rf.rdx_file(bundles, n, 65536, level=6)
+    del d, chans, sh_chans, sh
+    ctx = rb.Context(local)
+    rb.decode_rdxfile(raw, ctx=ctx)
+    payload = n * 6 * 16
+
+    def step():
+        rb.decode_rdxfile(raw, ctx=ctx)
+
+    marks = {}
+
+    def start_counting():
+        marks["launches"] = ctx.launches()
+
+    ms_total, clock_info = timed(step, args.steps, args.warmup, world, local, start_counting)
+    launches = ctx.launches() - marks["launches"]
+    ms_step = ms_total / args.steps
+    # the un-transpose alone: phase events around its launch, outside the timed region
+    ctx.set_profiling(True)
+    ctx.phase_times()
+    for _ in range(5):
+        rb.decode_rdxfile(raw, ctx=ctx)
+    torch.cuda.synchronize()
+    kt, kr = ctx.phase_times()["project"]
+    ctx.set_profiling(False)
+    kernel_ms = kt / max(kr, 1)
+    peak, peak_kind = peak_hbm()
+    bytes_per = 2 * 6 * 16  # the inflated payload read, the channel arrays written
+    achieved = bytes_per * n / (kernel_ms / 1e3) / 1e9
+    value = replicas_throughput(n, args.steps, world, ms_total)
+    return {
+        "metric": "Msplats/s (RDX decode, host bytes to device channels)", "value": value,
+        "unit": "Msplats/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (an RDX file of the seeded SH-3 mixture's float32 words)",
+        "config": {"workload": f"RDX decode: {n} splats, extSplats + extSh degree 3 (6 uint32x4 channels, "
+                               f"64k-row chunks, {len(raw)} B file), host bytes to device channel arrays", "n": n,
+                   "parallelism": f"replicas{world}", "file_bytes": len(raw), "kernel_ms": kernel_ms,
+                   "note": "a step: the payloads inflated on one host thread (zlib), copied, un-transposed on the GPU"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_untranspose", "bytes_per_splat": bytes_per, "peak_kind": peak_kind},
+        "e2e": {"value": value, "unit": "Msplats/s", "h2d_bytes_per_step": payload, "d2h_bytes_per_step": 0},
+        "gpu_launches": launches, "clocks": clock_info,
+    }
+
+
 def main():
     global BITS, FRAME_BYTES
     args = parse()
@@ -603,7 +677,7 @@ def main():
             from datetime import timedelta
             dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
         run = {"batched": run_batched, "stereo": run_stereo, "backward": run_backward, "ply": run_ply,
-               "spz": run_spz}[args.workload]
+               "spz": run_spz, "rdx": run_rdx}[args.workload]
         line = run(args, world, rank, local, device)
         if rank == 0:
             print(json.dumps(line))

@@ -1695,11 +1695,8 @@ int rdx_decode_rdxfile(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, void* c
   layout(a);
   if (status != RDX_OK) return status;
   std::vector<rdx::RdxPiece> pieces;
-  uint32_t max_count = 0;
-  for (const rdx::RdxSpan& sp : spans) {
+  for (const rdx::RdxSpan& sp : spans)
     pieces.push_back({sp.src, outs[sp.channel] + sp.start * (uint64_t)sp.bytes, sp.count, sp.bytes});
-    max_count = std::max(max_count, sp.count);
-  }
   if (!staged.empty())
     RDX_CUDA(cudaMemcpyAsync(dev_staged, staged.data(), staged.size(), cudaMemcpyHostToDevice, ctx->stream), "RDX copy");
   if (!pieces.empty())
@@ -1708,7 +1705,7 @@ int rdx_decode_rdxfile(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, void* c
              "RDX pieces");
   {
     Phase decoding(ctx, RDX_PHASE_PROJECT);
-    RDX_CUDA(rdx::launch_untranspose(dev_pieces, (int)pieces.size(), max_count, dev_staged, ctx->stream),
+    RDX_CUDA(rdx::launch_untranspose(dev_pieces, pieces.data(), (int)pieces.size(), dev_staged, ctx->stream),
              "RDX transpose launch");
     if (!pieces.empty()) ctx->launches += (uint64_t)((pieces.size() + 65534) / 65535);
   }

@@ -279,9 +279,10 @@ const char* rdxfile_header(const unsigned char* bytes, uint64_t nbytes, RdxFile*
 // Every chunk's payloads of the wanted channels inflated into `staged`: null or an error text
 const char* rdxfile_unpack(const unsigned char* bytes, uint64_t nbytes, const RdxFile& f, const bool* wanted,
                            std::vector<unsigned char>* staged, std::vector<RdxSpan>* spans);
-// The staged bytes transposed back into the pieces' destinations (one launch per 65535 pieces)
-cudaError_t launch_untranspose(const RdxPiece* pieces_dev, int n_pieces, uint32_t max_count, const unsigned char* staged,
-                               cudaStream_t stream);
+// The staged bytes transposed back into the pieces' destinations (one launch
+// per 65535 pieces; pieces_host is the host copy of pieces_dev)
+cudaError_t launch_untranspose(const RdxPiece* pieces_dev, const RdxPiece* pieces_host, int n_pieces,
+                               const unsigned char* staged, cudaStream_t stream);
 
 // One persistent launch over every descriptor of one table kind (descs in device memory)
 // ---- PLY files (src/core/ply.ts) to raw tables ----

@@ -291,11 +291,44 @@ int64_t gunzip_all(const unsigned char* in, uint64_t n, std::vector<unsigned cha
 
 constexpr int kTransposeThreads = 256;
 
+// A piece of 16-byte elements whose rows come in fours and whose byte planes
+// are word-aligned (its source) and whose elements are 16-byte aligned (its
+// destination) goes four elements a thread
+__host__ __device__ __forceinline__ bool by_quads(const RdxPiece& pc, const unsigned char* staged) {
+  return pc.bytes == 16 && pc.count % 4 == 0 && ((uintptr_t)(staged + pc.src) & 3u) == 0 &&
+         ((uintptr_t)pc.dst & 15u) == 0;
+}
+
 // Element i's byte b sits at src[b * count + i]: blockIdx.y picks the piece
 __global__ void __launch_bounds__(kTransposeThreads) k_untranspose(const RdxPiece* __restrict__ pieces,
                                                                    const unsigned char* __restrict__ staged) {
   const RdxPiece pc = pieces[blockIdx.y];
   const unsigned char* src = staged + pc.src;
+  if (by_quads(pc, staged)) {
+    // one word of each of the 16 byte planes (elements 4g to 4g + 3), then a
+    // 4x4 byte transpose for each of the elements' four words
+    const uint32_t* planes = reinterpret_cast<const uint32_t*>(src);
+    const uint32_t quads = pc.count / 4;
+    uint4* dst = reinterpret_cast<uint4*>(pc.dst);
+    for (uint32_t g = blockIdx.x * kTransposeThreads + threadIdx.x; g < quads; g += gridDim.x * kTransposeThreads) {
+      uint32_t p[16];
+#pragma unroll
+      for (int b = 0; b < 16; b++) p[b] = __ldg(planes + (uint64_t)b * quads + g);
+      uint32_t e[4][4];  // e[j][k]: word k of element 4g + j (bytes 4k to 4k + 3: planes 4k to 4k + 3, byte j)
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const uint32_t lo01 = __byte_perm(p[4 * k], p[4 * k + 1], 0x5140), lo23 = __byte_perm(p[4 * k + 2], p[4 * k + 3], 0x5140);
+        const uint32_t hi01 = __byte_perm(p[4 * k], p[4 * k + 1], 0x7362), hi23 = __byte_perm(p[4 * k + 2], p[4 * k + 3], 0x7362);
+        e[0][k] = __byte_perm(lo01, lo23, 0x5410);
+        e[1][k] = __byte_perm(lo01, lo23, 0x7632);
+        e[2][k] = __byte_perm(hi01, hi23, 0x5410);
+        e[3][k] = __byte_perm(hi01, hi23, 0x7632);
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++) dst[(uint64_t)g * 4 + j] = make_uint4(e[j][0], e[j][1], e[j][2], e[j][3]);
+    }
+    return;
+  }
   for (uint32_t i = blockIdx.x * kTransposeThreads + threadIdx.x; i < pc.count; i += gridDim.x * kTransposeThreads) {
     unsigned char* d = pc.dst + (uint64_t)i * pc.bytes;
     if (pc.bytes == 16 && (reinterpret_cast<uintptr_t>(d) & 15u) == 0) {
@@ -386,10 +419,15 @@ const char* rdxfile_unpack(const unsigned char* bytes, uint64_t nbytes, const Rd
   return nullptr;
 }
 
-cudaError_t launch_untranspose(const RdxPiece* pieces_dev, int n_pieces, uint32_t max_count, const unsigned char* staged,
+cudaError_t launch_untranspose(const RdxPiece* pieces_dev, const RdxPiece* pieces_host, int n_pieces,
+                               const unsigned char* staged,
                                cudaStream_t stream) {
-  if (n_pieces == 0 || max_count == 0) return cudaSuccess;
-  const uint32_t gx = std::min<uint32_t>((max_count + kTransposeThreads - 1) / kTransposeThreads, 1024u);
+  // threads' work: a quarter of the rows for pieces taken four elements a thread
+  uint32_t max_work = 0;
+  for (int k = 0; k < n_pieces; k++)
+    max_work = std::max(max_work, by_quads(pieces_host[k], staged) ? pieces_host[k].count / 4 : pieces_host[k].count);
+  if (max_work == 0) return cudaSuccess;
+  const uint32_t gx = std::min<uint32_t>((max_work + kTransposeThreads - 1) / kTransposeThreads, 1024u);
   for (int first = 0; first < n_pieces; first += 65535) {
     const int batch = std::min(n_pieces - first, 65535);
     k_untranspose<<<dim3(gx, (unsigned)batch), kTransposeThreads, 0, stream>>>(pieces_dev + first, staged);

@@ -39,15 +39,15 @@ def container(magic, meta, payloads):
     return bytes(out)
 
 
-def transposed_gzip(raw, eb):
+def transposed_gzip(raw, eb, level=9):
     """Byte k of every element together, then gzip (Compression.compressTransposed)."""
     a = np.frombuffer(raw, dtype=np.uint8).reshape(-1, eb)
-    return gzip.compress(np.ascontiguousarray(a.T).tobytes(), mtime=0)
+    return gzip.compress(np.ascontiguousarray(a.T).tobytes(), compresslevel=level, mtime=0)
 
 
-def rdx_file(bundles, count, chunk_size=65536, meta=None):
+def rdx_file(bundles, count, chunk_size=65536, meta=None, level=9):
     """A whole RDX file. bundles: {name: (channels {label: format}, bundle meta, {label: numpy array [count, ...]})},
-    in payload order."""
+    in payload order; payloads gzipped at `level`."""
     assert chunk_size > 0 and chunk_size % 4096 == 0
     chunks = []
     for start in range(0, count, chunk_size):
@@ -58,7 +58,7 @@ def rdx_file(bundles, count, chunk_size=65536, meta=None):
                 eb = element_bytes(fmt)
                 raw = np.ascontiguousarray(data[label]).view(np.uint8).reshape(count, -1)
                 assert raw.shape[1] == eb, (label, raw.shape, eb)
-                payloads.append(transposed_gzip(raw[start:start + n].tobytes(), eb))
+                payloads.append(transposed_gzip(raw[start:start + n].tobytes(), eb, level))
         chunks.append(container(CHUNK_MAGIC, {"start": start, "count": n}, payloads))
     header = {"version": 1, "count": count, "chunkSize": chunk_size, "meta": meta or {},
               "bundles": {name: {"def": {"channels": channels, "packing": "float32", "serialize": True},

@@ -46,6 +46,18 @@ def test_channels_byte_exact(ctx, device):
             np.testing.assert_array_equal(host(ch[name][label]), ref[name][label], err_msg=f"{name}.{label}")
 
 
+def test_ragged_last_chunk(ctx):
+    # 70001 rows: the first chunk's 16-byte channels go four elements a thread, the
+    # last chunk's 4465 rows (not a multiple of 4) one element a thread, in one launch
+    n = 70_001
+    raw = rf.rdx_file(_mixed(n, seed=3), n, 65536)
+    _, ch = rb.decode_rdxfile(raw)
+    _, ref = orc.rdxfile_read(raw)
+    for name in ref:
+        for label in ref[name]:
+            np.testing.assert_array_equal(host(ch[name][label]), ref[name][label], err_msg=f"{name}.{label}")
+
+
 def test_errors_carry_the_reference_texts(ctx):
     raw = rf.rdx_file(_mixed(5000), 5000, 4096)
     with pytest.raises(rb.RadixError, match="Not an RDX piece of the expected type"):
