@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <string>
 #include <utility>
 #include <vector>
@@ -274,6 +275,9 @@ struct RdxPiece {
   uint32_t count;
   uint32_t bytes;
 };
+// fn(0) .. fn(n - 1) shared among host threads (a thread per MB of work_bytes
+// at most, up to the host's threads), returning when all are done
+void parallel_for(size_t n, uint64_t work_bytes, const std::function<void(size_t)>& fn);
 // An RDX file's header from host bytes: null, or the reference's error text
 const char* rdxfile_header(const unsigned char* bytes, uint64_t nbytes, RdxFile* f);
 // Every chunk's payloads of the wanted channels inflated into `staged`: null or an error text

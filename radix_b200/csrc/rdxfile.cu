@@ -6,9 +6,10 @@
 // holds { start, count } and, per channel, that channel's elements gzipped
 // with their bytes transposed (byte b of every element together).
 //
-// The host parses the JSON and inflates the payloads (DEFLATE is sequential);
-// the device transposes the bytes back, every chunk and channel in one launch,
-// into the caller's channel arrays.
+// The host parses the JSON and inflates the payloads (DEFLATE is sequential
+// within a stream, but every payload is a stream of its own, so host threads
+// share them); the device transposes the bytes back, every chunk and channel
+// in one launch, into the caller's channel arrays.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -16,7 +17,10 @@
 #include <zlib.h>
 
 #include <algorithm>
+#include <atomic>
+#include <functional>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -387,36 +391,91 @@ const char* rdxfile_header(const unsigned char* bytes, uint64_t nbytes, RdxFile*
   return nullptr;
 }
 
+void parallel_for(size_t n, uint64_t work_bytes, const std::function<void(size_t)>& fn) {
+  // a thread per MB of input at most, up to the host's threads (32 at most)
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const size_t threads = (size_t)std::min<uint64_t>({(uint64_t)hw, (uint64_t)n, 32, 1 + work_bytes / (1u << 20)});
+  std::atomic<size_t> next{0};
+  auto drain = [&] {
+    for (size_t i = next++; i < n; i = next++) fn(i);
+  };
+  std::vector<std::thread> pool;
+  for (size_t t = 1; t < threads; t++) {
+    try {
+      pool.emplace_back(drain);
+    } catch (...) {
+      break;  // no more threads: the others and this one share the rest
+    }
+  }
+  drain();
+  for (auto& th : pool) th.join();
+}
+
 const char* rdxfile_unpack(const unsigned char* bytes, uint64_t nbytes, const RdxFile& f, const bool* wanted,
                            std::vector<unsigned char>* staged, std::vector<RdxSpan>* spans) {
   (void)nbytes;  // rdxfile_header checked that every chunk lies inside the file
   staged->clear();
   spans->clear();
-  uint64_t at = f.header_bytes;
-  std::vector<unsigned char> buf;
-  for (size_t ci = 0; ci < f.chunk_bytes.size(); ci++) {
+  // Every chunk's container first (in file order, stopping at the first bad
+  // one), then every payload inflated, the payloads shared among host threads
+  // (each is its own gzip stream); errors are reported in the order a serial
+  // read would meet them
+  struct Payload {
+    const unsigned char* in;
+    uint64_t size, expect, start, dst;
+    int channel;
+    bool keep;
+  };
+  std::vector<Payload> jobs;
+  const char* parse_error = nullptr;
+  uint64_t at = f.header_bytes, total = 0, packed = 0;
+  for (size_t ci = 0; ci < f.chunk_bytes.size() && !parse_error; ci++) {
     Json meta;
     std::vector<std::pair<uint64_t, uint64_t>> payloads;
     uint64_t length = 0;
     const char* err = read_container(bytes + at, f.chunk_bytes[ci], kChunkMagic, &meta, &payloads, &length);
-    if (err) return err;
     const uint64_t start = as_u64(meta.get("start")), count = as_u64(meta.get("count"));
-    if (start + count > f.count) return error_text("RDX chunk at %s%s%llu runs past the %llu elements", "", "", start, f.count);
-    if (payloads.size() != f.channels.size())
-      return error_text("RDX chunk %s%s%llu holds %llu payloads", "", "", (uint64_t)ci, (uint64_t)payloads.size());
-    for (size_t k = 0; k < f.channels.size(); k++) {
-      const RdxChannel& ch = f.channels[k];
-      if (gunzip_all(bytes + at + payloads[k].first, payloads[k].second, &buf) < 0) return "RDX payload is not a gzip stream";
-      if (buf.size() != count * (uint64_t)ch.element_bytes)
-        return error_text("Chunk at %s: %s holds %llu bytes, expected %llu", std::to_string(start).c_str(),
-                          (ch.bundle + "." + ch.label).c_str(), (uint64_t)buf.size(), count * (uint64_t)ch.element_bytes);
-      if (!wanted[k] || count == 0) continue;
-      spans->push_back({staged->size(), (int)k, start, (uint32_t)count, (uint32_t)ch.element_bytes});
-      staged->insert(staged->end(), buf.begin(), buf.end());
+    if (err) {
+      parse_error = err;
+    } else if (start + count > f.count) {
+      parse_error = error_text("RDX chunk at %s%s%llu runs past the %llu elements", "", "", start, f.count);
+    } else if (payloads.size() != f.channels.size()) {
+      parse_error = error_text("RDX chunk %s%s%llu holds %llu payloads", "", "", (uint64_t)ci, (uint64_t)payloads.size());
+    } else {
+      for (size_t k = 0; k < f.channels.size(); k++) {
+        const uint64_t eb = (uint64_t)f.channels[k].element_bytes;
+        Payload j{bytes + at + payloads[k].first, payloads[k].second, count * eb, start, total, (int)k,
+                  wanted[k] && count > 0};
+        if (j.keep) {
+          spans->push_back({total, (int)k, start, (uint32_t)count, (uint32_t)eb});
+          total += j.expect;
+        }
+        packed += j.size;
+        jobs.push_back(j);
+      }
     }
     at += f.chunk_bytes[ci];
   }
-  return nullptr;
+  staged->resize(total);
+  std::vector<int64_t> got(jobs.size(), 0);
+  parallel_for(jobs.size(), packed, [&](size_t q) {
+    const Payload& j = jobs[q];
+    std::vector<unsigned char> buf;
+    buf.reserve(j.expect);
+    got[q] = gunzip_all(j.in, j.size, &buf);
+    if (j.keep && got[q] == (int64_t)j.expect) memcpy(staged->data() + j.dst, buf.data(), buf.size());
+  });
+  for (size_t q = 0; q < jobs.size(); q++) {
+    const Payload& j = jobs[q];
+    if (got[q] < 0) return "RDX payload is not a gzip stream";
+    if ((uint64_t)got[q] != j.expect) {
+      const RdxChannel& ch = f.channels[j.channel];
+      return error_text("Chunk at %s: %s holds %llu bytes, expected %llu", std::to_string(j.start).c_str(),
+                        (ch.bundle + "." + ch.label).c_str(), (uint64_t)got[q], j.expect);
+    }
+  }
+  if (parse_error) spans->clear();
+  return parse_error;
 }
 
 cudaError_t launch_untranspose(const RdxPiece* pieces_dev, const RdxPiece* pieces_host, int n_pieces,

@@ -16,6 +16,7 @@
 #include <zlib.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "device_common.cuh"
 #include "rdx_internal.h"
@@ -330,18 +331,33 @@ const char* spz_unpack(const unsigned char* bytes, uint64_t nbytes, const SpzDes
   }
   const Zstd& z = zstd();
   if (!z.decompress || !z.is_error) return "SPZ 4 files need libzstd (libzstd.so.1 was not found)";
-  uint64_t at = d.toc_at + (uint64_t)d.n_streams * 16;
+  // the streams (one a present column) decompressed side by side on host threads
+  struct Stream {
+    uint64_t at, comp;
+    int column;
+  };
+  std::vector<Stream> streams;
+  uint64_t at = d.toc_at + (uint64_t)d.n_streams * 16, packed = 0;
   int k = 0;
   for (int s = 0; s < d.n_streams; s++) {
     while (d.col_size[k] == 0) k++;
     const unsigned char* e = bytes + d.toc_at + (uint64_t)s * 16;
     const uint64_t comp = ((uint64_t)le32(e + 4) << 32) | le32(e);
-    const size_t out = z.decompress(payload + d.col_off[k], d.col_size[k], bytes + at, comp);
-    if (z.is_error(out) || out != d.col_size[k])
-      return error_text("SPZ 4 stream %llu does not decompress to its %llu bytes", (uint64_t)s, d.col_size[k]);
+    streams.push_back({at, comp, k});
     at += comp;
+    packed += comp;
     k++;
   }
+  std::vector<char> ok(streams.size(), 0);
+  parallel_for(streams.size(), packed, [&](size_t s) {
+    const Stream& st = streams[s];
+    const size_t out = z.decompress(payload + d.col_off[st.column], d.col_size[st.column], bytes + st.at, st.comp);
+    ok[s] = !z.is_error(out) && out == d.col_size[st.column];
+  });
+  for (size_t s = 0; s < streams.size(); s++)
+    if (!ok[s])
+      return error_text("SPZ 4 stream %llu does not decompress to its %llu bytes", (uint64_t)s,
+                        d.col_size[streams[s].column]);
   return nullptr;
 }
 
