@@ -579,7 +579,8 @@ def run_spz(args, world, rank, local, device):
                    "parallelism": f"replicas{world}", "file_bytes": len(raw), "kernel_ms": kernel_ms,
                    "note": "a step: gzip inflated on one host thread (zlib), columns copied, decoded on the GPU"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_decode_spz", "bytes_per_splat": bytes_per, "peak_kind": peak_kind},
+                     "traffic": ncu_traffic("spz_decode_kernel_1m_sh3.md", n / 1_000_000), "kernel": "k_decode_spz",
+                     "bytes_per_splat": bytes_per, "peak_kind": peak_kind},
         "e2e": {"value": value, "unit": "Msplats/s", "h2d_bytes_per_step": payload, "d2h_bytes_per_step": 0},
         "gpu_launches": launches, "clocks": clock_info,
     }
@@ -651,7 +652,8 @@ def run_rdx(args, world, rank, local, device):
                    "parallelism": f"replicas{world}", "file_bytes": len(raw), "kernel_ms": kernel_ms,
                    "note": "a step: the payloads inflated on one host thread (zlib), copied, un-transposed on the GPU"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_untranspose", "bytes_per_splat": bytes_per, "peak_kind": peak_kind},
+                     "traffic": ncu_traffic("rdx_untranspose_kernel_1m.md", n / 1_000_000), "kernel": "k_untranspose",
+                     "bytes_per_splat": bytes_per, "peak_kind": peak_kind},
         "e2e": {"value": value, "unit": "Msplats/s", "h2d_bytes_per_step": payload, "d2h_bytes_per_step": 0},
         "gpu_launches": launches, "clocks": clock_info,
     }
