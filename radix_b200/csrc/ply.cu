@@ -3,8 +3,9 @@
 // of its compressed reader (ply.ts:170-264, SuperSplat / PlayCanvas chunks),
 // written as float32 columns (centres, ln scales, normalised quaternions
 // x y z w, opacities, base rgb + SH coefficient-major) instead of Radix's
-// quantised layouts. The header is read on the host; one thread decodes a
-// splat, in float64, and rounds once to float32.
+// quantised layouts. The header is read on the host; on the device a lane
+// decodes a splat, in float64, and rounds once to float32 (standard files and
+// point clouds a warp of 32 records at a time, staged in shared memory).
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>

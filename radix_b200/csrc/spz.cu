@@ -1,10 +1,11 @@
 // SPZ files (Niantic's format, as src/core/spz.ts reads it) to raw tables.
 // The host unpacks the container: a gzip stream (versions 1 to 4; 4 there is
 // version 3's layout) is inflated by zlib up to the end of the SH column,
-// SPZ 4's NGSP container has its zstd streams decompressed by libzstd, which
-// is loaded the first time such a file is read. The byte columns then go to
-// the device, where a thread per splat decodes them (SpzFile.read,
-// src/core/spz.ts:285-348, and decodeSmallestThree, 571-586) into float32
+// SPZ 4's NGSP container has its zstd streams decompressed by libzstd (loaded
+// the first time such a file is read), on host threads side by side. The byte
+// columns then go to the device, where a warp decodes 32 splats, a lane each
+// for the small columns and the whole warp for the colour rows (SpzFile.read,
+// src/core/spz.ts:285-348, and decodeSmallestThree, 571-586), into float32
 // raw-table columns: float64 arithmetic with every operation explicitly
 // rounded, in the order the reference evaluates it, then one rounding to float32.
 #include <cuda_fp16.h>
