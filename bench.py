@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--bits", type=int, default=32, choices=[16, 24, 32],
                    help="sort-key width (32 for the headline; 24 is the reference's default)")
+    p.add_argument("--spz-container", default="gzip", choices=["gzip", "ngsp"],
+                   help="spz workload: version 3 in gzip (one DEFLATE stream) or SPZ 4 (NGSP, a zstd stream a column)")
     p.add_argument("--workload", default="frame",
                    choices=["frame", "batched", "stereo", "backward", "ply", "spz", "rdx"],
                    help="frame: 4M SH-3 splats, one view (the headline); batched: 16 scenes x 64 views in one "
@@ -538,7 +540,8 @@ def run_spz(args, world, rank, local, device):
     from tests import spz_fixtures as sf
     n = 1_000_000 if args.n == N_SPLATS else args.n
     d = syn.mixture_table(n, seed=0, sh_degree=SH_DEGREE)
-    raw = sf.gzip_spz(d, version=3)
+    raw = sf.gzip_spz(d, version=3) if args.spz_container == "gzip" else sf.ngsp_spz(d)
+    form = "version 3 in gzip" if args.spz_container == "gzip" else "SPZ 4 (NGSP, zstd streams)"
     del d
     ctx = rb.Context(local)
     rb.decode_spz(raw, ctx=ctx)
@@ -574,10 +577,11 @@ def run_spz(args, world, rank, local, device):
         "unit": "Msplats/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8 in, f64 maths, f32 out",
         "data": "synthetic (an SPZ file written from the seeded SH-3 mixture)",
-        "config": {"workload": f"SPZ decode: {n} splats, version 3 in gzip ({len(raw)} B file, {payload} B of columns), "
+        "config": {"workload": f"SPZ decode: {n} splats, {form} ({len(raw)} B file, {payload} B of columns), "
                                "SH 3, host bytes to a raw float32 table on the GPU", "n": n,
                    "parallelism": f"replicas{world}", "file_bytes": len(raw), "kernel_ms": kernel_ms,
-                   "note": "a step: gzip inflated on one host thread (zlib), columns copied, decoded on the GPU"},
+                   "note": "a step: the container unpacked on the host (gzip: zlib on one thread; NGSP: libzstd, "
+                           "the streams on host threads side by side), columns copied, decoded on the GPU"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": ncu_traffic("spz_decode_kernel_1m_sh3.md", n / 1_000_000), "kernel": "k_decode_spz",
                      "bytes_per_splat": bytes_per, "peak_kind": peak_kind},
