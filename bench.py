@@ -139,42 +139,42 @@ def table_of(cols):
     return rb.Table.raw(cols["centers"], cols["log_scales"], cols["quats"], cols["opacities"], cols["colors"], SH_DEGREE)
 
 
-def cpu_baseline(n_sample):
-    """The oracle (float64 port of the reference's CPU path) on a bounded sample:
-    projection + SH + keys on all host threads, SortKeys.sort single-threaded."""
-    import numpy as np
+def keys_sort_only(dist, n, reps=3):
+    """The reference's own CPU path as bench-core.ts times it (SortKeys.compute
+    + SortKeys.sort, one worker thread): Msplats/s, median of reps after one warm-up."""
+    from oracle import oracle as orc
+    ks = []
+    for i in range(reps + 1):
+        t0 = time.perf_counter()
+        keys = orc.sort_keys(dist, BITS)
+        orc.sort(keys, n, BITS)
+        if i:
+            ks.append(time.perf_counter() - t0)
+    return n / statistics.median(ks) / 1e6
 
+
+def cpu_baseline(n_sample):
+    """The oracle (float64 port of the reference's CPU path) on the workload:
+    projection + SH + keys on all host threads, SortKeys.sort single-threaded."""
     import radix_b200 as rb
     from oracle import oracle as orc
     from radix_b200 import synthetic as syn
     d = syn.mixture_table(n_sample, seed=0, sh_degree=SH_DEGREE)
     obj = [rb.SplatObject(rb.Table.from_dict(d))]
     cam = syn.scale_camera()
-    times, sort_times = [], []
+    times = []
     for i in range(4):
         t0 = time.perf_counter()
         ref = orc.project(obj, cam, None, BITS, cull_keys=True, threads=0)
-        t1 = time.perf_counter()
         orc.sort(ref["keys"], n_sample, BITS)
-        t2 = time.perf_counter()
         if i:
-            times.append(t2 - t0)
-            sort_times.append(t2 - t1)
+            times.append(time.perf_counter() - t0)
     t = statistics.median(times)
-    # the reference's own CPU path (SortKeys.compute + SortKeys.sort, one worker)
-    dist = ref["distance"]
-    ks = []
-    for i in range(4):
-        t0 = time.perf_counter()
-        keys = orc.sort_keys(dist, BITS)
-        orc.sort(keys, n_sample, BITS)
-        if i:
-            ks.append(time.perf_counter() - t0)
     threads = os.cpu_count() or 1
     return {"value": n_sample / t / 1e6, "unit": "Msplats/s", "cores": threads, "kind": "port",
             "sample": f"{n_sample} splats of the same workload; float64 projection+SH+keys on {threads} threads "
                       f"(OpenMP), SortKeys.sort restated in C on 1 thread; median of 3 after 1 warm-up",
-            "keys_sort_only_msplats_s_1thread": n_sample / statistics.median(ks) / 1e6}
+            "keys_sort_only_msplats_s_1thread": keys_sort_only(ref["distance"], n_sample)}
 
 
 def run_reference(args):
@@ -184,7 +184,7 @@ def run_reference(args):
     import radix_b200 as rb
     from oracle import oracle as orc
     from radix_b200 import synthetic as syn
-    n = min(args.n, 1_000_000)
+    n = args.n
     d = syn.mixture_table(n, seed=0, sh_degree=SH_DEGREE)
     obj = [rb.SplatObject(rb.Table.from_dict(d))]
     cam = syn.scale_camera()
@@ -202,10 +202,13 @@ def run_reference(args):
         "metric": METRIC, "value": value, "unit": "Msplats/s", "impl": "reference", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded mulberry32)",
-        "config": {"workload": f"project+SH+key+sort, {n} splats (a bounded sample of the 4M SH-3 workload), "
-                               f"1920x1080 fov 50, {BITS}-bit keys", "n": n, "sh_degree": SH_DEGREE, "bits": BITS},
+        "config": {"workload": f"project+SH+key+sort, {n} splats, SH degree 3 fp32, Gaussian-mixture centres, "
+                               f"1920x1080 fov 50, {BITS}-bit keys, stable order",
+                   "n": n, "sh_degree": SH_DEGREE, "bits": BITS},
         "cpu_baseline": {"value": value, "unit": "Msplats/s", "cores": threads, "kind": "port",
-                         "sample": f"{n} splats per step; float64 projection on {threads} threads, sort on 1"},
+                         "sample": f"the whole workload ({n} splats) every step; float64 projection+SH+keys on "
+                                   f"{threads} threads (OpenMP), SortKeys.sort restated in C on 1 thread",
+                         "keys_sort_only_msplats_s_1thread": keys_sort_only(ref["distance"], n)},
         "e2e": {"value": value, "unit": "Msplats/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -776,7 +779,7 @@ def main():
         "metric": METRIC, "value": value, "unit": "Msplats/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded mulberry32 + Box-Muller)",
-        "config": {"workload": "project+SH+key+sort, 4M splats, SH degree 3 fp32, Gaussian-mixture centres, "
+        "config": {"workload": f"project+SH+key+sort, {n} splats, SH degree 3 fp32, Gaussian-mixture centres, "
                                f"1920x1080 fov 50, {BITS}-bit keys, stable order",
                    "n": n, "sh_degree": SH_DEGREE, "bits": BITS, "parallelism": f"replicas{world}",
                    "l2": "inputs 944 MB > 126 MB L2 (no flush)",
@@ -793,7 +796,7 @@ def main():
         "clocks": clock_info,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(500_000)
+        line["cpu_baseline"] = cpu_baseline(n)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -497,9 +497,11 @@ int rdx_batch_destroy(rdx_batch* batch);
  * keys, ordering and visible (may be NULL) must be device memory
  * (RDX_ERR_ARG otherwise). The work is enqueued on `stream` (NULL: the legacy
  * default stream); *visible becomes 0xffffffff if a bounded device wait gave
- * up. The first call on a device looks up the array's device address, so make
- * it before capturing a stream. All calls share the array: calls that overlap
- * on the GPU race; issue them one after another.
+ * up, and with visible == NULL such a wait goes unreported. Every call looks
+ * up the array's device address on the current device (no cached address
+ * outlives a context); the first call on a device also loads the library's
+ * device code there, so make it before capturing a stream. All calls share
+ * the array: calls that overlap on the GPU race; issue them one after another.
  * No counterpart in the reference: its sorts allocate their buffers.
  */
 int rdx_sort_noalloc(const uint32_t* keys, uint64_t count, int bits, uint32_t* ordering,

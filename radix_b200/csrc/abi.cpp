@@ -1626,9 +1626,8 @@ static int read_rdxfile_header(rdx_ctx* ctx, const void* bytes, uint64_t nbytes,
   return err ? fail(ctx, RDX_ERR_ARG, "%s", err) : RDX_OK;
 }
 
-int rdx_rdxfile_read_info(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx_rdxfile_info* info,
-                          rdx_rdxfile_channel* channels, int capacity, char* header_json, uint64_t json_capacity) {
-  if (!ctx || !info) return RDX_ERR_ARG;
+static int rdxfile_read_info(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx_rdxfile_info* info,
+                             rdx_rdxfile_channel* channels, int capacity, char* header_json, uint64_t json_capacity) {
   cudaSetDevice(ctx->device);
   rdx::RdxFile f;
   int s = read_rdxfile_header(ctx, bytes, nbytes, &f);
@@ -1656,8 +1655,30 @@ int rdx_rdxfile_read_info(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx_
   return RDX_OK;
 }
 
+// A malformed file may ask for more host memory than there is: no C++
+// exception crosses the C ABI, it becomes an error status and text
+int rdx_rdxfile_read_info(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, rdx_rdxfile_info* info,
+                          rdx_rdxfile_channel* channels, int capacity, char* header_json, uint64_t json_capacity) {
+  if (!ctx || !info) return RDX_ERR_ARG;
+  try {
+    return rdxfile_read_info(ctx, bytes, nbytes, info, channels, capacity, header_json, json_capacity);
+  } catch (const std::exception& e) {
+    return fail(ctx, RDX_ERR_NOMEM, "RDX header: %s", e.what());
+  }
+}
+
+static int decode_rdxfile(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, void* const* channels);
+
 int rdx_decode_rdxfile(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, void* const* channels) {
   if (!ctx) return RDX_ERR_ARG;
+  try {
+    return decode_rdxfile(ctx, bytes, nbytes, channels);
+  } catch (const std::exception& e) {
+    return fail(ctx, RDX_ERR_NOMEM, "RDX decode: %s", e.what());
+  }
+}
+
+static int decode_rdxfile(rdx_ctx* ctx, const void* bytes, uint64_t nbytes, void* const* channels) {
   cudaSetDevice(ctx->device);
   rdx::RdxFile f;
   int s = read_rdxfile_header(ctx, bytes, nbytes, &f);

@@ -17,6 +17,9 @@
 // advances the epoch, so words of earlier calls never match. Two calls that
 // overlap on the GPU (different streams, or different host threads) race on
 // that array: issue them one after another.
+//
+// A bounded device wait that gave up is reported only through *visible
+// (0xffffffff): with visible == NULL the call has no way to report it.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -28,7 +31,6 @@ namespace {
 
 constexpr uint64_t kNoAllocMaxKeys = 1ull << 20;
 constexpr uint32_t kNoAllocMaxTiles = (uint32_t)(kNoAllocMaxKeys / kSortTile);
-constexpr int kMaxDevices = 64;
 
 // Byte offsets inside the array (every region 256-byte aligned)
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -48,11 +50,9 @@ constexpr size_t kLookbackBytes = (size_t)kMaxPasses * kNoAllocMaxTiles * kRadix
 constexpr size_t kScratchBytes = kLookbackOff + kLookbackBytes;
 
 // The scratch. In host code `g_noalloc_scratch` only names the symbol; its
-// device address comes from cudaGetSymbolAddress, once per device.
+// device address comes from cudaGetSymbolAddress with the device current.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// Device address of g_noalloc_scratch on each device (null: not looked up yet)
-unsigned char* g_base[kMaxDevices];
 
 // Segment descriptors of one n-key sort, and the error flag cleared
 __global__ void k_noalloc_prepare(uint64_t* begin, uint64_t* end, uint32_t* tiles, uint64_t n, uint32_t* flag) {
@@ -98,18 +98,16 @@ extern "C" int rdx_sort_noalloc(const uint32_t* keys, uint64_t count, int bits, 
   }
   if (!keys || !ordering || !on_device(keys) || !on_device(ordering) || (visible && !on_device(visible)))
     return RDX_ERR_ARG;
-  int device = 0;
-  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) return RDX_ERR_CUDA;
-  if (!g_base[device]) {
-    // First call on this device: the symbol's device address, with the device current
-    void* ptr = nullptr;
-    if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
-      cudaGetLastError();
-      return RDX_ERR_CUDA;
-    }
-    g_base[device] = reinterpret_cast<unsigned char*>(ptr);
+  // The array's address on the current device, looked up on every call: the
+  // lookup allocates nothing, and no cached address can outlive its context
+  // (after a cudaDeviceReset the array lives at a new address). The first
+  // call on a device loads the library's device code there.
+  void* ptr = nullptr;
+  if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr) {
+    cudaGetLastError();
+    return RDX_ERR_CUDA;
   }
-  unsigned char* b = g_base[device];
+  unsigned char* b = reinterpret_cast<unsigned char*>(ptr);
   const int passes = bits / 8;
   SortScratch sc{};
   uint32_t* small = reinterpret_cast<uint32_t*>(b + kSmallOff);

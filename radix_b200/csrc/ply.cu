@@ -433,9 +433,11 @@ const char* parse_ply_header(const unsigned char* head, uint64_t head_bytes, uin
           g_error = "PLY element " + b.name + " before " + el->name + " has list properties";
           return g_error.c_str();
         }
+      // each product checked by a division first, so no count wraps past the file's end
+      if (off > nbytes || (b.record && b.count > (nbytes - off) / b.record)) return "PLY file ended unexpectedly";
       off += b.count * b.record;
     }
-    if (off + el->count * el->record > nbytes) return "PLY file ended unexpectedly";
+    if (off > nbytes || (el->record && el->count > (nbytes - off) / el->record)) return "PLY file ended unexpectedly";
     *out = off;
     return nullptr;
   };
@@ -448,6 +450,10 @@ const char* parse_ply_header(const unsigned char* head, uint64_t head_bytes, uin
     if (e.name == "sh" && !sh) sh = &e;
   }
   if (!vertex) return "PLY has no vertex element";
+  // splat indices are 32-bit on the device (as in SPZ files)
+  if (vertex->count > 0x7fffffffull) return "PLY vertex count above 2^31 - 1";
+  for (const Element& e : elements)
+    if (e.count > 0x7fffffffull) return "PLY element count above 2^31 - 1";
   d->count = vertex->count;
   d->record = vertex->record;
   uint64_t off = 0;

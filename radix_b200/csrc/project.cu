@@ -31,14 +31,18 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
+
 #include "device_common.cuh"
 #include "rdx_internal.h"
 
 namespace rdx {
 namespace {
 
-constexpr int kWarps = 4;              // warps per block
-constexpr int kThreads = kWarps * 32;  // 128
+constexpr int kWarps = 4;                // warps per block unless a launch asks otherwise
+constexpr int kMaxWarps = 8;             // the most warps per block a launch may ask for
+constexpr int kMaxThreads = kMaxWarps * 32;
 constexpr int kChunk = kProjTile;      // splats per chunk (a warp's phase 1)
 constexpr int kQueue = 64;             // candidate ring of a warp
 static_assert(kChunk == 32, "a chunk is one warp wide");
@@ -393,7 +397,7 @@ struct WarpSmem {
 };
 
 template <int LAYOUT, int DEG, int VAR, int EYES>
-__global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict__ descs, int n_desc, uint32_t total_chunks,
+__global__ void __launch_bounds__(kMaxThreads) k_project(const ProjDesc* __restrict__ descs, int n_desc, uint32_t total_chunks,
                                                       ProjOutputs out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -635,8 +639,9 @@ __global__ void __launch_bounds__(kThreads) k_project(const ProjDesc* __restrict
     __syncwarp();
   };
 
-  const uint32_t gw = blockIdx.x * kWarps + (uint32_t)warp;
-  const uint32_t nw = gridDim.x * kWarps;
+  const uint32_t wpb = blockDim.x >> 5;  // warps per block (independent of one another)
+  const uint32_t gw = blockIdx.x * wpb + (uint32_t)warp;
+  const uint32_t nw = gridDim.x * wpb;
   // One loop with a single site for each phase keeps the kernel's code small
   // (phase 2 is large; inlined at several sites it thrashes the instruction
   // cache). Each turn either runs phase 2 on a batch of queued splats or
@@ -845,9 +850,10 @@ struct Picked {
   int smem;
 };
 
+// smem: shared memory per warp (a block holds one WarpSmem per warp)
 template <int LAYOUT, int DEG, int VAR, int EYES>
 Picked picked() {
-  return {k_project<LAYOUT, DEG, VAR, EYES>, (int)(kWarps * sizeof(WarpSmem<EYES>))};
+  return {k_project<LAYOUT, DEG, VAR, EYES>, (int)sizeof(WarpSmem<EYES>)};
 }
 
 template <int LAYOUT, int DEG, int VAR>
@@ -884,26 +890,63 @@ Picked pick_kernel(const DevTable& t, int eyes) {
   }
 }
 
+// Resident blocks of one projection kernel at a block size on a device, found
+// once (with its shared-memory attribute set) and kept: launches then cost no
+// attribute or occupancy queries
+int resident_blocks(const Picked& k, int warps, int* smem, cudaError_t* err) {
+  struct Key {
+    int device;
+    ProjKernel fn;
+    int warps;
+    bool operator<(const Key& o) const {
+      return device != o.device ? device < o.device : (fn != o.fn ? fn < o.fn : warps < o.warps);
+    }
+  };
+  static std::mutex mu;
+  static std::map<Key, int> cache;
+  *smem = k.smem * warps;
+  int device = 0;
+  *err = cudaGetDevice(&device);
+  if (*err != cudaSuccess) return 0;
+  const Key key{device, k.fn, warps};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  int sms = 0, per_sm = 0;
+  *err = cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem);
+  if (*err != cudaSuccess) return 0;
+  *err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (*err != cudaSuccess) return 0;
+  *err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, warps * 32, *smem);
+  if (*err != cudaSuccess) return 0;
+  const int blocks = sms * (per_sm < 1 ? 1 : per_sm);
+  std::lock_guard<std::mutex> lock(mu);
+  cache[key] = blocks;
+  return blocks;
+}
+
 }  // namespace
 
+int project_warps_supported(int warps) { return warps == 2 || warps == 4 || warps == 8; }
+
 cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host, int n_desc, uint32_t total_chunks,
-                           const ProjOutputs& out, uint32_t* error_flag, cudaStream_t stream) {
+                           const ProjOutputs& out, uint32_t* error_flag, cudaStream_t stream, int warps) {
   (void)error_flag;  // no device wait in this kernel
   if (total_chunks == 0 || n_desc == 0) return cudaSuccess;
+  if (warps == 0) warps = kWarps;
+  if (!project_warps_supported(warps)) return cudaErrorInvalidValue;
   // One kernel per launch: the caller groups objects by table kind
   const ProjDesc& d0 = descs_host[0];
   const Picked k = pick_kernel(d0.table, d0.eyes);
-  cudaError_t err = cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem);
+  int smem = 0;
+  cudaError_t err = cudaSuccess;
+  const int blocks = resident_blocks(k, warps, &smem, &err);
   if (err != cudaSuccess) return err;
-  int device = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&device);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, kThreads, k.smem);
-  if (err != cudaSuccess) return err;
-  if (per_sm < 1) per_sm = 1;
-  const uint32_t want = (total_chunks + kWarps - 1) / kWarps;
-  const uint32_t grid = min(want, (uint32_t)(sms * per_sm));
-  k.fn<<<grid, kThreads, k.smem, stream>>>(descs_dev, n_desc, total_chunks, out);
+  const uint32_t want = (total_chunks + (uint32_t)warps - 1) / (uint32_t)warps;
+  const uint32_t grid = min(want, (uint32_t)blocks);
+  k.fn<<<grid, warps * 32, smem, stream>>>(descs_dev, n_desc, total_chunks, out);
   return cudaGetLastError();
 }
 

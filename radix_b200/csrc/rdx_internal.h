@@ -357,8 +357,10 @@ struct GradsOut {
 cudaError_t launch_project_backward(const ProjDesc* descs_dev, const GradsOut* grads_dev, const ProjDesc* descs_host,
                                     int n_desc, uint32_t total_chunks, const GradsIn& in, cudaStream_t stream);
 
+// warps: warps per block (2, 4 or 8; 0: 4)
 cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host, int n_desc,
                            uint32_t total_tiles, const ProjOutputs& out,
-                           uint32_t* error_flag, cudaStream_t stream);
+                           uint32_t* error_flag, cudaStream_t stream, int warps = 0);
+int project_warps_supported(int warps);
 
 }  // namespace rdx

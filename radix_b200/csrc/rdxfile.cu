@@ -264,10 +264,25 @@ const char* read_container(const unsigned char* bytes, uint64_t n, uint32_t magi
   return nullptr;
 }
 
-uint64_t as_u64(const Json* v) { return v && v->kind == Json::kNum && v->num >= 0 ? (uint64_t)v->num : 0; }
+// A JSON number as a count: false unless it is a whole number in [0, 2^53)
+// (the integers a JavaScript writer represents exactly)
+bool as_u64(const Json* v, uint64_t* out) {
+  *out = 0;
+  if (!v || v->kind != Json::kNum || !(v->num >= 0.0) || v->num >= 9007199254740992.0) return false;
+  if (v->num != (double)(uint64_t)v->num) return false;
+  *out = (uint64_t)v->num;
+  return true;
+}
 
-// Inflate one gzip payload completely: the bytes, or -1 on a bad stream
-int64_t gunzip_all(const unsigned char* in, uint64_t n, std::vector<unsigned char>* out) {
+// Elements a chunk may hold (the reference's element indices are u32)
+constexpr uint64_t kMaxChunkElements = 0xffffffffull;
+// DEFLATE expands at most 1032:1, so a payload of n bytes inflates to fewer
+// than this: larger claims are rejected before any buffer is sized by them
+uint64_t max_inflated(uint64_t n) { return n * 1032 + 1024; }
+
+// Inflate one gzip payload completely: the bytes, or -1 on a bad stream;
+// stops (returning more than cap) once the output passes cap bytes
+int64_t gunzip_all(const unsigned char* in, uint64_t n, std::vector<unsigned char>* out, uint64_t cap) {
   z_stream zs;
   memset(&zs, 0, sizeof(zs));
   if (inflateInit2(&zs, 16 + MAX_WBITS) != Z_OK) return -1;
@@ -282,12 +297,14 @@ int64_t gunzip_all(const unsigned char* in, uint64_t n, std::vector<unsigned cha
     status = inflate(&zs, Z_NO_FLUSH);
     if (status != Z_OK && status != Z_STREAM_END) break;
     out->insert(out->end(), buf, buf + (sizeof(buf) - zs.avail_out));
+    if (out->size() > cap) break;  // more than the chunk claims: a size mismatch, not a bad stream
     if (status == Z_OK && zs.avail_in == 0 && zs.avail_out != 0) {
       status = Z_BUF_ERROR;
       break;
     }
   }
   inflateEnd(&zs);
+  if (out->size() > cap) return (int64_t)out->size();
   return status == Z_STREAM_END ? (int64_t)out->size() : -1;
 }
 
@@ -365,8 +382,9 @@ const char* rdxfile_header(const unsigned char* bytes, uint64_t nbytes, RdxFile*
   const Json* version = meta.get("version");
   if (!version || version->kind != Json::kNum || version->num != kRdxVersion)
     return error_text("RDX version %s is not 1", version && version->kind == Json::kNum ? std::to_string((long long)version->num).c_str() : "undefined");
-  f->count = as_u64(meta.get("count"));
-  f->chunk_size = as_u64(meta.get("chunkSize"));
+  if (!as_u64(meta.get("count"), &f->count)) return "RDX header without a valid count";
+  if (f->count > kMaxChunkElements) return error_text("RDX header count %s%s%llu is above 2^32 - 1", "", "", f->count);
+  if (meta.get("chunkSize") && !as_u64(meta.get("chunkSize"), &f->chunk_size)) return "RDX header with an invalid chunkSize";
   const Json* bundles = meta.get("bundles");
   if (!bundles || bundles->kind != Json::kObj) return "RDX header without bundles";
   for (const auto& b : bundles->obj) {
@@ -384,8 +402,11 @@ const char* rdxfile_header(const unsigned char* bytes, uint64_t nbytes, RdxFile*
   if (!chunks || chunks->kind != Json::kArr) return "RDX header without chunks";
   uint64_t total = length;
   for (const Json& c : chunks->arr) {
-    f->chunk_bytes.push_back(as_u64(&c));
-    total += f->chunk_bytes.back();
+    uint64_t b = 0;
+    if (!as_u64(&c, &b)) return "RDX header with an invalid chunk size";
+    if (b > nbytes - std::min(total, nbytes)) return "RDX file ended unexpectedly";
+    f->chunk_bytes.push_back(b);
+    total += b;
   }
   if (total > nbytes) return "RDX file ended unexpectedly";
   return nullptr;
@@ -434,16 +455,28 @@ const char* rdxfile_unpack(const unsigned char* bytes, uint64_t nbytes, const Rd
     std::vector<std::pair<uint64_t, uint64_t>> payloads;
     uint64_t length = 0;
     const char* err = read_container(bytes + at, f.chunk_bytes[ci], kChunkMagic, &meta, &payloads, &length);
-    const uint64_t start = as_u64(meta.get("start")), count = as_u64(meta.get("count"));
+    uint64_t start = 0, count = 0;
     if (err) {
       parse_error = err;
-    } else if (start + count > f.count) {
+    } else if (!as_u64(meta.get("start"), &start) || !as_u64(meta.get("count"), &count)) {
+      parse_error = error_text("RDX chunk %s%s%llu without a valid start and count", "", "", (uint64_t)ci);
+    } else if (count > kMaxChunkElements) {
+      parse_error = error_text("RDX chunk %s%s%llu holds %llu elements (at most 2^32 - 1)", "", "", (uint64_t)ci, count);
+    } else if (start > f.count || count > f.count - start) {
       parse_error = error_text("RDX chunk at %s%s%llu runs past the %llu elements", "", "", start, f.count);
     } else if (payloads.size() != f.channels.size()) {
       parse_error = error_text("RDX chunk %s%s%llu holds %llu payloads", "", "", (uint64_t)ci, (uint64_t)payloads.size());
     } else {
-      for (size_t k = 0; k < f.channels.size(); k++) {
+      for (size_t k = 0; k < f.channels.size() && !parse_error; k++) {
         const uint64_t eb = (uint64_t)f.channels[k].element_bytes;
+        if (count * eb > max_inflated(payloads[k].second)) {
+          // more bytes than the payload can inflate to: refused before any buffer is sized by it
+          const RdxChannel& ch = f.channels[k];
+          parse_error = error_text("Chunk at %s: %s expects %llu bytes from a %llu-byte payload",
+                                   std::to_string(start).c_str(), (ch.bundle + "." + ch.label).c_str(), count * eb,
+                                   payloads[k].second);
+          break;
+        }
         Payload j{bytes + at + payloads[k].first, payloads[k].second, count * eb, start, total, (int)k,
                   wanted[k] && count > 0};
         if (j.keep) {
@@ -456,17 +489,27 @@ const char* rdxfile_unpack(const unsigned char* bytes, uint64_t nbytes, const Rd
     }
     at += f.chunk_bytes[ci];
   }
-  staged->resize(total);
+  try {
+    staged->resize(total);
+  } catch (const std::exception&) {
+    return error_text("RDX file needs %s%s%llu bytes of host memory to inflate", "", "", total);
+  }
+  constexpr int64_t kNoMemory = -2;
   std::vector<int64_t> got(jobs.size(), 0);
   parallel_for(jobs.size(), packed, [&](size_t q) {
     const Payload& j = jobs[q];
-    std::vector<unsigned char> buf;
-    buf.reserve(j.expect);
-    got[q] = gunzip_all(j.in, j.size, &buf);
-    if (j.keep && got[q] == (int64_t)j.expect) memcpy(staged->data() + j.dst, buf.data(), buf.size());
+    try {
+      std::vector<unsigned char> buf;
+      buf.reserve(j.expect);
+      got[q] = gunzip_all(j.in, j.size, &buf, j.expect);
+      if (j.keep && got[q] == (int64_t)j.expect) memcpy(staged->data() + j.dst, buf.data(), buf.size());
+    } catch (const std::exception&) {
+      got[q] = kNoMemory;  // no exception leaves a worker thread
+    }
   });
   for (size_t q = 0; q < jobs.size(); q++) {
     const Payload& j = jobs[q];
+    if (got[q] == kNoMemory) return "RDX payload could not be inflated: out of host memory";
     if (got[q] < 0) return "RDX payload is not a gzip stream";
     if ((uint64_t)got[q] != j.expect) {
       const RdxChannel& ch = f.channels[j.channel];

@@ -1,15 +1,16 @@
 """Write tests/golden/kats.json: the known answers and tolerances that the
 reference's own checks hold for this path, with the file:line of each.
 
-Run from the repository root. When the reference sources are at
-/root/reference, every cited line is read and checked to contain the quoted
-text, so the fixture cannot drift from its source.
+Run from the repository root as `python tests/golden/make_kats.py [REFERENCE]`,
+where REFERENCE is the reference project's root (or set RADIX_REFERENCE).
+When it is given and present, every cited line is read and checked to contain
+the quoted text, so the fixture cannot drift from its source.
 """
 import json
 import os
 import sys
 
-REF = "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("RADIX_REFERENCE", "")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 KATS = {
