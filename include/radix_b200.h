@@ -223,6 +223,27 @@ int rdx_version(void);
 #define RDX_PHASES 5
 int rdx_ctx_set_profiling(rdx_ctx* ctx, int on);
 int rdx_ctx_phase_times(rdx_ctx* ctx, double* ms, uint64_t* runs);
+/*
+ * Bounded device waits of this context's sorts. `polls`: how often a wait on
+ * another tile's lookback word is polled before it gives up, sets the
+ * context's error flag and lets its kernel finish (0: 2^22, the default);
+ * the call that synchronises (or rdx_ctx_synchronize) then returns
+ * RDX_ERR_TIMEOUT, and the context stays usable. `silent_pass` >= 0 is a test
+ * hook: in the next sort only, the first tile of that digit pass publishes no
+ * lookback word, so its successors' waits run out. A batch takes `polls` when
+ * it is created. No counterpart in the reference, whose sorts throw on
+ * misuse (WgpuRadixSort.ts:150-152) and have no device waits.
+ */
+int rdx_ctx_set_wait(rdx_ctx* ctx, uint32_t polls, int silent_pass);
+/*
+ * How this context's one-segment sorts run their digit passes: -1 chosen by
+ * size (the default), 0 one onesweep kernel per pass, 1-3 one cooperative
+ * kernel for every pass (1: 1024 threads x 16 keys per block, 2: 512 x 16,
+ * 3: 1024 x 8). Every variant gives the same order. A batch takes the choice
+ * when it is created. No counterpart in the reference (its radix sort takes
+ * keysPerThread 8 or 16, WgpuRadixSort.ts:80-91).
+ */
+int rdx_ctx_set_sort_variant(rdx_ctx* ctx, int variant);
 /* Kernels this context has launched since it was created. */
 int rdx_ctx_launches(rdx_ctx* ctx, uint64_t* launches);
 

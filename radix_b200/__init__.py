@@ -109,6 +109,16 @@ class Context:
         """Record CUDA events around each phase (project, sort, copies) of later calls."""
         _abi.check(_abi.lib().rdx_ctx_set_profiling(self.handle, 1 if on else 0), self.handle)
 
+    def set_wait(self, polls=0, silent_pass=-1):
+        """Polls of a bounded device wait before it gives up (0: the default), and
+        the test hook that silences the first tile of one digit pass of the next sort."""
+        _abi.check(_abi.lib().rdx_ctx_set_wait(self.handle, int(polls), int(silent_pass)), self.handle)
+
+    def set_sort_variant(self, variant=-1):
+        """Digit passes of one-segment sorts: -1 by size, 0 onesweep kernels,
+        1-3 a cooperative kernel (1024x16, 512x16, 1024x8 threads x keys)."""
+        _abi.check(_abi.lib().rdx_ctx_set_sort_variant(self.handle, int(variant)), self.handle)
+
     def phase_times(self):
         """{phase: (summed ms, runs)} since the last read (waits for the stream)."""
         ms = (ctypes.c_double * _abi.RDX_PHASES)()

@@ -174,6 +174,8 @@ SIGNATURES = {
     "rdx_ctx_reserve": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "rdx_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "rdx_ctx_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "rdx_ctx_set_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int]),
+    "rdx_ctx_set_sort_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "rdx_ctx_phase_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_ctx_launches": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_sort_keys_compute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),

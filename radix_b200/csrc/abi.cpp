@@ -51,6 +51,13 @@ struct rdx_ctx {
   // device word (error_flag + 1) that each sort advances on the device.
   uint64_t* lookback = nullptr;
   size_t lookback_words = 0;
+  // Bounded device waits: polls before a wait gives up (0: the default), and
+  // the one-shot test hook that silences a digit pass's first tile
+  uint32_t spin_limit = 0;
+  int silent_pass = -1;
+  // Digit passes of one-segment sorts: -1 chosen by size, 0 the onesweep
+  // passes, else a cooperative variant (rdx::kCoop*)
+  int sort_variant = -1;
 };
 
 static const size_t kRingBytes = 4u << 20;
@@ -215,6 +222,7 @@ rdx::SortScratch take_sort_scratch(Arena& a, int segments, int passes, uint64_t 
   s.vals_a = a.take<uint32_t>(total);
   s.keys_b = a.take<uint32_t>(total);
   s.vals_b = a.take<uint32_t>(total);
+  s.block_counts = segments == 1 ? a.take<uint32_t>((size_t)rdx::kMaxCoopBlocks * rdx::kRadix) : nullptr;
   return s;
 }
 
@@ -686,6 +694,16 @@ int check_objects(rdx_ctx* ctx, const rdx_object* objects, int n_objects) {
   return RDX_OK;
 }
 
+// Keys up to which a one-segment sort takes the cooperative digit passes by default
+constexpr uint64_t kCoopDefaultMaxKeys = 1ull << 23;
+
+// The digit-pass variant of a sort of `segments` segments and `n` keys
+int sort_variant(const rdx_ctx* ctx, int segments, uint64_t n) {
+  if (segments != 1) return rdx::kCoopNone;
+  if (ctx->sort_variant >= 0) return ctx->sort_variant;
+  return n <= kCoopDefaultMaxKeys ? rdx::kCoop1024x16 : rdx::kCoopNone;
+}
+
 // Enqueue one sort (every pass); it takes a fresh lookback epoch on the device
 int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
              const SegBufs& sb, int segments, uint32_t max_tiles, int bits, const rdx::SortScratch& sc,
@@ -706,6 +724,10 @@ int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uin
   c.lookback_words = ctx->lookback_words;
   c.epoch = ctx->error_flag + 1;
   c.error_flag = ctx->error_flag;
+  c.spin_limit = ctx->spin_limit;
+  c.silent_pass = ctx->silent_pass;
+  ctx->silent_pass = -1;  // one sort only
+  c.coop = sort_variant(ctx, segments, (uint64_t)max_tiles * rdx::kSortTile);
   int launches = 0;
   RDX_CUDA(rdx::sort_segments(c, ctx->stream, &launches), "sort launch");
   ctx->launches += (uint64_t)launches;
@@ -807,6 +829,21 @@ int rdx_ctx_reserve(rdx_ctx* ctx, uint64_t max_keys) {
   a.take<uint32_t>(max_keys * 3);  // keys / staged buffers of a frame or splat sort
   int st = ensure_arena(ctx, a.used);
   return st != RDX_OK ? st : ensure_lookback(ctx, (size_t)4 * lookback_tiles(tiles_of(max_keys)) * rdx::kRadix);
+}
+
+int rdx_ctx_set_wait(rdx_ctx* ctx, uint32_t polls, int silent_pass) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (silent_pass >= rdx::kMaxPasses) return fail(ctx, RDX_ERR_ARG, "silent_pass %d (at most %d)", silent_pass, rdx::kMaxPasses - 1);
+  ctx->spin_limit = polls;
+  ctx->silent_pass = silent_pass < 0 ? -1 : silent_pass;
+  return RDX_OK;
+}
+
+int rdx_ctx_set_sort_variant(rdx_ctx* ctx, int variant) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (variant < -1 || variant >= rdx::kCoopVariants) return fail(ctx, RDX_ERR_ARG, "sort variant %d", variant);
+  ctx->sort_variant = variant;
+  return RDX_OK;
 }
 
 int rdx_ctx_set_profiling(rdx_ctx* ctx, int on) {
@@ -1141,6 +1178,9 @@ struct FrameDev {
   uint64_t* lookback = nullptr;
   uint64_t lookback_words = 0;
   uint32_t* error_flag = nullptr;  // word 0: the error flag, word 1: the lookback epoch
+  uint32_t spin_limit = 0;         // polls of a bounded wait (0: the default)
+  int silent_pass = -1;            // test hook (see rdx_ctx_set_wait)
+  int coop = 0;                    // the digit passes' variant (rdx::kCoop*)
 };
 
 // Enqueue a planned frame on `stream`: the projection, then the segmented sort
@@ -1181,6 +1221,9 @@ cudaError_t enqueue_frame(rdx_ctx* timing, const ProjectCall& call, const FrameD
     c.lookback_words = fd.lookback_words;
     c.epoch = fd.error_flag + 1;
     c.error_flag = fd.error_flag;
+    c.spin_limit = fd.spin_limit;
+    c.silent_pass = fd.silent_pass;
+    c.coop = fd.coop;
     int n_launch = 0;
     e = rdx::sort_segments(c, stream, &n_launch);
     *launches += (uint64_t)n_launch;
@@ -1305,6 +1348,12 @@ int frame_common(rdx_ctx* ctx, const ViewRef* views, int n_views, const rdx_para
   fd.lookback = ctx->lookback;
   fd.lookback_words = ctx->lookback_words;
   fd.error_flag = ctx->error_flag;
+  fd.spin_limit = ctx->spin_limit;
+  fd.coop = sort_variant(ctx, n_views, n);
+  if (sort && n > 0) {
+    fd.silent_pass = ctx->silent_pass;
+    ctx->silent_pass = -1;  // one sort only
+  }
   RDX_CUDA(enqueue_frame(ctx, call, fd, sort_bits, sort, ctx->stream, &ctx->launches), "frame launch");
   if (sort && visible) {
     RDX_CUDA(cudaMemcpyAsync(visible, fd.vis, (size_t)n_views * 4,
@@ -1821,6 +1870,8 @@ int rdx_batch_create(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx
   b->fd.lookback = b->lookback;
   b->fd.lookback_words = lookback_words;
   b->fd.error_flag = b->words;
+  b->fd.spin_limit = ctx->spin_limit;
+  b->fd.coop = sort_variant(ctx, n_views, n);
   // descriptors and segments stay in the batch's memory; the graph only reads them
   std::vector<uint32_t> tiles;
   segment_tiles(b->call, &tiles);

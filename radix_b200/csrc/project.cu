@@ -715,59 +715,79 @@ __global__ void __launch_bounds__(kMaxThreads) k_project(const ProjDesc* __restr
       const bool invisible = op <= 0.0 || op < (double)p.min_alpha || degenerate;
       bool guarded = true;
       if (p.sort_guard > 0.0f && !invisible) {
-        // inSortGuard (projection.tsl.ts:145-155), cov form, float32: the head-space
-        // covariance's largest diagonal element
-        float inflate = 1.0f;
+        // inSortGuard (projection.tsl.ts:145-155), cov form: the head-space
+        // covariance's largest diagonal element. float64 with every operation
+        // explicitly rounded, in the oracle's order, so the guard's decisions
+        // (and the keys) are the oracle's
+        double inflate2 = 1.0;
         if (opac > 1.0f && p.lod_inflate) {
-          const float o = fminf(opac * 4.0f - 3.0f, 5.0f);
-          inflate = expf((o * o - 1.0f) * (1.0f / (3.0f * 2.718281828459045f)));
+          const double o = fmin(dadd(dmul((double)opac, 4.0), -3.0), 5.0);
+          const double inflate = pow(exp(__ddiv_rn(dadd(dmul(o, o), -1.0), 2.71828182845904523536)), 1.0 / 3.0);
+          inflate2 = dmul(inflate, inflate);
         }
-        float ext2 = 0.0f;
+        double cv[9];  // object-space covariance, row-major
         if constexpr (LAYOUT == RDX_LAYOUT_COV) {
-          double cv[6];
-          load_cov(sd.table, i, cv);
-#pragma unroll
-          for (int r = 0; r < 3; r++) {
-            const float a0 = (float)sd.a[r * 4 + 0], a1 = (float)sd.a[r * 4 + 1], a2 = (float)sd.a[r * 4 + 2];
-            const float v = a0 * a0 * (float)cv[0] + a1 * a1 * (float)cv[1] + a2 * a2 * (float)cv[2] +
-                            2.0f * (a0 * a1 * (float)cv[3] + a0 * a2 * (float)cv[4] + a1 * a2 * (float)cv[5]);
-            ext2 = fmaxf(ext2, v * inflate * inflate);
-          }
+          double c6[6];
+          load_cov(sd.table, i, c6);
+          cv[0] = c6[0], cv[1] = c6[3], cv[2] = c6[4];
+          cv[3] = c6[3], cv[4] = c6[1], cv[5] = c6[5];
+          cv[6] = c6[4], cv[7] = c6[5], cv[8] = c6[2];
         } else {
-          double qd[4];
-          load_quat<LAYOUT>(sd.table, i, qd);
-          float qx = (float)qd[0], qy = (float)qd[1], qz = (float)qd[2], qw = (float)qd[3];
-          const float ql2 = qx * qx + qy * qy + qz * qz + qw * qw;
-          const float qi = ql2 > 0.0f ? rsqrtf(ql2) : 0.0f;
-          qx *= qi;
-          qy *= qi;
-          qz *= qi;
-          qw = ql2 > 0.0f ? qw * qi : 1.0f;
-          const float R[9] = {1.f - 2.f * (qy * qy + qz * qz), 2.f * (qx * qy - qw * qz), 2.f * (qx * qz + qw * qy),
-                              2.f * (qx * qy + qw * qz), 1.f - 2.f * (qx * qx + qz * qz), 2.f * (qy * qz - qw * qx),
-                              2.f * (qx * qz - qw * qy), 2.f * (qy * qz + qw * qx), 1.f - 2.f * (qx * qx + qy * qy)};
-          const float sx = expf((float)ls[0]) * inflate, sy = expf((float)ls[1]) * inflate,
-                      sz = expf((float)ls[2]) * inflate;
-#pragma unroll
-          for (int r = 0; r < 3; r++) {
-            const float a0 = (float)sd.a[r * 4 + 0], a1 = (float)sd.a[r * 4 + 1], a2 = (float)sd.a[r * 4 + 2];
-            const float g0 = (a0 * R[0] + a1 * R[3] + a2 * R[6]) * sx;
-            const float g1 = (a0 * R[1] + a1 * R[4] + a2 * R[7]) * sy;
-            const float g2 = (a0 * R[2] + a1 * R[5] + a2 * R[8]) * sz;
-            ext2 = fmaxf(ext2, g0 * g0 + g1 * g1 + g2 * g2);
+          // M = R(q) diag(s) (math.tsl.ts:26-44), Sigma = M M^T
+          double q[4];
+          load_quat<LAYOUT>(sd.table, i, q);
+          double qx = q[0], qy = q[1], qz = q[2], qw = q[3];
+          const double ql = __dsqrt_rn(dadd(dadd(dadd(dmul(qx, qx), dmul(qy, qy)), dmul(qz, qz)), dmul(qw, qw)));
+          if (!(ql > 0.0)) {
+            qx = qy = qz = 0.0;
+            qw = 1.0;
+          } else {
+            qx = __ddiv_rn(qx, ql);
+            qy = __ddiv_rn(qy, ql);
+            qz = __ddiv_rn(qz, ql);
+            qw = __ddiv_rn(qw, ql);
           }
+          const double sx = exp(ls[0]), sy = exp(ls[1]), sz = exp(ls[2]);
+          const double M[9] = {
+              dmul(sx, dadd(1.0, -dmul(2.0, dadd(dmul(qy, qy), dmul(qz, qz))))),
+              dmul(dmul(sy, 2.0), dadd(dmul(qx, qy), -dmul(qw, qz))),
+              dmul(dmul(sz, 2.0), dadd(dmul(qx, qz), dmul(qw, qy))),
+              dmul(dmul(sx, 2.0), dadd(dmul(qx, qy), dmul(qw, qz))),
+              dmul(sy, dadd(1.0, -dmul(2.0, dadd(dmul(qx, qx), dmul(qz, qz))))),
+              dmul(dmul(sz, 2.0), dadd(dmul(qy, qz), -dmul(qw, qx))),
+              dmul(dmul(sx, 2.0), dadd(dmul(qx, qz), -dmul(qw, qy))),
+              dmul(dmul(sy, 2.0), dadd(dmul(qy, qz), dmul(qw, qx))),
+              dmul(sz, dadd(1.0, -dmul(2.0, dadd(dmul(qx, qx), dmul(qy, qy))))),
+          };
+#pragma unroll
+          for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+              cv[r * 3 + c] = dadd(dadd(dmul(M[r * 3 + 0], M[c * 3 + 0]), dmul(M[r * 3 + 1], M[c * 3 + 1])),
+                                   dmul(M[r * 3 + 2], M[c * 3 + 2]));
         }
-        const float radius = sqrtf(ext2) * p.max_std_dev;
+        // diag(A Sigma A^T) as (A Sigma) A^T, each sum left to right
+        double ext2 = 0.0;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          const double a0 = sd.a[r * 4 + 0], a1 = sd.a[r * 4 + 1], a2 = sd.a[r * 4 + 2];
+          double t[3];
+#pragma unroll
+          for (int c = 0; c < 3; c++) t[c] = dadd(dadd(dmul(a0, cv[c]), dmul(a1, cv[3 + c])), dmul(a2, cv[6 + c]));
+          const double v = dmul(dadd(dadd(dmul(t[0], a0), dmul(t[1], a1)), dmul(t[2], a2)), inflate2);
+          ext2 = r == 0 ? v : fmax(ext2, v);
+        }
+        const double radius = dmul(__dsqrt_rn(ext2), (double)p.max_std_dev);
         const double* P = sd.eye[0].proj;
-        const float clx = (float)(P[0] * hx + P[4] * hy + P[8] * hz + P[12]);
-        const float cly = (float)(P[1] * hx + P[5] * hy + P[9] * hz + P[13]);
-        const float clw = (float)(P[3] * hx + P[7] * hy + P[11] * hz + P[15]);
-        const float w = fmaxf(clw, 1e-6f);
-        const float rx = (float)P[0] * radius / w, ry = (float)P[5] * radius / w;
-        const bool inside =
-            fabsf(clx / w) - rx <= p.sort_guard + 1.0f && fabsf(cly / w) - ry <= p.sort_guard + 1.0f;
-        const bool near_head = -(float)hz <= radius;
-        guarded = (float)hz < radius && (inside || near_head);
+        const double clx = dadd(dadd(dadd(dmul(P[0], hx), dmul(P[4], hy)), dmul(P[8], hz)), P[12]);
+        const double cly = dadd(dadd(dadd(dmul(P[1], hx), dmul(P[5], hy)), dmul(P[9], hz)), P[13]);
+        const double clw = dadd(dadd(dadd(dmul(P[3], hx), dmul(P[7], hy)), dmul(P[11], hz)), P[15]);
+        const double w = fmax(clw, 1e-6);
+        const double rx = __ddiv_rn(dmul(P[0], radius), w), ry = __ddiv_rn(dmul(P[5], radius), w);
+        const double edge = dadd((double)p.sort_guard, 1.0);
+        const bool inside = dadd(fabs(__ddiv_rn(clx, w)), -rx) <= edge && dadd(fabs(__ddiv_rn(cly, w)), -ry) <= edge;
+        const bool near_head = -hz <= radius;
+        guarded = hz < radius && (inside || near_head);
       }
       kv = key_of_bits(__float_as_uint(__double2float_rn(distance)), sd.sort_bits);
       if (!cull_keys && !invisible && guarded) key = kv;

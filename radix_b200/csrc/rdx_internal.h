@@ -58,6 +58,15 @@ constexpr int kMaxPasses = 4;
 constexpr uint32_t kMaxSegmentKeys = (1u << 30) - 1u;
 // Bounded device waits: polls of a lookback word before the kernel gives up
 constexpr uint32_t kSpinLimit = 1u << 22;
+// Digit passes of a one-segment sort in one cooperative kernel (SortCall.coop):
+// threads per block x keys per thread of a sub-tile
+constexpr int kCoopNone = 0;
+constexpr int kCoop1024x16 = 1;
+constexpr int kCoop512x16 = 2;
+constexpr int kCoop1024x8 = 3;
+constexpr int kCoopVariants = 4;
+// Blocks a cooperative sort may have (2 per SM on up to 256 SMs): its per-block counts
+constexpr uint32_t kMaxCoopBlocks = 512;
 
 // Segments of one sort, in device memory: segment s is [begin[s], end[s]);
 // tiles[S + 1] is the running count of 4096-key tiles. A sort of one array is
@@ -84,6 +93,7 @@ struct SortScratch {
   uint32_t* vals_a;
   uint32_t* keys_b;
   uint32_t* vals_b;
+  uint32_t* block_counts;  // [kMaxCoopBlocks][256] of a cooperative sort (null: none)
 };
 
 // hist, valid, ref_hidden, counters and tile_valid are contiguous: words zeroed before a sort
@@ -115,8 +125,13 @@ struct SortCall {
   uint64_t lookback_words;  // its capacity
   uint32_t* epoch;
   uint32_t* error_flag;
+  uint32_t spin_limit = 0;  // polls of a bounded device wait (0: kSpinLimit)
+  int silent_pass = -1;     // a digit pass whose first tile publishes no lookback word (a test hook; -1: none)
+  int coop = kCoopNone;     // one segment: the digit passes in this cooperative variant (needs block_counts)
 };
 cudaError_t sort_segments(const SortCall& call, cudaStream_t stream, int* launches);
+// Blocks of a cooperative variant resident on the current device (0: it cannot launch)
+int coop_blocks(int variant);
 
 // ---- keys, compaction ----
 

@@ -23,6 +23,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "rdx_internal.h"
 
 namespace rdx {
@@ -343,6 +348,8 @@ struct PassArgs {
   const uint32_t* epoch;     // this sort's lookback epoch (device word)
   uint32_t* counter;
   uint32_t* error_flag;
+  uint32_t spin_limit;       // polls of a lookback word before a tile gives up
+  uint32_t silent_tile;      // a tile that publishes no lookback word (a test of the bounded wait; ~0u: none)
 };
 
 template <bool FIRST, bool WRITE_KEYS, int ITEMS>
@@ -435,7 +442,8 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   uint64_t* my_word = &a.lookback[(size_t)tile * kRadix + d];
   const uint32_t epoch = *a.epoch;
   const uint64_t ep = (uint64_t)epoch << 32;
-  st_relaxed64(my_word, ep | (local_tile == 0 ? kFlagInclusive : kFlagAggregate) | total);
+  const bool silent = tile == a.silent_tile;
+  if (!silent) st_relaxed64(my_word, ep | (local_tile == 0 ? kFlagInclusive : kFlagAggregate) | total);
 
   // Tile-local digit starts (low word) and the segment's digit offsets (high word) in one scan
   const uint32_t seg_count = a.hist[((size_t)seg * a.passes + a.place) * kRadix + d];
@@ -455,7 +463,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
       const uint64_t v = ld_relaxed64(&a.lookback[(size_t)t * kRadix + d]);
       const uint64_t flag = (v >> 32) == epoch ? (v & kFlagMask) : 0;
       if (flag == 0) {
-        if (++spins > kSpinLimit) {
+        if (++spins > a.spin_limit) {
           atomicExch(a.error_flag, 1u);
           break;
         }
@@ -466,7 +474,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
       if (flag == kFlagInclusive) break;
       t--;
     }
-    st_relaxed64(my_word, ep | kFlagInclusive | (prefix + total));
+    if (!silent) st_relaxed64(my_word, ep | kFlagInclusive | (prefix + total));
   }
   s_dest[d] = (uint32_t)seg_begin + seg_digit + prefix - tile_start;
   asm volatile("cp.async.wait_all;" ::: "memory");  // this thread's value copies have landed
@@ -513,7 +521,336 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   }
 }
 
+// ---- cooperative: every digit pass of one segment in one persistent kernel ----
+//
+// One block per SM slot, all resident (a cooperative launch). Block b owns
+// the keys [b * C, (b + 1) * C) of each pass's input (C = V / blocks, a
+// multiple of 4), in sub-tiles of THREADS * ITEMS keys. A pass: the block
+// ranks its keys (the same warp multisplit as the onesweep) and publishes its
+// 256 digit counts; after a grid barrier every block sums the earlier blocks'
+// counts per digit (its offsets, no chain of predecessors to wait on) and
+// scatters through shared memory; a second barrier ends the pass. When a
+// block's keys fit one sub-tile they stay in registers across the barrier.
+// Data written by other blocks of this kernel is read through L2 only (.cg):
+// an SM's L1 may still hold lines of the same buffer from two passes before.
+
+struct CoopArgs {
+  const uint32_t* keys_in;   // the first pass's input
+  const uint32_t* vals_in;   // null: each key's index within the segment
+  uint32_t* keys_a;          // ping-pong pairs
+  uint32_t* vals_a;
+  uint32_t* keys_b;
+  uint32_t* vals_b;
+  uint32_t* keys_out;        // the last pass's keys (null: values only)
+  uint32_t* vals_out;
+  const uint64_t* begin;     // the segment sorted: [begin[0], end[0])
+  const uint64_t* end;
+  const uint32_t* hist;      // [passes][256] digit totals of the keys sorted
+  uint32_t* block_counts;    // [blocks][256]
+  uint32_t* barrier;         // grid-barrier arrivals of this sort (zero at its start)
+  uint32_t* error_flag;
+  uint32_t key_mask;
+  int passes;
+  int drop;                  // the first pass reads the partition's A buffers (ping-pong B, A, ...)
+  uint32_t spin_limit;
+  int silent_pass;           // test hook: block 0 does not arrive at that pass's first barrier
+};
+
+__device__ __forceinline__ uint32_t ld_acquire32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid-wide barrier (every block resident): the sort's `count`-th. A wait is
+// bounded: after spin_limit polls the block sets the error flag and goes on.
+__device__ __forceinline__ void grid_barrier(const CoopArgs& a, uint32_t target, bool arrive) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (arrive) atomicAdd(a.barrier, 1u);
+    uint32_t spins = 0;
+    while (ld_acquire32(a.barrier) < target) {
+      if (++spins > a.spin_limit) {
+        atomicExch(a.error_flag, 1u);
+        break;
+      }
+      if (spins > 16) __nanosleep(64);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// Exclusive scan of one value per digit (threads 0-255; the others pass 0 and
+// get 0) over a block of THREADS; warp_sums: 8 words of shared memory
+template <int THREADS>
+__device__ __forceinline__ uint32_t digit_exclusive_scan(uint32_t v, uint32_t* warp_sums) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (warp < kRadix / 32 && lane == 31) warp_sums[warp] = x;
+  __syncthreads();
+  uint32_t before = 0;
+  if (warp < kRadix / 32) {
+#pragma unroll
+    for (int w = 0; w < kRadix / 32; w++) before += w < warp ? warp_sums[w] : 0u;
+  }
+  __syncthreads();
+  return warp < kRadix / 32 ? before + x - v : 0u;
+}
+
+template <int THREADS, int ITEMS>
+struct CoopShape {
+  static constexpr int kWarps = THREADS / 32;
+  static constexpr uint32_t kSub = THREADS * ITEMS;  // keys of a sub-tile
+  // shared words: per-warp digit counts, exchange, values, and 256-word tables
+  static constexpr size_t kWords = (size_t)kWarps * kRadix + 2 * (size_t)kSub + 8 * kRadix + 32;
+  static constexpr size_t kBytes = kWords * 4;
+};
+
+template <int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs a) {
+  using Shape = CoopShape<THREADS, ITEMS>;
+  constexpr int kWarps = Shape::kWarps;
+  constexpr uint32_t kSub = Shape::kSub;
+  extern __shared__ __align__(16) uint32_t smem[];
+  uint32_t* s_whist = smem;                            // [warps][256]: counts, then exclusive over warps
+  uint32_t* s_exchange = s_whist + kWarps * kRadix;    // [kSub]
+  uint32_t* s_vals = s_exchange + kSub;                // [kSub]: the sub-tile's values (cp.async)
+  uint32_t* s_cnt = s_vals + kSub;                     // [256] the sub-tile's digit counts
+  uint32_t* s_start = s_cnt + kRadix;                  // [256] their exclusive scan (tile-local starts)
+  uint32_t* s_blk = s_start + kRadix;                  // [256] the block's digit counts of this pass
+  uint32_t* s_base = s_blk + kRadix;                   // [256] the next destination of each digit
+  uint32_t* s_part = s_base + kRadix;                  // [4][256] partial sums over earlier blocks
+  uint32_t* s_wsum = s_part + 4 * kRadix;              // [8] scan scratch
+
+  const int tid = threadIdx.x;
+  const int lane = tid & 31;
+  const int warp = tid >> 5;
+  const uint32_t G = gridDim.x;
+  const uint32_t b = blockIdx.x;
+  const uint64_t seg_begin = a.begin[0];
+  const uint32_t V = (uint32_t)min(a.end[0] - seg_begin, (uint64_t)kMaxSegmentKeys);
+  const uint32_t C = (((V + G - 1) / G) + 3u) & ~3u;
+  const uint32_t lo = min(b * C, V);
+  const uint32_t len = min(C, V - lo);
+  const uint32_t nsub = (len + kSub - 1) / kSub;
+  const uint32_t warp_base = (uint32_t)warp * (ITEMS * 32);
+  const uint32_t lt = lanemask_lt();
+  uint32_t key[ITEMS], rank[ITEMS];
+  uint32_t barriers = 0;
+  const uint32_t* kin = a.keys_in;
+  const uint32_t* vin = a.vals_in;
+
+  // Load sub-tile `sub` (keys to registers, values to s_vals when `vals`) and
+  // rank it: rank[j] = earlier items of its digit in the warp, s_cnt = the
+  // sub-tile's counts, s_start their exclusive scan, s_whist exclusive over warps
+  auto load_rank = [&](uint32_t sub, int shift, bool vals) -> uint32_t {
+    const uint64_t start = seg_begin + lo + (uint64_t)sub * kSub;
+    const uint32_t n = min(kSub, len - sub * kSub);
+    for (int w = tid; w < kWarps * kRadix; w += THREADS) s_whist[w] = 0;
+    if (vals && vin) {
+      // whole 16-byte groups of values straight to shared memory (L2 only); the tail at use
+      const bool vec = (reinterpret_cast<uintptr_t>(vin + start) & 15u) == 0;
+      const uint32_t groups = vec ? n / 4 : 0;
+      for (uint32_t g = tid; g < groups; g += THREADS) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(&s_vals[4 * g])),
+                     "l"(vin + start + 4 * g)
+                     : "memory");
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    }
+#pragma unroll
+    for (int j = 0; j < ITEMS; j++) {
+      const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+      key[j] = pos < n ? __ldcg(&kin[start + pos]) & a.key_mask : 0u;
+    }
+    __syncthreads();  // s_whist cleared
+#pragma unroll
+    for (int j = 0; j < ITEMS; j++) {
+      const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+      const bool ranked = pos < n;
+      const uint32_t d = ranked ? (key[j] >> shift) & 0xffu : kNotRanked;
+      const uint32_t peers = peers_of(d, ranked);
+      const int leader = __ffs(peers) - 1;
+      uint32_t old = 0;
+      uint32_t* h = s_whist + warp * kRadix;
+      if (lane == leader && d != kNotRanked) {
+        old = h[d];
+        h[d] = old + (uint32_t)__popc(peers);
+      }
+      old = __shfl_sync(0xffffffffu, old, leader);
+      rank[j] = old + (uint32_t)__popc(peers & lt);
+      __syncwarp();
+    }
+    __syncthreads();
+    uint32_t total = 0;
+    if (tid < kRadix) {
+      for (int w = 0; w < kWarps; w++) {
+        const uint32_t c = s_whist[w * kRadix + tid];
+        s_whist[w * kRadix + tid] = total;
+        total += c;
+      }
+      s_cnt[tid] = total;
+    }
+    const uint32_t st = digit_exclusive_scan<THREADS>(tid < kRadix ? total : 0u, s_wsum);
+    if (tid < kRadix) s_start[tid] = st;
+    __syncthreads();
+    return n;
+  };
+
+  for (int place = 0; place < a.passes; place++) {
+    const int shift = 8 * place;
+    const bool last = place == a.passes - 1;
+    const bool to_a = a.drop ? (place & 1) != 0 : (place & 1) == 0;
+    uint32_t* kout = last ? a.keys_out : (to_a ? a.keys_a : a.keys_b);
+    uint32_t* vout = last ? a.vals_out : (to_a ? a.vals_a : a.vals_b);
+
+    // The block's digit counts of this pass
+    if (tid < kRadix) s_blk[tid] = 0;
+    for (uint32_t sub = 0; sub < nsub; sub++) {
+      load_rank(sub, shift, nsub == 1);
+      if (tid < kRadix) s_blk[tid] += s_cnt[tid];
+    }
+    __syncthreads();
+    if (tid < kRadix) __stcg(&a.block_counts[(size_t)b * kRadix + tid], s_blk[tid]);
+    barriers++;
+    grid_barrier(a, barriers * G, !(place == a.silent_pass && b == 0));
+
+    // Offsets: the digit's start in the segment plus the earlier blocks' counts of it
+    {
+      constexpr int kQuarters = THREADS >= 4 * kRadix ? 4 : THREADS / kRadix;
+      const int q = tid / kRadix, d = tid % kRadix;
+      if (q < kQuarters) {
+        uint32_t sum = 0;
+        const uint32_t per = (b + kQuarters - 1) / kQuarters;
+        const uint32_t from = min((uint32_t)q * per, b), to = min(from + per, b);
+#pragma unroll 8
+        for (uint32_t e = from; e < to; e++) sum += __ldcg(&a.block_counts[(size_t)e * kRadix + d]);
+        s_part[q * kRadix + d] = sum;
+      }
+      const uint32_t total = tid < kRadix ? a.hist[place * kRadix + tid] : 0u;
+      const uint32_t digit_start = digit_exclusive_scan<THREADS>(total, s_wsum);  // syncs the partials too
+      if (tid < kRadix) {
+        uint32_t before = 0;
+#pragma unroll
+        for (int k = 0; k < kQuarters; k++) before += s_part[k * kRadix + tid];
+        s_base[tid] = (uint32_t)seg_begin + digit_start + before;
+      }
+      __syncthreads();
+    }
+
+    // Scatter, sub-tile by sub-tile in order
+    const uint32_t seg_end = (uint32_t)seg_begin + V;
+    for (uint32_t sub = 0; sub < nsub; sub++) {
+      const uint32_t n = nsub == 1 ? min(kSub, len) : load_rank(sub, shift, true);
+      const uint64_t start = seg_begin + lo + (uint64_t)sub * kSub;
+#pragma unroll
+      for (int j = 0; j < ITEMS; j++) {
+        const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+        if (pos < n) {
+          const uint32_t dj = (key[j] >> shift) & 0xffu;
+          rank[j] += s_start[dj] + s_whist[warp * kRadix + dj];
+          s_exchange[rank[j]] = key[j];
+        } else {
+          rank[j] = 0xffffffffu;
+        }
+      }
+      __syncthreads();
+      uint32_t dest[ITEMS];
+#pragma unroll
+      for (int k = 0; k < ITEMS; k++) {
+        const uint32_t i = (uint32_t)k * THREADS + tid;
+        dest[k] = 0xffffffffu;
+        if (i < n) {
+          const uint32_t kk = s_exchange[i];
+          const uint32_t dd = (kk >> shift) & 0xffu;
+          const uint32_t dst = s_base[dd] + (i - s_start[dd]);
+          if (dst >= (uint32_t)seg_begin && dst < seg_end) {  // in bounds even if a wait gave up
+            dest[k] = dst;
+            if (kout) kout[dst] = kk;
+          }
+        }
+      }
+      if (vin) asm volatile("cp.async.wait_all;" ::: "memory");
+      __syncthreads();
+      const bool vec = vin && (reinterpret_cast<uintptr_t>(vin + start) & 15u) == 0;
+      const uint32_t staged = vec ? (n & ~3u) : 0u;
+#pragma unroll
+      for (int j = 0; j < ITEMS; j++) {
+        if (rank[j] != 0xffffffffu) {
+          const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+          const uint32_t v = !vin ? (uint32_t)(start - seg_begin) + pos
+                                  : (pos < staged ? s_vals[pos] : __ldcg(&vin[start + pos]));
+          s_exchange[rank[j]] = v;
+        }
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < ITEMS; k++) {
+        if (dest[k] != 0xffffffffu) vout[dest[k]] = s_exchange[(uint32_t)k * THREADS + tid];
+      }
+      if (tid < kRadix) s_base[tid] += s_cnt[tid];
+      __syncthreads();
+    }
+    if (!last) {
+      barriers++;
+      grid_barrier(a, barriers * G, true);
+    }
+    kin = kout;
+    vin = vout;
+  }
+}
+
+// The cooperative variants: threads per block and keys per thread of a sub-tile
+using CoopKernel = void (*)(CoopArgs);
+struct CoopVariant {
+  CoopKernel fn;
+  int threads;
+  size_t smem;
+};
+
+CoopVariant coop_variant(int id) {
+  switch (id) {
+    case kCoop512x16: return {k_sort_coop<512, 16>, 512, CoopShape<512, 16>::kBytes};
+    case kCoop1024x8: return {k_sort_coop<1024, 8>, 1024, CoopShape<1024, 8>::kBytes};
+    default: return {k_sort_coop<1024, 16>, 1024, CoopShape<1024, 16>::kBytes};
+  }
+}
+
 }  // namespace
+
+// Blocks of a variant resident on the current device (0: it cannot launch
+// cooperatively), found once per device and variant
+int coop_blocks(int id) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, int> cache;
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return 0;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find({device, id});
+    if (it != cache.end()) return it->second;
+  }
+  const CoopVariant v = coop_variant(id);
+  int sms = 0, per_sm = 0, coop = 0;
+  int blocks = 0;
+  if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device) == cudaSuccess && coop &&
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
+      cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem) == cudaSuccess &&
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.threads, v.smem) == cudaSuccess) {
+    blocks = sms * std::min(per_sm, 1024 / v.threads);
+  }
+  cudaGetLastError();
+  std::lock_guard<std::mutex> lock(mu);
+  cache[{device, id}] = blocks;
+  return blocks;
+}
 
 uint32_t sort_small_pass_tiles(uint32_t max_tiles) {
   return max_tiles <= kSmallSortTiles ? max_tiles * (uint32_t)(kSortItems / kSmallItems) : 0u;
@@ -572,6 +909,7 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
   a.passes = passes;
   a.epoch = c.epoch;
   a.error_flag = c.error_flag;
+  a.spin_limit = c.spin_limit ? c.spin_limit : kSpinLimit;
   const uint32_t* ki = c.keys_in;
   const uint32_t* vi = c.vals_in;
   if (drop) {
@@ -598,6 +936,47 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     ki = sc.keys_a;
     vi = sc.vals_a;
   }
+  if (c.coop != kCoopNone && c.segs.count == 1 && sc.block_counts) {
+    const int blocks = coop_blocks(c.coop);
+    if (blocks > 0 && (uint32_t)blocks <= kMaxCoopBlocks) {
+      const CoopVariant v = coop_variant(c.coop);
+      CoopArgs ca{};
+      ca.keys_in = ki;
+      ca.vals_in = vi;
+      ca.keys_a = sc.keys_a;
+      ca.vals_a = sc.vals_a;
+      ca.keys_b = sc.keys_b;
+      ca.vals_b = sc.vals_b;
+      ca.keys_out = c.keys_out;
+      ca.vals_out = c.vals_out;
+      ca.begin = vsegs.begin;
+      ca.end = vsegs.end;
+      ca.hist = sc.hist;
+      ca.block_counts = sc.block_counts;
+      ca.barrier = sc.counters;  // the first pass's tile counter, which the onesweep would use (zeroed per sort)
+      ca.error_flag = c.error_flag;
+      ca.key_mask = mask;
+      ca.passes = passes;
+      ca.drop = drop;
+      ca.spin_limit = a.spin_limit;
+      ca.silent_pass = c.silent_pass;
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = dim3((unsigned)blocks);
+      cfg.blockDim = dim3((unsigned)v.threads);
+      cfg.dynamicSmemBytes = v.smem;
+      cfg.stream = stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeCooperative;
+      attr[0].val.cooperative = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      err = cudaLaunchKernelEx(&cfg, v.fn, ca);
+      if (err != cudaSuccess) return err;
+      n_launch++;
+      if (launches) *launches += n_launch;
+      return cudaGetLastError();
+    }
+  }
   for (int place = 0; place < passes; place++) {
     const bool last = place == passes - 1;
     // Ping-pong: after the partition the passes read A, B, A, ...; without it the first reads the input
@@ -611,6 +990,7 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     a.place = place;
     a.lookback = c.lookback + (size_t)place * pass_tiles * kRadix;
     a.counter = sc.counters + place;
+    a.silent_tile = place == c.silent_pass ? 0u : ~0u;
     const bool first = place == 0 && !drop;
     void (*kernel)(PassArgs) =
         first ? k_onesweep<true, true, kSortItems>

@@ -137,8 +137,28 @@ def test_keys_pass_and_sort_guard(ctx, bits):
         gpu = rb.project_collection([rb.SplatObject(cuda_table(d))], cam, params, bits, pass_="keys")
         ref = orc.project([rb.SplatObject(rb.Table.from_dict(d))], cam, params, bits, cull_keys=False)
         mismatch = int(np.sum(u32(gpu["keys"]) != ref["keys"]))
-        # the guard's reach is float32: a splat within a rounding of its edge may differ
-        assert mismatch <= (0 if guard == 0 else 3), mismatch
+        # the guard's reach is float64 in the oracle's operation order: the same keys
+        assert mismatch == 0, (guard, mismatch)
+        if guard:
+            assert int(np.sum(ref["keys"] == rb.SortKeys.invalid(bits))) > int(np.sum(
+                orc.project([rb.SplatObject(rb.Table.from_dict(d))], cam, rb.SplatParams(), bits,
+                            cull_keys=False)["keys"] == rb.SortKeys.invalid(bits)))  # the guard dropped keys
+
+
+def test_sort_guard_on_ext_and_lod_splats(ctx):
+    """The guard's float64 reach on the ext layout, with LoD opacities above 1
+    (the inflated covariance), keys equal to the oracle's."""
+    d = syn.mixture_table(60_000, seed=15, sh_degree=1)
+    d["opacities"][::4] = np.float32(1.4)
+    a, b, sh = orc.encode_ext(d)
+    host_table = rb.Table.ext(a, b, sh, 1)
+    dev_table = rb.Table.ext(to_cuda(a.view(np.int32)), to_cuda(b.view(np.int32)), [to_cuda(c.view(np.int32)) for c in sh], 1)
+    cam = syn.scale_camera()
+    for lod_inflate in (True, False):
+        params = rb.SplatParams(sort_guard=0.2, lod_inflate=lod_inflate)
+        gpu = rb.project_collection([rb.SplatObject(dev_table)], cam, params, 32, pass_="keys")
+        ref = orc.project([rb.SplatObject(host_table)], cam, params, 32, cull_keys=False)
+        assert int(np.sum(u32(gpu["keys"]) != ref["keys"])) == 0
 
 
 def test_orthographic_eye(ctx):

@@ -8,6 +8,7 @@ import torch
 
 import radix_b200 as rb
 from oracle import oracle as orc
+from radix_b200 import _abi
 from radix_b200.synthetic import Mulberry32
 from tests.parity import host, to_cuda, u32
 
@@ -154,3 +155,82 @@ def test_sort_keys_sort_at_the_small_tile_threshold(ctx, n):
     expected, exp_visible = orc.sort(keys, n, 32)
     assert visible == exp_visible
     np.testing.assert_array_equal(u32(got)[:n], expected[:n])
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+@pytest.mark.parametrize("bits", [24, 32])
+def test_a_wait_that_runs_out_reports_a_timeout_and_the_context_recovers(bits, variant):
+    """A test hook silences one digit pass: with onesweep passes (variant 0)
+    its first tile publishes no lookback word, in the cooperative kernel
+    (variant 1) block 0 does not arrive at the pass's grid barrier. The waits
+    on it run out after 64 polls: the call returns RDX_ERR_TIMEOUT with its
+    text, every kernel finishes, and the same context then sorts bit-exact
+    again (the reference throws on misuse, src/wgpu/WgpuRadixSort.ts:150-152;
+    it has no device waits)."""
+    c = rb.Context(0)
+    c.set_sort_variant(variant)
+    n = 150_000
+    keys = random_keys(n, bits, 21)
+    keys[::3] = rb.SortKeys.invalid(bits)
+    expected, visible = orc.sort(keys, n, bits)
+    for silent_pass in range(bits // 8):
+        c.set_wait(64, silent_pass)
+        with pytest.raises(rb.RadixError) as e:
+            rb.SortKeys.sort(keys, n, bits, ctx=c)  # host buffers: the call synchronises
+        assert e.value.code == _abi.RDX_ERR_TIMEOUT
+        assert "device wait gave up" in str(e.value)
+        c.set_wait(0, -1)
+        order, vis = rb.SortKeys.sort(keys, n, bits, ctx=c)
+        assert vis == visible
+        np.testing.assert_array_equal(u32(order)[:n], expected[:n])
+    c.close()
+
+
+SIZES = [0, 1, 4095, 4096, 4097, 70000, 1_000_003, 4_000_000]
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("bits", BITS)
+def test_every_digit_pass_variant_sorts_bit_exact(variant, bits):
+    """Onesweep passes (0) and the cooperative kernel's variants (1024x16,
+    512x16, 1024x8 threads x keys): SortKeys.sort (partition, then the valid
+    keys) and WgpuRadixSort.sort (in place, every key ranked) on the reference
+    grid, up to 4M keys (several sub-tiles a block)."""
+    c = rb.Context(0)
+    c.set_sort_variant(variant)
+    for count in SIZES:
+        keys = random_keys(count, bits, 100 + count + bits + variant)
+        if count:
+            keys[::5] = rb.SortKeys.invalid(bits)
+        expected, visible = orc.sort(keys, count, bits)
+        order, vis = rb.SortKeys.sort(to_cuda(keys.view(np.int32)), count, bits, ctx=c)
+        torch.cuda.synchronize()
+        assert vis == visible, (variant, bits, count)
+        np.testing.assert_array_equal(u32(order)[:count], expected[:count], err_msg=f"{variant} {bits} {count}")
+        kt, vt = to_cuda(keys.view(np.int32)), to_cuda(np.arange(max(count, 1), dtype=np.int32))
+        rb.RadixSort(kt, vt, c).sort(count, bits)
+        np.testing.assert_array_equal(u32(vt)[:count], expected[:count], err_msg=f"pairs {variant} {bits} {count}")
+        np.testing.assert_array_equal(u32(kt)[:count], keys[expected[:count]])
+    c.close()
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_every_digit_pass_variant_gives_the_frame_order(variant):
+    from radix_b200 import synthetic as syn
+    d = syn.mixture_table(1_000_000, seed=4, sh_degree=1)
+    cam = syn.scale_camera()
+    c = rb.Context(0)
+    c.set_sort_variant(variant)
+    t = rb.Table.from_dict(d, to=to_cuda)
+    res = rb.frame([rb.SplatObject(t)], cam, None, 32, ("keys",), ctx=c)
+    keys = u32(res["keys"])
+    expected, visible = orc.sort(keys, keys.size, 32)
+    assert res["visible"] == visible
+    np.testing.assert_array_equal(u32(res["ordering"]), expected[:keys.size])
+    batch = rb.Batch([([rb.SplatObject(t)], cam)], None, 32, ("keys",), ctx=c)
+    for _ in range(2):
+        batch.launch()
+        batch.synchronize()
+        np.testing.assert_array_equal(u32(batch.results()["ordering"]), expected[:keys.size])
+    batch.close()
+    c.close()
