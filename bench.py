@@ -46,6 +46,10 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--bits", type=int, default=32, choices=[16, 24, 32],
                    help="sort-key width (32 for the headline; 24 is the reference's default)")
+    p.add_argument("--pose", default="scale", choices=["scale", "all-visible"],
+                   help="frame: the configuration's camera at (0, 0.5, 3) (about half the splats in view), or a "
+                        "camera at (0, 0.5, 30) that keeps every splat inside the culls")
+    p.add_argument("--no-tune", action="store_true", help="keep the default kernel choices (no autotuning)")
     p.add_argument("--spz-container", default="gzip", choices=["gzip", "ngsp"],
                    help="spz workload: version 3 in gzip (one DEFLATE stream) or SPZ 4 (NGSP, a zstd stream a column)")
     p.add_argument("--workload", default="frame",
@@ -281,10 +285,25 @@ def run_batched(args, world, rank, local, device):
     names = ("mean2d", "conic", "depth", "opacity", "rgb", "keys")
     ctx = rb.Context(local)
     batch = rb.Batch(views, None, BITS, names, device=device, ctx=ctx)
+    tuning = None if args.no_tune else batch.tune(reps=5)
     graph_kernels = batch.launches()
     ms_total, clock_info = timed(batch.launch, args.steps, args.warmup, world, local)
     batch.synchronize()
     ms_step = ms_total / args.steps
+    # the plain path for the same 64 views: one single-view graph each (every
+    # view's own projection and sort), launched back to back
+    singles = [rb.Batch([view], None, BITS, names, device=device, ctx=ctx) for view in views]
+
+    def plain_step():
+        for b in singles:
+            b.launch()
+
+    plain_total, _ = timed(plain_step, max(3, args.steps // 4), 2, world, local)
+    plain_ms = plain_total / max(3, args.steps // 4)
+    for b in singles:
+        b.synchronize()
+        b.close()
+    del singles
     # the projection / sort split of the same batch, from the direct call's phase events
     out = rb._alloc_outputs(names, n_views, 1, device)
     ordering = torch.empty(n_views, dtype=torch.int32, device=device)
@@ -315,7 +334,10 @@ def run_batched(args, world, rank, local, device):
                    "scenes": counts, "splat_views": n_views, "bits": BITS, "parallelism": f"replicas{world}",
                    "l2": "inputs 2 GB > 126 MB L2 (no flush)", "frame_bytes_per_splat_view": FRAME_BYTES,
                    "hbm_frac_frame": FRAME_BYTES * n_views / (ms_step / 1e3) / 1e9 / peak,
-                   "project_ms": proj_ms, "sort_ms": sort_ms},
+                   "project_ms": proj_ms, "sort_ms": sort_ms,
+                   "plain_ms": plain_ms, "batched_over_plain": ms_step / plain_ms,
+                   "plain": "the same 64 views as 64 single-view CUDA graphs (projection + sort each)",
+                   "tuning": tuning},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "kernel": "k_project (raw, SH 3, 1 eye), all 64 views in one launch",
                      "bytes_per_splat": PROJECT_BYTES, "peak_kind": peak_kind},
@@ -367,6 +389,23 @@ def run_stereo(args, world, rank, local, device):
     proj_ms = phases["project"][0] / max(phases["project"][1], 1)
     sort_ms = phases["sort"][0] / max(phases["sort"][1], 1)
     ms_step = ms_total / args.steps
+    # the batched form of the same stereo frame (one CUDA graph, tuned), and a
+    # mono frame of the same table and pose (one eye at the head, same size and fov)
+    batch = rb.Batch([(obj, cam)], None, BITS, names, device=device, ctx=ctx)
+    tuning = None if args.no_tune else batch.tune(reps=3)
+    batched_total, _ = timed(batch.launch, args.steps, 2, world, local)
+    batch.synchronize()
+    batch.close()
+    batched_ms = batched_total / args.steps
+    mono = syn.Camera.mono((0.0, 0.5, 3.0), (0.0, 0.0, 0.0), 100.0, 2064, 2208)
+    out_mono = rb._alloc_outputs(names, n, 1, device)
+
+    def mono_step():
+        rb.frame(obj, mono, None, BITS, names, ctx=ctx, out=out_mono, ordering=ordering, visible=visible)
+
+    mono_total, _ = timed(mono_step, args.steps, 2, world, local)
+    mono_ms = mono_total / args.steps
+    del out_mono
     in_bytes = 12 + 12 + 16 + 4 + 96
     proj_bytes = in_bytes + 2 * 40 + 4
     frame_bytes = in_bytes + 2 * 40 + 8 + 16 * (BITS // 8) + 4
@@ -383,7 +422,11 @@ def run_stereo(args, world, rank, local, device):
                    "n": n, "eyes": 2, "bits": BITS, "parallelism": f"replicas{world}",
                    "l2": "inputs 2.2 GB > 126 MB L2 (no flush)", "frame_bytes_per_splat": frame_bytes,
                    "hbm_frac_frame": frame_bytes * n / (ms_step / 1e3) / 1e9 / peak,
-                   "project_ms": proj_ms, "sort_ms": sort_ms, "phase_runs": runs},
+                   "project_ms": proj_ms, "sort_ms": sort_ms, "phase_runs": runs,
+                   "batched_ms": batched_ms, "batched_over_plain": batched_ms / ms_step,
+                   "mono_ms": mono_ms, "stereo_over_mono": ms_step / mono_ms,
+                   "mono": "one eye at the head, 2064x2208 fov 100, the same table (rb.frame)",
+                   "tuning": tuning},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": ncu_traffic("project_kernel_stereo_2m.md", n / 2_000_000),
                      "kernel": "k_project (raw, SH 3 fp16, 2 eyes)",
@@ -710,7 +753,7 @@ def main():
 
     n = args.n
     d, host_cols, dev_cols = make_workload(n, device)
-    cam = syn.scale_camera()
+    cam = syn.scale_camera() if args.pose == "scale" else syn.all_visible_camera()
     ctx = rb.Context(local)
     table = table_of(dev_cols)
     obj = [rb.SplatObject(table)]
@@ -726,6 +769,7 @@ def main():
     # The frame captured once in a CUDA graph (rb.Batch with one view): each
     # step is one graph launch of the projection and the sort
     batch = rb.Batch([(obj, cam)], None, BITS, names, device=device, ctx=ctx)
+    tuning = None if args.no_tune else batch.tune(reps=5)
     graph_kernels = batch.launches()
     ms_total, clock_info = timed(batch.launch, args.steps, args.warmup, world, local)
     batch.synchronize()
@@ -743,6 +787,7 @@ def main():
     phases = ctx.phase_times()
     ctx.set_profiling(False)
     batch.close()
+    drawn = int(visible.cpu().numpy()[0])
 
     # end to end through the public API: pinned host tables in, the order and
     # the visible count out, copies inside the timed region
@@ -786,8 +831,9 @@ def main():
                    "frame_bytes_per_splat": FRAME_BYTES,
                    "hbm_frac_frame": FRAME_BYTES * n / (ms_step / 1e3) / 1e9 / peak,
                    "project_ms": proj_avg, "sort_ms": sort_ms / max(sort_runs, 1),
-                   "step": "one CUDA-graph launch of the frame (rb.Batch, one view)",
-                   "rb_frame_ms": frame_ms / args.steps},
+                   "step": "one CUDA-graph launch of the frame (rb.Batch, one view, autotuned)",
+                   "rb_frame_ms": frame_ms / args.steps, "pose": args.pose,
+                   "drawn_fraction": drawn / n, "tuning": tuning},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "kernel": "k_project (raw, SH 3, 1 eye)",
                      "bytes_per_splat": PROJECT_BYTES, "peak_kind": peak_kind},

@@ -236,14 +236,20 @@ int rdx_ctx_phase_times(rdx_ctx* ctx, double* ms, uint64_t* runs);
  */
 int rdx_ctx_set_wait(rdx_ctx* ctx, uint32_t polls, int silent_pass);
 /*
- * How this context's one-segment sorts run their digit passes: -1 chosen by
- * size (the default), 0 one onesweep kernel per pass, 1-3 one cooperative
- * kernel for every pass (1: 1024 threads x 16 keys per block, 2: 512 x 16,
- * 3: 1024 x 8). Every variant gives the same order. A batch takes the choice
- * when it is created. No counterpart in the reference (its radix sort takes
- * keysPerThread 8 or 16, WgpuRadixSort.ts:80-91).
+ * How this context's sorts run their digit passes (every variant gives the
+ * same order): -1 a choice of rdx_batch_tune / rdx_sort_tune for the
+ * workload's shape, else variant 0 (the default); 0 one onesweep kernel per
+ * pass, 1024-key tiles for sorts of at most 1M keys and 4096-key tiles above;
+ * 1-3 one cooperative kernel for every pass of a one-segment sort (1: 1024
+ * threads x 16 keys per block, 2: 512 x 16, 3: 1024 x 8); 4-6 onesweep
+ * passes in 4096-, 2048- or 1024-key tiles. A variant a sort cannot take
+ * (cooperative with several segments, tiles its lookback words do not hold)
+ * falls back to 0's tiles. A batch takes the choice when it is created. The
+ * reference's radix sort has one such knob, keysPerThread 8 or 16
+ * (WgpuRadixSort.ts:80-91).
  */
 int rdx_ctx_set_sort_variant(rdx_ctx* ctx, int variant);
+
 /* Kernels this context has launched since it was created. */
 int rdx_ctx_launches(rdx_ctx* ctx, uint64_t* launches);
 
@@ -505,6 +511,33 @@ int rdx_batch_launch(rdx_batch* batch);
 int rdx_batch_synchronize(rdx_batch* batch);
 int rdx_batch_launches(const rdx_batch* batch, uint64_t* launches);  /* kernels per launch */
 int rdx_batch_destroy(rdx_batch* batch);
+
+/*
+ * Autotuning. rdx_batch_tune times, on the batch's own buffers and stream
+ * (CUDA events, the median of `reps` frames after one warm-up each), the
+ * projection at 2, 4 and 8 warps per block and then every digit-pass variant
+ * the batch can take; it keeps the fastest pair (never slower than the
+ * defaults, which are candidate 0), captures the batch's graph again with
+ * it, and remembers it in the context for frames of the same shape (key
+ * width, one view or many, the row count's power of two, the first table's
+ * kind). rdx_sort_tune does the same for one-segment sorts of `count` device
+ * keys (the keys are read, not changed). Both synchronise the stream.
+ * No counterpart in the reference, whose keysPerThread is chosen by hand.
+ */
+#define RDX_TUNE_MAX 16
+typedef struct rdx_tune_result {
+  int32_t sort_variant;          /* chosen digit-pass variant */
+  int32_t project_warps;         /* chosen warps per projection block (0: no projection) */
+  int32_t candidates;            /* entries below */
+  int32_t reserved;
+  double default_ms;             /* a frame (sort) with the defaults */
+  double tuned_ms;               /* with the choice */
+  int32_t cand_sort[RDX_TUNE_MAX];
+  int32_t cand_warps[RDX_TUNE_MAX];
+  double cand_ms[RDX_TUNE_MAX];  /* median ms of each candidate */
+} rdx_tune_result;
+int rdx_batch_tune(rdx_batch* batch, int reps, rdx_tune_result* out);
+int rdx_sort_tune(rdx_ctx* ctx, const uint32_t* keys, uint64_t count, int bits, int reps, rdx_tune_result* out);
 
 /* ---- sorting without allocating ---- */
 

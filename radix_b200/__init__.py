@@ -115,9 +115,18 @@ class Context:
         _abi.check(_abi.lib().rdx_ctx_set_wait(self.handle, int(polls), int(silent_pass)), self.handle)
 
     def set_sort_variant(self, variant=-1):
-        """Digit passes of one-segment sorts: -1 by size, 0 onesweep kernels,
-        1-3 a cooperative kernel (1024x16, 512x16, 1024x8 threads x keys)."""
+        """How sorts run their digit passes: -1 tuned for the shape or 0; 0
+        onesweep kernels with tiles by size; 1-3 one cooperative kernel
+        (1024x16, 512x16, 1024x8 threads x keys); 4-6 onesweep kernels with
+        4096-, 2048- or 1024-key tiles."""
         _abi.check(_abi.lib().rdx_ctx_set_sort_variant(self.handle, int(variant)), self.handle)
+
+    def tune_sort(self, keys, count, bits, reps=5):
+        """Time every digit-pass variant on `count` device keys and remember the
+        fastest for sorts of that shape; returns the timings."""
+        r = _abi.rdx_tune_result()
+        self.call("rdx_sort_tune", _ptr(keys), int(count), int(bits), int(reps), ctypes.byref(r))
+        return r.as_dict()
 
     def phase_times(self):
         """{phase: (summed ms, runs)} since the last read (waits for the stream)."""
@@ -637,6 +646,14 @@ class Batch:
         n = ctypes.c_uint64(0)
         self._call("rdx_batch_launches", ctypes.byref(n))
         return n.value
+
+    def tune(self, reps=5):
+        """Time projection block sizes and digit-pass variants on this batch,
+        capture its graph again with the fastest and remember the choice in the
+        context; returns the timings (the defaults are candidate 0)."""
+        r = _abi.rdx_tune_result()
+        self._call("rdx_batch_tune", int(reps), ctypes.byref(r))
+        return r.as_dict()
 
     def results(self):
         res = dict(self.out)

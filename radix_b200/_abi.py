@@ -150,6 +150,29 @@ class rdx_rdxfile_channel(ctypes.Structure):
                 ("element_bytes", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
+RDX_TUNE_MAX = 16
+
+
+class rdx_tune_result(ctypes.Structure):
+    _fields_ = [
+        ("sort_variant", ctypes.c_int32),
+        ("project_warps", ctypes.c_int32),
+        ("candidates", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("default_ms", ctypes.c_double),
+        ("tuned_ms", ctypes.c_double),
+        ("cand_sort", ctypes.c_int32 * RDX_TUNE_MAX),
+        ("cand_warps", ctypes.c_int32 * RDX_TUNE_MAX),
+        ("cand_ms", ctypes.c_double * RDX_TUNE_MAX),
+    ]
+
+    def as_dict(self):
+        return {"sort_variant": self.sort_variant, "project_warps": self.project_warps,
+                "default_ms": self.default_ms, "tuned_ms": self.tuned_ms,
+                "candidates": [{"sort_variant": self.cand_sort[i], "project_warps": self.cand_warps[i],
+                                "ms": self.cand_ms[i]} for i in range(self.candidates)]}
+
+
 class rdx_outputs(ctypes.Structure):
     _fields_ = [
         ("mean2d", ctypes.c_void_p),
@@ -176,6 +199,9 @@ SIGNATURES = {
     "rdx_ctx_set_profiling": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "rdx_ctx_set_wait": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int]),
     "rdx_ctx_set_sort_variant": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "rdx_batch_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    "rdx_sort_tune": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_void_p]),
     "rdx_ctx_phase_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_ctx_launches": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_sort_keys_compute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),

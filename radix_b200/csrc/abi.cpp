@@ -55,9 +55,14 @@ struct rdx_ctx {
   // the one-shot test hook that silences a digit pass's first tile
   uint32_t spin_limit = 0;
   int silent_pass = -1;
-  // Digit passes of one-segment sorts: -1 chosen by size, 0 the onesweep
-  // passes, else a cooperative variant (rdx::kCoop*)
+  // How sorts run their digit passes (rdx_ctx_set_sort_variant; -1: tuned or default)
   int sort_variant = -1;
+  // Choices of rdx_batch_tune / rdx_sort_tune, by workload shape (tune_key)
+  struct Tuned {
+    int sort_variant;
+    int project_warps;
+  };
+  std::map<uint64_t, Tuned> tuned;
 };
 
 static const size_t kRingBytes = 4u << 20;
@@ -197,8 +202,11 @@ bool valid_bits(int bits) { return bits == 16 || bits == 24 || bits == 32; }
 
 uint32_t tiles_of(uint64_t n) { return (uint32_t)((n + rdx::kSortTile - 1) / rdx::kSortTile); }
 
-// Lookback tiles a pass of a sort of max_tiles 4096-key tiles may use (small sorts: 1024-key tiles)
-size_t lookback_tiles(uint32_t max_tiles) { return std::max(max_tiles, rdx::sort_small_pass_tiles(max_tiles)); }
+// Lookback tiles a pass of a sort of max_tiles 4096-key tiles may use: room
+// for 2048-key digit-pass tiles always, and 1024-key tiles for small sorts
+size_t lookback_tiles(uint32_t max_tiles) {
+  return std::max((size_t)max_tiles * 2, (size_t)rdx::sort_small_pass_tiles(max_tiles));
+}
 
 // Sort scratch for `segments` segments of `total` keys
 rdx::SortScratch take_sort_scratch(Arena& a, int segments, int passes, uint64_t total) {
@@ -607,6 +615,11 @@ rdx::ProjDesc make_desc(const rdx_camera& cam, const Camera& c, const rdx_object
   return d;
 }
 
+// One launch per kind: layout, SH degree and colour type or SH codec (also a tuning key)
+int table_kind_of(const rdx_table& t) {
+  return t.layout * 100 + t.sh_degree * 10 + (t.layout == RDX_LAYOUT_RAW ? t.color_dtype : t.sh_codec);
+}
+
 struct ProjectCall {
   std::vector<rdx::ProjDesc> descs;
   std::vector<int> groups;  // start of each group of one kernel kind in descs (+ end)
@@ -643,7 +656,7 @@ int plan_views(rdx_ctx* ctx, Arena& a, const ViewRef* views, int n_views, const 
       const rdx_object& o = vw.objects[i];
       const rdx_table& t = *o.table;
       if (!staged.count(o.table)) staged[o.table] = stage_table(ctx, a, t, &status);
-      const int kind = t.layout * 100 + t.sh_degree * 10 + (t.layout == RDX_LAYOUT_RAW ? t.color_dtype : t.sh_codec);
+      const int kind = table_kind_of(t);
       if (o.count > 0) {
         rdx::ProjDesc d = make_desc(*vw.camera, c, o, staged[o.table], *params, offset, n, bits, pass, cull_keys);
         d.segment = v;
@@ -694,15 +707,56 @@ int check_objects(rdx_ctx* ctx, const rdx_object* objects, int n_objects) {
   return RDX_OK;
 }
 
-// Keys up to which a one-segment sort takes the cooperative digit passes by default
-constexpr uint64_t kCoopDefaultMaxKeys = 1ull << 23;
+// ---- digit-pass variants (rdx_ctx_set_sort_variant's numbering) and tuning ----
 
-// The digit-pass variant of a sort of `segments` segments and `n` keys
-int sort_variant(const rdx_ctx* ctx, int segments, uint64_t n) {
-  if (segments != 1) return rdx::kCoopNone;
-  if (ctx->sort_variant >= 0) return ctx->sort_variant;
-  return n <= kCoopDefaultMaxKeys ? rdx::kCoop1024x16 : rdx::kCoopNone;
+constexpr int kSortVariants = 7;  // 0 onesweep by size, 1-3 cooperative, 4-6 onesweep 4096/2048/1024-key tiles
+
+struct SortPlan {
+  int coop = rdx::kCoopNone;
+  int pass_items = 0;
+};
+
+SortPlan plan_of(int variant) {
+  SortPlan p;
+  if (variant >= 1 && variant <= 3) p.coop = variant;  // kCoop1024x16, kCoop512x16, kCoop1024x8
+  if (variant == 4) p.pass_items = 16;
+  if (variant == 5) p.pass_items = 8;
+  if (variant == 6) p.pass_items = 4;
+  return p;
 }
+
+// Whether `variant` can run a sort of `segments` segments of max_tiles
+// 4096-key tiles with `lookback_words` lookback words
+bool variant_feasible(int variant, int segments, uint32_t max_tiles, int passes, size_t lookback_words) {
+  const SortPlan p = plan_of(variant);
+  if (p.coop != rdx::kCoopNone) return segments == 1 && rdx::coop_blocks(p.coop) > 0;
+  if (p.pass_items) return (size_t)passes * max_tiles * (size_t)(16 / p.pass_items) * rdx::kRadix <= lookback_words;
+  return true;
+}
+
+// A workload's shape for the tuning cache: sort or frame, key width, one
+// segment or many, the key count's power of two and the frame's table kind
+uint64_t tune_key(int frame, int bits, int segments, uint64_t n, int table_kind) {
+  int log2n = 0;
+  while (log2n < 63 && (1ull << log2n) < n) log2n++;
+  return ((((uint64_t)frame * 8 + (uint64_t)(bits / 8)) * 2 + (segments > 1 ? 1 : 0)) * 64 + (uint64_t)log2n) * 4096 +
+         (uint64_t)(table_kind & 4095);
+}
+
+// The digit-pass variant of a sort: the context's forced choice, else a tuned
+// one for this shape, else the onesweep passes with tiles by size
+int sort_variant(const rdx_ctx* ctx, int segments, uint64_t n, int bits, int frame, int table_kind) {
+  if (ctx->sort_variant >= 0) return ctx->sort_variant;
+  auto it = ctx->tuned.find(tune_key(frame, bits, segments, n, table_kind));
+  if (it != ctx->tuned.end()) return it->second.sort_variant;
+  return 0;
+}
+
+int project_warps(const rdx_ctx* ctx, int segments, uint64_t n, int bits, int table_kind) {
+  auto it = ctx->tuned.find(tune_key(1, bits, segments, n, table_kind));
+  return it != ctx->tuned.end() ? it->second.project_warps : 0;
+}
+
 
 // Enqueue one sort (every pass); it takes a fresh lookback epoch on the device
 int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
@@ -727,7 +781,10 @@ int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uin
   c.spin_limit = ctx->spin_limit;
   c.silent_pass = ctx->silent_pass;
   ctx->silent_pass = -1;  // one sort only
-  c.coop = sort_variant(ctx, segments, (uint64_t)max_tiles * rdx::kSortTile);
+  const int variant = sort_variant(ctx, segments, (uint64_t)max_tiles * rdx::kSortTile, bits, 0, 0);
+  const SortPlan plan = plan_of(variant);
+  c.coop = plan.coop;
+  c.pass_items = plan.pass_items;
   int launches = 0;
   RDX_CUDA(rdx::sort_segments(c, ctx->stream, &launches), "sort launch");
   ctx->launches += (uint64_t)launches;
@@ -841,7 +898,7 @@ int rdx_ctx_set_wait(rdx_ctx* ctx, uint32_t polls, int silent_pass) {
 
 int rdx_ctx_set_sort_variant(rdx_ctx* ctx, int variant) {
   if (!ctx) return RDX_ERR_ARG;
-  if (variant < -1 || variant >= rdx::kCoopVariants) return fail(ctx, RDX_ERR_ARG, "sort variant %d", variant);
+  if (variant < -1 || variant >= kSortVariants) return fail(ctx, RDX_ERR_ARG, "sort variant %d", variant);
   ctx->sort_variant = variant;
   return RDX_OK;
 }
@@ -1181,6 +1238,8 @@ struct FrameDev {
   uint32_t spin_limit = 0;         // polls of a bounded wait (0: the default)
   int silent_pass = -1;            // test hook (see rdx_ctx_set_wait)
   int coop = 0;                    // the digit passes' variant (rdx::kCoop*)
+  int pass_items = 0;              // onesweep digit-pass tile (keys a thread; 0: by size)
+  int proj_warps = 0;              // warps per projection block (0: the default)
 };
 
 // Enqueue a planned frame on `stream`: the projection, then the segmented sort
@@ -1203,7 +1262,7 @@ cudaError_t enqueue_frame(rdx_ctx* timing, const ProjectCall& call, const FrameD
       out.zero = sorting && g == 0 ? fd.sc.hist : nullptr;
       out.zero_words = out.zero ? rdx::sort_small_state_words(views, passes, segment_tiles(call, nullptr)) : 0;
       e = rdx::launch_project(fd.descs + start, call.descs.data() + start, count, call.group_tiles[g], out,
-                              fd.error_flag, stream);
+                              fd.error_flag, stream, fd.proj_warps);
       if (e != cudaSuccess) return e;
       if (call.group_tiles[g]) *launches += 1;
     }
@@ -1224,6 +1283,7 @@ cudaError_t enqueue_frame(rdx_ctx* timing, const ProjectCall& call, const FrameD
     c.spin_limit = fd.spin_limit;
     c.silent_pass = fd.silent_pass;
     c.coop = fd.coop;
+    c.pass_items = fd.pass_items;
     int n_launch = 0;
     e = rdx::sort_segments(c, stream, &n_launch);
     *launches += (uint64_t)n_launch;
@@ -1236,6 +1296,13 @@ cudaError_t enqueue_frame(rdx_ctx* timing, const ProjectCall& call, const FrameD
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+// The table kind of a frame's first object (0: no objects): a tuning key
+int first_table_kind(const ViewRef* views, int n_views) {
+  for (int v = 0; v < n_views; v++)
+    if (views[v].n_objects > 0) return table_kind_of(*views[v].objects[0].table);
+  return 0;
 }
 
 // Argument checks shared by the frame entry points; *n = rows of all views
@@ -1349,7 +1416,13 @@ int frame_common(rdx_ctx* ctx, const ViewRef* views, int n_views, const rdx_para
   fd.lookback_words = ctx->lookback_words;
   fd.error_flag = ctx->error_flag;
   fd.spin_limit = ctx->spin_limit;
-  fd.coop = sort_variant(ctx, n_views, n);
+  {
+    const int kind = first_table_kind(views, n_views);
+    const SortPlan plan = plan_of(sort_variant(ctx, n_views, n, sort_bits, 1, kind));
+    fd.coop = plan.coop;
+    fd.pass_items = plan.pass_items;
+    fd.proj_warps = project_warps(ctx, n_views, n, sort_bits, kind);
+  }
   if (sort && n > 0) {
     fd.silent_pass = ctx->silent_pass;
     ctx->silent_pass = -1;  // one sort only
@@ -1398,9 +1471,31 @@ struct rdx_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint64_t graph_launches = 0;               // kernels in the graph
+  size_t lookback_words = 0;
+  int table_kind = 0;                        // of the first object (the tuning key)
+  uint64_t n = 0;                            // rows of all views
 };
 
 namespace {
+
+// Capture the batch's frame (its current plan) in a CUDA graph, replacing any earlier one
+int capture_batch(rdx_batch* b) {
+  rdx_ctx* ctx = b->ctx;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+  b->graph_launches = 0;
+  cudaError_t e = cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamBeginCapture");
+  cudaError_t le = enqueue_frame(nullptr, b->call, b->fd, b->bits, true, b->capture, &b->graph_launches);
+  e = cudaStreamEndCapture(b->capture, &b->graph);
+  if (le != cudaSuccess) return cuda_fail(ctx, le, "batch capture");
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGraphInstantiate");
+  return RDX_OK;
+}
 
 void free_batch(rdx_batch* b) {
   if (!b) return;
@@ -1871,7 +1966,15 @@ int rdx_batch_create(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx
   b->fd.lookback_words = lookback_words;
   b->fd.error_flag = b->words;
   b->fd.spin_limit = ctx->spin_limit;
-  b->fd.coop = sort_variant(ctx, n_views, n);
+  b->table_kind = first_table_kind(refs.data(), n_views);
+  b->n = n;
+  b->lookback_words = lookback_words;
+  {
+    const SortPlan plan = plan_of(sort_variant(ctx, n_views, n, sort_bits, 1, b->table_kind));
+    b->fd.coop = plan.coop;
+    b->fd.pass_items = plan.pass_items;
+    b->fd.proj_warps = project_warps(ctx, n_views, n, sort_bits, b->table_kind);
+  }
   // descriptors and segments stay in the batch's memory; the graph only reads them
   std::vector<uint32_t> tiles;
   segment_tiles(b->call, &tiles);
@@ -1887,15 +1990,8 @@ int rdx_batch_create(rdx_ctx* ctx, const rdx_view* views, int n_views, const rdx
     e = cudaMemcpyAsync(b->fd.sb.tiles, tiles.data(), tiles.size() * 4, cudaMemcpyHostToDevice, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "batch set-up"));
-  // capture the frame's kernels once
-  e = cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeRelaxed);
-  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "cudaStreamBeginCapture"));
-  cudaError_t le = enqueue_frame(nullptr, b->call, b->fd, sort_bits, true, b->capture, &b->graph_launches);
-  e = cudaStreamEndCapture(b->capture, &b->graph);
-  if (le != cudaSuccess) return bail(cuda_fail(ctx, le, "batch capture"));
-  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "cudaStreamEndCapture"));
-  e = cudaGraphInstantiate(&b->exec, b->graph, 0);
-  if (e != cudaSuccess) return bail(cuda_fail(ctx, e, "cudaGraphInstantiate"));
+  const int st = capture_batch(b);
+  if (st != RDX_OK) return bail(st);
   *batch = b;
   return RDX_OK;
 }
@@ -1963,6 +2059,187 @@ int rdx_batch_synchronize(rdx_batch* b) {
 int rdx_batch_launches(const rdx_batch* b, uint64_t* launches) {
   if (!b || !launches) return RDX_ERR_ARG;
   *launches = b->graph_launches;
+  return RDX_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Median milliseconds of `reps` runs of enqueue() on the context's stream
+// (one warm-up first), each between its own pair of events
+template <class F>
+int time_runs(rdx_ctx* ctx, int reps, F&& enqueue, double* ms) {
+  std::vector<cudaEvent_t> ev(2 * (size_t)reps + 2, nullptr);
+  int st = RDX_OK;
+  for (auto& x : ev) {
+    if (cudaEventCreate(&x) != cudaSuccess) {
+      cudaGetLastError();
+      st = fail(ctx, RDX_ERR_CUDA, "tuning events");
+      break;
+    }
+  }
+  if (st == RDX_OK) st = enqueue();  // warm-up
+  for (int r = 0; r < reps && st == RDX_OK; r++) {
+    cudaEventRecord(ev[2 * r], ctx->stream);
+    st = enqueue();
+    cudaEventRecord(ev[2 * r + 1], ctx->stream);
+  }
+  std::vector<double> t;
+  if (st == RDX_OK && cudaStreamSynchronize(ctx->stream) == cudaSuccess) {
+    for (int r = 0; r < reps; r++) {
+      float x = 0.0f;
+      if (cudaEventElapsedTime(&x, ev[2 * r], ev[2 * r + 1]) == cudaSuccess) t.push_back(x);
+    }
+  }
+  cudaGetLastError();
+  for (auto& x : ev)
+    if (x) cudaEventDestroy(x);
+  if (st != RDX_OK) return st;
+  if (t.empty()) return fail(ctx, RDX_ERR_CUDA, "tuning timings");
+  std::sort(t.begin(), t.end());
+  *ms = t[t.size() / 2];
+  return RDX_OK;
+}
+
+void add_candidate(rdx_tune_result* out, int sort_variant, int warps, double ms) {
+  if (!out || out->candidates >= RDX_TUNE_MAX) return;
+  out->cand_sort[out->candidates] = sort_variant;
+  out->cand_warps[out->candidates] = warps;
+  out->cand_ms[out->candidates] = ms;
+  out->candidates++;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rdx_batch_tune(rdx_batch* b, int reps, rdx_tune_result* out) {
+  if (!b) return RDX_ERR_ARG;
+  rdx_ctx* ctx = b->ctx;
+  cudaSetDevice(ctx->device);
+  if (reps < 1) reps = 5;
+  if (out) memset(out, 0, sizeof(*out));
+  const int views = (int)b->view_objects.size();
+  const int passes = b->bits / 8;
+  const uint32_t max_tiles = segment_tiles(b->call, nullptr);
+  FrameDev fd = b->fd;
+  auto run = [&]() -> int {
+    uint64_t launches = 0;
+    cudaError_t e = enqueue_frame(nullptr, b->call, fd, b->bits, true, ctx->stream, &launches);
+    return e == cudaSuccess ? RDX_OK : cuda_fail(ctx, e, "tuning frame");
+  };
+  // The defaults first (onesweep passes with tiles by size, 4-warp projection blocks)
+  fd.coop = rdx::kCoopNone;
+  fd.pass_items = 0;
+  fd.proj_warps = 0;
+  double default_ms = 0.0;
+  int st = time_runs(ctx, reps, run, &default_ms);
+  if (st != RDX_OK) return st;
+  add_candidate(out, 0, 4, default_ms);
+  // Projection block sizes, with the default sort
+  int best_warps = 0;
+  double best = default_ms;
+  for (int w : {2, 8}) {
+    fd.proj_warps = w;
+    double ms = 0.0;
+    st = time_runs(ctx, reps, run, &ms);
+    if (st != RDX_OK) return st;
+    add_candidate(out, 0, w, ms);
+    if (ms < best) {
+      best = ms;
+      best_warps = w;
+    }
+  }
+  fd.proj_warps = best_warps;
+  // Digit-pass variants, with the chosen projection
+  int best_variant = 0;
+  for (int v = 1; v < kSortVariants; v++) {
+    if (!variant_feasible(v, views, max_tiles, passes, b->lookback_words)) continue;
+    const SortPlan p = plan_of(v);
+    fd.coop = p.coop;
+    fd.pass_items = p.pass_items;
+    double ms = 0.0;
+    st = time_runs(ctx, reps, run, &ms);
+    if (st != RDX_OK) return st;
+    add_candidate(out, v, best_warps ? best_warps : 4, ms);
+    if (ms < best) {
+      best = ms;
+      best_variant = v;
+    }
+  }
+  st = rdx_batch_synchronize(b);  // a bounded wait that gave up during tuning
+  if (st != RDX_OK) return st;
+  const SortPlan p = plan_of(best_variant);
+  b->fd.coop = p.coop;
+  b->fd.pass_items = p.pass_items;
+  b->fd.proj_warps = best_warps;
+  ctx->tuned[tune_key(1, b->bits, views, b->n, b->table_kind)] = {best_variant, best_warps};
+  st = capture_batch(b);
+  if (st != RDX_OK) return st;
+  if (out) {
+    out->sort_variant = best_variant;
+    out->project_warps = best_warps ? best_warps : 4;
+    out->default_ms = default_ms;
+    out->tuned_ms = best;
+  }
+  return RDX_OK;
+}
+
+int rdx_sort_tune(rdx_ctx* ctx, const uint32_t* keys, uint64_t count, int bits, int reps, rdx_tune_result* out) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (!valid_bits(bits)) return fail(ctx, RDX_ERR_ARG, "SortKeys.sort: bits must be 16, 24 or 32 (got %d)", bits);
+  if (count == 0 || count > rdx::kMaxSegmentKeys) return fail(ctx, RDX_ERR_ARG, "rdx_sort_tune: %llu keys", (unsigned long long)count);
+  if (!keys || !is_device_ptr(keys)) return fail(ctx, RDX_ERR_ARG, "rdx_sort_tune takes device keys");
+  cudaSetDevice(ctx->device);
+  if (reps < 1) reps = 5;
+  if (out) memset(out, 0, sizeof(*out));
+  const int passes = bits / 8;
+  const uint32_t tiles = tiles_of(count);
+  uint32_t* o;
+  SegBufs sb;
+  rdx::SortScratch sc;
+  auto layout = [&](Arena& a) {
+    o = a.take<uint32_t>(count);
+    sb = take_segs(a, 1);
+    sc = take_sort_scratch(a, 1, passes, count);
+  };
+  Arena dry(nullptr);
+  layout(dry);
+  int st = ensure_arena(ctx, dry.used);
+  if (st != RDX_OK) return st;
+  st = ensure_lookback(ctx, (size_t)passes * lookback_tiles(tiles) * rdx::kRadix);
+  if (st != RDX_OK) return st;
+  Arena a(ctx->arena);
+  layout(a);
+  st = single_segment(ctx, sb, count);
+  if (st != RDX_OK) return st;
+  const int forced = ctx->sort_variant;
+  int best_variant = 0;
+  double best = 0.0, default_ms = 0.0;
+  for (int v = 0; v < kSortVariants && st == RDX_OK; v++) {
+    if (!variant_feasible(v, 1, tiles, passes, ctx->lookback_words)) continue;
+    ctx->sort_variant = v;
+    double ms = 0.0;
+    st = time_runs(ctx, reps, [&]() { return run_sort(ctx, keys, nullptr, nullptr, o, sb, 1, tiles, bits, sc, false); }, &ms);
+    if (st != RDX_OK) break;
+    add_candidate(out, v, 0, ms);
+    if (v == 0) default_ms = ms;
+    if (v == 0 || ms < best) {
+      best = ms;
+      best_variant = v;
+    }
+  }
+  ctx->sort_variant = forced;
+  if (st != RDX_OK) return st;
+  st = finish(ctx);
+  if (st != RDX_OK) return st;
+  ctx->tuned[tune_key(0, bits, 1, (uint64_t)tiles * rdx::kSortTile, 0)] = {best_variant, 0};
+  if (out) {
+    out->sort_variant = best_variant;
+    out->default_ms = default_ms;
+    out->tuned_ms = best;
+  }
   return RDX_OK;
 }
 

@@ -128,6 +128,7 @@ struct SortCall {
   uint32_t spin_limit = 0;  // polls of a bounded device wait (0: kSpinLimit)
   int silent_pass = -1;     // a digit pass whose first tile publishes no lookback word (a test hook; -1: none)
   int coop = kCoopNone;     // one segment: the digit passes in this cooperative variant (needs block_counts)
+  int pass_items = 0;       // onesweep digit passes after a partition: keys a thread (4, 8, 16; 0: by size)
 };
 cudaError_t sort_segments(const SortCall& call, cudaStream_t stream, int* launches);
 // Blocks of a cooperative variant resident on the current device (0: it cannot launch)

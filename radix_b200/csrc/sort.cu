@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <type_traits>
 #include <utility>
 
 #include "rdx_internal.h"
@@ -69,6 +70,23 @@ __device__ __forceinline__ uint32_t peers_of(uint32_t d, bool ranked) {
     const bool bit = (d >> b) & 1u;
     const uint32_t m = __ballot_sync(0xffffffffu, bit);
     peers &= bit ? m : ~m;
+  }
+  return peers;
+}
+
+// The same over the low `nbits` bits of a code that is unique per digit present
+// (a place holding few distinct digits ranks with fewer ballots); nbits is
+// uniform over the block
+__device__ __forceinline__ uint32_t peers_of_code(uint32_t c, bool ranked, int nbits) {
+  const uint32_t r = __ballot_sync(0xffffffffu, ranked);
+  uint32_t peers = ranked ? r : ~r;
+#pragma unroll
+  for (int b = 0; b < 8; b++) {
+    if (b < nbits) {
+      const bool bit = (c >> b) & 1u;
+      const uint32_t m = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? m : ~m;
+    }
   }
   return peers;
 }
@@ -360,6 +378,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   __shared__ uint32_t s_vals[TILE];  // the tile's values, copied in asynchronously
   __shared__ uint32_t s_tile_start[kRadix];
   __shared__ uint32_t s_dest[kRadix];
+  __shared__ uint32_t s_code[kRadix];  // each present digit's compact code (few-digit places)
   __shared__ uint64_t s_sums[kSortWarps];
   __shared__ uint32_t s_tile;
 
@@ -383,6 +402,21 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   const uint64_t seg_end = a.segs.end[seg];
   const uint64_t base = seg_begin + (uint64_t)local_tile * TILE;
   const uint32_t n = (uint32_t)min((uint64_t)TILE, seg_end - base);
+
+  // A place of the segment holding k < 129 distinct digits ranks on a compact
+  // code of ceil(log2 k) bits (the high places of depth keys: a few exponents)
+  const uint32_t* seg_hist = a.hist + ((size_t)seg * a.passes + a.place) * kRadix;
+  int nbits = 8;
+  {
+    const bool present = seg_hist[tid] != 0u;
+    const int distinct = __syncthreads_count(present);
+    if (distinct <= 128) {
+      uint64_t unused;
+      s_code[tid] = (uint32_t)block_exclusive_scan(present ? 1u : 0u, s_sums, &unused);
+      nbits = distinct <= 1 ? 0 : 32 - __clz(distinct - 1);
+      __syncthreads();
+    }
+  }
 
   // Load: warp w holds tile positions [w * 512, (w + 1) * 512), item j at j * 32 + lane.
   // Keys go to registers; values go straight to shared memory (cp.async, no
@@ -412,21 +446,33 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
 
   // Rank the keys: items in position order, equal digits counted by their lowest lane
   const uint32_t lt = lanemask_lt();
+  auto rank_items = [&](auto compact) {
 #pragma unroll
-  for (int j = 0; j < ITEMS; j++) {
-    const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
-    const bool ranked = pos < n;
-    const uint32_t d = ranked ? (key[j] >> a.shift) & 0xffu : kNotRanked;
-    const uint32_t peers = peers_of(d, ranked);
-    const int leader = __ffs(peers) - 1;
-    uint32_t old = 0;
-    if (lane == leader && d != kNotRanked) {
-      old = s_whist[warp][d];
-      s_whist[warp][d] = old + (uint32_t)__popc(peers);
+    for (int j = 0; j < ITEMS; j++) {
+      const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+      const bool ranked = pos < n;
+      const uint32_t d = ranked ? (key[j] >> a.shift) & 0xffu : kNotRanked;
+      uint32_t peers;
+      if constexpr (decltype(compact)::value) {
+        peers = peers_of_code(ranked ? s_code[d] : 0u, ranked, nbits);
+      } else {
+        peers = peers_of(d, ranked);
+      }
+      const int leader = __ffs(peers) - 1;
+      uint32_t old = 0;
+      if (lane == leader && d != kNotRanked) {
+        old = s_whist[warp][d];
+        s_whist[warp][d] = old + (uint32_t)__popc(peers);
+      }
+      old = __shfl_sync(0xffffffffu, old, leader);
+      rank[j] = old + (uint32_t)__popc(peers & lt);
+      __syncwarp();
     }
-    old = __shfl_sync(0xffffffffu, old, leader);
-    rank[j] = old + (uint32_t)__popc(peers & lt);
-    __syncwarp();
+  };
+  if (nbits >= 8) {
+    rank_items(std::false_type{});
+  } else {
+    rank_items(std::true_type{});
   }
   __syncthreads();
 
@@ -446,7 +492,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   if (!silent) st_relaxed64(my_word, ep | (local_tile == 0 ? kFlagInclusive : kFlagAggregate) | total);
 
   // Tile-local digit starts (low word) and the segment's digit offsets (high word) in one scan
-  const uint32_t seg_count = a.hist[((size_t)seg * a.passes + a.place) * kRadix + d];
+  const uint32_t seg_count = seg_hist[d];
   uint64_t both_total;
   const uint64_t both = block_exclusive_scan(((uint64_t)seg_count << 32) | total, s_sums, &both_total);
   const uint32_t tile_start = (uint32_t)both;
@@ -609,7 +655,7 @@ struct CoopShape {
   static constexpr int kWarps = THREADS / 32;
   static constexpr uint32_t kSub = THREADS * ITEMS;  // keys of a sub-tile
   // shared words: per-warp digit counts, exchange, values, and 256-word tables
-  static constexpr size_t kWords = (size_t)kWarps * kRadix + 2 * (size_t)kSub + 8 * kRadix + 32;
+  static constexpr size_t kWords = (size_t)kWarps * kRadix + 2 * (size_t)kSub + 9 * kRadix + 32;
   static constexpr size_t kBytes = kWords * 4;
 };
 
@@ -626,8 +672,9 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
   uint32_t* s_start = s_cnt + kRadix;                  // [256] their exclusive scan (tile-local starts)
   uint32_t* s_blk = s_start + kRadix;                  // [256] the block's digit counts of this pass
   uint32_t* s_base = s_blk + kRadix;                   // [256] the next destination of each digit
-  uint32_t* s_part = s_base + kRadix;                  // [4][256] partial sums over earlier blocks
-  uint32_t* s_wsum = s_part + 4 * kRadix;              // [8] scan scratch
+  uint32_t* s_part = s_base + kRadix;                  // [4][256] partial sums (earlier blocks, warp groups)
+  uint32_t* s_code = s_part + 4 * kRadix;              // [256] each present digit's compact code
+  uint32_t* s_wsum = s_code + kRadix;                  // [8] scan scratch, [9]: the code's bits
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -671,33 +718,52 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
       key[j] = pos < n ? __ldcg(&kin[start + pos]) & a.key_mask : 0u;
     }
     __syncthreads();  // s_whist cleared
-#pragma unroll
-    for (int j = 0; j < ITEMS; j++) {
-      const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
-      const bool ranked = pos < n;
-      const uint32_t d = ranked ? (key[j] >> shift) & 0xffu : kNotRanked;
-      const uint32_t peers = peers_of(d, ranked);
-      const int leader = __ffs(peers) - 1;
-      uint32_t old = 0;
+    if (warp_base < n) {  // warps past the sub-tile's keys have nothing to rank
+      const int nbits = (int)s_wsum[9];
       uint32_t* h = s_whist + warp * kRadix;
-      if (lane == leader && d != kNotRanked) {
-        old = h[d];
-        h[d] = old + (uint32_t)__popc(peers);
+#pragma unroll
+      for (int j = 0; j < ITEMS; j++) {
+        const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+        const bool ranked = pos < n;
+        const uint32_t d = ranked ? (key[j] >> shift) & 0xffu : kNotRanked;
+        const uint32_t peers = nbits >= 8 ? peers_of(d, ranked) : peers_of_code(ranked ? s_code[d] : 0u, ranked, nbits);
+        const int leader = __ffs(peers) - 1;
+        uint32_t old = 0;
+        if (lane == leader && d != kNotRanked) {
+          old = h[d];
+          h[d] = old + (uint32_t)__popc(peers);
+        }
+        old = __shfl_sync(0xffffffffu, old, leader);
+        rank[j] = old + (uint32_t)__popc(peers & lt);
+        __syncwarp();
       }
-      old = __shfl_sync(0xffffffffu, old, leader);
-      rank[j] = old + (uint32_t)__popc(peers & lt);
-      __syncwarp();
     }
     __syncthreads();
-    uint32_t total = 0;
-    if (tid < kRadix) {
-      for (int w = 0; w < kWarps; w++) {
-        const uint32_t c = s_whist[w * kRadix + tid];
-        s_whist[w * kRadix + tid] = total;
-        total += c;
-      }
-      s_cnt[tid] = total;
+    // Each digit's counts made exclusive over the warps: thread (q, d) takes
+    // warps [8q, 8q + 8), then adds the earlier groups' totals
+    constexpr int kGroups = THREADS / kRadix;
+    const int q = tid / kRadix, dg = tid % kRadix;
+    uint32_t part = 0;
+#pragma unroll
+    for (int w = q * 8; w < q * 8 + 8; w++) {
+      const uint32_t c = s_whist[w * kRadix + dg];
+      s_whist[w * kRadix + dg] = part;
+      part += c;
     }
+    s_part[q * kRadix + dg] = part;
+    __syncthreads();
+    uint32_t total = 0, before = 0;
+#pragma unroll
+    for (int g = 0; g < kGroups; g++) {
+      const uint32_t v = s_part[g * kRadix + dg];
+      before += g < q ? v : 0u;
+      total += v;
+    }
+    if (q > 0) {
+#pragma unroll
+      for (int w = q * 8; w < q * 8 + 8; w++) s_whist[w * kRadix + dg] += before;
+    }
+    if (tid < kRadix) s_cnt[tid] = total;
     const uint32_t st = digit_exclusive_scan<THREADS>(tid < kRadix ? total : 0u, s_wsum);
     if (tid < kRadix) s_start[tid] = st;
     __syncthreads();
@@ -711,6 +777,15 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
     uint32_t* kout = last ? a.keys_out : (to_a ? a.keys_a : a.keys_b);
     uint32_t* vout = last ? a.vals_out : (to_a ? a.vals_a : a.vals_b);
 
+    // A compact code of the digits this place holds (from its histogram): a
+    // place of k distinct digits ranks with ceil(log2 k) ballots
+    {
+      const bool present = tid < kRadix && a.hist[place * kRadix + tid] != 0u;
+      const uint32_t code = digit_exclusive_scan<THREADS>(present ? 1u : 0u, s_wsum);
+      if (tid < kRadix) s_code[tid] = code;
+      const int distinct = __syncthreads_count(present);
+      if (tid == 0) s_wsum[9] = distinct <= 1 ? 0u : (uint32_t)(32 - __clz(distinct - 1));
+    }
     // The block's digit counts of this pass
     if (tid < kRadix) s_blk[tid] = 0;
     for (uint32_t sub = 0; sub < nsub; sub++) {
@@ -750,15 +825,18 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
     for (uint32_t sub = 0; sub < nsub; sub++) {
       const uint32_t n = nsub == 1 ? min(kSub, len) : load_rank(sub, shift, true);
       const uint64_t start = seg_begin + lo + (uint64_t)sub * kSub;
+      const bool busy = warp_base < n;  // the warp holds keys of this sub-tile
+      if (busy) {
 #pragma unroll
-      for (int j = 0; j < ITEMS; j++) {
-        const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
-        if (pos < n) {
-          const uint32_t dj = (key[j] >> shift) & 0xffu;
-          rank[j] += s_start[dj] + s_whist[warp * kRadix + dj];
-          s_exchange[rank[j]] = key[j];
-        } else {
-          rank[j] = 0xffffffffu;
+        for (int j = 0; j < ITEMS; j++) {
+          const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+          if (pos < n) {
+            const uint32_t dj = (key[j] >> shift) & 0xffu;
+            rank[j] += s_start[dj] + s_whist[warp * kRadix + dj];
+            s_exchange[rank[j]] = key[j];
+          } else {
+            rank[j] = 0xffffffffu;
+          }
         }
       }
       __syncthreads();
@@ -767,7 +845,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
       for (int k = 0; k < ITEMS; k++) {
         const uint32_t i = (uint32_t)k * THREADS + tid;
         dest[k] = 0xffffffffu;
-        if (i < n) {
+        if ((uint32_t)k * THREADS < n && i < n) {
           const uint32_t kk = s_exchange[i];
           const uint32_t dd = (kk >> shift) & 0xffu;
           const uint32_t dst = s_base[dd] + (i - s_start[dd]);
@@ -781,19 +859,21 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
       __syncthreads();
       const bool vec = vin && (reinterpret_cast<uintptr_t>(vin + start) & 15u) == 0;
       const uint32_t staged = vec ? (n & ~3u) : 0u;
+      if (busy) {
 #pragma unroll
-      for (int j = 0; j < ITEMS; j++) {
-        if (rank[j] != 0xffffffffu) {
-          const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
-          const uint32_t v = !vin ? (uint32_t)(start - seg_begin) + pos
-                                  : (pos < staged ? s_vals[pos] : __ldcg(&vin[start + pos]));
-          s_exchange[rank[j]] = v;
+        for (int j = 0; j < ITEMS; j++) {
+          if (rank[j] != 0xffffffffu) {
+            const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+            const uint32_t v = !vin ? (uint32_t)(start - seg_begin) + pos
+                                    : (pos < staged ? s_vals[pos] : __ldcg(&vin[start + pos]));
+            s_exchange[rank[j]] = v;
+          }
         }
       }
       __syncthreads();
 #pragma unroll
       for (int k = 0; k < ITEMS; k++) {
-        if (dest[k] != 0xffffffffu) vout[dest[k]] = s_exchange[(uint32_t)k * THREADS + tid];
+        if ((uint32_t)k * THREADS < n && dest[k] != 0xffffffffu) vout[dest[k]] = s_exchange[(uint32_t)k * THREADS + tid];
       }
       if (tid < kRadix) s_base[tid] += s_cnt[tid];
       __syncthreads();
@@ -894,12 +974,18 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
   }
   if (err != cudaSuccess) return err;
   n_launch++;
-  // Small sorts after a partition take their digit passes in 1024-key tiles: a
-  // pass's time is then one short tile's chain (its tile count at most four times
-  // the 4096-key count), when the lookback words hold the extra tiles
-  const uint32_t small_tiles = sort_small_pass_tiles(c.segs.max_tiles);
-  const bool small = drop && small_tiles != 0 && (uint64_t)passes * small_tiles * kRadix <= c.lookback_words;
-  const uint32_t pass_tiles = small ? small_tiles : c.segs.max_tiles;
+  // After a partition the digit passes may take shorter tiles (c.pass_items
+  // keys a thread; 0: 1024-key tiles for small sorts, else 4096): a pass's
+  // time is then one short tile's chain, when the lookback words hold the
+  // extra tiles. Without the partition the passes keep the 4096-key tiles of
+  // the segments as given.
+  int items = kSortItems;
+  if (drop) {
+    const int want = c.pass_items ? c.pass_items : (sort_small_pass_tiles(c.segs.max_tiles) ? kSmallItems : kSortItems);
+    const uint32_t tiles = c.segs.max_tiles * (uint32_t)(kSortItems / want);
+    if ((want == 4 || want == 8 || want == 16) && (uint64_t)passes * tiles * kRadix <= c.lookback_words) items = want;
+  }
+  const uint32_t pass_tiles = c.segs.max_tiles * (uint32_t)(kSortItems / items);
   // Without the partition every key is valid: the digit passes use the segments as given
   SortSegments vsegs = drop ? SortSegments{sc.vbegin, sc.vend, sc.vtiles, c.segs.count, pass_tiles} : c.segs;
 
@@ -929,7 +1015,7 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     p.vbegin = sc.vbegin;
     p.vend = sc.vend;
     p.vtiles = sc.vtiles;
-    p.pass_tile = small ? (uint32_t)(kSortThreads * kSmallItems) : (uint32_t)kSortTile;
+    p.pass_tile = (uint32_t)(kSortThreads * items);
     err = launch_after(k_partition, c.segs.max_tiles, kSortThreads, 0, stream, p);
     if (err != cudaSuccess) return err;
     n_launch++;
@@ -992,10 +1078,12 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     a.counter = sc.counters + place;
     a.silent_tile = place == c.silent_pass ? 0u : ~0u;
     const bool first = place == 0 && !drop;
+    const bool keys = !(last && a.keys_out == nullptr);
     void (*kernel)(PassArgs) =
         first ? k_onesweep<true, true, kSortItems>
-              : (last && a.keys_out == nullptr) ? (small ? k_onesweep<false, false, kSmallItems> : k_onesweep<false, false, kSortItems>)
-                                                : (small ? k_onesweep<false, true, kSmallItems> : k_onesweep<false, true, kSortItems>);
+        : items == 4 ? (keys ? k_onesweep<false, true, 4> : k_onesweep<false, false, 4>)
+        : items == 8 ? (keys ? k_onesweep<false, true, 8> : k_onesweep<false, false, 8>)
+                     : (keys ? k_onesweep<false, true, kSortItems> : k_onesweep<false, false, kSortItems>);
     err = launch_after(kernel, pass_tiles, kSortThreads, 0, stream, a);
     if (err != cudaSuccess) return err;
     n_launch++;

@@ -119,6 +119,12 @@ def scale_camera():
     return Camera.mono((0.0, 0.5, 3.0), (0.0, 0.0, 0.0), 50.0, 1920, 1080)
 
 
+def all_visible_camera():
+    """1920x1080, vertical fov 50, at (0, 0.5, 30) looking at the origin: the
+    whole [-5, 5]^3 box of the mixture tables lies inside the view's culls."""
+    return Camera.mono((0.0, 0.5, 30.0), (0.0, 0.0, 0.0), 50.0, 1920, 1080)
+
+
 def stereo_camera():
     """Two eyes 64 mm apart, 2064x2208 each, vertical fov 100, the head at (0, 0.5, 3)."""
     return Camera.stereo((0.0, 0.5, 3.0), (0.0, 0.0, 0.0), 100.0, 2064, 2208, baseline=0.064)

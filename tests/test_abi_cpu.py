@@ -47,15 +47,17 @@ def test_struct_layouts_match_the_c_compiler(tmp_path):
     src = tmp_path / "sizes.c"
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "radix_b200.h"\n'
-        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(rdx_table), sizeof(rdx_params),'
+        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(rdx_table), sizeof(rdx_params),'
         ' sizeof(rdx_eye), sizeof(rdx_camera), sizeof(rdx_object), sizeof(rdx_outputs), sizeof(rdx_view),'
-        ' offsetof(rdx_camera, width), offsetof(rdx_table, ext_sh), offsetof(rdx_view, camera)); return 0;}\n')
+        ' sizeof(rdx_tune_result), offsetof(rdx_camera, width), offsetof(rdx_table, ext_sh), offsetof(rdx_view, camera),'
+        ' offsetof(rdx_tune_result, cand_ms)); return 0;}\n')
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     want = [ctypes.sizeof(t) for t in (_abi.rdx_table, _abi.rdx_params, _abi.rdx_eye, _abi.rdx_camera, _abi.rdx_object,
-                                       _abi.rdx_outputs, _abi.rdx_view)]
-    want += [_abi.rdx_camera.width.offset, _abi.rdx_table.ext_sh.offset, _abi.rdx_view.camera.offset]
+                                       _abi.rdx_outputs, _abi.rdx_view, _abi.rdx_tune_result)]
+    want += [_abi.rdx_camera.width.offset, _abi.rdx_table.ext_sh.offset, _abi.rdx_view.camera.offset,
+             _abi.rdx_tune_result.cand_ms.offset]
     assert got == want
 
 

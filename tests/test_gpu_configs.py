@@ -123,3 +123,21 @@ def test_gradient_against_finite_differences_on_1k_sampled_splats(ctx):
            for f, (frac, worst, count) in rep.items()})
     for f, (frac, worst, count) in rep.items():
         assert count > 0 and frac == 1.0, (f, frac, worst, rep)
+
+
+def test_all_visible_pose_draws_every_splat(ctx):
+    """The camera that keeps the whole mixture box inside the culls (the pose
+    that makes the projection read every splat's full row)."""
+    n = 200_000
+    d = syn.mixture_table(n, seed=5, sh_degree=3)
+    cam = syn.all_visible_camera()
+    res = rb.frame([rb.SplatObject(cuda_table(d))], cam, None, 32, NAMES)
+    ref = orc.project([rb.SplatObject(rb.Table.from_dict(d))], cam, None, 32, cull_keys=True)
+    r = compare_projection(res, ref)
+    assert r["cull_disagreements"] == 0 and r["key_mismatches"] == 0, r
+    assert r["drawn"] >= 0.999 * n, r["drawn"]
+    for name, e in r["errors"].items():
+        assert e < TOLERANCE, (name, e)
+    order, visible = orc.sort(ref["keys"], n, 32)
+    assert res["visible"] == visible
+    np.testing.assert_array_equal(u32(res["ordering"]), order[:n])

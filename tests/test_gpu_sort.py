@@ -189,13 +189,14 @@ def test_a_wait_that_runs_out_reports_a_timeout_and_the_context_recovers(bits, v
 SIZES = [0, 1, 4095, 4096, 4097, 70000, 1_000_003, 4_000_000]
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", range(7))
 @pytest.mark.parametrize("bits", BITS)
 def test_every_digit_pass_variant_sorts_bit_exact(variant, bits):
-    """Onesweep passes (0) and the cooperative kernel's variants (1024x16,
-    512x16, 1024x8 threads x keys): SortKeys.sort (partition, then the valid
-    keys) and WgpuRadixSort.sort (in place, every key ranked) on the reference
-    grid, up to 4M keys (several sub-tiles a block)."""
+    """Onesweep passes with tiles by size (0) or of 4096, 2048 and 1024 keys
+    (4-6) and the cooperative kernel's variants (1-3: 1024x16, 512x16, 1024x8
+    threads x keys): SortKeys.sort (partition, then the valid keys) and
+    WgpuRadixSort.sort (in place, every key ranked) on the reference grid, up
+    to 4M keys (several sub-tiles a block)."""
     c = rb.Context(0)
     c.set_sort_variant(variant)
     for count in SIZES:
@@ -214,7 +215,7 @@ def test_every_digit_pass_variant_sorts_bit_exact(variant, bits):
     c.close()
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", range(7))
 def test_every_digit_pass_variant_gives_the_frame_order(variant):
     from radix_b200 import synthetic as syn
     d = syn.mixture_table(1_000_000, seed=4, sh_degree=1)
