@@ -33,6 +33,7 @@
 
 #include <map>
 #include <mutex>
+#include <utility>
 
 #include "device_common.cuh"
 #include "rdx_internal.h"
@@ -40,9 +41,7 @@
 namespace rdx {
 namespace {
 
-constexpr int kWarps = 4;                // warps per block unless a launch asks otherwise
-constexpr int kMaxWarps = 8;             // the most warps per block a launch may ask for
-constexpr int kMaxThreads = kMaxWarps * 32;
+constexpr int kWarps = 4;  // warps per block of the launches that do not choose (the warps are independent)
 constexpr int kChunk = kProjTile;      // splats per chunk (a warp's phase 1)
 constexpr int kQueue = 64;             // candidate ring of a warp
 static_assert(kChunk == 32, "a chunk is one warp wide");
@@ -385,6 +384,88 @@ __device__ __forceinline__ void colour(const DevTable& t, uint64_t i, double dx,
   }
 }
 
+// inSortGuard (projection.tsl.ts:145-155), cov form: whether splat i may show
+// in the head's view widened by the guard. The head-space covariance's largest
+// diagonal element and the reach in float64 with every operation explicitly
+// rounded, in the oracle's order, so the guard's decisions (and the keys) are
+// the oracle's. Kept out of line: inlined, its code alone slows the
+// projection of every frame by 5 %, guard or not.
+template <int LAYOUT>
+__device__ __noinline__ bool in_sort_guard(const ProjDesc& sd, uint64_t i, float opac, double ls0, double ls1,
+                                           double ls2, double hx, double hy, double hz) {
+  const DevParams& p = sd.params;
+  const double ls[3] = {ls0, ls1, ls2};
+  double inflate2 = 1.0;
+  if (opac > 1.0f && p.lod_inflate) {
+    const double o = fmin(dadd(dmul((double)opac, 4.0), -3.0), 5.0);
+    const double inflate = pow(exp(__ddiv_rn(dadd(dmul(o, o), -1.0), 2.71828182845904523536)), 1.0 / 3.0);
+    inflate2 = dmul(inflate, inflate);
+  }
+  double cv[9];  // object-space covariance, row-major
+  if constexpr (LAYOUT == RDX_LAYOUT_COV) {
+    double c6[6];
+    load_cov(sd.table, i, c6);
+    cv[0] = c6[0], cv[1] = c6[3], cv[2] = c6[4];
+    cv[3] = c6[3], cv[4] = c6[1], cv[5] = c6[5];
+    cv[6] = c6[4], cv[7] = c6[5], cv[8] = c6[2];
+  } else {
+    // M = R(q) diag(s) (math.tsl.ts:26-44), Sigma = M M^T
+    double q[4];
+    load_quat<LAYOUT>(sd.table, i, q);
+    double qx = q[0], qy = q[1], qz = q[2], qw = q[3];
+    const double ql = __dsqrt_rn(dadd(dadd(dadd(dmul(qx, qx), dmul(qy, qy)), dmul(qz, qz)), dmul(qw, qw)));
+    if (!(ql > 0.0)) {
+      qx = qy = qz = 0.0;
+      qw = 1.0;
+    } else {
+      qx = __ddiv_rn(qx, ql);
+      qy = __ddiv_rn(qy, ql);
+      qz = __ddiv_rn(qz, ql);
+      qw = __ddiv_rn(qw, ql);
+    }
+    const double sx = exp(ls[0]), sy = exp(ls[1]), sz = exp(ls[2]);
+    const double M[9] = {
+        dmul(sx, dadd(1.0, -dmul(2.0, dadd(dmul(qy, qy), dmul(qz, qz))))),
+        dmul(dmul(sy, 2.0), dadd(dmul(qx, qy), -dmul(qw, qz))),
+        dmul(dmul(sz, 2.0), dadd(dmul(qx, qz), dmul(qw, qy))),
+        dmul(dmul(sx, 2.0), dadd(dmul(qx, qy), dmul(qw, qz))),
+        dmul(sy, dadd(1.0, -dmul(2.0, dadd(dmul(qx, qx), dmul(qz, qz))))),
+        dmul(dmul(sz, 2.0), dadd(dmul(qy, qz), -dmul(qw, qx))),
+        dmul(dmul(sx, 2.0), dadd(dmul(qx, qz), -dmul(qw, qy))),
+        dmul(dmul(sy, 2.0), dadd(dmul(qy, qz), dmul(qw, qx))),
+        dmul(sz, dadd(1.0, -dmul(2.0, dadd(dmul(qx, qx), dmul(qy, qy))))),
+    };
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int c = 0; c < 3; c++)
+        cv[r * 3 + c] = dadd(dadd(dmul(M[r * 3 + 0], M[c * 3 + 0]), dmul(M[r * 3 + 1], M[c * 3 + 1])),
+                             dmul(M[r * 3 + 2], M[c * 3 + 2]));
+  }
+  // diag(A Sigma A^T) as (A Sigma) A^T, each sum left to right
+  double ext2 = 0.0;
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    const double a0 = sd.a[r * 4 + 0], a1 = sd.a[r * 4 + 1], a2 = sd.a[r * 4 + 2];
+    double t[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) t[c] = dadd(dadd(dmul(a0, cv[c]), dmul(a1, cv[3 + c])), dmul(a2, cv[6 + c]));
+    const double v = dmul(dadd(dadd(dmul(t[0], a0), dmul(t[1], a1)), dmul(t[2], a2)), inflate2);
+    ext2 = r == 0 ? v : fmax(ext2, v);
+  }
+  const double radius = dmul(__dsqrt_rn(ext2), (double)p.max_std_dev);
+  const double* P = sd.eye[0].proj;
+  const double clx = dadd(dadd(dadd(dmul(P[0], hx), dmul(P[4], hy)), dmul(P[8], hz)), P[12]);
+  const double cly = dadd(dadd(dadd(dmul(P[1], hx), dmul(P[5], hy)), dmul(P[9], hz)), P[13]);
+  const double clw = dadd(dadd(dadd(dmul(P[3], hx), dmul(P[7], hy)), dmul(P[11], hz)), P[15]);
+  const double w = fmax(clw, 1e-6);
+  const double rx = __ddiv_rn(dmul(P[0], radius), w), ry = __ddiv_rn(dmul(P[5], radius), w);
+  const double edge = dadd((double)p.sort_guard, 1.0);
+  const bool inside = dadd(fabs(__ddiv_rn(clx, w)), -rx) <= edge && dadd(fabs(__ddiv_rn(cly, w)), -ry) <= edge;
+  const bool near_head = -hz <= radius;
+  return hz < radius && (inside || near_head);
+}
+
 // A warp's shared memory: its descriptor and its candidate queue (a ring)
 template <int EYES>
 struct WarpSmem {
@@ -396,8 +477,8 @@ struct WarpSmem {
   double e[EYES][6][kQueue];  // per eye: centre ex, ey, ez and clip x, y, w (float64)
 };
 
-template <int LAYOUT, int DEG, int VAR, int EYES>
-__global__ void __launch_bounds__(kMaxThreads) k_project(const ProjDesc* __restrict__ descs, int n_desc, uint32_t total_chunks,
+template <int LAYOUT, int DEG, int VAR, int EYES, int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_project(const ProjDesc* __restrict__ descs, int n_desc, uint32_t total_chunks,
                                                       ProjOutputs out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -639,9 +720,8 @@ __global__ void __launch_bounds__(kMaxThreads) k_project(const ProjDesc* __restr
     __syncwarp();
   };
 
-  const uint32_t wpb = blockDim.x >> 5;  // warps per block (independent of one another)
-  const uint32_t gw = blockIdx.x * wpb + (uint32_t)warp;
-  const uint32_t nw = gridDim.x * wpb;
+  const uint32_t gw = blockIdx.x * WPB + (uint32_t)warp;
+  const uint32_t nw = gridDim.x * WPB;
   // One loop with a single site for each phase keeps the kernel's code small
   // (phase 2 is large; inlined at several sites it thrashes the instruction
   // cache). Each turn either runs phase 2 on a batch of queued splats or
@@ -714,81 +794,9 @@ __global__ void __launch_bounds__(kMaxThreads) k_project(const ProjDesc* __restr
       const bool degenerate = sd.degenerate || zero_cov;
       const bool invisible = op <= 0.0 || op < (double)p.min_alpha || degenerate;
       bool guarded = true;
-      if (p.sort_guard > 0.0f && !invisible) {
-        // inSortGuard (projection.tsl.ts:145-155), cov form: the head-space
-        // covariance's largest diagonal element. float64 with every operation
-        // explicitly rounded, in the oracle's order, so the guard's decisions
-        // (and the keys) are the oracle's
-        double inflate2 = 1.0;
-        if (opac > 1.0f && p.lod_inflate) {
-          const double o = fmin(dadd(dmul((double)opac, 4.0), -3.0), 5.0);
-          const double inflate = pow(exp(__ddiv_rn(dadd(dmul(o, o), -1.0), 2.71828182845904523536)), 1.0 / 3.0);
-          inflate2 = dmul(inflate, inflate);
-        }
-        double cv[9];  // object-space covariance, row-major
-        if constexpr (LAYOUT == RDX_LAYOUT_COV) {
-          double c6[6];
-          load_cov(sd.table, i, c6);
-          cv[0] = c6[0], cv[1] = c6[3], cv[2] = c6[4];
-          cv[3] = c6[3], cv[4] = c6[1], cv[5] = c6[5];
-          cv[6] = c6[4], cv[7] = c6[5], cv[8] = c6[2];
-        } else {
-          // M = R(q) diag(s) (math.tsl.ts:26-44), Sigma = M M^T
-          double q[4];
-          load_quat<LAYOUT>(sd.table, i, q);
-          double qx = q[0], qy = q[1], qz = q[2], qw = q[3];
-          const double ql = __dsqrt_rn(dadd(dadd(dadd(dmul(qx, qx), dmul(qy, qy)), dmul(qz, qz)), dmul(qw, qw)));
-          if (!(ql > 0.0)) {
-            qx = qy = qz = 0.0;
-            qw = 1.0;
-          } else {
-            qx = __ddiv_rn(qx, ql);
-            qy = __ddiv_rn(qy, ql);
-            qz = __ddiv_rn(qz, ql);
-            qw = __ddiv_rn(qw, ql);
-          }
-          const double sx = exp(ls[0]), sy = exp(ls[1]), sz = exp(ls[2]);
-          const double M[9] = {
-              dmul(sx, dadd(1.0, -dmul(2.0, dadd(dmul(qy, qy), dmul(qz, qz))))),
-              dmul(dmul(sy, 2.0), dadd(dmul(qx, qy), -dmul(qw, qz))),
-              dmul(dmul(sz, 2.0), dadd(dmul(qx, qz), dmul(qw, qy))),
-              dmul(dmul(sx, 2.0), dadd(dmul(qx, qy), dmul(qw, qz))),
-              dmul(sy, dadd(1.0, -dmul(2.0, dadd(dmul(qx, qx), dmul(qz, qz))))),
-              dmul(dmul(sz, 2.0), dadd(dmul(qy, qz), -dmul(qw, qx))),
-              dmul(dmul(sx, 2.0), dadd(dmul(qx, qz), -dmul(qw, qy))),
-              dmul(dmul(sy, 2.0), dadd(dmul(qy, qz), dmul(qw, qx))),
-              dmul(sz, dadd(1.0, -dmul(2.0, dadd(dmul(qx, qx), dmul(qy, qy))))),
-          };
-#pragma unroll
-          for (int r = 0; r < 3; r++)
-#pragma unroll
-            for (int c = 0; c < 3; c++)
-              cv[r * 3 + c] = dadd(dadd(dmul(M[r * 3 + 0], M[c * 3 + 0]), dmul(M[r * 3 + 1], M[c * 3 + 1])),
-                                   dmul(M[r * 3 + 2], M[c * 3 + 2]));
-        }
-        // diag(A Sigma A^T) as (A Sigma) A^T, each sum left to right
-        double ext2 = 0.0;
-#pragma unroll
-        for (int r = 0; r < 3; r++) {
-          const double a0 = sd.a[r * 4 + 0], a1 = sd.a[r * 4 + 1], a2 = sd.a[r * 4 + 2];
-          double t[3];
-#pragma unroll
-          for (int c = 0; c < 3; c++) t[c] = dadd(dadd(dmul(a0, cv[c]), dmul(a1, cv[3 + c])), dmul(a2, cv[6 + c]));
-          const double v = dmul(dadd(dadd(dmul(t[0], a0), dmul(t[1], a1)), dmul(t[2], a2)), inflate2);
-          ext2 = r == 0 ? v : fmax(ext2, v);
-        }
-        const double radius = dmul(__dsqrt_rn(ext2), (double)p.max_std_dev);
-        const double* P = sd.eye[0].proj;
-        const double clx = dadd(dadd(dadd(dmul(P[0], hx), dmul(P[4], hy)), dmul(P[8], hz)), P[12]);
-        const double cly = dadd(dadd(dadd(dmul(P[1], hx), dmul(P[5], hy)), dmul(P[9], hz)), P[13]);
-        const double clw = dadd(dadd(dadd(dmul(P[3], hx), dmul(P[7], hy)), dmul(P[11], hz)), P[15]);
-        const double w = fmax(clw, 1e-6);
-        const double rx = __ddiv_rn(dmul(P[0], radius), w), ry = __ddiv_rn(dmul(P[5], radius), w);
-        const double edge = dadd((double)p.sort_guard, 1.0);
-        const bool inside = dadd(fabs(__ddiv_rn(clx, w)), -rx) <= edge && dadd(fabs(__ddiv_rn(cly, w)), -ry) <= edge;
-        const bool near_head = -hz <= radius;
-        guarded = hz < radius && (inside || near_head);
-      }
+      // inSortGuard, off by default: out of line, so the kernel's code stays small
+      if (p.sort_guard > 0.0f && !invisible)
+        guarded = in_sort_guard<LAYOUT>(sd, i, opac, ls[0], ls[1], ls[2], hx, hy, hz);
       kv = key_of_bits(__float_as_uint(__double2float_rn(distance)), sd.sort_bits);
       if (!cull_keys && !invisible && guarded) key = kv;
       if (!sd.keys_only && !invisible) {
@@ -867,83 +875,79 @@ using ProjKernel = void (*)(const ProjDesc*, int, uint32_t, ProjOutputs);
 
 struct Picked {
   ProjKernel fn;
-  int smem;
+  int smem;   // per block
+  int warps;  // per block
 };
 
-// smem: shared memory per warp (a block holds one WarpSmem per warp)
+// Raw tables (the benchmark's) may launch with 2, 4 or 8 warps per block; the
+// other layouts with 4
 template <int LAYOUT, int DEG, int VAR, int EYES>
-Picked picked() {
-  return {k_project<LAYOUT, DEG, VAR, EYES>, (int)sizeof(WarpSmem<EYES>)};
+Picked picked(int warps) {
+  if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
+    if (warps == 2) return {k_project<LAYOUT, DEG, VAR, EYES, 2>, (int)(2 * sizeof(WarpSmem<EYES>)), 2};
+    if (warps == 8) return {k_project<LAYOUT, DEG, VAR, EYES, 8>, (int)(8 * sizeof(WarpSmem<EYES>)), 8};
+  }
+  return {k_project<LAYOUT, DEG, VAR, EYES, kWarps>, (int)(kWarps * sizeof(WarpSmem<EYES>)), kWarps};
 }
 
 template <int LAYOUT, int DEG, int VAR>
-Picked pick_eyes(int eyes) {
-  return eyes == 2 ? picked<LAYOUT, DEG, VAR, 2>() : picked<LAYOUT, DEG, VAR, 1>();
+Picked pick_eyes(int eyes, int warps) {
+  return eyes == 2 ? picked<LAYOUT, DEG, VAR, 2>(warps) : picked<LAYOUT, DEG, VAR, 1>(warps);
 }
 
 template <int LAYOUT, int VAR>
-Picked pick_degree(int degree, int eyes) {
+Picked pick_degree(int degree, int eyes, int warps) {
   switch (degree) {
-    case 0: return pick_eyes<LAYOUT, 0, VAR>(eyes);
-    case 1: return pick_eyes<LAYOUT, 1, VAR>(eyes);
-    case 2: return pick_eyes<LAYOUT, 2, VAR>(eyes);
-    case 3: return pick_eyes<LAYOUT, 3, VAR>(eyes);
-    default: return pick_eyes<LAYOUT, 4, VAR>(eyes);
+    case 0: return pick_eyes<LAYOUT, 0, VAR>(eyes, warps);
+    case 1: return pick_eyes<LAYOUT, 1, VAR>(eyes, warps);
+    case 2: return pick_eyes<LAYOUT, 2, VAR>(eyes, warps);
+    case 3: return pick_eyes<LAYOUT, 3, VAR>(eyes, warps);
+    default: return pick_eyes<LAYOUT, 4, VAR>(eyes, warps);
   }
 }
 
 template <int LAYOUT>
-Picked pick_codec(int degree, int codec, int eyes) {
+Picked pick_codec(int degree, int codec, int eyes, int warps) {
   // without SH the codec is immaterial: one kernel
-  if (codec == RDX_SH_PACKED && degree > 0) return pick_degree<LAYOUT, RDX_SH_PACKED>(degree, eyes);
-  return pick_degree<LAYOUT, RDX_SH_EXT>(degree, eyes);
+  if (codec == RDX_SH_PACKED && degree > 0) return pick_degree<LAYOUT, RDX_SH_PACKED>(degree, eyes, warps);
+  return pick_degree<LAYOUT, RDX_SH_EXT>(degree, eyes, warps);
 }
 
-Picked pick_kernel(const DevTable& t, int eyes) {
+Picked pick_kernel(const DevTable& t, int eyes, int warps) {
   switch (t.layout) {
-    case RDX_LAYOUT_EXT: return pick_codec<RDX_LAYOUT_EXT>(t.sh_degree, t.sh_codec, eyes);
-    case RDX_LAYOUT_PACKED: return pick_codec<RDX_LAYOUT_PACKED>(t.sh_degree, t.sh_codec, eyes);
-    case RDX_LAYOUT_COV: return pick_codec<RDX_LAYOUT_COV>(t.sh_degree, t.sh_codec, eyes);
+    case RDX_LAYOUT_EXT: return pick_codec<RDX_LAYOUT_EXT>(t.sh_degree, t.sh_codec, eyes, warps);
+    case RDX_LAYOUT_PACKED: return pick_codec<RDX_LAYOUT_PACKED>(t.sh_degree, t.sh_codec, eyes, warps);
+    case RDX_LAYOUT_COV: return pick_codec<RDX_LAYOUT_COV>(t.sh_degree, t.sh_codec, eyes, warps);
     default:
-      if (t.color_dtype == RDX_DTYPE_F16) return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F16>(t.sh_degree, eyes);
-      return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F32>(t.sh_degree, eyes);
+      if (t.color_dtype == RDX_DTYPE_F16) return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F16>(t.sh_degree, eyes, warps);
+      return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F32>(t.sh_degree, eyes, warps);
   }
 }
 
-// Resident blocks of one projection kernel at a block size on a device, found
-// once (with its shared-memory attribute set) and kept: launches then cost no
-// attribute or occupancy queries
-int resident_blocks(const Picked& k, int warps, int* smem, cudaError_t* err) {
-  struct Key {
-    int device;
-    ProjKernel fn;
-    int warps;
-    bool operator<(const Key& o) const {
-      return device != o.device ? device < o.device : (fn != o.fn ? fn < o.fn : warps < o.warps);
-    }
-  };
+// Resident blocks of one projection kernel on the current device, found once
+// (with its shared-memory attribute set) and kept: a launch then makes no
+// attribute or occupancy query
+int resident_blocks(const Picked& k, cudaError_t* err) {
   static std::mutex mu;
-  static std::map<Key, int> cache;
-  *smem = k.smem * warps;
+  static std::map<std::pair<int, ProjKernel>, int> cache;
   int device = 0;
   *err = cudaGetDevice(&device);
   if (*err != cudaSuccess) return 0;
-  const Key key{device, k.fn, warps};
   {
     std::lock_guard<std::mutex> lock(mu);
-    auto it = cache.find(key);
+    auto it = cache.find({device, k.fn});
     if (it != cache.end()) return it->second;
   }
   int sms = 0, per_sm = 0;
-  *err = cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, *smem);
+  *err = cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k.smem);
   if (*err != cudaSuccess) return 0;
   *err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   if (*err != cudaSuccess) return 0;
-  *err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, warps * 32, *smem);
+  *err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.warps * 32, k.smem);
   if (*err != cudaSuccess) return 0;
   const int blocks = sms * (per_sm < 1 ? 1 : per_sm);
   std::lock_guard<std::mutex> lock(mu);
-  cache[key] = blocks;
+  cache[{device, k.fn}] = blocks;
   return blocks;
 }
 
@@ -959,14 +963,13 @@ cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host
   if (!project_warps_supported(warps)) return cudaErrorInvalidValue;
   // One kernel per launch: the caller groups objects by table kind
   const ProjDesc& d0 = descs_host[0];
-  const Picked k = pick_kernel(d0.table, d0.eyes);
-  int smem = 0;
+  const Picked k = pick_kernel(d0.table, d0.eyes, warps);
   cudaError_t err = cudaSuccess;
-  const int blocks = resident_blocks(k, warps, &smem, &err);
+  const int blocks = resident_blocks(k, &err);
   if (err != cudaSuccess) return err;
-  const uint32_t want = (total_chunks + (uint32_t)warps - 1) / (uint32_t)warps;
+  const uint32_t want = (total_chunks + (uint32_t)k.warps - 1) / (uint32_t)k.warps;
   const uint32_t grid = min(want, (uint32_t)blocks);
-  k.fn<<<grid, warps * 32, smem, stream>>>(descs_dev, n_desc, total_chunks, out);
+  k.fn<<<grid, k.warps * 32, k.smem, stream>>>(descs_dev, n_desc, total_chunks, out);
   return cudaGetLastError();
 }
 

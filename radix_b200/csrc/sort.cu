@@ -26,7 +26,6 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
-#include <type_traits>
 #include <utility>
 
 #include "rdx_internal.h"
@@ -378,7 +377,6 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   __shared__ uint32_t s_vals[TILE];  // the tile's values, copied in asynchronously
   __shared__ uint32_t s_tile_start[kRadix];
   __shared__ uint32_t s_dest[kRadix];
-  __shared__ uint32_t s_code[kRadix];  // each present digit's compact code (few-digit places)
   __shared__ uint64_t s_sums[kSortWarps];
   __shared__ uint32_t s_tile;
 
@@ -402,21 +400,6 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   const uint64_t seg_end = a.segs.end[seg];
   const uint64_t base = seg_begin + (uint64_t)local_tile * TILE;
   const uint32_t n = (uint32_t)min((uint64_t)TILE, seg_end - base);
-
-  // A place of the segment holding k < 129 distinct digits ranks on a compact
-  // code of ceil(log2 k) bits (the high places of depth keys: a few exponents)
-  const uint32_t* seg_hist = a.hist + ((size_t)seg * a.passes + a.place) * kRadix;
-  int nbits = 8;
-  {
-    const bool present = seg_hist[tid] != 0u;
-    const int distinct = __syncthreads_count(present);
-    if (distinct <= 128) {
-      uint64_t unused;
-      s_code[tid] = (uint32_t)block_exclusive_scan(present ? 1u : 0u, s_sums, &unused);
-      nbits = distinct <= 1 ? 0 : 32 - __clz(distinct - 1);
-      __syncthreads();
-    }
-  }
 
   // Load: warp w holds tile positions [w * 512, (w + 1) * 512), item j at j * 32 + lane.
   // Keys go to registers; values go straight to shared memory (cp.async, no
@@ -446,33 +429,21 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
 
   // Rank the keys: items in position order, equal digits counted by their lowest lane
   const uint32_t lt = lanemask_lt();
-  auto rank_items = [&](auto compact) {
 #pragma unroll
-    for (int j = 0; j < ITEMS; j++) {
-      const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
-      const bool ranked = pos < n;
-      const uint32_t d = ranked ? (key[j] >> a.shift) & 0xffu : kNotRanked;
-      uint32_t peers;
-      if constexpr (decltype(compact)::value) {
-        peers = peers_of_code(ranked ? s_code[d] : 0u, ranked, nbits);
-      } else {
-        peers = peers_of(d, ranked);
-      }
-      const int leader = __ffs(peers) - 1;
-      uint32_t old = 0;
-      if (lane == leader && d != kNotRanked) {
-        old = s_whist[warp][d];
-        s_whist[warp][d] = old + (uint32_t)__popc(peers);
-      }
-      old = __shfl_sync(0xffffffffu, old, leader);
-      rank[j] = old + (uint32_t)__popc(peers & lt);
-      __syncwarp();
+  for (int j = 0; j < ITEMS; j++) {
+    const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
+    const bool ranked = pos < n;
+    const uint32_t d = ranked ? (key[j] >> a.shift) & 0xffu : kNotRanked;
+    const uint32_t peers = peers_of(d, ranked);
+    const int leader = __ffs(peers) - 1;
+    uint32_t old = 0;
+    if (lane == leader && d != kNotRanked) {
+      old = s_whist[warp][d];
+      s_whist[warp][d] = old + (uint32_t)__popc(peers);
     }
-  };
-  if (nbits >= 8) {
-    rank_items(std::false_type{});
-  } else {
-    rank_items(std::true_type{});
+    old = __shfl_sync(0xffffffffu, old, leader);
+    rank[j] = old + (uint32_t)__popc(peers & lt);
+    __syncwarp();
   }
   __syncthreads();
 
@@ -492,7 +463,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
   if (!silent) st_relaxed64(my_word, ep | (local_tile == 0 ? kFlagInclusive : kFlagAggregate) | total);
 
   // Tile-local digit starts (low word) and the segment's digit offsets (high word) in one scan
-  const uint32_t seg_count = seg_hist[d];
+  const uint32_t seg_count = a.hist[((size_t)seg * a.passes + a.place) * kRadix + d];
   uint64_t both_total;
   const uint64_t both = block_exclusive_scan(((uint64_t)seg_count << 32) | total, s_sums, &both_total);
   const uint32_t tile_start = (uint32_t)both;
