@@ -388,10 +388,10 @@ __device__ __forceinline__ void colour(const DevTable& t, uint64_t i, double dx,
 // in the head's view widened by the guard. The head-space covariance's largest
 // diagonal element and the reach in float64 with every operation explicitly
 // rounded, in the oracle's order, so the guard's decisions (and the keys) are
-// the oracle's. Kept out of line: inlined, its code alone slows the
-// projection of every frame by 5 %, guard or not.
+// the oracle's. Only the kernels of launches with a guard hold this code: in
+// the others, even unexecuted, it slowed every frame's projection by 5 %.
 template <int LAYOUT>
-__device__ __noinline__ bool in_sort_guard(const ProjDesc& sd, uint64_t i, float opac, double ls0, double ls1,
+__device__ __forceinline__ bool in_sort_guard(const ProjDesc& sd, uint64_t i, float opac, double ls0, double ls1,
                                            double ls2, double hx, double hy, double hz) {
   const DevParams& p = sd.params;
   const double ls[3] = {ls0, ls1, ls2};
@@ -477,7 +477,7 @@ struct WarpSmem {
   double e[EYES][6][kQueue];  // per eye: centre ex, ey, ez and clip x, y, w (float64)
 };
 
-template <int LAYOUT, int DEG, int VAR, int EYES, int WPB>
+template <int LAYOUT, int DEG, int VAR, int EYES, int WPB, bool GUARD>
 __global__ void __launch_bounds__(WPB * 32) k_project(const ProjDesc* __restrict__ descs, int n_desc, uint32_t total_chunks,
                                                       ProjOutputs out) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -794,9 +794,10 @@ __global__ void __launch_bounds__(WPB * 32) k_project(const ProjDesc* __restrict
       const bool degenerate = sd.degenerate || zero_cov;
       const bool invisible = op <= 0.0 || op < (double)p.min_alpha || degenerate;
       bool guarded = true;
-      // inSortGuard, off by default: out of line, so the kernel's code stays small
-      if (p.sort_guard > 0.0f && !invisible)
-        guarded = in_sort_guard<LAYOUT>(sd, i, opac, ls[0], ls[1], ls[2], hx, hy, hz);
+      // inSortGuard (off by default): compiled into the guard's kernels only
+      if constexpr (GUARD) {
+        if (p.sort_guard > 0.0f && !invisible) guarded = in_sort_guard<LAYOUT>(sd, i, opac, ls[0], ls[1], ls[2], hx, hy, hz);
+      }
       kv = key_of_bits(__float_as_uint(__double2float_rn(distance)), sd.sort_bits);
       if (!cull_keys && !invisible && guarded) key = kv;
       if (!sd.keys_only && !invisible) {
@@ -880,47 +881,50 @@ struct Picked {
 };
 
 // Raw tables (the benchmark's) may launch with 2, 4 or 8 warps per block; the
-// other layouts with 4
+// other layouts, and every launch with a sort guard, with 4
 template <int LAYOUT, int DEG, int VAR, int EYES>
-Picked picked(int warps) {
+Picked picked(int warps, bool guard) {
+  constexpr int kSmem = (int)sizeof(WarpSmem<EYES>);
+  if (guard) return {k_project<LAYOUT, DEG, VAR, EYES, kWarps, true>, kWarps * kSmem, kWarps};
   if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
-    if (warps == 2) return {k_project<LAYOUT, DEG, VAR, EYES, 2>, (int)(2 * sizeof(WarpSmem<EYES>)), 2};
-    if (warps == 8) return {k_project<LAYOUT, DEG, VAR, EYES, 8>, (int)(8 * sizeof(WarpSmem<EYES>)), 8};
+    if (warps == 2) return {k_project<LAYOUT, DEG, VAR, EYES, 2, false>, 2 * kSmem, 2};
+    if (warps == 8) return {k_project<LAYOUT, DEG, VAR, EYES, 8, false>, 8 * kSmem, 8};
   }
-  return {k_project<LAYOUT, DEG, VAR, EYES, kWarps>, (int)(kWarps * sizeof(WarpSmem<EYES>)), kWarps};
+  return {k_project<LAYOUT, DEG, VAR, EYES, kWarps, false>, kWarps * kSmem, kWarps};
 }
 
 template <int LAYOUT, int DEG, int VAR>
-Picked pick_eyes(int eyes, int warps) {
-  return eyes == 2 ? picked<LAYOUT, DEG, VAR, 2>(warps) : picked<LAYOUT, DEG, VAR, 1>(warps);
+Picked pick_eyes(int eyes, int warps, bool guard) {
+  return eyes == 2 ? picked<LAYOUT, DEG, VAR, 2>(warps, guard) : picked<LAYOUT, DEG, VAR, 1>(warps, guard);
 }
 
 template <int LAYOUT, int VAR>
-Picked pick_degree(int degree, int eyes, int warps) {
+Picked pick_degree(int degree, int eyes, int warps, bool guard) {
   switch (degree) {
-    case 0: return pick_eyes<LAYOUT, 0, VAR>(eyes, warps);
-    case 1: return pick_eyes<LAYOUT, 1, VAR>(eyes, warps);
-    case 2: return pick_eyes<LAYOUT, 2, VAR>(eyes, warps);
-    case 3: return pick_eyes<LAYOUT, 3, VAR>(eyes, warps);
-    default: return pick_eyes<LAYOUT, 4, VAR>(eyes, warps);
+    case 0: return pick_eyes<LAYOUT, 0, VAR>(eyes, warps, guard);
+    case 1: return pick_eyes<LAYOUT, 1, VAR>(eyes, warps, guard);
+    case 2: return pick_eyes<LAYOUT, 2, VAR>(eyes, warps, guard);
+    case 3: return pick_eyes<LAYOUT, 3, VAR>(eyes, warps, guard);
+    default: return pick_eyes<LAYOUT, 4, VAR>(eyes, warps, guard);
   }
 }
 
 template <int LAYOUT>
-Picked pick_codec(int degree, int codec, int eyes, int warps) {
+Picked pick_codec(int degree, int codec, int eyes, int warps, bool guard) {
   // without SH the codec is immaterial: one kernel
-  if (codec == RDX_SH_PACKED && degree > 0) return pick_degree<LAYOUT, RDX_SH_PACKED>(degree, eyes, warps);
-  return pick_degree<LAYOUT, RDX_SH_EXT>(degree, eyes, warps);
+  if (codec == RDX_SH_PACKED && degree > 0) return pick_degree<LAYOUT, RDX_SH_PACKED>(degree, eyes, warps, guard);
+  return pick_degree<LAYOUT, RDX_SH_EXT>(degree, eyes, warps, guard);
 }
 
-Picked pick_kernel(const DevTable& t, int eyes, int warps) {
+Picked pick_kernel(const DevTable& t, int eyes, int warps, bool guard) {
   switch (t.layout) {
-    case RDX_LAYOUT_EXT: return pick_codec<RDX_LAYOUT_EXT>(t.sh_degree, t.sh_codec, eyes, warps);
-    case RDX_LAYOUT_PACKED: return pick_codec<RDX_LAYOUT_PACKED>(t.sh_degree, t.sh_codec, eyes, warps);
-    case RDX_LAYOUT_COV: return pick_codec<RDX_LAYOUT_COV>(t.sh_degree, t.sh_codec, eyes, warps);
+    case RDX_LAYOUT_EXT: return pick_codec<RDX_LAYOUT_EXT>(t.sh_degree, t.sh_codec, eyes, warps, guard);
+    case RDX_LAYOUT_PACKED: return pick_codec<RDX_LAYOUT_PACKED>(t.sh_degree, t.sh_codec, eyes, warps, guard);
+    case RDX_LAYOUT_COV: return pick_codec<RDX_LAYOUT_COV>(t.sh_degree, t.sh_codec, eyes, warps, guard);
     default:
-      if (t.color_dtype == RDX_DTYPE_F16) return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F16>(t.sh_degree, eyes, warps);
-      return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F32>(t.sh_degree, eyes, warps);
+      if (t.color_dtype == RDX_DTYPE_F16)
+        return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F16>(t.sh_degree, eyes, warps, guard);
+      return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F32>(t.sh_degree, eyes, warps, guard);
   }
 }
 
@@ -963,7 +967,9 @@ cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host
   if (!project_warps_supported(warps)) return cudaErrorInvalidValue;
   // One kernel per launch: the caller groups objects by table kind
   const ProjDesc& d0 = descs_host[0];
-  const Picked k = pick_kernel(d0.table, d0.eyes, warps);
+  bool guard = false;  // an object of the launch keys its splats through the sort guard
+  for (int j = 0; j < n_desc; j++) guard = guard || descs_host[j].params.sort_guard > 0.0f;
+  const Picked k = pick_kernel(d0.table, d0.eyes, warps, guard);
   cudaError_t err = cudaSuccess;
   const int blocks = resident_blocks(k, &err);
   if (err != cudaSuccess) return err;
