@@ -50,6 +50,8 @@ def parse():
                    help="frame: the configuration's camera at (0, 0.5, 3) (about half the splats in view), or a "
                         "camera at (0, 0.5, 30) that keeps every splat inside the culls")
     p.add_argument("--no-tune", action="store_true", help="keep the default kernel choices (no autotuning)")
+    p.add_argument("--variant", type=int, default=None,
+                   help="force a digit-pass variant (rdx_ctx_set_sort_variant's numbering) instead of tuning")
     p.add_argument("--spz-container", default="gzip", choices=["gzip", "ngsp"],
                    help="spz workload: version 3 in gzip (one DEFLATE stream) or SPZ 4 (NGSP, a zstd stream a column)")
     p.add_argument("--workload", default="frame",
@@ -762,6 +764,8 @@ def main():
     ordering = torch.empty(n, dtype=torch.int32, device=device)
     visible = torch.zeros(1, dtype=torch.int32, device=device)
     ctx.reserve(n)
+    if args.variant is not None:
+        ctx.set_sort_variant(args.variant)
 
     def frame_step():
         rb.frame(obj, cam, None, BITS, names, ctx=ctx, out=out, ordering=ordering, visible=visible)
@@ -769,7 +773,7 @@ def main():
     # The frame captured once in a CUDA graph (rb.Batch with one view): each
     # step is one graph launch of the projection and the sort
     batch = rb.Batch([(obj, cam)], None, BITS, names, device=device, ctx=ctx)
-    tuning = None if args.no_tune else batch.tune(reps=5)
+    tuning = None if args.no_tune or args.variant is not None else batch.tune(reps=5)
     graph_kernels = batch.launches()
     ms_total, clock_info = timed(batch.launch, args.steps, args.warmup, world, local)
     batch.synchronize()
@@ -819,7 +823,9 @@ def main():
     sort_ms, sort_runs = phases["sort"]
     proj_avg = proj_ms / max(proj_runs, 1)
     achieved = PROJECT_BYTES * n / (proj_avg / 1e3) / 1e9
-    traffic = ncu_traffic()
+    # ncu DRAM bytes of the projection: captured on 1M splats of the same pose, scaled by the splats processed
+    traffic = ncu_traffic("project_kernel_4m_sh3.md" if args.pose == "scale" else "project_kernel_allvis_1m_sh3.md",
+                          n / (4_000_000 if args.pose == "scale" else 1_000_000))
     line = {
         "metric": METRIC, "value": value, "unit": "Msplats/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
