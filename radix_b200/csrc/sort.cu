@@ -626,7 +626,7 @@ struct CoopShape {
   static constexpr int kWarps = THREADS / 32;
   static constexpr uint32_t kSub = THREADS * ITEMS;  // keys of a sub-tile
   // shared words: per-warp digit counts, exchange, values, and 256-word tables
-  static constexpr size_t kWords = (size_t)kWarps * kRadix + 2 * (size_t)kSub + 9 * kRadix + 32;
+  static constexpr size_t kWords = (size_t)kWarps * kRadix + 2 * (size_t)kSub + (8 + kMaxPasses) * kRadix + 32;
   static constexpr size_t kBytes = kWords * 4;
 };
 
@@ -644,8 +644,8 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
   uint32_t* s_blk = s_start + kRadix;                  // [256] the block's digit counts of this pass
   uint32_t* s_base = s_blk + kRadix;                   // [256] the next destination of each digit
   uint32_t* s_part = s_base + kRadix;                  // [4][256] partial sums (earlier blocks, warp groups)
-  uint32_t* s_code = s_part + 4 * kRadix;              // [256] each present digit's compact code
-  uint32_t* s_wsum = s_code + kRadix;                  // [8] scan scratch, [9]: the code's bits
+  uint32_t* s_code = s_part + 4 * kRadix;              // [passes][256] each present digit's compact code
+  uint32_t* s_wsum = s_code + kMaxPasses * kRadix;     // [8] scan scratch, [9 + place]: the place's code bits
 
   const int tid = threadIdx.x;
   const int lane = tid & 31;
@@ -690,14 +690,14 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
     }
     __syncthreads();  // s_whist cleared
     if (warp_base < n) {  // warps past the sub-tile's keys have nothing to rank
-      const int nbits = (int)s_wsum[9];
+      const int nbits = (int)s_wsum[9 + shift / 8];
       uint32_t* h = s_whist + warp * kRadix;
 #pragma unroll
       for (int j = 0; j < ITEMS; j++) {
         const uint32_t pos = warp_base + (uint32_t)j * 32 + lane;
         const bool ranked = pos < n;
         const uint32_t d = ranked ? (key[j] >> shift) & 0xffu : kNotRanked;
-        const uint32_t peers = nbits >= 8 ? peers_of(d, ranked) : peers_of_code(ranked ? s_code[d] : 0u, ranked, nbits);
+        const uint32_t peers = nbits >= 8 ? peers_of(d, ranked) : peers_of_code(ranked ? s_code[(shift / 8) * kRadix + d] : 0u, ranked, nbits);
         const int leader = __ffs(peers) - 1;
         uint32_t old = 0;
         if (lane == leader && d != kNotRanked) {
@@ -741,6 +741,16 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
     return n;
   };
 
+  // A compact code of the digits each place holds (from its histogram): a
+  // place of k distinct digits ranks with ceil(log2 k) ballots
+  for (int place = 0; place < a.passes; place++) {
+    const bool present = tid < kRadix && a.hist[place * kRadix + tid] != 0u;
+    const uint32_t code = digit_exclusive_scan<THREADS>(present ? 1u : 0u, s_wsum);
+    if (tid < kRadix) s_code[place * kRadix + tid] = code;
+    const int distinct = __syncthreads_count(present);
+    if (tid == 0) s_wsum[9 + place] = distinct <= 1 ? 0u : (uint32_t)(32 - __clz(distinct - 1));
+  }
+
   for (int place = 0; place < a.passes; place++) {
     const int shift = 8 * place;
     const bool last = place == a.passes - 1;
@@ -748,15 +758,6 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
     uint32_t* kout = last ? a.keys_out : (to_a ? a.keys_a : a.keys_b);
     uint32_t* vout = last ? a.vals_out : (to_a ? a.vals_a : a.vals_b);
 
-    // A compact code of the digits this place holds (from its histogram): a
-    // place of k distinct digits ranks with ceil(log2 k) ballots
-    {
-      const bool present = tid < kRadix && a.hist[place * kRadix + tid] != 0u;
-      const uint32_t code = digit_exclusive_scan<THREADS>(present ? 1u : 0u, s_wsum);
-      if (tid < kRadix) s_code[tid] = code;
-      const int distinct = __syncthreads_count(present);
-      if (tid == 0) s_wsum[9] = distinct <= 1 ? 0u : (uint32_t)(32 - __clz(distinct - 1));
-    }
     // The block's digit counts of this pass
     if (tid < kRadix) s_blk[tid] = 0;
     for (uint32_t sub = 0; sub < nsub; sub++) {
