@@ -7,6 +7,7 @@
 // in the same order and build with -ffp-contract=off.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdarg.h>
 #include <stdio.h>
 #include <string.h>
@@ -143,17 +144,28 @@ int finish(rdx_ctx* ctx) {
   return RDX_OK;
 }
 
-// A phase between begin and end is timed with events on the stream when profiling
+// A phase between begin and end is timed with events on the stream when
+// profiling, and marked on the host timeline as an NVTX range named like the
+// reference's renderer phases ("project", "sort"; SplatRenderer.ts:141-142),
+// which a profiler attached to the process shows (a no-op without one)
 struct Phase {
   rdx_ctx* ctx;
   int phase;
   cudaEvent_t start = nullptr;
+  bool marked = false;
   Phase(rdx_ctx* c, int p) : ctx(c), phase(p) {
+    static const char* const kNames[RDX_PHASES] = {"project", "sort", "copy in", "copy out", "batch"};
+    nvtxRangePushA(p >= 0 && p < RDX_PHASES ? kNames[p] : "radix_b200");
+    marked = true;
     if (!ctx || !ctx->profiling) return;
     start = take_event(ctx);
     if (start) cudaEventRecord(start, ctx->stream);
   }
   void end() {
+    if (marked) {
+      nvtxRangePop();
+      marked = false;
+    }
     if (!start) return;
     cudaEvent_t stop = take_event(ctx);
     if (!stop) return;
