@@ -8,7 +8,9 @@ import ctypes
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libradix_b200.so")
+# RADIX_B200_CHECK=1 loads the bounds-checked build (radix_b200/build.py --check)
+LIB_PATH = os.path.join(HERE, "lib", "libradix_b200_check.so" if os.environ.get("RADIX_B200_CHECK") == "1"
+                        else "libradix_b200.so")
 
 RDX_OK = 0
 RDX_ERR_ARG = 1

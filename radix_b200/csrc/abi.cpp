@@ -131,15 +131,23 @@ int ensure_arena(rdx_ctx* ctx, size_t bytes) {
   return RDX_OK;
 }
 
-// Wait for the stream and report a device-side timeout
+// The status of a device error word's bits (cleared by the caller): a
+// bounded wait that gave up, else a clamped index (bounds-checked builds)
+int device_error(rdx_ctx* ctx, uint32_t bits) {
+  if (bits & rdx::kErrTimeout) return fail(ctx, RDX_ERR_TIMEOUT, "a device wait gave up (lookback of a tile never published)");
+  return fail(ctx, RDX_ERR_CUDA, "a device bounds check failed: a kernel computed an index outside its buffer");
+}
+
+// Wait for the stream and report a device-side error
 int finish(rdx_ctx* ctx) {
   RDX_CUDA(cudaMemcpyAsync(ctx->error_host, ctx->error_flag, 4, cudaMemcpyDeviceToHost, ctx->stream), "error flag");
   RDX_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
   if (*ctx->error_host) {
+    const uint32_t bits = *ctx->error_host;
     *ctx->error_host = 0;
     cudaMemsetAsync(ctx->error_flag, 0, 4, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
-    return fail(ctx, RDX_ERR_TIMEOUT, "a device wait gave up (lookback of a tile never published)");
+    return device_error(ctx, bits);
   }
   return RDX_OK;
 }
@@ -2060,10 +2068,11 @@ int rdx_batch_synchronize(rdx_batch* b) {
   RDX_CUDA(cudaMemcpyAsync(b->error_host, b->words, 4, cudaMemcpyDeviceToHost, ctx->stream), "error flag");
   RDX_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
   if (*b->error_host) {
+    const uint32_t bits = *b->error_host;
     *b->error_host = 0;
     cudaMemsetAsync(b->words, 0, 4, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
-    return fail(ctx, RDX_ERR_TIMEOUT, "a device wait gave up (lookback of a tile never published)");
+    return device_error(ctx, bits);
   }
   return RDX_OK;
 }

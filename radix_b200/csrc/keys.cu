@@ -110,7 +110,7 @@ __global__ void __launch_bounds__(kThreads) k_compact(const uint32_t* __restrict
         const uint32_t v = ld_relaxed(&lookback[1 + t]);
         if ((v & flags) == 0) {
           if (++spins > kSpinLimit) {
-            atomicExch(error_flag, 1u);
+            atomicOr(error_flag, kErrTimeout);
             break;
           }
           if (spins > 32) __nanosleep(32);
@@ -133,7 +133,10 @@ __global__ void __launch_bounds__(kThreads) k_compact(const uint32_t* __restrict
   for (int j = 0; j < kCompactItems; j++) {
     if (ballots[j] & (1u << lane)) {
       const uint32_t p = at + (uint32_t)__popc(ballots[j] & lt);
-      if ((uint64_t)p >= n) continue;  // only after a bounded wait gave up
+      if ((uint64_t)p >= n) {  // only after a bounded wait gave up
+        check_failed(error_flag);
+        continue;
+      }
       keys_out[p] = k[j];
       vals_out[p] = (uint32_t)(base + (uint64_t)j * 32 + lane);
     }

@@ -766,8 +766,15 @@ __global__ void __launch_bounds__(WPB * 32) k_project(const ProjDesc* __restrict
     const bool cull_keys = sd.cull_keys && !sd.keys_only;
     const uint64_t i0 = (uint64_t)(chunk - sd.first_tile) * kChunk;
     const uint64_t i = i0 + (uint64_t)lane;
-    const bool live = i < sd.count;
     const uint64_t gi = sd.out_offset + i;
+#ifdef RDX_CHECK
+    // a row of the object whose outputs would fall past the launch's (a planning error)
+    const bool outside = i < sd.count && gi >= sd.out_n;
+    if (outside) check_failed(out.check_flag);
+    const bool live = i < sd.count && !outside;
+#else
+    const bool live = i < sd.count;
+#endif
     if (i0 + (uint64_t)nw * kChunk < sd.count) prefetch_head<LAYOUT>(sd.table, i0 + (uint64_t)nw * kChunk, sd.count, lane);
 
     // ---- phase 1: centre, distance, centre culls ----
@@ -961,8 +968,9 @@ int project_warps_supported(int warps) { return warps == 2 || warps == 4 || warp
 
 cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host, int n_desc, uint32_t total_chunks,
                            const ProjOutputs& out, uint32_t* error_flag, cudaStream_t stream, int warps) {
-  (void)error_flag;  // no device wait in this kernel
   if (total_chunks == 0 || n_desc == 0) return cudaSuccess;
+  ProjOutputs outs = out;
+  outs.check_flag = error_flag;  // no device wait in this kernel: the word records only clamped rows
   if (warps == 0) warps = kWarps;
   if (!project_warps_supported(warps)) return cudaErrorInvalidValue;
   // One kernel per launch: the caller groups objects by table kind
@@ -975,7 +983,7 @@ cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host
   if (err != cudaSuccess) return err;
   const uint32_t want = (total_chunks + (uint32_t)k.warps - 1) / (uint32_t)k.warps;
   const uint32_t grid = min(want, (uint32_t)blocks);
-  k.fn<<<grid, k.warps * 32, k.smem, stream>>>(descs_dev, n_desc, total_chunks, out);
+  k.fn<<<grid, k.warps * 32, k.smem, stream>>>(descs_dev, n_desc, total_chunks, outs);
   return cudaGetLastError();
 }
 

@@ -42,6 +42,23 @@ cudaError_t launch_after(void (*kernel)(Params...), dim3 grid, dim3 block, size_
 }
 #endif
 
+// ---- the device error flag ----
+// Bits of a context's (or batch's) device error word: a bounded wait gave
+// up; an index a kernel computed fell outside its buffer (the kernels clamp
+// such accesses; a build with RDX_CHECK defined also records that they did,
+// since a correct launch never clamps)
+constexpr uint32_t kErrTimeout = 1u;
+constexpr uint32_t kErrBounds = 2u;
+#ifdef __CUDACC__
+__device__ __forceinline__ void check_failed(uint32_t* flag) {
+#ifdef RDX_CHECK
+  if (flag) atomicOr(flag, kErrBounds);
+#else
+  (void)flag;
+#endif
+}
+#endif
+
 // ---- sort ----
 
 constexpr int kSortThreads = 256;
@@ -227,6 +244,7 @@ struct ProjOutputs {
   // memset separates the projection from the sort's kernels); may be null
   uint32_t* zero;
   uint64_t zero_words;
+  uint32_t* check_flag;  // the device error word (bounds-checked builds record clamped rows there)
 };
 
 // Splats per projection chunk (one warp)

@@ -248,6 +248,7 @@ struct PartArgs {
   uint64_t* vend;
   uint32_t* vtiles;            // in tiles of pass_tile keys
   uint32_t pass_tile;
+  uint32_t* error_flag;
 };
 
 constexpr int kPartBlocksPerSm = 8;
@@ -336,12 +337,16 @@ __global__ void __launch_bounds__(kSortThreads, kPartBlocksPerSm) k_partition(Pa
         if (dst < seg_begin + seg_valid) {
           a.keys_front[dst] = key[j];
           a.vals_front[dst] = value;
+        } else {
+          check_failed(a.error_flag);
         }
       } else {
         const uint64_t dst = tail + (pos - r);
         if (dst < seg_end) {
           a.tail_vals[dst] = value;
           if (a.tail_keys) a.tail_keys[dst] = key[j];
+        } else {
+          check_failed(a.error_flag);
         }
       }
     }
@@ -481,7 +486,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
       const uint64_t flag = (v >> 32) == epoch ? (v & kFlagMask) : 0;
       if (flag == 0) {
         if (++spins > a.spin_limit) {
-          atomicExch(a.error_flag, 1u);
+          atomicOr(a.error_flag, kErrTimeout);
           break;
         }
         if (spins > 32) __nanosleep(32);
@@ -522,6 +527,8 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSm) k_onesweep(Pas
       if (dst >= (uint32_t)seg_begin && dst < (uint32_t)seg_end) {
         dest[k] = dst;
         if (WRITE_KEYS) a.keys_out[dst] = kk;
+      } else {
+        check_failed(a.error_flag);
       }
     }
   }
@@ -589,7 +596,7 @@ __device__ __forceinline__ void grid_barrier(const CoopArgs& a, uint32_t target,
     uint32_t spins = 0;
     while (ld_acquire32(a.barrier) < target) {
       if (++spins > a.spin_limit) {
-        atomicExch(a.error_flag, 1u);
+        atomicOr(a.error_flag, kErrTimeout);
         break;
       }
       if (spins > 16) __nanosleep(64);
@@ -824,6 +831,8 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
           if (dst >= (uint32_t)seg_begin && dst < seg_end) {  // in bounds even if a wait gave up
             dest[k] = dst;
             if (kout) kout[dst] = kk;
+          } else {
+            check_failed(a.error_flag);
           }
         }
       }
@@ -988,6 +997,7 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     p.vend = sc.vend;
     p.vtiles = sc.vtiles;
     p.pass_tile = (uint32_t)(kSortThreads * items);
+    p.error_flag = c.error_flag;
     err = launch_after(k_partition, c.segs.max_tiles, kSortThreads, 0, stream, p);
     if (err != cudaSuccess) return err;
     n_launch++;
