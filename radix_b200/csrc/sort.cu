@@ -159,7 +159,9 @@ __device__ __forceinline__ void hist_add16(uint32_t* h, uint32_t d, bool valid) 
 // hidden count. Block 0 also advances the lookback epoch: the word is bumped
 // on the device, so a sort replayed from a CUDA graph still tags its words
 // with a new epoch.
-template <int PASSES>
+// TOP_ONLY: only the top place's histogram (what the cooperative digit passes
+// need; they sum the other places' digit totals from their blocks' counts)
+template <int PASSES, bool TOP_ONLY>
 __global__ void __launch_bounds__(kSortThreads, kCountBlocksPerSm)
     k_sort_count(const uint32_t* __restrict__ keys, uint32_t key_mask, int ref_shift, uint32_t ref_top, int drop,
                  SortSegments segs, uint32_t* __restrict__ hist, uint32_t* __restrict__ valid_count,
@@ -199,7 +201,7 @@ __global__ void __launch_bounds__(kSortThreads, kCountBlocksPerSm)
     const bool valid = in && (!drop || key[j] != key_mask);
     nvalid += valid;
 #pragma unroll
-    for (int p = 0; p < PASSES; p++) hist_add16(sh[warp][p], (key[j] >> (8 * p)) & 0xffu, valid);
+    for (int p = TOP_ONLY ? PASSES - 1 : 0; p < PASSES; p++) hist_add16(sh[warp][p], (key[j] >> (8 * p)) & 0xffu, valid);
   }
   nvalid = __reduce_add_sync(0xffffffffu, nvalid);
   hidden = __reduce_add_sync(0xffffffffu, hidden);
@@ -211,7 +213,7 @@ __global__ void __launch_bounds__(kSortThreads, kCountBlocksPerSm)
   // thread d sums bin d of every place over the warps
   const uint32_t d = (uint32_t)tid;
 #pragma unroll
-  for (int p = 0; p < PASSES; p++) {
+  for (int p = TOP_ONLY ? PASSES - 1 : 0; p < PASSES; p++) {
     uint32_t c = 0;
 #pragma unroll
     for (int w = 0; w < kSortWarps; w++) c += (sh[w][p][d >> 1] >> ((d & 1u) * 16)) & 0xffffu;
@@ -569,7 +571,7 @@ struct CoopArgs {
   uint32_t* vals_out;
   const uint64_t* begin;     // the segment sorted: [begin[0], end[0])
   const uint64_t* end;
-  const uint32_t* hist;      // [passes][256] digit totals of the keys sorted
+  const uint32_t* hist;      // [passes][256]: the top place's digit counts of the keys sorted
   uint32_t* block_counts;    // [blocks][256]
   uint32_t* barrier;         // grid-barrier arrivals of this sort (zero at its start)
   uint32_t* error_flag;
@@ -748,14 +750,17 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
     return n;
   };
 
-  // A compact code of the digits each place holds (from its histogram): a
-  // place of k distinct digits ranks with ceil(log2 k) ballots
-  for (int place = 0; place < a.passes; place++) {
-    const bool present = tid < kRadix && a.hist[place * kRadix + tid] != 0u;
+  // Every place ranks with 8 ballots but the top one, whose histogram the
+  // counting kernel built: a place of k distinct digits (the top byte of depth
+  // keys: a few exponents) ranks on a compact code with ceil(log2 k) ballots
+  if (tid < kMaxPasses) s_wsum[9 + tid] = 8u;
+  {
+    const int top = a.passes - 1;
+    const bool present = tid < kRadix && a.hist[top * kRadix + tid] != 0u;
     const uint32_t code = digit_exclusive_scan<THREADS>(present ? 1u : 0u, s_wsum);
-    if (tid < kRadix) s_code[place * kRadix + tid] = code;
+    if (tid < kRadix) s_code[top * kRadix + tid] = code;
     const int distinct = __syncthreads_count(present);
-    if (tid == 0) s_wsum[9 + place] = distinct <= 1 ? 0u : (uint32_t)(32 - __clz(distinct - 1));
+    if (tid == 0) s_wsum[9 + top] = distinct <= 1 ? 0u : (uint32_t)(32 - __clz(distinct - 1));
   }
 
   for (int place = 0; place < a.passes; place++) {
@@ -780,16 +785,28 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
     {
       constexpr int kQuarters = THREADS >= 4 * kRadix ? 4 : THREADS / kRadix;
       const int q = tid / kRadix, d = tid % kRadix;
+      // every block's count of the digit (its total) and the earlier blocks'; the
+      // exchange buffer is free until the scatter and holds the totals' partial sums
       if (q < kQuarters) {
-        uint32_t sum = 0;
-        const uint32_t per = (b + kQuarters - 1) / kQuarters;
-        const uint32_t from = min((uint32_t)q * per, b), to = min(from + per, b);
+        uint32_t sum = 0, all = 0;
+        const uint32_t per = (G + kQuarters - 1) / kQuarters;
+        const uint32_t from = min((uint32_t)q * per, G), to = min(from + per, G);
 #pragma unroll 8
-        for (uint32_t e = from; e < to; e++) sum += __ldcg(&a.block_counts[(size_t)e * kRadix + d]);
+        for (uint32_t e = from; e < to; e++) {
+          const uint32_t c = __ldcg(&a.block_counts[(size_t)e * kRadix + d]);
+          all += c;
+          sum += e < b ? c : 0u;
+        }
         s_part[q * kRadix + d] = sum;
+        s_exchange[q * kRadix + d] = all;
       }
-      const uint32_t total = tid < kRadix ? a.hist[place * kRadix + tid] : 0u;
-      const uint32_t digit_start = digit_exclusive_scan<THREADS>(total, s_wsum);  // syncs the partials too
+      __syncthreads();
+      uint32_t total = 0;
+      if (tid < kRadix) {
+#pragma unroll
+        for (int k = 0; k < kQuarters; k++) total += s_exchange[k * kRadix + tid];
+      }
+      const uint32_t digit_start = digit_exclusive_scan<THREADS>(total, s_wsum);
       if (tid < kRadix) {
         uint32_t before = 0;
 #pragma unroll
@@ -939,20 +956,16 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     err = cudaMemsetAsync(sc.hist, 0, sort_small_state_words(c.segs.count, passes, c.segs.max_tiles) * 4, stream);
     if (err != cudaSuccess) return err;
   }
-  switch (passes) {
-    case 2:
-      err = launch_after(k_sort_count<2>, c.segs.max_tiles, kSortThreads, 0, stream, c.keys_in, mask, ref_shift, ref_top,
-                         drop, c.segs, sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid, c.epoch);
-      break;
-    case 3:
-      err = launch_after(k_sort_count<3>, c.segs.max_tiles, kSortThreads, 0, stream, c.keys_in, mask, ref_shift, ref_top,
-                         drop, c.segs, sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid, c.epoch);
-      break;
-    default:
-      err = launch_after(k_sort_count<4>, c.segs.max_tiles, kSortThreads, 0, stream, c.keys_in, mask, ref_shift, ref_top,
-                         drop, c.segs, sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid, c.epoch);
-      break;
-  }
+  // One segment may take the cooperative digit passes, which need only the top place's histogram
+  const int n_coop = c.coop != kCoopNone && c.segs.count == 1 && sc.block_counts ? coop_blocks(c.coop) : 0;
+  const bool coop = n_coop > 0 && (uint32_t)n_coop <= kMaxCoopBlocks;
+  using CountKernel = void (*)(const uint32_t*, uint32_t, int, uint32_t, int, SortSegments, uint32_t*, uint32_t*,
+                               uint32_t*, uint32_t*, uint32_t*);
+  const CountKernel count = passes == 2 ? (coop ? k_sort_count<2, true> : k_sort_count<2, false>)
+                            : passes == 3 ? (coop ? k_sort_count<3, true> : k_sort_count<3, false>)
+                                          : (coop ? k_sort_count<4, true> : k_sort_count<4, false>);
+  err = launch_after(count, c.segs.max_tiles, kSortThreads, 0, stream, c.keys_in, mask, ref_shift, ref_top, drop, c.segs,
+                     sc.hist, sc.valid, sc.ref_hidden, sc.tile_valid, c.epoch);
   if (err != cudaSuccess) return err;
   n_launch++;
   // After a partition the digit passes may take shorter tiles (c.pass_items
@@ -1004,9 +1017,9 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     ki = sc.keys_a;
     vi = sc.vals_a;
   }
-  if (c.coop != kCoopNone && c.segs.count == 1 && sc.block_counts) {
-    const int blocks = coop_blocks(c.coop);
-    if (blocks > 0 && (uint32_t)blocks <= kMaxCoopBlocks) {
+  if (coop) {
+    const int blocks = n_coop;
+    {
       const CoopVariant v = coop_variant(c.coop);
       CoopArgs ca{};
       ca.keys_in = ki;
