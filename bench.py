@@ -55,11 +55,12 @@ def parse():
     p.add_argument("--spz-container", default="gzip", choices=["gzip", "ngsp"],
                    help="spz workload: version 3 in gzip (one DEFLATE stream) or SPZ 4 (NGSP, a zstd stream a column)")
     p.add_argument("--workload", default="frame",
-                   choices=["frame", "batched", "stereo", "backward", "ply", "spz", "rdx"],
+                   choices=["frame", "batched", "stereo", "backward", "ply", "spz", "rdx", "census"],
                    help="frame: 4M SH-3 splats, one view (the headline); batched: 16 scenes x 64 views in one "
                         "CUDA graph; stereo: 16M SH-3 fp16 splats, two eyes; backward: the projection's gradient, 1M; "
                         "ply: decoding a 1M-splat PLY file; spz: decoding a 1M-splat SPZ file from host bytes; "
-                        "rdx: decoding a 1M-splat RDX file from host bytes")
+                        "rdx: decoding a 1M-splat RDX file from host bytes; census: every device entry point "
+                        "once a step, each timed alone")
     return p.parse_args()
 
 
@@ -711,6 +712,123 @@ def run_rdx(args, world, rank, local, device):
     }
 
 
+def run_census(args, world, rank, local, device):
+    """Every device entry point once a step, each timed with CUDA events on the
+    library's stream at a size above L2 (or the entry point's own limit), with
+    its algorithmic bytes per unit: the census that an ncu launch list of this
+    workload turns into DRAM bytes and throughput for every kernel."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    import radix_b200 as rb
+    from radix_b200 import _abi
+    from radix_b200 import synthetic as syn
+    ctx = rb.Context(local)
+    n = 32_000_000
+    rng = syn.Mulberry32(11)
+    dist64 = torch.from_numpy(rng.uniform(n) * 10.0).to(device)
+    dist32 = dist64.float()
+    keys = torch.empty(n, dtype=torch.int32, device=device)
+    out_k = torch.empty(n, dtype=torch.int32, device=device)
+    out_v = torch.empty(n, dtype=torch.int32, device=device)
+    count = torch.zeros(1, dtype=torch.int32, device=device)
+    ctx.call("rdx_sort_keys_compute", dist64.data_ptr(), n, 32, keys.data_ptr())
+    keys[::3] = -1  # a third invalid, as a frame's culled splats
+    ordering = torch.empty(rb.align_capacity(n), dtype=torch.int32, device=device)
+    scratch_k, scratch_v = torch.empty_like(keys), torch.empty_like(keys)
+    d = syn.mixture_table(4_000_000, seed=0, sh_degree=SH_DEGREE, device=device)
+    cols = {k: torch.from_numpy(np.ascontiguousarray(d[k])).to(device)
+            for k in ("centers", "log_scales", "quats", "opacities", "colors")}
+    del d
+    table = rb.Table.raw(cols["centers"], cols["log_scales"], cols["quats"], cols["opacities"], cols["colors"],
+                         SH_DEGREE)
+    obj = [rb.SplatObject(table)]
+    cam = syn.scale_camera()
+    names = ("mean2d", "conic", "depth", "opacity", "rgb", "keys")
+    fout = rb._alloc_outputs(names, 4_000_000, 1, device)
+    ford = torch.empty(4_000_000, dtype=torch.int32, device=device)
+    fvis = torch.zeros(1, dtype=torch.int32, device=device)
+    b1 = 1_000_000
+    bobj = [rb.SplatObject(rb.Table.raw(*(cols[k][:b1] for k in ("centers", "log_scales", "quats", "opacities",
+                                                                   "colors")), SH_DEGREE))]
+    bout = rb._alloc_outputs(names, b1, 1, device)
+    g = torch.Generator(device=device).manual_seed(1)
+    up = {k: torch.randn(bout[k].shape, device=device, generator=g) for k in ("mean2d", "conic", "opacity", "rgb")}
+    vis = torch.zeros(1, dtype=torch.int32, device=device)
+
+    def sort(m, variant):
+        ctx.set_sort_variant(variant)
+        ctx.call("rdx_sort", keys.data_ptr(), m, 32, ordering.data_ptr(), ordering.numel(), None)
+
+    def pairs(m):
+        ctx.set_sort_variant(0)
+        ctx.call("rdx_sort_pairs", scratch_k.data_ptr(), scratch_v.data_ptr(), m, 32)
+
+    def noalloc(m):
+        st = _abi.lib().rdx_sort_noalloc(ctypes.c_void_p(keys.data_ptr()), m, 32, ctypes.c_void_p(ordering.data_ptr()),
+                                         ordering.numel(), ctypes.c_void_p(vis.data_ptr()),
+                                         ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream))
+        assert st == _abi.RDX_OK, st
+
+    def frame():
+        ctx.set_sort_variant(1)
+        rb.frame(obj, cam, None, BITS, names, ctx=ctx, out=fout, ordering=ford, visible=fvis)
+
+    # (name, call, units, algorithmic bytes a unit, before: untimed set-up of each call)
+    families = [
+        ("keys from float64 distances", lambda: ctx.call("rdx_sort_keys_compute", dist64.data_ptr(), n, 32,
+                                                         out_k.data_ptr()), n, 12, None),
+        ("keys from float32 distances", lambda: ctx.call("rdx_sort_keys_compute_f32", dist32.data_ptr(), n, 32,
+                                                         out_k.data_ptr()), n, 8, None),
+        ("compaction (a third invalid)", lambda: ctx.call("rdx_compact", keys.data_ptr(), n,
+                                                          ctypes.c_uint32(0xFFFFFFFF), out_k.data_ptr(),
+                                                          out_v.data_ptr(), count.data_ptr()), n, 4 + 8 * 2 / 3, None),
+        ("SortKeys.sort 32M, onesweep passes", lambda: sort(n, 0), n, 68, None),
+        ("SortKeys.sort 2M, cooperative passes", lambda: sort(2_000_000, 1), 2_000_000, 68, None),
+        ("WgpuRadixSort.sort 16M in place", lambda: pairs(16_000_000), 16_000_000, 68,
+         lambda: (scratch_k[:16_000_000].copy_(keys[:16_000_000]), scratch_v[:16_000_000].copy_(keys[:16_000_000]))),
+        ("rdx_sort_noalloc 1M", lambda: noalloc(b1), b1, 68, None),
+        ("frame 4M (projection + sort)", frame, 4_000_000, FRAME_BYTES, None),
+        ("projection backward 1M", lambda: rb.project_backward(bobj, cam, up, bout["opacity"], None, ctx=ctx), b1, 512,
+         lambda: rb.project_collection(bobj, cam, None, BITS, "full", True, names, ctx=ctx, out=bout)),
+    ]
+    peak, peak_kind = peak_hbm()
+    stream = torch.cuda.current_stream(device)
+    results = []
+    launches0 = ctx.launches()
+    for name, call, units, per_unit, before in families:
+        times = []
+        for step in range(args.warmup + args.steps):
+            if before:
+                before()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            call()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if step >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+        ms = statistics.median(times)
+        gbs = per_unit * units / (ms / 1e3) / 1e9
+        results.append({"call": name, "ms": ms, "units": units, "bytes_per_unit": per_unit, "gb_s": gbs,
+                        "frac": gbs / peak})
+    ctx.set_sort_variant(-1)
+    ctx.synchronize()
+    return {
+        "metric": "GB/s of algorithmic bytes per call (every device entry point)",
+        "value": min(r["frac"] for r in results), "unit": "fraction of measured HBM peak (the lowest call)",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sum(r["ms"] for r in results),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 keys, f32+f64 maths",
+        "data": "synthetic (seeded mulberry32)",
+        "config": {"workload": "census: each device entry point once a step, timed alone with CUDA events",
+                   "results": results, "peak": peak, "peak_kind": peak_kind},
+        "e2e": None, "e2e_note": "device-resident inputs; a per-call census",
+        "gpu_launches": ctx.launches() - launches0,
+    }
+
+
 def main():
     global BITS, FRAME_BYTES
     args = parse()
@@ -731,7 +849,7 @@ def main():
             from datetime import timedelta
             dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
         run = {"batched": run_batched, "stereo": run_stereo, "backward": run_backward, "ply": run_ply,
-               "spz": run_spz, "rdx": run_rdx}[args.workload]
+               "spz": run_spz, "rdx": run_rdx, "census": run_census}[args.workload]
         line = run(args, world, rank, local, device)
         if rank == 0:
             print(json.dumps(line))
