@@ -1178,7 +1178,7 @@ int rdx_compact(rdx_ctx* ctx, const uint32_t* keys, uint64_t n, uint32_t invalid
   layout(a);
   if (hk) RDX_CUDA(cudaMemcpyAsync((void*)k, keys, n * 4, cudaMemcpyHostToDevice, ctx->stream), "copy in");
   RDX_CUDA(rdx::launch_compact(k, n, invalid, ko, vo, c, lb, ctx->error_flag, ctx->stream), "compact launch");
-  ctx->launches += n ? 1 : 0;
+  ctx->launches += n ? 3 : 0;
   if (hc) RDX_CUDA(cudaMemcpyAsync(count_out, c, 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");
   // only the first *count_out pairs are meaningful: all n are copied, the rest unspecified
   if (hko) RDX_CUDA(cudaMemcpyAsync(keys_out, ko, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "copy out");

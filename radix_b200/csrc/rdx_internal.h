@@ -158,9 +158,10 @@ cudaError_t launch_keys_f32(const float* d, uint64_t n, int bits, uint32_t* keys
 // visible[s] = (end - begin) - ref_hidden[s], or valid[s] (ref_hidden null)
 cudaError_t launch_visible(const uint64_t* begin, const uint64_t* end, const uint32_t* ref_hidden,
                            const uint32_t* valid, int segments, uint32_t* visible, cudaStream_t s);
-// Order-preserving compaction of keys != invalid; lookback: [tiles] zeroed here
+// Order-preserving compaction of keys != invalid (three launches); tile_valid:
+// ceil(n / 4096) words of scratch
 cudaError_t launch_compact(const uint32_t* keys, uint64_t n, uint32_t invalid, uint32_t* keys_out,
-                           uint32_t* vals_out, uint32_t* count_out, uint32_t* lookback,
+                           uint32_t* vals_out, uint32_t* count_out, uint32_t* tile_valid,
                            uint32_t* error_flag, cudaStream_t s);
 // One segment [0, min(*count, capacity)) and its tiles
 cudaError_t launch_indirect_segments(const uint32_t* count, uint64_t capacity, uint64_t* begin, uint64_t* end,

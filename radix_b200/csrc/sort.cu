@@ -133,28 +133,11 @@ __device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t* s
 
 // ---- counting: every digit place's histogram, valid keys per tile and segment ----
 
-// Per-warp histogram increment, two 16-bit bins a word (a warp adds at most
-// 512 keys, so a bin cannot carry into its neighbour). When every valid lane
-// has the same digit (the high places of depth keys: few exponents) one lane
-// adds them all; otherwise each lane adds its own (the hardware serialises
-// the few lanes that share a bin).
-__device__ __forceinline__ void hist_add16(uint32_t* h, uint32_t d, bool valid) {
-  const uint32_t active = __ballot_sync(0xffffffffu, valid);
-  if (!active) return;
-  const int lane = threadIdx.x & 31;
-  const int first = __ffs(active) - 1;
-  const uint32_t d0 = __shfl_sync(0xffffffffu, d, first);
-  const uint32_t same = __ballot_sync(0xffffffffu, valid && d == d0);
-  if (same == active) {
-    if (lane == first) atomicAdd(&h[d0 >> 1], (uint32_t)__popc(active) << ((d0 & 1u) * 16));
-  } else if (valid) {
-    atomicAdd(&h[d >> 1], 1u << ((d & 1u) * 16));
-  }
-}
-
 // One block per tile: the tile's keys in one read give every digit place's
-// histogram of the valid keys (per-warp shared-memory histograms, summed into
-// the segment's by one global atomic per non-zero bin), the tile's valid count
+// histogram of the valid keys (one 32-bit shared-memory histogram a place for
+// the block, one shared atomic per key and place: the hardware merges the
+// lanes of a warp that add to one bin; summed into the segment's by one global
+// atomic per non-zero bin), the tile's valid count
 // (the partition's offsets), the segment's valid count and the reference's
 // hidden count. Block 0 also advances the lookback epoch: the word is bumped
 // on the device, so a sort replayed from a CUDA graph still tags its words
@@ -166,13 +149,16 @@ __global__ void __launch_bounds__(kSortThreads, kCountBlocksPerSm)
     k_sort_count(const uint32_t* __restrict__ keys, uint32_t key_mask, int ref_shift, uint32_t ref_top, int drop,
                  SortSegments segs, uint32_t* __restrict__ hist, uint32_t* __restrict__ valid_count,
                  uint32_t* __restrict__ ref_hidden, uint32_t* __restrict__ tile_valid, uint32_t* epoch) {
-  __shared__ uint32_t sh[kSortWarps][PASSES][kRadix / 2];
+  static_assert(kSortThreads == kRadix, "a thread a bin");
+  constexpr int kFirst = TOP_ONLY ? PASSES - 1 : 0;  // the first place counted
+  __shared__ uint32_t sh[PASSES - kFirst][kRadix];
   __shared__ uint32_t s_valid[kSortWarps], s_hidden[kSortWarps];
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;
 #pragma unroll
-  for (int w = lane; w < PASSES * kRadix / 2; w += 32) (&sh[warp][0][0])[w] = 0;
+  for (int p = 0; p < PASSES - kFirst; p++) sh[p][tid] = 0;
+  __syncthreads();
   pdl_wait();
   pdl_trigger();
   if (tid == 0 && blockIdx.x == 0) {
@@ -200,8 +186,10 @@ __global__ void __launch_bounds__(kSortThreads, kCountBlocksPerSm)
     hidden += in && (key[j] >> ref_shift) == ref_top;
     const bool valid = in && (!drop || key[j] != key_mask);
     nvalid += valid;
+    if (valid) {
 #pragma unroll
-    for (int p = TOP_ONLY ? PASSES - 1 : 0; p < PASSES; p++) hist_add16(sh[warp][p], (key[j] >> (8 * p)) & 0xffu, valid);
+      for (int p = kFirst; p < PASSES; p++) atomicAdd(&sh[p - kFirst][(key[j] >> (8 * p)) & 0xffu], 1u);
+    }
   }
   nvalid = __reduce_add_sync(0xffffffffu, nvalid);
   hidden = __reduce_add_sync(0xffffffffu, hidden);
@@ -210,13 +198,11 @@ __global__ void __launch_bounds__(kSortThreads, kCountBlocksPerSm)
     s_hidden[warp] = hidden;
   }
   __syncthreads();
-  // thread d sums bin d of every place over the warps
+  // thread d adds bin d of every place to the segment's histogram
   const uint32_t d = (uint32_t)tid;
 #pragma unroll
-  for (int p = TOP_ONLY ? PASSES - 1 : 0; p < PASSES; p++) {
-    uint32_t c = 0;
-#pragma unroll
-    for (int w = 0; w < kSortWarps; w++) c += (sh[w][p][d >> 1] >> ((d & 1u) * 16)) & 0xffffu;
+  for (int p = kFirst; p < PASSES; p++) {
+    const uint32_t c = sh[p - kFirst][d];
     if (c) atomicAdd(&hist[((size_t)seg * PASSES + p) * kRadix + d], c);
   }
   if (tid == 0) {

@@ -108,6 +108,36 @@ def test_compact_keeps_input_order(ctx):
     np.testing.assert_array_equal(u32(ck)[:idx.size], keys[idx])
 
 
+@pytest.mark.parametrize("n", [0, 1, 4095, 4096, 4097, 70_001, 4096 * 1030 + 7])
+@pytest.mark.parametrize("valid", [0.0, 0.5, 1.0])
+def test_compact_ragged_sizes_and_fractions(ctx, n, valid):
+    """Tile edges (4096 keys a tile, more tiles than the scan's 1024 threads),
+    no valid key, every key valid, and an invalid value other than the largest
+    key: the kept keys and their indices in input order, and their count."""
+    invalid = 0x00ABCDEF
+    keys = random_keys(n, 32, n + 3) if n else np.zeros(0, np.uint32)
+    keys[keys == invalid] = 0
+    keys[Mulberry32(7).uniform(n) >= valid] = invalid
+    ck, cv, count = rb.Compact(ctx, invalid=invalid).compact(to_cuda(keys.view(np.int32)) if n else
+                                                          torch.zeros(1, dtype=torch.int32, device="cuda"), n)
+    idx = np.flatnonzero(keys != invalid)
+    assert int(u32(count)[0]) == idx.size
+    np.testing.assert_array_equal(u32(cv)[:idx.size], idx)
+    np.testing.assert_array_equal(u32(ck)[:idx.size], keys[idx])
+
+
+def test_compact_from_host_buffers(ctx):
+    """The same call with host (numpy) buffers: copies in and out around the launches."""
+    n = 300_001
+    keys = random_keys(n, 32, 5)
+    keys[::4] = 0xFFFFFFFF
+    ck, cv, count = rb.Compact(ctx).compact(keys)
+    idx = np.flatnonzero(keys != 0xFFFFFFFF)
+    assert int(count[0]) == idx.size
+    np.testing.assert_array_equal(cv[:idx.size].view(np.uint32), idx)
+    np.testing.assert_array_equal(ck[:idx.size].view(np.uint32), keys[idx])
+
+
 @pytest.mark.parametrize("bits", BITS)
 def test_splat_sorter_values_count_and_draw_args(ctx, bits):
     n = 123_457
@@ -132,8 +162,17 @@ def test_keys_compute_bit_exact(ctx, bits):
     got = u32(rb.SortKeys.compute(to_cuda(d), bits, ctx))
     np.testing.assert_array_equal(got, orc.sort_keys(d, bits))
     d32 = d.astype(np.float32)
+    ref32 = np.array([orc.sort_key_f32(x, bits) for x in d32], dtype=np.uint32)
     got32 = u32(rb.SortKeys.compute(to_cuda(d32), bits, ctx))
-    np.testing.assert_array_equal(got32, np.array([orc.sort_key_f32(x, bits) for x in d32], dtype=np.uint32))
+    np.testing.assert_array_equal(got32, ref32)
+    # distances not 16-byte aligned (the scalar kernels) and lengths of every remainder mod 4
+    for off in (1, 2, 3):
+        for cut in (0, 1, 2, 3):
+            end = d.size - cut
+            got = u32(rb.SortKeys.compute(to_cuda(d)[off:end], bits, ctx))
+            np.testing.assert_array_equal(got, orc.sort_keys(d[off:end], bits), err_msg=f"f64 {off} {cut}")
+            got32 = u32(rb.SortKeys.compute(to_cuda(d32)[off:end], bits, ctx))
+            np.testing.assert_array_equal(got32, ref32[off:end], err_msg=f"f32 {off} {cut}")
 
 
 def test_sort_large_random_32bit(ctx):
