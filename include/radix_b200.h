@@ -253,6 +253,28 @@ int rdx_ctx_set_sort_variant(rdx_ctx* ctx, int variant);
 /* Kernels this context has launched since it was created. */
 int rdx_ctx_launches(rdx_ctx* ctx, uint64_t* launches);
 
+/*
+ * How frame and projection calls read tables in host memory.
+ * RDX_HOST_IN_PLACE (the default): the colour rows of a raw SH-3 table (the
+ * largest column, which only drawn candidates read) are read by the
+ * projection kernel in place when they are pinned host memory mapped into the
+ * device's address space: a warp stages each batch of 32 candidates' rows in
+ * whole 16-byte pieces, so only the rows of splats that pass the centre culls
+ * cross the bus, in full requests. Every other host column (and pageable
+ * memory, and every column of a call with a sort guard) is copied in before
+ * the projection. RDX_HOST_COPY: every host column is copied in. In place
+ * moves fewer bytes when the view culls splats; with every splat in view the
+ * copy is a little faster. Either way the call returns once the device is
+ * done with the host columns.
+ */
+#define RDX_HOST_COPY 0
+#define RDX_HOST_IN_PLACE 1
+int rdx_ctx_set_host_reads(rdx_ctx* ctx, int mode);
+/* Bytes of table columns that frame and projection calls moved from host
+ * memory (copies, and rows read in place) since the last query; waits for the
+ * context's stream. */
+int rdx_ctx_host_bytes(rdx_ctx* ctx, uint64_t* bytes);
+
 /* Fill `p` with the reference's defaults (splatParams.ts:68-72). */
 void rdx_params_default(rdx_params* p);
 

@@ -142,6 +142,18 @@ class Context:
         _abi.check(_abi.lib().rdx_ctx_launches(self.handle, ctypes.byref(n)), self.handle)
         return n.value
 
+    def set_host_reads(self, in_place=True):
+        """Host tables: read the drawn candidates' rows of pinned columns in
+        place (True, the default), or copy every host column in (False)."""
+        _abi.check(_abi.lib().rdx_ctx_set_host_reads(self.handle, 1 if in_place else 0), self.handle)
+
+    def host_bytes(self):
+        """Bytes of table columns moved from host memory since the last query
+        (copies and rows read in place); waits for the context's stream."""
+        n = ctypes.c_uint64(0)
+        _abi.check(_abi.lib().rdx_ctx_host_bytes(self.handle, ctypes.byref(n)), self.handle)
+        return n.value
+
     def reserve(self, max_keys):
         _abi.check(_abi.lib().rdx_ctx_reserve(self.handle, int(max_keys)), self.handle)
 

@@ -206,6 +206,8 @@ SIGNATURES = {
                                      ctypes.c_void_p]),
     "rdx_ctx_phase_times": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_ctx_launches": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "rdx_ctx_set_host_reads": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "rdx_ctx_host_bytes": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_sort_keys_compute": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),
     "rdx_sort_keys_compute_f32": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p]),
     "rdx_sort": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_void_p,

@@ -64,6 +64,11 @@ struct rdx_ctx {
     int project_warps;
   };
   std::map<uint64_t, Tuned> tuned;
+  // Host tables (rdx_ctx_set_host_reads): read the drawn rows of pinned columns
+  // in place, or copy every host column in; bytes moved since the last query
+  int host_reads = RDX_HOST_IN_PLACE;
+  unsigned long long* host_bytes_dev = nullptr;  // rows read in place (the projection counts them)
+  uint64_t host_bytes = 0;                       // columns copied in
 };
 
 static const size_t kRingBytes = 4u << 20;
@@ -101,6 +106,18 @@ bool is_device_ptr(const void* p) {
 }
 
 bool aligned(const void* p, size_t a) { return ((uintptr_t)p % a) == 0; }
+
+// The device address of pinned host memory mapped into the device's address
+// space (null: not such memory)
+const void* mapped_host(const void* p) {
+  if (!p) return nullptr;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
 
 // Bump allocation over the context's arena: a dry run sizes it, the real run carves it
 struct Arena {
@@ -427,23 +444,41 @@ int check_table(rdx_ctx* ctx, const rdx_table* t, int index) {
   return RDX_OK;
 }
 
+// A column as the kernels read it: the caller's device pointer, pinned host
+// memory in place (`in_place`: a column that only drawn candidates read, whose
+// rows then cross the bus alone; *row_bytes grows by the bytes of its row), or
+// a staged copy of host memory
 template <class T>
-const T* stage_column(rdx_ctx* ctx, Arena& a, const T* src, size_t bytes, size_t align, int* status) {
+const T* stage_column(rdx_ctx* ctx, Arena& a, const T* src, size_t bytes, size_t align, int* status,
+                      bool in_place = false, uint64_t n = 0, uint32_t* row_bytes = nullptr) {
   if (is_device_ptr(src)) {
     if (!aligned(src, align)) *status = fail(ctx, RDX_ERR_ARG, "a device column is not %zu-byte aligned", align);
     a.take<char>(0);
     return src;
   }
+  if (in_place && ctx->host_reads == RDX_HOST_IN_PLACE && n > 0) {
+    const void* m = mapped_host(src);
+    if (m && aligned(m, align)) {
+      if (row_bytes) *row_bytes += (uint32_t)(bytes / n);
+      a.take<char>(0);
+      return reinterpret_cast<const T*>(m);
+    }
+  }
   char* dst = a.take<char>(bytes);
   if (dst && bytes) {
     cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
     if (e != cudaSuccess) *status = cuda_fail(ctx, e, "copy of a host column");
+    ctx->host_bytes += bytes;
   }
   return reinterpret_cast<const T*>(dst);
 }
 
-// A table whose columns are on the device: the caller's pointers, or staged copies of host columns
-rdx::DevTable stage_table(rdx_ctx* ctx, Arena& a, const rdx_table& t, int* status) {
+// A table whose columns the kernels can read: the caller's device pointers,
+// staged copies of host columns, and (pinned host memory, `in_place`) a raw
+// SH-3 table's colour rows, which only drawn candidates read, in place;
+// *row_bytes: the bytes of a candidate's row read in place
+rdx::DevTable stage_table(rdx_ctx* ctx, Arena& a, const rdx_table& t, int* status, uint32_t* row_bytes,
+                          bool in_place) {
   rdx::DevTable d{};
   d.layout = t.layout;
   d.sh_degree = t.sh_degree;
@@ -451,12 +486,15 @@ rdx::DevTable stage_table(rdx_ctx* ctx, Arena& a, const rdx_table& t, int* statu
   d.sh_codec = t.sh_codec;
   const uint64_t n = t.count;
   const TableBytes b = table_bytes(t, n);
+  *row_bytes = 0;
   if (t.layout == RDX_LAYOUT_RAW) {
     d.centers = stage_column(ctx, a, t.centers, b.centers, 4, status);
     d.log_scales = stage_column(ctx, a, t.log_scales, b.scales, 4, status);
     d.quats = stage_column(ctx, a, t.quats, b.quats, 16, status);
     d.opacities = stage_column(ctx, a, t.opacities, b.opacities, 4, status);
-    d.colors = stage_column(ctx, a, reinterpret_cast<const char*>(t.colors), b.colors, color_vec_bytes(t), status);
+    // colour rows in place where a kernel flavour stages them in whole 16-byte pieces
+    d.colors = stage_column(ctx, a, reinterpret_cast<const char*>(t.colors), b.colors, color_vec_bytes(t), status,
+                            in_place && rdx::project_host_rows_supported(d), n, row_bytes);
     return d;
   }
   if (t.layout == RDX_LAYOUT_PACKED) {
@@ -662,6 +700,12 @@ int plan_views(rdx_ctx* ctx, Arena& a, const ViewRef* views, int n_views, const 
                int cull_keys, ProjectCall& call) {
   int status = RDX_OK;
   std::map<const rdx_table*, rdx::DevTable> staged;
+  std::map<const rdx_table*, uint32_t> row_bytes;  // of each table's columns read in place
+  // rows are read in place only in launches without the sort guard (its kernels stage no rows)
+  bool guarded = params->sort_guard > 0.0f;
+  for (int v = 0; v < n_views; v++)
+    for (int i = 0; i < views[v].n_objects; i++)
+      guarded = guarded || (views[v].objects[i].params && views[v].objects[i].params->sort_guard > 0.0f);
   uint64_t n = 0;
   for (int v = 0; v < n_views; v++)
     for (int i = 0; i < views[v].n_objects; i++) n += views[v].objects[i].count;
@@ -675,10 +719,11 @@ int plan_views(rdx_ctx* ctx, Arena& a, const ViewRef* views, int n_views, const 
     for (int i = 0; i < vw.n_objects; i++) {
       const rdx_object& o = vw.objects[i];
       const rdx_table& t = *o.table;
-      if (!staged.count(o.table)) staged[o.table] = stage_table(ctx, a, t, &status);
+      if (!staged.count(o.table)) staged[o.table] = stage_table(ctx, a, t, &status, &row_bytes[o.table], !guarded);
       const int kind = table_kind_of(t);
       if (o.count > 0) {
         rdx::ProjDesc d = make_desc(*vw.camera, c, o, staged[o.table], *params, offset, n, bits, pass, cull_keys);
+        d.host_row_bytes = row_bytes[o.table];
         d.segment = v;
         d.object = i;
         by_kind[kind].push_back(d);
@@ -853,7 +898,8 @@ int rdx_ctx_create(int device, rdx_ctx** out) {
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&ctx->error_flag, 8) != cudaSuccess || cudaMallocHost(&ctx->error_host, 4) != cudaSuccess ||
-      cudaMemset(ctx->error_flag, 0, 8) != cudaSuccess || cudaMallocHost(&ctx->ring, kRingBytes) != cudaSuccess ||
+      cudaMemset(ctx->error_flag, 0, 8) != cudaSuccess || cudaMalloc(&ctx->host_bytes_dev, 8) != cudaSuccess ||
+      cudaMemset(ctx->host_bytes_dev, 0, 8) != cudaSuccess || cudaMallocHost(&ctx->ring, kRingBytes) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ring_event, cudaEventDisableTiming) != cudaSuccess) {
     cudaGetLastError();
     rdx_ctx_destroy(ctx);
@@ -872,6 +918,7 @@ int rdx_ctx_destroy(rdx_ctx* ctx) {
   if (ctx->arena) cudaFree(ctx->arena);
   if (ctx->lookback) cudaFree(ctx->lookback);
   if (ctx->error_flag) cudaFree(ctx->error_flag);
+  if (ctx->host_bytes_dev) cudaFree(ctx->host_bytes_dev);
   if (ctx->error_host) cudaFreeHost(ctx->error_host);
   for (auto& p : ctx->pending) {
     cudaEventDestroy(p.start);
@@ -882,6 +929,25 @@ int rdx_ctx_destroy(rdx_ctx* ctx) {
   if (ctx->ring) cudaFreeHost(ctx->ring);
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
+  return RDX_OK;
+}
+
+int rdx_ctx_set_host_reads(rdx_ctx* ctx, int mode) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (mode != RDX_HOST_COPY && mode != RDX_HOST_IN_PLACE) return fail(ctx, RDX_ERR_ARG, "host reads: mode %d", mode);
+  ctx->host_reads = mode;
+  return RDX_OK;
+}
+
+int rdx_ctx_host_bytes(rdx_ctx* ctx, uint64_t* bytes) {
+  if (!ctx || !bytes) return RDX_ERR_ARG;
+  cudaSetDevice(ctx->device);
+  unsigned long long rows = 0;
+  RDX_CUDA(cudaMemcpyAsync(&rows, ctx->host_bytes_dev, 8, cudaMemcpyDeviceToHost, ctx->stream), "host bytes");
+  RDX_CUDA(cudaMemsetAsync(ctx->host_bytes_dev, 0, 8, ctx->stream), "host bytes");
+  RDX_CUDA(cudaStreamSynchronize(ctx->stream), "cudaStreamSynchronize");
+  *bytes = ctx->host_bytes + (uint64_t)rows;
+  ctx->host_bytes = 0;
   return RDX_OK;
 }
 
@@ -1394,6 +1460,7 @@ int frame_common(rdx_ctx* ctx, const ViewRef* views, int n_views, const rdx_para
       d.words = stage_out(ctx, a, o->words, E * n * 16, 16, plan, &status);
     }
     d.keys = stage_out(ctx, a, o->keys, n * 4, 4, plan, &status);
+    d.host_bytes = ctx->host_bytes_dev;
     if (sort) {
       if (!d.keys) d.keys = a.take<uint32_t>(n);
       fd.ord = host_order ? a.take<uint32_t>(n) : ordering;

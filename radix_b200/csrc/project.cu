@@ -281,7 +281,7 @@ __device__ __forceinline__ void load_vec(const unsigned char* p, unsigned char* 
 // the table has SH (GpuShReader.apply); without SH no clamp
 template <int LAYOUT, int DEG, int VAR>
 __device__ __forceinline__ void colour(const DevTable& t, uint64_t i, double dx, double dy, double dz, int cap,
-                                       double rgb[3]) {
+                                       double rgb[3], const uint4* staged = nullptr) {
   constexpr int K = ShCount<DEG>::value;
   double acc[3] = {0.0, 0.0, 0.0};
   const double l2 = dx * dx + dy * dy + dz * dz;
@@ -290,9 +290,17 @@ __device__ __forceinline__ void colour(const DevTable& t, uint64_t i, double dx,
   if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
     using CR = ColorRow<DEG, VAR>;
     alignas(16) unsigned char buf[(CR::kBytes + 15) / 16 * 16];
-    const unsigned char* row = reinterpret_cast<const unsigned char*>(t.colors) + i * CR::kBytes;
+    if constexpr (CR::kBytes % 16 == 0) {
+      if (staged) {  // the row a warp staged in shared memory
 #pragma unroll
-    for (int b = 0; b < CR::kBytes; b += CR::kVec) load_vec<CR::kVec>(row + b, buf + b);
+        for (int b = 0; b < CR::kBytes / 16; b++) reinterpret_cast<uint4*>(buf)[b] = staged[b];
+      }
+    }
+    if (!staged) {
+      const unsigned char* row = reinterpret_cast<const unsigned char*>(t.colors) + i * CR::kBytes;
+#pragma unroll
+      for (int b = 0; b < CR::kBytes; b += CR::kVec) load_vec<CR::kVec>(row + b, buf + b);
+    }
     auto value = [&](int v) -> double {
       if constexpr (VAR == RDX_DTYPE_F16) {
         return (double)__half2float(*reinterpret_cast<const __half*>(buf + v * 2));
@@ -477,12 +485,33 @@ struct WarpSmem {
   double e[EYES][6][kQueue];  // per eye: centre ex, ey, ez and clip x, y, w (float64)
 };
 
-template <int LAYOUT, int DEG, int VAR, int EYES, int WPB, bool GUARD>
+// Kernel flavours: plain; with the sort guard's code (launches where an object
+// sets a guard); host rows (raw tables whose colour rows may be pinned host
+// memory read in place: a warp stages each batch's rows in shared memory with
+// whole 16-byte pieces in row order, so a row crosses the bus in full requests
+// instead of a lane's scattered ones)
+constexpr int kPlain = 0, kGuarded = 1, kHostRows = 2;
+
+// A warp's staged colour rows: 32 rows, each padded to an odd number of
+// 16-byte pieces (a lane's reads of its row then fall in distinct banks)
+template <int DEG, int VAR>
+struct RowStage {
+  static constexpr int kPieces = ColorRow<DEG, VAR>::kBytes / 16;
+  static constexpr int kStride = kPieces | 1;
+  static constexpr int kBytes = 32 * kStride * 16;
+};
+
+template <int LAYOUT, int DEG, int VAR, int EYES, int WPB, int FLAVOR>
 __global__ void __launch_bounds__(WPB * 32) k_project(const ProjDesc* __restrict__ descs, int n_desc, uint32_t total_chunks,
                                                       ProjOutputs out) {
+  constexpr bool GUARD = FLAVOR == kGuarded;
+  constexpr bool HOST_ROWS = FLAVOR == kHostRows;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   WarpSmem<EYES>& W = reinterpret_cast<WarpSmem<EYES>*>(smem_raw)[warp];
+  uint4* const rows = HOST_ROWS ? reinterpret_cast<uint4*>(smem_raw + WPB * sizeof(WarpSmem<EYES>) +
+                                                           (size_t)warp * RowStage<DEG, VAR>::kBytes)
+                                : nullptr;
   const ProjDesc& sd = W.desc;
   const uint32_t lt = (1u << lane) - 1u;
 
@@ -499,6 +528,24 @@ __global__ void __launch_bounds__(WPB * 32) k_project(const ProjDesc* __restrict
     const DevParams& p = sd.params;
     const bool busy = (uint32_t)lane < nb;
     const uint32_t q = (head + (uint32_t)lane) & (kQueue - 1);
+    if constexpr (HOST_ROWS) {
+      using RS = RowStage<DEG, VAR>;
+      const uint4* colors = reinterpret_cast<const uint4*>(sd.table.colors);
+      uint4 piece[RS::kPieces];
+#pragma unroll
+      for (int j = 0; j < RS::kPieces; j++) {
+        const uint32_t f = (uint32_t)j * 32 + (uint32_t)lane;  // piece f of the batch: row f / kPieces
+        const uint32_t r = f / RS::kPieces;
+        if (r < nb) piece[j] = __ldg(colors + (uint64_t)W.idx[(head + r) & (kQueue - 1)] * RS::kPieces + (f - r * RS::kPieces));
+      }
+#pragma unroll
+      for (int j = 0; j < RS::kPieces; j++) {
+        const uint32_t f = (uint32_t)j * 32 + (uint32_t)lane;
+        const uint32_t r = f / RS::kPieces;
+        if (r < nb) rows[r * RS::kStride + (f - r * RS::kPieces)] = piece[j];
+      }
+      __syncwarp();
+    }
     uint32_t key_out = invalid_key(sd.sort_bits);
     bool any_visible = false;
     if (busy) {
@@ -510,7 +557,8 @@ __global__ void __launch_bounds__(WPB * 32) k_project(const ProjDesc* __restrict
       load_head<LAYOUT>(sd.table, i, cf, opac, ls, zero_cov);
       double rgb[3];
       colour<LAYOUT, DEG, VAR>(sd.table, i, (double)W.c[0][q] - sd.origin[0], (double)W.c[1][q] - sd.origin[1],
-                               (double)W.c[2][q] - sd.origin[2], min(p.max_sh_degree, DEG), rgb);
+                               (double)W.c[2][q] - sd.origin[2], min(p.max_sh_degree, DEG), rgb,
+                               HOST_ROWS ? rows + lane * RowStage<DEG, VAR>::kStride : nullptr);
       // prepareSplat (projection.tsl.ts:42-64), float64
       double op = opac, inflate2 = 1.0;
       if (op > 1.0) {
@@ -837,7 +885,11 @@ __global__ void __launch_bounds__(WPB * 32) k_project(const ProjDesc* __restrict
       }
       candidate = eye_ok != 0;
       if (candidate) {
-        prefetch_rows<LAYOUT, DEG, VAR>(sd.table, i);
+        if constexpr (HOST_ROWS) {
+          prefetch_l2(sd.table.quats + i * 4);
+        } else {
+          prefetch_rows<LAYOUT, DEG, VAR>(sd.table, i);
+        }
       } else if (!sd.keys_only) {
         // culled in every eye: zeros, as a zero opacity byte marks a culled eye
 #pragma unroll
@@ -858,6 +910,9 @@ __global__ void __launch_bounds__(WPB * 32) k_project(const ProjDesc* __restrict
     if (key_final && out.keys) out.keys[gi] = key;
     // enqueue the candidates, in row order
     const uint32_t ballot = __ballot_sync(0xffffffffu, candidate);
+    // their rows of host columns read in place cross the bus: counted once a chunk
+    if (sd.host_row_bytes && lane == 0 && ballot && out.host_bytes)
+      atomicAdd(out.host_bytes, (unsigned long long)__popc(ballot) * sd.host_row_bytes);
     if (candidate) {
       const uint32_t q = (head + queued + (uint32_t)__popc(ballot & lt)) & (kQueue - 1);
       W.idx[q] = (uint32_t)i;
@@ -889,49 +944,61 @@ struct Picked {
 
 // Raw tables (the benchmark's) may launch with 2, 4 or 8 warps per block; the
 // other layouts, and every launch with a sort guard, with 4
+// Raw SH-3 tables (the benchmark's) also have the host-rows flavour (4-warp
+// blocks): their rows are whole 16-byte pieces
+template <int LAYOUT, int DEG, int VAR>
+constexpr bool kHasHostRows = LAYOUT == RDX_LAYOUT_RAW && DEG == 3 && ColorRow<DEG, VAR>::kBytes % 16 == 0;
+
 template <int LAYOUT, int DEG, int VAR, int EYES>
-Picked picked(int warps, bool guard) {
+Picked picked(int warps, bool guard, bool host_rows) {
   constexpr int kSmem = (int)sizeof(WarpSmem<EYES>);
-  if (guard) return {k_project<LAYOUT, DEG, VAR, EYES, kWarps, true>, kWarps * kSmem, kWarps};
-  if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
-    if (warps == 2) return {k_project<LAYOUT, DEG, VAR, EYES, 2, false>, 2 * kSmem, 2};
-    if (warps == 8) return {k_project<LAYOUT, DEG, VAR, EYES, 8, false>, 8 * kSmem, 8};
+  if (guard) return {k_project<LAYOUT, DEG, VAR, EYES, kWarps, kGuarded>, kWarps * kSmem, kWarps};
+  if constexpr (kHasHostRows<LAYOUT, DEG, VAR>) {
+    if (host_rows) {
+      constexpr int kStage = RowStage<DEG, VAR>::kBytes;
+      return {k_project<LAYOUT, DEG, VAR, EYES, kWarps, kHostRows>, kWarps * (kSmem + kStage), kWarps};
+    }
   }
-  return {k_project<LAYOUT, DEG, VAR, EYES, kWarps, false>, kWarps * kSmem, kWarps};
+  if constexpr (LAYOUT == RDX_LAYOUT_RAW) {
+    if (warps == 2) return {k_project<LAYOUT, DEG, VAR, EYES, 2, kPlain>, 2 * kSmem, 2};
+    if (warps == 8) return {k_project<LAYOUT, DEG, VAR, EYES, 8, kPlain>, 8 * kSmem, 8};
+  }
+  return {k_project<LAYOUT, DEG, VAR, EYES, kWarps, kPlain>, kWarps * kSmem, kWarps};
 }
 
 template <int LAYOUT, int DEG, int VAR>
-Picked pick_eyes(int eyes, int warps, bool guard) {
-  return eyes == 2 ? picked<LAYOUT, DEG, VAR, 2>(warps, guard) : picked<LAYOUT, DEG, VAR, 1>(warps, guard);
+Picked pick_eyes(int eyes, int warps, bool guard, bool host_rows) {
+  return eyes == 2 ? picked<LAYOUT, DEG, VAR, 2>(warps, guard, host_rows)
+                   : picked<LAYOUT, DEG, VAR, 1>(warps, guard, host_rows);
 }
 
 template <int LAYOUT, int VAR>
-Picked pick_degree(int degree, int eyes, int warps, bool guard) {
+Picked pick_degree(int degree, int eyes, int warps, bool guard, bool host_rows) {
   switch (degree) {
-    case 0: return pick_eyes<LAYOUT, 0, VAR>(eyes, warps, guard);
-    case 1: return pick_eyes<LAYOUT, 1, VAR>(eyes, warps, guard);
-    case 2: return pick_eyes<LAYOUT, 2, VAR>(eyes, warps, guard);
-    case 3: return pick_eyes<LAYOUT, 3, VAR>(eyes, warps, guard);
-    default: return pick_eyes<LAYOUT, 4, VAR>(eyes, warps, guard);
+    case 0: return pick_eyes<LAYOUT, 0, VAR>(eyes, warps, guard, host_rows);
+    case 1: return pick_eyes<LAYOUT, 1, VAR>(eyes, warps, guard, host_rows);
+    case 2: return pick_eyes<LAYOUT, 2, VAR>(eyes, warps, guard, host_rows);
+    case 3: return pick_eyes<LAYOUT, 3, VAR>(eyes, warps, guard, host_rows);
+    default: return pick_eyes<LAYOUT, 4, VAR>(eyes, warps, guard, host_rows);
   }
 }
 
 template <int LAYOUT>
 Picked pick_codec(int degree, int codec, int eyes, int warps, bool guard) {
   // without SH the codec is immaterial: one kernel
-  if (codec == RDX_SH_PACKED && degree > 0) return pick_degree<LAYOUT, RDX_SH_PACKED>(degree, eyes, warps, guard);
-  return pick_degree<LAYOUT, RDX_SH_EXT>(degree, eyes, warps, guard);
+  if (codec == RDX_SH_PACKED && degree > 0) return pick_degree<LAYOUT, RDX_SH_PACKED>(degree, eyes, warps, guard, false);
+  return pick_degree<LAYOUT, RDX_SH_EXT>(degree, eyes, warps, guard, false);
 }
 
-Picked pick_kernel(const DevTable& t, int eyes, int warps, bool guard) {
+Picked pick_kernel(const DevTable& t, int eyes, int warps, bool guard, bool host_rows) {
   switch (t.layout) {
     case RDX_LAYOUT_EXT: return pick_codec<RDX_LAYOUT_EXT>(t.sh_degree, t.sh_codec, eyes, warps, guard);
     case RDX_LAYOUT_PACKED: return pick_codec<RDX_LAYOUT_PACKED>(t.sh_degree, t.sh_codec, eyes, warps, guard);
     case RDX_LAYOUT_COV: return pick_codec<RDX_LAYOUT_COV>(t.sh_degree, t.sh_codec, eyes, warps, guard);
     default:
       if (t.color_dtype == RDX_DTYPE_F16)
-        return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F16>(t.sh_degree, eyes, warps, guard);
-      return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F32>(t.sh_degree, eyes, warps, guard);
+        return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F16>(t.sh_degree, eyes, warps, guard, host_rows);
+      return pick_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F32>(t.sh_degree, eyes, warps, guard, host_rows);
   }
 }
 
@@ -966,6 +1033,12 @@ int resident_blocks(const Picked& k, cudaError_t* err) {
 
 int project_warps_supported(int warps) { return warps == 2 || warps == 4 || warps == 8; }
 
+bool project_host_rows_supported(const DevTable& t) {
+  if (t.layout != RDX_LAYOUT_RAW || t.sh_degree != 3) return false;
+  return t.color_dtype == RDX_DTYPE_F16 ? kHasHostRows<RDX_LAYOUT_RAW, 3, RDX_DTYPE_F16>
+                                        : kHasHostRows<RDX_LAYOUT_RAW, 3, RDX_DTYPE_F32>;
+}
+
 cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host, int n_desc, uint32_t total_chunks,
                            const ProjOutputs& out, uint32_t* error_flag, cudaStream_t stream, int warps) {
   if (total_chunks == 0 || n_desc == 0) return cudaSuccess;
@@ -976,8 +1049,13 @@ cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host
   // One kernel per launch: the caller groups objects by table kind
   const ProjDesc& d0 = descs_host[0];
   bool guard = false;  // an object of the launch keys its splats through the sort guard
-  for (int j = 0; j < n_desc; j++) guard = guard || descs_host[j].params.sort_guard > 0.0f;
-  const Picked k = pick_kernel(d0.table, d0.eyes, warps, guard);
+  bool host_rows = false;  // an object's colour rows are read from host memory in place
+  for (int j = 0; j < n_desc; j++) {
+    guard = guard || descs_host[j].params.sort_guard > 0.0f;
+    host_rows = host_rows || descs_host[j].host_row_bytes > 0;
+  }
+  if (host_rows && guard) return cudaErrorInvalidValue;  // the caller copies the rows of guarded launches
+  const Picked k = pick_kernel(d0.table, d0.eyes, warps, guard, host_rows);
   cudaError_t err = cudaSuccess;
   const int blocks = resident_blocks(k, &err);
   if (err != cudaSuccess) return err;

@@ -229,7 +229,7 @@ struct ProjDesc {
   uint32_t first_tile;   // running count of projection tiles before this object
   int object;            // index of the object in its view's collection
   int segment;           // the sort segment the keys belong to (a view of a batch)
-  int reserved3;
+  uint32_t host_row_bytes;  // bytes a drawn candidate reads from host memory in place (0: none)
 };
 
 struct ProjOutputs {
@@ -246,6 +246,7 @@ struct ProjOutputs {
   uint32_t* zero;
   uint64_t zero_words;
   uint32_t* check_flag;  // the device error word (bounds-checked builds record clamped rows there)
+  unsigned long long* host_bytes;  // adds host_row_bytes for each candidate of an object read in place (may be null)
 };
 
 // Splats per projection chunk (one warp)
@@ -397,5 +398,8 @@ cudaError_t launch_project(const ProjDesc* descs_dev, const ProjDesc* descs_host
                            uint32_t total_tiles, const ProjOutputs& out,
                            uint32_t* error_flag, cudaStream_t stream, int warps = 0);
 int project_warps_supported(int warps);
+// Raw tables whose colour rows the projection may read from pinned host memory
+// in place (a kernel flavour stages them a warp at a time)
+bool project_host_rows_supported(const DevTable& t);
 
 }  // namespace rdx

@@ -45,6 +45,84 @@ def test_frame_from_host_buffers(ctx):
     _frame_check(syn.plain_table(30_000, seed=5), syn.plain_camera(), 24, device=None)
 
 
+NAMES = ("mean2d", "conic", "depth", "opacity", "rgb", "keys")
+
+
+def _same_frame(got, ref):
+    for k in NAMES:
+        np.testing.assert_array_equal(host(got[k]), host(ref[k]), err_msg=k)
+    np.testing.assert_array_equal(u32(got["ordering"]), u32(ref["ordering"]))
+    assert got["visible"] == ref["visible"]
+
+
+@pytest.mark.parametrize("eyes", [1, 2])
+def test_frame_reads_pinned_host_columns_in_place(ctx, eyes):
+    """A raw SH-3 table in pinned host memory. Read in place (the default), the
+    kernel stages the colour rows of the splats that pass the centre culls from
+    host memory and the other columns are copied in; with copies, every column
+    is. Both give the device table's bits; the bytes moved are the copied
+    columns plus a 192-byte row per candidate, or the whole table."""
+    n = 200_000
+    d = syn.mixture_table(n, seed=7, sh_degree=3)
+    cam = syn.scale_camera() if eyes == 1 else syn.stereo_camera()
+    cols = ("centers", "log_scales", "quats", "opacities", "colors")
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(d[k])).pin_memory() for k in cols}
+    dev = {k: v.cuda() for k, v in pinned.items()}
+
+    def table(c):
+        return rb.Table.raw(c["centers"], c["log_scales"], c["quats"], c["opacities"], c["colors"], 3)
+
+    ref = rb.frame([rb.SplatObject(table(dev))], cam, None, 32, NAMES, ctx=ctx)
+    size = {k: v.numel() * v.element_size() for k, v in pinned.items()}
+    copied = size["centers"] + size["log_scales"] + size["opacities"] + size["quats"]
+    row = 16 * 3 * 4
+    try:
+        for in_place in (True, False):
+            ctx.set_host_reads(in_place)
+            ctx.host_bytes()
+            got = rb.frame([rb.SplatObject(table(pinned))], cam, None, 32, NAMES, ctx=ctx)
+            moved = ctx.host_bytes()
+            _same_frame(got, ref)
+            if in_place:
+                assert (moved - copied) % row == 0, moved
+                candidates = (moved - copied) // row
+                assert ref["visible"] <= candidates < n, (candidates, ref["visible"])
+            else:
+                assert moved == sum(size.values())
+    finally:
+        ctx.set_host_reads(True)
+
+
+def test_pinned_ext_table_and_guarded_raw_table_are_copied(ctx):
+    """Tables whose rows no kernel flavour stages are copied in whole: an ext
+    table whose SH texel channels are pinned and whose extA/extB words are
+    pageable, and a pinned raw SH-3 table under a sort guard. The device
+    tables' bits either way."""
+    d = syn.mixture_table(60_000, seed=9, sh_degree=3)
+    a, b, sh = orc.encode_ext(d)
+    dev = rb.Table.ext(torch.from_numpy(a.view(np.int32)).cuda(), torch.from_numpy(b.view(np.int32)).cuda(),
+                       [torch.from_numpy(c.view(np.int32)).cuda() for c in sh], 3)
+    pinned_sh = [torch.from_numpy(np.ascontiguousarray(c.view(np.int32))).pin_memory() for c in sh]
+    mixed = rb.Table.ext(a, b, pinned_sh, 3)
+    cam = syn.scale_camera()
+    ref = rb.frame([rb.SplatObject(dev)], cam, None, 32, NAMES, ctx=ctx)
+    ctx.host_bytes()
+    got = rb.frame([rb.SplatObject(mixed)], cam, None, 32, NAMES, ctx=ctx)
+    moved = ctx.host_bytes()
+    _same_frame(got, ref)
+    assert moved == a.nbytes + b.nbytes + sum(c.nbytes for c in sh)
+    cols = ("centers", "log_scales", "quats", "opacities", "colors")
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(d[k])).pin_memory() for k in cols}
+    raw = rb.Table.raw(*(pinned[k] for k in cols), 3)
+    raw_dev = rb.Table.raw(*(pinned[k].cuda() for k in cols), 3)
+    params = rb.SplatParams(sort_guard=1.5)
+    ref = rb.frame([rb.SplatObject(raw_dev)], cam, params, 32, NAMES, ctx=ctx)
+    ctx.host_bytes()
+    got = rb.frame([rb.SplatObject(raw)], cam, params, 32, NAMES, ctx=ctx)
+    assert ctx.host_bytes() == sum(v.numel() * v.element_size() for v in pinned.values())
+    _same_frame(got, ref)
+
+
 def test_frame_empty_collection(ctx):
     d = syn.plain_table(10, seed=1)
     res = rb.frame([rb.SplatObject(cuda_table(d), count=0)], syn.plain_camera(), None, 32)
