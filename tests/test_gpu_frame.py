@@ -93,6 +93,30 @@ def test_frame_reads_pinned_host_columns_in_place(ctx, eyes):
         ctx.set_host_reads(True)
 
 
+def test_in_place_rows_float16_and_a_mixed_collection(ctx):
+    """Float16 SH-3 rows (96 bytes: six 16-byte pieces) read in place, and a
+    collection of a pinned table and a device table of the same kind in one
+    launch (the staging flavour reads both): the device tables' bits."""
+    cols = ("centers", "log_scales", "quats", "opacities", "colors")
+    d0 = syn.mixture_table(90_000, seed=11, sh_degree=3, color_dtype=np.float16)
+    d1 = syn.mixture_table(70_000, seed=12, sh_degree=3, color_dtype=np.float16)
+    pin0 = {k: torch.from_numpy(np.ascontiguousarray(d0[k])).pin_memory() for k in cols}
+    dev0 = {k: v.cuda() for k, v in pin0.items()}
+    dev1 = {k: torch.from_numpy(np.ascontiguousarray(d1[k])).cuda() for k in cols}
+
+    def table(c):
+        return rb.Table.raw(*(c[k] for k in cols), 3)
+
+    cam = syn.scale_camera()
+    ref = rb.frame([rb.SplatObject(table(dev0)), rb.SplatObject(table(dev1))], cam, None, 32, NAMES, ctx=ctx)
+    ctx.host_bytes()
+    got = rb.frame([rb.SplatObject(table(pin0)), rb.SplatObject(table(dev1))], cam, None, 32, NAMES, ctx=ctx)
+    moved = ctx.host_bytes()
+    _same_frame(got, ref)
+    copied = sum(pin0[k].numel() * pin0[k].element_size() for k in ("centers", "log_scales", "quats", "opacities"))
+    assert moved > copied and (moved - copied) % 96 == 0 and (moved - copied) // 96 < 90_000
+
+
 def test_pinned_ext_table_and_guarded_raw_table_are_copied(ctx):
     """Tables whose rows no kernel flavour stages are copied in whole: an ext
     table whose SH texel channels are pinned and whose extA/extB words are
