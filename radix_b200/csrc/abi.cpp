@@ -826,7 +826,7 @@ int project_warps(const rdx_ctx* ctx, int segments, uint64_t n, int bits, int ta
 // Enqueue one sort (every pass); it takes a fresh lookback epoch on the device
 int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out, uint32_t* vals_out,
              const SegBufs& sb, int segments, uint32_t max_tiles, int bits, const rdx::SortScratch& sc,
-             bool zeroed) {
+             bool zeroed, uint32_t* visible = nullptr, bool visible_ref = false) {
   const int passes = bits / 8;
   int st = ensure_lookback(ctx, (size_t)passes * lookback_tiles(max_tiles) * rdx::kRadix);
   if (st != RDX_OK) return st;
@@ -850,6 +850,8 @@ int run_sort(rdx_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in, uin
   const SortPlan plan = plan_of(variant);
   c.coop = plan.coop;
   c.pass_items = plan.pass_items;
+  c.visible = visible;
+  c.visible_ref = visible_ref;
   int launches = 0;
   RDX_CUDA(rdx::sort_segments(c, ctx->stream, &launches), "sort launch");
   ctx->launches += (uint64_t)launches;
@@ -1136,12 +1138,10 @@ int rdx_sort(rdx_ctx* ctx, const uint32_t* keys, uint64_t count, int bits, uint3
   if (s != RDX_OK) return s;
   {
     Phase sorting(ctx, RDX_PHASE_SORT);
-    s = run_sort(ctx, k, nullptr, nullptr, o, sb, 1, tiles, bits, sc, false);
+    s = run_sort(ctx, k, nullptr, nullptr, o, sb, 1, tiles, bits, sc, false, visible ? vis : nullptr, true);
     if (s != RDX_OK) return s;
   }
   if (visible) {
-    RDX_CUDA(rdx::launch_visible(sb.begin, sb.end, sc.ref_hidden, sc.valid, 1, vis, ctx->stream), "visible");
-    ctx->launches += 1;
     RDX_CUDA(cudaMemcpyAsync(visible, vis, 4, host_visible ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, ctx->stream),
              "visible copy");
   }
@@ -1288,10 +1288,8 @@ int rdx_splat_sort(rdx_ctx* ctx, const uint32_t* keys, uint64_t count, int bits,
   if (count > 0) {
     s = single_segment(ctx, sb, count);
     if (s != RDX_OK) return s;
-    s = run_sort(ctx, k, nullptr, nullptr, v, sb, 1, tiles, bits, sc, false);
+    s = run_sort(ctx, k, nullptr, nullptr, v, sb, 1, tiles, bits, sc, false, c, false);
     if (s != RDX_OK) return s;
-    RDX_CUDA(rdx::launch_visible(sb.begin, sb.end, nullptr, sc.valid, 1, c, ctx->stream), "count");
-    ctx->launches += 1;
   } else {
     RDX_CUDA(cudaMemsetAsync(c, 0, 4, ctx->stream), "count");
   }
@@ -1370,12 +1368,10 @@ cudaError_t enqueue_frame(rdx_ctx* timing, const ProjectCall& call, const FrameD
     c.silent_pass = fd.silent_pass;
     c.coop = fd.coop;
     c.pass_items = fd.pass_items;
+    c.visible = fd.vis;
     int n_launch = 0;
     e = rdx::sort_segments(c, stream, &n_launch);
     *launches += (uint64_t)n_launch;
-    if (e != cudaSuccess) return e;
-    e = rdx::launch_visible(fd.sb.begin, fd.sb.end, nullptr, fd.sc.valid, views, fd.vis, stream);
-    *launches += 1;
     if (e != cudaSuccess) return e;
   } else if (sort && fd.vis) {
     e = cudaMemsetAsync(fd.vis, 0, (size_t)views * 4, stream);

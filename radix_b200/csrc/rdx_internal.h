@@ -146,6 +146,10 @@ struct SortCall {
   int silent_pass = -1;     // a digit pass whose first tile publishes no lookback word (a test hook; -1: none)
   int coop = kCoopNone;     // one segment: the digit passes in this cooperative variant (needs block_counts)
   int pass_items = 0;       // onesweep digit passes after a partition: keys a thread (4, 8, 16; 0: by size)
+  // Per segment (may be null): the reference's visible count, (end - begin) - ref_hidden
+  // (visible_ref), or the valid keys; the partition writes it, else a kernel after the passes
+  uint32_t* visible = nullptr;
+  bool visible_ref = false;
 };
 cudaError_t sort_segments(const SortCall& call, cudaStream_t stream, int* launches);
 // Blocks of a cooperative variant resident on the current device (0: it cannot launch)

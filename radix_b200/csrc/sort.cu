@@ -237,6 +237,8 @@ struct PartArgs {
   uint32_t* vtiles;            // in tiles of pass_tile keys
   uint32_t pass_tile;
   uint32_t* error_flag;
+  uint32_t* visible;           // out (block 0, may be null): each segment's visible count
+  const uint32_t* ref_hidden;  // the reference's count of it (null: the valid keys)
 };
 
 constexpr int kPartBlocksPerSm = 8;
@@ -253,7 +255,7 @@ __global__ void __launch_bounds__(kSortThreads, kPartBlocksPerSm) k_partition(Pa
   pdl_wait();
   pdl_trigger();
   if (tid == 0 && blockIdx.x == 0) {
-    // The valid keys' segments [begin, begin + valid) and their tiles
+    // The valid keys' segments [begin, begin + valid) and their tiles; the visible counts
     uint32_t t = 0;
     for (int s = 0; s < a.segs.count; s++) {
       const uint64_t b = a.segs.begin[s];
@@ -262,6 +264,7 @@ __global__ void __launch_bounds__(kSortThreads, kPartBlocksPerSm) k_partition(Pa
       a.vend[s] = b + v;
       a.vtiles[s] = t;
       t += (uint32_t)((v + a.pass_tile - 1) / a.pass_tile);
+      if (a.visible) a.visible[s] = a.ref_hidden ? (uint32_t)(a.segs.end[s] - b) - a.ref_hidden[s] : a.valid_count[s];
     }
     a.vtiles[a.segs.count] = t;
   }
@@ -932,7 +935,9 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
   const int ref_shift = c.bits == 16 ? 0 : (c.bits == 24 ? 11 : 16);
   const uint32_t ref_top = c.bits == 24 ? 0x1fffu : 0xffffu;
   const SortScratch& sc = c.scratch;
-  if (c.segs.max_tiles == 0) return cudaSuccess;
+  if (c.segs.max_tiles == 0) {
+    return c.visible ? cudaMemsetAsync(c.visible, 0, (size_t)c.segs.count * 4, stream) : cudaSuccess;
+  }
   // In place (a WgpuRadixSort): the partition may not write the tail while
   // other tiles still read there, so the largest key is ranked like any other
   const int drop = c.keys_out != c.keys_in && c.vals_out != c.vals_in && !c.no_drop ? 1 : 0;
@@ -997,6 +1002,8 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     p.vtiles = sc.vtiles;
     p.pass_tile = (uint32_t)(kSortThreads * items);
     p.error_flag = c.error_flag;
+    p.visible = c.visible;
+    p.ref_hidden = c.visible_ref ? sc.ref_hidden : nullptr;
     err = launch_after(k_partition, c.segs.max_tiles, kSortThreads, 0, stream, p);
     if (err != cudaSuccess) return err;
     n_launch++;
@@ -1040,6 +1047,12 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
       err = cudaLaunchKernelEx(&cfg, v.fn, ca);
       if (err != cudaSuccess) return err;
       n_launch++;
+      if (!drop && c.visible) {
+        err = launch_visible(c.segs.begin, c.segs.end, c.visible_ref ? sc.ref_hidden : nullptr, sc.valid, c.segs.count,
+                             c.visible, stream);
+        if (err != cudaSuccess) return err;
+        n_launch++;
+      }
       if (launches) *launches += n_launch;
       return cudaGetLastError();
     }
@@ -1070,6 +1083,12 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     n_launch++;
     ki = a.keys_out;
     vi = a.vals_out;
+  }
+  if (!drop && c.visible) {
+    err = launch_visible(c.segs.begin, c.segs.end, c.visible_ref ? sc.ref_hidden : nullptr, sc.valid, c.segs.count,
+                         c.visible, stream);
+    if (err != cudaSuccess) return err;
+    n_launch++;
   }
   if (launches) *launches += n_launch;
   return cudaGetLastError();

@@ -105,7 +105,7 @@ def test_graph_batch_replays_and_updates(ctx):
     assign = [0, 1, 2, 2, 1, 0]
     views = _views(tables, cams, assign)
     batch = rb.Batch(views, None, 32, NAMES)
-    assert batch.launches() >= 7  # projection, sort passes, visible: one graph
+    assert batch.launches() >= 7  # projection, counting, partition (and visible counts), 4 digit passes: one graph
     direct = rb.frame_batched(views, None, 32, NAMES)
     for _ in range(3):  # replays: fresh lookback epochs, cleared histograms
         batch.launch()
