@@ -117,6 +117,35 @@ def test_in_place_rows_float16_and_a_mixed_collection(ctx):
     assert moved > copied and (moved - copied) % 96 == 0 and (moved - copied) // 96 < 90_000
 
 
+def test_in_place_rows_in_batched_frames_and_projections(ctx):
+    """The other calls that stage tables: a batched frame of three views of one
+    pinned table (the rows are read once per view) and projections with keys
+    only (no candidate reads a row) or with every output: the device table's bits."""
+    cols = ("centers", "log_scales", "quats", "opacities", "colors")
+    d = syn.mixture_table(80_000, seed=13, sh_degree=3)
+    pinned = {k: torch.from_numpy(np.ascontiguousarray(d[k])).pin_memory() for k in cols}
+    dev = {k: v.cuda() for k, v in pinned.items()}
+    host_t = rb.Table.raw(*(pinned[k] for k in cols), 3)
+    dev_t = rb.Table.raw(*(dev[k] for k in cols), 3)
+    cams = syn.sphere_cameras(3, seed=14)
+    ref = rb.frame_batched([([rb.SplatObject(dev_t)], c) for c in cams], None, 32, NAMES, ctx=ctx)
+    got = rb.frame_batched([([rb.SplatObject(host_t)], c) for c in cams], None, 32, NAMES, ctx=ctx)
+    for k in NAMES:
+        np.testing.assert_array_equal(host(got[k]), host(ref[k]), err_msg=k)
+    np.testing.assert_array_equal(u32(got["ordering"]), u32(ref["ordering"]))
+    np.testing.assert_array_equal(host(got["visible"]), host(ref["visible"]))
+    cam = syn.scale_camera()
+    for pass_ in ("keys", "full"):
+        a = rb.project_collection([rb.SplatObject(dev_t)], cam, None, 32, pass_, True, NAMES, ctx=ctx)
+        ctx.host_bytes()
+        b = rb.project_collection([rb.SplatObject(host_t)], cam, None, 32, pass_, True, NAMES, ctx=ctx)
+        moved = ctx.host_bytes()
+        for k in a:
+            np.testing.assert_array_equal(host(b[k]), host(a[k]), err_msg=f"{pass_} {k}")
+        copied = sum(pinned[k].numel() * pinned[k].element_size() for k in ("centers", "log_scales", "quats", "opacities"))
+        assert moved == copied if pass_ == "keys" else moved > copied
+
+
 def test_pinned_ext_table_and_guarded_raw_table_are_copied(ctx):
     """Tables whose rows no kernel flavour stages are copied in whole: an ext
     table whose SH texel channels are pinned and whose extA/extB words are
