@@ -2,8 +2,8 @@
 kernel clamps also recorded in the device error word, which the calls report
 as an error. compute-sanitizer is closed on the GPUs these tests run on; this
 build checks, without faulting anything, that no launch of the sort, frame,
-batch, splat-sort and gradient paths ever computes an index outside its
-buffer. The paths run in a child process that loads
+batch, splat-sort, pinned-table and gradient paths ever computes an index
+outside its buffer. The paths run in a child process that loads
 radix_b200/lib/libradix_b200_check.so (RADIX_B200_CHECK=1), and their results
 are compared with the float64 oracle there."""
 import os
@@ -62,6 +62,14 @@ values, count, args = sorter.sort(res["keys"][:n0], n0, 24)
 ctx.synchronize()
 valid = int((keys[:n0] != rb.SortKeys.invalid(24)).sum())
 assert sorter.read_count() == valid and np.array_equal(u32(values)[:valid], o0[:valid])
+# a pinned host table: colour rows read in place by the staging flavour
+cols = ("centers", "log_scales", "quats", "opacities", "colors")
+pinned = rb.Table.raw(*(torch.from_numpy(np.ascontiguousarray(d[k])).pin_memory() for k in cols), 3)
+ref_frame = rb.frame([rb.SplatObject(t)], syn.stereo_camera(), None, 32, names, ctx=ctx)
+got_frame = rb.frame([rb.SplatObject(pinned)], syn.stereo_camera(), None, 32, names, ctx=ctx)
+for k in names:
+    assert np.array_equal(u32(got_frame[k]), u32(ref_frame[k])), ("pinned", k)
+assert np.array_equal(u32(got_frame["ordering"]), u32(ref_frame["ordering"]))
 fwd = rb.project_collection([rb.SplatObject(t)], cam, None, 32, "full", True, outputs=("opacity",), ctx=ctx)
 up = {k: torch.randn(fwd["opacity"].shape + ((2,) if k == "mean2d" else (3,) if k in ("conic", "rgb") else ()),
                      device="cuda") for k in ("mean2d", "conic", "opacity", "rgb")}
