@@ -1011,7 +1011,10 @@ cudaError_t sort_segments(const SortCall& c, cudaStream_t stream, int* launches)
     vi = sc.vals_a;
   }
   if (coop) {
-    const int blocks = n_coop;
+    // A block a 4096-key tile of the sort's capacity, up to every SM slot: a
+    // small sort's passes then wait on fewer blocks at their grid barriers and
+    // sum fewer blocks' counts
+    const int blocks = (int)std::min<uint32_t>((uint32_t)n_coop, std::max<uint32_t>(1u, c.segs.max_tiles));
     {
       const CoopVariant v = coop_variant(c.coop);
       CoopArgs ca{};
