@@ -107,16 +107,17 @@ bool is_device_ptr(const void* p) {
 
 bool aligned(const void* p, size_t a) { return ((uintptr_t)p % a) == 0; }
 
-// The device address of pinned host memory mapped into the device's address
-// space (null: not such memory)
-const void* mapped_host(const void* p) {
+// The device address of pinned host memory mapped into `device`'s address
+// space (null: not such memory, or memory pinned for another device, which is
+// then copied instead of read in place)
+const void* mapped_host(const void* p, int device) {
   if (!p) return nullptr;
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return nullptr;
   }
-  return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+  return a.type == cudaMemoryTypeHost && a.device == device ? a.devicePointer : nullptr;
 }
 
 // Bump allocation over the context's arena: a dry run sizes it, the real run carves it
@@ -457,7 +458,7 @@ const T* stage_column(rdx_ctx* ctx, Arena& a, const T* src, size_t bytes, size_t
     return src;
   }
   if (in_place && ctx->host_reads == RDX_HOST_IN_PLACE && n > 0) {
-    const void* m = mapped_host(src);
+    const void* m = mapped_host(src, ctx->device);
     if (m && aligned(m, align)) {
       if (row_bytes) *row_bytes += (uint32_t)(bytes / n);
       a.take<char>(0);
