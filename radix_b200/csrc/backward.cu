@@ -101,7 +101,6 @@ template <int DEG, int CDT, int EYES>
 __device__ __forceinline__ void splat_backward(const ProjDesc& sd, const GradsOut& go_, const GradsIn& in, uint64_t i,
                                                uint32_t drawn, float* col) {
   constexpr int K = Coeffs<DEG>::value;
-  constexpr int kRow = (1 + K) * 3;
   const uint64_t gi = sd.out_offset + i;
   const DevParams& p = sd.params;
   const DevTable& tb = sd.table;

@@ -28,11 +28,13 @@ __global__ void k_keys_f64(const double* __restrict__ d, uint64_t n, int bits, u
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   const uint64_t nv = VEC ? n / 4 : 0;
-  for (uint64_t i = t; i < nv; i += stride) {
-    const double2 a = __ldcs(reinterpret_cast<const double2*>(d) + 2 * i);
-    const double2 b = __ldcs(reinterpret_cast<const double2*>(d) + 2 * i + 1);
-    __stcs(reinterpret_cast<uint4*>(keys) + i,
-           make_uint4(key_f64(a.x, bits), key_f64(a.y, bits), key_f64(b.x, bits), key_f64(b.y, bits)));
+  if constexpr (VEC) {
+    for (uint64_t i = t; i < nv; i += stride) {
+      const double2 a = __ldcs(reinterpret_cast<const double2*>(d) + 2 * i);
+      const double2 b = __ldcs(reinterpret_cast<const double2*>(d) + 2 * i + 1);
+      __stcs(reinterpret_cast<uint4*>(keys) + i,
+             make_uint4(key_f64(a.x, bits), key_f64(a.y, bits), key_f64(b.x, bits), key_f64(b.y, bits)));
+    }
   }
   for (uint64_t i = nv * 4 + t; i < n; i += stride) keys[i] = key_f64(d[i], bits);
 }
@@ -42,10 +44,12 @@ __global__ void k_keys_f32(const float* __restrict__ d, uint64_t n, int bits, ui
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   const uint64_t nv = VEC ? n / 4 : 0;
-  for (uint64_t i = t; i < nv; i += stride) {
-    const float4 v = __ldcs(reinterpret_cast<const float4*>(d) + i);
-    __stcs(reinterpret_cast<uint4*>(keys) + i,
-           make_uint4(key_f32(v.x, bits), key_f32(v.y, bits), key_f32(v.z, bits), key_f32(v.w, bits)));
+  if constexpr (VEC) {
+    for (uint64_t i = t; i < nv; i += stride) {
+      const float4 v = __ldcs(reinterpret_cast<const float4*>(d) + i);
+      __stcs(reinterpret_cast<uint4*>(keys) + i,
+             make_uint4(key_f32(v.x, bits), key_f32(v.y, bits), key_f32(v.z, bits), key_f32(v.w, bits)));
+    }
   }
   for (uint64_t i = nv * 4 + t; i < n; i += stride) keys[i] = key_f32(d[i], bits);
 }
