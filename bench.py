@@ -44,6 +44,8 @@ def parse():
     p.add_argument("--n", type=int, default=N_SPLATS)
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-forms", action="store_true",
+                   help="frame workload: skip the batched, stereo and backward forms timed after the headline frame")
     p.add_argument("--bits", type=int, default=32, choices=[16, 24, 32],
                    help="sort-key width (32 for the headline; 24 is the reference's default)")
     p.add_argument("--pose", default="scale", choices=["scale", "all-visible"],
@@ -829,6 +831,37 @@ def run_census(args, world, rank, local, device):
     }
 
 
+def other_forms(args, world, rank, local, device):
+    """The other north-star forms, after the headline frame in the same run: the 64-view batch, the
+    16M-splat stereo frame and the 1M-splat gradient, each the leg of its own workload (--workload
+    batched / stereo / backward) with 10 timed steps after 3 warm-up steps; a summary of each line,
+    or the error of a leg that failed (the headline line is printed either way)."""
+    import copy
+    import gc
+
+    import torch
+    sub = copy.copy(args)
+    sub.steps, sub.warmup = 10, 3
+    legs = (("batched", run_batched, ("plain_ms", "batched_over_plain", "hbm_frac_frame", "project_ms", "sort_ms",
+                                      "splat_views", "tuning")),
+            ("stereo", run_stereo, ("batched_ms", "batched_over_plain", "mono_ms", "stereo_over_mono", "project_ms",
+                                    "sort_ms", "hbm_frac_frame", "n")),
+            ("backward", run_backward, ("forward_ms", "backward_over_forward", "n")))
+    forms = {}
+    for name, run, keys in legs:
+        try:
+            r = run(sub, world, rank, local, device)
+            forms[name] = {"metric": r["metric"], "value": r["value"], "unit": r["unit"], "ms_per_step": r["ms_per_step"],
+                           "steps": r["steps"], "roofline_frac": r["roofline"]["frac"],
+                           "roofline_kernel": r["roofline"].get("kernel"), "gpu_launches": r.get("gpu_launches"),
+                           "clocks": r.get("clocks"), **{k: r["config"][k] for k in keys if k in r["config"]}}
+        except Exception as e:  # noqa: BLE001 - recorded in the line, the headline stands
+            forms[name] = {"error": f"{type(e).__name__}: {e}"}
+        gc.collect()
+        torch.cuda.empty_cache()
+    return forms
+
+
 def main():
     global BITS, FRAME_BYTES
     args = parse()
@@ -982,6 +1015,8 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(n)
+    if world == 1 and not args.no_forms and args.n == N_SPLATS and args.pose == "scale" and args.variant is None:
+        line["config"]["forms"] = other_forms(args, world, rank, local, device)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
