@@ -832,7 +832,7 @@ def run_census(args, world, rank, local, device):
 
 
 def other_forms(args, world, rank, local, device):
-    """The other north-star forms, after the headline frame in the same run: the 64-view batch, the
+    """The path's other forms, after the headline frame in the same run: the 64-view batch, the
     16M-splat stereo frame and the 1M-splat gradient, each the leg of its own workload (--workload
     batched / stereo / backward) with 10 timed steps after 3 warm-up steps; a summary of each line,
     or the error of a leg that failed (the headline line is printed either way)."""
