@@ -506,6 +506,7 @@ __global__ void __launch_bounds__(WPB * 32) k_project(const ProjDesc* __restrict
                                                       ProjOutputs out) {
   constexpr bool GUARD = FLAVOR == kGuarded;
   constexpr bool HOST_ROWS = FLAVOR == kHostRows;
+  static_assert(!HOST_ROWS || (WPB * sizeof(WarpSmem<EYES>)) % 16 == 0, "the staged rows start 16-byte aligned");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   WarpSmem<EYES>& W = reinterpret_cast<WarpSmem<EYES>*>(smem_raw)[warp];
