@@ -743,6 +743,7 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
   // counting kernel built: a place of k distinct digits (the top byte of depth
   // keys: a few exponents) ranks on a compact code with ceil(log2 k) ballots
   if (tid < kMaxPasses) s_wsum[9 + tid] = 8u;
+  int passes = a.passes;
   {
     const int top = a.passes - 1;
     const bool present = tid < kRadix && a.hist[top * kRadix + tid] != 0u;
@@ -750,11 +751,14 @@ __global__ void __launch_bounds__(THREADS, 1024 / THREADS) k_sort_coop(CoopArgs 
     if (tid < kRadix) s_code[top * kRadix + tid] = code;
     const int distinct = __syncthreads_count(present);
     if (tid == 0) s_wsum[9 + top] = distinct <= 1 ? 0u : (uint32_t)(32 - __clz(distinct - 1));
+    // Every valid key has the same top digit (depths within one top-byte range): the top pass
+    // would keep the order, so the pass before it writes the outputs
+    if (distinct == 1 && passes > 1) passes--;
   }
 
-  for (int place = 0; place < a.passes; place++) {
+  for (int place = 0; place < passes; place++) {
     const int shift = 8 * place;
-    const bool last = place == a.passes - 1;
+    const bool last = place == passes - 1;
     const bool to_a = a.drop ? (place & 1) != 0 : (place & 1) == 0;
     uint32_t* kout = last ? a.keys_out : (to_a ? a.keys_a : a.keys_b);
     uint32_t* vout = last ? a.vals_out : (to_a ? a.vals_a : a.vals_b);

@@ -138,6 +138,31 @@ def test_compact_from_host_buffers(ctx):
     np.testing.assert_array_equal(ck[:idx.size].view(np.uint32), keys[idx])
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("bits", [24, 32])
+def test_keys_sharing_one_top_digit(ctx, bits, variant):
+    """Every valid key has the same top byte (depths within one top-byte range):
+    the cooperative passes skip the top pass, which would keep the order; every
+    variant's order equals the oracle's."""
+    n = 300_001
+    rng = Mulberry32(17 + bits)
+    low = (rng.uniform(n) * 2.0 ** (bits - 8)).astype(np.uint64).astype(np.uint32)
+    low[::7] = low[3]  # ties
+    keys = (np.uint32(0xA5) << np.uint32(bits - 8)) | low
+    keys[Mulberry32(19).uniform(n) < 0.3] = rb.SortKeys.invalid(bits)
+    ctx.set_sort_variant(variant)
+    try:
+        got, visible = rb.SortKeys.sort(to_cuda(keys.view(np.int32)), n, bits, ctx=ctx)
+        kt, vt = to_cuda(keys.view(np.int32)), torch.arange(n, dtype=torch.int32, device="cuda")
+        rb.RadixSort(kt, vt, ctx).sort(n, bits)
+    finally:
+        ctx.set_sort_variant(-1)
+    expected, exp_visible = orc.sort(keys, n, bits)
+    assert visible == exp_visible
+    np.testing.assert_array_equal(u32(got)[:n], expected[:n])
+    np.testing.assert_array_equal(u32(vt), expected[:n])
+
+
 @pytest.mark.parametrize("bits", BITS)
 def test_splat_sorter_values_count_and_draw_args(ctx, bits):
     n = 123_457
