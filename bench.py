@@ -57,12 +57,13 @@ def parse():
     p.add_argument("--spz-container", default="gzip", choices=["gzip", "ngsp"],
                    help="spz workload: version 3 in gzip (one DEFLATE stream) or SPZ 4 (NGSP, a zstd stream a column)")
     p.add_argument("--workload", default="frame",
-                   choices=["frame", "batched", "stereo", "backward", "ply", "spz", "rdx", "census"],
+                   choices=["frame", "batched", "stereo", "backward", "ply", "spz", "rdx", "census", "rays"],
                    help="frame: 4M SH-3 splats, one view (the headline); batched: 16 scenes x 64 views in one "
                         "CUDA graph; stereo: 16M SH-3 fp16 splats, two eyes; backward: the projection's gradient, 1M; "
                         "ply: decoding a 1M-splat PLY file; spz: decoding a 1M-splat SPZ file from host bytes; "
                         "rdx: decoding a 1M-splat RDX file from host bytes; census: every device entry point "
-                        "once a step, each timed alone")
+                        "once a step, each timed alone; rays: the 3dgut, htgs and raygs words and keys of the 4M "
+                        "SH-3 frame")
     return p.parse_args()
 
 
@@ -796,6 +797,12 @@ def run_census(args, world, rank, local, device):
         ("projection backward 1M", lambda: rb.project_backward(bobj, cam, up, bout["opacity"], None, ctx=ctx), b1, 512,
          lambda: rb.project_collection(bobj, cam, None, BITS, "full", True, names, ctx=ctx, out=bout)),
     ]
+    for method in ("3dgut", "htgs", "raygs"):
+        wout = {"words": torch.empty((4_000_000, rb.method_words(method, 1)), dtype=torch.int32, device=device),
+                "keys": fout["keys"]}
+        families.append((f"{method} words 4M", lambda m=method, o=wout: rb.project_words(obj, cam, m, None, BITS, True,
+                                                                                      ctx=ctx, out=o),
+                         4_000_000, RAY_BYTES[method], None))
     peak, peak_kind = peak_hbm()
     stream = torch.cuda.current_stream(device)
     results = []
@@ -827,6 +834,68 @@ def run_census(args, world, rank, local, device):
         "config": {"workload": "census: each device entry point once a step, timed alone with CUDA events",
                    "results": results, "peak": peak, "peak_kind": peak_kind},
         "e2e": None, "e2e_note": "device-resident inputs; a per-call census",
+        "gpu_launches": ctx.launches() - launches0,
+    }
+
+
+RAY_BYTES = {"3dgut": 236 + 8 * 4 + 4, "htgs": 236 + 8 * 4 + 4, "raygs": 236 + 7 * 4 + 4}
+
+
+def run_rays(args, world, rank, local, device):
+    """The ray projection methods (3dgut, htgs, raygs) on the frame's 4M SH-3
+    table and camera: each method's words and keys (rdx_project_words), timed
+    with CUDA events on the library's stream. A splat's algorithmic bytes: its
+    236 bytes of fields, read once, plus its words and key."""
+    import numpy as np
+    import torch
+
+    import radix_b200 as rb
+    from radix_b200 import synthetic as syn
+    ctx = rb.Context(local)
+    n = args.n
+    d = syn.mixture_table(n, seed=0, sh_degree=SH_DEGREE, device=device)
+    cols = {k: torch.from_numpy(np.ascontiguousarray(d[k])).to(device)
+            for k in ("centers", "log_scales", "quats", "opacities", "colors")}
+    del d
+    obj = [rb.SplatObject(rb.Table.raw(cols["centers"], cols["log_scales"], cols["quats"], cols["opacities"],
+                                       cols["colors"], SH_DEGREE))]
+    cam = syn.scale_camera()
+    peak, peak_kind = peak_hbm()
+    stream = torch.cuda.current_stream(device)
+    results = {}
+    launches0 = ctx.launches()
+    clocks = Clocks(local)  # sampled across the three methods' steps
+    for method in ("3dgut", "htgs", "raygs"):
+        out = {"words": torch.empty((n, rb.method_words(method, 1)), dtype=torch.int32, device=device),
+               "keys": torch.empty(n, dtype=torch.int32, device=device)}
+        times = []
+        for step in range(args.warmup + args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rb.project_words(obj, cam, method, None, BITS, True, ctx=ctx, out=out)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            if step >= args.warmup:
+                times.append(e0.elapsed_time(e1))
+        ms = statistics.median(times)
+        gbs = RAY_BYTES[method] * n / (ms / 1e3) / 1e9
+        results[method] = {"ms": ms, "msplats_s": n / (ms / 1e3) / 1e6, "bytes_per_splat": RAY_BYTES[method],
+                           "gb_s": gbs, "frac": gbs / peak,
+                           "drawn": int((out["keys"] != -1).sum().item())}
+        del out
+    clk = clocks.stop()
+    ctx.synchronize()
+    head = results["3dgut"]
+    return {
+        "metric": "Msplats/s (ray projection words + keys, 3dgut)", "value": head["msplats_s"], "unit": "Msplats/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 maths, u32 words",
+        "data": "synthetic (seeded mulberry32)",
+        "config": {"workload": f"rays: {n} splats SH {SH_DEGREE} fp32, 1920x1080 fov 50, {BITS}-bit keys; "
+                               "each method timed alone (inputs larger than L2)", "methods": results},
+        "roofline": {"bound": "hbm", "achieved": head["gb_s"], "peak": peak, "unit": "GB/s", "frac": head["frac"],
+                     "traffic": None, "kernel": "k_project_rays", "peak_kind": peak_kind},
+        "clocks": clk, "e2e": None, "e2e_note": "device-resident inputs",
         "gpu_launches": ctx.launches() - launches0,
     }
 
@@ -882,7 +951,7 @@ def main():
             from datetime import timedelta
             dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=device)
         run = {"batched": run_batched, "stereo": run_stereo, "backward": run_backward, "ply": run_ply,
-               "spz": run_spz, "rdx": run_rdx, "census": run_census}[args.workload]
+               "spz": run_spz, "rdx": run_rdx, "census": run_census, "rays": run_rays}[args.workload]
         line = run(args, world, rank, local, device)
         if rank == 0:
             print(json.dumps(line))

@@ -360,6 +360,47 @@ int rdx_frame(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_
               const rdx_params* params, int sort_bits, const rdx_outputs* out,
               uint32_t* ordering, uint32_t* visible);
 
+/* ---- the projection methods ---- */
+
+/*
+ * ProjectionMethod (src/render/projections.tsl.ts:42, 469-474). ewa is the
+ * method of rdx_project; the ray methods bound each splat per eye and keep its
+ * 3D shape for the draw's ray evaluation:
+ *   3dgut  a 2D bound from 7 sigma points (gutBound, projections.tsl.ts:183-220)
+ *   htgs   the exact outline of the ellipsoid (htgsBound, 223-262)
+ *   raygs  a tilted 3D quad facing the eye (raygsFrame / raygs, 336-467)
+ */
+#define RDX_METHOD_EWA 0
+#define RDX_METHOD_3DGUT 1
+#define RDX_METHOD_HTGS 2
+#define RDX_METHOD_RAYGS 3
+
+/* Words per splat of `method` with `eyes` eyes (ProjectionDef.headWords +
+   eyes * eyeWords): 4E (ewa), 6 + 2E (3dgut, htgs), 4 + 3E (raygs); -1 when
+   either is out of range. */
+int rdx_method_words(int method, int eyes);
+
+/*
+ * The words and keys of one projection with `method`, as SplatProjection.write
+ * stores them (src/render/SplatProjection.ts:139-153) for
+ * projectCollection (SplatProjector.ts:106-139):
+ *   words  uint32 [n][rdx_method_words(method, E)]: the head words, then each
+ *          eye's, in the reference's order (projections.tsl.ts:5-17); the
+ *          reference's channel c (w<c>, a uint32x4 or uint32x2 texture) holds
+ *          words 4c .. 4c + 3 of a row. A culled eye's words are zero, and so
+ *          are the head words of a splat that no eye can show.
+ *   keys   uint32 [n], as rdx_project's (cull_keys: keys of splats that no
+ *          eye shows are invalid).
+ * Either output may be NULL. ewa forwards to rdx_project (its words output).
+ * The ray methods take device memory only, raw / ext / packed tables, and
+ * object-to-head transforms that are a rotation times a uniform scale:
+ * RDX_ERR_UNSUPPORTED for a cov table or another transform (the reference
+ * converts those through fromCov, not built here).
+ */
+int rdx_project_words(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
+                      const rdx_params* params, int method, int sort_bits, int cull_keys, uint32_t* words,
+                      uint32_t* keys);
+
 /* ---- the projection's gradient ---- */
 
 /* Upstream gradients, laid out as rdx_project's outputs (float32, device

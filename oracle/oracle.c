@@ -622,16 +622,15 @@ static int mat_equal(const double a[16], const double b[16]) {
   return 1;
 }
 
-/* One splat: outputs at index `gi` of the collection (n splats, E eyes) */
-static void project_one(const orc_splat* s, const object_setup* o, const eye_setup* eyes, int n_eyes,
-                        const rdx_camera* cam, int sort_bits, int cull_keys, uint64_t gi, uint64_t n,
-                        const orc_outputs* out) {
+/* SH in object space from the view origin: splatGenerator.ts:152-158, sh.tsl.ts:255-266.
+   A table with SH gets rgb + SH clamped at 0 even when the cap draws no band
+   (GpuShReader.apply); a table without SH has no reader and no clamp. A splat
+   at the view origin has no direction and gets no SH. */
+static void splat_rgb(const orc_splat* s, const object_setup* o, double rgb[3]) {
   const rdx_params* p = &o->params;
-  /* SH in object space from the view origin: splatGenerator.ts:152-158, sh.tsl.ts:255-266 */
-  /* A table with SH gets rgb + SH clamped at 0 even when the cap draws no band
-     (GpuShReader.apply); a table without SH has no reader and no clamp. A splat
-     at the view origin has no direction and gets no SH. */
-  double rgb[3] = {s->rgb[0], s->rgb[1], s->rgb[2]};
+  rgb[0] = s->rgb[0];
+  rgb[1] = s->rgb[1];
+  rgb[2] = s->rgb[2];
   int degree = s->sh_degree < p->max_sh_degree ? s->sh_degree : p->max_sh_degree;
   if (s->sh_degree >= 1) {
     double sh[3] = {0.0, 0.0, 0.0};
@@ -648,6 +647,15 @@ static void project_one(const orc_splat* s, const object_setup* o, const eye_set
     }
     for (int c = 0; c < 3; c++) rgb[c] = fmax(rgb[c] + sh[c], 0.0);
   }
+}
+
+/* One splat: outputs at index `gi` of the collection (n splats, E eyes) */
+static void project_one(const orc_splat* s, const object_setup* o, const eye_setup* eyes, int n_eyes,
+                        const rdx_camera* cam, int sort_bits, int cull_keys, uint64_t gi, uint64_t n,
+                        const orc_outputs* out) {
+  const rdx_params* p = &o->params;
+  double rgb[3];
+  splat_rgb(s, o, rgb);
   /* toCov: splats.tsl.ts:176-187, math.ts:12-45 */
   double qx = s->quat[0], qy = s->quat[1], qz = s->quat[2], qw = s->quat[3];
   double ql = sqrt(qx * qx + qy * qy + qz * qz + qw * qw);
@@ -916,6 +924,607 @@ int orc_project(const rdx_object* objects, int n_objects, const rdx_camera* cam,
     orc_load_splat(objects[oi].table, (uint64_t)gi - objs[oi].offset, &s);
     project_one(&s, &objs[oi], eyes, cam->eyes, cam, sort_bits, cull_keys, (uint64_t)gi, n, out);
   }
+  free(objs);
+  return 0;
+}
+
+/* ---- the ray projection methods: src/render/projections.tsl.ts:170-474 ---- */
+
+static double dot3(const double a[3], const double b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+/* quatRotate (src/gpu/math.tsl.ts:12-15): v + w t + q.xyz x t with t = 2 q.xyz x v */
+static void quat_rotate(const double q[4], const double v[3], double out[3]) {
+  const double t[3] = {2.0 * (q[1] * v[2] - q[2] * v[1]), 2.0 * (q[2] * v[0] - q[0] * v[2]),
+                       2.0 * (q[0] * v[1] - q[1] * v[0])};
+  const double r[3] = {v[0] + q[3] * t[0] + (q[1] * t[2] - q[2] * t[1]), v[1] + q[3] * t[1] + (q[2] * t[0] - q[0] * t[2]),
+                       v[2] + q[3] * t[2] + (q[0] * t[1] - q[1] * t[0])};
+  memcpy(out, r, sizeof(r));
+}
+
+/* quatMul (math.tsl.ts:17-23): a applied after b */
+static void quat_mul(const double a[4], const double b[4], double out[4]) {
+  const double r[4] = {a[3] * b[0] + a[0] * b[3] + a[1] * b[2] - a[2] * b[1],
+                       a[3] * b[1] - a[0] * b[2] + a[1] * b[3] + a[2] * b[0],
+                       a[3] * b[2] + a[0] * b[1] - a[1] * b[0] + a[2] * b[3],
+                       a[3] * b[3] - a[0] * b[0] - a[1] * b[1] - a[2] * b[2]};
+  memcpy(out, r, sizeof(r));
+}
+
+static void quat_normalize(const double q[4], double out[4]) { /* a zero quaternion: the identity */
+  const double l = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  if (!(l > 0)) {
+    out[0] = out[1] = out[2] = 0.0;
+    out[3] = 1.0;
+    return;
+  }
+  for (int k = 0; k < 4; k++) out[k] = q[k] / l;
+}
+
+/* The unit quaternion of a rotation matrix (row-major), by the trace and the
+   largest diagonal element (Shoemake's method), as three.js Matrix4.decompose
+   finds the quaternions of setTransform (splatTransform.tsl.ts:64-74) and
+   SplatCamera.setViews (splatCamera.ts:129-131) */
+static void rotation_to_quat(const double m[9], double q[4]) {
+  const double tr = m[0] + m[4] + m[8];
+  if (tr > 0.0) {
+    const double s = 0.5 / sqrt(tr + 1.0);
+    q[3] = 0.25 / s;
+    q[0] = (m[7] - m[5]) * s;
+    q[1] = (m[2] - m[6]) * s;
+    q[2] = (m[3] - m[1]) * s;
+  } else if (m[0] > m[4] && m[0] > m[8]) {
+    const double s = 2.0 * sqrt(1.0 + m[0] - m[4] - m[8]);
+    q[3] = (m[7] - m[5]) / s;
+    q[0] = 0.25 * s;
+    q[1] = (m[1] + m[3]) / s;
+    q[2] = (m[2] + m[6]) / s;
+  } else if (m[4] > m[8]) {
+    const double s = 2.0 * sqrt(1.0 + m[4] - m[0] - m[8]);
+    q[3] = (m[2] - m[6]) / s;
+    q[0] = (m[1] + m[3]) / s;
+    q[1] = 0.25 * s;
+    q[2] = (m[5] + m[7]) / s;
+  } else {
+    const double s = 2.0 * sqrt(1.0 + m[8] - m[0] - m[4]);
+    q[3] = (m[3] - m[1]) / s;
+    q[0] = (m[2] + m[6]) / s;
+    q[1] = (m[5] + m[7]) / s;
+    q[2] = 0.25 * s;
+  }
+}
+
+static double det3_cols(const double* c0, const double* c1, const double* c2) {
+  return c0[0] * (c1[1] * c2[2] - c1[2] * c2[1]) - c1[0] * (c0[1] * c2[2] - c0[2] * c2[1]) +
+         c2[0] * (c0[1] * c1[2] - c0[2] * c1[1]);
+}
+
+/* The rotation of a column-major 4x4's 3x3 part (columns divided by their
+   lengths, the first negated when the determinant is negative) as a quaternion */
+static void decompose_quat(const double m[16], double q[4]) {
+  const double* c[3] = {m, m + 4, m + 8};
+  double len[3] = {sqrt(dot3(c[0], c[0])), sqrt(dot3(c[1], c[1])), sqrt(dot3(c[2], c[2]))};
+  if (det3_cols(c[0], c[1], c[2]) < 0.0) len[0] = -len[0];
+  double r[9];
+  for (int row = 0; row < 3; row++)
+    for (int col = 0; col < 3; col++) r[row * 3 + col] = c[col][row] / len[col];
+  rotation_to_quat(r, q);
+}
+
+/* isUniformScale (splatTransform.tsl.ts:46-62) of the object -> head matrix:
+   with G = M^T M and s2 = trace(G) / 3, every entry of G - s2 I within 1e-6 s2
+   and det(M) > 0; then the rotation and |det(M)|^(1/3) (setTransform, 64-74) */
+static int uniform_transform(const double a[16], double q[4], double* scale) {
+  const double* c[3] = {a, a + 4, a + 8};
+  const double s2 = (dot3(c[0], c[0]) + dot3(c[1], c[1]) + dot3(c[2], c[2])) / 3.0;
+  if (!(s2 > 0)) return 0;
+  for (int i = 0; i < 3; i++)
+    for (int j = i; j < 3; j++)
+      if (fabs(dot3(c[i], c[j]) - (i == j ? s2 : 0.0)) > 1e-6 * s2) return 0;
+  const double det = det3_cols(c[0], c[1], c[2]);
+  if (!(det > 0)) return 0;
+  decompose_quat(a, q);
+  *scale = cbrt(fabs(det));
+  return 1;
+}
+
+/* basisToQuat (math.tsl.ts:117-150): the w >= 0 quaternion of the orthonormal
+   columns x, y, z */
+static void basis_to_quat(const double x[3], const double y[3], const double z[3], double q[4]) {
+  double four, inv;
+  if (z[2] <= 0.0) {
+    const double dif10 = y[1] - x[0], omm22 = 1.0 - z[2];
+    if (dif10 <= 0.0) {
+      four = omm22 - dif10;
+      inv = 0.5 / sqrt(fmax(four, 1e-30));
+      q[0] = four * inv, q[1] = (x[1] + y[0]) * inv, q[2] = (x[2] + z[0]) * inv, q[3] = (y[2] - z[1]) * inv;
+    } else {
+      four = omm22 + dif10;
+      inv = 0.5 / sqrt(fmax(four, 1e-30));
+      q[0] = (x[1] + y[0]) * inv, q[1] = four * inv, q[2] = (y[2] + z[1]) * inv, q[3] = (z[0] - x[2]) * inv;
+    }
+  } else {
+    const double sum10 = y[1] + x[0], opm22 = 1.0 + z[2];
+    if (sum10 <= 0.0) {
+      four = opm22 - sum10;
+      inv = 0.5 / sqrt(fmax(four, 1e-30));
+      q[0] = (x[2] + z[0]) * inv, q[1] = (y[2] + z[1]) * inv, q[2] = four * inv, q[3] = (x[1] - y[0]) * inv;
+    } else {
+      four = opm22 + sum10;
+      inv = 0.5 / sqrt(fmax(four, 1e-30));
+      q[0] = (y[2] - z[1]) * inv, q[1] = (z[0] - x[2]) * inv, q[2] = (x[1] - y[0]) * inv, q[3] = four * inv;
+    }
+  }
+  const double l = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  for (int k = 0; k < 4; k++) q[k] /= l;
+  if (q[3] < 0.0)
+    for (int k = 0; k < 4; k++) q[k] = -q[k];
+}
+
+/* scaleQuatMatrix (math.tsl.ts:25-44): column k is axis k of R(q) times s[k] */
+static void scale_quat_cols(const double s[3], const double q[4], double col[3][3]) {
+  const double x = q[0], y = q[1], z = q[2], w = q[3];
+  col[0][0] = s[0] * (1.0 - 2.0 * (y * y + z * z));
+  col[0][1] = s[0] * (2.0 * (x * y + w * z));
+  col[0][2] = s[0] * (2.0 * (x * z - w * y));
+  col[1][0] = s[1] * (2.0 * (x * y - w * z));
+  col[1][1] = s[1] * (1.0 - 2.0 * (x * x + z * z));
+  col[1][2] = s[1] * (2.0 * (y * z + w * x));
+  col[2][0] = s[2] * (2.0 * (x * z + w * y));
+  col[2][1] = s[2] * (2.0 * (y * z - w * x));
+  col[2][2] = s[2] * (1.0 - 2.0 * (x * x + y * y));
+}
+
+/* P (column-major) times (v, 0) */
+static void proj_dir(const double p[16], const double v[3], double out[4]) {
+  for (int row = 0; row < 4; row++) {
+    double s = p[0 * 4 + row] * v[0];
+    s = s + p[1 * 4 + row] * v[1];
+    s = s + p[2 * 4 + row] * v[2];
+    out[row] = s;
+  }
+}
+
+typedef struct orc_bound { /* Bound, projection.tsl.ts:206-210 */
+  double ndc[2], angle, scales[2];
+} orc_bound;
+
+/* eigenvector2 (projection.tsl.ts:215-219) */
+static void eigenvector2(double a, double b, double d, double eig, double v[2]) {
+  double vx, vy;
+  if (fabs(a - eig) >= fabs(d - eig)) {
+    vx = b;
+    vy = eig - a;
+  } else {
+    vx = eig - d;
+    vy = b;
+  }
+  const double len = sqrt(vx * vx + vy * vy);
+  v[0] = len > 0.0 ? vx / len : 1.0;
+  v[1] = len > 0.0 ? vy / len : 0.0;
+}
+
+/* boundFromCov (projection.tsl.ts:223-240) */
+static int bound_from_cov(double a, double b, double d, double std_dev, const rdx_params* p, orc_bound* bd) {
+  const double det = a * d - b * b;
+  const double half = (a - d) * 0.5;
+  const double eigen1 = (a + d) * 0.5 + sqrt(half * half + b * b);
+  const double eigen2 = eigen1 > 0.0 ? fmax(det / eigen1, 0.0) : 0.0;
+  const double scale1 = fmin((double)p->max_pixel_radius, std_dev * sqrt(fmax(eigen1, 0.0)));
+  const double scale2 = fmin((double)p->max_pixel_radius, std_dev * sqrt(eigen2));
+  const int ok = scale1 >= (double)p->min_pixel_radius || scale2 >= (double)p->min_pixel_radius;
+  if (ok) {
+    double v[2];
+    eigenvector2(a, b, d, eigen1, v);
+    const double angle = atan2(v[1], v[0]);
+    bd->angle = angle < 0.0 ? angle + PI : angle;
+    bd->scales[0] = scale1;
+    bd->scales[1] = scale2;
+  }
+  return ok;
+}
+
+/* screenBound (projection.tsl.ts:243-247) */
+static void screen_bound(const rdx_camera* cam, const rdx_params* p, orc_bound* bd) {
+  bd->ndc[0] = bd->ndc[1] = 0.0;
+  bd->angle = 0.0;
+  bd->scales[0] = bd->scales[1] = fmin((double)p->max_pixel_radius, sqrt(cam->width * cam->width + cam->height * cam->height) * 0.5);
+}
+
+/* clipBoundToScreen (projection.tsl.ts:250-273) */
+static int clip_bound_to_screen(const rdx_camera* cam, orc_bound* bd) {
+  const double hx = cam->width * 0.5, hy = cam->height * 0.5;
+  const double ca = cos(bd->angle), sa = sin(bd->angle);
+  const double cx = ca * bd->scales[0], cy = ca * bd->scales[1], sx = sa * bd->scales[0], sy = sa * bd->scales[1];
+  const double ex = sqrt(cx * cx + sy * sy), ey = sqrt(sx * sx + cy * cy);
+  const double mx = bd->ndc[0] * hx, my = bd->ndc[1] * hy;
+  double lox = mx - ex, loy = my - ey, hix = mx + ex, hiy = my + ey;
+  if (!(lox >= -hx && loy >= -hy && hix <= hx && hiy <= hy)) {
+    lox = fmax(lox, -hx);
+    loy = fmax(loy, -hy);
+    hix = fmin(hix, hx);
+    hiy = fmin(hiy, hy);
+    if (lox >= hix || loy >= hiy) return 0;
+    bd->ndc[0] = (lox + hix) * 0.5 / hx;
+    bd->ndc[1] = (loy + hiy) * 0.5 / hy;
+    bd->angle = 0.0;
+    bd->scales[0] = (hix - lox) * 0.5;
+    bd->scales[1] = (hiy - loy) * 0.5;
+  }
+  return 1;
+}
+
+/* encodeLogScale (projection.tsl.ts:299-303) in `bits`, rounded up when outward */
+static uint32_t encode_log_scale_bits(double scale, int bits, int outward) {
+  const double top = (double)((1u << bits) - 2u);
+  const double normalized = (clampd(log2(fmax(scale, 1e-20)), -4.0, 12.0) + 4.0) / 16.0 * top;
+  return (uint32_t)clampd(outward ? ceil(normalized) : floor(normalized + 0.5), 0.0, top) + 1u;
+}
+
+/* encodeBound (projection.tsl.ts:352-360): NDC 2x16; 10-bit angle | 2 x 11-bit
+   log2 scales rounded outward, widened by the angle's half step */
+static void encode_bound(const orc_bound* bd, uint32_t w[2]) {
+  const uint32_t angle_code = (uint32_t)floor(bd->angle / PI * 1024.0 + 0.5) & 1023u;
+  const double slack = fmax(bd->scales[0], bd->scales[1]) * (sin(PI / 1024.0 / 2.0) * 1.001);
+  w[0] = encode_fixed16(bd->ndc[0]) | (encode_fixed16(bd->ndc[1]) << 16);
+  w[1] = angle_code | (encode_log_scale_bits(bd->scales[0] + slack, 11, 1) << 10) |
+         (encode_log_scale_bits(bd->scales[1] + slack, 11, 1) << 21);
+}
+
+/* encodeCenter (projection.tsl.ts:317-332): [direction's top 16 + 16 bits,
+   float32 distance, low 4 + 4 bits at bits 24-31] */
+static void encode_center(const double c[3], uint32_t w[3]) {
+  const double distance = sqrt(dot3(c, c));
+  const double l1 = fmax(fabs(c[0]) + fabs(c[1]) + fabs(c[2]), 1e-30);
+  double px = c[0] / l1, py = c[1] / l1;
+  const double sx = px >= 0.0 ? 1.0 : -1.0, sy = py >= 0.0 ? 1.0 : -1.0;
+  if (c[2] < 0.0) {
+    const double ax = fabs(px);
+    px = (1.0 - fabs(py)) * sx;
+    py = (1.0 - ax) * sy;
+  }
+  const uint32_t qx = (uint32_t)floor((px * 0.5 + 0.5) * 1048575.0 + 0.5);
+  const uint32_t qy = (uint32_t)floor((py * 0.5 + 0.5) * 1048575.0 + 0.5);
+  const float df = (float)distance;
+  uint32_t db;
+  memcpy(&db, &df, 4);
+  w[0] = (qx >> 4) | ((qy >> 4) << 16);
+  w[1] = db;
+  w[2] = ((qx & 15u) << 24) | (qy << 28);
+}
+
+/* gutBound (projections.tsl.ts:183-220): the unscented transform of 7 sigma points */
+static int gut_bound(const double ce[3], const eye_setup* e, const double q[4], const double s[3], double std_dev,
+                     const rdx_params* p, const rdx_camera* cam, orc_bound* bd) {
+  const double r3 = sqrt(3.0);
+  const double ss[3] = {s[0] * r3, s[1] * r3, s[2] * r3};
+  double col[3][3];
+  scale_quat_cols(ss, q, col);
+  const double hx = cam->width * 0.5, hy = cam->height * 0.5;
+  double px[7], py[7];
+  int in_front = 1;
+  for (int i = 0; i < 7; i++) {
+    double pt[3] = {ce[0], ce[1], ce[2]};
+    if (i > 0) {
+      const double sign = (i & 1) ? 1.0 : -1.0;
+      for (int k = 0; k < 3; k++) pt[k] = ce[k] + sign * col[(i - 1) / 2][k];
+    }
+    double clip[4];
+    clip_of(e->proj, pt, clip);
+    in_front = in_front && clip[3] > 0.0;
+    px[i] = clip[0] / clip[3] * hx;
+    py[i] = clip[1] / clip[3] * hy;
+  }
+  if (!in_front) {
+    screen_bound(cam, p, bd);
+    return 1;
+  }
+  const double sixth = 1.0 / 6.0;
+  double mx = 0.0, my = 0.0;
+  for (int i = 1; i < 7; i++) {
+    mx += px[i] * sixth;
+    my += py[i] * sixth;
+  }
+  const double d0x = px[0] - mx, d0y = py[0] - my;
+  double a = d0x * d0x * 2.0, b = d0x * d0y * 2.0, d = d0y * d0y * 2.0;
+  for (int i = 1; i < 7; i++) {
+    const double dx = px[i] - mx, dy = py[i] - my;
+    a += dx * dx * sixth;
+    b += dx * dy * sixth;
+    d += dy * dy * sixth;
+  }
+  const int ok = bound_from_cov(a, b, d, std_dev, p, bd);
+  bd->ndc[0] = mx / hx;
+  bd->ndc[1] = my / hy;
+  return ok;
+}
+
+/* htgsBound (projections.tsl.ts:223-262): the exact outline of the std-dev ellipsoid */
+static int htgs_bound(const double ce[3], const double ndc[2], const eye_setup* e, const double q[4], const double s[3],
+                      double std_dev, const rdx_params* p, const rdx_camera* cam, orc_bound* bd) {
+  const double ss[3] = {s[0] * std_dev, s[1] * std_dev, s[2] * std_dev};
+  double col[3][3], T[3][4], c3[4];
+  scale_quat_cols(ss, q, col);
+  for (int k = 0; k < 3; k++) proj_dir(e->proj, col[k], T[k]);
+  clip_of(e->proj, ce, c3);
+  const double xs[3] = {T[0][0], T[1][0], T[2][0]}, ys[3] = {T[0][1], T[1][1], T[2][1]},
+               ws[3] = {T[0][3], T[1][3], T[2][3]};
+  const double qww = dot3(ws, ws) - c3[3] * c3[3];
+  int valid = qww < 0.0 && c3[3] > 0.0;
+  double cx = 0.0, cy = 0.0, a = 0.0, b = 0.0, d = 0.0;
+  if (valid) {
+    double u[3], v[3];
+    for (int k = 0; k < 3; k++) {
+      u[k] = xs[k] * c3[3] - ws[k] * c3[0];
+      v[k] = ys[k] * c3[3] - ws[k] * c3[1];
+    }
+    const double sww = dot3(ws, ws), xw = dot3(xs, ws), yw = dot3(ys, ws);
+    const double inv_c2 = 1.0 / (qww * qww);
+    const double hx = cam->width * 0.5, hy = cam->height * 0.5;
+    a = (dot3(u, u) - (sww * dot3(xs, xs) - xw * xw)) * inv_c2 * hx * hx;
+    b = (dot3(u, v) - (sww * dot3(xs, ys) - xw * yw)) * inv_c2 * hx * hy;
+    d = (dot3(v, v) - (sww * dot3(ys, ys) - yw * yw)) * inv_c2 * hy * hy;
+    cx = ndc[0] + dot3(ws, u) / (c3[3] * qww);
+    cy = ndc[1] + dot3(ws, v) / (c3[3] * qww);
+    valid = a > 0.0 && d > 0.0 && a * d - b * b > 0.0;
+  }
+  if (!valid) {
+    screen_bound(cam, p, bd);
+    return 1;
+  }
+  const int ok = bound_from_cov(a, b, d, 1.0, p, bd);
+  bd->ndc[0] = cx;
+  bd->ndc[1] = cy;
+  return ok;
+}
+
+/* quadOffScreen (projections.tsl.ts:336-352) */
+static int quad_off_screen(const double proj[16], const double mu[3], const double a0[3], const double a1[3]) {
+  double c[4], p0[4], p1[4];
+  clip_of(proj, mu, c);
+  proj_dir(proj, a0, p0);
+  proj_dir(proj, a1, p1);
+  int in_front = 1, o0 = 1, o1 = 1, o2 = 1, o3 = 1;
+  for (int i = 0; i < 4; i++) {
+    double clip[4];
+    for (int k = 0; k < 4; k++) clip[k] = c[k] + ((i & 1) ? p0[k] : -p0[k]) + ((i & 2) ? p1[k] : -p1[k]);
+    in_front = in_front && clip[3] > 0.0;
+    o0 = o0 && clip[0] < -clip[3];
+    o1 = o1 && clip[0] > clip[3];
+    o2 = o2 && clip[1] < -clip[3];
+    o3 = o3 && clip[1] > clip[3];
+  }
+  return in_front && (o0 || o1 || o2 || o3);
+}
+
+/* raygsFrame (projections.tsl.ts:356-397): the quad facing the eye */
+static int raygs_frame(const double ce[3], const eye_setup* e, const double q[4], const double s[3], double std_dev,
+                       double fq[4], double lengths[2], double* c2_out) {
+  int ok = 1;
+  const double kappa = std_dev * std_dev;
+  const double conj[4] = {-q[0], -q[1], -q[2], q[3]};
+  double local[3], mu[3];
+  quat_rotate(conj, ce, local);
+  for (int k = 0; k < 3; k++) local[k] /= s[k];
+  double c2 = dot3(local, local);
+  if (e->ortho) {
+    const double back[3] = {0.0, 0.0, -1.0};
+    double v[3];
+    quat_rotate(conj, back, v);
+    for (int k = 0; k < 3; k++) v[k] /= s[k];
+    const double l = sqrt(dot3(v, v));
+    for (int k = 0; k < 3; k++) mu[k] = v[k] / l;
+    c2 = 1e18;
+  } else {
+    ok = c2 > kappa * 1.0001;
+    const double inv = 1.0 / sqrt(c2);
+    for (int k = 0; k < 3; k++) mu[k] = local[k] * inv;
+  }
+  const double t[3] = {mu[0], mu[1], mu[2] + (mu[2] >= 0.0 ? 1.0 : -1.0)};
+  const double inv_den = 2.0 / dot3(t, t);
+  const double v0[3] = {s[0] * (t[0] * (t[0] * inv_den) - 1.0), s[1] * (t[1] * (t[0] * inv_den)),
+                        s[2] * (t[2] * (t[0] * inv_den))};
+  const double v1[3] = {s[0] * (t[0] * (t[1] * inv_den)), s[1] * (t[1] * (t[1] * inv_den) - 1.0),
+                        s[2] * (t[2] * (t[1] * inv_den))};
+  double q0[3], q1[3];
+  quat_rotate(q, v0, q0);
+  quat_rotate(q, v1, q1);
+  const double bxx = dot3(q0, q0), bxy = dot3(q0, q1), byy = dot3(q1, q1);
+  const double diff = bxx - byy;
+  const double eig1 = (bxx + byy) * 0.5 + sqrt(fmax(0.0, diff * diff * 0.25 + bxy * bxy));
+  double u1[2];
+  eigenvector2(bxx, bxy, byy, eig1, u1);
+  const double u0[2] = {-u1[1], u1[0]};
+  double axis0[3], axis1[3];
+  for (int k = 0; k < 3; k++) {
+    axis0[k] = q0[k] * u0[0] + q1[k] * u0[1];
+    axis1[k] = q0[k] * u1[0] + q1[k] * u1[1];
+  }
+  lengths[0] = sqrt(dot3(axis0, axis0));
+  lengths[1] = sqrt(dot3(axis1, axis1));
+  ok = ok && lengths[0] > 0.0 && lengths[1] > 0.0;
+  const double z_scale = std_dev / sqrt(fmax(1.0 - kappa / c2, 1e-4));
+  double za0[3], za1[3];
+  for (int k = 0; k < 3; k++) {
+    za0[k] = axis0[k] * z_scale;
+    za1[k] = axis1[k] * z_scale;
+  }
+  ok = ok && !quad_off_screen(e->proj, ce, za0, za1);
+  double n0[3], n1[3], n2[3];
+  for (int k = 0; k < 3; k++) {
+    n0[k] = axis0[k] / lengths[0];
+    n1[k] = axis1[k] / lengths[1];
+  }
+  n2[0] = n0[1] * n1[2] - n0[2] * n1[1];
+  n2[1] = n0[2] * n1[0] - n0[0] * n1[2];
+  n2[2] = n0[0] * n1[1] - n0[1] * n1[0];
+  basis_to_quat(n0, n1, n2, fq);
+  *c2_out = c2;
+  return ok;
+}
+
+/* One splat of a ray method: its head and eye words (row `gi`) and its key
+   (SplatProjection.project/write, SplatProjection.ts:126-153; rayProjection
+   and raygs, projections.tsl.ts:266-333, 399-467) */
+static void rays_one(const orc_splat* s, const object_setup* o, const eye_setup* eyes, const double eye_q[2][4],
+                     int n_eyes, const rdx_camera* cam, int method, const double tq[4], double tscale, int sort_bits,
+                     int cull_keys, uint64_t gi, uint32_t* words, uint32_t* keys) {
+  const rdx_params* p = &o->params;
+  const int head_words = method == ORC_METHOD_RAYGS ? 4 : 6, eye_words = method == ORC_METHOD_RAYGS ? 3 : 2;
+  uint32_t* row = words ? words + gi * (uint64_t)(head_words + n_eyes * eye_words) : NULL;
+  double rgb[3];
+  splat_rgb(s, o, rgb);
+  /* transformUniform (splatTransform.tsl.ts:143-152) */
+  double ch[3], qn[4], qh[4];
+  xform_point(o->a, s->center, ch);
+  quat_normalize(s->quat, qn);
+  quat_mul(tq, qn, qh);
+  double sc[3] = {s->scales[0] * tscale, s->scales[1] * tscale, s->scales[2] * tscale};
+  /* prepareSplat, splat form (projection.tsl.ts:42-64) */
+  double opacity = s->opacity, inflate = 1.0;
+  if (opacity > 1.0) {
+    opacity = fmin(opacity * 4.0 - 3.0, 5.0);
+    if (p->lod_inflate) {
+      inflate = pow(exp((opacity * opacity - 1.0) / E_CONST), 1.0 / 3.0);
+      opacity = 1.0;
+    }
+  }
+  for (int k = 0; k < 3; k++) sc[k] *= inflate;
+  const double std_dev = opacity > 1.0 ? (double)p->max_std_dev + (opacity - 1.0) * 0.7 : (double)p->max_std_dev;
+  const int invisible = opacity <= 0.0 || opacity < (double)p->min_alpha || (sc[0] == 0.0 && sc[1] == 0.0 && sc[2] == 0.0);
+  /* the head: splatInView(headFrame()), eye 0's lens */
+  const eye_setup* e0 = &eyes[0];
+  double hclip[4];
+  clip_of(e0->proj, ch, hclip);
+  double hblur = p->blur_amount;
+  if (p->focal_distance > 0.0f && p->aperture_tan > 0.0f && ch[2] < 0.0) {
+    const double depth = -ch[2];
+    const double coc_view = fabs(depth - (double)p->focal_distance) * (double)p->aperture_tan;
+    const double focal_pixels = cam->height * 0.5 * e0->proj[5];
+    const double coc = e0->ortho ? coc_view * focal_pixels : coc_view * focal_pixels / depth;
+    hblur = fmin(fmax(coc * coc, hblur), (double)p->max_pixel_radius * p->max_pixel_radius);
+  }
+  const double distance = sqrt(ch[0] * ch[0] + ch[1] * ch[1] + ch[2] * ch[2]);
+  int guarded = 1;
+  if (p->sort_guard > 0.0f) { /* inSortGuard, splat form (projection.tsl.ts:145-155) */
+    const double radius = fmax(fmax(sc[0], sc[1]), sc[2]) * p->max_std_dev;
+    const double w = fmax(hclip[3], 1e-6);
+    const double rx = e0->proj[0] * radius / w, ry = e0->proj[5] * radius / w;
+    const int inside = fabs(hclip[0] / w) - rx <= (double)p->sort_guard + 1.0 &&
+                       fabs(hclip[1] / w) - ry <= (double)p->sort_guard + 1.0;
+    guarded = ch[2] < radius && (inside || -ch[2] <= radius);
+  }
+  /* headBasis (projections.tsl.ts:173-180): viewBasis, then mipInflate (projection.tsl.ts:169-197) */
+  int ok = !invisible;
+  double op = opacity, hq[4], hs[3];
+  quat_normalize(qh, hq);
+  const double smax = fmax(sc[0], fmax(sc[1], sc[2])) * 1e-4;
+  for (int k = 0; k < 3; k++) hs[k] = fmax(sc[k], smax);
+  {
+    const double conj[4] = {-hq[0], -hq[1], -hq[2], hq[3]};
+    double local[3];
+    quat_rotate(conj, ch, local);
+    const double l2[3] = {local[0] * local[0], local[1] * local[1], local[2] * local[2]};
+    const double pixel = 2.0 / (cam->height * e0->proj[5]);
+    const double footprint = pixel * pixel * (e0->ortho ? 1.0 : dot3(ch, ch));
+    double s2[3], s2b[3];
+    for (int k = 0; k < 3; k++) {
+      s2[k] = hs[k] * hs[k] + (double)p->pre_blur_amount * footprint;
+      s2b[k] = s2[k] + hblur * footprint;
+    }
+    const double num = l2[0] * s2[1] * s2[2] + l2[1] * s2[0] * s2[2] + l2[2] * s2[0] * s2[1];
+    const double den = l2[0] * s2b[1] * s2b[2] + l2[1] * s2b[0] * s2b[2] + l2[2] * s2b[0] * s2b[1];
+    op *= den > 0.0 ? sqrt(fmax(num / den, 0.0)) : 1.0;
+    for (int k = 0; k < 3; k++) hs[k] = sqrt(s2b[k]);
+  }
+  ok = ok && op >= (double)p->min_alpha;
+  int any_visible = 0;
+  for (int v = 0; v < n_eyes; v++) {
+    const eye_setup* e = &eyes[v];
+    uint32_t ew[3] = {0u, 0u, 0u};
+    double ce[3], clip[4];
+    xform_point(e->from_head, ch, ce);
+    clip_of(e->proj, ce, clip);
+    const int cull_depth = ce[2] >= 0.0 || clip[2] < cam->ndc_z_min * clip[3] || clip[2] >= clip[3];
+    if (ok && !cull_depth) {
+      double eq[4];
+      quat_mul(eye_q[v], hq, eq); /* frameQuat (projection.tsl.ts:101) */
+      if (method == ORC_METHOD_RAYGS) {
+        double fq[4], lengths[2], c2;
+        if (raygs_frame(ce, e, eq, hs, std_dev, fq, lengths, &c2)) {
+          const float c2f = (float)c2;
+          ew[0] = orc_encode_quat_oct32(fq);
+          memcpy(&ew[1], &c2f, 4);
+          ew[2] = orc_encode_half(log(lengths[0])) | (orc_encode_half(log(lengths[1])) << 16);
+          any_visible = 1;
+        }
+      } else {
+        const double ndc[2] = {clip[3] > 0.0 ? clip[0] / clip[3] : 0.0, clip[3] > 0.0 ? clip[1] / clip[3] : 0.0};
+        orc_bound bd = {{0.0, 0.0}, 0.0, {0.0, 0.0}};
+        const int bound_ok = method == ORC_METHOD_3DGUT ? gut_bound(ce, e, eq, hs, std_dev, p, cam, &bd)
+                                                        : htgs_bound(ce, ndc, e, eq, hs, std_dev, p, cam, &bd);
+        const int on_screen = clip_bound_to_screen(cam, &bd);
+        if (bound_ok && on_screen) {
+          encode_bound(&bd, ew);
+          any_visible = 1;
+        }
+      }
+    }
+    if (row)
+      for (int k = 0; k < eye_words; k++) row[head_words + v * eye_words + k] = ew[k];
+  }
+  if (row) {
+    uint32_t hw[6] = {0u, 0u, 0u, 0u, 0u, 0u};
+    if (ok) {
+      uint32_t c[3];
+      encode_center(ch, c);
+      const double stored = op > 1.0 ? (op + 3.0) * 0.25 : op;
+      hw[0] = c[0];
+      hw[1] = c[1];
+      hw[2] = orc_encode_ext_rgb(rgb);
+      if (method == ORC_METHOD_RAYGS) {
+        hw[3] = encode_opacity8(stored) | c[2];
+      } else {
+        hw[3] = orc_encode_quat_oct32(hq);
+        hw[4] = orc_encode_half(log(hs[0])) | (orc_encode_half(log(hs[1])) << 16);
+        hw[5] = orc_encode_half(log(hs[2])) | (encode_opacity8(stored) << 16) | c[2];
+      }
+    }
+    for (int k = 0; k < head_words; k++) row[k] = hw[k];
+  }
+  const int keyed = cull_keys ? any_visible : (!invisible && guarded);
+  if (keys) keys[gi] = keyed ? orc_sort_key(distance, sort_bits) : orc_invalid_key(sort_bits);
+}
+
+int orc_project_rays(const rdx_object* objects, int n_objects, const rdx_camera* cam, const rdx_params* params,
+                     int method, int sort_bits, int cull_keys, int threads, uint32_t* words, uint32_t* keys) {
+  if (cam->eyes < 1 || cam->eyes > 2) return -1;
+  if (method != ORC_METHOD_3DGUT && method != ORC_METHOD_HTGS && method != ORC_METHOD_RAYGS) return -1;
+  eye_setup eyes[2];
+  uint64_t n = 0;
+  object_setup* objs = setup_frame(objects, n_objects, cam, params, eyes, &n);
+  double eye_q[2][4];
+  for (int v = 0; v < cam->eyes; v++) decompose_quat(eyes[v].from_head, eye_q[v]);
+  double* tq = (double*)calloc((size_t)(n_objects > 0 ? n_objects : 1) * 5, sizeof(double));
+  for (int i = 0; i < n_objects; i++) {
+    if (objects[i].table->layout == RDX_LAYOUT_COV || !uniform_transform(objs[i].a, tq + i * 5, tq + i * 5 + 4)) {
+      free(tq);
+      free(objs);
+      return -2; /* the covariance form (fromCov) is not restated */
+    }
+  }
+#ifdef _OPENMP
+  int nt = threads > 0 ? threads : omp_get_max_threads();
+#pragma omp parallel for schedule(static, 4096) num_threads(nt)
+#endif
+  for (int64_t gi = 0; gi < (int64_t)n; gi++) {
+    int oi = 0;
+    while (oi + 1 < n_objects && (uint64_t)gi >= objs[oi + 1].offset) oi++;
+    orc_splat s;
+    orc_load_splat(objects[oi].table, (uint64_t)gi - objs[oi].offset, &s);
+    rays_one(&s, &objs[oi], eyes, (const double(*)[4])eye_q, cam->eyes, cam, method, tq + oi * 5, tq[oi * 5 + 4],
+             sort_bits, cull_keys, (uint64_t)gi, words, keys);
+  }
+  free(tq);
   free(objs);
   return 0;
 }

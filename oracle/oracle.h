@@ -82,6 +82,20 @@ int orc_project(const rdx_object* objects, int n_objects, const rdx_camera* came
                 const rdx_params* params, int sort_bits, int cull_keys, int threads,
                 const orc_outputs* out);
 
+/*
+ * The ray projection methods (projections.tsl.ts:170-474: rayProjection with
+ * gutBound or htgsBound, and raygs) in float64: words [n][H + E * W] (head
+ * words first, then each eye's; H, W = 6, 2 for 3dgut and htgs, 4, 3 for
+ * raygs) and keys [n] (either may be NULL). -2 when an object is a cov table or
+ * its object -> head matrix is not a rotation times a uniform scale (the
+ * reference converts those through fromCov, which is not restated).
+ */
+#define ORC_METHOD_3DGUT 1
+#define ORC_METHOD_HTGS 2
+#define ORC_METHOD_RAYGS 3
+int orc_project_rays(const rdx_object* objects, int n_objects, const rdx_camera* camera, const rdx_params* params,
+                     int method, int sort_bits, int cull_keys, int threads, uint32_t* words, uint32_t* keys);
+
 /* d(basis)/d(x, y, z) of the 24 basis functions above, as polynomials in x, y, z */
 void orc_sh_basis_grad(const double dir[3], double out[24][3]);
 

@@ -68,6 +68,8 @@ def lib():
             "orc_sh_evaluate": (None, [vp, vp, i, vp]),
             "orc_project": (i, [ctypes.POINTER(_abi.rdx_object), i, ctypes.POINTER(_abi.rdx_camera),
                                 ctypes.POINTER(_abi.rdx_params), i, i, i, ctypes.POINTER(orc_outputs)]),
+            "orc_project_rays": (i, [ctypes.POINTER(_abi.rdx_object), i, ctypes.POINTER(_abi.rdx_camera),
+                                     ctypes.POINTER(_abi.rdx_params), i, i, i, i, vp, vp]),
             "orc_encode_ext_table": (i, [ctypes.POINTER(_abi.rdx_table), vp, vp, vp]),
             "orc_sh_basis_grad": (None, [vp, vp]),
             "orc_ply_decode": (i, [vp, ctypes.c_uint64, i, vp, vp, vp, vp, vp, vp, vp, vp]),
@@ -203,6 +205,30 @@ def project(objects, camera, params=None, sort_bits=24, cull_keys=False, threads
     if st != 0:
         raise ValueError("orc_project failed")
     return out
+
+
+RAY_METHODS = {"3dgut": 1, "htgs": 2, "raygs": 3}
+RAY_WORDS = {"3dgut": (6, 2), "htgs": (6, 2), "raygs": (4, 3)}  # head words, words per eye
+
+
+def project_rays(objects, camera, method, params=None, sort_bits=24, cull_keys=False, threads=0):
+    """The float64 words and keys of a ray projection method ("3dgut", "htgs",
+    "raygs"): {"words": uint32 [n][H + E * W], "keys": uint32 [n]}."""
+    import radix_b200 as rb
+    params = params or rb.SplatParams()
+    n = sum(o.count for o in objects)
+    head, per_eye = RAY_WORDS[method]
+    words = np.zeros((n, head + len(camera.eyes) * per_eye), dtype=np.uint32)
+    keys = np.zeros(n, dtype=np.uint32)
+    objs, keep = rb._c_objects(objects)
+    cam = camera.to_c(_abi)
+    prm = params.to_c()
+    st = lib().orc_project_rays(objs, len(objects), ctypes.byref(cam), ctypes.byref(prm), RAY_METHODS[method],
+                                sort_bits, 1 if cull_keys else 0, threads, _p(words), _p(keys))
+    del keep
+    if st != 0:
+        raise ValueError("orc_project_rays failed (%d)" % st)
+    return {"words": words, "keys": keys}
 
 
 def encode_ext(raw):

@@ -500,6 +500,42 @@ def project_collection(objects, camera, params=None, sort_bits=24, pass_="full",
     return out
 
 
+PROJECTION_METHODS = {"ewa": _abi.RDX_METHOD_EWA, "3dgut": _abi.RDX_METHOD_3DGUT, "htgs": _abi.RDX_METHOD_HTGS,
+                      "raygs": _abi.RDX_METHOD_RAYGS}
+
+
+def method_words(method, eyes):
+    """Words per splat of a projection method ("ewa", "3dgut", "htgs",
+    "raygs") with 1 or 2 eyes: ProjectionDef.headWords + eyes * eyeWords."""
+    w = _abi.lib().rdx_method_words(PROJECTION_METHODS[method], eyes)
+    if w < 0:
+        raise ValueError(f"{method!r} with {eyes} eyes")
+    return w
+
+
+def project_words(objects, camera, method, params=None, sort_bits=24, cull_keys=True, ctx=None, out=None):
+    """projectCollection with any projection method: {'words': uint32
+    [n][method_words(method, E)] (head words, then each eye's), 'keys':
+    uint32 [n]} as CUDA tensors (or into `out`). The ray methods take CUDA
+    tables of the raw, ext or packed layout whose object-to-head transforms
+    are a rotation times a uniform scale."""
+    torch = _torch()
+    n = sum(o.count for o in objects)
+    if out is None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        out = {"words": torch.zeros((n, method_words(method, len(camera.eyes))), dtype=torch.int32, device=dev),
+               "keys": torch.zeros(n, dtype=torch.int32, device=dev)}
+    params = params or SplatParams()
+    objs, keep = _c_objects(objects)
+    cam = camera.to_c(_abi)
+    prm = params.to_c()
+    c = ctx or default_context(0)
+    c.call("rdx_project_words", objs, len(objects), ctypes.byref(cam), ctypes.byref(prm), PROJECTION_METHODS[method],
+           sort_bits, 1 if cull_keys else 0, ctypes.c_void_p(_ptr(out.get("words"))), ctypes.c_void_p(_ptr(out.get("keys"))))
+    del keep
+    return out
+
+
 def frame(objects, camera, params=None, sort_bits=24, outputs=DEFAULT_OUTPUTS, device="cuda", ctx=None,
           out=None, ordering=None, visible=None):
     """One frame: the projection (keys of splats culled in every eye invalid)

@@ -30,6 +30,10 @@ RDX_DTYPE_F32 = 0
 RDX_DTYPE_F16 = 1
 RDX_PASS_FULL = 0
 RDX_PASS_KEYS = 1
+RDX_METHOD_EWA = 0
+RDX_METHOD_3DGUT = 1
+RDX_METHOD_HTGS = 2
+RDX_METHOD_RAYGS = 3
 RDX_PHASE_PROJECT = 0
 RDX_PHASE_SORT = 1
 RDX_PHASE_COPY_IN = 2
@@ -227,6 +231,10 @@ SIGNATURES = {
     "rdx_frame": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_object), ctypes.c_int, ctypes.POINTER(rdx_camera),
                                  ctypes.POINTER(rdx_params), ctypes.c_int, ctypes.POINTER(rdx_outputs), ctypes.c_void_p,
                                  ctypes.c_void_p]),
+    "rdx_method_words": (ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    "rdx_project_words": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_object), ctypes.c_int,
+                                         ctypes.POINTER(rdx_camera), ctypes.POINTER(rdx_params), ctypes.c_int,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
     "rdx_project_backward": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(rdx_object), ctypes.c_int,
                                             ctypes.POINTER(rdx_camera), ctypes.POINTER(rdx_params),
                                             ctypes.POINTER(rdx_grads_in), ctypes.POINTER(rdx_table_grads)]),

@@ -22,7 +22,10 @@ CHECK_LIB = os.path.join(LIB_DIR, "libradix_b200_check.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "--expt-relaxed-constexpr"]
-SOURCES = ["sort.cu", "keys.cu", "project.cu", "backward.cu", "ply.cu", "spz.cu", "rdxfile.cu", "noalloc.cu", "abi.cpp"]
+SOURCES = ["sort.cu", "keys.cu", "project.cu", "rays.cu", "backward.cu", "ply.cu", "spz.cu", "rdxfile.cu", "noalloc.cu",
+           "abi.cpp"]
+# Per-file flags: the ray methods round every float64 step as the CPU oracle does
+EXTRA = {"rays.cu": ["--fmad=false"]}
 
 
 def _compile(src, verbose, check=False):
@@ -32,7 +35,7 @@ def _compile(src, verbose, check=False):
     deps.append(os.path.join(HERE, "..", "include", "radix_b200.h"))
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj, ""
-    cmd = [NVCC, *ARCH, *FLAGS, *(["-DRDX_CHECK"] if check else []), "-c", path, "-o", obj]
+    cmd = [NVCC, *ARCH, *FLAGS, *EXTRA.get(src, []), *(["-DRDX_CHECK"] if check else []), "-c", path, "-o", obj]
     if verbose and src.endswith(".cu"):
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -674,6 +674,75 @@ rdx::ProjDesc make_desc(const rdx_camera& cam, const Camera& c, const rdx_object
   return d;
 }
 
+// The unit quaternion of a rotation matrix (row-major), by the trace and the
+// largest diagonal element (Shoemake's method): the rotation three.js
+// Matrix4.decompose gives setTransform (src/render/splatTransform.tsl.ts:64-74)
+// and SplatCamera.setViews (src/render/splatCamera.ts:129-131)
+void rotation_quat(const double m[9], double q[4]) {
+  const double tr = m[0] + m[4] + m[8];
+  if (tr > 0.0) {
+    const double s = 0.5 / sqrt(tr + 1.0);
+    q[3] = 0.25 / s;
+    q[0] = (m[7] - m[5]) * s;
+    q[1] = (m[2] - m[6]) * s;
+    q[2] = (m[3] - m[1]) * s;
+  } else if (m[0] > m[4] && m[0] > m[8]) {
+    const double s = 2.0 * sqrt(1.0 + m[0] - m[4] - m[8]);
+    q[3] = (m[7] - m[5]) / s;
+    q[0] = 0.25 * s;
+    q[1] = (m[1] + m[3]) / s;
+    q[2] = (m[2] + m[6]) / s;
+  } else if (m[4] > m[8]) {
+    const double s = 2.0 * sqrt(1.0 + m[4] - m[0] - m[8]);
+    q[3] = (m[2] - m[6]) / s;
+    q[0] = (m[1] + m[3]) / s;
+    q[1] = 0.25 * s;
+    q[2] = (m[5] + m[7]) / s;
+  } else {
+    const double s = 2.0 * sqrt(1.0 + m[8] - m[0] - m[4]);
+    q[3] = (m[3] - m[1]) / s;
+    q[0] = (m[2] + m[6]) / s;
+    q[1] = (m[5] + m[7]) / s;
+    q[2] = 0.25 * s;
+  }
+}
+
+double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+
+double det3_cols(const double* c0, const double* c1, const double* c2) {
+  return c0[0] * (c1[1] * c2[2] - c1[2] * c2[1]) - c1[0] * (c0[1] * c2[2] - c0[2] * c2[1]) +
+         c2[0] * (c0[1] * c1[2] - c0[2] * c1[1]);
+}
+
+// Matrix4.decompose's rotation of a column-major 4x4: columns over their
+// lengths, the first negated when the determinant is negative
+void decompose_rotation(const double m[16], double q[4]) {
+  const double* c[3] = {m, m + 4, m + 8};
+  double len[3] = {sqrt(dot3(c[0], c[0])), sqrt(dot3(c[1], c[1])), sqrt(dot3(c[2], c[2]))};
+  if (det3_cols(c[0], c[1], c[2]) < 0.0) len[0] = -len[0];
+  double r[9];
+  for (int row = 0; row < 3; row++)
+    for (int col = 0; col < 3; col++) r[row * 3 + col] = c[col][row] / len[col];
+  rotation_quat(r, q);
+}
+
+// isUniformScale (src/render/splatTransform.tsl.ts:46-62): with G = M^T M and
+// s2 = trace(G) / 3, every entry of G - s2 I within 1e-6 s2 and det(M) > 0;
+// then the rotation and |det(M)|^(1/3) of setTransform (64-74)
+bool uniform_transform(const double a[16], double q[4], double* scale) {
+  const double* c[3] = {a, a + 4, a + 8};
+  const double s2 = (dot3(c[0], c[0]) + dot3(c[1], c[1]) + dot3(c[2], c[2])) / 3.0;
+  if (!(s2 > 0)) return false;
+  for (int i = 0; i < 3; i++)
+    for (int j = i; j < 3; j++)
+      if (fabs(dot3(c[i], c[j]) - (i == j ? s2 : 0.0)) > 1e-6 * s2) return false;
+  const double det = det3_cols(c[0], c[1], c[2]);
+  if (!(det > 0)) return false;
+  decompose_rotation(a, q);
+  *scale = cbrt(fabs(det));
+  return true;
+}
+
 // One launch per kind: layout, SH degree and colour type or SH codec (also a tuning key)
 int table_kind_of(const rdx_table& t) {
   return t.layout * 100 + t.sh_degree * 10 + (t.layout == RDX_LAYOUT_RAW ? t.color_dtype : t.sh_codec);
@@ -1672,6 +1741,100 @@ int rdx_project_backward(rdx_ctx* ctx, const rdx_object* objects, int n_objects,
     RDX_CUDA(rdx::launch_project_backward(descs + start, gdev + start, call.descs.data() + start, count,
                                           call.group_tiles[g], in, ctx->stream),
              "backward launch");
+    if (call.group_tiles[g]) ctx->launches += 1;
+  }
+  return RDX_OK;
+}
+
+int rdx_method_words(int method, int eyes) {
+  if (eyes < 1 || eyes > 2) return -1;
+  switch (method) {
+    case RDX_METHOD_EWA: return 4 * eyes;
+    case RDX_METHOD_3DGUT:
+    case RDX_METHOD_HTGS: return 6 + 2 * eyes;
+    case RDX_METHOD_RAYGS: return 4 + 3 * eyes;
+    default: return -1;
+  }
+}
+
+int rdx_project_words(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
+                      const rdx_params* params, int method, int sort_bits, int cull_keys, uint32_t* words,
+                      uint32_t* keys) {
+  if (!ctx) return RDX_ERR_ARG;
+  if (method == RDX_METHOD_EWA) {
+    rdx_outputs out{};
+    out.words = words;
+    out.keys = keys;
+    return rdx_project(ctx, objects, n_objects, camera, params, sort_bits, RDX_PASS_FULL, cull_keys, &out);
+  }
+  if (method < RDX_METHOD_3DGUT || method > RDX_METHOD_RAYGS)
+    return fail(ctx, RDX_ERR_ARG, "projection method %d (ewa 0, 3dgut 1, htgs 2, raygs 3)", method);
+  const ViewRef view{objects, n_objects, camera};
+  uint64_t n = 0;
+  int s = check_views(ctx, &view, 1, sort_bits, RDX_PASS_FULL, &n);
+  if (s != RDX_OK) return s;
+  std::vector<rdx::RayDesc> per_object((size_t)std::max(n_objects, 1));
+  for (int i = 0; i < n_objects; i++) {
+    const rdx_table& t = *objects[i].table;
+    if (t.layout == RDX_LAYOUT_COV)
+      return fail(ctx, RDX_ERR_UNSUPPORTED, "object %d: the ray methods read scales and rotations, not covariances", i);
+    if (!all_device(t)) return fail(ctx, RDX_ERR_ARG, "the ray methods take device memory only (object %d's table)", i);
+    double a[16];
+    mat4_mul(camera->head, objects[i].world, a);
+    if (!uniform_transform(a, per_object[i].tq, &per_object[i].tscale))
+      return fail(ctx, RDX_ERR_UNSUPPORTED,
+                  "object %d: the ray methods take object-to-head transforms that are a rotation times a uniform scale", i);
+  }
+  if ((words && !is_device_ptr(words)) || (keys && !is_device_ptr(keys)))
+    return fail(ctx, RDX_ERR_ARG, "the ray methods write device memory only");
+  if (n == 0) return RDX_OK;
+  for (int v = 0; v < camera->eyes; v++) {
+    double fh[16];
+    if (std::equal(camera->eye[v].view, camera->eye[v].view + 16, camera->head)) {
+      memset(fh, 0, sizeof(fh));
+      fh[0] = fh[5] = fh[10] = fh[15] = 1.0;
+    } else {
+      double head_world[16];
+      mat4_invert(camera->head, head_world);
+      mat4_mul(camera->eye[v].view, head_world, fh);
+    }
+    double q[4];
+    decompose_rotation(fh, q);
+    for (int i = 0; i < n_objects; i++) memcpy(per_object[i].eye_q[v], q, sizeof(q));
+  }
+  rdx_params defaults;
+  rdx_params_default(&defaults);
+  cudaSetDevice(ctx->device);
+  ProjectCall call;
+  rdx::ProjDesc* descs = nullptr;
+  rdx::RayDesc* rays = nullptr;
+  int status = RDX_OK;
+  auto layout = [&](Arena& a) {
+    call = ProjectCall();
+    status = plan_views(ctx, a, &view, 1, params ? params : &defaults, sort_bits, RDX_PASS_FULL, cull_keys, call);
+    descs = a.take<rdx::ProjDesc>(call.descs.size());
+    rays = a.take<rdx::RayDesc>(call.descs.size());
+  };
+  Arena dry(nullptr);
+  layout(dry);
+  if (status != RDX_OK) return status;
+  s = ensure_arena(ctx, dry.used);
+  if (s != RDX_OK) return s;
+  Arena a(ctx->arena);
+  layout(a);
+  if (status != RDX_OK) return status;
+  std::vector<rdx::RayDesc> rh;
+  for (const rdx::ProjDesc& d : call.descs) rh.push_back(per_object[d.object]);
+  s = upload(ctx, descs, call.descs.data(), call.descs.size() * sizeof(rdx::ProjDesc));
+  if (s == RDX_OK) s = upload(ctx, rays, rh.data(), rh.size() * sizeof(rdx::RayDesc));
+  if (s != RDX_OK) return s;
+  Phase project(ctx, RDX_PHASE_PROJECT);
+  for (size_t g = 0; g + 1 < call.groups.size(); g++) {
+    const int start = call.groups[g];
+    const int count = call.groups[g + 1] - start;
+    RDX_CUDA(rdx::launch_project_rays(descs + start, rays + start, call.descs.data() + start, count,
+                                      call.group_tiles[g], method, words, keys, ctx->stream),
+             "ray projection launch");
     if (call.group_tiles[g]) ctx->launches += 1;
   }
   return RDX_OK;

@@ -1,0 +1,99 @@
+"""The float64 oracle of the ray projection methods (3dgut, htgs, raygs;
+src/render/projections.tsl.ts:170-474), checked on the CPU against what the
+reference's own checks hold of them and against the ewa oracle: head words
+decode to the head-space centre, the 3dgut and htgs bounds of small on-screen
+splats cover the ewa bound as closely as the reference's EWA check allows
+(test/gpu/renderTests.ts:242-277 holds its EWA to 1 % / 2 % of a CPU EWA), keys
+follow the drawn eyes, and transforms the reference routes through fromCov are
+refused."""
+import numpy as np
+import pytest
+
+import radix_b200 as rb
+from oracle import oracle as orc
+from radix_b200 import synthetic as syn
+from tests import ray_words as rw
+
+METHODS = ("3dgut", "htgs", "raygs")
+
+
+@pytest.fixture(scope="module")
+def scene():
+    d = syn.mixture_table(20_000, seed=3, sh_degree=3)
+    cam = syn.scale_camera()
+    objs = [rb.SplatObject(rb.Table.from_dict(d))]
+    head = cam.head.reshape(4, 4).T
+    c = np.asarray(d["centers"], dtype=np.float64)
+    return d, cam, objs, (head[:3, :3] @ c.T).T + head[:3, 3]
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_head_words_decode_to_the_head_centre(scene, method):
+    """decodeCenter of the head words: a 20 + 20-bit direction and a float32 distance."""
+    _, cam, objs, centre = scene
+    w = orc.project_rays(objs, cam, method, None, 32, True)["words"]
+    ok = w[:, 1] != 0
+    assert ok.sum() > 1000
+    err = np.linalg.norm(rw.decode_center(w[ok], method) - centre[ok], axis=1) / np.linalg.norm(centre[ok], axis=1)
+    assert err.max() < 1e-5, err.max()
+
+
+@pytest.mark.parametrize("method", ["3dgut", "htgs"])
+def test_bounds_cover_the_ewa_bound(scene, method):
+    """Small splats well inside the screen: the outward-rounded bound's half
+    extents are at least the ewa ones and within a few per cent of them."""
+    _, cam, objs, _ = scene
+    ewa = orc.project(objs, cam, None, 32, True)
+    w = orc.project_rays(objs, cam, method, None, 32, True)["words"]
+    vis = rw.drawn(w, method, 0) & ewa["visible"][0].astype(bool)
+    ew = rw.eye_words(w, method, 0)
+    ndc, _, scales = rw.decode_bound(ew[vis, 0], ew[vis, 1])
+    radii = ewa["radii"][0][vis]
+    centre_ndc = ewa["mean2d"][0][vis] / np.array([cam.width, cam.height]) * 2 - 1
+    sel = (radii[:, 0] > 2) & (radii[:, 0] < 30) & np.all(np.abs(centre_ndc) < 0.9, axis=1)
+    assert sel.sum() > 500
+    major = scales[sel, 0] / radii[sel, 0]
+    minor = scales[sel, 1] / radii[sel, 1]
+    assert major.min() >= 1.0 and minor.min() >= 1.0, (major.min(), minor.min())
+    assert np.median(major) < 1.02 and np.median(minor) < 1.04, (np.median(major), np.median(minor))
+    assert np.percentile(major, 99) < 1.1 and np.percentile(minor, 99) < 1.15
+    # 3dgut centres its bound on the mean of the sigma points; htgs on the outline's centre
+    shift = np.abs(ndc[sel] - centre_ndc[sel]).max(1) * cam.width / 2
+    assert np.percentile(shift, 99) < (0.2 if method == "3dgut" else 1.0), np.percentile(shift, 99)
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_keys_follow_the_drawn_eyes(scene, method):
+    _, cam, objs, _ = scene
+    invalid = orc.lib().orc_invalid_key(32)
+    r = orc.project_rays(objs, cam, method, None, 32, True)
+    assert np.array_equal(r["keys"] != invalid, rw.drawn(r["words"], method, 0))
+    # without cull_keys a key is the splat's as in every method (SplatProjection.ts:150-151)
+    r = orc.project_rays(objs, cam, method, None, 32, False)
+    assert np.array_equal(r["keys"], orc.project(objs, cam, None, 32, False)["keys"])
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_stereo_rows_and_culled_eyes(scene, method):
+    d, _, objs, _ = scene
+    cam = syn.stereo_camera()
+    w = orc.project_rays(objs, cam, method, None, 24, True)["words"]
+    h, e = rw.LAYOUT[method]
+    assert w.shape == (20_000, h + 2 * e)
+    either = rw.drawn(w, method, 0) | rw.drawn(w, method, 1)
+    assert either.sum() > 0
+    # a splat that no eye draws has zero eye words; its head words are written
+    # only when the head basis keeps it
+    assert not w[~either, h:].any()
+
+
+def test_transforms_through_from_cov_are_refused(scene):
+    d, cam, _, _ = scene
+    world = np.diag([1.0, 2.0, 1.0, 1.0]).reshape(16)
+    with pytest.raises(ValueError):
+        orc.project_rays([rb.SplatObject(rb.Table.from_dict(d), world=world)], cam, "3dgut")
+    # a rotation times a uniform scale is taken
+    c, s = np.cos(0.4), np.sin(0.4)
+    world = np.array([[2 * c, -2 * s, 0, 0.1], [2 * s, 2 * c, 0, 0], [0, 0, 2, -0.5], [0, 0, 0, 1]]).T.reshape(16)
+    r = orc.project_rays([rb.SplatObject(rb.Table.from_dict(d), world=world)], cam, "raygs")
+    assert rw.drawn(r["words"], "raygs", 0).sum() > 0
