@@ -894,7 +894,8 @@ def run_rays(args, world, rank, local, device):
         "config": {"workload": f"rays: {n} splats SH {SH_DEGREE} fp32, 1920x1080 fov 50, {BITS}-bit keys; "
                                "each method timed alone (inputs larger than L2)", "methods": results},
         "roofline": {"bound": "hbm", "achieved": head["gb_s"], "peak": peak, "unit": "GB/s", "frac": head["frac"],
-                     "traffic": None, "kernel": "k_project_rays", "peak_kind": peak_kind},
+                     "traffic": ncu_traffic("project_rays_kernel_1m_sh3.md", n / 1_000_000), "kernel": "k_project_rays",
+                     "peak_kind": peak_kind},
         "clocks": clk, "e2e": None, "e2e_note": "device-resident inputs",
         "gpu_launches": ctx.launches() - launches0,
     }
