@@ -392,10 +392,11 @@ int rdx_method_words(int method, int eyes);
  *   keys   uint32 [n], as rdx_project's (cull_keys: keys of splats that no
  *          eye shows are invalid).
  * Either output may be NULL. ewa forwards to rdx_project (its words output).
- * The ray methods take device memory only, raw / ext / packed tables, and
- * object-to-head transforms that are a rotation times a uniform scale:
- * RDX_ERR_UNSUPPORTED for a cov table or another transform (the reference
- * converts those through fromCov, not built here).
+ * The ray methods take device memory only. Objects whose object-to-head
+ * transform is a rotation times a uniform scale use transformUniform
+ * (splatTransform.tsl.ts:143-152); other transforms and cov tables reach the
+ * splat form through the covariance and fromCov (src/gpu/splats.tsl.ts:
+ * 189-199), as the reference's transformSplat and transformForm do.
  */
 int rdx_project_words(rdx_ctx* ctx, const rdx_object* objects, int n_objects, const rdx_camera* camera,
                       const rdx_params* params, int method, int sort_bits, int cull_keys, uint32_t* words,

@@ -1074,6 +1074,87 @@ static void scale_quat_cols(const double s[3], const double q[4], double col[3][
   col[2][2] = s[2] * (1.0 - 2.0 * (x * x + y * y));
 }
 
+/* symEigens (math.tsl.ts:46-112): Jacobi rotations on the symmetric matrix
+   (xx, yy, zz | xy, xz, yz), at most 16, stopping once every off-diagonal
+   element is within 1e-6 of the diagonal's absolute sum; eigenvalues
+   descending, eigenvectors right-handed. A[c][r] and V[c][r] are column c,
+   row r, as the reference indexes them. */
+static void sym_eigens(const double d[3], const double o[3], double values[3], double vec[3][3]) {
+  const double eps = 1e-6 * (fabs(d[0]) + fabs(d[1]) + fabs(d[2]));
+  double A[3][3] = {{d[0], o[0], o[1]}, {o[0], d[1], o[2]}, {o[1], o[2], d[2]}};
+  double V[3][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+  for (int it = 0; it < 16; it++) {
+    int p = 0, q = 1;
+    double mx = fabs(A[0][1]);
+    if (fabs(A[0][2]) > mx) {
+      mx = fabs(A[0][2]);
+      q = 2;
+    }
+    if (fabs(A[1][2]) > mx) {
+      mx = fabs(A[1][2]);
+      p = 1;
+      q = 2;
+    }
+    if (mx <= eps) break;
+    const double phi = atan2(A[p][q] * 2.0, A[q][q] - A[p][p]) * 0.5;
+    const double c = cos(phi), sn = sin(phi);
+    for (int r = 0; r < 3; r++) {
+      const double x = A[r][p], y = A[r][q];
+      A[r][p] = c * x - sn * y;
+      A[r][q] = sn * x + c * y;
+    }
+    for (int r = 0; r < 3; r++) {
+      const double x = A[p][r], y = A[q][r];
+      A[p][r] = c * x - sn * y;
+      A[q][r] = sn * x + c * y;
+    }
+    A[p][q] = 0.0;
+    A[q][p] = 0.0;
+    for (int r = 0; r < 3; r++) {
+      const double x = V[r][p], y = V[r][q];
+      V[r][p] = c * x - sn * y;
+      V[r][q] = sn * x + c * y;
+    }
+  }
+  double l[3] = {A[0][0], A[1][1], A[2][2]};
+  double v[3][3];
+  for (int i = 0; i < 3; i++) {
+    const double w[3] = {V[0][i], V[1][i], V[2][i]};
+    const double len = sqrt(dot3(w, w));
+    for (int k = 0; k < 3; k++) v[i][k] = w[k] / len;
+  }
+  const int pairs[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+  for (int k = 0; k < 3; k++) {
+    const int i = pairs[k][0], j = pairs[k][1];
+    if (l[i] < l[j]) {
+      const double t = l[i];
+      l[i] = l[j];
+      l[j] = t;
+      double w[3];
+      memcpy(w, v[i], sizeof(w));
+      memcpy(v[i], v[j], sizeof(w));
+      memcpy(v[j], w, sizeof(w));
+    }
+  }
+  const double cr[3] = {v[0][1] * v[1][2] - v[0][2] * v[1][1], v[0][2] * v[1][0] - v[0][0] * v[1][2],
+                        v[0][0] * v[1][1] - v[0][1] * v[1][0]};
+  if (dot3(cr, v[2]) < 0.0)
+    for (int k = 0; k < 3; k++) v[2][k] = -v[2][k];
+  memcpy(values, l, sizeof(l));
+  memcpy(vec, v, sizeof(v));
+}
+
+/* The splat form of a head-space covariance (row-major): fromCov
+   (src/gpu/splats.tsl.ts:189-199), scales sqrt(max(eigenvalue, 0)) and the
+   rotation of the eigenvector basis */
+static void from_cov(const double cov[9], double scales[3], double q[4]) {
+  const double d[3] = {cov[0], cov[4], cov[8]}, o[3] = {cov[3], cov[6], cov[7]};
+  double values[3], v[3][3];
+  sym_eigens(d, o, values, v);
+  for (int k = 0; k < 3; k++) scales[k] = sqrt(fmax(values[k], 0.0));
+  basis_to_quat(v[0], v[1], v[2], q);
+}
+
 /* P (column-major) times (v, 0) */
 static void proj_dir(const double p[16], const double v[3], double out[4]) {
   for (int row = 0; row < 4; row++) {
@@ -1366,19 +1447,40 @@ static int raygs_frame(const double ce[3], const eye_setup* e, const double q[4]
    (SplatProjection.project/write, SplatProjection.ts:126-153; rayProjection
    and raygs, projections.tsl.ts:266-333, 399-467) */
 static void rays_one(const orc_splat* s, const object_setup* o, const eye_setup* eyes, const double eye_q[2][4],
-                     int n_eyes, const rdx_camera* cam, int method, const double tq[4], double tscale, int sort_bits,
-                     int cull_keys, uint64_t gi, uint32_t* words, uint32_t* keys) {
+                     int n_eyes, const rdx_camera* cam, int method, const double tq[4], double tscale, int uniform,
+                     int sort_bits, int cull_keys, uint64_t gi, uint32_t* words, uint32_t* keys) {
   const rdx_params* p = &o->params;
   const int head_words = method == ORC_METHOD_RAYGS ? 4 : 6, eye_words = method == ORC_METHOD_RAYGS ? 3 : 2;
   uint32_t* row = words ? words + gi * (uint64_t)(head_words + n_eyes * eye_words) : NULL;
   double rgb[3];
   splat_rgb(s, o, rgb);
-  /* transformUniform (splatTransform.tsl.ts:143-152) */
-  double ch[3], qn[4], qh[4];
+  double ch[3], qn[4], qh[4], sc[3];
   xform_point(o->a, s->center, ch);
   quat_normalize(s->quat, qn);
-  quat_mul(tq, qn, qh);
-  double sc[3] = {s->scales[0] * tscale, s->scales[1] * tscale, s->scales[2] * tscale};
+  if (uniform && !s->has_cov) { /* transformUniform (splatTransform.tsl.ts:143-152) */
+    quat_mul(tq, qn, qh);
+    for (int k = 0; k < 3; k++) sc[k] = s->scales[k] * tscale;
+  } else {
+    /* transformSplat's other branch (toCov, transformCov, fromCov: splatTransform.tsl.ts:117-162,
+       splats.tsl.ts:176-199), or a cov table's transformCov and fromCov (transformForm, convertForm) */
+    double cov[9];
+    if (s->has_cov) {
+      const double c6[9] = {s->cov[0], s->cov[3], s->cov[4], s->cov[3], s->cov[1], s->cov[5], s->cov[4], s->cov[5], s->cov[2]};
+      memcpy(cov, c6, sizeof(cov));
+    } else {
+      double col[3][3], M[9], Mt[9];
+      scale_quat_cols(s->scales, qn, col);
+      for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) M[r * 3 + c] = col[c][r];
+      m3_transpose(M, Mt);
+      m3_mul(M, Mt, cov);
+    }
+    double a3t[9], tmp[9], covh[9];
+    m3_transpose(o->a3, a3t);
+    m3_mul(o->a3, cov, tmp);
+    m3_mul(tmp, a3t, covh);
+    from_cov(covh, sc, qh);
+  }
   /* prepareSplat, splat form (projection.tsl.ts:42-64) */
   double opacity = s->opacity, inflate = 1.0;
   if (opacity > 1.0) {
@@ -1504,14 +1606,8 @@ int orc_project_rays(const rdx_object* objects, int n_objects, const rdx_camera*
   object_setup* objs = setup_frame(objects, n_objects, cam, params, eyes, &n);
   double eye_q[2][4];
   for (int v = 0; v < cam->eyes; v++) decompose_quat(eyes[v].from_head, eye_q[v]);
-  double* tq = (double*)calloc((size_t)(n_objects > 0 ? n_objects : 1) * 5, sizeof(double));
-  for (int i = 0; i < n_objects; i++) {
-    if (objects[i].table->layout == RDX_LAYOUT_COV || !uniform_transform(objs[i].a, tq + i * 5, tq + i * 5 + 4)) {
-      free(tq);
-      free(objs);
-      return -2; /* the covariance form (fromCov) is not restated */
-    }
-  }
+  double* tq = (double*)calloc((size_t)(n_objects > 0 ? n_objects : 1) * 6, sizeof(double));
+  for (int i = 0; i < n_objects; i++) tq[i * 6 + 5] = uniform_transform(objs[i].a, tq + i * 6, tq + i * 6 + 4);
 #ifdef _OPENMP
   int nt = threads > 0 ? threads : omp_get_max_threads();
 #pragma omp parallel for schedule(static, 4096) num_threads(nt)
@@ -1521,8 +1617,8 @@ int orc_project_rays(const rdx_object* objects, int n_objects, const rdx_camera*
     while (oi + 1 < n_objects && (uint64_t)gi >= objs[oi + 1].offset) oi++;
     orc_splat s;
     orc_load_splat(objects[oi].table, (uint64_t)gi - objs[oi].offset, &s);
-    rays_one(&s, &objs[oi], eyes, (const double(*)[4])eye_q, cam->eyes, cam, method, tq + oi * 5, tq[oi * 5 + 4],
-             sort_bits, cull_keys, (uint64_t)gi, words, keys);
+    rays_one(&s, &objs[oi], eyes, (const double(*)[4])eye_q, cam->eyes, cam, method, tq + oi * 6, tq[oi * 6 + 4],
+             (int)tq[oi * 6 + 5], sort_bits, cull_keys, (uint64_t)gi, words, keys);
   }
   free(tq);
   free(objs);

@@ -86,9 +86,10 @@ int orc_project(const rdx_object* objects, int n_objects, const rdx_camera* came
  * The ray projection methods (projections.tsl.ts:170-474: rayProjection with
  * gutBound or htgsBound, and raygs) in float64: words [n][H + E * W] (head
  * words first, then each eye's; H, W = 6, 2 for 3dgut and htgs, 4, 3 for
- * raygs) and keys [n] (either may be NULL). -2 when an object is a cov table or
- * its object -> head matrix is not a rotation times a uniform scale (the
- * reference converts those through fromCov, which is not restated).
+ * raygs) and keys [n] (either may be NULL). Cov tables, and objects whose
+ * object -> head matrix is not a rotation times a uniform scale, reach the
+ * splat form through fromCov (the eigen decomposition of the head-space
+ * covariance, src/gpu/splats.tsl.ts:189-199).
  */
 #define ORC_METHOD_3DGUT 1
 #define ORC_METHOD_HTGS 2

@@ -1775,15 +1775,12 @@ int rdx_project_words(rdx_ctx* ctx, const rdx_object* objects, int n_objects, co
   if (s != RDX_OK) return s;
   std::vector<rdx::RayDesc> per_object((size_t)std::max(n_objects, 1));
   for (int i = 0; i < n_objects; i++) {
-    const rdx_table& t = *objects[i].table;
-    if (t.layout == RDX_LAYOUT_COV)
-      return fail(ctx, RDX_ERR_UNSUPPORTED, "object %d: the ray methods read scales and rotations, not covariances", i);
-    if (!all_device(t)) return fail(ctx, RDX_ERR_ARG, "the ray methods take device memory only (object %d's table)", i);
+    if (!all_device(*objects[i].table))
+      return fail(ctx, RDX_ERR_ARG, "the ray methods take device memory only (object %d's table)", i);
     double a[16];
     mat4_mul(camera->head, objects[i].world, a);
-    if (!uniform_transform(a, per_object[i].tq, &per_object[i].tscale))
-      return fail(ctx, RDX_ERR_UNSUPPORTED,
-                  "object %d: the ray methods take object-to-head transforms that are a rotation times a uniform scale", i);
+    // other transforms, and cov tables, reach the splat form through the covariance (fromCov)
+    per_object[i].uniform = uniform_transform(a, per_object[i].tq, &per_object[i].tscale) ? 1 : 0;
   }
   if ((words && !is_device_ptr(words)) || (keys && !is_device_ptr(keys)))
     return fail(ctx, RDX_ERR_ARG, "the ray methods write device memory only");

@@ -113,6 +113,90 @@ __device__ __forceinline__ void scale_quat_cols(const double s[3], const double 
   col[2][2] = s[2] * (1.0 - 2.0 * (x * x + y * y));
 }
 
+// symEigens (src/gpu/math.tsl.ts:46-112): Jacobi rotations on the symmetric
+// matrix (xx, yy, zz | xy, xz, yz), at most 16, stopping once every
+// off-diagonal element is within 1e-6 of the diagonal's absolute sum;
+// eigenvalues descending, eigenvectors (vec[i]) right-handed. A[c][r] and
+// V[c][r] are column c, row r, as the reference indexes them.
+__device__ void sym_eigens(const double d[3], const double o[3], double values[3], double vec[3][3]) {
+  const double eps = 1e-6 * (fabs(d[0]) + fabs(d[1]) + fabs(d[2]));
+  double A[3][3] = {{d[0], o[0], o[1]}, {o[0], d[1], o[2]}, {o[1], o[2], d[2]}};
+  double V[3][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+  for (int it = 0; it < 16; it++) {
+    int p = 0, q = 1;
+    double mx = fabs(A[0][1]);
+    if (fabs(A[0][2]) > mx) {
+      mx = fabs(A[0][2]);
+      q = 2;
+    }
+    if (fabs(A[1][2]) > mx) {
+      mx = fabs(A[1][2]);
+      p = 1;
+      q = 2;
+    }
+    if (mx <= eps) break;
+    const double phi = atan2(A[p][q] * 2.0, A[q][q] - A[p][p]) * 0.5;
+    const double c = cos(phi), sn = sin(phi);
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      const double x = A[r][p], y = A[r][q];
+      A[r][p] = c * x - sn * y;
+      A[r][q] = sn * x + c * y;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      const double x = A[p][r], y = A[q][r];
+      A[p][r] = c * x - sn * y;
+      A[q][r] = sn * x + c * y;
+    }
+    A[p][q] = 0.0;
+    A[q][p] = 0.0;
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      const double x = V[r][p], y = V[r][q];
+      V[r][p] = c * x - sn * y;
+      V[r][q] = sn * x + c * y;
+    }
+  }
+  double l[3] = {A[0][0], A[1][1], A[2][2]};
+  double v[3][3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const double w[3] = {V[0][i], V[1][i], V[2][i]};
+    const double len = sqrt(dot3(w, w));
+#pragma unroll
+    for (int k = 0; k < 3; k++) v[i][k] = w[k] / len;
+  }
+  const int pairs[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const int i = pairs[k][0], j = pairs[k][1];
+    if (l[i] < l[j]) {
+      const double t = l[i];
+      l[i] = l[j];
+      l[j] = t;
+#pragma unroll
+      for (int m = 0; m < 3; m++) {
+        const double w = v[i][m];
+        v[i][m] = v[j][m];
+        v[j][m] = w;
+      }
+    }
+  }
+  const double cr[3] = {v[0][1] * v[1][2] - v[0][2] * v[1][1], v[0][2] * v[1][0] - v[0][0] * v[1][2],
+                        v[0][0] * v[1][1] - v[0][1] * v[1][0]};
+  if (dot3(cr, v[2]) < 0.0) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) v[2][k] = -v[2][k];
+  }
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    values[k] = l[k];
+#pragma unroll
+    for (int m = 0; m < 3; m++) vec[k][m] = v[k][m];
+  }
+}
+
 // P (column-major) times (c, 1), and times (v, 0)
 __device__ __forceinline__ void clip_of(const double* P, const double c[3], double clip[4]) {
 #pragma unroll
@@ -122,6 +206,40 @@ __device__ __forceinline__ void clip_of(const double* P, const double c[3], doub
 __device__ __forceinline__ void proj_dir(const double* P, const double v[3], double out[4]) {
 #pragma unroll
   for (int r = 0; r < 4; r++) out[r] = P[r] * v[0] + P[4 + r] * v[1] + P[8 + r] * v[2];
+}
+
+// The head-space splat form of an object-space covariance (row-major) seen
+// through the object's 3x3 `a` (rows of 4): transformCov then fromCov
+// (src/render/splatTransform.tsl.ts:117-140, src/gpu/splats.tsl.ts:189-199),
+// the products in the oracle's order. Out of line: objects that take it are
+// rare, and inlined its registers would weigh on every launch.
+struct Cov3 {  // a symmetric 3x3, row-major
+  double m[9];
+};
+struct SplatBasis {  // scales and rotation
+  double s[3];
+  double q[4];
+};
+
+__device__ __noinline__ SplatBasis cov_to_splat(const double* a, const Cov3 c) {
+  const double* cov = c.m;
+  double tmp[9], covh[9];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) tmp[i * 3 + j] = a[i * 4 + 0] * cov[0 * 3 + j] + a[i * 4 + 1] * cov[1 * 3 + j] + a[i * 4 + 2] * cov[2 * 3 + j];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) covh[i * 3 + j] = tmp[i * 3 + 0] * a[j * 4 + 0] + tmp[i * 3 + 1] * a[j * 4 + 1] + tmp[i * 3 + 2] * a[j * 4 + 2];
+  const double d[3] = {covh[0], covh[4], covh[8]}, o[3] = {covh[3], covh[6], covh[7]};
+  double values[3], v[3][3];
+  sym_eigens(d, o, values, v);
+  SplatBasis out;
+#pragma unroll
+  for (int k = 0; k < 3; k++) out.s[k] = sqrt(fmax(values[k], 0.0));
+  basis_to_quat(v[0], v[1], v[2], out.q);
+  return out;
 }
 
 struct Bound {  // projection.tsl.ts:206-210: ndc centre, angle, pixel half extents
@@ -489,15 +607,42 @@ __device__ __forceinline__ void ray_one(const ProjDesc& sd, const RayDesc& rd, u
   double q[4];
   load_quat<LAYOUT>(sd.table, i, q);
   const double cx = cf[0], cy = cf[1], cz = cf[2];
-  // transformUniform (splatTransform.tsl.ts:143-152)
   const double ch[3] = {affine_row(sd.a + 0, cx, cy, cz), affine_row(sd.a + 4, cx, cy, cz),
                         affine_row(sd.a + 8, cx, cy, cz)};
-  double qn[4], qh[4];
+  double qn[4], qh[4], sc[3];
   quat_normalize(q, qn);
-  quat_mul(rd.tq, qn, qh);
-  double sc[3];
+  if (LAYOUT != RDX_LAYOUT_COV && rd.uniform) {  // transformUniform (splatTransform.tsl.ts:143-152)
+    quat_mul(rd.tq, qn, qh);
 #pragma unroll
-  for (int k = 0; k < 3; k++) sc[k] = exp(ls[k]) * rd.tscale;
+    for (int k = 0; k < 3; k++) sc[k] = exp(ls[k]) * rd.tscale;
+  } else {
+    // transformSplat's other branch (toCov, transformCov, fromCov), or a cov
+    // table's transformCov and fromCov (transformForm / convertForm,
+    // splatTransform.tsl.ts:154-181)
+    Cov3 c3;
+    double* cov = c3.m;
+    if constexpr (LAYOUT == RDX_LAYOUT_COV) {
+      double c6[6];
+      load_cov(sd.table, i, c6);
+      cov[0] = c6[0], cov[1] = c6[3], cov[2] = c6[4];
+      cov[3] = c6[3], cov[4] = c6[1], cov[5] = c6[5];
+      cov[6] = c6[4], cov[7] = c6[5], cov[8] = c6[2];
+    } else {
+      // covFromScaleQuat (math.tsl.ts:171-175): M M^T, M = R(q) diag(s)
+      const double s0[3] = {exp(ls[0]), exp(ls[1]), exp(ls[2])};
+      double col[3][3];
+      scale_quat_cols(s0, qn, col);
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) cov[r * 3 + c] = col[0][r] * col[0][c] + col[1][r] * col[1][c] + col[2][r] * col[2][c];
+    }
+    const SplatBasis b = cov_to_splat(sd.a, c3);
+#pragma unroll
+    for (int k = 0; k < 3; k++) sc[k] = b.s[k];
+#pragma unroll
+    for (int k = 0; k < 4; k++) qh[k] = b.q[k];
+  }
   // prepareSplat, splat form (projection.tsl.ts:42-64), and cullInvisible (66-69)
   double opacity = opac, inflate = 1.0;
   if (opacity > 1.0) {
@@ -680,8 +825,6 @@ RayKernel ray_codec(int degree, int codec, int method) {
 
 }  // namespace
 
-bool ray_table_supported(const DevTable& t) { return t.layout != RDX_LAYOUT_COV; }
-
 cudaError_t launch_project_rays(const ProjDesc* descs_dev, const RayDesc* rays_dev, const ProjDesc* descs_host,
                                 int n_desc, uint32_t total_tiles, int method, uint32_t* words, uint32_t* keys,
                                 cudaStream_t stream) {
@@ -691,11 +834,12 @@ cudaError_t launch_project_rays(const ProjDesc* descs_dev, const RayDesc* rays_d
   switch (t.layout) {
     case RDX_LAYOUT_EXT: k = ray_codec<RDX_LAYOUT_EXT>(t.sh_degree, t.sh_codec, method); break;
     case RDX_LAYOUT_PACKED: k = ray_codec<RDX_LAYOUT_PACKED>(t.sh_degree, t.sh_codec, method); break;
+    case RDX_LAYOUT_COV: k = ray_codec<RDX_LAYOUT_COV>(t.sh_degree, t.sh_codec, method); break;
     case RDX_LAYOUT_RAW:
       k = t.color_dtype == RDX_DTYPE_F16 ? ray_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F16>(t.sh_degree, method)
                                          : ray_degree<RDX_LAYOUT_RAW, RDX_DTYPE_F32>(t.sh_degree, method);
       break;
-    default: return cudaErrorInvalidValue;  // the cov layout: the splat form needs fromCov
+    default: return cudaErrorInvalidValue;
   }
   const uint32_t grid = (total_tiles + kRayWarps - 1) / kRayWarps;
   k<<<grid, kRayWarps * 32, 0, stream>>>(descs_dev, rays_dev, n_desc, total_tiles, words, keys);

@@ -410,21 +410,23 @@ bool project_host_rows_supported(const DevTable& t);
 
 constexpr int kMethodEwa = 0, kMethod3dgut = 1, kMethodHtgs = 2, kMethodRaygs = 3;
 
-// What a ray method reads beside an object's ProjDesc: the object -> head
-// transform as a rotation and a uniform scale (setTransform,
-// src/render/splatTransform.tsl.ts:64-74), and each eye's rotation from the
+// What a ray method reads beside an object's ProjDesc: whether the object ->
+// head transform is a rotation times a uniform scale, and then that rotation
+// and scale (setTransform, src/render/splatTransform.tsl.ts:64-74; other
+// transforms go through the covariance), and each eye's rotation from the
 // head (SplatCamera.setViews, src/render/splatCamera.ts:129-131)
 struct RayDesc {
   double tq[4];
   double tscale;
   double eye_q[2][4];
+  int uniform;
+  int reserved;
 };
 
-// rays_dev[k] belongs to descs_dev[k]; one launch per table kind (not the cov
-// layout); words [n][H + E * W] and keys [n] by each descriptor's out_offset
+// rays_dev[k] belongs to descs_dev[k]; one launch per table kind; words
+// [n][H + E * W] and keys [n] by each descriptor's out_offset
 cudaError_t launch_project_rays(const ProjDesc* descs_dev, const RayDesc* rays_dev, const ProjDesc* descs_host,
                                 int n_desc, uint32_t total_tiles, int method, uint32_t* words, uint32_t* keys,
                                 cudaStream_t stream);
-bool ray_table_supported(const DevTable& t);
 
 }  // namespace rdx

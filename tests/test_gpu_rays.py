@@ -1,9 +1,10 @@
 """The ray projection methods (3dgut, htgs, raygs) on the GPU against the
 float64 oracle, through rdx_project_words: every head and eye word of the
 reference's layout (src/render/projections.tsl.ts:5-17) and the keys, for raw
-float32 / float16 tables, ext and packed tables with either SH codec, stereo,
-an orthographic eye, collections with rotated and uniformly scaled objects,
-per-object params, and keys without cull_keys.
+float32 / float16 tables, ext, packed and cov tables with either SH codec,
+stereo, an orthographic eye, collections with rotated and uniformly scaled
+objects, non-uniform and mirrored objects (through fromCov), per-object
+params, and keys without cull_keys.
 
 Both sides compute in float64 with the same operation order (the kernel's file
 is compiled without multiply-add contraction), so words are bit-equal except
@@ -114,17 +115,35 @@ def test_ewa_method_forwards_to_the_projection(ctx):
     assert np.array_equal(u32(w["keys"]), u32(p["keys"]))
 
 
+@pytest.mark.parametrize("method", METHODS)
+def test_non_uniform_and_mirrored_objects(ctx, method):
+    """Object matrices that are not a rotation times a uniform scale reach the
+    splat form through the covariance and fromCov's Jacobi eigen decomposition."""
+    d1 = syn.mixture_table(30_000, seed=49, sh_degree=2)
+    d2 = syn.plain_table(20_000, seed=50)
+    stretch = _world(0.5, 1.0, (0.2, 0.0, -0.3))
+    stretch[4:7] *= 1.8  # columns 1 and 2 scaled: R diag(1, 1.8, 0.6), a non-uniform scale
+    stretch[8:11] *= 0.6
+    mirror = _world(0.2, 1.0, (0.0, 0.1, -0.3))
+    mirror[0:3] = -mirror[0:3]  # the first column negated: a mirror
+    objs_gpu = [rb.SplatObject(cuda_table(d1), world=stretch), rb.SplatObject(cuda_table(d2), world=mirror)]
+    objs_orc = [rb.SplatObject(rb.Table.from_dict(d1), world=stretch), rb.SplatObject(rb.Table.from_dict(d2), world=mirror)]
+    check(objs_gpu, objs_orc, syn.scale_camera(), method, bits=24)
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("codec", ["ext", "packed"])
+def test_cov_tables(ctx, method, codec):
+    d = syn.mixture_table(30_000, seed=51, sh_degree=3)
+    d["opacities"][::7] = np.float32(1.5)
+    dev, hst = _tables(d, "cov", codec, False)
+    check([rb.SplatObject(dev)], [rb.SplatObject(hst)], syn.scale_camera(), method)
+    check([rb.SplatObject(dev)], [rb.SplatObject(hst)], syn.stereo_camera(), method, bits=16)
+
+
 def test_refusals(ctx):
     d = syn.mixture_table(5_000, seed=48, sh_degree=1)
     cam = syn.scale_camera()
-    stretch = np.diag([1.0, 2.0, 1.0, 1.0]).reshape(16)
-    with pytest.raises(_abi.RadixError) as e:
-        rb.project_words([rb.SplatObject(cuda_table(d), world=stretch)], cam, "htgs")
-    assert e.value.code == _abi.RDX_ERR_UNSUPPORTED
-    dev, _ = _tables(d, "cov", "ext", False)
-    with pytest.raises(_abi.RadixError) as e:
-        rb.project_words([rb.SplatObject(dev)], cam, "raygs")
-    assert e.value.code == _abi.RDX_ERR_UNSUPPORTED
     with pytest.raises(_abi.RadixError) as e:
         rb.project_words([rb.SplatObject(rb.Table.from_dict(d))], cam, "3dgut")  # host memory
     assert e.value.code == _abi.RDX_ERR_ARG
