@@ -34,6 +34,20 @@ def test_library_exports_every_declared_symbol():
         assert name in _abi.SIGNATURES, f"{name} has no ctypes signature"
 
 
+def test_method_words_match_the_reference_layouts():
+    """ProjectionDef.headWords + eyes * eyeWords (src/render/projections.tsl.ts:5-17; the
+    reference's test table at test/gpu/renderUtils.ts:116-117), and -1 out of range."""
+    head = {"ewa": 0, "3dgut": 6, "htgs": 6, "raygs": 4}
+    per_eye = {"ewa": 4, "3dgut": 2, "htgs": 2, "raygs": 3}
+    for name, method in rb.PROJECTION_METHODS.items():
+        for eyes in (1, 2):
+            assert _abi.lib().rdx_method_words(method, eyes) == head[name] + eyes * per_eye[name]
+        assert _abi.lib().rdx_method_words(method, 3) == -1
+    assert _abi.lib().rdx_method_words(4, 1) == -1
+    with pytest.raises(ValueError):
+        rb.method_words("raygs", 0)
+
+
 def test_version_and_default_params():
     assert _abi.lib().rdx_version() == 1
     p = _abi.rdx_params()

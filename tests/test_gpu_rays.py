@@ -24,7 +24,7 @@ from oracle import oracle as orc
 from radix_b200 import camera as cm
 from radix_b200 import synthetic as syn
 from tests import ray_words as rw
-from tests.parity import cuda_table, host, u32
+from tests.parity import cuda_table, u32
 from tests.test_gpu_layouts import _tables
 
 pytestmark = pytest.mark.gpu
