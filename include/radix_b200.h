@@ -387,8 +387,9 @@ int rdx_method_words(int method, int eyes);
  *   words  uint32 [n][rdx_method_words(method, E)]: the head words, then each
  *          eye's, in the reference's order (projections.tsl.ts:5-17); the
  *          reference's channel c (w<c>, a uint32x4 or uint32x2 texture) holds
- *          words 4c .. 4c + 3 of a row. A culled eye's words are zero, and so
- *          are the head words of a splat that no eye can show.
+ *          words 4c .. 4c + 3 of a row. A culled eye's words are zero; the
+ *          head words are zero when the head basis drops the splat (invisible,
+ *          or its blur-compensated opacity below min_alpha).
  *   keys   uint32 [n], as rdx_project's (cull_keys: keys of splats that no
  *          eye shows are invalid).
  * Either output may be NULL. ewa forwards to rdx_project (its words output).

@@ -4,18 +4,21 @@
 // Restates rayProjection with gutBound / htgsBound and raygs
 // (src/render/projections.tsl.ts:170-474), headBasis / viewBasis / mipInflate,
 // the bounds and their codecs (src/render/projection.tsl.ts:167-366),
-// transformUniform (src/render/splatTransform.tsl.ts:143-152) and
-// SplatProjection.project / write (src/render/SplatProjection.ts:126-153).
+// transformUniform and transformSplat (src/render/splatTransform.tsl.ts:
+// 117-162), fromCov with symEigens (src/gpu/splats.tsl.ts:189-199,
+// src/gpu/math.tsl.ts:46-112) and SplatProjection.project / write
+// (src/render/SplatProjection.ts:126-153).
 //
 // A row holds H head words, then W words per eye (H, W = 6, 2 for 3dgut and
-// htgs; 4, 3 for raygs), in the reference's word order; a culled eye's words
-// are zero, and so are the head words of a splat that no eye can show.
+// htgs; 4, 3 for raygs), in the reference's word order. A culled eye's words
+// are zero; the head words are zero when the head basis drops the splat
+// (invisible, or its MIP-compensated opacity below minAlpha).
 //
 // Precision: float64 throughout, rounded once into the words. This file is
 // compiled without contraction of multiplies and adds (--fmad=false), so
 // every arithmetic step rounds as the float64 CPU oracle's does; only the
-// library's transcendental functions (exp, log, sin, cos, atan2, acos, cbrt)
-// may differ from the host's by an ulp. The head-space centre, the key
+// library's transcendental functions (exp, log, log2, pow, sin, cos, atan2,
+// acos) may differ from the host's by an ulp. The head-space centre, the key
 // distance and the depth cull therefore equal the oracle's, and with them
 // the keys.
 #include <cuda_fp16.h>
