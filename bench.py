@@ -843,9 +843,10 @@ RAY_BYTES = {"3dgut": 236 + 8 * 4 + 4, "htgs": 236 + 8 * 4 + 4, "raygs": 236 + 7
 
 def run_rays(args, world, rank, local, device):
     """The ray projection methods (3dgut, htgs, raygs) on the frame's 4M SH-3
-    table and camera: each method's words and keys (rdx_project_words), timed
-    with CUDA events on the library's stream. A splat's algorithmic bytes: its
-    236 bytes of fields, read once, plus its words and key."""
+    table and camera: each method's words and keys (rdx_project_words), K
+    steps timed between barriers with CUDA events (the slowest rank's time),
+    one replica a GPU. A splat's algorithmic bytes: its 236 bytes of fields,
+    read once, plus its words and key."""
     import numpy as np
     import torch
 
@@ -861,29 +862,25 @@ def run_rays(args, world, rank, local, device):
                                        cols["colors"], SH_DEGREE))]
     cam = syn.scale_camera()
     peak, peak_kind = peak_hbm()
-    stream = torch.cuda.current_stream(device)
     results = {}
     launches0 = ctx.launches()
-    clocks = Clocks(local)  # sampled across the three methods' steps
+    clock_info = None
     for method in ("3dgut", "htgs", "raygs"):
         out = {"words": torch.empty((n, rb.method_words(method, 1)), dtype=torch.int32, device=device),
                "keys": torch.empty(n, dtype=torch.int32, device=device)}
-        times = []
-        for step in range(args.warmup + args.steps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            rb.project_words(obj, cam, method, None, BITS, True, ctx=ctx, out=out)
-            e1.record(stream)
-            torch.cuda.synchronize()
-            if step >= args.warmup:
-                times.append(e0.elapsed_time(e1))
-        ms = statistics.median(times)
+
+        def step(m=method, o=out):
+            rb.project_words(obj, cam, m, None, BITS, True, ctx=ctx, out=o)
+
+        ms_total, clocks = timed(step, args.steps, args.warmup, world, local)
+        if clock_info is None:
+            clock_info = clocks
+        ms = ms_total / args.steps
         gbs = RAY_BYTES[method] * n / (ms / 1e3) / 1e9
-        results[method] = {"ms": ms, "msplats_s": n / (ms / 1e3) / 1e6, "bytes_per_splat": RAY_BYTES[method],
-                           "gb_s": gbs, "frac": gbs / peak,
+        results[method] = {"ms": ms, "msplats_s": replicas_throughput(n, args.steps, world, ms_total),
+                           "bytes_per_splat": RAY_BYTES[method], "gb_s_per_gpu": gbs, "frac": gbs / peak,
                            "drawn": int((out["keys"] != -1).sum().item())}
         del out
-    clk = clocks.stop()
     ctx.synchronize()
     head = results["3dgut"]
     return {
@@ -891,12 +888,13 @@ def run_rays(args, world, rank, local, device):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 maths, u32 words",
         "data": "synthetic (seeded mulberry32)",
-        "config": {"workload": f"rays: {n} splats SH {SH_DEGREE} fp32, 1920x1080 fov 50, {BITS}-bit keys; "
-                               "each method timed alone (inputs larger than L2)", "methods": results},
-        "roofline": {"bound": "hbm", "achieved": head["gb_s"], "peak": peak, "unit": "GB/s", "frac": head["frac"],
-                     "traffic": ncu_traffic("project_rays_kernel_1m_sh3.md", n / 1_000_000), "kernel": "k_project_rays",
-                     "peak_kind": peak_kind},
-        "clocks": clk, "e2e": None, "e2e_note": "device-resident inputs",
+        "config": {"workload": f"rays: {n} splats a GPU, SH {SH_DEGREE} fp32, 1920x1080 fov 50, {BITS}-bit keys; "
+                               "each method timed alone (inputs larger than L2)", "parallelism": f"replicas x{world}",
+                   "methods": results},
+        "roofline": {"bound": "hbm", "achieved": head["gb_s_per_gpu"], "peak": peak, "unit": "GB/s",
+                     "frac": head["frac"], "traffic": ncu_traffic("project_rays_kernel_1m_sh3.md", n / 1_000_000),
+                     "kernel": "k_project_rays", "peak_kind": peak_kind},
+        "clocks": clock_info, "e2e": None, "e2e_note": "device-resident inputs",
         "gpu_launches": ctx.launches() - launches0,
     }
 
