@@ -6,7 +6,9 @@ against the ewa oracle: head words decode to the head-space centre, the bounds
 of small on-screen splats cover the ewa bound within a few per cent, keys
 follow the drawn eyes, and an object's matrix (uniform, non-uniform through
 fromCov, mirrored) equals its splats moved by it beforehand, within the
-reference's tolerances (test/gpu/sceneTests.ts:42-70, 120-141)."""
+reference's tolerances (test/gpu/sceneTests.ts:42-70, 120-141); and the
+reference's cull known answers and draw coverage run for every method
+(test/gpu/renderTests.ts:112-131, 302-321)."""
 import numpy as np
 import pytest
 
@@ -220,3 +222,47 @@ def test_small_distant_splats_agree_with_ewa():
         ndc, _, scales = rw.decode_bound(ew[:, 0], ew[:, 1])
         assert np.abs(ndc - e_ndc).max() <= 2.0 / 128, (method, np.abs(ndc - e_ndc).max())
         assert np.abs(scales[:, 0] / e_major - 1.0).max() <= 0.06, (method, np.abs(scales[:, 0] / e_major - 1.0).max())
+
+
+@pytest.mark.parametrize("method", METHODS)
+def test_culling_and_cull_keys_every_method(method):
+    """The reference's cull check runs for every method (test/gpu/renderTests.ts:302-321, the
+    known answers in tests/golden/kats.json): a splat in front is drawn; one behind the camera,
+    one far off screen and one under minAlpha are not; their keys are invalid with cullKeys, and
+    without it only the invisible one's."""
+    from tests.test_oracle_kats import KATS, _splat_table, _test_camera
+    k = KATS["culling"]
+    data = _splat_table(k["centers"], [[k["scale"]] * 3] * 4, opacities=k["opacities"])
+    obj = [rb.SplatObject(rb.Table.from_dict(data))]
+    cam = _test_camera((0, 0, 0))
+    invalid = orc.lib().orc_invalid_key(32)
+    for cull_keys, expected in ((True, k["invalid_cull_keys"]), (False, k["invalid_no_cull_keys"])):
+        r = orc.project_rays(obj, cam, method, rb.SplatParams(), 32, cull_keys)
+        assert [not bool(v) for v in rw.drawn(r["words"], method, 0)] == k["culled"]
+        assert [int(key) == invalid for key in r["keys"]] == expected
+
+
+@pytest.mark.parametrize("method", METHODS)
+@pytest.mark.parametrize("layout", ["ext", "cov", "packed"])
+def test_every_layout_and_eye_count_draws_most_splats_in_view(method, layout):
+    """The reference's check that every method and layout, with 1 and 2 eyes, draws at least half
+    of 3000 random splats in view (test/gpu/renderTests.ts:112-131): eyes at x = -0.03 and
+    +0.03, the head at the first eye."""
+    from radix_b200 import camera as cm
+    from tests.test_oracle_kats import random_test_splats
+    data = random_test_splats(3000, 3)
+    if layout == "ext":
+        a, b, _ = orc.encode_ext(data)
+        table = rb.Table.ext(a, b)
+    elif layout == "cov":
+        a, b = orc.encode_cov(data)
+        table = rb.Table.cov(a, b)
+    else:
+        table = rb.Table.packed(orc.encode_packed(data))
+    proj = cm.perspective(60.0, 2.0, 0.1, 100.0)
+    views = [cm.invert(cm.translation(x, 0.0, 0.0)) for x in (-0.03, 0.03)]
+    for eyes in (1, 2):
+        cam = rb.Camera(views[0], [(v, proj, False) for v in views[:eyes]], 128, 64)
+        w = orc.project_rays([rb.SplatObject(table)], cam, method, None, 32, True)["words"]
+        for e in range(eyes):
+            assert rw.drawn(w, method, e).sum() >= 0.5 * 3000, (layout, eyes, e, int(rw.drawn(w, method, e).sum()))
